@@ -1,0 +1,378 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 DEM packing step: particle-steps/s on the
+500,000-sphere lognormal random-sequential-addition workload (100x100x400 mm
+box, dt = 5e-7 s, re-list every 20 steps), mixed precision (FP32
+list/forces/accumulation, FP64 positions/velocities/tangential history).
+
+One bench step = one re-list window: the list build plus 20 DEM time steps,
+replayed as one CUDA graph.  The default K = 500 windows is the workload's
+full 10,000 steps from its initial state.  L2 is flushed (256 MiB write)
+between bench steps, outside the timed events; within a window the state
+stays as hot as it is in a real run.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (under torchrun): independent replicas, one per GPU (the step has no
+data-path exchange); time = max over ranks; value = all ranks' work / time.
+--impl reference: the CPU restatement of the reference step (the reference
+itself does not build: its force laws, four kernels and SDK sort/scan are not
+in its repository) on the host cores, one DEM step per bench step.
+"""
+import argparse
+import json
+import math
+import os
+import pathlib
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "discrete-element-method-for-packing-cuda-c-code_b200"
+BYTES_PER_PARTICLE = {"mixed": 172, "fp64": 200}   # per particle-step, all fields touched once
+BYTES_PER_PAIR = 56                                 # ids 8 + FP64 history r+w 48, per pair-step
+METRIC = "particle-steps/s @500K spheres"
+UNIT = "particle-steps/s"
+KERNELS_PER_WINDOW = 13 + 2 * 20   # re-list (incl. 3 scans x 3 launches) + 2 per step
+
+
+def load_pkg():
+    import importlib.util
+    if "dem_b200" in sys.modules:
+        return sys.modules["dem_b200"]
+    spec = importlib.util.spec_from_file_location("dem_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["dem_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch from a committed ncu summary (profiles/<name>.md)."""
+    p = ROOT / "profiles" / f"{name}.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(dem, precision, rank):
+    import dem_b200.workloads as w
+    return w.rsa_500k(seed=w.SEED + rank, precision=precision)
+
+
+def time_windows(torch, eng, stream, K, flush_buf, win):
+    """Per-window CUDA events on the engine's stream; L2 flush between windows
+    outside the events.  Returns total ms."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush_buf.zero_()
+            evs[k][0].record(stream)
+            eng.step(win)
+            evs[k][1].record(stream)
+    stream.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    dem = load_pkg()
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    precision = dem.PREC_MIXED if args.precision == "mixed" else dem.PREC_FP64
+    w = workload(dem, precision, rank)
+    win = w.relist_interval
+    K, W = args.steps, args.warmup
+    stream = torch.cuda.Stream(device=dev)
+    eng = dem.Engine(**w.engine_kwargs())
+    eng.set_stream(stream.cuda_stream)
+    eng.set_material(w.pp, w.pw)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    # warm-up from the initial state, then restart from it for the timed run
+    eng.upload(w.pos, w.rad)
+    for _ in range(W):
+        eng.step(win)
+    eng.scalars()
+    eng.upload(w.pos, w.rad)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    total_ms = time_windows(torch, eng, stream, K, flush, win)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    sc = eng.scalars()
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    dem_steps = K * win
+    value = w.n * dem_steps * ws / (max_ms / 1e3)
+
+    # --- dominant kernel duration (CUDA events around each launch, eager mode,
+    # same state continued for 3 windows)
+    eng.set_profiling(True)
+    with torch.cuda.stream(stream):
+        eng.step(3 * win)
+    stream.synchronize()
+    kt = eng.kernel_times()
+    eng.set_profiling(False)
+    peak, peak_kind = measured_peak()
+    bp = BYTES_PER_PARTICLE[args.precision]
+    part_bytes = w.n * bp
+    achieved = part_bytes / (kt["particle_ms"] / 1e3) / 1e9 if kt["particle_ms"] > 0 else None
+    pairs = sc["pairs"]
+    window_bytes = win * (w.n * bp + pairs * BYTES_PER_PAIR) + w.n * (24 + 8 + 16 + 4) + pairs * 64
+    traffic = profile_traffic(f"k_particle_rsa500k_{args.precision}")
+
+    # --- FP64 plain form of the same step (throughput bar for mixed)
+    fp64 = None
+    if args.precision == "mixed" and not args.skip_fp64:
+        e2 = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_FP64})
+        e2.set_stream(stream.cuda_stream)
+        e2.set_material(w.pp, w.pw)
+        e2.upload(w.pos, w.rad)
+        with torch.cuda.stream(stream):
+            e2.step(3 * win)
+        e2.upload(w.pos, w.rad)
+        k2 = max(10, K // 5)
+        ms2 = time_windows(torch, e2, stream, k2, flush, win)
+        s2 = e2.scalars()
+        e2.close()
+        v2 = w.n * k2 * win / (ms2 / 1e3)
+        fp64 = {"value": v2, "unit": UNIT, "windows": k2, "ms_per_window": ms2 / k2,
+                "mixed_over_fp64": value / ws / v2, "packing_fraction": s2["packing_fraction"],
+                "packing_fraction_mixed": sc["packing_fraction"]}
+
+    # --- end to end through the public API with host buffers: pinned host
+    # state -> dem_upload_state -> K windows with a scalar read-back each
+    # (dem_get_scalars, a host sync) -> final dem_download_state to pinned host
+    e2e = None
+    if not args.skip_e2e:
+        hp = torch.from_numpy(w.pos).pin_memory()
+        hr = torch.from_numpy(w.rad).pin_memory()
+        out = torch.empty(3 * w.n, dtype=torch.float64).pin_memory()
+        outd = torch.empty(3 * w.n, dtype=torch.float64).pin_memory()
+        outa = torch.empty(3 * w.n, dtype=torch.float64).pin_memory()
+        ke = max(10, K // 5)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(stream)
+        eng.upload(hp.numpy(), hr.numpy())
+        for _ in range(ke):
+            eng.step(win)
+            eng.scalars()
+        pos_o, pdis_o, angv_o = out.numpy(), outd.numpy(), outa.numpy()
+        from dem_b200 import _ptr, check, lib
+        check(lib().dem_download_state(eng.handle, _ptr(pos_o), _ptr(pdis_o), _ptr(angv_o)), "download")
+        b.record(stream)
+        stream.synchronize()
+        wall = time.perf_counter() - t0
+        ev_ms = a.elapsed_time(b)
+        e2e_s = max(wall, ev_ms / 1e3)
+        t2 = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        e2e_s = float(t2.item())
+        h2d = 3 * w.n * 8 + w.n * 8
+        d2h = 9 * w.n * 8 + ke * 64
+        e2e = {"value": w.n * ke * win * ws / e2e_s, "unit": UNIT, "windows": ke,
+               "h2d_bytes_per_step": h2d / ke, "d2h_bytes_per_step": d2h / ke,
+               "timing": "host wall clock and CUDA events, larger of the two"}
+
+    # --- CPU baseline: the FP64 oracle on this host's cores, bounded sample
+    cpu = None
+    if rank == 0 and ws == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(dem, w, args.cpu_steps)
+    eng.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic (seeded RSA packing)",
+        "config": {"workload": w.name, "n_particles": w.n, "box_mm": list(w.world), "dt_s": 5e-7,
+                   "dem_steps_per_bench_step": win, "dem_steps_timed": dem_steps, "precision": args.precision,
+                   "relist_interval": win, "skin_d": w.skin, "parallelism": f"replicas x{ws}",
+                   "l2": "flushed between bench steps (256 MiB write, outside the timed events)",
+                   "ms_per_dem_step": max_ms / dem_steps, "pairs_per_particle": pairs / w.n,
+                   "contacts_per_particle": sc["contacts"] / w.n, "packing_fraction": sc["packing_fraction"],
+                   "mean_cn": sc["mean_cn"]},
+        "roofline": {"bound": "hbm", "kernel": "k_particle", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": part_bytes,
+                     "kernel_ms": kt, "step_bytes_per_window": window_bytes,
+                     "step_achieved_gbs": window_bytes / (max_ms / K / 1e3) / 1e9},
+        "clocks": clk,
+        "gpu_launches": KERNELS_PER_WINDOW * K,
+        "fp64_plain": fp64,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(dem, w, steps):
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as orc
+    threads = orc.num_threads()
+    mat = dem.material_array(w.pp, w.pw)
+    st = orc.Stepper(w.pos, w.rad, w.world, w.dt, w.skin, w.cell(), w.density, mat,
+                     w.precision == dem.PREC_MIXED, w.relist_interval)
+    t0 = time.perf_counter()
+    st.step(steps)
+    dt = time.perf_counter() - t0
+    st.close()
+    return {"value": w.n * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} DEM steps ({steps // w.relist_interval} re-lists) of {w.name} from its initial "
+                      f"state, FP64 oracle, OpenMP {threads} threads"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    dem = load_pkg()
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as orc
+    import dem_b200.workloads as wmod
+    precision = dem.PREC_MIXED if args.precision == "mixed" else dem.PREC_FP64
+    w = wmod.rsa_500k(precision=precision)
+    threads = orc.num_threads()
+    mat = dem.material_array(w.pp, w.pw)
+    st = orc.Stepper(w.pos, w.rad, w.world, w.dt, w.skin, w.cell(), w.density, mat,
+                     precision == dem.PREC_MIXED, w.relist_interval)
+    for _ in range(args.warmup):
+        st.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st.step(1)
+    dt = time.perf_counter() - t0
+    st.close()
+    value = w.n * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RSA packing)",
+        "config": {"workload": w.name, "n_particles": w.n, "dem_steps_per_bench_step": 1,
+                   "note": "the reference repository does not build (calforceij/calforceiw, neighborarrayD, "
+                           "pairlistD, sumallforceiD, outputporositycnD and the SDK sort/scan are absent); this "
+                           "is its step restated in FP64 C++/OpenMP (oracle/dem_oracle.cpp)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} DEM steps of {w.name} after {args.warmup} warm-up steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--cpu-steps", type=int, default=60)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1159 @@
+// dem_engine.cu -- the context API: structure-of-arrays DEM step on sm_100a.
+//
+// Same physics and step order as the reference's loop (dempacking.cu:535-739:
+// re-list -> pair force -> gather -> wall + gravity -> integrate), laid out
+// for B200:
+//  * particle state as SoA planes (FP64 position / per-step displacement,
+//    working-precision rotation and radius, FP64 wall history) so every
+//    per-particle kernel streams fully coalesced 8/4-byte lanes;
+//  * the half contact-candidate list as CSR by particle id (j ascending per
+//    row) plus a reverse CSR of pair slots, replacing the fixed 30-slot Anei /
+//    Aref rows (dempacking.cu:21-22) -- the gather onto particles stays
+//    deterministic and atomic-free as in the reference;
+//  * re-list without a general sort: cell counting (atomics) -> scan ->
+//    scatter -> in-cell ranking by id, which is exactly the stable sort by
+//    cell of calcHash + RadixSort (dempacking.cu:545-555) and yields cell
+//    ranges directly (no cellStart memset);
+//  * the FP32 (mixed) or FP64 candidate test evaluated on a cell-sorted
+//    float4/double4 copy of (x, y, z, r);
+//  * history carry by binary search in the previous CSR row (pairlistD's
+//    contract, particleSystem.cu:143-191);
+//  * the wall, gravity and integrator fused into one per-particle kernel that
+//    also reduces the observables (max height, contacts) on the device;
+//  * a whole re-list window (re-list + K steps) captured once as a CUDA graph;
+//    no host synchronisation inside dem_step_n.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include "dem_common.cuh"
+#include "dem_law.cuh"
+
+namespace dem {
+
+enum : uint {
+    kStCapacity = 1u,
+    kStNonfinite = 2u,
+    kStSkin = 4u,
+};
+
+// device words: [0] status bits, [1] max row count
+struct EngineWords {
+    uint status;
+    uint max_row;
+    uint pad[2];
+};
+
+template <typename Real> struct Planes3 { Real* x; Real* y; Real* z; };
+
+// --------------------------------------------------------------- helpers
+template <typename Real> __device__ __forceinline__ Real mul_rn(Real a, Real b);
+template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
+template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
+template <typename Real> __device__ __forceinline__ Real add_rn(Real a, Real b);
+template <> __device__ __forceinline__ float add_rn<float>(float a, float b) { return __fadd_rn(a, b); }
+template <> __device__ __forceinline__ double add_rn<double>(double a, double b) { return __dadd_rn(a, b); }
+template <typename Real> __device__ __forceinline__ Real sub_rn(Real a, Real b);
+template <> __device__ __forceinline__ float sub_rn<float>(float a, float b) { return __fsub_rn(a, b); }
+template <> __device__ __forceinline__ double sub_rn<double>(double a, double b) { return __dsub_rn(a, b); }
+template <typename Real> __device__ __forceinline__ Real div_rn(Real a, Real b);
+template <> __device__ __forceinline__ float div_rn<float>(float a, float b) { return __fdiv_rn(a, b); }
+template <> __device__ __forceinline__ double div_rn<double>(double a, double b) { return __ddiv_rn(a, b); }
+
+struct GridC {
+    double ox, oy, oz;   // world origin
+    double cs;
+    int gx, gy, gz;      // grid size
+};
+
+// Cell coordinate on one axis.  FP32: xf = (float)(x - o), floorf(xf / cs);
+// FP64: floor((x - o) / cs).  Clamped to [0, g-1] (after a clamp of the
+// quotient to [-1, g] so far-away positions cannot overflow the int).
+template <typename Real> __device__ __forceinline__ int cell_axis(double x, double o, Real csr, int g, Real& xl) {
+    xl = (Real)(x - o);
+    Real v = div_rn<Real>(xl, csr);
+    v = v < (Real)-1 ? (Real)-1 : (v > (Real)g ? (Real)g : v);
+    int c = (int)floor(v);
+    return c < 0 ? 0 : (c > g - 1 ? g - 1 : c);
+}
+
+// Candidate test, every operation rounded on its own (no FMA contraction):
+// (dx*dx + dy*dy) + dz*dz < ((ri + rj) + skin)^2.
+template <typename Real> __device__ __forceinline__ bool cand_test(const R4<Real>& a, const R4<Real>& b, Real skin) {
+    Real dx = sub_rn<Real>(b.x, a.x), dy = sub_rn<Real>(b.y, a.y), dz = sub_rn<Real>(b.z, a.z);
+    Real d2 = add_rn<Real>(mul_rn<Real>(dx, dx), mul_rn<Real>(dy, dy));
+    d2 = add_rn<Real>(d2, mul_rn<Real>(dz, dz));
+    Real cut = add_rn<Real>(add_rn<Real>(a.w, b.w), skin);
+    return d2 < mul_rn<Real>(cut, cut);
+}
+
+__device__ __forceinline__ uint lane_id() { return threadIdx.x & 31; }
+
+// ------------------------------------------------------------ state I/O
+template <typename Real>
+__global__ void k_from_aos(long long n, const double* __restrict__ pos, const double* __restrict__ pdis,
+                           const double* __restrict__ angv, const double* __restrict__ rad, Planes3<double> P,
+                           Planes3<double> D, Planes3<Real> A, Real* __restrict__ R, float4* __restrict__ Q,
+                           Planes3<double> W) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    P.x[i] = pos[3 * i]; P.y[i] = pos[3 * i + 1]; P.z[i] = pos[3 * i + 2];
+    D.x[i] = pdis ? pdis[3 * i] : 0.0; D.y[i] = pdis ? pdis[3 * i + 1] : 0.0; D.z[i] = pdis ? pdis[3 * i + 2] : 0.0;
+    A.x[i] = angv ? (Real)angv[3 * i] : (Real)0;
+    A.y[i] = angv ? (Real)angv[3 * i + 1] : (Real)0;
+    A.z[i] = angv ? (Real)angv[3 * i + 2] : (Real)0;
+    R[i] = (Real)rad[i];
+    Q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    W.x[i] = 0.0; W.y[i] = 0.0; W.z[i] = 0.0;
+}
+
+template <typename Real>
+__global__ void k_to_aos(long long n, Planes3<double> P, Planes3<double> D, Planes3<Real> A, double* __restrict__ pos,
+                         double* __restrict__ pdis, double* __restrict__ angv) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (pos) { pos[3 * i] = P.x[i]; pos[3 * i + 1] = P.y[i]; pos[3 * i + 2] = P.z[i]; }
+    if (pdis) { pdis[3 * i] = D.x[i]; pdis[3 * i + 1] = D.y[i]; pdis[3 * i + 2] = D.z[i]; }
+    if (angv) { angv[3 * i] = (double)A.x[i]; angv[3 * i + 1] = (double)A.y[i]; angv[3 * i + 2] = (double)A.z[i]; }
+}
+
+// --------------------------------------------------------------- re-list
+// Cell key per particle (calcHashD's role, neiglist.cu:77-97) and per-cell
+// counts; resets the displacement-since-list q (dempacking.cu:541).
+template <typename Real>
+__global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count,
+                             float4* __restrict__ Q) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Real csr = (Real)g.cs;
+    Real xl;
+    int cx = cell_axis<Real>(P.x[i], g.ox, csr, g.gx, xl);
+    int cy = cell_axis<Real>(P.y[i], g.oy, csr, g.gy, xl);
+    int cz = cell_axis<Real>(P.z[i], g.oz, csr, g.gz, xl);
+    uint c = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
+    key[i] = c;
+    atomicAdd(&count[c], 1u);
+    float4 q = Q[i];
+    Q[i] = make_float4(0.f, 0.f, 0.f, q.w);
+}
+
+// Scatter ids into their cell's range; the count array returns to zero.
+__global__ void k_scatter(long long n, const uint* __restrict__ key, const uint* __restrict__ cstart,
+                          uint* __restrict__ count, uint* __restrict__ sid) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint c = key[i];
+    uint slot = cstart[c] + atomicSub(&count[c], 1u) - 1u;
+    sid[slot] = (uint)i;
+}
+
+// Order each cell's members by id (stable sort by cell) and build the
+// cell-sorted list coordinates (x, y, z, r) in the list precision.
+template <typename Real>
+__global__ void k_rank(long long n, const uint* __restrict__ key, const uint* __restrict__ cstart,
+                       const uint* __restrict__ sid, Planes3<double> P, const Real* __restrict__ R, GridC g,
+                       uint* __restrict__ sid2, R4<Real>* __restrict__ spos) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint i = sid[t];
+    const uint c = key[i];
+    const uint s = cstart[c], e = cstart[c + 1];
+    uint rank = 0;
+    for (uint u = s; u < e; u++) rank += (sid[u] < i) ? 1u : 0u;
+    sid2[s + rank] = i;
+    R4<Real> v;
+    v.x = (Real)(P.x[i] - g.ox);
+    v.y = (Real)(P.y[i] - g.oy);
+    v.z = (Real)(P.z[i] - g.oz);
+    v.w = R[i];
+    spos[s + rank] = v;
+}
+
+// Walk the 27 cells around sorted slot t and either count (FILL=false) or
+// write (FILL=true) candidates.  Returns (count of j>i, count of all).
+template <typename Real, bool FILL>
+__device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, uint c, GridC g,
+                                       const uint* __restrict__ cstart, const uint* __restrict__ sid2,
+                                       const R4<Real>* __restrict__ spos, Real skin, uint& nup, uint& nall,
+                                       uint* __restrict__ out, uint outcap) {
+    const int cx = (int)(c % (uint)g.gx);
+    const int cy = (int)((c / (uint)g.gx) % (uint)g.gy);
+    const int cz = (int)(c / ((uint)g.gx * (uint)g.gy));
+    nup = 0;
+    nall = 0;
+    for (int z = cz - 1; z <= cz + 1; z++) {
+        if (z < 0 || z >= g.gz) continue;
+        for (int y = cy - 1; y <= cy + 1; y++) {
+            if (y < 0 || y >= g.gy) continue;
+            const uint rowc = ((uint)z * (uint)g.gy + (uint)y) * (uint)g.gx;
+            const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < g.gx - 1 ? cx + 1 : g.gx - 1;
+            // cells x0..x1 of this row are contiguous in the sorted order
+            const uint s = cstart[rowc + x0], e = cstart[rowc + x1 + 1];
+            for (uint u = s; u < e; u++) {
+                if ((long long)u == t) continue;
+                const R4<Real> o = spos[u];
+                if (cand_test<Real>(me, o, skin)) {
+                    nall++;
+                    const uint j = sid2[u];
+                    if (j > i) {
+                        if (FILL && nup < outcap) out[nup] = j;
+                        nup++;
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <typename Real>
+__global__ void k_nbr_count(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
+                            const uint* __restrict__ key, const uint* __restrict__ cstart, GridC g, Real skin,
+                            uint* __restrict__ njgi, uint* __restrict__ njli, EngineWords* words) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    uint nall = 0;
+    if (t < n) {
+        const uint i = sid2[t];
+        uint nup;
+        walk27<Real, false>(t, i, spos[t], key[i], g, cstart, sid2, spos, skin, nup, nall, nullptr, 0);
+        njgi[i] = nup;
+        njli[i] = nall - nup;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nall = max(nall, __shfl_xor_sync(0xffffffffu, nall, o));
+    if (lane_id() == 0 && nall) atomicMax(&words->max_row, nall);
+}
+
+__device__ __forceinline__ void isort_u32(uint* a, uint len) {
+    for (uint s = 1; s < len; s++) {
+        uint v = a[s];
+        uint u = s;
+        while (u > 0 && a[u - 1] > v) { a[u] = a[u - 1]; u--; }
+        a[u] = v;
+    }
+}
+
+// Fill the CSR row of i (j>i ascending), carry the FP64 tangential history
+// from the previous list, record the reverse slots.
+template <typename Real>
+__global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
+                           const uint* __restrict__ key, const uint* __restrict__ cstart, GridC g, Real skin,
+                           const uint* __restrict__ off, const uint* __restrict__ roff, uint* __restrict__ njli,
+                           uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
+                           const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
+                           uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint total = off[n];
+    if ((long long)total > cap) {
+        if (t == 0) atomicOr(&words->status, kStCapacity);
+        return;
+    }
+    const uint i = sid2[t];
+    const uint b = off[i], e = off[i + 1];
+    uint nup, nall;
+    walk27<Real, true>(t, i, spos[t], key[i], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
+    isort_u32(ln + b, e - b);
+    const bool old_ok = (long long)ooff[n] <= cap;   // an overflowed old list carries nothing
+    const uint ob = old_ok ? ooff[i] : 0u, oe = old_ok ? ooff[i + 1] : 0u;
+    for (uint k = b; k < e; k++) {
+        const uint j = ln[k];
+        lp[k] = i;
+        // binary search j in the previous row of i (ascending)
+        uint lo = ob, hi = oe;
+        while (lo < hi) {
+            uint mid = (lo + hi) >> 1;
+            if (oln[mid] < j) lo = mid + 1; else hi = mid;
+        }
+        if (lo < oe && oln[lo] == j) {
+            H.x[k] = OH.x[lo]; H.y[k] = OH.y[lo]; H.z[k] = OH.z[lo];
+        } else {
+            H.x[k] = 0.0; H.y[k] = 0.0; H.z[k] = 0.0;
+        }
+        R4<Real> z4;
+        z4.x = z4.y = z4.z = z4.w = (Real)0;
+        pf[k] = z4;
+        const uint left = atomicSub(&njli[j], 1u);
+        if (left == 0u) {   // counts of the two walks disagree: cannot happen with the symmetric test
+            atomicOr(&words->status, kStCapacity);
+            continue;
+        }
+        rk[roff[j] + left - 1u] = k;
+    }
+}
+
+__global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, const uint* __restrict__ off,
+                           long long cap) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if ((long long)off[n] > cap) return;
+    isort_u32(rk + roff[i], roff[i + 1] - roff[i]);
+}
+
+// ------------------------------------------------------------ pair force
+// One thread per candidate pair (calculateforcepairD, neiglist.cu:156-233).
+// Geometry from FP64 positions; in the mixed form the overlap is formed as
+// (s^2 - d^2)/(s + d) in FP64 and rounded once, the rest of the law is FP32
+// except the FP64 history update.
+template <typename Real>
+__global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long long n, long long cap,
+                                              const uint* __restrict__ lp, const uint* __restrict__ ln,
+                                              Planes3<double> P, Planes3<double> D, Planes3<Real> A,
+                                              const Real* __restrict__ R, Planes3<double> H, LawParams<Real> pp,
+                                              Real inv_dt, Real density, R4<Real>* __restrict__ pf,
+                                              R4<Real>* __restrict__ pti, R4<Real>* __restrict__ ptj) {
+    const uint total = off[n];
+    if ((long long)total > cap) return;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total; k += stride) {
+        const uint i = lp[k], j = ln[k];
+        const V3<double> xi = mk(P.x[i], P.y[i], P.z[i]), xj = mk(P.x[j], P.y[j], P.z[j]);
+        const V3<double> Dv = xj - xi;
+        const double d2 = dot(Dv, Dv);
+        const Real ri = R[i], rj = R[j];
+        const double s = (double)ri + (double)rj;
+        const double dist = sqrt(d2);
+        Real delta;
+        if (sizeof(Real) == 4) delta = (Real)((s * s - d2) / (s + dist));
+        else delta = (Real)(s - dist);
+        R4<Real> fo;
+        if (delta > (Real)0 && dist > 0.0) {
+            const double inv = 1.0 / dist;
+            const V3<Real> nn = cvt<Real>(Dv * inv);
+            const Real rstar = ri * rj / (ri + rj);
+            const Real mi = density * (Real)8 * ri * ri * ri, mj = density * (Real)8 * rj * rj * rj;
+            const Real mstar = mi * mj / (mi + mj);
+            const V3<Real> ai = mk(A.x[i], A.y[i], A.z[i]), aj = mk(A.x[j], A.y[j], A.z[j]);
+            const V3<double> dd = mk(D.x[j] - D.x[i], D.y[j] - D.y[i], D.z[j] - D.z[i]);
+            const V3<Real> U = cvt<Real>(dd) - cross(ri * ai + rj * aj, nn);
+            V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
+            V3<Real> Fi, Ft, Mr;
+            contact_law<Real>(delta, nn, rstar, mstar, U, ai - aj, h, inv_dt, pp, Fi, Ft, Mr);
+            const V3<Real> nxf = cross(nn, Ft);
+            const V3<Real> Ti = ri * nxf + Mr, Tj = rj * nxf - Mr;
+            H.x[k] = h.x; H.y[k] = h.y; H.z[k] = h.z;
+            fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
+            R4<Real> a4, b4;
+            a4.x = Ti.x; a4.y = Ti.y; a4.z = Ti.z; a4.w = (Real)0;
+            b4.x = Tj.x; b4.y = Tj.y; b4.z = Tj.z; b4.w = (Real)0;
+            pti[k] = a4;
+            ptj[k] = b4;
+        } else {
+            H.x[k] = 0.0; H.y[k] = 0.0; H.z[k] = 0.0;
+            fo.x = fo.y = fo.z = fo.w = (Real)0;
+        }
+        pf[k] = fo;
+    }
+}
+
+// --------------------------------------------------- particle update
+// Gather (sumallforceiD's role) + gravity + walls (calculateforceiwD,
+// neiglist.cu:238-306) + integrator (updatepositionD, neiglist.cu:308-409),
+// one thread per particle, with the block reductions of max height, contact
+// count and status flags finished on the device.
+struct StepSlot { unsigned long long maxhz_bits; unsigned long long contacts; };
+
+template <typename Real>
+__global__ void __launch_bounds__(256) k_particle(long long n, const uint* __restrict__ off,
+                                                  const uint* __restrict__ roff, const uint* __restrict__ rk,
+                                                  long long cap, const R4<Real>* __restrict__ pf,
+                                                  const R4<Real>* __restrict__ pti, const R4<Real>* __restrict__ ptj,
+                                                  Planes3<double> P, Planes3<double> D, Planes3<Real> A,
+                                                  const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
+                                                  LawParams<Real> pw, double dt, Real dtr, Real inv_dt, Real density,
+                                                  double hx, double hy, float half_skin2, StepSlot* slot,
+                                                  EngineWords* words, double* dbgF, double* dbgT, uint* dbgC) {
+    __shared__ unsigned long long s_mz[8];
+    __shared__ uint s_cnt[8], s_fl[8];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    if (i < n) {
+        V3<Real> F = zero3<Real>(), T = zero3<Real>();
+        const uint total = off[n];
+        if ((long long)total <= cap) {
+            const uint o0 = off[i], o1 = off[i + 1];
+            for (uint k = o0; k < o1; k++) {
+                const R4<Real> f = pf[k];
+                if (f.w != (Real)0) {
+                    const R4<Real> t = pti[k];
+                    F.x += f.x; F.y += f.y; F.z += f.z;
+                    T.x += t.x; T.y += t.y; T.z += t.z;
+                    cnt++;
+                }
+            }
+            const uint r0 = roff[i], r1 = roff[i + 1];
+            for (uint u = r0; u < r1; u++) {
+                const uint k = rk[u];
+                if (k >= total) continue;
+                const R4<Real> f = pf[k];
+                if (f.w != (Real)0) {
+                    const R4<Real> t = ptj[k];
+                    F.x -= f.x; F.y -= f.y; F.z -= f.z;
+                    T.x += t.x; T.y += t.y; T.z += t.z;
+                    cnt++;
+                }
+            }
+        }
+        const Real r = R[i];
+        const Real m = density * (Real)8 * r * r * r;
+        const Real I = (Real)0.4 * m * (r * r);
+        F.z += -m;
+        V3<double> x = mk(P.x[i], P.y[i], P.z[i]);
+        V3<double> d = mk(D.x[i], D.y[i], D.z[i]);
+        V3<Real> a = mk(A.x[i], A.y[i], A.z[i]);
+        float4 q = Q[i];
+        uint wflag = __float_as_uint(q.w);
+        const double rd = (double)r;
+        const bool touch = (x.z < rd) || (x.x + hx < rd) || (hx - x.x < rd) || (x.y + hy < rd) || (hy - x.y < rd);
+        if (touch || wflag) {
+            V3<double> h = wflag ? mk(W.x[i], W.y[i], W.z[i]) : zero3<double>();
+            const int hit = wall_contacts<Real>(hx, hy, x, cvt<Real>(d), a, r, m, h, inv_dt, pw, F, T, (Real*)nullptr);
+            if (hit || wflag) { W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z; }
+            wflag = hit ? 1u : 0u;
+        }
+        // symplectic Euler in displacement form (neiglist.cu:356-360)
+        d.x = d.x + (double)F.x * dt * dt / (double)m;
+        d.y = d.y + (double)F.y * dt * dt / (double)m;
+        d.z = d.z + (double)F.z * dt * dt / (double)m;
+        x.x += d.x; x.y += d.y; x.z += d.z;
+        a.x = a.x + T.x * dtr * dtr / I;
+        a.y = a.y + T.y * dtr * dtr / I;
+        a.z = a.z + T.z * dtr * dtr / I;
+        q.x += (float)d.x; q.y += (float)d.y; q.z += (float)d.z;
+        q.w = __uint_as_float(wflag);
+        P.x[i] = x.x; P.y[i] = x.y; P.z[i] = x.z;
+        D.x[i] = d.x; D.y[i] = d.y; D.z[i] = d.z;
+        A.x[i] = a.x; A.y[i] = a.y; A.z[i] = a.z;
+        Q[i] = q;
+        if (q.x * q.x + q.y * q.y + q.z * q.z > half_skin2) flags |= kStSkin;
+        if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
+        mz = x.z > 0.0 ? x.z : 0.0;
+        if (dbgF) {
+            dbgF[3 * i] = F.x; dbgF[3 * i + 1] = F.y; dbgF[3 * i + 2] = F.z;
+            dbgT[3 * i] = T.x; dbgT[3 * i + 1] = T.y; dbgT[3 * i + 2] = T.z;
+            dbgC[i] = cnt;
+        }
+    }
+    unsigned long long mb = (unsigned long long)__double_as_longlong(mz);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long ob = __shfl_xor_sync(0xffffffffu, mb, o);
+        mb = ob > mb ? ob : mb;
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        flags |= __shfl_xor_sync(0xffffffffu, flags, o);
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane_id() == 0) { s_mz[warp] = mb; s_cnt[warp] = cnt; s_fl[warp] = flags; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int w = 1; w < nw; w++) { mb = s_mz[w] > mb ? s_mz[w] : mb; cnt += s_cnt[w]; flags |= s_fl[w]; }
+        if (mb) atomicMax(&slot->maxhz_bits, mb);
+        if (cnt) atomicAdd(&slot->contacts, (unsigned long long)cnt);
+        if (flags) atomicOr(&words->status, flags);
+    }
+}
+
+__global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned long long* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double r = i < n ? rad[i] : 0.0;
+    unsigned long long b = (unsigned long long)__double_as_longlong(r > 0.0 ? r : 0.0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+        b = ob > b ? ob : b;
+    }
+    if (lane_id() == 0 && b) atomicMax(out, b);
+}
+
+__global__ void k_vol(long long n, const double* __restrict__ rad, double* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < n) { const double r = rad[i]; v = r * r * r; }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane_id() == 0 && v != 0.0) atomicAdd(out, v);
+}
+
+__global__ void k_pairs_out(const uint* __restrict__ off, long long n, long long cap, const uint* __restrict__ lp,
+                            const uint* __restrict__ ln, Planes3<double> H, uint* __restrict__ olp, uint* __restrict__ oln,
+                            double* __restrict__ oh) {
+    const uint total = off[n];
+    if ((long long)total > cap) return;
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long long)total) return;
+    olp[k] = lp[k];
+    oln[k] = ln[k];
+    oh[3 * k] = H.x[k]; oh[3 * k + 1] = H.y[k]; oh[3 * k + 2] = H.z[k];
+}
+
+}  // namespace dem
+
+using namespace dem;
+
+// ===================================================================== ctx
+struct dem_ctx {
+    dem_config cfg{};
+    int prec = DEM_PREC_MIXED;
+    long long n = 0, npad = 0, cap = 0;
+    int device = 0;
+    cudaStream_t stream = 0;
+    cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one
+    cudaEvent_t ext_ready = nullptr;  // orders legacy-stream work before device uploads
+    dem_material mat{};
+    bool have_mat = false;
+    // grid
+    GridC grid{};
+    long long ncells = 0;
+    double rmax = 0.0;
+    double vol = 0.0;        // sum (4/3) pi r^3
+    // state
+    double* pos = nullptr;   // 3 planes
+    double* disp = nullptr;  // 3 planes
+    void* ang = nullptr;     // 3 planes, Real
+    void* rad = nullptr;     // Real
+    float4* q = nullptr;
+    double* wh = nullptr;    // 3 planes
+    double* staging = nullptr;   // 10n doubles
+    // list
+    uint* key = nullptr;
+    uint* sid = nullptr;
+    uint* sid2 = nullptr;
+    void* spos = nullptr;
+    uint* ccount = nullptr;
+    uint* cstart = nullptr;
+    uint* njgi = nullptr;
+    uint* njli = nullptr;
+    uint* off[2] = {nullptr, nullptr};
+    uint* roff = nullptr;
+    uint* ln[2] = {nullptr, nullptr};
+    uint* lp = nullptr;
+    double* hist[2] = {nullptr, nullptr};  // 3 planes of cap
+    uint* rk = nullptr;
+    void* pf = nullptr;
+    void* pti = nullptr;
+    void* ptj = nullptr;
+    uint* scan_tmp = nullptr;
+    size_t scan_words = 0;
+    // scalars
+    EngineWords* words = nullptr;
+    StepSlot* slots = nullptr;       // relist_interval slots
+    unsigned long long* rmax_bits = nullptr;
+    void* host_pinned = nullptr;     // mirror for scalars
+    // debug force record
+    bool record = false;
+    double* dbgF = nullptr;
+    double* dbgT = nullptr;
+    uint* dbgC = nullptr;
+    // schedule
+    int cur = 0;
+    long long step = 0, in_window = 0, relists = 0;
+    int last_slot = -1;
+    bool uploaded = false;
+    // graphs (window starting from list buffer 0 or 1)
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    // profiling
+    bool profiling = false;
+    double ktime[3] = {0, 0, 0};
+    long long kcount[3] = {0, 0, 0};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+template <typename T> int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    DEM_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+    return DEM_OK;
+}
+
+template <typename Real> Planes3<Real> planes(void* base, long long npad) {
+    Real* b = (Real*)base;
+    return Planes3<Real>{b, b + npad, b + 2 * npad};
+}
+
+void free_graphs(dem_ctx* c) {
+    for (int s = 0; s < 2; s++)
+        if (c->gexec[s]) { cudaGraphExecDestroy(c->gexec[s]); c->gexec[s] = nullptr; }
+}
+
+void free_cells(dem_ctx* c) {
+    if (c->ccount) cudaFree(c->ccount);
+    if (c->cstart) cudaFree(c->cstart);
+    c->ccount = c->cstart = nullptr;
+}
+
+template <typename Real> int launch_relist(dem_ctx* c, int src) {
+    const long long n = c->n, np = c->npad;
+    const int dst = 1 - src;
+    const int B = 256;
+    cudaStream_t s = c->stream;
+    Planes3<double> P = planes<double>(c->pos, np);
+    GridC g = c->grid;
+    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount, c->q);
+    int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
+    if (rc) return rc;
+    k_scatter<<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->ccount, c->sid);
+    k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->sid, P, (const Real*)c->rad, g, c->sid2,
+                                              (R4<Real>*)c->spos);
+    const Real skin = (Real)c->cfg.skin;
+    k_nbr_count<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->key, c->cstart, g, skin,
+                                                   c->njgi, c->njli, c->words);
+    rc = exclusive_scan_u32(c->njgi, c->off[dst], n, c->off[dst] + n, c->scan_tmp, s);
+    if (rc) return rc;
+    rc = exclusive_scan_u32(c->njli, c->roff, n, c->roff + n, c->scan_tmp, s);
+    if (rc) return rc;
+    k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
+        n, c->sid2, (const R4<Real>*)c->spos, c->key, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
+        c->lp, planes<double>(c->hist[dst], c->cap), c->off[src], c->ln[src], planes<double>(c->hist[src], c->cap),
+        c->rk, (R4<Real>*)c->pf, c->cap, c->words);
+    k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->off[dst], c->cap);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+template <typename Real> int launch_pair(dem_ctx* c, int lst) {
+    const long long np = c->npad;
+    LawParams<Real> pp = make_law<Real>(c->mat.pp);
+    long long want = (c->cap + 255) / 256;
+    unsigned grid = (unsigned)std::min<long long>(std::max<long long>(want, 1), 148LL * 8);
+    k_pair<Real><<<grid, 256, 0, c->stream>>>(c->off[lst], c->n, c->cap, c->lp, c->ln[lst], planes<double>(c->pos, np),
+                                               planes<double>(c->disp, np), planes<Real>(c->ang, np),
+                                               (const Real*)c->rad, planes<double>(c->hist[lst], c->cap), pp,
+                                               (Real)(1.0 / c->cfg.dt), (Real)c->cfg.density, (R4<Real>*)c->pf,
+                                               (R4<Real>*)c->pti, (R4<Real>*)c->ptj);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
+    const long long n = c->n, np = c->npad;
+    LawParams<Real> pw = make_law<Real>(c->mat.pw);
+    const double dt = c->cfg.dt;
+    const float hs = (float)(0.5 * c->cfg.skin);
+    k_particle<Real><<<grid_for(n, 256), 256, 0, c->stream>>>(
+        n, c->off[lst], c->roff, c->rk, c->cap, (const R4<Real>*)c->pf, (const R4<Real>*)c->pti,
+        (const R4<Real>*)c->ptj, planes<double>(c->pos, np), planes<double>(c->disp, np), planes<Real>(c->ang, np),
+        (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw, dt, (Real)dt, (Real)(1.0 / dt),
+        (Real)c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, hs * hs, c->slots + slot, c->words,
+        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+int relist(dem_ctx* c, int src) {
+    return c->prec == DEM_PREC_MIXED ? launch_relist<float>(c, src) : launch_relist<double>(c, src);
+}
+int pair_step(dem_ctx* c, int lst) {
+    return c->prec == DEM_PREC_MIXED ? launch_pair<float>(c, lst) : launch_pair<double>(c, lst);
+}
+int particle_step(dem_ctx* c, int lst, int slot) {
+    return c->prec == DEM_PREC_MIXED ? launch_particle<float>(c, lst, slot) : launch_particle<double>(c, lst, slot);
+}
+
+// Enqueue one full window (re-list from list `src`, then K steps) on c->stream.
+int enqueue_window(dem_ctx* c, int src) {
+    const int K = c->cfg.relist_interval;
+    DEM_CUDA_TRY(cudaMemsetAsync(c->slots, 0, (size_t)K * sizeof(StepSlot), c->stream));
+    int rc = relist(c, src);
+    if (rc) return rc;
+    const int lst = 1 - src;
+    for (int s = 0; s < K; s++) {
+        rc = pair_step(c, lst);
+        if (rc) return rc;
+        rc = particle_step(c, lst, s);
+        if (rc) return rc;
+    }
+    return DEM_OK;
+}
+
+int build_graph(dem_ctx* c, int src) {
+    if (c->gexec[src]) return DEM_OK;
+    cudaGraph_t g = nullptr;
+    DEM_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_window(c, src);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&c->gexec[src], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return DEM_OK;
+}
+
+int ev_ms(cudaEvent_t a, cudaEvent_t b, double* out) {
+    float ms = 0.f;
+    DEM_CUDA_TRY(cudaEventSynchronize(b));
+    DEM_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+    *out = ms;
+    return DEM_OK;
+}
+
+size_t real_size(int prec) { return prec == DEM_PREC_MIXED ? sizeof(float) : sizeof(double); }
+
+}  // namespace
+
+extern "C" {
+
+int dem_create(const dem_config* cfg, dem_ctx** out) {
+    if (!cfg || !out) return fail(DEM_ERR_ARG, "dem_create: null argument");
+    *out = nullptr;
+    if (cfg->n <= 0 || cfg->n > 0x7fffffffLL) return fail(DEM_ERR_ARG, "dem_create: n out of range (%lld)", cfg->n);
+    if (cfg->precision != DEM_PREC_FP64 && cfg->precision != DEM_PREC_MIXED)
+        return fail(DEM_ERR_ARG, "dem_create: unknown precision %d", cfg->precision);
+    if (cfg->relist_interval <= 0 || cfg->relist_interval > 100000)
+        return fail(DEM_ERR_ARG, "dem_create: relist_interval must be in [1, 100000]");
+    if (!(cfg->dt > 0.0) || !(cfg->skin > 0.0) || !(cfg->density > 0.0))
+        return fail(DEM_ERR_ARG, "dem_create: dt, skin and density must be > 0");
+    for (int a = 0; a < 3; a++)
+        if (!(cfg->world[a] > 0.0)) return fail(DEM_ERR_ARG, "dem_create: world sizes must be > 0");
+    dem_ctx* c = new dem_ctx();
+    c->cfg = *cfg;
+    c->prec = cfg->precision;
+    c->n = cfg->n;
+    c->npad = (cfg->n + 63) / 64 * 64;
+    c->cap = cfg->pair_capacity > 0 ? cfg->pair_capacity : 8 * cfg->n;
+    if (c->cap > 0x7fffffffLL) c->cap = 0x7fffffffLL;
+    int rc = DEM_OK;
+    auto bail = [&](int code) { dem_destroy(c); return code; };
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaGetDevice", __FILE__, __LINE__));
+    const long long n = c->n, np = c->npad, cap = c->cap;
+    const size_t rs = real_size(c->prec);
+    if ((rc = dalloc(&c->pos, 3 * np)) || (rc = dalloc(&c->disp, 3 * np)) || (rc = dalloc(&c->wh, 3 * np)) ||
+        (rc = dalloc(&c->q, np)) || (rc = dalloc(&c->staging, 10 * np)) || (rc = dalloc(&c->key, np)) ||
+        (rc = dalloc(&c->sid, np)) || (rc = dalloc(&c->sid2, np)) || (rc = dalloc(&c->njgi, np)) ||
+        (rc = dalloc(&c->njli, np)) || (rc = dalloc(&c->off[0], np + 1)) || (rc = dalloc(&c->off[1], np + 1)) ||
+        (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
+        (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->hist[0], 3 * cap)) || (rc = dalloc(&c->hist[1], 3 * cap)) ||
+        (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->words, 1)) ||
+        (rc = dalloc(&c->slots, (size_t)cfg->relist_interval)) || (rc = dalloc(&c->rmax_bits, 2)))
+        return bail(rc);
+    e = cudaMalloc(&c->ang, 3 * np * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&c->rad, np * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&c->spos, np * 4 * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&c->pf, cap * 4 * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&c->pti, cap * 4 * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&c->ptj, cap * 4 * rs);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->host_pinned, 4096);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (engine buffers)", __FILE__, __LINE__));
+    (void)n;
+    c->scan_words = scan_scratch_words(std::max<long long>(np + 1, 1));
+    if ((rc = dalloc(&c->scan_tmp, c->scan_words))) return bail(rc);
+    e = cudaMemset(c->words, 0, sizeof(EngineWords));
+    if (e == cudaSuccess) e = cudaMemset(c->off[0], 0, (np + 1) * sizeof(uint));
+    if (e == cudaSuccess) e = cudaMemset(c->off[1], 0, (np + 1) * sizeof(uint));
+    if (e == cudaSuccess) e = cudaMemset(c->roff, 0, (np + 1) * sizeof(uint));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (engine init)", __FILE__, __LINE__));
+    for (int k = 0; k < 4; k++) {
+        e = cudaEventCreate(&c->ev[k]);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaEventCreate", __FILE__, __LINE__));
+    }
+    e = cudaEventCreateWithFlags(&c->ext_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__));
+    c->stream = c->own_stream;
+    *out = c;
+    return DEM_OK;
+}
+
+int dem_destroy(dem_ctx* c) {
+    if (!c) return DEM_OK;
+    cudaStreamSynchronize(c->stream);
+    free_graphs(c);
+    free_cells(c);
+    void* ptrs[] = {c->pos, c->disp, c->ang, c->rad, c->q, c->wh, c->staging, c->key, c->sid, c->sid2, c->spos,
+                    c->njgi, c->njli, c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0],
+                    c->hist[1], c->rk, c->pf, c->pti, c->ptj, c->scan_tmp, c->words, c->slots, c->rmax_bits,
+                    c->dbgF, c->dbgT, c->dbgC};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    for (int k = 0; k < 4; k++)
+        if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+    if (c->ext_ready) cudaEventDestroy(c->ext_ready);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return DEM_OK;
+}
+
+int dem_set_stream(dem_ctx* c, void* s) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_set_stream: null ctx");
+    cudaStream_t ns = s ? (cudaStream_t)s : c->own_stream;
+    if (ns != c->stream) {
+        DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        free_graphs(c);
+    }
+    c->stream = ns;
+    return DEM_OK;
+}
+
+int dem_set_material(dem_ctx* c, const dem_material* m) {
+    if (!c || !m) return fail(DEM_ERR_ARG, "dem_set_material: null argument");
+    const dem_contact* cs[2] = {&m->pp, &m->pw};
+    for (const dem_contact* k : cs) {
+        if (!(k->estar > 0.0) || k->mu < 0.0 || !(k->nu < 1.0) || k->damp_n < 0.0 || k->damp_t < 0.0 ||
+            k->roll < 0.0 || k->roll_rel < 0.0)
+            return fail(DEM_ERR_ARG, "dem_set_material: out-of-range contact parameter");
+    }
+    c->mat = *m;
+    c->have_mat = true;
+    free_graphs(c);   // parameters are baked into captured kernels
+    return DEM_OK;
+}
+
+static int setup_grid(dem_ctx* c) {
+    const double cs = c->cfg.cell > 0.0 ? c->cfg.cell : 2.0 * c->rmax + c->cfg.skin + 1e-4;
+    if (!(cs >= 2.0 * c->rmax + c->cfg.skin))
+        return fail(DEM_ERR_ARG, "cell %.6g smaller than 2*r_max+skin = %.6g", cs, 2.0 * c->rmax + c->cfg.skin);
+    GridC g;
+    g.ox = -c->cfg.world[0] * 0.5;
+    g.oy = -c->cfg.world[1] * 0.5;
+    g.oz = 0.0;
+    g.cs = cs;
+    g.gx = (int)(c->cfg.world[0] / cs) + 1;
+    g.gy = (int)(c->cfg.world[1] / cs) + 1;
+    g.gz = (int)(c->cfg.world[2] / cs) + 1;
+    const long long nc = (long long)g.gx * g.gy * g.gz;
+    if (nc > 0x7fffffffLL) return fail(DEM_ERR_ARG, "grid of %lld cells too large", nc);
+    if (nc != c->ncells) {
+        free_graphs(c);
+        free_cells(c);
+        int rc;
+        if ((rc = dalloc(&c->ccount, nc)) || (rc = dalloc(&c->cstart, nc + 1))) return rc;
+        DEM_CUDA_TRY(cudaMemsetAsync(c->ccount, 0, nc * sizeof(uint), c->stream));
+        c->ncells = nc;
+        size_t need = scan_scratch_words(std::max<long long>(nc, c->npad + 1));
+        if (need > c->scan_words) {
+            DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            cudaFree(c->scan_tmp);
+            c->scan_tmp = nullptr;
+            if ((rc = dalloc(&c->scan_tmp, need))) return rc;
+            c->scan_words = need;
+        }
+    }
+    if (g.cs != c->grid.cs || g.gx != c->grid.gx || g.gy != c->grid.gy || g.gz != c->grid.gz) free_graphs(c);
+    c->grid = g;
+    return DEM_OK;
+}
+
+static int finish_upload(dem_ctx* c) {
+    // fresh start: empty previous list, zero histories, re-list on next step
+    DEM_CUDA_TRY(cudaMemsetAsync(c->off[0], 0, (c->npad + 1) * sizeof(uint), c->stream));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->off[1], 0, (c->npad + 1) * sizeof(uint), c->stream));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->words, 0, sizeof(EngineWords), c->stream));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->slots, 0, (size_t)c->cfg.relist_interval * sizeof(StepSlot), c->stream));
+    c->cur = 0;
+    c->step = 0;
+    c->in_window = 0;
+    c->relists = 0;
+    c->last_slot = -1;
+    c->uploaded = true;
+    return setup_grid(c);
+}
+
+static int upload_common(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad,
+                         bool host) {
+    if (!c || !pos || !rad) return fail(DEM_ERR_ARG, "dem_upload_state: null argument");
+    const long long n = c->n, np = c->npad;
+    double* st = c->staging;
+    double *spos = st, *sd = st + 3 * np, *sa = st + 6 * np, *sr = st + 9 * np;
+    const double *ppos = pos, *ppd = pdis, *ppa = angv, *prad = rad;
+    if (host) {
+        DEM_CUDA_TRY(cudaMemcpyAsync(spos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if (pdis) DEM_CUDA_TRY(cudaMemcpyAsync(sd, pdis, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if (angv) DEM_CUDA_TRY(cudaMemcpyAsync(sa, angv, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        DEM_CUDA_TRY(cudaMemcpyAsync(sr, rad, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        ppos = spos; ppd = pdis ? sd : nullptr; ppa = angv ? sa : nullptr; prad = sr;
+        double rm = 0.0, v3 = 0.0;
+        for (long long i = 0; i < n; i++) {
+            if (!(rad[i] > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state: radius %lld not positive", i);
+            rm = std::max(rm, rad[i]);
+            v3 += rad[i] * rad[i] * rad[i];
+        }
+        c->rmax = rm;
+        c->vol = 4.0 / 3.0 * M_PI * v3;
+    } else {
+        // the caller's buffers may have been written on the legacy stream
+        DEM_CUDA_TRY(cudaEventRecord(c->ext_ready, 0));
+        DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ext_ready, 0));
+        DEM_CUDA_TRY(cudaMemsetAsync(c->rmax_bits, 0, 2 * sizeof(unsigned long long), c->stream));
+        k_rmax<<<grid_for(n, 256), 256, 0, c->stream>>>(n, rad, c->rmax_bits);
+        k_vol<<<grid_for(n, 256), 256, 0, c->stream>>>(n, rad, reinterpret_cast<double*>(c->rmax_bits + 1));
+        DEM_LAUNCH_CHECK();
+        unsigned long long b[2] = {0, 0};
+        DEM_CUDA_TRY(cudaMemcpyAsync(c->host_pinned, c->rmax_bits, sizeof(b), cudaMemcpyDeviceToHost, c->stream));
+        DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        memcpy(b, c->host_pinned, sizeof(b));
+        memcpy(&c->rmax, &b[0], sizeof(double));
+        double v3;
+        memcpy(&v3, &b[1], sizeof(double));
+        c->vol = 4.0 / 3.0 * M_PI * v3;
+        if (!(c->rmax > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state_device: radii not positive");
+    }
+    if (c->prec == DEM_PREC_MIXED)
+        k_from_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(
+            n, ppos, ppd, ppa, prad, planes<double>(c->pos, np), planes<double>(c->disp, np), planes<float>(c->ang, np),
+            (float*)c->rad, c->q, planes<double>(c->wh, np));
+    else
+        k_from_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(
+            n, ppos, ppd, ppa, prad, planes<double>(c->pos, np), planes<double>(c->disp, np),
+            planes<double>(c->ang, np), (double*)c->rad, c->q, planes<double>(c->wh, np));
+    DEM_LAUNCH_CHECK();
+    return finish_upload(c);
+}
+
+int dem_upload_state(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
+    return upload_common(c, pos, pdis, angv, rad, true);
+}
+int dem_upload_state_device(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
+    return upload_common(c, pos, pdis, angv, rad, false);
+}
+
+static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, bool host) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_download_state: null ctx");
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_download_state: no state uploaded");
+    const long long n = c->n, np = c->npad;
+    double* st = c->staging;
+    double *tp = host ? st : pos, *td = host ? st + 3 * np : pdis, *ta = host ? st + 6 * np : angv;
+    if (!pos) tp = nullptr;
+    if (!pdis) td = nullptr;
+    if (!angv) ta = nullptr;
+    if (c->prec == DEM_PREC_MIXED)
+        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos, np),
+                                                                planes<double>(c->disp, np), planes<float>(c->ang, np),
+                                                                tp, td, ta);
+    else
+        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos, np),
+                                                                 planes<double>(c->disp, np),
+                                                                 planes<double>(c->ang, np), tp, td, ta);
+    DEM_LAUNCH_CHECK();
+    if (host) {
+        if (pos) DEM_CUDA_TRY(cudaMemcpyAsync(pos, tp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (pdis) DEM_CUDA_TRY(cudaMemcpyAsync(pdis, td, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (angv) DEM_CUDA_TRY(cudaMemcpyAsync(angv, ta, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DEM_OK;
+}
+
+int dem_download_state(dem_ctx* c, double* pos, double* pdis, double* angv) {
+    return download_common(c, pos, pdis, angv, true);
+}
+int dem_download_state_device(dem_ctx* c, double* pos, double* pdis, double* angv) {
+    return download_common(c, pos, pdis, angv, false);
+}
+
+int dem_step_n(dem_ctx* c, long long nsteps) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_step_n: null ctx");
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_step_n: no state uploaded");
+    if (!c->have_mat) return fail(DEM_ERR_STATE, "dem_step_n: material not set");
+    if (nsteps < 0) return fail(DEM_ERR_ARG, "dem_step_n: negative step count");
+    const int K = c->cfg.relist_interval;
+    int rc;
+    while (nsteps > 0) {
+        if (c->in_window == 0 && nsteps >= K && !c->profiling) {
+            // whole window: replay the captured graph
+            rc = build_graph(c, c->cur);
+            if (rc) return rc;
+            DEM_CUDA_TRY(cudaGraphLaunch(c->gexec[c->cur], c->stream));
+            c->cur = 1 - c->cur;
+            c->relists++;
+            c->step += K;
+            nsteps -= K;
+            c->last_slot = K - 1;
+            continue;
+        }
+        if (c->in_window == 0) {
+            DEM_CUDA_TRY(cudaMemsetAsync(c->slots, 0, (size_t)K * sizeof(StepSlot), c->stream));
+            if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+            rc = relist(c, c->cur);
+            if (rc) return rc;
+            if (c->profiling) {
+                DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+                double ms;
+                if ((rc = ev_ms(c->ev[0], c->ev[1], &ms))) return rc;
+                c->ktime[0] += ms;
+                c->kcount[0]++;
+            }
+            c->cur = 1 - c->cur;
+            c->relists++;
+        }
+        const int slot = (int)c->in_window;
+        if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+        rc = pair_step(c, c->cur);
+        if (rc) return rc;
+        if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+        rc = particle_step(c, c->cur, slot);
+        if (rc) return rc;
+        if (c->profiling) {
+            DEM_CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
+            double a, b;
+            if ((rc = ev_ms(c->ev[0], c->ev[1], &a)) || (rc = ev_ms(c->ev[1], c->ev[2], &b))) return rc;
+            c->ktime[1] += a; c->kcount[1]++;
+            c->ktime[2] += b; c->kcount[2]++;
+        }
+        c->last_slot = slot;
+        c->step++;
+        nsteps--;
+        c->in_window++;
+        if (c->in_window == K) c->in_window = 0;
+    }
+    return DEM_OK;
+}
+
+int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
+    if (!c || !out) return fail(DEM_ERR_ARG, "dem_get_scalars: null argument");
+    memset(out, 0, sizeof(*out));
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_get_scalars: no state uploaded");
+    char* hp = (char*)c->host_pinned;
+    DEM_CUDA_TRY(cudaMemcpyAsync(hp, c->words, sizeof(EngineWords), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaMemcpyAsync(hp + 64, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    if (c->last_slot >= 0)
+        DEM_CUDA_TRY(cudaMemcpyAsync(hp + 128, c->slots + c->last_slot, sizeof(StepSlot), cudaMemcpyDeviceToHost,
+                                     c->stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    EngineWords w;
+    memcpy(&w, hp, sizeof(w));
+    uint P;
+    memcpy(&P, hp + 64, sizeof(P));
+    StepSlot sl{0, 0};
+    if (c->last_slot >= 0) memcpy(&sl, hp + 128, sizeof(sl));
+    double mz;
+    memcpy(&mz, &sl.maxhz_bits, sizeof(mz));
+    out->step = c->step;
+    out->pairs = c->relists ? (long long)P : 0;
+    out->contacts = (long long)(sl.contacts / 2);
+    out->maxhz = mz;
+    out->relists = c->relists;
+    out->max_row = (int)w.max_row;
+    // packing fraction sum (4/3) pi r^3 / (Wx Wy maxhz): dempacking.cu:768-771
+    // with the monodisperse N pi/6 generalised; mean CN = pcntot/N (:768).
+    out->mean_cn = c->n > 0 ? (double)sl.contacts / (double)c->n : 0.0;
+    out->packing_fraction = mz > 0.0 ? c->vol / (c->cfg.world[0] * c->cfg.world[1] * mz) : 0.0;
+    int status = DEM_OK;
+    if (w.status & kStNonfinite) status = DEM_ERR_NONFINITE;
+    else if (w.status & kStCapacity) status = DEM_ERR_CAPACITY;
+    else if (w.status & kStSkin) status = DEM_ERR_SKIN;
+    out->status = status;
+    if (status == DEM_ERR_CAPACITY)
+        return fail(DEM_ERR_CAPACITY, "pair list exceeded capacity %lld (rows up to %u candidates)", c->cap, w.max_row);
+    if (status == DEM_ERR_NONFINITE) return fail(DEM_ERR_NONFINITE, "non-finite position or velocity");
+    if (status == DEM_ERR_SKIN)
+        return fail(DEM_ERR_SKIN, "a particle moved more than skin/2 = %g within a re-list window", 0.5 * c->cfg.skin);
+    return DEM_OK;
+}
+
+int dem_record_forces(dem_ctx* c, int on) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_record_forces: null ctx");
+    if (on && !c->dbgF) {
+        int rc;
+        if ((rc = dalloc(&c->dbgF, 3 * c->npad)) || (rc = dalloc(&c->dbgT, 3 * c->npad)) ||
+            (rc = dalloc(&c->dbgC, c->npad)))
+            return rc;
+    }
+    if ((bool)on != c->record) free_graphs(c);
+    c->record = on != 0;
+    return DEM_OK;
+}
+
+int dem_download_forces(dem_ctx* c, double* force, double* torque, unsigned int* contacts) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_download_forces: null ctx");
+    if (!c->record || !c->dbgF) return fail(DEM_ERR_STATE, "dem_download_forces: enable dem_record_forces first");
+    const long long n = c->n;
+    if (force) DEM_CUDA_TRY(cudaMemcpyAsync(force, c->dbgF, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (torque) DEM_CUDA_TRY(cudaMemcpyAsync(torque, c->dbgT, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (contacts) DEM_CUDA_TRY(cudaMemcpyAsync(contacts, c->dbgC, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DEM_OK;
+}
+
+int dem_download_pairs(dem_ctx* c, unsigned int* lp, unsigned int* ln, double* hist, long long capn, long long* npairs) {
+    if (!c || !npairs) return fail(DEM_ERR_ARG, "dem_download_pairs: null argument");
+    *npairs = 0;
+    if (!c->uploaded || c->relists == 0) return DEM_OK;
+    const int lst = c->cur;
+    uint P = 0;
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->host_pinned, c->off[lst] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    memcpy(&P, c->host_pinned, sizeof(uint));
+    if ((long long)P > c->cap) return fail(DEM_ERR_CAPACITY, "dem_download_pairs: list overflowed capacity");
+    *npairs = P;
+    if (P == 0 || !lp || !ln) return DEM_OK;
+    if ((long long)P > capn) return fail(DEM_ERR_ARG, "dem_download_pairs: host capacity %lld < %u pairs", capn, P);
+    uint *dlp, *dln;
+    double* dh;
+    int rc;
+    if ((rc = dalloc(&dlp, P)) || (rc = dalloc(&dln, P)) || (rc = dalloc(&dh, 3 * (size_t)P))) return rc;
+    k_pairs_out<<<grid_for(P, 256), 256, 0, c->stream>>>(c->off[lst], c->n, c->cap, c->lp, c->ln[lst],
+                                                          planes<double>(c->hist[lst], c->cap), dlp, dln, dh);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lp, dlp, P * sizeof(uint), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ln, dln, P * sizeof(uint), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && hist) e = cudaMemcpyAsync(hist, dh, 3 * (size_t)P * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dlp);
+    cudaFree(dln);
+    cudaFree(dh);
+    if (e != cudaSuccess) return cuda_fail(e, "dem_download_pairs", __FILE__, __LINE__);
+    return DEM_OK;
+}
+
+int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsigned int* cell_start,
+                       unsigned int* cell_end, long long ncells_cap) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_download_cells: null ctx");
+    if (!c->uploaded || c->relists == 0) return fail(DEM_ERR_STATE, "dem_download_cells: no list built yet");
+    const long long n = c->n, nc = c->ncells;
+    if (ids) DEM_CUDA_TRY(cudaMemcpyAsync(ids, c->sid2, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<uint> cs;
+    if (cell_start || cell_end || keys) {
+        if (ncells_cap < nc && (cell_start || cell_end))
+            return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
+        cs.resize(nc + 1);
+        DEM_CUDA_TRY(cudaMemcpyAsync(cs.data(), c->cstart, (nc + 1) * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    }
+    std::vector<uint> k;
+    if (keys) {
+        k.resize(n);
+        DEM_CUDA_TRY(cudaMemcpyAsync(k.data(), c->key, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    }
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (keys) {
+        // sorted keys: expand the cell ranges
+        for (long long cc = 0; cc < nc; cc++)
+            for (uint t = cs[cc]; t < cs[cc + 1]; t++) keys[t] = (uint)cc;
+    }
+    if (cell_start || cell_end) {
+        for (long long cc = 0; cc < nc; cc++) {
+            bool empty = cs[cc] == cs[cc + 1];
+            if (cell_start) cell_start[cc] = empty ? kEmpty : cs[cc];
+            if (cell_end) cell_end[cc] = empty ? kEmpty : cs[cc + 1];
+        }
+    }
+    return DEM_OK;
+}
+
+int dem_grid_info(dem_ctx* c, unsigned int grid[3], double* cell, long long* ncells) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_grid_info: null ctx");
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_grid_info: no state uploaded");
+    if (grid) { grid[0] = c->grid.gx; grid[1] = c->grid.gy; grid[2] = c->grid.gz; }
+    if (cell) *cell = c->grid.cs;
+    if (ncells) *ncells = c->ncells;
+    return DEM_OK;
+}
+
+int dem_set_profiling(dem_ctx* c, int on) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_set_profiling: null ctx");
+    c->profiling = on != 0;
+    for (int k = 0; k < 3; k++) { c->ktime[k] = 0; c->kcount[k] = 0; }
+    return DEM_OK;
+}
+
+int dem_kernel_times(dem_ctx* c, double out[3]) {
+    if (!c || !out) return fail(DEM_ERR_ARG, "dem_kernel_times: null argument");
+    for (int k = 0; k < 3; k++) out[k] = c->kcount[k] ? c->ktime[k] / c->kcount[k] : 0.0;
+    return DEM_OK;
+}
+
+}  // extern "C"

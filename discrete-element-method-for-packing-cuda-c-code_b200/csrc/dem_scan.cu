@@ -1,0 +1,131 @@
+// dem_scan.cu -- device-wide exclusive prefix sum of uint32 (cell counts,
+// per-particle pair counts, radix digit histograms).  Three launches:
+// tile reduce -> scan of tile sums (one CTA) -> tile scan + offset.  256
+// threads x 16 items per tile; items are loaded as uint4 when aligned.
+#include "dem_common.cuh"
+
+namespace dem {
+
+namespace {
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint warp_incl_scan(uint v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Exclusive block scan of one value per thread; returns the block total.
+__device__ __forceinline__ uint block_excl_scan(uint v, uint* smem_warp, uint& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint inc = warp_incl_scan(v);
+    if (lane == 31) smem_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint w = lane < (kScanThreads / 32) ? smem_warp[lane] : 0u;
+        uint wi = warp_incl_scan(w);
+        if (lane < (kScanThreads / 32)) smem_warp[lane] = wi - w;
+        if (lane == (kScanThreads / 32) - 1) smem_warp[kScanThreads / 32] = wi;
+    }
+    __syncthreads();
+    uint r = smem_warp[warp] + inc - v;
+    total = smem_warp[kScanThreads / 32];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ void load_items(const uint* in, long long n, long long base, uint (&it)[kScanItems]) {
+    const long long b = base + (long long)threadIdx.x * kScanItems;
+    if (b + kScanItems <= n && ((reinterpret_cast<uintptr_t>(in + b) & 15) == 0)) {
+        const uint4* p = reinterpret_cast<const uint4*>(in + b);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; q++) {
+            uint4 v = p[q];
+            it[4 * q] = v.x; it[4 * q + 1] = v.y; it[4 * q + 2] = v.z; it[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < kScanItems; q++) it[q] = (b + q < n) ? in[b + q] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_reduce(const uint* __restrict__ in, long long n,
+                                                              uint* __restrict__ sums) {
+    __shared__ uint sw[kScanThreads / 32 + 1];
+    uint it[kScanItems];
+    load_items(in, n, (long long)blockIdx.x * kScanTile, it);
+    uint s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; q++) s += it[q];
+    uint tot;
+    block_excl_scan(s, sw, tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// One CTA scans the tile sums in chunks of 256.
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint* sums, long long nt, uint* total) {
+    __shared__ uint sw[kScanThreads / 32 + 1];
+    uint carry = 0;
+    for (long long base = 0; base < nt; base += kScanThreads) {
+        long long i = base + threadIdx.x;
+        uint v = i < nt ? sums[i] : 0u;
+        uint tot;
+        uint e = block_excl_scan(v, sw, tot);
+        if (i < nt) sums[i] = e + carry;
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint* in, uint* out,
+                                                            long long n, const uint* __restrict__ sums) {
+    __shared__ uint sw[kScanThreads / 32 + 1];
+    uint it[kScanItems];
+    const long long base = (long long)blockIdx.x * kScanTile;
+    load_items(in, n, base, it);
+    uint s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; q++) s += it[q];
+    uint tot;
+    uint run = block_excl_scan(s, sw, tot) + sums[blockIdx.x];
+    const long long b = base + (long long)threadIdx.x * kScanItems;
+    uint o[kScanItems];
+#pragma unroll
+    for (int q = 0; q < kScanItems; q++) { o[q] = run; run += it[q]; }
+    if (b + kScanItems <= n && ((reinterpret_cast<uintptr_t>(out + b) & 15) == 0)) {
+        uint4* p = reinterpret_cast<uint4*>(out + b);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; q++) p[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < kScanItems; q++)
+            if (b + q < n) out[b + q] = o[q];
+    }
+}
+}  // namespace
+
+size_t scan_scratch_words(long long n) {
+    long long nt = (n + kScanTile - 1) / kScanTile;
+    return (size_t)(nt < 1 ? 1 : nt) + 4;
+}
+
+int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s) {
+    if (n <= 0) {
+        if (total) DEM_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(uint), s));
+        return DEM_OK;
+    }
+    long long nt = (n + kScanTile - 1) / kScanTile;
+    k_tile_reduce<<<(unsigned)nt, kScanThreads, 0, s>>>(in, n, tmp);
+    k_scan_sums<<<1, kScanThreads, 0, s>>>(tmp, nt, total);
+    k_tile_scan<<<(unsigned)nt, kScanThreads, 0, s>>>(in, out, n, tmp);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+}  // namespace dem

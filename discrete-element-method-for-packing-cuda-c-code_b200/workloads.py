@@ -1,0 +1,120 @@
+"""Workloads of the DEM packing step, in the reference's reduced units.
+
+Length unit d_ref = 1 mm (the median diameter), time unit tau = sqrt(d_ref/g)
+= 0.010096 s, mass unit rho*pi*d_ref^3/6 (dempacking.cu:146-149,213-225,311).
+All share E = 1e7 Pa, nu = 0.29, rho = 2500 kg/m^3, restitution 0.5 (viscous
+damping, normal and tangential), flat frictional walls, gravity -z, skin
+0.1*R with R the median radius (0.05 d), re-list every 20 steps.
+
+  lattice_2k     2,000 monodisperse r = 0.5 mm, 20x20x100 mm box, cubic lattice
+                 a = 1.1 mm (18x18 per layer), jitter +-0.04 mm, dt = 1e-6 s,
+                 20,000 steps, mu = 0.3, mu_r = 0.002 R*.  FP64.
+  rsa_500k       500,000 lognormal radii (median 0.5 mm, sigma 0.2, [0.3, 0.8] mm)
+                 placed by random sequential addition in 100x100x400 mm,
+                 dt = 5e-7 s, 10,000 steps, mu = 0.3, mu_r = 0.002 R*.
+                 FP64 (plain form) or mixed precision.
+  bidisperse_4m  4,000,000 radii 0.4/0.6 mm 1:1, 200x200x600 mm, dt = 4e-7 s,
+                 5,000 steps, mu = 0.5, mu_r = 0.005 R*.  Mixed precision.
+  settle_50k     50,000 lognormal (as rsa_500k) in 40x40x150 mm, dt = 5e-7 s,
+                 pre-settled 20,000 steps, then a 2,000-step window.
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (PREC_FP64, PREC_MIXED, RADII_BIDISPERSE, RADII_LOGNORMAL, contact, damp_from_restitution, estar,
+               gen_lattice, gen_radii, gen_rsa)
+
+D_REF = 1e-3                       # m
+G = 9.81
+TAU = math.sqrt(D_REF / G)         # s
+SEED = 20261203
+
+
+def reduced_dt(dt_seconds):
+    return dt_seconds / TAU
+
+
+def material(E=1e7, nu=0.29, rho=2500.0, mu=0.3, mu_w=None, roll_rel=0.002, e=0.5):
+    """pp and pw contact dicts (reduced units).  Rolling length roll_rel * R*."""
+    es = estar(E, nu, rho, D_REF)
+    c = damp_from_restitution(e)
+    pp = contact(es, mu, nu, c, c, 0.0, roll_rel)
+    pw = contact(es, mu if mu_w is None else mu_w, nu, c, c, 0.0, roll_rel)
+    return pp, pw
+
+
+@dataclass
+class Workload:
+    name: str
+    n: int
+    pos: np.ndarray
+    rad: np.ndarray
+    world: tuple
+    dt: float
+    steps: int
+    relist_interval: int
+    skin: float
+    precision: int
+    pp: dict
+    pw: dict
+    density: float = 1.0
+    pair_capacity: int = 0
+    meta: dict = field(default_factory=dict)
+
+    def cell(self):
+        return 2.0 * float(self.rad.max()) + self.skin + 1e-4
+
+    def engine_kwargs(self):
+        return dict(n=self.n, world=self.world, dt=self.dt, skin=self.skin, precision=self.precision,
+                    relist_interval=self.relist_interval, density=self.density, pair_capacity=self.pair_capacity)
+
+
+def lattice_2k(seed=SEED, n=2000):
+    a = 1.1
+    pos, rad = gen_lattice(n, a, 18, 18, 0.55, 0.04, 0.5, seed)
+    pp, pw = material(mu=0.3, roll_rel=0.002)
+    return Workload("lattice_2k", n, pos, rad, (20.0, 20.0, 100.0), reduced_dt(1e-6), 20000, 20, 0.05, PREC_FP64,
+                    pp, pw, meta={"init": "cubic lattice a=1.1 mm, jitter 0.04 mm"})
+
+
+def rsa_500k(seed=SEED, precision=PREC_MIXED, n=500_000, box=(100.0, 100.0, 400.0)):
+    rad = gen_radii(n, RADII_LOGNORMAL, 0.5, 0.2, 0.3, 0.8, seed)
+    pos = gen_rsa(box, rad, seed + 1)
+    pp, pw = material(mu=0.3, roll_rel=0.002)
+    name = "rsa_500k" if n == 500_000 else f"rsa_{n}"
+    return Workload(name, n, pos, rad, tuple(box), reduced_dt(5e-7), 10000, 20, 0.05, precision, pp, pw,
+                    meta={"init": "RSA, lognormal radii median 0.5 mm sigma 0.2 in [0.3,0.8] mm"})
+
+
+def bidisperse_4m(seed=SEED, n=4_000_000, box=(200.0, 200.0, 600.0)):
+    rad = gen_radii(n, RADII_BIDISPERSE, 0.4, 0.6, 0.0, 0.0, seed)
+    pos = gen_rsa(box, rad, seed + 1)
+    pp, pw = material(mu=0.5, roll_rel=0.005)
+    return Workload("bidisperse_4m", n, pos, rad, tuple(box), reduced_dt(4e-7), 5000, 20, 0.05, PREC_MIXED, pp, pw,
+                    meta={"init": "RSA, radii 0.4/0.6 mm 1:1"})
+
+
+def settle_50k(seed=SEED, n=50_000, box=(40.0, 40.0, 150.0)):
+    rad = gen_radii(n, RADII_LOGNORMAL, 0.5, 0.2, 0.3, 0.8, seed)
+    pos = gen_rsa(box, rad, seed + 1)
+    pp, pw = material(mu=0.3, roll_rel=0.002)
+    return Workload("settle_50k", n, pos, rad, tuple(box), reduced_dt(5e-7), 2000, 20, 0.05, PREC_MIXED, pp, pw,
+                    meta={"init": "RSA then 20,000 settling steps", "presettle_steps": 20000})
+
+
+def small_box(n=3000, box=(16.0, 16.0, 40.0), seed=SEED, precision=PREC_FP64, compress=1.0):
+    """A small polydisperse case for parity tests: RSA (solid fraction about
+    0.16), optionally compressed towards the floor and the box axis by the
+    factor `compress` (< 1 creates overlapping contacts)."""
+    rad = gen_radii(n, RADII_LOGNORMAL, 0.5, 0.2, 0.3, 0.8, seed)
+    pos = gen_rsa(box, rad, seed + 1)
+    if compress != 1.0:
+        p = pos.reshape(-1, 3)
+        p[:, 0] *= compress
+        p[:, 1] *= compress
+        p[:, 2] = rad + (p[:, 2] - rad) * compress
+        pos = p.reshape(-1).copy()
+    pp, pw = material(mu=0.3, roll_rel=0.002)
+    return Workload("small_box", n, pos, rad, tuple(box), reduced_dt(5e-7), 200, 20, 0.05, precision, pp, pw)

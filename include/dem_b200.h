@@ -1,0 +1,325 @@
+/*
+ * dem_b200.h -- C ABI of the B200 (sm_100a) DEM packing time step.
+ *
+ * Two layers are exported from libdem_b200.so:
+ *
+ *  1. Reference-compatible entry points.  They keep the names, argument order
+ *     and argument meaning of the host launch wrappers in the reference's
+ *     extern "C" block (particleSystem.cu:13-424) plus the SDK RadixSort call
+ *     (dempacking.cu:553-555), so dempacking.cu's step loop can link against
+ *     this library instead.  All array arguments are DEVICE pointers in the
+ *     reference's layout (xyz-interleaved double, i.e. double3 AoS).  The one
+ *     change: every call returns an int status (DEM_OK ...) instead of calling
+ *     exit() (particleSystem.cu:15-23); a caller that ignores the return value
+ *     behaves as before.  The __constant__ symbols Par/ParW/cua/cub that the
+ *     reference fills with cudaMemcpyToSymbol (dempacking.cu:355-356,
+ *     neiglist.cu:27-49) are set through setMaterialProperties/setListCutoff.
+ *
+ *  2. The context API (dem_*).  An opaque dem_ctx owns structure-of-arrays
+ *     device buffers, a CSR contact-candidate list and CUDA graphs of whole
+ *     re-list windows; dem_step_n advances the packing with no host sync.
+ *     Precision is FP64 throughout (DEM_PREC_FP64) or mixed (DEM_PREC_MIXED:
+ *     FP32 hashing/list/forces/accumulation, FP64 positions, velocities and
+ *     tangential history).
+ *
+ * Units are the reference's reduced units (dempacking.cu:146-149,213-225):
+ * length = particle diameter d, mass = rho*pi*d^3/6, force = that mass times
+ * g, time = sqrt(d/g).  pdis and angv are per-step displacement and rotation
+ * (velocity*dt, angular velocity*dt), as in the reference.
+ */
+#ifndef DEM_B200_H
+#define DEM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status -- */
+#define DEM_OK              0
+#define DEM_ERR_ARG         1  /* bad argument (null pointer, size, mode)          */
+#define DEM_ERR_CUDA        2  /* a CUDA runtime call or kernel launch failed      */
+#define DEM_ERR_CAPACITY    3  /* neighbour / pair capacity exceeded (list cut)    */
+#define DEM_ERR_NONFINITE   4  /* NaN or Inf appeared in positions/velocities      */
+#define DEM_ERR_SKIN        5  /* a particle moved more than skin/2 inside a window */
+#define DEM_ERR_IO          6  /* deck / output file error                          */
+#define DEM_ERR_STATE       7  /* call out of order (e.g. step before upload)       */
+
+/* Text of the last error raised on the calling host thread. */
+const char* dem_last_error_string(void);
+/* Library build identification (arch, precision modes). */
+const char* dem_version(void);
+
+/* ============================================================================
+ * 1. Reference-compatible entry points (device pointers, reference layout)
+ * ==========================================================================*/
+
+/* Key/value record of the SDK radix sort used at dempacking.cu:553-555. */
+typedef struct {
+    unsigned int key;
+    unsigned int value;
+} KeyValuePair;
+
+/* Material constants, same fields and order as the reference's __constant__
+ * structs (neiglist.cu:32-47).  estar* already contain the 4/3 Hertz factor
+ * (dempacking.cu:148-149); upp/upw are rolling-friction lengths in units of d. */
+typedef struct {
+    double estarp, ufricp, vpois, dampnp, damptp, upp;
+} Matproperties;
+typedef struct {
+    double estarw, ufricw, vpoisw, dampnw, damptw, upw;
+} Wallproperties;
+
+/* Replaces cudaMemcpyToSymbol(Par/ParW, ...) at dempacking.cu:355-356. */
+int setMaterialProperties(const Matproperties* par, const Wallproperties* parw);
+/* Replaces the __constant__ cua/cub of neiglist.cu:27-28: contact distance
+ * (cua) and candidate cut-off distance (cub) between centres, in units of d.
+ * neighborarray lists j when |x_i - x_j| < cub; updateposition raises the
+ * re-list flag when |q_i| > 0.5*(cub-cua) (neiglist.cu:335,370). */
+int setListCutoff(double cua, double cub);
+/* Stream used by all reference-compatible calls (default: legacy stream 0). */
+int dem_compat_set_stream(void* cuda_stream);
+
+/* RadixSort(pData0, pData1, elements, keybits)  -- dempacking.cu:553-555.
+ * Stable LSD sort of `elements` records by the low `keybits` bits of key;
+ * result in pData0, pData1 is the ping-pong buffer.  Scratch for the digit
+ * histograms is allocated by the library on the first call per device and
+ * kept until exit. */
+int RadixSort(KeyValuePair* pData0, KeyValuePair* pData1,
+              unsigned int elements, unsigned int keybits);
+
+/* calcHash  -- particleSystem.cu:27-45, kernel neiglist.cu:54-97.
+ * particleHash[2i] = clamped linear cell id of particle i, [2i+1] = i. */
+int calcHash(double* Pos, unsigned int* particleHash, unsigned int gridSize[3],
+             double cellSize[3], double worldOrigin[3], int numBodies);
+
+/* findCellStart  -- particleSystem.cu:49-64, kernel neiglist.cu:102-120.
+ * cellStart[c] = first sorted index with key c, 0xffffffff if empty. */
+int findCellStart(unsigned int* particleHash, unsigned int* cellStart,
+                  int numBodies, unsigned int numGridCells);
+
+/* neighborarray  -- particleSystem.cu:67-97 (kernel neighborarrayD absent from
+ * the reference).  Row i of Anei (maxParticlesPerCell slots) holds the
+ * njgi[i] neighbours j>i in ascending id order, then the njli[i] neighbours
+ * j<i in ascending order; unused slots are 0xffffffff (particleSystem.cu:83).
+ * Returns DEM_ERR_CAPACITY if a row would overflow (the row is cut). */
+int neighborarray(double* pos, unsigned int* particleHash, unsigned int* cellStart,
+                  unsigned int gridSize[3], double cellSize[3], double worldOrigin[3],
+                  int maxParticlesPerCell, int numBodies,
+                  unsigned int* Anei, unsigned int* njgi, unsigned int* njli);
+
+/* prefixsum  -- particleSystem.cu:126-140.  oldsjgi <- sjgi; sjgi = inclusive
+ * scan of njgi; *totalcontacts (HOST) = sjgi[numBodies-1].  Synchronises. */
+int prefixsum(unsigned int numBodies, unsigned int* njgi, unsigned int* sjgi,
+              unsigned int* oldsjgi, unsigned int* totalcontacts);
+
+/* pairlist  -- particleSystem.cu:143-191 (kernel pairlistD absent).
+ * Pairs of i occupy [sjgi[i]-njgi[i], sjgi[i]): Lp=i, Ln=j (j>i ascending).
+ * Aref row i: list slot of each neighbour in Anei row order.  Tangential
+ * history dispt (double3) / fricp of pair (i,j) is copied from the previous
+ * list (olddispt/oldfricp at the slot where oldLn==j inside i's previous range
+ * [oldsjgi[i-1], oldsjgi[i])), else zero. */
+int pairlist(unsigned int* sjgi, unsigned int* oldsjgi, unsigned int* oldLn,
+             unsigned int* Anei, unsigned int* njgi, unsigned int* njli,
+             double* olddispt, double* oldfricp,
+             int maxParticlesPerCell, int maxCnPerParticle, unsigned int numBodies,
+             unsigned int* Aref, unsigned int* Lp, unsigned int* Ln,
+             double* dispt, double* fricp);
+
+/* calculateforcepair  -- particleSystem.cu:194-240, kernel neiglist.cu:156-233.
+ * One thread per candidate pair: Hertz-Mindlin normal + damping, Mindlin
+ * tangential spring with Coulomb cap, rolling resistance.  forcepair = force
+ * on Lp (the Ln side receives minus it), torqpairi/j = torques on Lp/Ln,
+ * contactpair = 1 when touching.  dispt/fricp and olddispt/oldfricp/oldLn are
+ * updated as at neiglist.cu:211-231. */
+int calculateforcepair(double* pos, double* pdis, double* angv, double* rad, double* rmass,
+                       unsigned int* Lp, unsigned int* Ln, unsigned int* oldLn,
+                       double* dispt, double* fricp, double* olddispt, double* oldfricp,
+                       double dt,
+                       double* forcepair, double* torqpairi, double* torqpairj,
+                       unsigned int* contactpair, unsigned int totalcontacts);
+
+/* sumallforcei  -- particleSystem.cu:243-277 (kernel sumallforceiD absent).
+ * Gather through Aref: forcei = sum own-pair forces - sum forces of pairs
+ * where i is Ln; torquei likewise with torqpairi / torqpairj; contacti =
+ * number of touching pairs.  Deterministic, no atomics. */
+int sumallforcei(int maxParticlesPerCell, int numBodies, unsigned int* njgi, unsigned int* njli,
+                 double* forcepair, double* torqpairi, double* torqpairj,
+                 unsigned int* contactpair, unsigned int* Aref,
+                 double* forcei, double* torquei, unsigned int* contacti);
+
+/* calculateforceiw  -- particleSystem.cu:279-313, kernel neiglist.cu:238-306.
+ * Adds gravity (0,0,-m) and flat-wall contact (x=+-Wx/2, y=+-Wy/2, z=0, open
+ * top) to forcei/torquei (pair sums are used only if totalcontacts != 0).
+ * One wall-history slot per particle (disptw/fricpw). */
+int calculateforceiw(double worldSize[3], double* pos, double* pdis, double* angv,
+                     double* rad, double* rmass, double dt, unsigned int totalcontacts,
+                     int numBodies, double* disptw, double* fricpw,
+                     double* forcei, double* torquei);
+
+/* updateposition  -- particleSystem.cu:315-384, kernel neiglist.cu:308-409.
+ * Symplectic Euler in displacement form; *iall (HOST) = 1 if any |q_i| >
+ * 0.5*(cub-cua), *maxhz (HOST) = max(0, max_i z_i).  Synchronises. */
+int updateposition(double worldSize[3], int numBodies, double* pos, double* pdis,
+                   double* angv, double* rmass, double* inert, double* forcei,
+                   double* torquei, double* qi, double dt, double cdamp,
+                   unsigned int* iall, double* maxhz);
+
+/* outputporositycn  -- particleSystem.cu:386-422.  *pcntot (HOST) = sum of
+ * contacti.  Synchronises. */
+int outputporositycn(unsigned int numBodies, unsigned int* contacti, double maxhz,
+                     double worldSize[3], unsigned int* pcntot);
+
+/* ============================================================================
+ * 2. Context API (structure-of-arrays engine, CUDA-graph windows)
+ * ==========================================================================*/
+#define DEM_PREC_FP64   0
+#define DEM_PREC_MIXED  1
+
+typedef struct dem_ctx dem_ctx;
+
+/* Contact parameters in reduced units.  Rolling-friction length of a pair is
+ * roll + roll_rel * R*, with R* = r_i r_j/(r_i+r_j) (R* = r for a wall). */
+typedef struct {
+    double estar;    /* (4/3) E/(2(1-nu^2)) reduced, as dempacking.cu:148      */
+    double mu;       /* sliding friction                                       */
+    double nu;       /* Poisson ratio (slip length mu(2-nu)/(2(1-nu)) delta)   */
+    double damp_n;   /* normal damping coefficient (hopp3d.inp line 10)        */
+    double damp_t;   /* tangential damping coefficient                         */
+    double roll;     /* rolling-friction length, units of d                    */
+    double roll_rel; /* rolling-friction length per unit R*                    */
+} dem_contact;
+
+typedef struct {
+    dem_contact pp;  /* particle-particle */
+    dem_contact pw;  /* particle-wall     */
+} dem_material;
+
+typedef struct {
+    long long n;            /* particles                                        */
+    int precision;          /* DEM_PREC_FP64 / DEM_PREC_MIXED                   */
+    int relist_interval;    /* steps per window (re-list at window start)       */
+    double world[3];        /* box Wx, Wy, Wz; origin (-Wx/2,-Wy/2,0)           */
+    double dt;              /* reduced time step                                */
+    double skin;            /* list skin: candidates |dx| < r_i+r_j+skin        */
+    double cell;            /* cell edge; 0 -> 2*r_max+skin (+1e-4)             */
+    double density;         /* mass = density*8r^3 (1 in reduced units)         */
+    long long pair_capacity;/* half-list capacity; 0 -> 8*n                     */
+} dem_config;
+
+/* Per-step observables (reference ppor.dat columns, dempacking.cu:766-776). */
+typedef struct {
+    long long step;          /* steps taken since upload                        */
+    long long pairs;         /* candidate pairs in the current list (half list) */
+    long long contacts;      /* touching pairs (= pcntot/2)                     */
+    double maxhz;            /* max(0, max_i z_i)                               */
+    double packing_fraction; /* sum (4/3)pi r^3 / (Wx*Wy*maxhz)                 */
+    double mean_cn;          /* 2*contacts/n                                    */
+    long long relists;       /* list builds since upload                        */
+    int status;              /* sticky device status (DEM_OK / DEM_ERR_*)       */
+    int max_row;             /* largest per-particle candidate count seen       */
+} dem_scalars;
+
+int dem_create(const dem_config* cfg, dem_ctx** out);
+int dem_destroy(dem_ctx* ctx);
+int dem_set_stream(dem_ctx* ctx, void* cuda_stream);
+int dem_set_material(dem_ctx* ctx, const dem_material* mat);
+/* Host AoS (xyz-interleaved) double arrays of length 3n (rad: n).  pdis/angv
+ * may be NULL (zero).  Resets histories and forces a re-list. */
+int dem_upload_state(dem_ctx* ctx, const double* pos, const double* pdis,
+                     const double* angv, const double* rad);
+/* Same with device pointers (AoS double), no host copy. */
+int dem_upload_state_device(dem_ctx* ctx, const double* pos, const double* pdis,
+                            const double* angv, const double* rad);
+int dem_download_state(dem_ctx* ctx, double* pos, double* pdis, double* angv);
+int dem_download_state_device(dem_ctx* ctx, double* pos, double* pdis, double* angv);
+/* Advance nsteps (any count; whole windows replay a captured CUDA graph). */
+int dem_step_n(dem_ctx* ctx, long long nsteps);
+/* Synchronises; observables of the last step and the sticky status. */
+int dem_get_scalars(dem_ctx* ctx, dem_scalars* out);
+/* Record per-particle force/torque/contact count of each step into device
+ * buffers (off by default; costs 52 bytes per particle-step of writes). */
+int dem_record_forces(dem_ctx* ctx, int on);
+/* Per-particle force/torque/contact count of the last step (host, AoS);
+ * needs dem_record_forces(ctx, 1) before the step. */
+int dem_download_forces(dem_ctx* ctx, double* force, double* torque, unsigned int* contacts);
+/* Current half list in canonical order (i ascending, then j): host arrays of
+ * capacity `cap`; *npairs receives the count. */
+int dem_download_pairs(dem_ctx* ctx, unsigned int* lp, unsigned int* ln,
+                       double* hist, long long cap, long long* npairs);
+/* Sorted (cell key, particle id) of the last re-list and cell ranges. */
+int dem_download_cells(dem_ctx* ctx, unsigned int* keys, unsigned int* ids,
+                       unsigned int* cell_start, unsigned int* cell_end, long long ncells_cap);
+int dem_grid_info(dem_ctx* ctx, unsigned int grid[3], double* cell, long long* ncells);
+/* Mean kernel time of the last dem_step_n call per kernel family (ms):
+ * out[0]=re-list, out[1]=pair force, out[2]=particle update.  Enabled by
+ * dem_set_profiling(ctx,1); adds events, so off for timing runs. */
+int dem_set_profiling(dem_ctx* ctx, int on);
+int dem_kernel_times(dem_ctx* ctx, double out[3]);
+
+/* ============================================================================
+ * 3. Host utilities (deck, initial states, reference output files)
+ * ==========================================================================*/
+
+/* hopp3d.inp deck as read at dempacking.cu:107-126, and the reduced-unit
+ * constants derived at dempacking.cu:141-149,213-225. */
+typedef struct {
+    int iforcemode, ntot;
+    double emod, vpois, denp, diam;
+    double dt; unsigned int tstop;
+    double dmt1, dmt2, thick, zht1, zht2;
+    double vel0; int nrings;
+    double ufricp, ufricw;
+    double dampnp, damptp, dampnw, damptw, cdamp;
+    double stiffness, dampcoeffn, dampcoefft;
+    double upp, upw;
+    /* derived (reduced units) */
+    double emod_red, estarp, estarw;
+    double world[3];          /* dmt2/diam, thick/diam, (zht1+zht2)/diam */
+    double upp_red, upw_red;
+} dem_deck;
+int dem_read_deck(const char* path, dem_deck* out);
+/* Material for the context API from a deck (pp and pw blocks). */
+int dem_deck_material(const dem_deck* deck, dem_material* out);
+
+/* Reduced-unit Hertz/restitution helpers.
+ * dem_estar: (4/3)*emod_red/(2(1-nu^2)) with emod_red = 6E/(pi rho g d).
+ * dem_damp_from_restitution: coefficient c with c*sqrt(6 m* E* sqrt(R* d))
+ * equal to the viscous term of restitution e (E* = (3/4) estar). */
+double dem_reduced_modulus(double E, double rho, double d);
+double dem_estar(double E, double nu, double rho, double d);
+double dem_damp_from_restitution(double e);
+
+/* Initial states, reproducible from a 64-bit seed (SplitMix64).  Output is
+ * host AoS pos[3n] and rad[n] in reduced units; world is the box.
+ * Lattice: spacing a, nx*ny per layer centred in x,y, first layer z0, uniform
+ * jitter +-jit, radius r (configuration of 2,000 spheres in a 20x20 box).
+ * RSA: random sequential non-overlapping insertion with wall clearance r;
+ * radii from dem_radius_* below.  Returns DEM_ERR_ARG when it cannot place. */
+int dem_gen_lattice(long long n, double spacing, int nx, int ny, double z0, double jitter,
+                    double radius, unsigned long long seed, double* pos, double* rad);
+#define DEM_RADII_MONO       0  /* all r = a                                    */
+#define DEM_RADII_LOGNORMAL  1  /* exp(ln a + b Z) truncated to [c, d]          */
+#define DEM_RADII_BIDISPERSE 2  /* a and b, 1:1 by number, shuffled             */
+int dem_gen_radii(long long n, int kind, double a, double b, double c, double d,
+                  unsigned long long seed, double* rad);
+int dem_gen_rsa(long long n, const double world[3], const double* rad,
+                unsigned long long seed, double* pos);
+
+/* Reference output files (formats of dempacking.cu:227-234,772-776,787-791,
+ * 802,812-819,904-913). */
+int dem_write_view(const char* path, const dem_deck* deck);
+int dem_write_ppor(const char* path, long long it, long long n, long long pcntot,
+                   double porosity, double packing, double avercn, double maxhz);
+int dem_write_particles(const char* path, int zone, long long n, const double* pos,
+                        const double* rad, double diam);
+int dem_write_preflow(const char* path, long long it, long long n, long long itime,
+                      const double* pos, const double* pdis, const double* angv);
+int dem_write_timesteps(const char* path, double tret, long long it);
+int dem_write_finish(const char* jobfinished_path, const char* restart_path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DEM_B200_H */

@@ -1,0 +1,270 @@
+"""GPU parity of the context API (SoA engine) against the CPU oracle.
+
+Bit-exact: sorted cell keys / ids, cell ranges and the canonical candidate
+pair set, for the FP64 list and the FP32 (mixed) list.
+Tolerances (stated per result):
+  FP64 engine vs FP64 oracle   forces rel-L2 <= 1e-9, positions RMS <= 1e-9 d
+  mixed engine vs FP64 oracle  forces rel-L2 <= 2e-4 (max-abs <= 2e-3 of the
+                               largest), positions RMS <= 1e-5 d after the run,
+                               packing fraction |delta| <= 1e-3 (the target),
+                               mean coordination number |delta| <= 0.02
+"""
+import numpy as np
+import pytest
+
+from _cases import dense_lattice
+
+pytestmark = pytest.mark.gpu
+
+
+def make_engine(dem, w, precision=None, **over):
+    kw = w.engine_kwargs()
+    if precision is not None:
+        kw["precision"] = precision
+    kw.update(over)
+    e = dem.Engine(**kw)
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad)
+    return e
+
+
+def oracle_cells(orc, w, cell, fp32):
+    g = orc.grid(w.world, cell)
+    keys = orc.hash_keys(w.pos, w.world, cell, fp32)
+    sk, si, cs, ce = orc.sort_cells(keys, int(g.prod()))
+    return g, sk, si, cs, ce
+
+
+def case_workload(dem, wl, case):
+    if case == "lattice":
+        return wl.lattice_2k()
+    if case == "small":
+        return wl.small_box(n=4000, compress=0.62)
+    return dense_lattice(dem)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["lattice", "small", "dense"])
+def test_cells_and_pairs_bit_exact(dem, orc, wl, cuda, prec, case):
+    w = case_workload(dem, wl, case)
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    fp32 = prec == "mixed"
+    e = make_engine(dem, w, p)
+    e.step(1)
+    grid, cell, nc = e.grid_info()
+    assert abs(cell - w.cell()) < 1e-15
+    keys, ids, st, en = e.cells()
+    g, sk, si, cs, ce = oracle_cells(orc, w, cell, fp32)
+    assert tuple(g) == tuple(grid)
+    np.testing.assert_array_equal(keys, sk)
+    np.testing.assert_array_equal(ids, si)
+    np.testing.assert_array_equal(st, cs)
+    np.testing.assert_array_equal(en, ce)
+    lp, ln, hist = e.pairs()
+    off, oln, ohist, _ = orc.build_list(w.pos, w.rad, w.world, cell, w.skin, fp32)
+    olp = np.repeat(np.arange(w.n, dtype=np.uint32), np.diff(off))
+    np.testing.assert_array_equal(lp, olp)
+    np.testing.assert_array_equal(ln, oln)
+    assert lp.size > 0
+
+
+@pytest.mark.parametrize("case", ["small", "dense"])
+@pytest.mark.parametrize("prec,rtol", [("fp64", 1e-9), ("mixed", 2e-4)])
+def test_first_step_forces(dem, orc, wl, cuda, prec, rtol, case):
+    """Forces of step 1 on overlapping polydisperse packings (strongly
+    compressed RSA; gently overlapping lattice)."""
+    w = case_workload(dem, wl, case)
+    rng = np.random.default_rng(3)
+    pdis = rng.normal(0, 1e-6, 3 * w.n)
+    angv = rng.normal(0, 1e-6, 3 * w.n)
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    e = dem.Engine(**{**w.engine_kwargs(), "precision": p})
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad, pdis, angv)
+    e.record_forces(True)
+    e.step(1)
+    F, T, C = e.forces()
+    cell = e.grid_info()[1]
+    mat = dem.material_array(w.pp, w.pw)
+    oF, oT, oC, npairs = orc.forces_once(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, mat, prec == "mixed",
+                                         pdis, angv)
+    assert oC.sum() > w.n // 4, "test needs contacts"
+    rel = np.linalg.norm(F - oF) / np.linalg.norm(oF)
+    relT = np.linalg.norm(T - oT) / np.linalg.norm(oT)
+    assert rel <= rtol, rel
+    assert relT <= (rtol if prec == "fp64" else 1e-3), relT
+    if prec == "fp64":
+        np.testing.assert_array_equal(C, oC)
+    else:
+        assert np.count_nonzero(C != oC) <= max(2, w.n // 1000)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_trajectory_lattice_2k(dem, orc, wl, cuda, prec):
+    """2,000 spheres, 2,000 steps (100 re-lists with history carry)."""
+    w = wl.lattice_2k()
+    steps = 2000
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    e = make_engine(dem, w, p)
+    e.step(steps)
+    s = e.scalars()
+    pos, pdis, angv = e.download()
+    cell = e.grid_info()[1]
+    mat = dem.material_array(w.pp, w.pw)
+    o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, mat, prec == "mixed", steps,
+                w.relist_interval)
+    assert o["status"] == 0
+    rms = np.sqrt(np.mean((pos - o["pos"]) ** 2))
+    tol = 1e-9 if prec == "fp64" else 1e-5
+    assert rms <= tol, rms
+    assert s["relists"] == steps // w.relist_interval
+    assert s["pairs"] == int(o["npairs"][-1])
+    oc = int(o["ncontacts"][-1])
+    if prec == "fp64":
+        assert s["contacts"] == oc
+    assert abs(s["maxhz"] - o["maxhz"][-1]) < 1e-6
+    pf_o = np.sum(4.0 / 3.0 * np.pi * w.rad ** 3) / (w.world[0] * w.world[1] * o["maxhz"][-1])
+    assert abs(s["packing_fraction"] - pf_o) <= 1e-3
+    assert abs(s["mean_cn"] - 2.0 * oc / w.n) <= 0.02
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_dense_trajectory_and_history_carry(dem, orc, wl, cuda, prec):
+    """A bed with ~3,500 persistent contacts, 401 steps (21 re-lists): every
+    pair's carried FP64 tangential history, the positions and the contact
+    count against the oracle loop."""
+    w = dense_lattice(dem)
+    rng = np.random.default_rng(5)
+    pdis = rng.normal(0, 2e-6, 3 * w.n)
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    e = dem.Engine(**{**w.engine_kwargs(), "precision": p})
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad, pdis, None)
+    steps = 20 * w.relist_interval + 1
+    e.step(steps)
+    s = e.scalars()
+    lp, ln, hist = e.pairs()
+    cell = e.grid_info()[1]
+    mat = dem.material_array(w.pp, w.pw)
+    o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, mat, prec == "mixed", steps,
+                w.relist_interval, pdis=pdis)
+    assert o["status"] == 0 and s["status"] == 0
+    pos_g, _, _ = e.download()
+    rms = np.sqrt(np.mean((pos_g - o["pos"]) ** 2))
+    assert rms < (1e-10 if prec == "fp64" else 1e-6), rms
+    np.testing.assert_array_equal(ln, o["list_ln"])
+    live = np.count_nonzero(np.abs(o["list_hist"]) > 0)
+    assert live > 1000
+    herr = np.linalg.norm(hist - o["list_hist"]) / np.linalg.norm(o["list_hist"])
+    assert herr < (1e-8 if prec == "fp64" else 2e-3), herr
+    oc = int(o["ncontacts"][-1])
+    assert oc > 3000
+    if prec == "fp64":
+        assert s["contacts"] == oc
+    else:
+        assert abs(s["contacts"] - oc) <= max(3, oc // 500)
+
+
+def test_full_size_rsa_500k_list_bit_exact(dem, orc, wl, cuda):
+    """The 500,000-sphere workload: FP32 cell keys and the canonical pair set
+    match the oracle exactly at full size."""
+    w = wl.rsa_500k(precision=dem.PREC_MIXED)
+    e = make_engine(dem, w)
+    e.step(1)
+    keys, ids, st, en = e.cells()
+    cell = e.grid_info()[1]
+    g, sk, si, cs, ce = oracle_cells(orc, w, cell, True)
+    np.testing.assert_array_equal(keys, sk)
+    np.testing.assert_array_equal(ids, si)
+    lp, ln, _ = e.pairs()
+    off, oln, _, _ = orc.build_list(w.pos, w.rad, w.world, cell, w.skin, True)
+    np.testing.assert_array_equal(ln, oln)
+    np.testing.assert_array_equal(lp, np.repeat(np.arange(w.n, dtype=np.uint32), np.diff(off)))
+    # size-independent properties: rows sorted, i < j, each pair once
+    assert np.all(lp < ln)
+    key = lp.astype(np.uint64) << np.uint64(32) | ln.astype(np.uint64)
+    assert np.all(np.diff(key) > 0)
+
+
+def test_mixed_vs_fp64_oracle_packing_fraction(dem, orc, wl, cuda):
+    """Mixed-precision run of a reduced rsa workload (20,000 spheres, 1,000
+    steps) against the FP64 oracle: packing fraction within 1e-3."""
+    w = wl.rsa_500k(precision=dem.PREC_MIXED, n=20_000, box=(30.0, 30.0, 120.0))
+    steps = 1000
+    e = make_engine(dem, w)
+    e.step(steps)
+    s = e.scalars()
+    pos, _, _ = e.download()
+    cell = e.grid_info()[1]
+    o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, dem.material_array(w.pp, w.pw), False, steps,
+                w.relist_interval)
+    pf_o = np.sum(4.0 / 3.0 * np.pi * w.rad ** 3) / (w.world[0] * w.world[1] * o["maxhz"][-1])
+    assert abs(s["packing_fraction"] - pf_o) <= 1e-3
+    assert np.sqrt(np.mean((pos - o["pos"]) ** 2)) <= 1e-5
+
+
+def test_capacity_overflow_is_reported(dem, wl, cuda):
+    w = wl.small_box(n=3000, compress=0.8)
+    e = make_engine(dem, w, pair_capacity=10)
+    e.step(5)
+    with pytest.raises(dem.DemError) as ei:
+        e.scalars()
+    assert ei.value.code == dem.DEM_ERR_CAPACITY
+
+
+def test_skin_violation_is_reported(dem, wl, cuda):
+    w = wl.small_box(n=2000)
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_material(w.pp, w.pw)
+    pdis = np.zeros(3 * w.n)
+    pdis[0::3] = 0.01   # 0.01 d per step: skin/2 = 0.025 passed after 3 steps
+    e.upload(w.pos, w.rad, pdis, None)
+    e.step(10)
+    with pytest.raises(dem.DemError) as ei:
+        e.scalars()
+    assert ei.value.code == dem.DEM_ERR_SKIN
+
+
+def test_nonfinite_is_reported(dem, wl, cuda):
+    w = wl.small_box(n=2000)
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_material(w.pp, w.pw)
+    pdis = np.zeros(3 * w.n)
+    pdis[5] = np.nan
+    e.upload(w.pos, w.rad, pdis, None)
+    e.step(2)
+    with pytest.raises(dem.DemError) as ei:
+        e.scalars()
+    assert ei.value.code == dem.DEM_ERR_NONFINITE
+
+
+def test_partial_windows_equal_graph_windows(dem, wl, cuda):
+    """dem_step_n(1) x N (eager launches) and dem_step_n(N) (graphs) agree bit
+    for bit."""
+    w = wl.small_box(n=3000)
+    a = make_engine(dem, w)
+    b = make_engine(dem, w)
+    a.step(45)
+    for _ in range(45):
+        b.step(1)
+    pa, da, aa = a.download()
+    pb, db, ab = b.download()
+    np.testing.assert_array_equal(pa, pb)
+    np.testing.assert_array_equal(da, db)
+    np.testing.assert_array_equal(aa, ab)
+
+
+def test_device_upload_download_roundtrip(dem, wl, cuda):
+    torch = cuda
+    w = wl.small_box(n=2000)
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_material(w.pp, w.pw)
+    tpos = torch.from_numpy(w.pos).cuda()
+    trad = torch.from_numpy(w.rad).cuda()
+    e.upload_device(tpos, trad)
+    out = torch.empty_like(tpos)
+    e.download_device(pos=out)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), w.pos)
+    g, cell, nc = e.grid_info()
+    assert abs(cell - w.cell()) < 1e-15

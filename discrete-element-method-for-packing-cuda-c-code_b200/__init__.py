@@ -120,6 +120,7 @@ _SIGS = [
     ("setListCutoff", ctypes.c_int, [ctypes.c_double, ctypes.c_double]),
     ("dem_compat_set_stream", ctypes.c_int, [_vp]),
     ("RadixSort", ctypes.c_int, [_vp, _vp, ctypes.c_uint, ctypes.c_uint]),
+    ("RadixSortNoAlloc", ctypes.c_int, [_vp, _vp, ctypes.c_uint, ctypes.c_uint]),
     ("calcHash", ctypes.c_int, [_vp, _vp, _c_uint_p, _c_double_p, _c_double_p, ctypes.c_int]),
     ("findCellStart", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint]),
     ("neighborarray", ctypes.c_int, [_vp, _vp, _vp, _c_uint_p, _c_double_p, _c_double_p, ctypes.c_int, ctypes.c_int,
@@ -247,6 +248,10 @@ class compat:
     @staticmethod
     def RadixSort(d0, d1, n, bits=32):
         return check(lib().RadixSort(_ptr(d0), _ptr(d1), int(n), int(bits)), "RadixSort")
+
+    @staticmethod
+    def RadixSortNoAlloc(d0, d1, n, bits=32):
+        return check(lib().RadixSortNoAlloc(_ptr(d0), _ptr(d1), int(n), int(bits)), "RadixSortNoAlloc")
 
     @staticmethod
     def calcHash(pos, phash, grid, cell, origin, n):

@@ -112,3 +112,62 @@ extern "C" int RadixSort(KeyValuePair* pData0, KeyValuePair* pData1, unsigned in
     return dem::radix_sort_pairs(reinterpret_cast<uint2*>(pData0), reinterpret_cast<uint2*>(pData1), elements, keybits,
                                  scratch, dem::compat_stream());
 }
+
+// ---------------------------------------------------------------------------
+// RadixSortNoAlloc: the same stable sort for callers that must not allocate
+// device memory, e.g. a host loop that owns all of HBM through its own pool
+// allocator, or a latency-critical loop in which a first-call cudaMalloc (and
+// the device synchronisation it may cause) is not acceptable.  Its scratch
+// (digit histograms and scan carries) lives in the fixed device array below,
+// sized for at most kNoAllocMaxRecords records (about 2 MiB); every GPU that
+// loads this library holds that array until the process exits.
+//
+// The first call on a device resolves the array's device address with
+// cudaGetSymbolAddress while that device is current (host code cannot use the
+// symbol itself: on the host it names a stand-in, not device memory); make
+// that first call before any stream capture.  All calls share the one array,
+// which keeps the contents of the last call: every histogram word is written
+// before it is read, so nothing needs clearing, but two calls that overlap on
+// the GPU (different streams, or different host threads on the same device)
+// race on it and must be serialised by the caller.
+namespace dem {
+namespace {
+constexpr unsigned kNoAllocMaxRecords = 1u << 22;                        // 4,194,304
+constexpr size_t kNoAllocHistWords = (size_t)256 * (kNoAllocMaxRecords / kRsTile);
+constexpr size_t kNoAllocWords = kNoAllocHistWords + kNoAllocHistWords / 4096 + 256;
+__device__ __align__(256) unsigned int g_noalloc_scratch[kNoAllocWords];
+
+std::mutex g_noalloc_mu;
+std::vector<std::pair<int, uint*>> g_noalloc_addr;   // (device, device address of g_noalloc_scratch)
+
+int noalloc_scratch(uint** out) {
+    int dev = 0;
+    DEM_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    for (auto& e : g_noalloc_addr)
+        if (e.first == dev) { *out = e.second; return DEM_OK; }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+    g_noalloc_addr.emplace_back(dev, (uint*)p);
+    *out = (uint*)p;
+    return DEM_OK;
+}
+}  // namespace
+}  // namespace dem
+
+extern "C" int RadixSortNoAlloc(KeyValuePair* pData0, KeyValuePair* pData1, unsigned int elements,
+                                unsigned int keybits) {
+    if (elements > dem::kNoAllocMaxRecords)
+        return dem::fail(DEM_ERR_ARG, "RadixSortNoAlloc: %u records exceed the fixed scratch limit of %u records",
+                         elements, dem::kNoAllocMaxRecords);
+    if (elements > 1 && (!pData0 || !pData1)) return dem::fail(DEM_ERR_ARG, "RadixSortNoAlloc: null buffer");
+    if (elements <= 1) return DEM_OK;
+    if (dem::radix_scratch_words(elements) > dem::kNoAllocWords)
+        return dem::fail(DEM_ERR_ARG, "RadixSortNoAlloc: scratch sizing error");
+    uint* scratch = nullptr;
+    int rc = dem::noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return dem::radix_sort_pairs(reinterpret_cast<uint2*>(pData0), reinterpret_cast<uint2*>(pData1), elements, keybits,
+                                 scratch, dem::compat_stream());
+}

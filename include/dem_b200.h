@@ -89,6 +89,19 @@ int dem_compat_set_stream(void* cuda_stream);
 int RadixSort(KeyValuePair* pData0, KeyValuePair* pData1,
               unsigned int elements, unsigned int keybits);
 
+/* RadixSortNoAlloc(pData0, pData1, elements, keybits) -- no counterpart in the
+ * reference.  RadixSort for callers that cannot allocate device memory (a
+ * host loop whose own pool allocator owns the GPU's memory, or a
+ * latency-critical loop that must not pay a first-call allocation): the same
+ * stable sort and result, with its scratch in a fixed device array inside the
+ * library instead of cudaMalloc'd memory.  At most 4,194,304 records (larger
+ * requests return DEM_ERR_ARG); the array (about 2 MiB) is held on every GPU
+ * that loads the library until exit.  The first call on each device sets up
+ * the array's address (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised. */
+int RadixSortNoAlloc(KeyValuePair* pData0, KeyValuePair* pData1,
+                     unsigned int elements, unsigned int keybits);
+
 /* calcHash  -- particleSystem.cu:27-45, kernel neiglist.cu:54-97.
  * particleHash[2i] = clamped linear cell id of particle i, [2i+1] = i. */
 int calcHash(double* Pos, unsigned int* particleHash, unsigned int gridSize[3],

@@ -26,6 +26,7 @@ LIB_PATH = PKG_DIR / "libdem_b200.so"
 DEM_OK, DEM_ERR_ARG, DEM_ERR_CUDA, DEM_ERR_CAPACITY = 0, 1, 2, 3
 DEM_ERR_NONFINITE, DEM_ERR_SKIN, DEM_ERR_IO, DEM_ERR_STATE = 4, 5, 6, 7
 PREC_FP64, PREC_MIXED = 0, 1
+FORCE_PCCP, FORCE_PP = 0, 1
 RADII_MONO, RADII_LOGNORMAL, RADII_BIDISPERSE = 0, 1, 2
 
 _c_uint_p = ctypes.POINTER(ctypes.c_uint)
@@ -70,6 +71,7 @@ class Config(ctypes.Structure):
         ("cell", ctypes.c_double),
         ("density", ctypes.c_double),
         ("pair_capacity", ctypes.c_longlong),
+        ("force_mode", ctypes.c_int),
     ]
 
 
@@ -332,7 +334,7 @@ class Engine:
     """Owns a dem_ctx.  Host arrays are numpy float64 (AoS xyz-interleaved)."""
 
     def __init__(self, n, world, dt, skin, precision=PREC_MIXED, relist_interval=20, cell=0.0, density=1.0,
-                 pair_capacity=0):
+                 pair_capacity=0, force_mode=FORCE_PCCP):
         L = lib()
         cfg = Config()
         cfg.n = int(n)
@@ -344,6 +346,7 @@ class Engine:
         cfg.cell = float(cell)
         cfg.density = float(density)
         cfg.pair_capacity = int(pair_capacity)
+        cfg.force_mode = int(force_mode)
         self.n = int(n)
         self.cfg = cfg
         h = ctypes.c_void_p()

@@ -31,6 +31,18 @@
 
 namespace dem {
 
+// Minimum resident blocks per SM requested for the per-particle kernels (caps
+// their registers), and the largest grid of the grid-stride pair kernel.
+#ifndef DEM_PARTICLE_MINB
+#define DEM_PARTICLE_MINB 4
+#endif
+#ifndef DEM_PP_MINB
+#define DEM_PP_MINB 3
+#endif
+#ifndef DEM_PAIR_GRID_MAX
+#define DEM_PAIR_GRID_MAX (148 * 8)
+#endif
+
 enum : uint {
     kStCapacity = 1u,
     kStNonfinite = 2u,
@@ -121,8 +133,7 @@ __global__ void k_to_aos(long long n, Planes3<double> P, Planes3<double> D, Plan
 // Cell key per particle (calcHashD's role, neiglist.cu:77-97) and per-cell
 // counts; resets the displacement-since-list q (dempacking.cu:541).
 template <typename Real>
-__global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count,
-                             float4* __restrict__ Q) {
+__global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Real csr = (Real)g.cs;
@@ -133,40 +144,45 @@ __global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __re
     uint c = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
     key[i] = c;
     atomicAdd(&count[c], 1u);
-    float4 q = Q[i];
-    Q[i] = make_float4(0.f, 0.f, 0.f, q.w);
 }
 
-// Scatter ids into their cell's range; the count array returns to zero.
+// Scatter each particle (id, cell, list coordinates x,y,z,r in the list
+// precision) into its cell's range, unordered inside the cell; the count
+// array returns to zero.  Reads are coalesced by id.
+template <typename Real>
 __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint* __restrict__ cstart,
-                          uint* __restrict__ count, uint* __restrict__ sid) {
+                          uint* __restrict__ count, Planes3<double> P, const Real* __restrict__ R, GridC g,
+                          uint* __restrict__ sidu, uint* __restrict__ skeyu, R4<Real>* __restrict__ sposu) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    uint c = key[i];
-    uint slot = cstart[c] + atomicSub(&count[c], 1u) - 1u;
-    sid[slot] = (uint)i;
-}
-
-// Order each cell's members by id (stable sort by cell) and build the
-// cell-sorted list coordinates (x, y, z, r) in the list precision.
-template <typename Real>
-__global__ void k_rank(long long n, const uint* __restrict__ key, const uint* __restrict__ cstart,
-                       const uint* __restrict__ sid, Planes3<double> P, const Real* __restrict__ R, GridC g,
-                       uint* __restrict__ sid2, R4<Real>* __restrict__ spos) {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const uint i = sid[t];
     const uint c = key[i];
-    const uint s = cstart[c], e = cstart[c + 1];
-    uint rank = 0;
-    for (uint u = s; u < e; u++) rank += (sid[u] < i) ? 1u : 0u;
-    sid2[s + rank] = i;
     R4<Real> v;
     v.x = (Real)(P.x[i] - g.ox);
     v.y = (Real)(P.y[i] - g.oy);
     v.z = (Real)(P.z[i] - g.oz);
     v.w = R[i];
-    spos[s + rank] = v;
+    const uint slot = cstart[c] + atomicSub(&count[c], 1u) - 1u;
+    sidu[slot] = (uint)i;
+    skeyu[slot] = c;
+    sposu[slot] = v;
+}
+
+// Order each cell's members by id: together with the counting scatter this is
+// the stable sort by cell of calcHash + RadixSort (dempacking.cu:545-555).
+template <typename Real>
+__global__ void k_rank(long long n, const uint* __restrict__ cstart, const uint* __restrict__ sidu,
+                       const uint* __restrict__ skeyu, const R4<Real>* __restrict__ sposu, uint* __restrict__ sid2,
+                       uint* __restrict__ skey, R4<Real>* __restrict__ spos) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint i = sidu[t];
+    const uint c = skeyu[t];
+    const uint s = cstart[c], e = cstart[c + 1];
+    uint rank = 0;
+    for (uint u = s; u < e; u++) rank += (sidu[u] < i) ? 1u : 0u;
+    sid2[s + rank] = i;
+    skey[s + rank] = c;
+    spos[s + rank] = sposu[t];
 }
 
 // Walk the 27 cells around sorted slot t and either count (FILL=false) or
@@ -181,24 +197,30 @@ __device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, 
     const int cz = (int)(c / ((uint)g.gx * (uint)g.gy));
     nup = 0;
     nall = 0;
-    for (int z = cz - 1; z <= cz + 1; z++) {
-        if (z < 0 || z >= g.gz) continue;
-        for (int y = cy - 1; y <= cy + 1; y++) {
-            if (y < 0 || y >= g.gy) continue;
-            const uint rowc = ((uint)z * (uint)g.gy + (uint)y) * (uint)g.gx;
-            const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < g.gx - 1 ? cx + 1 : g.gx - 1;
-            // cells x0..x1 of this row are contiguous in the sorted order
-            const uint s = cstart[rowc + x0], e = cstart[rowc + x1 + 1];
-            for (uint u = s; u < e; u++) {
-                if ((long long)u == t) continue;
-                const R4<Real> o = spos[u];
-                if (cand_test<Real>(me, o, skin)) {
-                    nall++;
-                    const uint j = sid2[u];
-                    if (j > i) {
-                        if (FILL && nup < outcap) out[nup] = j;
-                        nup++;
-                    }
+    // The cells x-1..x+1 of one (y, z) row are contiguous in the sorted order:
+    // 9 ranges instead of 27 cells.  All 18 range bounds are loaded up front
+    // (independent loads), then the candidates are tested.
+    const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < g.gx - 1 ? cx + 1 : g.gx - 1;
+    uint rs[9], re[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        const int z = cz - 1 + r / 3, y = cy - 1 + r % 3;
+        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) { rs[r] = 0; re[r] = 0; continue; }
+        const uint rowc = ((uint)z * (uint)g.gy + (uint)y) * (uint)g.gx;
+        rs[r] = cstart[rowc + x0];
+        re[r] = cstart[rowc + x1 + 1];
+    }
+#pragma unroll 1
+    for (int r = 0; r < 9; r++) {
+        for (uint u = rs[r]; u < re[r]; u++) {
+            if ((long long)u == t) continue;
+            const R4<Real> o = spos[u];
+            if (cand_test<Real>(me, o, skin)) {
+                nall++;
+                const uint j = sid2[u];
+                if (j > i) {
+                    if (FILL && nup < outcap) out[nup] = j;
+                    nup++;
                 }
             }
         }
@@ -207,14 +229,14 @@ __device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, 
 
 template <typename Real>
 __global__ void k_nbr_count(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
-                            const uint* __restrict__ key, const uint* __restrict__ cstart, GridC g, Real skin,
+                            const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
                             uint* __restrict__ njgi, uint* __restrict__ njli, EngineWords* words) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     uint nall = 0;
     if (t < n) {
         const uint i = sid2[t];
         uint nup;
-        walk27<Real, false>(t, i, spos[t], key[i], g, cstart, sid2, spos, skin, nup, nall, nullptr, 0);
+        walk27<Real, false>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, nullptr, 0);
         njgi[i] = nup;
         njli[i] = nall - nup;
     }
@@ -236,7 +258,7 @@ __device__ __forceinline__ void isort_u32(uint* a, uint len) {
 // from the previous list, record the reverse slots.
 template <typename Real>
 __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
-                           const uint* __restrict__ key, const uint* __restrict__ cstart, GridC g, Real skin,
+                           const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
                            const uint* __restrict__ off, const uint* __restrict__ roff, uint* __restrict__ njli,
                            uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
                            const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
@@ -251,7 +273,7 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
     const uint i = sid2[t];
     const uint b = off[i], e = off[i + 1];
     uint nup, nall;
-    walk27<Real, true>(t, i, spos[t], key[i], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
+    walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
     isort_u32(ln + b, e - b);
     const bool old_ok = (long long)ooff[n] <= cap;   // an overflowed old list carries nothing
     const uint ob = old_ok ? ooff[i] : 0u, oe = old_ok ? ooff[i + 1] : 0u;
@@ -290,10 +312,42 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
 }
 
 // ------------------------------------------------------------ pair force
-// One thread per candidate pair (calculateforcepairD, neiglist.cu:156-233).
+// Contact of one listed pair (lo, hi) = (Lp, Ln), the body of
+// calculateforcepairD (neiglist.cu:156-233) with the law of dem_law.cuh.
 // Geometry from FP64 positions; in the mixed form the overlap is formed as
 // (s^2 - d^2)/(s + d) in FP64 and rounded once, the rest of the law is FP32
-// except the FP64 history update.
+// except the FP64 history update.  Returns 1 when touching; Fi is the force
+// on lo, Ti/Tj the torques on lo/hi; h is the pair's history (in/out).
+template <typename Real>
+__device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double> di, V3<double> dj, V3<Real> ai,
+                                         V3<Real> aj, Real ri, Real rj, V3<double>& h, const LawParams<Real>& pp,
+                                         Real inv_dt, Real density, V3<Real>& Fi, V3<Real>& Ti, V3<Real>& Tj) {
+    const V3<double> Dv = xj - xi;
+    const double d2 = dot(Dv, Dv);
+    const double s = (double)ri + (double)rj;
+    const double dist = sqrt(d2);
+    Real delta;
+    if (sizeof(Real) == 4) delta = (Real)((s * s - d2) / (s + dist));
+    else delta = (Real)(s - dist);
+    if (!(delta > (Real)0 && dist > 0.0)) {
+        h = zero3<double>();
+        return 0;
+    }
+    const double inv = 1.0 / dist;
+    const V3<Real> nn = cvt<Real>(Dv * inv);
+    const Real rstar = ri * rj / (ri + rj);
+    const Real mi = density * (Real)8 * ri * ri * ri, mj = density * (Real)8 * rj * rj * rj;
+    const Real mstar = mi * mj / (mi + mj);
+    const V3<Real> U = cvt<Real>(dj - di) - cross(ri * ai + rj * aj, nn);
+    V3<Real> Ft, Mr;
+    contact_law<Real>(delta, nn, rstar, mstar, U, ai - aj, h, inv_dt, pp, Fi, Ft, Mr);
+    const V3<Real> nxf = cross(nn, Ft);
+    Ti = ri * nxf + Mr;
+    Tj = rj * nxf - Mr;
+    return 1;
+}
+
+// PCCP: one thread per candidate pair; per-pair results for the gather.
 template <typename Real>
 __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long long n, long long cap,
                                               const uint* __restrict__ lp, const uint* __restrict__ ln,
@@ -306,31 +360,15 @@ __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total; k += stride) {
         const uint i = lp[k], j = ln[k];
-        const V3<double> xi = mk(P.x[i], P.y[i], P.z[i]), xj = mk(P.x[j], P.y[j], P.z[j]);
-        const V3<double> Dv = xj - xi;
-        const double d2 = dot(Dv, Dv);
-        const Real ri = R[i], rj = R[j];
-        const double s = (double)ri + (double)rj;
-        const double dist = sqrt(d2);
-        Real delta;
-        if (sizeof(Real) == 4) delta = (Real)((s * s - d2) / (s + dist));
-        else delta = (Real)(s - dist);
+        V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
+        V3<Real> Fi, Ti, Tj;
+        const int c = pair_eval<Real>(mk(P.x[i], P.y[i], P.z[i]), mk(P.x[j], P.y[j], P.z[j]),
+                                      mk(D.x[i], D.y[i], D.z[i]), mk(D.x[j], D.y[j], D.z[j]),
+                                      mk(A.x[i], A.y[i], A.z[i]), mk(A.x[j], A.y[j], A.z[j]), R[i], R[j], h, pp,
+                                      inv_dt, density, Fi, Ti, Tj);
+        H.x[k] = h.x; H.y[k] = h.y; H.z[k] = h.z;
         R4<Real> fo;
-        if (delta > (Real)0 && dist > 0.0) {
-            const double inv = 1.0 / dist;
-            const V3<Real> nn = cvt<Real>(Dv * inv);
-            const Real rstar = ri * rj / (ri + rj);
-            const Real mi = density * (Real)8 * ri * ri * ri, mj = density * (Real)8 * rj * rj * rj;
-            const Real mstar = mi * mj / (mi + mj);
-            const V3<Real> ai = mk(A.x[i], A.y[i], A.z[i]), aj = mk(A.x[j], A.y[j], A.z[j]);
-            const V3<double> dd = mk(D.x[j] - D.x[i], D.y[j] - D.y[i], D.z[j] - D.z[i]);
-            const V3<Real> U = cvt<Real>(dd) - cross(ri * ai + rj * aj, nn);
-            V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
-            V3<Real> Fi, Ft, Mr;
-            contact_law<Real>(delta, nn, rstar, mstar, U, ai - aj, h, inv_dt, pp, Fi, Ft, Mr);
-            const V3<Real> nxf = cross(nn, Ft);
-            const V3<Real> Ti = ri * nxf + Mr, Tj = rj * nxf - Mr;
-            H.x[k] = h.x; H.y[k] = h.y; H.z[k] = h.z;
+        if (c) {
             fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
             R4<Real> a4, b4;
             a4.x = Ti.x; a4.y = Ti.y; a4.z = Ti.z; a4.w = (Real)0;
@@ -338,7 +376,6 @@ __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long
             pti[k] = a4;
             ptj[k] = b4;
         } else {
-            H.x[k] = 0.0; H.y[k] = 0.0; H.z[k] = 0.0;
             fo.x = fo.y = fo.z = fo.w = (Real)0;
         }
         pf[k] = fo;
@@ -346,94 +383,69 @@ __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long
 }
 
 // --------------------------------------------------- particle update
-// Gather (sumallforceiD's role) + gravity + walls (calculateforceiwD,
-// neiglist.cu:238-306) + integrator (updatepositionD, neiglist.cu:308-409),
-// one thread per particle, with the block reductions of max height, contact
-// count and status flags finished on the device.
-struct StepSlot { unsigned long long maxhz_bits; unsigned long long contacts; };
+// Per-step observables are written as one partial per block (no same-address
+// atomics in the hot kernels) and reduced on the host when asked for.
+struct StepPartials { unsigned long long* maxhz_bits; uint* contacts; };
 
+struct ParticleCommon {
+    double dt, hx, hy;
+    float half_skin2;
+    int first;
+};
+
+// Gravity + walls (calculateforceiwD, neiglist.cu:238-306) + integrator
+// (updatepositionD, neiglist.cu:308-409) for particle i whose pair sums are
+// in F/T; writes the new state to the output planes.
 template <typename Real>
-__global__ void __launch_bounds__(256) k_particle(long long n, const uint* __restrict__ off,
-                                                  const uint* __restrict__ roff, const uint* __restrict__ rk,
-                                                  long long cap, const R4<Real>* __restrict__ pf,
-                                                  const R4<Real>* __restrict__ pti, const R4<Real>* __restrict__ ptj,
-                                                  Planes3<double> P, Planes3<double> D, Planes3<Real> A,
-                                                  const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
-                                                  LawParams<Real> pw, double dt, Real dtr, Real inv_dt, Real density,
-                                                  double hx, double hy, float half_skin2, StepSlot* slot,
-                                                  EngineWords* words, double* dbgF, double* dbgT, uint* dbgC) {
+__device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real> T, Real r, V3<double> x,
+                                                V3<double> d, V3<Real> a, float4 q, Planes3<double> Po,
+                                                Planes3<double> Do, Planes3<Real> Ao, float4* __restrict__ Q,
+                                                Planes3<double> W, const LawParams<Real>& pw, const ParticleCommon& pc,
+                                                Real dtr, Real inv_dt, Real density, double& mz, uint& flags,
+                                                uint cnt, double* dbgF, double* dbgT, uint* dbgC) {
+    const Real m = density * (Real)8 * r * r * r;
+    const Real I = (Real)0.4 * m * (r * r);
+    F.z += -m;
+    uint wflag = __float_as_uint(q.w);
+    if (pc.first) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }   // displacement since the list (dempacking.cu:541)
+    const double rd = (double)r;
+    const bool touch = (x.z < rd) || (x.x + pc.hx < rd) || (pc.hx - x.x < rd) || (x.y + pc.hy < rd) ||
+                       (pc.hy - x.y < rd);
+    if (touch || wflag) {
+        V3<double> h = wflag ? mk(W.x[i], W.y[i], W.z[i]) : zero3<double>();
+        const int hit = wall_contacts<Real>(pc.hx, pc.hy, x, cvt<Real>(d), a, r, m, h, inv_dt, pw, F, T, (Real*)nullptr);
+        if (hit || wflag) { W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z; }
+        wflag = hit ? 1u : 0u;
+    }
+    if (dbgF) {   // total force/torque of this step (pairs + gravity + walls), on request
+        dbgF[3 * i] = F.x; dbgF[3 * i + 1] = F.y; dbgF[3 * i + 2] = F.z;
+        dbgT[3 * i] = T.x; dbgT[3 * i + 1] = T.y; dbgT[3 * i + 2] = T.z;
+        dbgC[i] = cnt;
+    }
+    // symplectic Euler in displacement form (neiglist.cu:356-360)
+    const double dt = pc.dt;
+    d.x = d.x + (double)F.x * dt * dt / (double)m;
+    d.y = d.y + (double)F.y * dt * dt / (double)m;
+    d.z = d.z + (double)F.z * dt * dt / (double)m;
+    x.x += d.x; x.y += d.y; x.z += d.z;
+    a.x = a.x + T.x * dtr * dtr / I;
+    a.y = a.y + T.y * dtr * dtr / I;
+    a.z = a.z + T.z * dtr * dtr / I;
+    q.x += (float)d.x; q.y += (float)d.y; q.z += (float)d.z;
+    q.w = __uint_as_float(wflag);
+    Po.x[i] = x.x; Po.y[i] = x.y; Po.z[i] = x.z;
+    Do.x[i] = d.x; Do.y[i] = d.y; Do.z[i] = d.z;
+    Ao.x[i] = a.x; Ao.y[i] = a.y; Ao.z[i] = a.z;
+    Q[i] = q;
+    if (q.x * q.x + q.y * q.y + q.z * q.z > pc.half_skin2) flags |= kStSkin;
+    if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
+    mz = x.z > 0.0 ? x.z : 0.0;
+}
+
+__device__ __forceinline__ void block_observables(double mz, uint cnt, uint flags, StepPartials part,
+                                                  EngineWords* words) {
     __shared__ unsigned long long s_mz[8];
     __shared__ uint s_cnt[8], s_fl[8];
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double mz = 0.0;
-    uint cnt = 0, flags = 0;
-    if (i < n) {
-        V3<Real> F = zero3<Real>(), T = zero3<Real>();
-        const uint total = off[n];
-        if ((long long)total <= cap) {
-            const uint o0 = off[i], o1 = off[i + 1];
-            for (uint k = o0; k < o1; k++) {
-                const R4<Real> f = pf[k];
-                if (f.w != (Real)0) {
-                    const R4<Real> t = pti[k];
-                    F.x += f.x; F.y += f.y; F.z += f.z;
-                    T.x += t.x; T.y += t.y; T.z += t.z;
-                    cnt++;
-                }
-            }
-            const uint r0 = roff[i], r1 = roff[i + 1];
-            for (uint u = r0; u < r1; u++) {
-                const uint k = rk[u];
-                if (k >= total) continue;
-                const R4<Real> f = pf[k];
-                if (f.w != (Real)0) {
-                    const R4<Real> t = ptj[k];
-                    F.x -= f.x; F.y -= f.y; F.z -= f.z;
-                    T.x += t.x; T.y += t.y; T.z += t.z;
-                    cnt++;
-                }
-            }
-        }
-        const Real r = R[i];
-        const Real m = density * (Real)8 * r * r * r;
-        const Real I = (Real)0.4 * m * (r * r);
-        F.z += -m;
-        V3<double> x = mk(P.x[i], P.y[i], P.z[i]);
-        V3<double> d = mk(D.x[i], D.y[i], D.z[i]);
-        V3<Real> a = mk(A.x[i], A.y[i], A.z[i]);
-        float4 q = Q[i];
-        uint wflag = __float_as_uint(q.w);
-        const double rd = (double)r;
-        const bool touch = (x.z < rd) || (x.x + hx < rd) || (hx - x.x < rd) || (x.y + hy < rd) || (hy - x.y < rd);
-        if (touch || wflag) {
-            V3<double> h = wflag ? mk(W.x[i], W.y[i], W.z[i]) : zero3<double>();
-            const int hit = wall_contacts<Real>(hx, hy, x, cvt<Real>(d), a, r, m, h, inv_dt, pw, F, T, (Real*)nullptr);
-            if (hit || wflag) { W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z; }
-            wflag = hit ? 1u : 0u;
-        }
-        // symplectic Euler in displacement form (neiglist.cu:356-360)
-        d.x = d.x + (double)F.x * dt * dt / (double)m;
-        d.y = d.y + (double)F.y * dt * dt / (double)m;
-        d.z = d.z + (double)F.z * dt * dt / (double)m;
-        x.x += d.x; x.y += d.y; x.z += d.z;
-        a.x = a.x + T.x * dtr * dtr / I;
-        a.y = a.y + T.y * dtr * dtr / I;
-        a.z = a.z + T.z * dtr * dtr / I;
-        q.x += (float)d.x; q.y += (float)d.y; q.z += (float)d.z;
-        q.w = __uint_as_float(wflag);
-        P.x[i] = x.x; P.y[i] = x.y; P.z[i] = x.z;
-        D.x[i] = d.x; D.y[i] = d.y; D.z[i] = d.z;
-        A.x[i] = a.x; A.y[i] = a.y; A.z[i] = a.z;
-        Q[i] = q;
-        if (q.x * q.x + q.y * q.y + q.z * q.z > half_skin2) flags |= kStSkin;
-        if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
-        mz = x.z > 0.0 ? x.z : 0.0;
-        if (dbgF) {
-            dbgF[3 * i] = F.x; dbgF[3 * i + 1] = F.y; dbgF[3 * i + 2] = F.z;
-            dbgT[3 * i] = T.x; dbgT[3 * i + 1] = T.y; dbgT[3 * i + 2] = T.z;
-            dbgC[i] = cnt;
-        }
-    }
     unsigned long long mb = (unsigned long long)__double_as_longlong(mz);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -448,10 +460,118 @@ __global__ void __launch_bounds__(256) k_particle(long long n, const uint* __res
     if (threadIdx.x == 0) {
         const int nw = blockDim.x >> 5;
         for (int w = 1; w < nw; w++) { mb = s_mz[w] > mb ? s_mz[w] : mb; cnt += s_cnt[w]; flags |= s_fl[w]; }
-        if (mb) atomicMax(&slot->maxhz_bits, mb);
-        if (cnt) atomicAdd(&slot->contacts, (unsigned long long)cnt);
+        part.maxhz_bits[blockIdx.x] = mb;
+        part.contacts[blockIdx.x] = cnt;
         if (flags) atomicOr(&words->status, flags);
     }
+}
+
+// PCCP gather (sumallforceiD's role, through the CSR rows and the reverse
+// rows) + particle_finish, one thread per particle.  State is updated in place.
+template <typename Real>
+__global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n, const uint* __restrict__ off,
+                                                  const uint* __restrict__ roff, const uint* __restrict__ rk,
+                                                  long long cap, const R4<Real>* __restrict__ pf,
+                                                  const R4<Real>* __restrict__ pti, const R4<Real>* __restrict__ ptj,
+                                                  Planes3<double> P, Planes3<double> D, Planes3<Real> A,
+                                                  const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
+                                                  LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt,
+                                                  Real density, StepPartials part, EngineWords* words, double* dbgF,
+                                                  double* dbgT, uint* dbgC) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    if (i < n) {
+        // every per-particle load is issued before the data-dependent loops
+        const Real r = R[i];
+        const V3<double> x = mk(P.x[i], P.y[i], P.z[i]);
+        const V3<double> d = mk(D.x[i], D.y[i], D.z[i]);
+        const V3<Real> a = mk(A.x[i], A.y[i], A.z[i]);
+        const float4 q = Q[i];
+        const uint total = off[n];
+        const uint o0 = off[i], o1 = off[i + 1], r0 = roff[i], r1 = roff[i + 1];
+        V3<Real> F = zero3<Real>(), T = zero3<Real>();
+        if ((long long)total <= cap) {
+            for (uint k = o0; k < o1; k++) {
+                const R4<Real> f = pf[k];
+                if (f.w != (Real)0) {
+                    const R4<Real> t = pti[k];
+                    F.x += f.x; F.y += f.y; F.z += f.z;
+                    T.x += t.x; T.y += t.y; T.z += t.z;
+                    cnt++;
+                }
+            }
+            for (uint u = r0; u < r1; u++) {
+                const uint k = rk[u];
+                if (k >= total) continue;
+                const R4<Real> f = pf[k];
+                if (f.w != (Real)0) {
+                    const R4<Real> t = ptj[k];
+                    F.x -= f.x; F.y -= f.y; F.z -= f.z;
+                    T.x += t.x; T.y += t.y; T.z += t.z;
+                    cnt++;
+                }
+            }
+        }
+        particle_finish<Real>(i, F, T, r, x, d, a, q, P, D, A, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt,
+                              dbgF, dbgT, dbgC);
+    }
+    block_observables(mz, cnt, flags, part, words);
+}
+
+// PP (particle-parallel, the paper's Figure 1(b)): each particle evaluates all
+// of its pairs itself -- its own row (it is lo) and its reverse row (it is hi)
+// -- so one kernel does the whole step.  Each pair is evaluated by both of its
+// particles with the same arguments in the same order, so the two results are
+// bit-identical; only lo writes the pair's new history.  State and history
+// are read from the "in" buffers and written to the "out" buffers (ping-pong).
+template <typename Real>
+__global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
+    long long n, const uint* __restrict__ off, const uint* __restrict__ roff, const uint* __restrict__ rk,
+    const uint* __restrict__ lp, const uint* __restrict__ ln, long long cap, Planes3<double> Pi, Planes3<double> Di,
+    Planes3<Real> Ai, Planes3<double> Po, Planes3<double> Do, Planes3<Real> Ao, const Real* __restrict__ R,
+    float4* __restrict__ Q, Planes3<double> W, Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp,
+    LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt, Real density, StepPartials part,
+    EngineWords* words, double* dbgF, double* dbgT, uint* dbgC) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    if (i < n) {
+        const Real r = R[i];
+        const V3<double> x = mk(Pi.x[i], Pi.y[i], Pi.z[i]);
+        const V3<double> d = mk(Di.x[i], Di.y[i], Di.z[i]);
+        const V3<Real> a = mk(Ai.x[i], Ai.y[i], Ai.z[i]);
+        const float4 q = Q[i];
+        const uint total = off[n];
+        const uint o0 = off[i], o1 = off[i + 1], r0 = roff[i], r1 = roff[i + 1];
+        V3<Real> F = zero3<Real>(), T = zero3<Real>();
+        if ((long long)total <= cap) {
+            for (uint k = o0; k < o1; k++) {
+                const uint j = ln[k];
+                V3<double> h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
+                V3<Real> Fl, Tl, Th;
+                const int c = pair_eval<Real>(x, mk(Pi.x[j], Pi.y[j], Pi.z[j]), d, mk(Di.x[j], Di.y[j], Di.z[j]), a,
+                                              mk(Ai.x[j], Ai.y[j], Ai.z[j]), r, R[j], h, pp, inv_dt, density, Fl, Tl,
+                                              Th);
+                Ho.x[k] = h.x; Ho.y[k] = h.y; Ho.z[k] = h.z;
+                if (c) { F += Fl; T += Tl; cnt++; }
+            }
+            for (uint u = r0; u < r1; u++) {
+                const uint k = rk[u];
+                if (k >= total) continue;
+                const uint j = lp[k];
+                V3<double> h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
+                V3<Real> Fl, Tl, Th;
+                const int c = pair_eval<Real>(mk(Pi.x[j], Pi.y[j], Pi.z[j]), x, mk(Di.x[j], Di.y[j], Di.z[j]), d,
+                                              mk(Ai.x[j], Ai.y[j], Ai.z[j]), a, R[j], r, h, pp, inv_dt, density, Fl,
+                                              Tl, Th);
+                if (c) { F -= Fl; T += Th; cnt++; }
+            }
+        }
+        particle_finish<Real>(i, F, T, r, x, d, a, q, Po, Do, Ao, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt,
+                              dbgF, dbgT, dbgC);
+    }
+    block_observables(mz, cnt, flags, part, words);
 }
 
 __global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned long long* out) {
@@ -495,6 +615,7 @@ using namespace dem;
 struct dem_ctx {
     dem_config cfg{};
     int prec = DEM_PREC_MIXED;
+    int mode = DEM_FORCE_PCCP;
     long long n = 0, npad = 0, cap = 0;
     int device = 0;
     cudaStream_t stream = 0;
@@ -507,18 +628,22 @@ struct dem_ctx {
     long long ncells = 0;
     double rmax = 0.0;
     double vol = 0.0;        // sum (4/3) pi r^3
-    // state
-    double* pos = nullptr;   // 3 planes
-    double* disp = nullptr;  // 3 planes
-    void* ang = nullptr;     // 3 planes, Real
+    // state: [current buffer]; the second buffer exists in PP mode only
+    double* pos[2] = {nullptr, nullptr};   // 3 planes
+    double* disp[2] = {nullptr, nullptr};  // 3 planes
+    void* ang[2] = {nullptr, nullptr};     // 3 planes, Real
+    int sbuf = 0;
     void* rad = nullptr;     // Real
     float4* q = nullptr;
     double* wh = nullptr;    // 3 planes
     double* staging = nullptr;   // 10n doubles
     // list
     uint* key = nullptr;
-    uint* sid = nullptr;
-    uint* sid2 = nullptr;
+    uint* sid = nullptr;     // unordered within cells (scatter)
+    uint* sid2 = nullptr;    // sorted by (cell, id)
+    uint* skeyu = nullptr;
+    uint* skey = nullptr;
+    void* sposu = nullptr;
     void* spos = nullptr;
     uint* ccount = nullptr;
     uint* cstart = nullptr;
@@ -528,7 +653,8 @@ struct dem_ctx {
     uint* roff = nullptr;
     uint* ln[2] = {nullptr, nullptr};
     uint* lp = nullptr;
-    double* hist[2] = {nullptr, nullptr};  // 3 planes of cap
+    double* hist[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [list buffer][phase], 3 planes of cap
+    int hph = 0;             // history phase of the current list (PP ping-pong)
     uint* rk = nullptr;
     void* pf = nullptr;
     void* pti = nullptr;
@@ -537,7 +663,9 @@ struct dem_ctx {
     size_t scan_words = 0;
     // scalars
     EngineWords* words = nullptr;
-    StepSlot* slots = nullptr;       // relist_interval slots
+    unsigned long long* part_mz = nullptr;   // relist_interval x nblk
+    uint* part_cnt = nullptr;                // relist_interval x nblk
+    unsigned nblk = 0;                       // blocks of the particle kernel
     unsigned long long* rmax_bits = nullptr;
     void* host_pinned = nullptr;     // mirror for scalars
     // debug force record
@@ -550,8 +678,8 @@ struct dem_ctx {
     long long step = 0, in_window = 0, relists = 0;
     int last_slot = -1;
     bool uploaded = false;
-    // graphs (window starting from list buffer 0 or 1)
-    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    // window graphs keyed by (previous list buffer, state buffer, history phase)
+    cudaGraphExec_t gexec[2][2][2] = {};
     // profiling
     bool profiling = false;
     double ktime[3] = {0, 0, 0};
@@ -574,8 +702,10 @@ template <typename Real> Planes3<Real> planes(void* base, long long npad) {
 }
 
 void free_graphs(dem_ctx* c) {
-    for (int s = 0; s < 2; s++)
-        if (c->gexec[s]) { cudaGraphExecDestroy(c->gexec[s]); c->gexec[s] = nullptr; }
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int h = 0; h < 2; h++)
+                if (c->gexec[a][b][h]) { cudaGraphExecDestroy(c->gexec[a][b][h]); c->gexec[a][b][h] = nullptr; }
 }
 
 void free_cells(dem_ctx* c) {
@@ -584,30 +714,48 @@ void free_cells(dem_ctx* c) {
     c->ccount = c->cstart = nullptr;
 }
 
+ParticleCommon particle_common(const dem_ctx* c, int slot) {
+    ParticleCommon pc;
+    pc.dt = c->cfg.dt;
+    pc.hx = c->cfg.world[0] * 0.5;
+    pc.hy = c->cfg.world[1] * 0.5;
+    const float hs = (float)(0.5 * c->cfg.skin);
+    pc.half_skin2 = hs * hs;
+    pc.first = slot == 0 ? 1 : 0;
+    return pc;
+}
+
+StepPartials partials(const dem_ctx* c, int slot) {
+    return StepPartials{c->part_mz + (size_t)slot * c->nblk, c->part_cnt + (size_t)slot * c->nblk};
+}
+
+// List build from the current state, carrying history from list buffer src
+// (phase c->hph) into buffer 1-src (phase 0).
 template <typename Real> int launch_relist(dem_ctx* c, int src) {
     const long long n = c->n, np = c->npad;
     const int dst = 1 - src;
     const int B = 256;
     cudaStream_t s = c->stream;
-    Planes3<double> P = planes<double>(c->pos, np);
+    Planes3<double> P = planes<double>(c->pos[c->sbuf], np);
     GridC g = c->grid;
-    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount, c->q);
+    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount);
     int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
     if (rc) return rc;
-    k_scatter<<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->ccount, c->sid);
-    k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->sid, P, (const Real*)c->rad, g, c->sid2,
-                                              (R4<Real>*)c->spos);
+    k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->ccount, P, (const Real*)c->rad, g, c->sid,
+                                                 c->skeyu, (R4<Real>*)c->sposu);
+    k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->cstart, c->sid, c->skeyu, (const R4<Real>*)c->sposu, c->sid2,
+                                              c->skey, (R4<Real>*)c->spos);
     const Real skin = (Real)c->cfg.skin;
-    k_nbr_count<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->key, c->cstart, g, skin,
+    k_nbr_count<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin,
                                                    c->njgi, c->njli, c->words);
     rc = exclusive_scan_u32(c->njgi, c->off[dst], n, c->off[dst] + n, c->scan_tmp, s);
     if (rc) return rc;
     rc = exclusive_scan_u32(c->njli, c->roff, n, c->roff + n, c->scan_tmp, s);
     if (rc) return rc;
     k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
-        n, c->sid2, (const R4<Real>*)c->spos, c->key, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
-        c->lp, planes<double>(c->hist[dst], c->cap), c->off[src], c->ln[src], planes<double>(c->hist[src], c->cap),
-        c->rk, (R4<Real>*)c->pf, c->cap, c->words);
+        n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
+        c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
+        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words);
     k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->off[dst], c->cap);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
@@ -617,12 +765,13 @@ template <typename Real> int launch_pair(dem_ctx* c, int lst) {
     const long long np = c->npad;
     LawParams<Real> pp = make_law<Real>(c->mat.pp);
     long long want = (c->cap + 255) / 256;
-    unsigned grid = (unsigned)std::min<long long>(std::max<long long>(want, 1), 148LL * 8);
-    k_pair<Real><<<grid, 256, 0, c->stream>>>(c->off[lst], c->n, c->cap, c->lp, c->ln[lst], planes<double>(c->pos, np),
-                                               planes<double>(c->disp, np), planes<Real>(c->ang, np),
-                                               (const Real*)c->rad, planes<double>(c->hist[lst], c->cap), pp,
-                                               (Real)(1.0 / c->cfg.dt), (Real)c->cfg.density, (R4<Real>*)c->pf,
-                                               (R4<Real>*)c->pti, (R4<Real>*)c->ptj);
+    unsigned grid = (unsigned)std::min<long long>(std::max<long long>(want, 1), (long long)DEM_PAIR_GRID_MAX);
+    k_pair<Real><<<grid, 256, 0, c->stream>>>(c->off[lst], c->n, c->cap, c->lp, c->ln[lst],
+                                               planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
+                                               planes<Real>(c->ang[0], np), (const Real*)c->rad,
+                                               planes<double>(c->hist[lst][0], c->cap), pp, (Real)(1.0 / c->cfg.dt),
+                                               (Real)c->cfg.density, (R4<Real>*)c->pf, (R4<Real>*)c->pti,
+                                               (R4<Real>*)c->ptj);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -631,13 +780,29 @@ template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
     const long long n = c->n, np = c->npad;
     LawParams<Real> pw = make_law<Real>(c->mat.pw);
     const double dt = c->cfg.dt;
-    const float hs = (float)(0.5 * c->cfg.skin);
     k_particle<Real><<<grid_for(n, 256), 256, 0, c->stream>>>(
         n, c->off[lst], c->roff, c->rk, c->cap, (const R4<Real>*)c->pf, (const R4<Real>*)c->pti,
-        (const R4<Real>*)c->ptj, planes<double>(c->pos, np), planes<double>(c->disp, np), planes<Real>(c->ang, np),
-        (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw, dt, (Real)dt, (Real)(1.0 / dt),
-        (Real)c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, hs * hs, c->slots + slot, c->words,
+        (const R4<Real>*)c->ptj, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
+        planes<Real>(c->ang[0], np), (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw,
+        particle_common(c, slot), (Real)dt, (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words,
         c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+// PP step: reads state buffer sbuf and history phase hph, writes the others.
+template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, int hp) {
+    const long long n = c->n, np = c->npad;
+    LawParams<Real> pp = make_law<Real>(c->mat.pp), pw = make_law<Real>(c->mat.pw);
+    const double dt = c->cfg.dt;
+    k_step_pp<Real><<<grid_for(n, 256), 256, 0, c->stream>>>(
+        n, c->off[lst], c->roff, c->rk, c->lp, c->ln[lst], c->cap, planes<double>(c->pos[sb], np),
+        planes<double>(c->disp[sb], np), planes<Real>(c->ang[sb], np), planes<double>(c->pos[1 - sb], np),
+        planes<double>(c->disp[1 - sb], np), planes<Real>(c->ang[1 - sb], np), (const Real*)c->rad, c->q,
+        planes<double>(c->wh, np), planes<double>(c->hist[lst][hp], c->cap),
+        planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw, particle_common(c, slot), (Real)dt, (Real)(1.0 / dt),
+        (Real)c->cfg.density, partials(c, slot), c->words, c->record ? c->dbgF : nullptr,
+        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -645,48 +810,78 @@ template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
 int relist(dem_ctx* c, int src) {
     return c->prec == DEM_PREC_MIXED ? launch_relist<float>(c, src) : launch_relist<double>(c, src);
 }
-int pair_step(dem_ctx* c, int lst) {
-    return c->prec == DEM_PREC_MIXED ? launch_pair<float>(c, lst) : launch_pair<double>(c, lst);
-}
-int particle_step(dem_ctx* c, int lst, int slot) {
-    return c->prec == DEM_PREC_MIXED ? launch_particle<float>(c, lst, slot) : launch_particle<double>(c, lst, slot);
+
+// One DEM step on list buffer lst (window slot `slot`): PCCP = pair kernel +
+// particle kernel; PP = one kernel.  Advances the ping-pong indices.
+int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part) {
+    int rc;
+    const bool mixed = c->prec == DEM_PREC_MIXED;
+    if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+    if (c->mode == DEM_FORCE_PP) {
+        rc = mixed ? launch_pp<float>(c, lst, slot, c->sbuf, c->hph) : launch_pp<double>(c, lst, slot, c->sbuf, c->hph);
+        if (rc) return rc;
+        if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+        c->sbuf ^= 1;
+        c->hph ^= 1;
+    } else {
+        rc = mixed ? launch_pair<float>(c, lst) : launch_pair<double>(c, lst);
+        if (rc) return rc;
+        if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+        rc = mixed ? launch_particle<float>(c, lst, slot) : launch_particle<double>(c, lst, slot);
+        if (rc) return rc;
+    }
+    if (c->profiling) {
+        DEM_CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
+        float a = 0.f, b = 0.f;
+        DEM_CUDA_TRY(cudaEventSynchronize(c->ev[2]));
+        DEM_CUDA_TRY(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+        DEM_CUDA_TRY(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+        if (c->mode == DEM_FORCE_PP) { *ms_pair = 0.0; *ms_part = a; }
+        else { *ms_pair = a; *ms_part = b; }
+    }
+    return DEM_OK;
 }
 
-// Enqueue one full window (re-list from list `src`, then K steps) on c->stream.
+// Enqueue one full window (re-list from list `src`, then K steps).
 int enqueue_window(dem_ctx* c, int src) {
     const int K = c->cfg.relist_interval;
-    DEM_CUDA_TRY(cudaMemsetAsync(c->slots, 0, (size_t)K * sizeof(StepSlot), c->stream));
     int rc = relist(c, src);
     if (rc) return rc;
+    c->hph = 0;
     const int lst = 1 - src;
+    double a, b;
     for (int s = 0; s < K; s++) {
-        rc = pair_step(c, lst);
-        if (rc) return rc;
-        rc = particle_step(c, lst, s);
+        rc = step_kernels(c, lst, s, &a, &b);
         if (rc) return rc;
     }
     return DEM_OK;
 }
 
-int build_graph(dem_ctx* c, int src) {
-    if (c->gexec[src]) return DEM_OK;
-    cudaGraph_t g = nullptr;
-    DEM_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_window(c, src);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
-    e = cudaGraphInstantiate(&c->gexec[src], g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
-    return DEM_OK;
-}
-
-int ev_ms(cudaEvent_t a, cudaEvent_t b, double* out) {
-    float ms = 0.f;
-    DEM_CUDA_TRY(cudaEventSynchronize(b));
-    DEM_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
-    *out = ms;
+// Capture (once) and launch the window graph for the current buffers.
+int launch_window_graph(dem_ctx* c) {
+    const int src = c->cur, sb = c->sbuf, hp = c->hph;
+    cudaGraphExec_t& ge = c->gexec[src][sb][hp];
+    if (!ge) {
+        cudaGraph_t g = nullptr;
+        DEM_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_window(c, src);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        // capture only records: restore the indices, the launch below advances them
+        c->sbuf = sb;
+        c->hph = hp;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+        e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    }
+    DEM_CUDA_TRY(cudaGraphLaunch(ge, c->stream));
+    const int K = c->cfg.relist_interval;
+    c->hph = 0;
+    if (c->mode == DEM_FORCE_PP) {
+        c->sbuf = (sb + K) & 1;
+        c->hph = K & 1;
+    }
     return DEM_OK;
 }
 
@@ -702,6 +897,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if (cfg->n <= 0 || cfg->n > 0x7fffffffLL) return fail(DEM_ERR_ARG, "dem_create: n out of range (%lld)", cfg->n);
     if (cfg->precision != DEM_PREC_FP64 && cfg->precision != DEM_PREC_MIXED)
         return fail(DEM_ERR_ARG, "dem_create: unknown precision %d", cfg->precision);
+    if (cfg->force_mode != DEM_FORCE_PCCP && cfg->force_mode != DEM_FORCE_PP)
+        return fail(DEM_ERR_ARG, "dem_create: unknown force mode %d", cfg->force_mode);
     if (cfg->relist_interval <= 0 || cfg->relist_interval > 100000)
         return fail(DEM_ERR_ARG, "dem_create: relist_interval must be in [1, 100000]");
     if (!(cfg->dt > 0.0) || !(cfg->skin > 0.0) || !(cfg->density > 0.0))
@@ -711,6 +908,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     dem_ctx* c = new dem_ctx();
     c->cfg = *cfg;
     c->prec = cfg->precision;
+    c->mode = cfg->force_mode;
     c->n = cfg->n;
     c->npad = (cfg->n + 63) / 64 * 64;
     c->cap = cfg->pair_capacity > 0 ? cfg->pair_capacity : 8 * cfg->n;
@@ -721,24 +919,35 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaGetDevice", __FILE__, __LINE__));
     const long long n = c->n, np = c->npad, cap = c->cap;
     const size_t rs = real_size(c->prec);
-    if ((rc = dalloc(&c->pos, 3 * np)) || (rc = dalloc(&c->disp, 3 * np)) || (rc = dalloc(&c->wh, 3 * np)) ||
-        (rc = dalloc(&c->q, np)) || (rc = dalloc(&c->staging, 10 * np)) || (rc = dalloc(&c->key, np)) ||
-        (rc = dalloc(&c->sid, np)) || (rc = dalloc(&c->sid2, np)) || (rc = dalloc(&c->njgi, np)) ||
+    const int nstate = c->mode == DEM_FORCE_PP ? 2 : 1;
+    for (int b = 0; b < nstate; b++) {
+        if ((rc = dalloc(&c->pos[b], 3 * np)) || (rc = dalloc(&c->disp[b], 3 * np))) return bail(rc);
+        e = cudaMalloc(&c->ang[b], 3 * np * rs);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (state)", __FILE__, __LINE__));
+    }
+    for (int l = 0; l < 2; l++)
+        for (int h = 0; h < nstate; h++)
+            if ((rc = dalloc(&c->hist[l][h], 3 * cap))) return bail(rc);
+    if ((rc = dalloc(&c->wh, 3 * np)) || (rc = dalloc(&c->q, np)) || (rc = dalloc(&c->staging, 10 * np)) ||
+        (rc = dalloc(&c->key, np)) || (rc = dalloc(&c->sid, np)) || (rc = dalloc(&c->sid2, np)) ||
+        (rc = dalloc(&c->skeyu, np)) || (rc = dalloc(&c->skey, np)) || (rc = dalloc(&c->njgi, np)) ||
         (rc = dalloc(&c->njli, np)) || (rc = dalloc(&c->off[0], np + 1)) || (rc = dalloc(&c->off[1], np + 1)) ||
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
-        (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->hist[0], 3 * cap)) || (rc = dalloc(&c->hist[1], 3 * cap)) ||
-        (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->words, 1)) ||
-        (rc = dalloc(&c->slots, (size_t)cfg->relist_interval)) || (rc = dalloc(&c->rmax_bits, 2)))
+        (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->words, 1)) ||
+        (rc = dalloc(&c->rmax_bits, 2)))
         return bail(rc);
-    e = cudaMalloc(&c->ang, 3 * np * rs);
-    if (e == cudaSuccess) e = cudaMalloc(&c->rad, np * rs);
+    e = cudaMalloc(&c->rad, np * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->spos, np * 4 * rs);
+    if (e == cudaSuccess) e = cudaMalloc(&c->sposu, np * 4 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->pf, cap * 4 * rs);
-    if (e == cudaSuccess) e = cudaMalloc(&c->pti, cap * 4 * rs);
-    if (e == cudaSuccess) e = cudaMalloc(&c->ptj, cap * 4 * rs);
+    if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->pti, cap * 4 * rs);
+    if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->ptj, cap * 4 * rs);
     if (e == cudaSuccess) e = cudaMallocHost(&c->host_pinned, 4096);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (engine buffers)", __FILE__, __LINE__));
-    (void)n;
+    c->nblk = grid_for(n, 256);
+    if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->nblk)) ||
+        (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->nblk)))
+        return bail(rc);
     c->scan_words = scan_scratch_words(std::max<long long>(np + 1, 1));
     if ((rc = dalloc(&c->scan_tmp, c->scan_words))) return bail(rc);
     e = cudaMemset(c->words, 0, sizeof(EngineWords));
@@ -763,10 +972,11 @@ int dem_destroy(dem_ctx* c) {
     cudaStreamSynchronize(c->stream);
     free_graphs(c);
     free_cells(c);
-    void* ptrs[] = {c->pos, c->disp, c->ang, c->rad, c->q, c->wh, c->staging, c->key, c->sid, c->sid2, c->spos,
-                    c->njgi, c->njli, c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0],
-                    c->hist[1], c->rk, c->pf, c->pti, c->ptj, c->scan_tmp, c->words, c->slots, c->rmax_bits,
-                    c->dbgF, c->dbgT, c->dbgC};
+    void* ptrs[] = {c->pos[0], c->pos[1], c->disp[0], c->disp[1], c->ang[0], c->ang[1], c->rad, c->q, c->wh,
+                    c->staging, c->key, c->sid, c->sid2, c->spos, c->skeyu, c->skey, c->sposu, c->njgi, c->njli,
+                    c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
+                    c->hist[1][0], c->hist[1][1], c->rk, c->pf, c->pti, c->ptj, c->scan_tmp, c->words, c->part_mz,
+                    c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
@@ -843,8 +1053,9 @@ static int finish_upload(dem_ctx* c) {
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[0], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[1], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->words, 0, sizeof(EngineWords), c->stream));
-    DEM_CUDA_TRY(cudaMemsetAsync(c->slots, 0, (size_t)c->cfg.relist_interval * sizeof(StepSlot), c->stream));
     c->cur = 0;
+    c->sbuf = 0;
+    c->hph = 0;
     c->step = 0;
     c->in_window = 0;
     c->relists = 0;
@@ -894,12 +1105,12 @@ static int upload_common(dem_ctx* c, const double* pos, const double* pdis, cons
     }
     if (c->prec == DEM_PREC_MIXED)
         k_from_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(
-            n, ppos, ppd, ppa, prad, planes<double>(c->pos, np), planes<double>(c->disp, np), planes<float>(c->ang, np),
-            (float*)c->rad, c->q, planes<double>(c->wh, np));
+            n, ppos, ppd, ppa, prad, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
+            planes<float>(c->ang[0], np), (float*)c->rad, c->q, planes<double>(c->wh, np));
     else
         k_from_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(
-            n, ppos, ppd, ppa, prad, planes<double>(c->pos, np), planes<double>(c->disp, np),
-            planes<double>(c->ang, np), (double*)c->rad, c->q, planes<double>(c->wh, np));
+            n, ppos, ppd, ppa, prad, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
+            planes<double>(c->ang[0], np), (double*)c->rad, c->q, planes<double>(c->wh, np));
     DEM_LAUNCH_CHECK();
     return finish_upload(c);
 }
@@ -915,19 +1126,20 @@ static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, 
     if (!c) return fail(DEM_ERR_ARG, "dem_download_state: null ctx");
     if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_download_state: no state uploaded");
     const long long n = c->n, np = c->npad;
+    const int sb = c->sbuf;
     double* st = c->staging;
     double *tp = host ? st : pos, *td = host ? st + 3 * np : pdis, *ta = host ? st + 6 * np : angv;
     if (!pos) tp = nullptr;
     if (!pdis) td = nullptr;
     if (!angv) ta = nullptr;
     if (c->prec == DEM_PREC_MIXED)
-        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos, np),
-                                                                planes<double>(c->disp, np), planes<float>(c->ang, np),
-                                                                tp, td, ta);
+        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos[sb], np),
+                                                                planes<double>(c->disp[sb], np),
+                                                                planes<float>(c->ang[sb], np), tp, td, ta);
     else
-        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos, np),
-                                                                 planes<double>(c->disp, np),
-                                                                 planes<double>(c->ang, np), tp, td, ta);
+        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos[sb], np),
+                                                                 planes<double>(c->disp[sb], np),
+                                                                 planes<double>(c->ang[sb], np), tp, td, ta);
     DEM_LAUNCH_CHECK();
     if (host) {
         if (pos) DEM_CUDA_TRY(cudaMemcpyAsync(pos, tp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -955,9 +1167,8 @@ int dem_step_n(dem_ctx* c, long long nsteps) {
     while (nsteps > 0) {
         if (c->in_window == 0 && nsteps >= K && !c->profiling) {
             // whole window: replay the captured graph
-            rc = build_graph(c, c->cur);
+            rc = launch_window_graph(c);
             if (rc) return rc;
-            DEM_CUDA_TRY(cudaGraphLaunch(c->gexec[c->cur], c->stream));
             c->cur = 1 - c->cur;
             c->relists++;
             c->step += K;
@@ -966,31 +1177,26 @@ int dem_step_n(dem_ctx* c, long long nsteps) {
             continue;
         }
         if (c->in_window == 0) {
-            DEM_CUDA_TRY(cudaMemsetAsync(c->slots, 0, (size_t)K * sizeof(StepSlot), c->stream));
             if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
             rc = relist(c, c->cur);
             if (rc) return rc;
             if (c->profiling) {
-                DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
-                double ms;
-                if ((rc = ev_ms(c->ev[0], c->ev[1], &ms))) return rc;
+                DEM_CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
+                float ms = 0.f;
+                DEM_CUDA_TRY(cudaEventSynchronize(c->ev[3]));
+                DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev[0], c->ev[3]));
                 c->ktime[0] += ms;
                 c->kcount[0]++;
             }
             c->cur = 1 - c->cur;
+            c->hph = 0;
             c->relists++;
         }
         const int slot = (int)c->in_window;
-        if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
-        rc = pair_step(c, c->cur);
-        if (rc) return rc;
-        if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
-        rc = particle_step(c, c->cur, slot);
+        double a = 0, b = 0;
+        rc = step_kernels(c, c->cur, slot, &a, &b);
         if (rc) return rc;
         if (c->profiling) {
-            DEM_CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
-            double a, b;
-            if ((rc = ev_ms(c->ev[0], c->ev[1], &a)) || (rc = ev_ms(c->ev[1], c->ev[2], &b))) return rc;
             c->ktime[1] += a; c->kcount[1]++;
             c->ktime[2] += b; c->kcount[2]++;
         }
@@ -1010,27 +1216,37 @@ int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
     char* hp = (char*)c->host_pinned;
     DEM_CUDA_TRY(cudaMemcpyAsync(hp, c->words, sizeof(EngineWords), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaMemcpyAsync(hp + 64, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    if (c->last_slot >= 0)
-        DEM_CUDA_TRY(cudaMemcpyAsync(hp + 128, c->slots + c->last_slot, sizeof(StepSlot), cudaMemcpyDeviceToHost,
-                                     c->stream));
+    std::vector<unsigned long long> pm;
+    std::vector<uint> pc;
+    if (c->last_slot >= 0) {
+        pm.resize(c->nblk);
+        pc.resize(c->nblk);
+        DEM_CUDA_TRY(cudaMemcpyAsync(pm.data(), c->part_mz + (size_t)c->last_slot * c->nblk,
+                                     c->nblk * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        DEM_CUDA_TRY(cudaMemcpyAsync(pc.data(), c->part_cnt + (size_t)c->last_slot * c->nblk, c->nblk * sizeof(uint),
+                                     cudaMemcpyDeviceToHost, c->stream));
+    }
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     EngineWords w;
     memcpy(&w, hp, sizeof(w));
     uint P;
     memcpy(&P, hp + 64, sizeof(P));
-    StepSlot sl{0, 0};
-    if (c->last_slot >= 0) memcpy(&sl, hp + 128, sizeof(sl));
+    unsigned long long mzb = 0, csum = 0;
+    for (size_t b = 0; b < pm.size(); b++) {
+        mzb = std::max(mzb, pm[b]);
+        csum += pc[b];
+    }
     double mz;
-    memcpy(&mz, &sl.maxhz_bits, sizeof(mz));
+    memcpy(&mz, &mzb, sizeof(mz));
     out->step = c->step;
     out->pairs = c->relists ? (long long)P : 0;
-    out->contacts = (long long)(sl.contacts / 2);
+    out->contacts = (long long)(csum / 2);
     out->maxhz = mz;
     out->relists = c->relists;
     out->max_row = (int)w.max_row;
     // packing fraction sum (4/3) pi r^3 / (Wx Wy maxhz): dempacking.cu:768-771
     // with the monodisperse N pi/6 generalised; mean CN = pcntot/N (:768).
-    out->mean_cn = c->n > 0 ? (double)sl.contacts / (double)c->n : 0.0;
+    out->mean_cn = c->n > 0 ? (double)csum / (double)c->n : 0.0;
     out->packing_fraction = mz > 0.0 ? c->vol / (c->cfg.world[0] * c->cfg.world[1] * mz) : 0.0;
     int status = DEM_OK;
     if (w.status & kStNonfinite) status = DEM_ERR_NONFINITE;
@@ -1087,7 +1303,7 @@ int dem_download_pairs(dem_ctx* c, unsigned int* lp, unsigned int* ln, double* h
     int rc;
     if ((rc = dalloc(&dlp, P)) || (rc = dalloc(&dln, P)) || (rc = dalloc(&dh, 3 * (size_t)P))) return rc;
     k_pairs_out<<<grid_for(P, 256), 256, 0, c->stream>>>(c->off[lst], c->n, c->cap, c->lp, c->ln[lst],
-                                                          planes<double>(c->hist[lst], c->cap), dlp, dln, dh);
+                                                          planes<double>(c->hist[lst][c->hph], c->cap), dlp, dln, dh);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(lp, dlp, P * sizeof(uint), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ln, dln, P * sizeof(uint), cudaMemcpyDeviceToHost, c->stream);
@@ -1106,24 +1322,14 @@ int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsign
     if (!c->uploaded || c->relists == 0) return fail(DEM_ERR_STATE, "dem_download_cells: no list built yet");
     const long long n = c->n, nc = c->ncells;
     if (ids) DEM_CUDA_TRY(cudaMemcpyAsync(ids, c->sid2, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    if (keys) DEM_CUDA_TRY(cudaMemcpyAsync(keys, c->skey, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     std::vector<uint> cs;
-    if (cell_start || cell_end || keys) {
-        if (ncells_cap < nc && (cell_start || cell_end))
-            return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
+    if (cell_start || cell_end) {
+        if (ncells_cap < nc) return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
         cs.resize(nc + 1);
         DEM_CUDA_TRY(cudaMemcpyAsync(cs.data(), c->cstart, (nc + 1) * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     }
-    std::vector<uint> k;
-    if (keys) {
-        k.resize(n);
-        DEM_CUDA_TRY(cudaMemcpyAsync(k.data(), c->key, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    }
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    if (keys) {
-        // sorted keys: expand the cell ranges
-        for (long long cc = 0; cc < nc; cc++)
-            for (uint t = cs[cc]; t < cs[cc + 1]; t++) keys[t] = (uint)cc;
-    }
     if (cell_start || cell_end) {
         for (long long cc = 0; cc < nc; cc++) {
             bool empty = cs[cc] == cs[cc + 1];

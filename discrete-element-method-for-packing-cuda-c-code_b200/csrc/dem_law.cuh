@@ -108,7 +108,9 @@ DEM_HD int wall_contacts(double hx, double hy, V3<double> x, V3<F> d, V3<F> a, F
     }
     V3<double> newxi = zero3<double>();
     F newfr = F(0);
-#pragma unroll
+    // one copy of the law for all five walls (keeps the register footprint of
+    // the particle kernel small; touching a wall is the rare path)
+#pragma unroll 1
     for (int w = 0; w < 5; w++) {
         if (!(dl[w] > 0.0)) continue;
         V3<F> n;

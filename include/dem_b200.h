@@ -190,6 +190,14 @@ int outputporositycn(unsigned int numBodies, unsigned int* contacti, double maxh
 #define DEM_PREC_FP64   0
 #define DEM_PREC_MIXED  1
 
+/* Force decomposition.  PCCP (the reference's, README.md:4-6): one thread per
+ * candidate pair writes pair forces, one thread per particle gathers them.
+ * PP (the paper's particle-parallel form, Figure 1(b)): one thread per
+ * particle evaluates all of its pairs (each pair twice, bit-identically) and
+ * integrates, one kernel per step, with ping-pong state buffers. */
+#define DEM_FORCE_PCCP  0
+#define DEM_FORCE_PP    1
+
 typedef struct dem_ctx dem_ctx;
 
 /* Contact parameters in reduced units.  Rolling-friction length of a pair is
@@ -219,6 +227,7 @@ typedef struct {
     double cell;            /* cell edge; 0 -> 2*r_max+skin (+1e-4)             */
     double density;         /* mass = density*8r^3 (1 in reduced units)         */
     long long pair_capacity;/* half-list capacity; 0 -> 8*n                     */
+    int force_mode;         /* DEM_FORCE_PCCP (default 0) / DEM_FORCE_PP        */
 } dem_config;
 
 /* Per-step observables (reference ppor.dat columns, dempacking.cu:766-776). */

@@ -268,3 +268,52 @@ def test_device_upload_download_roundtrip(dem, wl, cuda):
     np.testing.assert_array_equal(out.cpu().numpy(), w.pos)
     g, cell, nc = e.grid_info()
     assert abs(cell - w.cell()) < 1e-15
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("interval", [20, 7])
+def test_pp_mode_matches_pccp(dem, wl, cuda, prec, interval):
+    """The particle-parallel step (each pair evaluated by both particles, one
+    kernel per step, ping-pong buffers) agrees with the pair-parallel step to
+    rounding (the compiler may contract multiply-adds differently in the two
+    kernels: ~1e-13 relative in FP64); an odd re-list interval exercises the
+    buffer parity of the captured windows."""
+    w = dense_lattice(dem)
+    rng = np.random.default_rng(9)
+    pdis = rng.normal(0, 2e-6, 3 * w.n)
+    angv = rng.normal(0, 2e-6, 3 * w.n)
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    out = []
+    for mode in (dem.FORCE_PCCP, dem.FORCE_PP):
+        e = dem.Engine(**{**w.engine_kwargs(), "precision": p, "relist_interval": interval, "force_mode": mode})
+        e.set_material(w.pp, w.pw)
+        e.upload(w.pos, w.rad, pdis, angv)
+        e.step(5 * interval + 3)     # graph windows, then an eager partial window
+        e.step(interval - 1)
+        s = e.scalars()
+        lp, ln, hist = e.pairs()
+        out.append((e.download(), s, ln, hist))
+        e.close()
+    (a, sa, lna, ha), (b, sb, lnb, hb) = out
+    tol = 1e-9 if prec == "fp64" else 1e-7
+    np.testing.assert_allclose(b[0], a[0], rtol=0, atol=tol)                      # positions
+    for x, y in zip(a[1:], b[1:]):                                                # per-step motion
+        np.testing.assert_allclose(y, x, rtol=0, atol=1e-6 * max(np.abs(x).max(), 1e-30))
+    np.testing.assert_array_equal(lna, lnb)
+    assert np.linalg.norm(ha - hb) <= 1e-6 * np.linalg.norm(ha)
+    assert abs(sa["contacts"] - sb["contacts"]) <= 2 and sa["contacts"] > 1000
+    assert abs(sa["maxhz"] - sb["maxhz"]) <= tol
+
+
+def test_pp_mode_trajectory_vs_oracle(dem, orc, wl, cuda):
+    w = wl.lattice_2k()
+    steps = 1000
+    e = dem.Engine(**{**w.engine_kwargs(), "force_mode": dem.FORCE_PP})
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad)
+    e.step(steps)
+    pos, _, _ = e.download()
+    cell = e.grid_info()[1]
+    o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, dem.material_array(w.pp, w.pw), False, steps,
+                w.relist_interval)
+    assert np.sqrt(np.mean((pos - o["pos"]) ** 2)) <= 1e-9

@@ -81,7 +81,7 @@ def profile_traffic(name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks/throttle reasons sampled every 50 ms while running."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -95,10 +95,14 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:   # sampler running before timing starts
+                time.sleep(0.02)
+            self.lines.clear()
         except Exception:
             self.proc = None
 
@@ -229,6 +233,27 @@ def run_ours(args):
                 "mixed_over_fp64": value / ws / v2, "packing_fraction": s2["packing_fraction"],
                 "packing_fraction_mixed": sc["packing_fraction"]}
 
+    # --- particle-parallel (PP) force mode on the same workload
+    ppm = None
+    if not args.skip_pp:
+        e3 = dem.Engine(**{**w.engine_kwargs(), "force_mode": dem.FORCE_PP})
+        e3.set_stream(stream.cuda_stream)
+        e3.set_material(w.pp, w.pw)
+        e3.upload(w.pos, w.rad)
+        with torch.cuda.stream(stream):
+            e3.step(3 * win)
+        e3.upload(w.pos, w.rad)
+        k3 = max(10, K // 5)
+        ms3 = time_windows(torch, e3, stream, k3, flush, win)
+        e3.close()
+        ppm = {"value": w.n * k3 * win / (ms3 / 1e3), "unit": UNIT, "windows": k3,
+               "pccp_over_pp": (value / ws) / (w.n * k3 * win / (ms3 / 1e3))}
+
+    # --- adjoint window cost on the pre-settled 50,000-sphere workload
+    adj = None
+    if not args.skip_adjoint:
+        adj = adjoint_cost(dem, torch, stream)
+
     # --- end to end through the public API with host buffers: pinned host
     # state -> dem_upload_state -> K windows with a scalar read-back each
     # (dem_get_scalars, a host sync) -> final dem_download_state to pinned host
@@ -295,10 +320,44 @@ def run_ours(args):
         "clocks": clk,
         "gpu_launches": KERNELS_PER_WINDOW * K,
         "fp64_plain": fp64,
+        "pp_mode": ppm,
+        "adjoint": adj,
         "e2e": e2e,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
+
+
+def adjoint_cost(dem, torch, stream):
+    """settle_50k: 50,000 lognormal spheres (40x40x150 mm) pre-settled for
+    20,000 steps, then a 2,000-step window, checkpoints every 100: time of
+    the reverse sweep (objective + recompute + reverse) against the plain
+    forward window, packing-fraction objective."""
+    import dem_b200.workloads as wm
+    w = wm.settle_50k()
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_stream(stream.cuda_stream)
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad)
+    e.step(w.meta["presettle_steps"])
+    pos, pdis, angv = e.download()
+    e.upload(pos, w.rad, pdis, angv)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    e.step(w.steps)
+    b.record(stream)
+    stream.synchronize()
+    fwd_ms = a.elapsed_time(b)
+    e.upload(pos, w.rad, pdis, angv)
+    e.adjoint(w.steps, 100, dem.OBJ_PACKING)           # warm-up (allocates the tape)
+    e.upload(pos, w.rad, pdis, angv)
+    r = e.adjoint(w.steps, 100, dem.OBJ_PACKING)
+    e.close()
+    return {"workload": w.name, "n_particles": w.n, "window_steps": w.steps, "checkpoint_every": 100,
+            "objective": "packing fraction", "forward_window_ms": fwd_ms,
+            "checkpointed_forward_ms": r["forward_ms"], "reverse_ms": r["adjoint_ms"],
+            "adjoint_over_forward": r["adjoint_ms"] / fwd_ms,
+            "d_mu": r["d_pp"]["mu"] + r["d_pw"]["mu"], "d_roll_rel": r["d_pp"]["roll_rel"] + r["d_pw"]["roll_rel"]}
 
 
 def cpu_baseline(dem, w, steps):
@@ -365,6 +424,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-pp", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -26,6 +26,7 @@ LIB_PATH = PKG_DIR / "libdem_b200.so"
 DEM_OK, DEM_ERR_ARG, DEM_ERR_CUDA, DEM_ERR_CAPACITY = 0, 1, 2, 3
 DEM_ERR_NONFINITE, DEM_ERR_SKIN, DEM_ERR_IO, DEM_ERR_STATE = 4, 5, 6, 7
 PREC_FP64, PREC_MIXED = 0, 1
+OBJ_PACKING, OBJ_POTENTIAL = 0, 1
 FORCE_PCCP, FORCE_PP = 0, 1
 RADII_MONO, RADII_LOGNORMAL, RADII_BIDISPERSE = 0, 1, 2
 
@@ -92,6 +93,11 @@ class Scalars(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AdjointResult(ctypes.Structure):
+    _fields_ = [("value", ctypes.c_double), ("d_pp", Contact), ("d_pw", Contact), ("forward_ms", ctypes.c_double),
+                ("adjoint_ms", ctypes.c_double)]
+
+
 class Deck(ctypes.Structure):
     _fields_ = [
         ("iforcemode", ctypes.c_int), ("ntot", ctypes.c_int),
@@ -155,6 +161,9 @@ _SIGS = [
     ("dem_grid_info", ctypes.c_int, [_vp, _c_uint_p, _c_double_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("dem_set_profiling", ctypes.c_int, [_vp, ctypes.c_int]),
     ("dem_kernel_times", ctypes.c_int, [_vp, _c_double_p]),
+    ("dem_adjoint_window", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(AdjointResult), _vp]),
+    ("dem_adjoint_release", ctypes.c_int, [_vp]),
     ("dem_read_deck", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(Deck)]),
     ("dem_deck_material", ctypes.c_int, [ctypes.POINTER(Deck), ctypes.POINTER(Material)]),
     ("dem_reduced_modulus", ctypes.c_double, [ctypes.c_double, ctypes.c_double, ctypes.c_double]),
@@ -451,6 +460,22 @@ class Engine:
         en = np.empty(nc, dtype=np.uint32)
         check(lib().dem_download_cells(self._h, _ptr(keys), _ptr(ids), _ptr(st), _ptr(en), nc), "dem_download_cells")
         return keys, ids, st, en
+
+    def adjoint(self, nsteps, checkpoint_every, objective=OBJ_PACKING, radii=True):
+        """Reverse mode over a window: returns the objective, its gradients
+        with respect to the contact parameters (pp, pw) and every radius, and
+        the device times of the forward and of the reverse sweep."""
+        r = AdjointResult()
+        dr = np.zeros(self.n) if radii else None
+        check(lib().dem_adjoint_window(self._h, int(nsteps), int(checkpoint_every), int(objective), ctypes.byref(r),
+                                       _ptr(dr)), "dem_adjoint_window")
+        keys = [k for k, _ in Contact._fields_]
+        return {"value": r.value, "d_pp": {k: getattr(r.d_pp, k) for k in keys},
+                "d_pw": {k: getattr(r.d_pw, k) for k in keys}, "d_radii": dr, "forward_ms": r.forward_ms,
+                "adjoint_ms": r.adjoint_ms}
+
+    def adjoint_release(self):
+        check(lib().dem_adjoint_release(self._h), "dem_adjoint_release")
 
     def set_profiling(self, on=True):
         check(lib().dem_set_profiling(self._h, 1 if on else 0), "dem_set_profiling")

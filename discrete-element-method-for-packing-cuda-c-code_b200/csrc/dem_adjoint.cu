@@ -1,0 +1,684 @@
+// dem_adjoint.cu -- reverse mode of the DEM step over a window of steps
+// (force + walls + integrator), with checkpoints every K steps and
+// recomputation in between.  No counterpart in the reference.
+//
+//   1. forward:  the engine runs the window; every K steps it saves a
+//      checkpoint (state, wall history, and the previous list with its
+//      tangential history, from which the next re-list carries).
+//   2. objective at the final state: packing fraction
+//      sum (4/3) pi r^3 / (Wx Wy max z) or potential energy
+//      sum m z + sum (2/5) estar sqrt(R*) delta^2.5 (pairs and walls); its
+//      gradient seeds the adjoint state.
+//   3. for each segment, last first: restore the checkpoint, recompute the K
+//      steps recording per-step state, force, torque and pair history, and
+//      every re-list's list and carry map; then sweep the steps backwards:
+//        k_adj_prep   integrator reverse (one thread per particle)
+//        k_adj_pairs  pair + wall VJP (dem_law_adj.cuh), particle-parallel:
+//                     each particle evaluates the reverse of all its pairs
+//                     and keeps its own share -- no atomics, deterministic
+//        k_adj_carry  at a re-list, the history adjoints of the new list go
+//                     back to the carried pairs of the previous list
+// The reverse runs in FP64 on the recorded FP64/FP32 trajectory.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+#include "dem_engine_internal.h"
+#include "dem_law_adj.cuh"
+
+namespace dem {
+
+namespace {
+constexpr int kB = 256;
+
+struct Ck {
+    double* pos = nullptr;   // 3 np
+    double* disp = nullptr;  // 3 np
+    void* ang = nullptr;     // 3 np Real
+    float4* q = nullptr;     // np
+    double* wh = nullptr;    // 3 np
+    uint* off = nullptr;     // np + 1 (previous list)
+    uint* ln = nullptr;      // cap
+    double* hist = nullptr;  // 3 cap
+    int cur = 0, sbuf = 0, hph = 0;
+};
+
+struct ListRec {
+    uint *off = nullptr, *ln = nullptr, *lp = nullptr, *roff = nullptr, *rk = nullptr, *carry = nullptr;
+    long long P = 0;
+};
+}  // namespace
+
+struct AdjWork {
+    long long seg = 0, nck = 0, nwin = 0;
+    std::vector<Ck> ck;
+    std::vector<ListRec> lists;
+    double *tx = nullptr, *td = nullptr, *twh = nullptr, *tF = nullptr, *tT = nullptr, *th = nullptr;
+    void* ta = nullptr;
+    double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Fb = nullptr, *Tb = nullptr, *Rb = nullptr;
+    double* Hb[2] = {nullptr, nullptr};
+    double* pbar = nullptr;      // nblk x 12
+    double* obj = nullptr;       // [0] value, [1..] scratch
+    unsigned long long* zmax = nullptr;  // [0] max z bits, [1] argmax
+    unsigned long long* save_mz = nullptr;   // observables of the forward's last step
+    uint* save_cnt = nullptr;
+};
+
+namespace {
+
+void free_ck(Ck& k) {
+    void* p[] = {k.pos, k.disp, k.ang, k.q, k.wh, k.off, k.ln, k.hist};
+    for (void* x : p)
+        if (x) cudaFree(x);
+    k = Ck();
+}
+
+size_t rsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(float) : sizeof(double); }
+
+int ensure_work(dem_ctx* c, long long seg, long long nck) {
+    AdjWork* w = c->adj;
+    if (!w) {
+        w = new AdjWork();
+        c->adj = w;
+    }
+    const long long np = c->npad, cap = c->cap;
+    const int K = c->cfg.relist_interval;
+    int rc;
+    if (!w->Xb) {
+        if ((rc = dalloc(&w->Xb, 3 * np)) || (rc = dalloc(&w->Db, 3 * np)) || (rc = dalloc(&w->Ab, 3 * np)) ||
+            (rc = dalloc(&w->Wb, 3 * np)) || (rc = dalloc(&w->Fb, 3 * np)) || (rc = dalloc(&w->Tb, 3 * np)) ||
+            (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
+            (rc = dalloc(&w->pbar, (size_t)c->nblk * 12)) || (rc = dalloc(&w->obj, 16)) || (rc = dalloc(&w->zmax, 2)) ||
+            (rc = dalloc(&w->save_mz, c->nblk)) || (rc = dalloc(&w->save_cnt, c->nblk)))
+            return rc;
+    }
+    if (seg > w->seg) {
+        void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta};
+        for (void* x : p)
+            if (x) cudaFree(x);
+        for (ListRec& l : w->lists) {
+            void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry};
+            for (void* x : q)
+                if (x) cudaFree(x);
+        }
+        w->lists.clear();
+        if ((rc = dalloc(&w->tx, 3 * np * seg)) || (rc = dalloc(&w->td, 3 * np * seg)) ||
+            (rc = dalloc(&w->twh, 3 * np * seg)) || (rc = dalloc(&w->tF, 3 * np * seg)) ||
+            (rc = dalloc(&w->tT, 3 * np * seg)) || (rc = dalloc(&w->th, 3 * cap * seg)))
+            return rc;
+        DEM_CUDA_TRY(cudaMalloc(&w->ta, 3 * np * seg * rsz(c)));
+        const long long nw = (seg + K - 1) / K;
+        w->lists.resize(nw);
+        for (ListRec& l : w->lists)
+            if ((rc = dalloc(&l.off, np + 1)) || (rc = dalloc(&l.ln, cap)) || (rc = dalloc(&l.lp, cap)) ||
+                (rc = dalloc(&l.roff, np + 1)) || (rc = dalloc(&l.rk, cap)) || (rc = dalloc(&l.carry, cap)))
+                return rc;
+        w->seg = seg;
+        w->nwin = nw;
+    }
+    if (nck > (long long)w->ck.size()) {
+        size_t old = w->ck.size();
+        w->ck.resize(nck);
+        for (size_t k = old; k < (size_t)nck; k++) {
+            Ck& x = w->ck[k];
+            if ((rc = dalloc(&x.pos, 3 * np)) || (rc = dalloc(&x.disp, 3 * np)) || (rc = dalloc(&x.q, np)) ||
+                (rc = dalloc(&x.wh, 3 * np)) || (rc = dalloc(&x.off, np + 1)) || (rc = dalloc(&x.ln, cap)) ||
+                (rc = dalloc(&x.hist, 3 * cap)))
+                return rc;
+            DEM_CUDA_TRY(cudaMalloc(&x.ang, 3 * np * rsz(c)));
+        }
+    }
+    w->nck = nck;
+    return DEM_OK;
+}
+
+int copy(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes) DEM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    return DEM_OK;
+}
+
+// Checkpoint = state of the current buffers + the previous list (the one the
+// next re-list carries history from).
+int save_ck(dem_ctx* c, Ck& k) {
+    const long long np = c->npad, cap = c->cap;
+    cudaStream_t s = c->stream;
+    int rc;
+    if ((rc = copy(k.pos, c->pos[c->sbuf], 3 * np * sizeof(double), s)) ||
+        (rc = copy(k.disp, c->disp[c->sbuf], 3 * np * sizeof(double), s)) ||
+        (rc = copy(k.ang, c->ang[c->sbuf], 3 * np * rsz(c), s)) || (rc = copy(k.q, c->q, np * sizeof(float4), s)) ||
+        (rc = copy(k.wh, c->wh, 3 * np * sizeof(double), s)) ||
+        (rc = copy(k.off, c->off[c->cur], (np + 1) * sizeof(uint), s)) ||
+        (rc = copy(k.ln, c->ln[c->cur], cap * sizeof(uint), s)) ||
+        (rc = copy(k.hist, c->hist[c->cur][c->hph], 3 * cap * sizeof(double), s)))
+        return rc;
+    k.cur = c->cur;
+    k.sbuf = c->sbuf;
+    k.hph = c->hph;
+    return DEM_OK;
+}
+
+int restore_ck(dem_ctx* c, const Ck& k) {
+    const long long np = c->npad, cap = c->cap;
+    cudaStream_t s = c->stream;
+    c->cur = k.cur;
+    c->sbuf = k.sbuf;
+    c->hph = k.hph;
+    int rc;
+    if ((rc = copy(c->pos[c->sbuf], k.pos, 3 * np * sizeof(double), s)) ||
+        (rc = copy(c->disp[c->sbuf], k.disp, 3 * np * sizeof(double), s)) ||
+        (rc = copy(c->ang[c->sbuf], k.ang, 3 * np * rsz(c), s)) || (rc = copy(c->q, k.q, np * sizeof(float4), s)) ||
+        (rc = copy(c->wh, k.wh, 3 * np * sizeof(double), s)) ||
+        (rc = copy(c->off[c->cur], k.off, (np + 1) * sizeof(uint), s)) ||
+        (rc = copy(c->ln[c->cur], k.ln, cap * sizeof(uint), s)) ||
+        (rc = copy(c->hist[c->cur][c->hph], k.hist, 3 * cap * sizeof(double), s)))
+        return rc;
+    return DEM_OK;
+}
+
+// ------------------------------------------------------------- kernels
+template <typename Real> __device__ __forceinline__ V3d ldA(const Real* a, long long np, long long i) {
+    return mk((double)a[i], (double)a[np + i], (double)a[2 * np + i]);
+}
+__device__ __forceinline__ V3d ld3(const double* a, long long np, long long i) {
+    return mk(a[i], a[np + i], a[2 * np + i]);
+}
+__device__ __forceinline__ void st3(double* a, long long np, long long i, V3d v) {
+    a[i] = v.x; a[np + i] = v.y; a[2 * np + i] = v.z;
+}
+
+// Integrator reverse (neiglist.cu:356-360 read backwards):
+//   d' = d + F dt^2/m,  x' = x + d',  a' = a + T dt^2/I,  F_z includes -m.
+template <typename Real>
+__global__ void k_adj_prep(long long n, long long np, const Real* __restrict__ R, const double* __restrict__ F,
+                           const double* __restrict__ T, double dt, double density, double* __restrict__ Xb,
+                           double* __restrict__ Db, const double* __restrict__ Ab, double* __restrict__ Fb,
+                           double* __restrict__ Tb, double* __restrict__ Rb) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double r = (double)R[i];
+    const double m = density * 8.0 * r * r * r, I = 0.4 * m * (r * r);
+    const double dmdr = density * 24.0 * r * r, dIdr = 0.4 * (dmdr * r * r + 2.0 * m * r);
+    const V3d xb = ld3(Xb, np, i), ab = ld3(Ab, np, i);
+    const V3d dtot = ld3(Db, np, i) + xb;
+    const V3d f = mk(F[3 * i], F[3 * i + 1], F[3 * i + 2]), t = mk(T[3 * i], T[3 * i + 1], T[3 * i + 2]);
+    const double k = dt * dt / m, kI = dt * dt / I;
+    const V3d fb = k * dtot;
+    st3(Fb, np, i, fb);
+    st3(Tb, np, i, kI * ab);
+    double mb = -dot(dtot, f) * k / m;   // d/dm of F dt^2/m
+    mb += -fb.z;                          // gravity F_z = ... - m
+    const double Ib = -dot(ab, t) * kI / I;
+    Rb[i] += mb * dmdr + Ib * dIdr;
+    st3(Db, np, i, dtot);
+}
+
+struct AdjList {
+    const uint *off, *ln, *lp, *roff, *rk;
+};
+
+// Pair and wall reverse, particle-parallel.  Each particle evaluates (forward
+// with tape, then reverse) every pair it belongs to and keeps its own share
+// of the input adjoints; the pair's history adjoint and its parameter
+// adjoints are kept by the lower index only.
+template <typename Real>
+__global__ void __launch_bounds__(128) k_adj_pairs(
+    long long n, long long np, long long cap, AdjList L, const double* __restrict__ tx, const double* __restrict__ td,
+    const Real* __restrict__ ta, const double* __restrict__ twh,
+    const double* __restrict__ th, const Real* __restrict__ R, LawParams<double> pp, LawParams<double> pw,
+    double inv_dt, double density, double hx, double hy, const double* __restrict__ Fb, const double* __restrict__ Tb,
+    const double* __restrict__ Hout, double* __restrict__ Hin, double* __restrict__ Xb, double* __restrict__ Db,
+    double* __restrict__ Ab, double* __restrict__ Wb, double* __restrict__ Rb, double* __restrict__ pbar) {
+    __shared__ double sp[12][kB / 32];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    LawBar bp, bw;
+    lawbar_zero(bp);
+    lawbar_zero(bw);
+    if (i < n) {
+        const V3d xi = ld3(tx, np, i), di = ld3(td, np, i), ai = ldA<Real>(ta, np, i);
+        const double ri = (double)R[i];
+        const V3d fbi = ld3(Fb, np, i), tbi = ld3(Tb, np, i);
+        V3d xb = zero3<double>(), dbv = zero3<double>(), ab = zero3<double>(), dum3 = zero3<double>();
+        double rb = 0.0, dum = 0.0;
+        const uint total = L.off[n];
+        if ((long long)total <= cap) {
+            for (uint k = L.off[i]; k < L.off[i + 1]; k++) {
+                const uint j = L.ln[k];
+                const V3d hin = mk(th[k], th[cap + k], th[2 * cap + k]);
+                PairTape t;
+                V3d Fi, Ti, Tj, ho;
+                if (!pair_fwd(xi, ld3(tx, np, j), di, ld3(td, np, j), ai, ldA<Real>(ta, np, j), ri, (double)R[j], hin,
+                              pp, inv_dt, density, t, Fi, Ti, Tj, ho)) {
+                    Hin[k] = 0.0; Hin[cap + k] = 0.0; Hin[2 * cap + k] = 0.0;
+                    continue;
+                }
+                V3d hinb = zero3<double>(), xjb = zero3<double>(), djb = zero3<double>(), ajb = zero3<double>();
+                pair_rev(t, pp, inv_dt, density, fbi - ld3(Fb, np, j), tbi, ld3(Tb, np, j),
+                         mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]), xb, xjb, dbv, djb, ab, ajb, rb, dum, hinb, bp);
+                Hin[k] = hinb.x; Hin[cap + k] = hinb.y; Hin[2 * cap + k] = hinb.z;
+            }
+            for (uint u = L.roff[i]; u < L.roff[i + 1]; u++) {
+                const uint k = L.rk[u];
+                if (k >= total) continue;
+                const uint j = L.lp[k];
+                const V3d hin = mk(th[k], th[cap + k], th[2 * cap + k]);
+                PairTape t;
+                V3d Fi, Ti, Tj, ho;
+                if (!pair_fwd(ld3(tx, np, j), xi, ld3(td, np, j), di, ldA<Real>(ta, np, j), ai, (double)R[j], ri, hin,
+                              pp, inv_dt, density, t, Fi, Ti, Tj, ho))
+                    continue;
+                LawBar scratch;
+                lawbar_zero(scratch);
+                V3d hinb = zero3<double>(), xlb = zero3<double>(), dlb = zero3<double>(), alb = zero3<double>();
+                pair_rev(t, pp, inv_dt, density, ld3(Fb, np, j) - fbi, ld3(Tb, np, j), tbi,
+                         mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]), xlb, xb, dlb, dbv, alb, ab, dum, rb, hinb,
+                         scratch);
+            }
+        }
+        // walls (the stored slot is the history input; it is zero whenever
+        // the particle did not touch a wall at the previous step)
+        const V3d hw = ld3(twh, np, i);
+        V3d hwb = zero3<double>();
+        wall_vjp(hx, hy, xi, di, ai, ri, density, hw, pw, inv_dt, fbi, tbi, ld3(Wb, np, i), xb, dbv, ab, rb, hwb, bw);
+        st3(Wb, np, i, hwb);
+        (void)dum3;
+        st3(Xb, np, i, ld3(Xb, np, i) + xb);
+        st3(Db, np, i, ld3(Db, np, i) + dbv);
+        st3(Ab, np, i, ld3(Ab, np, i) + ab);
+        Rb[i] += rb;
+    }
+    // parameter adjoints: block sums accumulated into this block's slot
+    double v[12] = {bp.estar, bp.mu, bp.cn, bp.ct, bp.roll, bp.roll_rel,
+                    bw.estar, bw.mu, bw.cn, bw.ct, bw.roll, bw.roll_rel};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sp[k][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) x += sp[threadIdx.x][w];
+        pbar[(size_t)blockIdx.x * 12 + threadIdx.x] += x;
+    }
+}
+
+// History adjoint across a re-list: new pair k carried old pair carry[k].
+__global__ void k_adj_carry(const uint* __restrict__ off, long long n, long long cap, const uint* __restrict__ carry,
+                            const double* __restrict__ Hnew, double* __restrict__ Hold) {
+    const uint total = off[n];
+    if ((long long)total > cap) return;
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long long)total) return;
+    const uint t = carry[k];
+    if (t == kEmpty || (long long)t >= cap) return;
+    Hold[t] = Hnew[k];
+    Hold[cap + t] = Hnew[cap + k];
+    Hold[2 * cap + t] = Hnew[2 * cap + k];
+}
+
+// Records the input of one recomputed step: state planes, wall history and
+// the pair history of the current list (count read on the device).
+template <typename Real>
+__global__ void k_tape(long long n, long long np, long long cap, const double* __restrict__ P,
+                       const double* __restrict__ D, const Real* __restrict__ A, const double* __restrict__ W,
+                       const uint* __restrict__ off, const double* __restrict__ H, double* __restrict__ tx,
+                       double* __restrict__ td, Real* __restrict__ ta, double* __restrict__ twh,
+                       double* __restrict__ th) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (long long k = t0; k < 3 * np; k += stride) {
+        tx[k] = P[k];
+        td[k] = D[k];
+        ta[k] = A[k];
+        twh[k] = W[k];
+    }
+    long long total = off[n];
+    if (total > cap) total = cap;
+    for (long long k = t0; k < total; k += stride) {
+        th[k] = H[k];
+        th[cap + k] = H[cap + k];
+        th[2 * cap + k] = H[2 * cap + k];
+    }
+}
+
+// ------------------------------------------------------------ objectives
+template <typename Real>
+__global__ void k_zmax(long long n, const double* __restrict__ Z, unsigned long long* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double z = i < n ? Z[i] : 0.0;
+    unsigned long long b = (unsigned long long)__double_as_longlong(z > 0.0 ? z : 0.0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+        b = ob > b ? ob : b;
+    }
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(out, b);
+}
+__global__ void k_zargmax(long long n, const double* __restrict__ Z, unsigned long long* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double z = Z[i];
+    unsigned long long b = (unsigned long long)__double_as_longlong(z > 0.0 ? z : 0.0);
+    if (b == out[0]) atomicMin(&out[1], (unsigned long long)i);
+}
+
+// Packing fraction phi = Vs / (Wx Wy H): dphi/dz_argmax = -phi/H,
+// dphi/dr_i = 4 pi r_i^2 / (Wx Wy H).
+template <typename Real>
+__global__ void k_obj_packing(long long n, long long np, const Real* __restrict__ R, double area, double vs,
+                              const unsigned long long* zm, double* Xb, double* Rb, double* obj) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double H;
+    memcpy(&H, &zm[0], sizeof(double));
+    if (!(H > 0.0)) return;
+    const double phi = vs / (area * H);
+    const double r = (double)R[i];
+    Rb[i] += 4.0 * M_PI * r * r / (area * H);
+    if ((unsigned long long)i == zm[1]) {
+        Xb[2 * np + i] += -phi / H;
+        obj[0] = phi;
+    }
+}
+
+// Potential energy sum m z + elastic (2/5) estar sqrt(R*) delta^2.5 of pairs
+// and walls at the final state; gradient into Xb, Rb and estar adjoints.
+template <typename Real>
+__global__ void k_obj_potential(long long n, long long np, long long cap, AdjList L, const double* __restrict__ P,
+                                const Real* __restrict__ R, double estar, double estar_w, double density, double hx,
+                                double hy, double* Xb, double* Rb, double* obj, double* pbar_est) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double U = 0.0, eb = 0.0, ebw = 0.0;
+    if (i < n) {
+        const V3d x = ld3(P, np, i);
+        const double r = (double)R[i];
+        const double m = density * 8.0 * r * r * r;
+        U += m * x.z;
+        V3d xb = mk(0.0, 0.0, m);
+        double rb = density * 24.0 * r * r * x.z;
+        // walls
+        double dl[5] = {r - x.z, r - (x.x + hx), r - (hx - x.x), r - (x.y + hy), r - (hy - x.y)};
+        for (int w = 0; w < 5; w++) {
+            if (!(dl[w] > 0.0)) continue;
+            const double d = dl[w], sr = sqrt(r), d15 = d * sqrt(d), d25 = d * d15;
+            U += 0.4 * estar_w * sr * d25;
+            const double fne = estar_w * sr * d15;
+            xb += fne * wall_normal(w);
+            rb += fne + 0.4 * estar_w * d25 / (2.0 * sr);
+            ebw += 0.4 * sr * d25;
+        }
+        const uint total = L.off[n];
+        if ((long long)total <= cap) {
+            for (int side = 0; side < 2; side++) {
+                const uint b = side ? L.roff[i] : L.off[i], e = side ? L.roff[i + 1] : L.off[i + 1];
+                for (uint u = b; u < e; u++) {
+                    const uint k = side ? L.rk[u] : u;
+                    if (k >= total) continue;
+                    const uint j = side ? L.lp[k] : L.ln[k];
+                    const V3d xj = ld3(P, np, j);
+                    const double rj = (double)R[j];
+                    const V3d D = xj - x;
+                    const double dist = sqrt(dot(D, D));
+                    const double d = (r + rj) - dist;
+                    if (!(d > 0.0 && dist > 0.0)) continue;
+                    const double Rs = r * rj / (r + rj), sR = sqrt(Rs), d15 = d * sqrt(d), d25 = d * d15;
+                    const double fne = estar * sR * d15;
+                    xb += (fne / dist) * D;                       // d delta / d x_i = n
+                    const double dRdr = rj * rj / ((r + rj) * (r + rj));
+                    rb += fne + 0.4 * estar * d25 * dRdr / (2.0 * sR);
+                    if (!side) {                                   // counted once, by the lower index
+                        U += 0.4 * estar * sR * d25;
+                        eb += 0.4 * sR * d25;
+                    }
+                }
+            }
+        }
+        st3(Xb, np, i, ld3(Xb, np, i) + xb);
+        Rb[i] += rb;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        U += __shfl_xor_sync(0xffffffffu, U, o);
+        eb += __shfl_xor_sync(0xffffffffu, eb, o);
+        ebw += __shfl_xor_sync(0xffffffffu, ebw, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (U != 0.0) atomicAdd(&obj[0], U);
+        if (eb != 0.0) atomicAdd(&pbar_est[0], eb);
+        if (ebw != 0.0) atomicAdd(&pbar_est[1], ebw);
+    }
+}
+
+template <typename Real> int adj_prep(dem_ctx* c, long long t) {
+    AdjWork* w = c->adj;
+    const long long np = c->npad;
+    k_adj_prep<Real><<<grid_for(c->n, kB), kB, 0, c->stream>>>(
+        c->n, np, (const Real*)c->rad, w->tF + 3 * np * t, w->tT + 3 * np * t, c->cfg.dt, c->cfg.density, w->Xb, w->Db,
+        w->Ab, w->Fb, w->Tb, w->Rb);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+template <typename Real> int adj_pairs(dem_ctx* c, long long t, const ListRec& l, int hb) {
+    AdjWork* w = c->adj;
+    const long long np = c->npad, cap = c->cap;
+    AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
+    const unsigned nb = grid_for(c->n, 128);
+    k_adj_pairs<Real><<<nb, 128, 0, c->stream>>>(
+        c->n, np, cap, L, w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t,
+        w->twh + 3 * np * t, w->th + 3 * cap * t, (const Real*)c->rad, make_law<double>(c->mat.pp),
+        make_law<double>(c->mat.pw), 1.0 / c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
+        w->Fb, w->Tb, w->Hb[hb], w->Hb[1 - hb], w->Xb, w->Db, w->Ab, w->Wb, w->Rb, w->pbar);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+template <typename Real> int objective(dem_ctx* c, int which) {
+    AdjWork* w = c->adj;
+    const long long n = c->n, np = c->npad, cap = c->cap;
+    const double* P = c->pos[c->sbuf];
+    cudaStream_t s = c->stream;
+    DEM_CUDA_TRY(cudaMemsetAsync(w->obj, 0, 16 * sizeof(double), s));
+    if (which == DEM_OBJ_PACKING) {
+        unsigned long long init[2] = {0ull, ~0ull};
+        DEM_CUDA_TRY(cudaMemcpyAsync(w->zmax, init, sizeof(init), cudaMemcpyHostToDevice, s));
+        k_zmax<Real><<<grid_for(n, kB), kB, 0, s>>>(n, P + 2 * np, w->zmax);
+        k_zargmax<<<grid_for(n, kB), kB, 0, s>>>(n, P + 2 * np, w->zmax);
+        k_obj_packing<Real><<<grid_for(n, kB), kB, 0, s>>>(n, np, (const Real*)c->rad,
+                                                           c->cfg.world[0] * c->cfg.world[1], c->vol, w->zmax, w->Xb,
+                                                           w->Rb, w->obj);
+    } else {
+        AdjList L{c->off[c->cur], c->ln[c->cur], c->lp, c->roff, c->rk};
+        k_obj_potential<Real><<<grid_for(n, kB), kB, 0, s>>>(n, np, cap, L, P, (const Real*)c->rad, c->mat.pp.estar,
+                                                             c->mat.pw.estar, c->cfg.density, c->cfg.world[0] * 0.5,
+                                                             c->cfg.world[1] * 0.5, w->Xb, w->Rb, w->obj, w->obj + 1);
+    }
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+int list_snapshot(dem_ctx* c, ListRec& l) {
+    cudaStream_t s = c->stream;
+    const long long np = c->npad;
+    uint P = 0;
+    DEM_CUDA_TRY(cudaMemcpyAsync(&P, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((long long)P > c->cap) return fail(DEM_ERR_CAPACITY, "adjoint: pair list exceeded capacity");
+    l.P = P;
+    int rc;
+    if ((rc = copy(l.off, c->off[c->cur], (np + 1) * sizeof(uint), s)) ||
+        (rc = copy(l.roff, c->roff, (np + 1) * sizeof(uint), s)) ||
+        (rc = copy(l.ln, c->ln[c->cur], P * sizeof(uint), s)) || (rc = copy(l.lp, c->lp, P * sizeof(uint), s)) ||
+        (rc = copy(l.rk, c->rk, P * sizeof(uint), s)))
+        return rc;
+    return DEM_OK;
+}
+
+}  // namespace
+}  // namespace dem
+
+using namespace dem;
+
+extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int which, dem_adjoint_result* out,
+                                  double* d_radii) {
+    if (!c || !out) return fail(DEM_ERR_ARG, "dem_adjoint_window: null argument");
+    memset(out, 0, sizeof(*out));
+    if (!c->uploaded || !c->have_mat) return fail(DEM_ERR_STATE, "dem_adjoint_window: upload state and material first");
+    const int K = c->cfg.relist_interval;
+    if (which != DEM_OBJ_PACKING && which != DEM_OBJ_POTENTIAL)
+        return fail(DEM_ERR_ARG, "dem_adjoint_window: unknown objective %d", which);
+    if (nsteps <= 0 || every <= 0 || every % K || nsteps % every)
+        return fail(DEM_ERR_ARG, "dem_adjoint_window: need nsteps %% every == 0 and every %% relist_interval == 0");
+    if (c->in_window != 0) return fail(DEM_ERR_STATE, "dem_adjoint_window: start at a re-list boundary");
+    if (c->profiling) return fail(DEM_ERR_STATE, "dem_adjoint_window: switch profiling off");
+    const long long nseg = nsteps / every;
+    int rc = ensure_work(c, every, nseg + 1);
+    if (rc) return rc;
+    AdjWork* w = c->adj;
+    cudaStream_t s = c->stream;
+    const long long np = c->npad, cap = c->cap;
+    const bool mixed = c->prec == DEM_PREC_MIXED;
+    const bool rec0 = c->record;
+    // ---------------------------------------------------- forward + checkpoints
+    DEM_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+    const long long step0 = c->step, relists0 = c->relists;
+    for (long long g = 0; g < nseg; g++) {
+        if ((rc = save_ck(c, w->ck[g]))) return rc;
+        if ((rc = dem_step_n(c, every))) return rc;
+    }
+    if ((rc = save_ck(c, w->ck[nseg]))) return rc;
+    const size_t last = (size_t)(K - 1) * c->nblk;
+    if ((rc = copy(w->save_mz, c->part_mz + last, c->nblk * sizeof(unsigned long long), s)) ||
+        (rc = copy(w->save_cnt, c->part_cnt + last, c->nblk * sizeof(uint), s)))
+        return rc;
+    DEM_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+    // --------------------------------------------------------------- objective
+    DEM_CUDA_TRY(cudaMemsetAsync(w->Xb, 0, 3 * np * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->Db, 0, 3 * np * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->Ab, 0, 3 * np * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->Wb, 0, 3 * np * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->Rb, 0, np * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->Hb[0], 0, 3 * cap * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->pbar, 0, (size_t)c->nblk * 12 * sizeof(double), s));
+    rc = mixed ? objective<float>(c, which) : objective<double>(c, which);
+    if (rc) return rc;
+    // ------------------------------------------------------- reverse segments
+    dem_record_forces(c, 1);
+    int hb = 0;   // Hb[hb]: adjoint of the pair history output by the step being reversed
+    for (long long g = nseg - 1; g >= 0; g--) {
+        if ((rc = restore_ck(c, w->ck[g]))) return rc;
+        // recompute the segment, recording what the reverse sweep needs
+        for (long long t = 0; t < every; t++) {
+            const int slot = (int)(t % K);
+            if (slot == 0) {
+                c->carry = w->lists[t / K].carry;
+                rc = relist(c, c->cur);
+                c->carry = nullptr;
+                if (rc) return rc;
+                c->cur = 1 - c->cur;
+                c->hph = 0;
+                if ((rc = list_snapshot(c, w->lists[t / K]))) return rc;
+            }
+            if (mixed)
+                k_tape<float><<<148 * 4, kB, 0, s>>>(c->n, np, cap, c->pos[c->sbuf], c->disp[c->sbuf],
+                                                     (const float*)c->ang[c->sbuf], c->wh, c->off[c->cur],
+                                                     c->hist[c->cur][c->hph], w->tx + 3 * np * t, w->td + 3 * np * t,
+                                                     (float*)w->ta + 3 * np * t, w->twh + 3 * np * t,
+                                                     w->th + 3 * cap * t);
+            else
+                k_tape<double><<<148 * 4, kB, 0, s>>>(c->n, np, cap, c->pos[c->sbuf], c->disp[c->sbuf],
+                                                      (const double*)c->ang[c->sbuf], c->wh, c->off[c->cur],
+                                                      c->hist[c->cur][c->hph], w->tx + 3 * np * t,
+                                                      w->td + 3 * np * t, (double*)w->ta + 3 * np * t,
+                                                      w->twh + 3 * np * t, w->th + 3 * cap * t);
+            DEM_LAUNCH_CHECK();
+            // the step writes its total force and torque straight into the tape
+            double* keepF = c->dbgF;
+            double* keepT = c->dbgT;
+            c->dbgF = w->tF + 3 * np * t;
+            c->dbgT = w->tT + 3 * np * t;
+            double a, b;
+            rc = step_kernels(c, c->cur, slot, &a, &b);
+            c->dbgF = keepF;
+            c->dbgT = keepT;
+            if (rc) return rc;
+        }
+        // reverse sweep
+        for (long long t = every - 1; t >= 0; t--) {
+            const ListRec& l = w->lists[t / K];
+            rc = mixed ? adj_prep<float>(c, t) : adj_prep<double>(c, t);
+            if (rc) return rc;
+            rc = mixed ? adj_pairs<float>(c, t, l, hb) : adj_pairs<double>(c, t, l, hb);
+            if (rc) return rc;
+            hb = 1 - hb;   // Hb[hb] now holds the adjoint of this step's input history
+            if (t % K == 0) {
+                // input history came from the re-list carry: route it to the
+                // previous list's output history
+                DEM_CUDA_TRY(cudaMemsetAsync(w->Hb[1 - hb], 0, 3 * cap * sizeof(double), s));
+                k_adj_carry<<<grid_for(std::max<long long>(l.P, 1), kB), kB, 0, s>>>(l.off, c->n, cap, l.carry,
+                                                                                      w->Hb[hb], w->Hb[1 - hb]);
+                DEM_LAUNCH_CHECK();
+                hb = 1 - hb;
+            }
+        }
+    }
+    DEM_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+    // ------------------------------------------------------------ results
+    std::vector<double> pb((size_t)c->nblk * 12);
+    double obj[2];
+    DEM_CUDA_TRY(cudaMemcpyAsync(pb.data(), w->pbar, pb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (d_radii) DEM_CUDA_TRY(cudaMemcpyAsync(d_radii, w->Rb, c->n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    double acc[12] = {0};
+    for (size_t b = 0; b < c->nblk; b++)
+        for (int k = 0; k < 12; k++) acc[k] += pb[b * 12 + k];
+    out->value = obj[0];
+    out->d_pp = dem_contact{acc[0], acc[1], 0.0, acc[2], acc[3], acc[4], acc[5]};
+    out->d_pw = dem_contact{acc[6], acc[7], 0.0, acc[8], acc[9], acc[10], acc[11]};
+    if (which == DEM_OBJ_POTENTIAL) {
+        // direct dependence of the elastic energy on estar
+        double eb[2];
+        DEM_CUDA_TRY(cudaMemcpy(eb, w->obj + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+        out->d_pp.estar += eb[0];
+        out->d_pw.estar += eb[1];
+    }
+    float f1 = 0.f, f2 = 0.f;
+    DEM_CUDA_TRY(cudaEventElapsedTime(&f1, c->ev[0], c->ev[1]));
+    DEM_CUDA_TRY(cudaEventElapsedTime(&f2, c->ev[1], c->ev[2]));
+    out->forward_ms = f1;
+    out->adjoint_ms = f2;
+    // leave the context at the end of the window, as dem_step_n(nsteps) would
+    if ((rc = restore_ck(c, w->ck[nseg]))) return rc;
+    if ((rc = copy(c->part_mz + last, w->save_mz, c->nblk * sizeof(unsigned long long), s)) ||
+        (rc = copy(c->part_cnt + last, w->save_cnt, c->nblk * sizeof(uint), s)))
+        return rc;
+    dem_record_forces(c, rec0 ? 1 : 0);
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    c->step = step0 + nsteps;
+    c->relists = relists0 + nsteps / K;
+    c->in_window = 0;
+    c->last_slot = K - 1;
+    return DEM_OK;
+}
+
+extern "C" int dem_adjoint_release(dem_ctx* c) {
+    if (!c || !c->adj) return DEM_OK;
+    AdjWork* w = c->adj;
+    cudaStreamSynchronize(c->stream);
+    for (Ck& k : w->ck) free_ck(k);
+    void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->Xb, w->Db, w->Ab, w->Wb, w->Fb, w->Tb,
+                 w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt};
+    for (void* x : p)
+        if (x) cudaFree(x);
+    for (ListRec& l : w->lists) {
+        void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry};
+        for (void* x : q)
+            if (x) cudaFree(x);
+    }
+    delete w;
+    c->adj = nullptr;
+    return DEM_OK;
+}

@@ -26,8 +26,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
-#include "dem_common.cuh"
-#include "dem_law.cuh"
+#include "dem_engine_internal.h"
 
 namespace dem {
 
@@ -43,20 +42,6 @@ namespace dem {
 #define DEM_PAIR_GRID_MAX (148 * 8)
 #endif
 
-enum : uint {
-    kStCapacity = 1u,
-    kStNonfinite = 2u,
-    kStSkin = 4u,
-};
-
-// device words: [0] status bits, [1] max row count
-struct EngineWords {
-    uint status;
-    uint max_row;
-    uint pad[2];
-};
-
-template <typename Real> struct Planes3 { Real* x; Real* y; Real* z; };
 
 // --------------------------------------------------------------- helpers
 template <typename Real> __device__ __forceinline__ Real mul_rn(Real a, Real b);
@@ -72,11 +57,6 @@ template <typename Real> __device__ __forceinline__ Real div_rn(Real a, Real b);
 template <> __device__ __forceinline__ float div_rn<float>(float a, float b) { return __fdiv_rn(a, b); }
 template <> __device__ __forceinline__ double div_rn<double>(double a, double b) { return __ddiv_rn(a, b); }
 
-struct GridC {
-    double ox, oy, oz;   // world origin
-    double cs;
-    int gx, gy, gz;      // grid size
-};
 
 // Cell coordinate on one axis.  FP32: xf = (float)(x - o), floorf(xf / cs);
 // FP64: floor((x - o) / cs).  Clamped to [0, g-1] (after a clamp of the
@@ -132,10 +112,27 @@ __global__ void k_to_aos(long long n, Planes3<double> P, Planes3<double> D, Plan
 // --------------------------------------------------------------- re-list
 // Cell key per particle (calcHashD's role, neiglist.cu:77-97) and per-cell
 // counts; resets the displacement-since-list q (dempacking.cu:541).
+// Also lists the wall candidates of the coming window: particles closer to a
+// wall than r + skin/2 (a particle moves less than skin/2 per window, which
+// the step checks, so no other particle can touch a wall before the next
+// re-list -- the same guarantee as the pair list's).
 template <typename Real>
-__global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count) {
+__global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count,
+                             const Real* __restrict__ R, double hx, double hy, double half_skin,
+                             uint* __restrict__ wslot, uint* __restrict__ wlist, uint* __restrict__ wcount) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    {
+        const double x = P.x[i], y = P.y[i], z = P.z[i];
+        const double mg = (double)R[i] + half_skin;
+        const bool near = (z < mg) || (x + hx < mg) || (hx - x < mg) || (y + hy < mg) || (hy - y < mg);
+        uint ws = kEmpty;
+        if (near) {
+            ws = atomicAdd(wcount, 1u);
+            wlist[ws] = (uint)i;
+        }
+        wslot[i] = ws;
+    }
     const Real csr = (Real)g.cs;
     Real xl;
     int cx = cell_axis<Real>(P.x[i], g.ox, csr, g.gx, xl);
@@ -262,7 +259,8 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
                            const uint* __restrict__ off, const uint* __restrict__ roff, uint* __restrict__ njli,
                            uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
                            const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
-                           uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words) {
+                           uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
+                           uint* __restrict__ carry) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const uint total = off[n];
@@ -288,8 +286,10 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
         }
         if (lo < oe && oln[lo] == j) {
             H.x[k] = OH.x[lo]; H.y[k] = OH.y[lo]; H.z[k] = OH.z[lo];
+            if (carry) carry[k] = lo;
         } else {
             H.x[k] = 0.0; H.y[k] = 0.0; H.z[k] = 0.0;
+            if (carry) carry[k] = kEmpty;
         }
         R4<Real> z4;
         z4.x = z4.y = z4.z = z4.w = (Real)0;
@@ -348,16 +348,39 @@ __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double
 }
 
 // PCCP: one thread per candidate pair; per-pair results for the gather.
+// PCCP: one thread per candidate pair; per-pair results for the gather.  The
+// same grid then evaluates the wall contacts of the window's wall candidates
+// (calforceiw's role, neiglist.cu:287-301): history W in place (zero when not
+// touching), wall force and torque per candidate in wf[2c], wf[2c+1].
 template <typename Real>
 __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long long n, long long cap,
                                               const uint* __restrict__ lp, const uint* __restrict__ ln,
                                               Planes3<double> P, Planes3<double> D, Planes3<Real> A,
                                               const Real* __restrict__ R, Planes3<double> H, LawParams<Real> pp,
                                               Real inv_dt, Real density, R4<Real>* __restrict__ pf,
-                                              R4<Real>* __restrict__ pti, R4<Real>* __restrict__ ptj) {
+                                              R4<Real>* __restrict__ pti, R4<Real>* __restrict__ ptj,
+                                              const uint* __restrict__ wlist, const uint* __restrict__ wcount,
+                                              Planes3<double> W, LawParams<Real> pw, double hx, double hy,
+                                              R4<Real>* __restrict__ wf) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const uint nw = *wcount;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < (long long)nw; c += stride) {
+        const uint i = wlist[c];
+        const Real r = R[i];
+        const Real m = density * (Real)8 * r * r * r;
+        V3<double> h = mk(W.x[i], W.y[i], W.z[i]);
+        V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
+        const int hit = wall_contacts<Real>(hx, hy, mk(P.x[i], P.y[i], P.z[i]), cvt<Real>(mk(D.x[i], D.y[i], D.z[i])),
+                                            mk(A.x[i], A.y[i], A.z[i]), r, m, h, inv_dt, pw, Fw, Tw, (Real*)nullptr);
+        W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z;
+        R4<Real> a4, b4;
+        a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
+        b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
+        wf[2 * c] = a4;
+        wf[2 * c + 1] = b4;
+    }
     const uint total = off[n];
     if ((long long)total > cap) return;
-    const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total; k += stride) {
         const uint i = lp[k], j = ln[k];
         V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
@@ -385,18 +408,11 @@ __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long
 // --------------------------------------------------- particle update
 // Per-step observables are written as one partial per block (no same-address
 // atomics in the hot kernels) and reduced on the host when asked for.
-struct StepPartials { unsigned long long* maxhz_bits; uint* contacts; };
-
-struct ParticleCommon {
-    double dt, hx, hy;
-    float half_skin2;
-    int first;
-};
 
 // Gravity + walls (calculateforceiwD, neiglist.cu:238-306) + integrator
 // (updatepositionD, neiglist.cu:308-409) for particle i whose pair sums are
 // in F/T; writes the new state to the output planes.
-template <typename Real>
+template <typename Real, bool WALLS>
 __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real> T, Real r, V3<double> x,
                                                 V3<double> d, V3<Real> a, float4 q, Planes3<double> Po,
                                                 Planes3<double> Do, Planes3<Real> Ao, float4* __restrict__ Q,
@@ -405,17 +421,20 @@ __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real
                                                 uint cnt, double* dbgF, double* dbgT, uint* dbgC) {
     const Real m = density * (Real)8 * r * r * r;
     const Real I = (Real)0.4 * m * (r * r);
-    F.z += -m;
-    uint wflag = __float_as_uint(q.w);
     if (pc.first) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }   // displacement since the list (dempacking.cu:541)
-    const double rd = (double)r;
-    const bool touch = (x.z < rd) || (x.x + pc.hx < rd) || (pc.hx - x.x < rd) || (x.y + pc.hy < rd) ||
-                       (pc.hy - x.y < rd);
-    if (touch || wflag) {
-        V3<double> h = wflag ? mk(W.x[i], W.y[i], W.z[i]) : zero3<double>();
-        const int hit = wall_contacts<Real>(pc.hx, pc.hy, x, cvt<Real>(d), a, r, m, h, inv_dt, pw, F, T, (Real*)nullptr);
-        if (hit || wflag) { W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z; }
-        wflag = hit ? 1u : 0u;
+    uint wflag = __float_as_uint(q.w);
+    if (WALLS) {   // walls evaluated here (PP step); the PCCP step adds gathered wall forces before
+        F.z += -m;
+        const double rd = (double)r;
+        const bool touch = (x.z < rd) || (x.x + pc.hx < rd) || (pc.hx - x.x < rd) || (x.y + pc.hy < rd) ||
+                           (pc.hy - x.y < rd);
+        if (touch || wflag) {
+            V3<double> h = wflag ? mk(W.x[i], W.y[i], W.z[i]) : zero3<double>();
+            const int hit = wall_contacts<Real>(pc.hx, pc.hy, x, cvt<Real>(d), a, r, m, h, inv_dt, pw, F, T,
+                                                (Real*)nullptr);
+            if (hit || wflag) { W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z; }
+            wflag = hit ? 1u : 0u;
+        }
     }
     if (dbgF) {   // total force/torque of this step (pairs + gravity + walls), on request
         dbgF[3 * i] = F.x; dbgF[3 * i + 1] = F.y; dbgF[3 * i + 2] = F.z;
@@ -477,7 +496,8 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n
                                                   const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
                                                   LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt,
                                                   Real density, StepPartials part, EngineWords* words, double* dbgF,
-                                                  double* dbgT, uint* dbgC) {
+                                                  double* dbgT, uint* dbgC, const uint* __restrict__ wslot,
+                                                  const R4<Real>* __restrict__ wf) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz = 0.0;
     uint cnt = 0, flags = 0;
@@ -488,6 +508,7 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n
         const V3<double> d = mk(D.x[i], D.y[i], D.z[i]);
         const V3<Real> a = mk(A.x[i], A.y[i], A.z[i]);
         const float4 q = Q[i];
+        const uint ws = wslot[i];
         const uint total = off[n];
         const uint o0 = off[i], o1 = off[i + 1], r0 = roff[i], r1 = roff[i + 1];
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
@@ -513,8 +534,14 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n
                 }
             }
         }
-        particle_finish<Real>(i, F, T, r, x, d, a, q, P, D, A, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt,
-                              dbgF, dbgT, dbgC);
+        F.z += -density * (Real)8 * r * r * r;   // gravity, then the walls (calculateforceiwD's order)
+        if (ws != kEmpty) {
+            const R4<Real> fw = wf[2 * ws], tw = wf[2 * ws + 1];
+            F.x += fw.x; F.y += fw.y; F.z += fw.z;
+            T.x += tw.x; T.y += tw.y; T.z += tw.z;
+        }
+        particle_finish<Real, false>(i, F, T, r, x, d, a, q, P, D, A, Q, W, pw, pc, dtr, inv_dt, density, mz, flags,
+                                     cnt, dbgF, dbgT, dbgC);
     }
     block_observables(mz, cnt, flags, part, words);
 }
@@ -568,8 +595,8 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
                 if (c) { F -= Fl; T += Th; cnt++; }
             }
         }
-        particle_finish<Real>(i, F, T, r, x, d, a, q, Po, Do, Ao, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt,
-                              dbgF, dbgT, dbgC);
+        particle_finish<Real, true>(i, F, T, r, x, d, a, q, Po, Do, Ao, Q, W, pw, pc, dtr, inv_dt, density, mz, flags,
+                                    cnt, dbgF, dbgT, dbgC);
     }
     block_observables(mz, cnt, flags, part, words);
 }
@@ -612,94 +639,8 @@ __global__ void k_pairs_out(const uint* __restrict__ off, long long n, long long
 using namespace dem;
 
 // ===================================================================== ctx
-struct dem_ctx {
-    dem_config cfg{};
-    int prec = DEM_PREC_MIXED;
-    int mode = DEM_FORCE_PCCP;
-    long long n = 0, npad = 0, cap = 0;
-    int device = 0;
-    cudaStream_t stream = 0;
-    cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one
-    cudaEvent_t ext_ready = nullptr;  // orders legacy-stream work before device uploads
-    dem_material mat{};
-    bool have_mat = false;
-    // grid
-    GridC grid{};
-    long long ncells = 0;
-    double rmax = 0.0;
-    double vol = 0.0;        // sum (4/3) pi r^3
-    // state: [current buffer]; the second buffer exists in PP mode only
-    double* pos[2] = {nullptr, nullptr};   // 3 planes
-    double* disp[2] = {nullptr, nullptr};  // 3 planes
-    void* ang[2] = {nullptr, nullptr};     // 3 planes, Real
-    int sbuf = 0;
-    void* rad = nullptr;     // Real
-    float4* q = nullptr;
-    double* wh = nullptr;    // 3 planes
-    double* staging = nullptr;   // 10n doubles
-    // list
-    uint* key = nullptr;
-    uint* sid = nullptr;     // unordered within cells (scatter)
-    uint* sid2 = nullptr;    // sorted by (cell, id)
-    uint* skeyu = nullptr;
-    uint* skey = nullptr;
-    void* sposu = nullptr;
-    void* spos = nullptr;
-    uint* ccount = nullptr;
-    uint* cstart = nullptr;
-    uint* njgi = nullptr;
-    uint* njli = nullptr;
-    uint* off[2] = {nullptr, nullptr};
-    uint* roff = nullptr;
-    uint* ln[2] = {nullptr, nullptr};
-    uint* lp = nullptr;
-    double* hist[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [list buffer][phase], 3 planes of cap
-    int hph = 0;             // history phase of the current list (PP ping-pong)
-    uint* rk = nullptr;
-    void* pf = nullptr;
-    void* pti = nullptr;
-    void* ptj = nullptr;
-    uint* scan_tmp = nullptr;
-    size_t scan_words = 0;
-    // scalars
-    EngineWords* words = nullptr;
-    unsigned long long* part_mz = nullptr;   // relist_interval x nblk
-    uint* part_cnt = nullptr;                // relist_interval x nblk
-    unsigned nblk = 0;                       // blocks of the particle kernel
-    unsigned long long* rmax_bits = nullptr;
-    void* host_pinned = nullptr;     // mirror for scalars
-    // debug force record
-    bool record = false;
-    double* dbgF = nullptr;
-    double* dbgT = nullptr;
-    uint* dbgC = nullptr;
-    // schedule
-    int cur = 0;
-    long long step = 0, in_window = 0, relists = 0;
-    int last_slot = -1;
-    bool uploaded = false;
-    // window graphs keyed by (previous list buffer, state buffer, history phase)
-    cudaGraphExec_t gexec[2][2][2] = {};
-    // profiling
-    bool profiling = false;
-    double ktime[3] = {0, 0, 0};
-    long long kcount[3] = {0, 0, 0};
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-};
 
 namespace {
-
-template <typename T> int dalloc(T** p, size_t count) {
-    *p = nullptr;
-    if (count == 0) count = 1;
-    DEM_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
-    return DEM_OK;
-}
-
-template <typename Real> Planes3<Real> planes(void* base, long long npad) {
-    Real* b = (Real*)base;
-    return Planes3<Real>{b, b + npad, b + 2 * npad};
-}
 
 void free_graphs(dem_ctx* c) {
     for (int a = 0; a < 2; a++)
@@ -738,7 +679,10 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     cudaStream_t s = c->stream;
     Planes3<double> P = planes<double>(c->pos[c->sbuf], np);
     GridC g = c->grid;
-    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount);
+    DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
+    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount, (const Real*)c->rad,
+                                                    c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
+                                                    c->wslot, c->wlist, c->wcount);
     int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
     if (rc) return rc;
     k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->ccount, P, (const Real*)c->rad, g, c->sid,
@@ -755,7 +699,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
         n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
         c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
-        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words);
+        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry);
     k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->off[dst], c->cap);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
@@ -771,7 +715,9 @@ template <typename Real> int launch_pair(dem_ctx* c, int lst) {
                                                planes<Real>(c->ang[0], np), (const Real*)c->rad,
                                                planes<double>(c->hist[lst][0], c->cap), pp, (Real)(1.0 / c->cfg.dt),
                                                (Real)c->cfg.density, (R4<Real>*)c->pf, (R4<Real>*)c->pti,
-                                               (R4<Real>*)c->ptj);
+                                               (R4<Real>*)c->ptj, c->wlist, c->wcount, planes<double>(c->wh, np),
+                                               make_law<Real>(c->mat.pw), c->cfg.world[0] * 0.5,
+                                               c->cfg.world[1] * 0.5, (R4<Real>*)c->wf);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -785,7 +731,8 @@ template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
         (const R4<Real>*)c->ptj, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
         planes<Real>(c->ang[0], np), (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw,
         particle_common(c, slot), (Real)dt, (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words,
-        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr);
+        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, c->wslot,
+        (const R4<Real>*)c->wf);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -807,6 +754,9 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
     return DEM_OK;
 }
 
+}  // namespace
+
+namespace dem {
 int relist(dem_ctx* c, int src) {
     return c->prec == DEM_PREC_MIXED ? launch_relist<float>(c, src) : launch_relist<double>(c, src);
 }
@@ -842,6 +792,9 @@ int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part
     return DEM_OK;
 }
 
+}  // namespace dem
+
+namespace {
 // Enqueue one full window (re-list from list `src`, then K steps).
 int enqueue_window(dem_ctx* c, int src) {
     const int K = c->cfg.relist_interval;
@@ -934,8 +887,11 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->njli, np)) || (rc = dalloc(&c->off[0], np + 1)) || (rc = dalloc(&c->off[1], np + 1)) ||
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
         (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->words, 1)) ||
-        (rc = dalloc(&c->rmax_bits, 2)))
+        (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
+        (rc = dalloc(&c->wcount, 1)))
         return bail(rc);
+    e = cudaMalloc(&c->wf, 2 * np * 4 * rs);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (wall forces)", __FILE__, __LINE__));
     e = cudaMalloc(&c->rad, np * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->spos, np * 4 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->sposu, np * 4 * rs);
@@ -970,13 +926,14 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
 int dem_destroy(dem_ctx* c) {
     if (!c) return DEM_OK;
     cudaStreamSynchronize(c->stream);
+    dem_adjoint_release(c);
     free_graphs(c);
     free_cells(c);
     void* ptrs[] = {c->pos[0], c->pos[1], c->disp[0], c->disp[1], c->ang[0], c->ang[1], c->rad, c->q, c->wh,
                     c->staging, c->key, c->sid, c->sid2, c->spos, c->skeyu, c->skey, c->sposu, c->njgi, c->njli,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->pf, c->pti, c->ptj, c->scan_tmp, c->words, c->part_mz,
-                    c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC};
+                    c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);

@@ -1,0 +1,144 @@
+// dem_engine_internal.h -- the engine context and the launchers shared by
+// dem_engine.cu (forward step) and dem_adjoint.cu (its reverse mode).
+#pragma once
+#include "dem_common.cuh"
+#include "dem_law.cuh"
+
+namespace dem {
+
+enum : uint {
+    kStCapacity = 1u,
+    kStNonfinite = 2u,
+    kStSkin = 4u,
+};
+
+// device words: [0] status bits, [1] max row count
+struct EngineWords {
+    uint status;
+    uint max_row;
+    uint pad[2];
+};
+
+template <typename Real> struct Planes3 { Real* x; Real* y; Real* z; };
+
+struct GridC {
+    double ox, oy, oz;   // world origin
+    double cs;
+    int gx, gy, gz;      // grid size
+};
+
+struct StepPartials { unsigned long long* maxhz_bits; uint* contacts; };
+
+struct ParticleCommon {
+    double dt, hx, hy;
+    float half_skin2;
+    int first;
+};
+
+}  // namespace dem
+
+using dem::EngineWords;
+using dem::GridC;
+using dem::uint;
+namespace dem { struct AdjWork; }
+
+struct dem_ctx {
+    dem_config cfg{};
+    int prec = DEM_PREC_MIXED;
+    int mode = DEM_FORCE_PCCP;
+    long long n = 0, npad = 0, cap = 0;
+    int device = 0;
+    cudaStream_t stream = 0;
+    cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one
+    cudaEvent_t ext_ready = nullptr;  // orders legacy-stream work before device uploads
+    dem_material mat{};
+    bool have_mat = false;
+    // grid
+    GridC grid{};
+    long long ncells = 0;
+    double rmax = 0.0;
+    double vol = 0.0;        // sum (4/3) pi r^3
+    // state: [current buffer]; the second buffer exists in PP mode only
+    double* pos[2] = {nullptr, nullptr};   // 3 planes
+    double* disp[2] = {nullptr, nullptr};  // 3 planes
+    void* ang[2] = {nullptr, nullptr};     // 3 planes, Real
+    int sbuf = 0;
+    void* rad = nullptr;     // Real
+    float4* q = nullptr;
+    double* wh = nullptr;    // 3 planes
+    double* staging = nullptr;   // 10n doubles
+    // list
+    uint* key = nullptr;
+    uint* sid = nullptr;     // unordered within cells (scatter)
+    uint* sid2 = nullptr;    // sorted by (cell, id)
+    uint* skeyu = nullptr;
+    uint* skey = nullptr;
+    void* sposu = nullptr;
+    void* spos = nullptr;
+    uint* ccount = nullptr;
+    uint* cstart = nullptr;
+    uint* njgi = nullptr;
+    uint* njli = nullptr;
+    uint* off[2] = {nullptr, nullptr};
+    uint* roff = nullptr;
+    uint* ln[2] = {nullptr, nullptr};
+    uint* lp = nullptr;
+    double* hist[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [list buffer][phase], 3 planes of cap
+    int hph = 0;             // history phase of the current list (PP ping-pong)
+    uint* rk = nullptr;
+    uint* carry = nullptr;   // optional carry-map output of relist (adjoint recompute)
+    uint* wslot = nullptr;   // per particle: wall-candidate slot of this window or kEmpty
+    uint* wlist = nullptr;   // wall candidates (particle ids)
+    uint* wcount = nullptr;  // number of wall candidates (device)
+    void* wf = nullptr;      // per candidate: wall force, wall torque (R4 each)
+    void* pf = nullptr;
+    void* pti = nullptr;
+    void* ptj = nullptr;
+    uint* scan_tmp = nullptr;
+    size_t scan_words = 0;
+    // scalars
+    EngineWords* words = nullptr;
+    unsigned long long* part_mz = nullptr;   // relist_interval x nblk
+    uint* part_cnt = nullptr;                // relist_interval x nblk
+    unsigned nblk = 0;                       // blocks of the particle kernel
+    unsigned long long* rmax_bits = nullptr;
+    void* host_pinned = nullptr;     // mirror for scalars
+    // debug force record
+    bool record = false;
+    double* dbgF = nullptr;
+    double* dbgT = nullptr;
+    uint* dbgC = nullptr;
+    // schedule
+    int cur = 0;
+    long long step = 0, in_window = 0, relists = 0;
+    int last_slot = -1;
+    bool uploaded = false;
+    // window graphs keyed by (previous list buffer, state buffer, history phase)
+    cudaGraphExec_t gexec[2][2][2] = {};
+    // profiling
+    bool profiling = false;
+    double ktime[3] = {0, 0, 0};
+    long long kcount[3] = {0, 0, 0};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    dem::AdjWork* adj = nullptr;     // adjoint workspace (dem_adjoint.cu)
+};
+
+
+namespace dem {
+// Launchers (dem_engine.cu).  relist(): list build from the current state,
+// carrying history from list buffer `src` into 1-src; when c->carry is set,
+// carry[k] receives the previous slot of new pair k (kEmpty if new).
+// step_kernels(): one DEM step on list buffer `lst`, window slot `slot`.
+int relist(dem_ctx* c, int src);
+int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part);
+template <typename Real> Planes3<Real> planes(void* base, long long npad) {
+    Real* b = (Real*)base;
+    return Planes3<Real>{b, b + npad, b + 2 * npad};
+}
+template <typename T> int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    DEM_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+    return DEM_OK;
+}
+}  // namespace dem

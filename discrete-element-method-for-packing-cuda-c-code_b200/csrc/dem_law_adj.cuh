@@ -298,15 +298,10 @@ DEM_HD void pair_rev(const PairTape& t, const LawParams<double>& p, double inv_d
     xib -= Db;
 }
 
-// Walls (same order and primary-wall rule as wall_contacts) with reverse.
-struct WallTape {
-    int hit, prim;
-    int on[5];
-    LawTape law[5];
-    V3d nxf[5];
-    double r, m;
-};
-
+// Walls (same order and primary-wall rule as wall_contacts): the forward
+// (wall_fwd, totals only) and the reverse (wall_vjp: each touching wall's law
+// is re-evaluated with its own tape and reversed at once -- the walls are
+// independent given the output adjoints, so no tape array is needed).
 DEM_HD V3d wall_normal(int w) {
     V3d n;
     n.x = (w == 1) ? -1.0 : ((w == 2) ? 1.0 : 0.0);
@@ -315,65 +310,78 @@ DEM_HD V3d wall_normal(int w) {
     return n;
 }
 
-DEM_HD int wall_fwd(double hx, double hy, V3d x, V3d d, V3d a, double r, double density, V3d h_in,
-                    const LawParams<double>& p, double inv_dt, WallTape& t, V3d& F, V3d& T, V3d& h_out) {
-    double dl[5];
+DEM_HD int wall_prim(double hx, double hy, V3d x, double r, double dl[5]) {
     dl[0] = r - x.z;
     dl[1] = r - (x.x + hx);
     dl[2] = r - (hx - x.x);
     dl[3] = r - (x.y + hy);
     dl[4] = r - (hy - x.y);
-    t.prim = -1;
+    int prim = -1;
     for (int w = 0; w < 5; w++)
-        if (dl[w] > 0.0 && (t.prim < 0 || dl[w] > dl[t.prim])) t.prim = w;
-    F = T = h_out = zero3<double>();
-    t.hit = t.prim >= 0;
-    t.r = r;
-    t.m = density * 8.0 * r * r * r;
-    for (int w = 0; w < 5; w++) {
-        t.on[w] = dl[w] > 0.0;
-        if (!t.on[w]) continue;
-        const V3d n = wall_normal(w);
-        const V3d U = (-d) - r * cross(a, n);
-        const V3d h = (w == t.prim) ? h_in : zero3<double>();
-        V3d Fi, Ft, Mr, ho;
-        law_fwd(dl[w], n, r, t.m, U, a, h, inv_dt, p, t.law[w], Fi, Ft, Mr, ho);
-        t.nxf[w] = cross(n, Ft);
-        F += Fi;
-        T += r * t.nxf[w] + Mr;
-        if (w == t.prim) h_out = ho;
-    }
-    return t.hit;
+        if (dl[w] > 0.0 && (prim < 0 || dl[w] > dl[prim])) prim = w;
+    return prim;
 }
 
-DEM_HD void wall_rev(const WallTape& t, const LawParams<double>& p, double inv_dt, double density, V3d Fb, V3d Tb,
-                     V3d hb, V3d& xb, V3d& db, V3d& ab, double& rb, V3d& hinb, LawBar& pb) {
-    if (!t.hit) return;
+DEM_HD int wall_fwd(double hx, double hy, V3d x, V3d d, V3d a, double r, double density, V3d h_in,
+                    const LawParams<double>& p, double inv_dt, V3d& F, V3d& T, V3d& h_out) {
+    double dl[5];
+    const int prim = wall_prim(hx, hy, x, r, dl);
+    F = T = h_out = zero3<double>();
+    if (prim < 0) return 0;
+    const double m = density * 8.0 * r * r * r;
     for (int w = 0; w < 5; w++) {
-        if (!t.on[w]) continue;
+        if (!(dl[w] > 0.0)) continue;
         const V3d n = wall_normal(w);
-        // T += r nxf + Mr
-        rb += dot(t.nxf[w], Tb);
-        const V3d nxfb = t.r * Tb;
+        const V3d U = (-d) - r * cross(a, n);
+        const V3d h = (w == prim) ? h_in : zero3<double>();
+        LawTape t;
+        V3d Fi, Ft, Mr, ho;
+        law_fwd(dl[w], n, r, m, U, a, h, inv_dt, p, t, Fi, Ft, Mr, ho);
+        F += Fi;
+        T += r * cross(n, Ft) + Mr;
+        if (w == prim) h_out = ho;
+    }
+    return 1;
+}
+
+// Adds the input adjoints of the wall contacts of one particle given the
+// adjoints of its wall force/torque (Fb, Tb) and of its output history (hb).
+// Returns 1 if a wall was touched.
+DEM_HD int wall_vjp(double hx, double hy, V3d x, V3d d, V3d a, double r, double density, V3d h_in,
+                    const LawParams<double>& p, double inv_dt, V3d Fb, V3d Tb, V3d hb, V3d& xb, V3d& db, V3d& ab,
+                    double& rb, V3d& hinb, LawBar& pb) {
+    double dl[5];
+    const int prim = wall_prim(hx, hy, x, r, dl);
+    if (prim < 0) return 0;
+    const double m = density * 8.0 * r * r * r;
+    for (int w = 0; w < 5; w++) {
+        if (!(dl[w] > 0.0)) continue;
+        const V3d n = wall_normal(w);
+        const V3d axn = cross(a, n);
+        const V3d U = (-d) - r * axn;
+        const V3d h = (w == prim) ? h_in : zero3<double>();
+        LawTape t;
+        V3d Fi, Ft, Mr, ho;
+        law_fwd(dl[w], n, r, m, U, a, h, inv_dt, p, t, Fi, Ft, Mr, ho);
+        // T += r (n x Ft) + Mr
+        const V3d nxf = cross(n, Ft);
+        rb += dot(nxf, Tb);
+        const V3d nxfb = r * Tb;
         V3d Ftb = cross(nxfb, n);
         double deltab = 0.0, rsb = 0.0, msb = 0.0;
         V3d nb = zero3<double>(), Ub = zero3<double>(), Wrb = zero3<double>(), hib = zero3<double>();
-        const V3d hbw = (w == t.prim) ? hb : zero3<double>();
-        law_rev(t.law[w], p, inv_dt, Fb, Ftb, Tb, hbw, deltab, nb, rsb, msb, Ub, Wrb, hib, pb);
-        if (w == t.prim) hinb += hib;
-        // Wr = a
-        ab += Wrb;
-        // U = -d - r (a x n)
-        db -= Ub;
-        const V3d cb = (-t.r) * Ub;
-        ab += cross(n, cb);
-        rb += -dot(cross(t.law[w].Wr, n), Ub);
-        // rs = r, ms = m = density 8 r^3
-        rb += rsb + msb * density * 24.0 * t.r * t.r;
-        // delta = r + x.n - c  (n fixed)
-        rb += deltab;
+        law_rev(t, p, inv_dt, Fb, Ftb, Tb, (w == prim) ? hb : zero3<double>(), deltab, nb, rsb, msb, Ub, Wrb, hib,
+                pb);
+        if (w == prim) hinb += hib;
+        ab += Wrb;                                  // Wr = a
+        db -= Ub;                                   // U = -d - r (a x n)
+        ab += cross(n, (-r) * Ub);
+        rb += -dot(axn, Ub);
+        rb += rsb + msb * density * 24.0 * r * r;   // R* = r, m* = density 8 r^3
+        rb += deltab;                               // delta = r + x.n - c
         xb += deltab * n;
     }
+    return 1;
 }
 
 }  // namespace dem

@@ -280,6 +280,32 @@ int dem_grid_info(dem_ctx* ctx, unsigned int grid[3], double* cell, long long* n
 int dem_set_profiling(dem_ctx* ctx, int on);
 int dem_kernel_times(dem_ctx* ctx, double out[3]);
 
+/* ---------------------------------------------------------------- adjoint --
+ * Reverse mode of the step (force + walls + integrator) over a window; no
+ * counterpart in the reference.  The forward runs nsteps from the current
+ * state (saving a checkpoint every `checkpoint_every` steps), the objective
+ * is evaluated at the final state, and the reverse sweep recomputes each
+ * segment from its checkpoint.  Gradients are with respect to the contact
+ * parameters (dem_contact layout; nu is not differentiated) and every radius.
+ * nsteps must be a multiple of checkpoint_every, which must be a multiple of
+ * relist_interval, and the call must start at a re-list boundary.  On return
+ * the context holds the state at the end of the window. */
+#define DEM_OBJ_PACKING    0   /* sum (4/3) pi r^3 / (Wx Wy max z)              */
+#define DEM_OBJ_POTENTIAL  1   /* sum m z + sum (2/5) estar sqrt(R*) delta^2.5  */
+
+typedef struct {
+    double value;          /* objective at the end of the window              */
+    dem_contact d_pp;      /* d objective / d particle-particle parameters    */
+    dem_contact d_pw;      /* d objective / d particle-wall parameters        */
+    double forward_ms;     /* device time of the checkpointed forward         */
+    double adjoint_ms;     /* device time of the objective + recompute + reverse */
+} dem_adjoint_result;
+
+int dem_adjoint_window(dem_ctx* ctx, long long nsteps, int checkpoint_every, int objective,
+                       dem_adjoint_result* out, double* d_radii /* host [n] or NULL */);
+/* Frees the adjoint workspace (checkpoints, tape); dem_destroy does it too. */
+int dem_adjoint_release(dem_ctx* ctx);
+
 /* ============================================================================
  * 3. Host utilities (deck, initial states, reference output files)
  * ==========================================================================*/

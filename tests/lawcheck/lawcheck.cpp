@@ -40,23 +40,20 @@ void lc_pair_vjp(const double* in, const double* p7, double inv_dt, double densi
 }
 // in: x d a (3x3) r h(3) = 13 ; out: F T h (9)
 int lc_wall_fwd(const double* in, double hx, double hy, const double* p7, double inv_dt, double density, double* out) {
-    WallTape t;
     V3d F, T, ho;
-    int c = wall_fwd(hx, hy, v(in), v(in + 3), v(in + 6), in[9], density, v(in + 10), par(p7), inv_dt, t, F, T, ho);
+    int c = wall_fwd(hx, hy, v(in), v(in + 3), v(in + 6), in[9], density, v(in + 10), par(p7), inv_dt, F, T, ho);
     put(out, F); put(out + 3, T); put(out + 6, ho);
     return c;
 }
 void lc_wall_vjp(const double* in, double hx, double hy, const double* p7, double inv_dt, double density,
                  const double* ob, double* ib, double* pbar) {
-    WallTape t;
-    V3d F, T, ho;
     LawParams<double> p = par(p7);
-    wall_fwd(hx, hy, v(in), v(in + 3), v(in + 6), in[9], density, v(in + 10), p, inv_dt, t, F, T, ho);
     V3d xb = zero3<double>(), db = xb, ab = xb, hb = xb;
     double rb = 0;
     LawBar pb;
     lawbar_zero(pb);
-    wall_rev(t, p, inv_dt, density, v(ob), v(ob + 3), v(ob + 6), xb, db, ab, rb, hb, pb);
+    wall_vjp(hx, hy, v(in), v(in + 3), v(in + 6), in[9], density, v(in + 10), p, inv_dt, v(ob), v(ob + 3), v(ob + 6),
+             xb, db, ab, rb, hb, pb);
     put(ib, xb); put(ib + 3, db); put(ib + 6, ab); ib[9] = rb; put(ib + 10, hb);
     pbar[0] = pb.estar; pbar[1] = pb.mu; pbar[2] = pb.cn; pbar[3] = pb.ct; pbar[4] = pb.roll; pbar[5] = pb.roll_rel;
 }

@@ -1,0 +1,168 @@
+"""GPU adjoint of the DEM step over a window (dem_adjoint_window) against
+central finite differences, on the GPU forward and on the FP64 CPU oracle.
+
+Case: a polydisperse bed with ~3 persistent contacts per sphere and random
+initial motion (sliding, rolling), 100 steps (5 re-lists with history carry),
+checkpoints every 20 steps.  Derivatives of the packing fraction and of the
+potential energy with respect to the sliding friction, the rolling friction,
+the contact stiffness (Young's modulus), the damping (restitution) -- each
+shared by particle-particle and particle-wall contacts -- and a random
+direction in the space of all radii.  Tolerance: 1e-3 relative, plus an
+absolute floor of 1e-8 of the objective for derivatives at the FD noise level
+(FD step 1e-5 relative in FP64; contacts stay closed, so the window is smooth).
+"""
+import numpy as np
+import pytest
+
+from _cases import dense_lattice
+
+pytestmark = pytest.mark.gpu
+
+STEPS, EVERY = 100, 20
+KEYS = {"mu": ("mu",), "roll_rel": ("roll_rel",), "estar": ("estar",), "damp": ("damp_n", "damp_t")}
+
+
+def case(dem):
+    w = dense_lattice(dem, nx=6, ny=6, nz=5, seed=3)
+    rng = np.random.default_rng(12)
+    pdis = rng.normal(0, 3e-6, 3 * w.n)
+    angv = rng.normal(0, 3e-5, 3 * w.n)
+    return w, pdis, angv
+
+
+def scaled(c: dict, key, f):
+    c = dict(c)
+    for k in KEYS[key]:
+        c[k] = c[k] * f
+    return c
+
+
+def run_adjoint(dem, w, pdis, angv, pp, pw, rad, objective):
+    e = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_FP64, "cell": w.cell() + 0.01})
+    e.set_material(pp, pw)
+    e.upload(w.pos, rad, pdis, angv)
+    r = e.adjoint(STEPS, EVERY, objective)
+    s = e.scalars()
+    assert s["status"] == 0
+    e.close()
+    return r
+
+
+def grad_from_adjoint(r, key):
+    return sum(r["d_pp"][k] for k in KEYS[key]) * 1.0, sum(r["d_pw"][k] for k in KEYS[key])
+
+
+def oracle_objective(orc, dem, w, pdis, angv, pp, pw, rad, objective, cell):
+    o = orc.run(w.pos, rad, w.world, w.dt, w.skin, cell, w.density, dem.material_array(pp, pw), False, STEPS,
+                w.relist_interval, pdis=pdis, angv=angv)
+    p = o["pos"].reshape(-1, 3)
+    area = w.world[0] * w.world[1]
+    if objective == dem.OBJ_PACKING:
+        return np.sum(4.0 / 3.0 * np.pi * rad ** 3) / (area * max(p[:, 2].max(), 0.0))
+    m = w.density * 8.0 * rad ** 3
+    U = np.sum(m * p[:, 2])
+    d = p[:, None, :] - p[None, :, :]
+    dist = np.sqrt((d ** 2).sum(-1))
+    ov = rad[:, None] + rad[None, :] - dist
+    iu = np.triu_indices(w.n, 1)
+    ov = ov[iu]
+    Rs = (rad[:, None] * rad[None, :] / (rad[:, None] + rad[None, :]))[iu]
+    touch = ov > 0
+    U += np.sum(0.4 * pp["estar"] * np.sqrt(Rs[touch]) * ov[touch] ** 2.5)
+    hx, hy = w.world[0] / 2, w.world[1] / 2
+    for dl in (rad - p[:, 2], rad - (p[:, 0] + hx), rad - (hx - p[:, 0]), rad - (p[:, 1] + hy), rad - (hy - p[:, 1])):
+        t = dl > 0
+        U += np.sum(0.4 * pw["estar"] * np.sqrt(rad[t]) * dl[t] ** 2.5)
+    return U
+
+
+@pytest.mark.parametrize("objective", [0, 1])
+def test_adjoint_matches_finite_differences(dem, orc, cuda, objective):
+    w, pdis, angv = case(dem)
+    base = run_adjoint(dem, w, pdis, angv, w.pp, w.pw, w.rad, objective)
+    assert np.isfinite(base["value"]) and base["value"] > 0
+    cell = w.cell() + 0.01
+    h = 1e-5
+    floor = 1e-8 * abs(base["value"])   # FD noise floor of the objective
+    for key in KEYS:
+        g_ad = sum(grad_from_adjoint(base, key)) * w.pp[KEYS[key][0]]   # d/d(log parameter)
+        vp = run_adjoint(dem, w, pdis, angv, scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h), w.rad, objective)
+        vm = run_adjoint(dem, w, pdis, angv, scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h), w.rad, objective)
+        g_fd = (vp["value"] - vm["value"]) / (2 * h)
+        op = oracle_objective(orc, dem, w, pdis, angv, scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h), w.rad,
+                              objective, cell)
+        om = oracle_objective(orc, dem, w, pdis, angv, scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h), w.rad,
+                              objective, cell)
+        g_or = (op - om) / (2 * h)
+        assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd) + floor, (key, g_ad, g_fd)
+        assert abs(g_ad - g_or) <= 1e-3 * abs(g_or) + floor, (key, g_ad, g_or)
+    # radii: directional derivative along a random direction
+    rng = np.random.default_rng(5)
+    v = rng.normal(size=w.n)
+    g_ad = float(base["d_radii"] @ v)
+    hr = 1e-7
+    vp = run_adjoint(dem, w, pdis, angv, w.pp, w.pw, w.rad + hr * v, objective)
+    vm = run_adjoint(dem, w, pdis, angv, w.pp, w.pw, w.rad - hr * v, objective)
+    g_fd = (vp["value"] - vm["value"]) / (2 * hr)
+    assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd), (g_ad, g_fd)
+
+
+def test_adjoint_leaves_forward_state(dem, cuda):
+    """After dem_adjoint_window the context holds the state of a plain
+    forward run of the same window, and its observables."""
+    w, pdis, angv = case(dem)
+    kw = {**w.engine_kwargs(), "precision": dem.PREC_FP64}
+    a = dem.Engine(**kw)
+    a.set_material(w.pp, w.pw)
+    a.upload(w.pos, w.rad, pdis, angv)
+    a.adjoint(STEPS, EVERY, dem.OBJ_POTENTIAL)
+    b = dem.Engine(**kw)
+    b.set_material(w.pp, w.pw)
+    b.upload(w.pos, w.rad, pdis, angv)
+    b.step(STEPS)
+    for x, y in zip(a.download(), b.download()):
+        np.testing.assert_array_equal(x, y)
+    sa, sb = a.scalars(), b.scalars()
+    assert sa["maxhz"] == sb["maxhz"] and sa["contacts"] == sb["contacts"] and sa["step"] == sb["step"]
+    a.step(20)   # and it can continue
+    assert a.scalars()["status"] == 0
+
+
+def test_adjoint_settle_50k_window(dem, wl, cuda):
+    """The 50,000-sphere configuration: pre-settled 20,000 steps, then a
+    2,000-step mixed-precision window with checkpoints every 100; gradients of
+    the potential energy against central differences of the GPU forward."""
+    w = wl.settle_50k()
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad)
+    e.step(w.meta["presettle_steps"])
+    pos, pdis, angv = e.download()
+    e.close()
+
+    def value(pp, pw, rad, grads=False):
+        x = dem.Engine(**{**w.engine_kwargs(), "cell": w.cell() + 0.01})
+        x.set_material(pp, pw)
+        x.upload(pos, rad, pdis, angv)
+        r = x.adjoint(w.steps, 100, dem.OBJ_POTENTIAL, radii=grads)
+        assert x.scalars()["status"] == 0
+        x.close()
+        return r
+
+    base = value(w.pp, w.pw, w.rad, grads=True)
+    floor = 1e-8 * abs(base["value"])
+    h = 1e-4
+    for key in ("estar", "damp"):
+        g_ad = sum(grad_from_adjoint(base, key)) * w.pp[KEYS[key][0]]
+        vp = value(scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h), w.rad)["value"]
+        vm = value(scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h), w.rad)["value"]
+        g_fd = (vp - vm) / (2 * h)
+        assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd) + floor, (key, g_ad, g_fd)
+    # radii are FP32 in the mixed form: a direction on the FP32 grid, scaled
+    rng = np.random.default_rng(2)
+    v = np.sign(rng.normal(size=w.n)) * 2.0 ** -16
+    g_ad = float(base["d_radii"] @ v)
+    vp = value(w.pp, w.pw, w.rad + v)["value"]
+    vm = value(w.pp, w.pw, w.rad - v)["value"]
+    g_fd = (vp - vm) / 2.0
+    assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd), (g_ad, g_fd)

@@ -29,6 +29,7 @@ namespace dem {
 
 namespace {
 constexpr int kB = 256;
+constexpr int kPairB = 128;   // block size of k_adj_pairs; pbar holds one 12-slot row per block
 
 struct Ck {
     double* pos = nullptr;   // 3 np
@@ -56,7 +57,8 @@ struct AdjWork {
     void* ta = nullptr;
     double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Fb = nullptr, *Tb = nullptr, *Rb = nullptr;
     double* Hb[2] = {nullptr, nullptr};
-    double* pbar = nullptr;      // nblk x 12
+    double* pbar = nullptr;      // npb x 12 (one row per k_adj_pairs block)
+    long long npb = 0;
     double* obj = nullptr;       // [0] value, [1..] scratch
     unsigned long long* zmax = nullptr;  // [0] max z bits, [1] argmax
     unsigned long long* save_mz = nullptr;   // observables of the forward's last step
@@ -87,9 +89,10 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
         if ((rc = dalloc(&w->Xb, 3 * np)) || (rc = dalloc(&w->Db, 3 * np)) || (rc = dalloc(&w->Ab, 3 * np)) ||
             (rc = dalloc(&w->Wb, 3 * np)) || (rc = dalloc(&w->Fb, 3 * np)) || (rc = dalloc(&w->Tb, 3 * np)) ||
             (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
-            (rc = dalloc(&w->pbar, (size_t)c->nblk * 12)) || (rc = dalloc(&w->obj, 16)) || (rc = dalloc(&w->zmax, 2)) ||
+            (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) || (rc = dalloc(&w->zmax, 2)) ||
             (rc = dalloc(&w->save_mz, c->nblk)) || (rc = dalloc(&w->save_cnt, c->nblk)))
             return rc;
+        w->npb = grid_for(c->n, kPairB);
     }
     if (seg > w->seg) {
         void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta};
@@ -220,14 +223,14 @@ struct AdjList {
 // of the input adjoints; the pair's history adjoint and its parameter
 // adjoints are kept by the lower index only.
 template <typename Real>
-__global__ void __launch_bounds__(128) k_adj_pairs(
+__global__ void __launch_bounds__(kPairB) k_adj_pairs(
     long long n, long long np, long long cap, AdjList L, const double* __restrict__ tx, const double* __restrict__ td,
     const Real* __restrict__ ta, const double* __restrict__ twh,
     const double* __restrict__ th, const Real* __restrict__ R, LawParams<double> pp, LawParams<double> pw,
     double inv_dt, double density, double hx, double hy, const double* __restrict__ Fb, const double* __restrict__ Tb,
     const double* __restrict__ Hout, double* __restrict__ Hin, double* __restrict__ Xb, double* __restrict__ Db,
     double* __restrict__ Ab, double* __restrict__ Wb, double* __restrict__ Rb, double* __restrict__ pbar) {
-    __shared__ double sp[12][kB / 32];
+    __shared__ double sp[12][kPairB / 32];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     LawBar bp, bw;
     lawbar_zero(bp);
@@ -465,8 +468,7 @@ template <typename Real> int adj_pairs(dem_ctx* c, long long t, const ListRec& l
     AdjWork* w = c->adj;
     const long long np = c->npad, cap = c->cap;
     AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
-    const unsigned nb = grid_for(c->n, 128);
-    k_adj_pairs<Real><<<nb, 128, 0, c->stream>>>(
+    k_adj_pairs<Real><<<(unsigned)w->npb, kPairB, 0, c->stream>>>(
         c->n, np, cap, L, w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t,
         w->twh + 3 * np * t, w->th + 3 * cap * t, (const Real*)c->rad, make_law<double>(c->mat.pp),
         make_law<double>(c->mat.pw), 1.0 / c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
@@ -561,7 +563,7 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     DEM_CUDA_TRY(cudaMemsetAsync(w->Wb, 0, 3 * np * sizeof(double), s));
     DEM_CUDA_TRY(cudaMemsetAsync(w->Rb, 0, np * sizeof(double), s));
     DEM_CUDA_TRY(cudaMemsetAsync(w->Hb[0], 0, 3 * cap * sizeof(double), s));
-    DEM_CUDA_TRY(cudaMemsetAsync(w->pbar, 0, (size_t)c->nblk * 12 * sizeof(double), s));
+    DEM_CUDA_TRY(cudaMemsetAsync(w->pbar, 0, (size_t)w->npb * 12 * sizeof(double), s));
     rc = mixed ? objective<float>(c, which) : objective<double>(c, which);
     if (rc) return rc;
     // ------------------------------------------------------- reverse segments
@@ -626,14 +628,14 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     }
     DEM_CUDA_TRY(cudaEventRecord(c->ev[2], s));
     // ------------------------------------------------------------ results
-    std::vector<double> pb((size_t)c->nblk * 12);
+    std::vector<double> pb((size_t)w->npb * 12);
     double obj[2];
     DEM_CUDA_TRY(cudaMemcpyAsync(pb.data(), w->pbar, pb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (d_radii) DEM_CUDA_TRY(cudaMemcpyAsync(d_radii, w->Rb, c->n * sizeof(double), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
     double acc[12] = {0};
-    for (size_t b = 0; b < c->nblk; b++)
+    for (size_t b = 0; b < (size_t)w->npb; b++)
         for (int k = 0; k < 12; k++) acc[k] += pb[b * 12 + k];
     out->value = obj[0];
     out->d_pp = dem_contact{acc[0], acc[1], 0.0, acc[2], acc[3], acc[4], acc[5]};

@@ -568,6 +568,7 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     if (rc) return rc;
     // ------------------------------------------------------- reverse segments
     dem_record_forces(c, 1);
+    c->observe_slot = -1;   // the recompute writes no observables
     int hb = 0;   // Hb[hb]: adjoint of the pair history output by the step being reversed
     for (long long g = nseg - 1; g >= 0; g--) {
         if ((rc = restore_ck(c, w->ck[g]))) return rc;

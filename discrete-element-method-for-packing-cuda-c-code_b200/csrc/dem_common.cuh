@@ -57,6 +57,32 @@ inline unsigned grid_for(long long n, int block) {
     return (unsigned)(g < 1 ? 1 : g);
 }
 
+// Programmatic dependent launch (sm_90+).  A kernel launched with
+// programmatic stream serialization may start while its predecessor in the
+// stream is still running; pdl_wait() returns once every predecessor has
+// completed and its writes are visible (immediately when the kernel was
+// launched normally).  pdl_trigger() lets the successor be scheduled as soon
+// as every block of this kernel has started.  Before pdl_wait() a kernel may
+// read only data written before the last normally launched kernel.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_ex(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, bool pdl,
+                      Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Device-wide exclusive scan of uint32 (3 launches, no host sync).
 // out[i] = sum_{t<i} in[i]; if total != nullptr, *total (device) = full sum.
 // out may alias in.  Scratch: tmp with scan_scratch_words(n) uint32.

@@ -23,6 +23,7 @@
 //  * a whole re-list window (re-list + K steps) captured once as a CUDA graph;
 //    no host synchronisation inside dem_step_n.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 #include <algorithm>
@@ -37,9 +38,6 @@ namespace dem {
 #endif
 #ifndef DEM_PP_MINB
 #define DEM_PP_MINB 3
-#endif
-#ifndef DEM_PAIR_GRID_MAX
-#define DEM_PAIR_GRID_MAX (148 * 8)
 #endif
 
 
@@ -303,12 +301,16 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
     }
 }
 
-__global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, const uint* __restrict__ off,
-                           long long cap) {
+// Sort each reverse row (pair indices ascending: a deterministic order for
+// the gather) and record each pair's reverse slot ru[k].
+__global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,
+                           const uint* __restrict__ off, long long cap) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if ((long long)off[n] > cap) return;
-    isort_u32(rk + roff[i], roff[i + 1] - roff[i]);
+    const uint b = roff[i], e = roff[i + 1];
+    isort_u32(rk + b, e - b);
+    for (uint u = b; u < e; u++) ru[rk[u]] = u;
 }
 
 // ------------------------------------------------------------ pair force
@@ -347,61 +349,90 @@ __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double
     return 1;
 }
 
-// PCCP: one thread per candidate pair; per-pair results for the gather.
-// PCCP: one thread per candidate pair; per-pair results for the gather.  The
-// same grid then evaluates the wall contacts of the window's wall candidates
-// (calforceiw's role, neiglist.cu:287-301): history W in place (zero when not
-// touching), wall force and torque per candidate in wf[2c], wf[2c+1].
+// PCCP pair kernel (calculateforcepairD's role, neiglist.cu:156-233, and
+// calforceiw's, neiglist.cu:287-301).  One item space: items [0, nw) are the
+// window's wall candidates, items [nw, nw + P) the listed pairs, so every
+// thread of the one-wave grid takes at most one item per pass.
+//   wall item c:  history W in place (zero when not touching); wall force and
+//                 torque in wf[2c], wf[2c+1]
+//   pair item k:  history H[k] in place; force/torque on lo in pf[k]/pti[k]
+//                 (row slot k), force/torque on hi in rfj[u]/rtj[u] at the
+//                 pair's reverse-row slot u = ru[k], so the gather reads both
+//                 of a sphere's row ranges directly.  .w = 1 marks a contact.
 template <typename Real>
 __global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long long n, long long cap,
                                               const uint* __restrict__ lp, const uint* __restrict__ ln,
-                                              Planes3<double> P, Planes3<double> D, Planes3<Real> A,
-                                              const Real* __restrict__ R, Planes3<double> H, LawParams<Real> pp,
-                                              Real inv_dt, Real density, R4<Real>* __restrict__ pf,
-                                              R4<Real>* __restrict__ pti, R4<Real>* __restrict__ ptj,
+                                              const uint* __restrict__ ru, Planes3<double> P, Planes3<double> D,
+                                              Planes3<Real> A, const Real* __restrict__ R, Planes3<double> H,
+                                              LawParams<Real> pp, Real inv_dt, Real density,
+                                              R4<Real>* __restrict__ pf, R4<Real>* __restrict__ pti,
+                                              R4<Real>* __restrict__ rfj, R4<Real>* __restrict__ rtj,
                                               const uint* __restrict__ wlist, const uint* __restrict__ wcount,
                                               Planes3<double> W, LawParams<Real> pw, double hx, double hy,
                                               R4<Real>* __restrict__ wf) {
+    pdl_trigger();
     const long long stride = (long long)gridDim.x * blockDim.x;
+    // list-time data (written by the re-list): safe before pdl_wait
     const uint nw = *wcount;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < (long long)nw; c += stride) {
-        const uint i = wlist[c];
-        const Real r = R[i];
-        const Real m = density * (Real)8 * r * r * r;
-        V3<double> h = mk(W.x[i], W.y[i], W.z[i]);
-        V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
-        const int hit = wall_contacts<Real>(hx, hy, mk(P.x[i], P.y[i], P.z[i]), cvt<Real>(mk(D.x[i], D.y[i], D.z[i])),
-                                            mk(A.x[i], A.y[i], A.z[i]), r, m, h, inv_dt, pw, Fw, Tw, (Real*)nullptr);
-        W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z;
-        R4<Real> a4, b4;
-        a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
-        b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
-        wf[2 * c] = a4;
-        wf[2 * c + 1] = b4;
-    }
     const uint total = off[n];
-    if ((long long)total > cap) return;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total; k += stride) {
-        const uint i = lp[k], j = ln[k];
-        V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
-        V3<Real> Fi, Ti, Tj;
-        const int c = pair_eval<Real>(mk(P.x[i], P.y[i], P.z[i]), mk(P.x[j], P.y[j], P.z[j]),
-                                      mk(D.x[i], D.y[i], D.z[i]), mk(D.x[j], D.y[j], D.z[j]),
-                                      mk(A.x[i], A.y[i], A.z[i]), mk(A.x[j], A.y[j], A.z[j]), R[i], R[j], h, pp,
-                                      inv_dt, density, Fi, Ti, Tj);
-        H.x[k] = h.x; H.y[k] = h.y; H.z[k] = h.z;
-        R4<Real> fo;
-        if (c) {
-            fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
+    const long long items = (long long)nw + ((long long)total <= cap ? (long long)total : 0ll);
+    long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    uint i = 0, j = 0, rslot = 0;
+    if (u < (long long)nw) {
+        i = wlist[u];
+    } else if (u < items) {
+        const long long k = u - nw;
+        i = lp[k]; j = ln[k]; rslot = ru[k];
+    }
+    pdl_wait();
+    for (; u < items; u += stride) {
+        if (u < (long long)nw) {
+            const Real r = R[i];
+            const Real m = density * (Real)8 * r * r * r;
+            V3<double> h = mk(W.x[i], W.y[i], W.z[i]);
+            V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
+            const int hit = wall_contacts<Real>(hx, hy, mk(P.x[i], P.y[i], P.z[i]),
+                                                cvt<Real>(mk(D.x[i], D.y[i], D.z[i])), mk(A.x[i], A.y[i], A.z[i]), r,
+                                                m, h, inv_dt, pw, Fw, Tw, (Real*)nullptr);
+            W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z;
             R4<Real> a4, b4;
-            a4.x = Ti.x; a4.y = Ti.y; a4.z = Ti.z; a4.w = (Real)0;
-            b4.x = Tj.x; b4.y = Tj.y; b4.z = Tj.z; b4.w = (Real)0;
-            pti[k] = a4;
-            ptj[k] = b4;
+            a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
+            b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
+            wf[2 * u] = a4;
+            wf[2 * u + 1] = b4;
         } else {
-            fo.x = fo.y = fo.z = fo.w = (Real)0;
+            const long long k = u - nw;
+            V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
+            V3<Real> Fi, Ti, Tj;
+            const int c = pair_eval<Real>(mk(P.x[i], P.y[i], P.z[i]), mk(P.x[j], P.y[j], P.z[j]),
+                                          mk(D.x[i], D.y[i], D.z[i]), mk(D.x[j], D.y[j], D.z[j]),
+                                          mk(A.x[i], A.y[i], A.z[i]), mk(A.x[j], A.y[j], A.z[j]), R[i], R[j], h,
+                                          pp, inv_dt, density, Fi, Ti, Tj);
+            H.x[k] = h.x; H.y[k] = h.y; H.z[k] = h.z;
+            R4<Real> fo, fr;
+            if (c) {
+                fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
+                fr.x = -Fi.x; fr.y = -Fi.y; fr.z = -Fi.z; fr.w = (Real)1;
+                R4<Real> a4, b4;
+                a4.x = Ti.x; a4.y = Ti.y; a4.z = Ti.z; a4.w = (Real)0;
+                b4.x = Tj.x; b4.y = Tj.y; b4.z = Tj.z; b4.w = (Real)0;
+                pti[k] = a4;
+                rtj[rslot] = b4;
+            } else {
+                fo.x = fo.y = fo.z = fo.w = (Real)0;
+                fr = fo;
+            }
+            pf[k] = fo;
+            rfj[rslot] = fr;
         }
-        pf[k] = fo;
+        // indices of this thread's next item (grid-stride pass)
+        const long long v = u + stride;
+        if (v < (long long)nw) {
+            i = wlist[v];
+        } else if (v < items) {
+            const long long k = v - nw;
+            i = lp[k]; j = ln[k]; rslot = ru[k];
+        }
     }
 }
 
@@ -441,15 +472,28 @@ __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real
         dbgT[3 * i] = T.x; dbgT[3 * i + 1] = T.y; dbgT[3 * i + 2] = T.z;
         dbgC[i] = cnt;
     }
-    // symplectic Euler in displacement form (neiglist.cu:356-360)
+    // symplectic Euler in displacement form (neiglist.cu:356-360).  FP64 form:
+    // the reference's F dt dt / m term by term; mixed form: one reciprocal
+    // dt^2/m (FP64) and dt^2/I (FP32) per particle.
     const double dt = pc.dt;
-    d.x = d.x + (double)F.x * dt * dt / (double)m;
-    d.y = d.y + (double)F.y * dt * dt / (double)m;
-    d.z = d.z + (double)F.z * dt * dt / (double)m;
+    if (sizeof(Real) == 8) {
+        d.x = d.x + (double)F.x * dt * dt / (double)m;
+        d.y = d.y + (double)F.y * dt * dt / (double)m;
+        d.z = d.z + (double)F.z * dt * dt / (double)m;
+        a.x = a.x + T.x * dtr * dtr / I;
+        a.y = a.y + T.y * dtr * dtr / I;
+        a.z = a.z + T.z * dtr * dtr / I;
+    } else {
+        const double km = dt * dt / (double)m;
+        const Real kI = dtr * dtr / I;
+        d.x = d.x + (double)F.x * km;
+        d.y = d.y + (double)F.y * km;
+        d.z = d.z + (double)F.z * km;
+        a.x = a.x + T.x * kI;
+        a.y = a.y + T.y * kI;
+        a.z = a.z + T.z * kI;
+    }
     x.x += d.x; x.y += d.y; x.z += d.z;
-    a.x = a.x + T.x * dtr * dtr / I;
-    a.y = a.y + T.y * dtr * dtr / I;
-    a.z = a.z + T.z * dtr * dtr / I;
     q.x += (float)d.x; q.y += (float)d.y; q.z += (float)d.z;
     q.w = __uint_as_float(wflag);
     Po.x[i] = x.x; Po.y[i] = x.y; Po.z[i] = x.z;
@@ -461,8 +505,17 @@ __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real
     mz = x.z > 0.0 ? x.z : 0.0;
 }
 
-__device__ __forceinline__ void block_observables(double mz, uint cnt, uint flags, StepPartials part,
+// Per-step observables: on the observed step (the last of a window, or of an
+// eager call) one partial per block -- max height, contact count -- with no
+// same-address atomics; on every step the status flags (skin, non-finite),
+// OR-ed into the status word by one lane per warp that saw any.
+__device__ __forceinline__ void block_observables(double mz, uint cnt, uint flags, int observe, StepPartials part,
                                                   EngineWords* words) {
+    if (!observe) {
+        flags = __reduce_or_sync(0xffffffffu, flags);
+        if (flags && lane_id() == 0) atomicOr(&words->status, flags);
+        return;
+    }
     __shared__ unsigned long long s_mz[8];
     __shared__ uint s_cnt[8], s_fl[8];
     unsigned long long mb = (unsigned long long)__double_as_longlong(mz);
@@ -470,9 +523,9 @@ __device__ __forceinline__ void block_observables(double mz, uint cnt, uint flag
     for (int o = 16; o > 0; o >>= 1) {
         unsigned long long ob = __shfl_xor_sync(0xffffffffu, mb, o);
         mb = ob > mb ? ob : mb;
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        flags |= __shfl_xor_sync(0xffffffffu, flags, o);
     }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    flags = __reduce_or_sync(0xffffffffu, flags);
     const int warp = threadIdx.x >> 5;
     if (lane_id() == 0) { s_mz[warp] = mb; s_cnt[warp] = cnt; s_fl[warp] = flags; }
     __syncthreads();
@@ -485,32 +538,39 @@ __device__ __forceinline__ void block_observables(double mz, uint cnt, uint flag
     }
 }
 
-// PCCP gather (sumallforceiD's role, through the CSR rows and the reverse
-// rows) + particle_finish, one thread per particle.  State is updated in place.
+// PCCP gather (sumallforceiD's role, through the CSR row and the reverse
+// row of the sphere, both read as contiguous ranges) + particle_finish, one
+// thread per particle.  State is updated in place.
 template <typename Real>
 __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n, const uint* __restrict__ off,
-                                                  const uint* __restrict__ roff, const uint* __restrict__ rk,
-                                                  long long cap, const R4<Real>* __restrict__ pf,
-                                                  const R4<Real>* __restrict__ pti, const R4<Real>* __restrict__ ptj,
+                                                  const uint* __restrict__ roff, long long cap,
+                                                  const R4<Real>* __restrict__ pf, const R4<Real>* __restrict__ pti,
+                                                  const R4<Real>* __restrict__ rfj, const R4<Real>* __restrict__ rtj,
                                                   Planes3<double> P, Planes3<double> D, Planes3<Real> A,
                                                   const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
                                                   LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt,
                                                   Real density, StepPartials part, EngineWords* words, double* dbgF,
                                                   double* dbgT, uint* dbgC, const uint* __restrict__ wslot,
                                                   const R4<Real>* __restrict__ wf) {
+    pdl_trigger();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz = 0.0;
     uint cnt = 0, flags = 0;
+    // list-time data and the radius: safe before pdl_wait
+    Real r = (Real)0;
+    uint ws = kEmpty, total = 0, o0 = 0, o1 = 0, r0 = 0, r1 = 0;
     if (i < n) {
-        // every per-particle load is issued before the data-dependent loops
-        const Real r = R[i];
+        r = R[i];
+        ws = wslot[i];
+        total = off[n];
+        o0 = off[i]; o1 = off[i + 1]; r0 = roff[i]; r1 = roff[i + 1];
+    }
+    pdl_wait();
+    if (i < n) {
         const V3<double> x = mk(P.x[i], P.y[i], P.z[i]);
         const V3<double> d = mk(D.x[i], D.y[i], D.z[i]);
         const V3<Real> a = mk(A.x[i], A.y[i], A.z[i]);
         const float4 q = Q[i];
-        const uint ws = wslot[i];
-        const uint total = off[n];
-        const uint o0 = off[i], o1 = off[i + 1], r0 = roff[i], r1 = roff[i + 1];
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
         if ((long long)total <= cap) {
             for (uint k = o0; k < o1; k++) {
@@ -523,12 +583,10 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n
                 }
             }
             for (uint u = r0; u < r1; u++) {
-                const uint k = rk[u];
-                if (k >= total) continue;
-                const R4<Real> f = pf[k];
+                const R4<Real> f = rfj[u];
                 if (f.w != (Real)0) {
-                    const R4<Real> t = ptj[k];
-                    F.x -= f.x; F.y -= f.y; F.z -= f.z;
+                    const R4<Real> t = rtj[u];
+                    F.x += f.x; F.y += f.y; F.z += f.z;
                     T.x += t.x; T.y += t.y; T.z += t.z;
                     cnt++;
                 }
@@ -543,7 +601,7 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n
         particle_finish<Real, false>(i, F, T, r, x, d, a, q, P, D, A, Q, W, pw, pc, dtr, inv_dt, density, mz, flags,
                                      cnt, dbgF, dbgT, dbgC);
     }
-    block_observables(mz, cnt, flags, part, words);
+    block_observables(mz, cnt, flags, pc.observe, part, words);
 }
 
 // PP (particle-parallel, the paper's Figure 1(b)): each particle evaluates all
@@ -560,17 +618,24 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     float4* __restrict__ Q, Planes3<double> W, Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp,
     LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt, Real density, StepPartials part,
     EngineWords* words, double* dbgF, double* dbgT, uint* dbgC) {
+    pdl_trigger();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz = 0.0;
     uint cnt = 0, flags = 0;
+    // list-time data and the radius: safe before pdl_wait
+    Real r = (Real)0;
+    uint total = 0, o0 = 0, o1 = 0, r0 = 0, r1 = 0;
     if (i < n) {
-        const Real r = R[i];
+        r = R[i];
+        total = off[n];
+        o0 = off[i]; o1 = off[i + 1]; r0 = roff[i]; r1 = roff[i + 1];
+    }
+    pdl_wait();
+    if (i < n) {
         const V3<double> x = mk(Pi.x[i], Pi.y[i], Pi.z[i]);
         const V3<double> d = mk(Di.x[i], Di.y[i], Di.z[i]);
         const V3<Real> a = mk(Ai.x[i], Ai.y[i], Ai.z[i]);
         const float4 q = Q[i];
-        const uint total = off[n];
-        const uint o0 = off[i], o1 = off[i + 1], r0 = roff[i], r1 = roff[i + 1];
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
         if ((long long)total <= cap) {
             for (uint k = o0; k < o1; k++) {
@@ -598,7 +663,7 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
         particle_finish<Real, true>(i, F, T, r, x, d, a, q, Po, Do, Ao, Q, W, pw, pc, dtr, inv_dt, density, mz, flags,
                                     cnt, dbgF, dbgT, dbgC);
     }
-    block_observables(mz, cnt, flags, part, words);
+    block_observables(mz, cnt, flags, pc.observe, part, words);
 }
 
 __global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned long long* out) {
@@ -663,6 +728,7 @@ ParticleCommon particle_common(const dem_ctx* c, int slot) {
     const float hs = (float)(0.5 * c->cfg.skin);
     pc.half_skin2 = hs * hs;
     pc.first = slot == 0 ? 1 : 0;
+    pc.observe = slot == c->observe_slot ? 1 : 0;
     return pc;
 }
 
@@ -700,25 +766,29 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
         c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
         planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry);
-    k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->off[dst], c->cap);
+    k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->ru, c->off[dst], c->cap);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
 
-template <typename Real> int launch_pair(dem_ctx* c, int lst) {
+// Step kernels after the first of a window may launch programmatically
+// (overlapping their predecessor's tail); never while profiling or recording,
+// where events or tape kernels sit between them.
+bool step_pdl(const dem_ctx* c, int slot, bool first_of_step) {
+    return c->pdl && !c->profiling && !c->record && (slot > 0 || !first_of_step);
+}
+
+template <typename Real> int launch_pair(dem_ctx* c, int lst, int slot) {
     const long long np = c->npad;
     LawParams<Real> pp = make_law<Real>(c->mat.pp);
-    long long want = (c->cap + 255) / 256;
-    unsigned grid = (unsigned)std::min<long long>(std::max<long long>(want, 1), (long long)DEM_PAIR_GRID_MAX);
-    k_pair<Real><<<grid, 256, 0, c->stream>>>(c->off[lst], c->n, c->cap, c->lp, c->ln[lst],
-                                               planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
-                                               planes<Real>(c->ang[0], np), (const Real*)c->rad,
-                                               planes<double>(c->hist[lst][0], c->cap), pp, (Real)(1.0 / c->cfg.dt),
-                                               (Real)c->cfg.density, (R4<Real>*)c->pf, (R4<Real>*)c->pti,
-                                               (R4<Real>*)c->ptj, c->wlist, c->wcount, planes<double>(c->wh, np),
-                                               make_law<Real>(c->mat.pw), c->cfg.world[0] * 0.5,
-                                               c->cfg.world[1] * 0.5, (R4<Real>*)c->wf);
-    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(launch_ex(k_pair<Real>, c->pair_grid, 256, c->stream, step_pdl(c, slot, true), c->off[lst], c->n,
+                           c->cap, c->lp, c->ln[lst], c->ru, planes<double>(c->pos[0], np),
+                           planes<double>(c->disp[0], np), planes<Real>(c->ang[0], np), (const Real*)c->rad,
+                           planes<double>(c->hist[lst][0], c->cap), pp, (Real)(1.0 / c->cfg.dt),
+                           (Real)c->cfg.density, (R4<Real>*)c->pf, (R4<Real>*)c->pti, (R4<Real>*)c->rfj,
+                           (R4<Real>*)c->rtj, c->wlist, c->wcount, planes<double>(c->wh, np),
+                           make_law<Real>(c->mat.pw), c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
+                           (R4<Real>*)c->wf));
     return DEM_OK;
 }
 
@@ -726,14 +796,14 @@ template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
     const long long n = c->n, np = c->npad;
     LawParams<Real> pw = make_law<Real>(c->mat.pw);
     const double dt = c->cfg.dt;
-    k_particle<Real><<<grid_for(n, 256), 256, 0, c->stream>>>(
-        n, c->off[lst], c->roff, c->rk, c->cap, (const R4<Real>*)c->pf, (const R4<Real>*)c->pti,
-        (const R4<Real>*)c->ptj, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
-        planes<Real>(c->ang[0], np), (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw,
-        particle_common(c, slot), (Real)dt, (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words,
-        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, c->wslot,
-        (const R4<Real>*)c->wf);
-    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(launch_ex(
+        k_particle<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, false), n, c->off[lst], c->roff,
+        c->cap, (const R4<Real>*)c->pf, (const R4<Real>*)c->pti, (const R4<Real>*)c->rfj, (const R4<Real>*)c->rtj,
+        planes<double>(c->pos[0], np), planes<double>(c->disp[0], np), planes<Real>(c->ang[0], np),
+        (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw, particle_common(c, slot), (Real)dt,
+        (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words, c->record ? c->dbgF : nullptr,
+        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, (const uint*)c->wslot,
+        (const R4<Real>*)c->wf));
     return DEM_OK;
 }
 
@@ -742,15 +812,14 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
     const long long n = c->n, np = c->npad;
     LawParams<Real> pp = make_law<Real>(c->mat.pp), pw = make_law<Real>(c->mat.pw);
     const double dt = c->cfg.dt;
-    k_step_pp<Real><<<grid_for(n, 256), 256, 0, c->stream>>>(
-        n, c->off[lst], c->roff, c->rk, c->lp, c->ln[lst], c->cap, planes<double>(c->pos[sb], np),
-        planes<double>(c->disp[sb], np), planes<Real>(c->ang[sb], np), planes<double>(c->pos[1 - sb], np),
-        planes<double>(c->disp[1 - sb], np), planes<Real>(c->ang[1 - sb], np), (const Real*)c->rad, c->q,
-        planes<double>(c->wh, np), planes<double>(c->hist[lst][hp], c->cap),
-        planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw, particle_common(c, slot), (Real)dt, (Real)(1.0 / dt),
-        (Real)c->cfg.density, partials(c, slot), c->words, c->record ? c->dbgF : nullptr,
-        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr);
-    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(launch_ex(
+        k_step_pp<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, true), n, c->off[lst], c->roff,
+        c->rk, c->lp, c->ln[lst], c->cap, planes<double>(c->pos[sb], np), planes<double>(c->disp[sb], np),
+        planes<Real>(c->ang[sb], np), planes<double>(c->pos[1 - sb], np), planes<double>(c->disp[1 - sb], np),
+        planes<Real>(c->ang[1 - sb], np), (const Real*)c->rad, c->q, planes<double>(c->wh, np),
+        planes<double>(c->hist[lst][hp], c->cap), planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw,
+        particle_common(c, slot), (Real)dt, (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words,
+        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr));
     return DEM_OK;
 }
 
@@ -774,7 +843,7 @@ int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part
         c->sbuf ^= 1;
         c->hph ^= 1;
     } else {
-        rc = mixed ? launch_pair<float>(c, lst) : launch_pair<double>(c, lst);
+        rc = mixed ? launch_pair<float>(c, lst, slot) : launch_pair<double>(c, lst, slot);
         if (rc) return rc;
         if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
         rc = mixed ? launch_particle<float>(c, lst, slot) : launch_particle<double>(c, lst, slot);
@@ -802,6 +871,7 @@ int enqueue_window(dem_ctx* c, int src) {
     if (rc) return rc;
     c->hph = 0;
     const int lst = 1 - src;
+    c->observe_slot = K - 1;
     double a, b;
     for (int s = 0; s < K; s++) {
         rc = step_kernels(c, lst, s, &a, &b);
@@ -886,7 +956,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->skeyu, np)) || (rc = dalloc(&c->skey, np)) || (rc = dalloc(&c->njgi, np)) ||
         (rc = dalloc(&c->njli, np)) || (rc = dalloc(&c->off[0], np + 1)) || (rc = dalloc(&c->off[1], np + 1)) ||
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
-        (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->words, 1)) ||
+        (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->ru, cap)) || (rc = dalloc(&c->words, 1)) ||
         (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
         (rc = dalloc(&c->wcount, 1)))
         return bail(rc);
@@ -897,10 +967,22 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if (e == cudaSuccess) e = cudaMalloc(&c->sposu, np * 4 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->pf, cap * 4 * rs);
     if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->pti, cap * 4 * rs);
-    if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->ptj, cap * 4 * rs);
+    if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->rfj, cap * 4 * rs);
+    if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->rtj, cap * 4 * rs);
     if (e == cudaSuccess) e = cudaMallocHost(&c->host_pinned, 4096);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (engine buffers)", __FILE__, __LINE__));
     c->nblk = grid_for(n, 256);
+    {   // one resident wave of the pair kernel (grid-stride over its items)
+        int nsm = 0, per = 0;
+        e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+        if (e == cudaSuccess)
+            e = c->prec == DEM_PREC_MIXED ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair<float>, 256, 0)
+                                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair<double>, 256, 0);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "pair kernel occupancy", __FILE__, __LINE__));
+        c->pair_grid = (unsigned)std::max(1, nsm * std::max(per, 1));
+        const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches inside a window
+        c->pdl = !(pdl && pdl[0] == '0');
+    }
     if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->nblk)) ||
         (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->nblk)))
         return bail(rc);
@@ -932,7 +1014,7 @@ int dem_destroy(dem_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->disp[0], c->disp[1], c->ang[0], c->ang[1], c->rad, c->q, c->wh,
                     c->staging, c->key, c->sid, c->sid2, c->spos, c->skeyu, c->skey, c->sposu, c->njgi, c->njli,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
-                    c->hist[1][0], c->hist[1][1], c->rk, c->pf, c->pti, c->ptj, c->scan_tmp, c->words, c->part_mz,
+                    c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1151,6 +1233,7 @@ int dem_step_n(dem_ctx* c, long long nsteps) {
         }
         const int slot = (int)c->in_window;
         double a = 0, b = 0;
+        c->observe_slot = nsteps == 1 ? slot : -1;   // the call's last step
         rc = step_kernels(c, c->cur, slot, &a, &b);
         if (rc) return rc;
         if (c->profiling) {

@@ -33,6 +33,7 @@ struct ParticleCommon {
     double dt, hx, hy;
     float half_skin2;
     int first;
+    int observe;   // write this step's per-block observables (max height, contacts)
 };
 
 }  // namespace dem
@@ -91,9 +92,13 @@ struct dem_ctx {
     uint* wlist = nullptr;   // wall candidates (particle ids)
     uint* wcount = nullptr;  // number of wall candidates (device)
     void* wf = nullptr;      // per candidate: wall force, wall torque (R4 each)
-    void* pf = nullptr;
-    void* pti = nullptr;
-    void* ptj = nullptr;
+    uint* ru = nullptr;      // per pair: its slot in the reverse rows
+    void* pf = nullptr;      // per pair (row slot): force on lo, .w = contact
+    void* pti = nullptr;     // per pair (row slot): torque on lo
+    void* rfj = nullptr;     // per reverse slot: force on hi, .w = contact
+    void* rtj = nullptr;     // per reverse slot: torque on hi
+    unsigned pair_grid = 1;  // one wave of the pair kernel
+    bool pdl = true;         // programmatic launches inside a window
     uint* scan_tmp = nullptr;
     size_t scan_words = 0;
     // scalars
@@ -112,6 +117,7 @@ struct dem_ctx {
     int cur = 0;
     long long step = 0, in_window = 0, relists = 0;
     int last_slot = -1;
+    int observe_slot = -1;   // window slot whose step writes the observables
     bool uploaded = false;
     // window graphs keyed by (previous list buffer, state buffer, history phase)
     cudaGraphExec_t gexec[2][2][2] = {};

@@ -116,8 +116,9 @@ __global__ void k_to_aos(long long n, Planes3<double> P, Planes3<double> D, Plan
 // re-list -- the same guarantee as the pair list's).
 template <typename Real>
 __global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count,
-                             const Real* __restrict__ R, double hx, double hy, double half_skin,
-                             uint* __restrict__ wslot, uint* __restrict__ wlist, uint* __restrict__ wcount) {
+                             uint* __restrict__ arrival, const Real* __restrict__ R, double hx, double hy,
+                             double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist,
+                             uint* __restrict__ wcount) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     {
@@ -138,16 +139,18 @@ __global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __re
     int cz = cell_axis<Real>(P.z[i], g.oz, csr, g.gz, xl);
     uint c = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
     key[i] = c;
-    atomicAdd(&count[c], 1u);
+    arrival[i] = atomicAdd(&count[c], 1u);   // the particle's slot among its cell's members (unordered)
 }
 
 // Scatter each particle (id, cell, list coordinates x,y,z,r in the list
-// precision) into its cell's range, unordered inside the cell; the count
-// array returns to zero.  Reads are coalesced by id.
+// precision) into its cell's range at its arrival slot, unordered inside the
+// cell; the count array returns to zero for the next re-list.  Reads are
+// coalesced by id.
 template <typename Real>
-__global__ void k_scatter(long long n, const uint* __restrict__ key, const uint* __restrict__ cstart,
-                          uint* __restrict__ count, Planes3<double> P, const Real* __restrict__ R, GridC g,
-                          uint* __restrict__ sidu, uint* __restrict__ skeyu, R4<Real>* __restrict__ sposu) {
+__global__ void k_scatter(long long n, const uint* __restrict__ key, const uint* __restrict__ arrival,
+                          const uint* __restrict__ cstart, uint* __restrict__ count, Planes3<double> P,
+                          const Real* __restrict__ R, GridC g, uint* __restrict__ sidu, uint* __restrict__ skeyu,
+                          R4<Real>* __restrict__ sposu) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint c = key[i];
@@ -156,7 +159,8 @@ __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint*
     v.y = (Real)(P.y[i] - g.oy);
     v.z = (Real)(P.z[i] - g.oz);
     v.w = R[i];
-    const uint slot = cstart[c] + atomicSub(&count[c], 1u) - 1u;
+    const uint slot = cstart[c] + arrival[i];
+    count[c] = 0u;
     sidu[slot] = (uint)i;
     skeyu[slot] = c;
     sposu[slot] = v;
@@ -205,7 +209,7 @@ __device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, 
         rs[r] = cstart[rowc + x0];
         re[r] = cstart[rowc + x1 + 1];
     }
-#pragma unroll 1
+#pragma unroll
     for (int r = 0; r < 9; r++) {
         for (uint u = rs[r]; u < re[r]; u++) {
             if ((long long)u == t) continue;
@@ -222,21 +226,27 @@ __device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, 
     }
 }
 
+// The re-list walk: per sorted slot t, count the candidates j > i (row of i)
+// and j < i (reverse row of i) and keep the first kScr j > i candidates in
+// scr[t * kScr ...]; rows longer than kScr are walked again by the fill.
+constexpr uint kScr = 8;
+
 template <typename Real>
-__global__ void k_nbr_count(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
-                            const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
-                            uint* __restrict__ njgi, uint* __restrict__ njli, EngineWords* words) {
+__global__ void k_nbr_walk(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
+                           const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
+                           uint* __restrict__ njgi, uint* __restrict__ njli, uint* __restrict__ scr,
+                           EngineWords* words) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     uint nall = 0;
     if (t < n) {
         const uint i = sid2[t];
         uint nup;
-        walk27<Real, false>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, nullptr, 0);
+        walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, scr + (size_t)t * kScr,
+                           kScr);
         njgi[i] = nup;
         njli[i] = nall - nup;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nall = max(nall, __shfl_xor_sync(0xffffffffu, nall, o));
+    nall = __reduce_max_sync(0xffffffffu, nall);
     if (lane_id() == 0 && nall) atomicMax(&words->max_row, nall);
 }
 
@@ -258,7 +268,7 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
                            uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
                            const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
                            uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
-                           uint* __restrict__ carry) {
+                           uint* __restrict__ carry, const uint* __restrict__ scr) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const uint total = off[n];
@@ -268,8 +278,12 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
     }
     const uint i = sid2[t];
     const uint b = off[i], e = off[i + 1];
-    uint nup, nall;
-    walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
+    if (e - b <= kScr) {
+        for (uint k = 0; k < e - b; k++) ln[b + k] = scr[(size_t)t * kScr + k];
+    } else {
+        uint nup, nall;
+        walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
+    }
     isort_u32(ln + b, e - b);
     const bool old_ok = (long long)ooff[n] <= cap;   // an overflowed old list carries nothing
     const uint ob = old_ok ? ooff[i] : 0u, oe = old_ok ? ooff[i + 1] : 0u;
@@ -746,26 +760,24 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     Planes3<double> P = planes<double>(c->pos[c->sbuf], np);
     GridC g = c->grid;
     DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
-    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount, (const Real*)c->rad,
+    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
                                                     c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
                                                     c->wslot, c->wlist, c->wcount);
     int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
     if (rc) return rc;
-    k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->cstart, c->ccount, P, (const Real*)c->rad, g, c->sid,
-                                                 c->skeyu, (R4<Real>*)c->sposu);
+    k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->arrival, c->cstart, c->ccount, P, (const Real*)c->rad,
+                                                 g, c->sid, c->skeyu, (R4<Real>*)c->sposu);
     k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->cstart, c->sid, c->skeyu, (const R4<Real>*)c->sposu, c->sid2,
                                               c->skey, (R4<Real>*)c->spos);
     const Real skin = (Real)c->cfg.skin;
-    k_nbr_count<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin,
-                                                   c->njgi, c->njli, c->words);
-    rc = exclusive_scan_u32(c->njgi, c->off[dst], n, c->off[dst] + n, c->scan_tmp, s);
-    if (rc) return rc;
-    rc = exclusive_scan_u32(c->njli, c->roff, n, c->roff + n, c->scan_tmp, s);
+    k_nbr_walk<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin,
+                                                  c->njgi, c->njli, c->scr, c->words);
+    rc = exclusive_scan2_u32(c->njgi, c->off[dst], c->off[dst] + n, c->njli, c->roff, c->roff + n, n, c->scan_tmp, s);
     if (rc) return rc;
     k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
         n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
         c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
-        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry);
+        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry, c->scr);
     k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->ru, c->off[dst], c->cap);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
@@ -958,7 +970,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
         (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->ru, cap)) || (rc = dalloc(&c->words, 1)) ||
         (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
-        (rc = dalloc(&c->wcount, 1)))
+        (rc = dalloc(&c->wcount, 1)) || (rc = dalloc(&c->arrival, np)) || (rc = dalloc(&c->scr, np * kScr)))
         return bail(rc);
     e = cudaMalloc(&c->wf, 2 * np * 4 * rs);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (wall forces)", __FILE__, __LINE__));
@@ -986,7 +998,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->nblk)) ||
         (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->nblk)))
         return bail(rc);
-    c->scan_words = scan_scratch_words(std::max<long long>(np + 1, 1));
+    c->scan_words = 2 * scan_scratch_words(std::max<long long>(np + 1, 1));
     if ((rc = dalloc(&c->scan_tmp, c->scan_words))) return bail(rc);
     e = cudaMemset(c->words, 0, sizeof(EngineWords));
     if (e == cudaSuccess) e = cudaMemset(c->off[0], 0, (np + 1) * sizeof(uint));
@@ -1015,7 +1027,8 @@ int dem_destroy(dem_ctx* c) {
                     c->staging, c->key, c->sid, c->sid2, c->spos, c->skeyu, c->skey, c->sposu, c->njgi, c->njli,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
-                    c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf};
+                    c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
+                    c->scr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);

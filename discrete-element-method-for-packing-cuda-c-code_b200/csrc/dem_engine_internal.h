@@ -80,6 +80,8 @@ struct dem_ctx {
     uint* cstart = nullptr;
     uint* njgi = nullptr;
     uint* njli = nullptr;
+    uint* arrival = nullptr; // per particle: slot among its cell's members (hash order)
+    uint* scr = nullptr;     // per sorted slot: the walk's first kScr row candidates
     uint* off[2] = {nullptr, nullptr};
     uint* roff = nullptr;
     uint* ln[2] = {nullptr, nullptr};

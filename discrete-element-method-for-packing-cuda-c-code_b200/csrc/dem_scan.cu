@@ -1,7 +1,9 @@
 // dem_scan.cu -- device-wide exclusive prefix sum of uint32 (cell counts,
 // per-particle pair counts, radix digit histograms).  Three launches:
-// tile reduce -> scan of tile sums (one CTA) -> tile scan + offset.  256
-// threads x 16 items per tile; items are loaded as uint4 when aligned.
+// tile reduce -> scan of tile sums (one CTA per array) -> tile scan + offset.
+// 256 threads x 16 items per tile; items are loaded as uint4 when aligned.
+// Up to two arrays of the same length are scanned by the same three launches
+// (blockIdx.y selects the array).
 #include "dem_common.cuh"
 
 namespace dem {
@@ -55,22 +57,30 @@ __device__ __forceinline__ void load_items(const uint* in, long long n, long lon
     }
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_tile_reduce(const uint* __restrict__ in, long long n,
-                                                              uint* __restrict__ sums) {
+struct ScanSet {
+    const uint* in[2];
+    uint* out[2];
+    uint* total[2];
+    uint* sums[2];
+};
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_reduce(ScanSet a, long long n) {
     __shared__ uint sw[kScanThreads / 32 + 1];
+    const int y = blockIdx.y;
     uint it[kScanItems];
-    load_items(in, n, (long long)blockIdx.x * kScanTile, it);
+    load_items(a.in[y], n, (long long)blockIdx.x * kScanTile, it);
     uint s = 0;
 #pragma unroll
     for (int q = 0; q < kScanItems; q++) s += it[q];
     uint tot;
     block_excl_scan(s, sw, tot);
-    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+    if (threadIdx.x == 0) a.sums[y][blockIdx.x] = tot;
 }
 
-// One CTA scans the tile sums in chunks of 256.
-__global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint* sums, long long nt, uint* total) {
+// One CTA per array scans its tile sums in chunks of 256.
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(ScanSet a, long long nt) {
     __shared__ uint sw[kScanThreads / 32 + 1];
+    uint* sums = a.sums[blockIdx.y];
     uint carry = 0;
     for (long long base = 0; base < nt; base += kScanThreads) {
         long long i = base + threadIdx.x;
@@ -80,12 +90,14 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint* sums, long lon
         if (i < nt) sums[i] = e + carry;
         carry += tot;
     }
-    if (threadIdx.x == 0 && total) *total = carry;
+    if (threadIdx.x == 0 && a.total[blockIdx.y]) *a.total[blockIdx.y] = carry;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint* in, uint* out,
-                                                            long long n, const uint* __restrict__ sums) {
+__global__ void __launch_bounds__(kScanThreads) k_tile_scan(ScanSet a, long long n) {
     __shared__ uint sw[kScanThreads / 32 + 1];
+    const int y = blockIdx.y;
+    const uint* in = a.in[y];
+    uint* out = a.out[y];
     uint it[kScanItems];
     const long long base = (long long)blockIdx.x * kScanTile;
     load_items(in, n, base, it);
@@ -93,7 +105,7 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint* in, uint
 #pragma unroll
     for (int q = 0; q < kScanItems; q++) s += it[q];
     uint tot;
-    uint run = block_excl_scan(s, sw, tot) + sums[blockIdx.x];
+    uint run = block_excl_scan(s, sw, tot) + a.sums[y][blockIdx.x];
     const long long b = base + (long long)threadIdx.x * kScanItems;
     uint o[kScanItems];
 #pragma unroll
@@ -108,6 +120,15 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint* in, uint
             if (b + q < n) out[b + q] = o[q];
     }
 }
+
+int scan_set(ScanSet a, int narr, long long n, cudaStream_t s) {
+    const long long nt = (n + kScanTile - 1) / kScanTile;
+    k_tile_reduce<<<dim3((unsigned)nt, narr), kScanThreads, 0, s>>>(a, n);
+    k_scan_sums<<<dim3(1, narr), kScanThreads, 0, s>>>(a, nt);
+    k_tile_scan<<<dim3((unsigned)nt, narr), kScanThreads, 0, s>>>(a, n);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
 }  // namespace
 
 size_t scan_scratch_words(long long n) {
@@ -120,12 +141,19 @@ int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint
         if (total) DEM_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(uint), s));
         return DEM_OK;
     }
-    long long nt = (n + kScanTile - 1) / kScanTile;
-    k_tile_reduce<<<(unsigned)nt, kScanThreads, 0, s>>>(in, n, tmp);
-    k_scan_sums<<<1, kScanThreads, 0, s>>>(tmp, nt, total);
-    k_tile_scan<<<(unsigned)nt, kScanThreads, 0, s>>>(in, out, n, tmp);
-    DEM_LAUNCH_CHECK();
-    return DEM_OK;
+    ScanSet a = {{in, nullptr}, {out, nullptr}, {total, nullptr}, {tmp, nullptr}};
+    return scan_set(a, 1, n, s);
+}
+
+int exclusive_scan2_u32(const uint* in0, uint* out0, uint* total0, const uint* in1, uint* out1, uint* total1,
+                        long long n, uint* tmp, cudaStream_t s) {
+    if (n <= 0) {
+        if (total0) DEM_CUDA_TRY(cudaMemsetAsync(total0, 0, sizeof(uint), s));
+        if (total1) DEM_CUDA_TRY(cudaMemsetAsync(total1, 0, sizeof(uint), s));
+        return DEM_OK;
+    }
+    ScanSet a = {{in0, in1}, {out0, out1}, {total0, total1}, {tmp, tmp + scan_scratch_words(n)}};
+    return scan_set(a, 2, n, s);
 }
 
 }  // namespace dem

@@ -161,6 +161,8 @@ _SIGS = [
     ("dem_grid_info", ctypes.c_int, [_vp, _c_uint_p, _c_double_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("dem_set_profiling", ctypes.c_int, [_vp, ctypes.c_int]),
     ("dem_kernel_times", ctypes.c_int, [_vp, _c_double_p]),
+    ("dem_set_window_timing", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("dem_window_kernel_times", ctypes.c_int, [_vp, _c_double_p]),
     ("dem_adjoint_window", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(AdjointResult), _vp]),
     ("dem_adjoint_release", ctypes.c_int, [_vp]),
@@ -483,6 +485,14 @@ class Engine:
     def kernel_times(self):
         out = (ctypes.c_double * 3)()
         check(lib().dem_kernel_times(self._h, out), "dem_kernel_times")
+        return {"relist_ms": out[0], "pair_ms": out[1], "particle_ms": out[2]}
+
+    def set_window_timing(self, on=True):
+        check(lib().dem_set_window_timing(self._h, 1 if on else 0), "dem_set_window_timing")
+
+    def window_kernel_times(self):
+        out = (ctypes.c_double * 3)()
+        check(lib().dem_window_kernel_times(self._h, out), "dem_window_kernel_times")
         return {"relist_ms": out[0], "pair_ms": out[1], "particle_ms": out[2]}
 
 

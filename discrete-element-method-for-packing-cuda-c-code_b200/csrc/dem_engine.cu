@@ -725,7 +725,11 @@ void free_graphs(dem_ctx* c) {
     for (int a = 0; a < 2; a++)
         for (int b = 0; b < 2; b++)
             for (int h = 0; h < 2; h++)
-                if (c->gexec[a][b][h]) { cudaGraphExecDestroy(c->gexec[a][b][h]); c->gexec[a][b][h] = nullptr; }
+                for (int t = 0; t < 2; t++)
+                    if (c->gexec[a][b][h][t]) {
+                        cudaGraphExecDestroy(c->gexec[a][b][h][t]);
+                        c->gexec[a][b][h][t] = nullptr;
+                    }
 }
 
 void free_cells(dem_ctx* c) {
@@ -848,7 +852,9 @@ int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part
     int rc;
     const bool mixed = c->prec == DEM_PREC_MIXED;
     if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+    const bool wt = c->wtiming_capture;
     if (c->mode == DEM_FORCE_PP) {
+        if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2 + 2 * slot], c->stream, cudaEventRecordExternal));
         rc = mixed ? launch_pp<float>(c, lst, slot, c->sbuf, c->hph) : launch_pp<double>(c, lst, slot, c->sbuf, c->hph);
         if (rc) return rc;
         if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
@@ -858,9 +864,11 @@ int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part
         rc = mixed ? launch_pair<float>(c, lst, slot) : launch_pair<double>(c, lst, slot);
         if (rc) return rc;
         if (c->profiling) DEM_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+        if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2 + 2 * slot], c->stream, cudaEventRecordExternal));
         rc = mixed ? launch_particle<float>(c, lst, slot) : launch_particle<double>(c, lst, slot);
         if (rc) return rc;
     }
+    if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[3 + 2 * slot], c->stream, cudaEventRecordExternal));
     if (c->profiling) {
         DEM_CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
         float a = 0.f, b = 0.f;
@@ -879,8 +887,10 @@ namespace {
 // Enqueue one full window (re-list from list `src`, then K steps).
 int enqueue_window(dem_ctx* c, int src) {
     const int K = c->cfg.relist_interval;
+    if (c->wtiming_capture) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[0], c->stream, cudaEventRecordExternal));
     int rc = relist(c, src);
     if (rc) return rc;
+    if (c->wtiming_capture) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[1], c->stream, cudaEventRecordExternal));
     c->hph = 0;
     const int lst = 1 - src;
     c->observe_slot = K - 1;
@@ -895,11 +905,14 @@ int enqueue_window(dem_ctx* c, int src) {
 // Capture (once) and launch the window graph for the current buffers.
 int launch_window_graph(dem_ctx* c) {
     const int src = c->cur, sb = c->sbuf, hp = c->hph;
-    cudaGraphExec_t& ge = c->gexec[src][sb][hp];
+    const int tm = c->wtiming ? 1 : 0;
+    cudaGraphExec_t& ge = c->gexec[src][sb][hp][tm];
     if (!ge) {
         cudaGraph_t g = nullptr;
         DEM_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->wtiming_capture = tm != 0;
         int rc = enqueue_window(c, src);
+        c->wtiming_capture = false;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         // capture only records: restore the indices, the launch below advances them
         c->sbuf = sb;
@@ -911,6 +924,7 @@ int launch_window_graph(dem_ctx* c) {
         if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
     }
     DEM_CUDA_TRY(cudaGraphLaunch(ge, c->stream));
+    if (tm) c->wtiming_ran = true;
     const int K = c->cfg.relist_interval;
     c->hph = 0;
     if (c->mode == DEM_FORCE_PP) {
@@ -1035,6 +1049,7 @@ int dem_destroy(dem_ctx* c) {
     for (int k = 0; k < 4; k++)
         if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->ext_ready) cudaEventDestroy(c->ext_ready);
+    for (cudaEvent_t e : c->wev) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return DEM_OK;
@@ -1412,6 +1427,39 @@ int dem_set_profiling(dem_ctx* c, int on) {
 int dem_kernel_times(dem_ctx* c, double out[3]) {
     if (!c || !out) return fail(DEM_ERR_ARG, "dem_kernel_times: null argument");
     for (int k = 0; k < 3; k++) out[k] = c->kcount[k] ? c->ktime[k] / c->kcount[k] : 0.0;
+    return DEM_OK;
+}
+
+int dem_set_window_timing(dem_ctx* c, int on) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_set_window_timing: null ctx");
+    const size_t need = 2 + 2 * (size_t)c->cfg.relist_interval;
+    if (on && c->wev.size() < need) {
+        for (size_t k = c->wev.size(); k < need; k++) {
+            cudaEvent_t e = nullptr;
+            DEM_CUDA_TRY(cudaEventCreate(&e));
+            c->wev.push_back(e);
+        }
+    }
+    c->wtiming = on != 0;
+    return DEM_OK;
+}
+
+int dem_window_kernel_times(dem_ctx* c, double out[3]) {
+    if (!c || !out) return fail(DEM_ERR_ARG, "dem_window_kernel_times: null argument");
+    out[0] = out[1] = out[2] = 0.0;
+    if (!c->wtiming_ran) return fail(DEM_ERR_STATE, "dem_window_kernel_times: no timed window has run");
+    const int K = c->cfg.relist_interval;
+    DEM_CUDA_TRY(cudaEventSynchronize(c->wev[3 + 2 * (K - 1)]));
+    float ms = 0.f;
+    DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[0], c->wev[1]));
+    out[0] = ms;
+    for (int s = 0; s < K; s++) {
+        cudaEvent_t prev = s == 0 ? c->wev[1] : c->wev[3 + 2 * (s - 1)];
+        DEM_CUDA_TRY(cudaEventElapsedTime(&ms, prev, c->wev[2 + 2 * s]));
+        out[1] += ms / K;
+        DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[2 + 2 * s], c->wev[3 + 2 * s]));
+        out[2] += ms / K;
+    }
     return DEM_OK;
 }
 

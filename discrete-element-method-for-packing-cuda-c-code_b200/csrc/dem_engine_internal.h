@@ -1,6 +1,7 @@
 // dem_engine_internal.h -- the engine context and the launchers shared by
 // dem_engine.cu (forward step) and dem_adjoint.cu (its reverse mode).
 #pragma once
+#include <vector>
 #include "dem_common.cuh"
 #include "dem_law.cuh"
 
@@ -121,8 +122,16 @@ struct dem_ctx {
     int last_slot = -1;
     int observe_slot = -1;   // window slot whose step writes the observables
     bool uploaded = false;
-    // window graphs keyed by (previous list buffer, state buffer, history phase)
-    cudaGraphExec_t gexec[2][2][2] = {};
+    // window graphs keyed by (previous list buffer, state buffer, history
+    // phase, with timing events)
+    cudaGraphExec_t gexec[2][2][2][2] = {};
+    // timing events inside window graphs: [0] window start, [1] after the
+    // re-list, [2 + 2s] after the pair launch of slot s, [3 + 2s] after its
+    // particle launch
+    bool wtiming = false;
+    bool wtiming_capture = false;
+    bool wtiming_ran = false;
+    std::vector<cudaEvent_t> wev;
     // profiling
     bool profiling = false;
     double ktime[3] = {0, 0, 0};

@@ -279,6 +279,14 @@ int dem_grid_info(dem_ctx* ctx, unsigned int grid[3], double* cell, long long* n
  * dem_set_profiling(ctx,1); adds events, so off for timing runs. */
 int dem_set_profiling(dem_ctx* ctx, int on);
 int dem_kernel_times(dem_ctx* ctx, double out[3]);
+/* Event timing inside the window graphs: while on, whole windows replay a
+ * second graph that also records CUDA events around the re-list and every
+ * pair / particle launch (plain windows carry no event nodes).
+ * dem_window_kernel_times gives the mean times (ms) of the last such window:
+ * out[0]=re-list, out[1]=pair force per step, out[2]=particle update per step
+ * (PP mode: out[1] ~ 0, out[2] the fused step). */
+int dem_set_window_timing(dem_ctx* ctx, int on);
+int dem_window_kernel_times(dem_ctx* ctx, double out[3]);
 
 /* ---------------------------------------------------------------- adjoint --
  * Reverse mode of the step (force + walls + integrator) over a window; no

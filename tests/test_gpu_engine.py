@@ -254,6 +254,38 @@ def test_partial_windows_equal_graph_windows(dem, wl, cuda):
     np.testing.assert_array_equal(aa, ab)
 
 
+def test_window_timing_graphs_equal_plain_graphs(dem, wl, cuda):
+    """Windows replayed from the graph variant with timing events give the
+    same state bit for bit, and per-kernel times of the last timed window."""
+    w = wl.small_box(n=3000)
+    a = make_engine(dem, w)
+    b = make_engine(dem, w)
+    K = w.relist_interval
+    a.step(3 * K)
+    b.step(K)
+    b.set_window_timing(True)
+    b.step(K)
+    b.set_window_timing(False)
+    b.step(K)
+    kt = b.window_kernel_times()
+    assert kt["relist_ms"] > 0 and kt["pair_ms"] > 0 and kt["particle_ms"] > 0, kt
+    for x, y in zip(a.download(), b.download()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_plain_launches_equal_programmatic_launches(dem, wl, cuda, monkeypatch):
+    """Step kernels launched programmatically inside a window (the default)
+    and launched plainly (DEM_B200_PDL=0) agree bit for bit."""
+    w = wl.small_box(n=3000)
+    a = make_engine(dem, w)
+    monkeypatch.setenv("DEM_B200_PDL", "0")
+    b = make_engine(dem, w)
+    a.step(45)
+    b.step(45)
+    for x, y in zip(a.download(), b.download()):
+        np.testing.assert_array_equal(x, y)
+
+
 def test_device_upload_download_roundtrip(dem, wl, cuda):
     torch = cuda
     w = wl.small_box(n=2000)

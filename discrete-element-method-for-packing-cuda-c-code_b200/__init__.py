@@ -24,7 +24,7 @@ PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libdem_b200.so"
 
 DEM_OK, DEM_ERR_ARG, DEM_ERR_CUDA, DEM_ERR_CAPACITY = 0, 1, 2, 3
-DEM_ERR_NONFINITE, DEM_ERR_SKIN, DEM_ERR_IO, DEM_ERR_STATE = 4, 5, 6, 7
+DEM_ERR_NONFINITE, DEM_ERR_SKIN, DEM_ERR_IO, DEM_ERR_STATE, DEM_ERR_TIMEOUT = 4, 5, 6, 7, 8
 PREC_FP64, PREC_MIXED = 0, 1
 OBJ_PACKING, OBJ_POTENTIAL = 0, 1
 FORCE_PCCP, FORCE_PP = 0, 1
@@ -491,9 +491,10 @@ class Engine:
         check(lib().dem_set_window_timing(self._h, 1 if on else 0), "dem_set_window_timing")
 
     def window_kernel_times(self):
-        out = (ctypes.c_double * 3)()
+        out = (ctypes.c_double * 5)()
         check(lib().dem_window_kernel_times(self._h, out), "dem_window_kernel_times")
-        return {"relist_ms": out[0], "pair_ms": out[1], "particle_ms": out[2]}
+        return {"relist_ms": out[0], "pair_ms": out[1], "particle_ms": out[2], "free_window_ms": out[3],
+                "window_kernel_ms": out[4]}
 
 
 # ------------------------------------------------------------ host helpers

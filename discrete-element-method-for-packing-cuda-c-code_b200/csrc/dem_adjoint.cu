@@ -90,7 +90,7 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
             (rc = dalloc(&w->Wb, 3 * np)) || (rc = dalloc(&w->Fb, 3 * np)) || (rc = dalloc(&w->Tb, 3 * np)) ||
             (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
             (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) || (rc = dalloc(&w->zmax, 2)) ||
-            (rc = dalloc(&w->save_mz, c->nblk)) || (rc = dalloc(&w->save_cnt, c->nblk)))
+            (rc = dalloc(&w->save_mz, c->npart)) || (rc = dalloc(&w->save_cnt, c->npart)))
             return rc;
         w->npb = grid_for(c->n, kPairB);
     }
@@ -551,9 +551,9 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
         if ((rc = dem_step_n(c, every))) return rc;
     }
     if ((rc = save_ck(c, w->ck[nseg]))) return rc;
-    const size_t last = (size_t)(K - 1) * c->nblk;
-    if ((rc = copy(w->save_mz, c->part_mz + last, c->nblk * sizeof(unsigned long long), s)) ||
-        (rc = copy(w->save_cnt, c->part_cnt + last, c->nblk * sizeof(uint), s)))
+    const size_t last = (size_t)(K - 1) * c->npart;
+    if ((rc = copy(w->save_mz, c->part_mz + last, c->npart * sizeof(unsigned long long), s)) ||
+        (rc = copy(w->save_cnt, c->part_cnt + last, c->npart * sizeof(uint), s)))
         return rc;
     DEM_CUDA_TRY(cudaEventRecord(c->ev[1], s));
     // --------------------------------------------------------------- objective
@@ -655,8 +655,8 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     out->adjoint_ms = f2;
     // leave the context at the end of the window, as dem_step_n(nsteps) would
     if ((rc = restore_ck(c, w->ck[nseg]))) return rc;
-    if ((rc = copy(c->part_mz + last, w->save_mz, c->nblk * sizeof(unsigned long long), s)) ||
-        (rc = copy(c->part_cnt + last, w->save_cnt, c->nblk * sizeof(uint), s)))
+    if ((rc = copy(c->part_mz + last, w->save_mz, c->npart * sizeof(unsigned long long), s)) ||
+        (rc = copy(c->part_cnt + last, w->save_cnt, c->npart * sizeof(uint), s)))
         return rc;
     dem_record_forces(c, rec0 ? 1 : 0);
     DEM_CUDA_TRY(cudaStreamSynchronize(s));

@@ -88,9 +88,9 @@ cudaError_t launch_ex(void (*kernel)(KArgs...), unsigned grid, unsigned block, c
 // out may alias in.  Scratch: tmp with scan_scratch_words(n) uint32.
 size_t scan_scratch_words(long long n);
 int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s);
-// Two arrays of length n in the same three launches; tmp holds
-// 2 * scan_scratch_words(n) uint32.  Outputs may alias their inputs.
-int exclusive_scan2_u32(const uint* in0, uint* out0, uint* total0, const uint* in1, uint* out1, uint* total1,
-                        long long n, uint* tmp, cudaStream_t s);
+// Up to three arrays of length n in the same three launches; tmp holds
+// narr * scan_scratch_words(n) uint32.  Outputs may alias their inputs.
+int exclusive_scan_multi_u32(int narr, const uint* const* in, uint* const* out, uint* const* total, long long n,
+                             uint* tmp, cudaStream_t s);
 
 }  // namespace dem

@@ -229,13 +229,15 @@ __device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, 
 // The re-list walk: per sorted slot t, count the candidates j > i (row of i)
 // and j < i (reverse row of i) and keep the first kScr j > i candidates in
 // scr[t * kScr ...]; rows longer than kScr are walked again by the fill.
+// A particle with any candidate or a wall candidacy is BOUND for the window
+// (bflag = 1), otherwise FREE.
 constexpr uint kScr = 8;
 
 template <typename Real>
 __global__ void k_nbr_walk(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
                            const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
-                           uint* __restrict__ njgi, uint* __restrict__ njli, uint* __restrict__ scr,
-                           EngineWords* words) {
+                           const uint* __restrict__ wslot, uint* __restrict__ njgi, uint* __restrict__ njli,
+                           uint* __restrict__ bflag, uint* __restrict__ scr, EngineWords* words) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     uint nall = 0;
     if (t < n) {
@@ -245,6 +247,7 @@ __global__ void k_nbr_walk(long long n, const uint* __restrict__ sid2, const R4<
                            kScr);
         njgi[i] = nup;
         njli[i] = nall - nup;
+        bflag[i] = (nall > 0 || wslot[i] != kEmpty) ? 1u : 0u;
     }
     nall = __reduce_max_sync(0xffffffffu, nall);
     if (lane_id() == 0 && nall) atomicMax(&words->max_row, nall);
@@ -268,9 +271,15 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
                            uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
                            const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
                            uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
-                           uint* __restrict__ carry, const uint* __restrict__ scr) {
+                           uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,
+                           const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
+    {   // bound / free lists, ascending particle id
+        const uint i = sid2[t], b = bpos[i];
+        if (bflag[i]) blist[b] = i;
+        else flist[i - b] = i;
+    }
     const uint total = off[n];
     if ((long long)total > cap) {
         if (t == 0) atomicOr(&words->status, kStCapacity);
@@ -363,96 +372,172 @@ __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double
     return 1;
 }
 
-// PCCP pair kernel (calculateforcepairD's role, neiglist.cu:156-233, and
-// calforceiw's, neiglist.cu:287-301).  One item space: items [0, nw) are the
-// window's wall candidates, items [nw, nw + P) the listed pairs, so every
-// thread of the one-wave grid takes at most one item per pass.
-//   wall item c:  history W in place (zero when not touching); wall force and
-//                 torque in wf[2c], wf[2c+1]
-//   pair item k:  history H[k] in place; force/torque on lo in pf[k]/pti[k]
-//                 (row slot k), force/torque on hi in rfj[u]/rtj[u] at the
-//                 pair's reverse-row slot u = ru[k], so the gather reads both
-//                 of a sphere's row ranges directly.  .w = 1 marks a contact.
+// Arguments of the PCCP step kernels (pair items, bound particles, free
+// particles) and of the window kernel that runs all of a window's steps.
+template <typename Real> struct StepArgs {
+    long long n, cap;
+    const uint *off, *lp, *ln, *ru, *roff, *wlist, *wcount, *wslot, *bpos, *blist, *flist;
+    Planes3<double> P, D, W, H;   // position, displacement, wall history, pair history (in place)
+    Planes3<Real> A;              // rotation
+    const Real* R;
+    float4* Q;                    // displacement since the list (xyz), wall flag (w)
+    R4<Real> *pf, *pti, *rfj, *rtj, *wf;
+    LawParams<Real> pp, pw;
+    ParticleCommon pc;
+    Real dtr, inv_dt, density;
+    EngineWords* words;
+    double *dbgF, *dbgT;
+    uint* dbgC;
+};
+
+// Loads of data that other blocks of the same launch write (the window
+// kernel): L2-coherent (.cg), never through the non-coherent or L1 paths.
+template <bool COH, typename T> __device__ __forceinline__ T ldx(const T* p) {
+    if constexpr (COH) return __ldcg(p);
+    else return *p;
+}
+template <bool COH> __device__ __forceinline__ R4<float> ld4(const R4<float>* p) {
+    float4 v = COH ? __ldcg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+    return R4<float>{v.x, v.y, v.z, v.w};
+}
+template <bool COH> __device__ __forceinline__ R4<double> ld4(const R4<double>* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 u = COH ? __ldcg(q) : q[0], v = COH ? __ldcg(q + 1) : q[1];
+    return R4<double>{u.x, u.y, v.x, v.y};
+}
+template <bool COH, typename T> __device__ __forceinline__ V3<T> ld3p(Planes3<T> p, uint i) {
+    return mk(ldx<COH>(p.x + i), ldx<COH>(p.y + i), ldx<COH>(p.z + i));
+}
+
+// Wall item c of particle i (calforceiw's role, neiglist.cu:287-301): history
+// W in place (zero when not touching), wall force and torque in wf[2c],
+// wf[2c+1].
+template <typename Real, bool COH>
+__device__ __forceinline__ void wall_item(const StepArgs<Real>& a, long long c, uint i) {
+    const Real r = a.R[i];
+    const Real m = a.density * (Real)8 * r * r * r;
+    V3<double> h = ld3p<COH>(a.W, i);
+    V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
+    const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, ld3p<COH>(a.P, i), cvt<Real>(ld3p<COH>(a.D, i)),
+                                        ld3p<COH>(a.A, i), r, m, h, a.inv_dt, a.pw, Fw, Tw, (Real*)nullptr);
+    a.W.x[i] = h.x; a.W.y[i] = h.y; a.W.z[i] = h.z;
+    R4<Real> a4, b4;
+    a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
+    b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
+    a.wf[2 * c] = a4;
+    a.wf[2 * c + 1] = b4;
+}
+
+// Pair item k = (lo i, hi j) (calculateforcepairD's role, neiglist.cu:156-233):
+// history H[k] in place; force/torque on lo in pf[k]/pti[k] (row slot k),
+// force/torque on hi in rfj[u]/rtj[u] at the pair's reverse-row slot
+// u = ru[k], so the gather reads both of a sphere's row ranges directly.
+// .w = 1 marks a contact.
+template <typename Real, bool COH>
+__device__ __forceinline__ void pair_item(const StepArgs<Real>& a, long long k, uint i, uint j, uint rslot) {
+    V3<double> h = mk(ldx<COH>(a.H.x + k), ldx<COH>(a.H.y + k), ldx<COH>(a.H.z + k));
+    V3<Real> Fi, Ti, Tj;
+    const int c = pair_eval<Real>(ld3p<COH>(a.P, i), ld3p<COH>(a.P, j), ld3p<COH>(a.D, i), ld3p<COH>(a.D, j),
+                                  ld3p<COH>(a.A, i), ld3p<COH>(a.A, j), a.R[i], a.R[j], h, a.pp, a.inv_dt, a.density,
+                                  Fi, Ti, Tj);
+    a.H.x[k] = h.x; a.H.y[k] = h.y; a.H.z[k] = h.z;
+    R4<Real> fo, fr;
+    if (c) {
+        fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
+        fr.x = -Fi.x; fr.y = -Fi.y; fr.z = -Fi.z; fr.w = (Real)1;
+        R4<Real> a4, b4;
+        a4.x = Ti.x; a4.y = Ti.y; a4.z = Ti.z; a4.w = (Real)0;
+        b4.x = Tj.x; b4.y = Tj.y; b4.z = Tj.z; b4.w = (Real)0;
+        a.pti[k] = a4;
+        a.rtj[rslot] = b4;
+    } else {
+        fo.x = fo.y = fo.z = fo.w = (Real)0;
+        fr = fo;
+    }
+    a.pf[k] = fo;
+    a.rfj[rslot] = fr;
+}
+
+// Indices of item u: items [0, nw) are the window's wall candidates, items
+// [nw, nw + P) the listed pairs.
 template <typename Real>
-__global__ void __launch_bounds__(256) k_pair(const uint* __restrict__ off, long long n, long long cap,
-                                              const uint* __restrict__ lp, const uint* __restrict__ ln,
-                                              const uint* __restrict__ ru, Planes3<double> P, Planes3<double> D,
-                                              Planes3<Real> A, const Real* __restrict__ R, Planes3<double> H,
-                                              LawParams<Real> pp, Real inv_dt, Real density,
-                                              R4<Real>* __restrict__ pf, R4<Real>* __restrict__ pti,
-                                              R4<Real>* __restrict__ rfj, R4<Real>* __restrict__ rtj,
-                                              const uint* __restrict__ wlist, const uint* __restrict__ wcount,
-                                              Planes3<double> W, LawParams<Real> pw, double hx, double hy,
-                                              R4<Real>* __restrict__ wf) {
+__device__ __forceinline__ void item_indices(const StepArgs<Real>& a, long long u, uint nw, long long items, uint& i,
+                                             uint& j, uint& rslot) {
+    if (u < (long long)nw) {
+        i = a.wlist[u];
+    } else if (u < items) {
+        const long long k = u - nw;
+        i = a.lp[k]; j = a.ln[k]; rslot = a.ru[k];
+    }
+}
+
+// PCCP pair kernel: wall candidates and listed pairs as one item space on a
+// one-wave grid (grid-stride), so every thread takes at most one item per
+// pass.
+template <typename Real>
+__global__ void __launch_bounds__(256) k_pair(StepArgs<Real> a) {
     pdl_trigger();
     const long long stride = (long long)gridDim.x * blockDim.x;
     // list-time data (written by the re-list): safe before pdl_wait
-    const uint nw = *wcount;
-    const uint total = off[n];
-    const long long items = (long long)nw + ((long long)total <= cap ? (long long)total : 0ll);
+    const uint nw = *a.wcount;
+    const uint total = a.off[a.n];
+    const long long items = (long long)nw + ((long long)total <= a.cap ? (long long)total : 0ll);
     long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     uint i = 0, j = 0, rslot = 0;
-    if (u < (long long)nw) {
-        i = wlist[u];
-    } else if (u < items) {
-        const long long k = u - nw;
-        i = lp[k]; j = ln[k]; rslot = ru[k];
-    }
+    item_indices(a, u, nw, items, i, j, rslot);
     pdl_wait();
     for (; u < items; u += stride) {
-        if (u < (long long)nw) {
-            const Real r = R[i];
-            const Real m = density * (Real)8 * r * r * r;
-            V3<double> h = mk(W.x[i], W.y[i], W.z[i]);
-            V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
-            const int hit = wall_contacts<Real>(hx, hy, mk(P.x[i], P.y[i], P.z[i]),
-                                                cvt<Real>(mk(D.x[i], D.y[i], D.z[i])), mk(A.x[i], A.y[i], A.z[i]), r,
-                                                m, h, inv_dt, pw, Fw, Tw, (Real*)nullptr);
-            W.x[i] = h.x; W.y[i] = h.y; W.z[i] = h.z;
-            R4<Real> a4, b4;
-            a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
-            b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
-            wf[2 * u] = a4;
-            wf[2 * u + 1] = b4;
-        } else {
-            const long long k = u - nw;
-            V3<double> h = mk(H.x[k], H.y[k], H.z[k]);
-            V3<Real> Fi, Ti, Tj;
-            const int c = pair_eval<Real>(mk(P.x[i], P.y[i], P.z[i]), mk(P.x[j], P.y[j], P.z[j]),
-                                          mk(D.x[i], D.y[i], D.z[i]), mk(D.x[j], D.y[j], D.z[j]),
-                                          mk(A.x[i], A.y[i], A.z[i]), mk(A.x[j], A.y[j], A.z[j]), R[i], R[j], h,
-                                          pp, inv_dt, density, Fi, Ti, Tj);
-            H.x[k] = h.x; H.y[k] = h.y; H.z[k] = h.z;
-            R4<Real> fo, fr;
-            if (c) {
-                fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
-                fr.x = -Fi.x; fr.y = -Fi.y; fr.z = -Fi.z; fr.w = (Real)1;
-                R4<Real> a4, b4;
-                a4.x = Ti.x; a4.y = Ti.y; a4.z = Ti.z; a4.w = (Real)0;
-                b4.x = Tj.x; b4.y = Tj.y; b4.z = Tj.z; b4.w = (Real)0;
-                pti[k] = a4;
-                rtj[rslot] = b4;
-            } else {
-                fo.x = fo.y = fo.z = fo.w = (Real)0;
-                fr = fo;
-            }
-            pf[k] = fo;
-            rfj[rslot] = fr;
-        }
-        // indices of this thread's next item (grid-stride pass)
-        const long long v = u + stride;
-        if (v < (long long)nw) {
-            i = wlist[v];
-        } else if (v < items) {
-            const long long k = v - nw;
-            i = lp[k]; j = ln[k]; rslot = ru[k];
-        }
+        if (u < (long long)nw) wall_item<Real, false>(a, u, i);
+        else pair_item<Real, false>(a, u - nw, i, j, rslot);
+        item_indices(a, u + stride, nw, items, i, j, rslot);
     }
 }
 
 // --------------------------------------------------- particle update
 // Per-step observables are written as one partial per block (no same-address
 // atomics in the hot kernels) and reduced on the host when asked for.
+
+// One step of the integrator for one particle, in registers (updatepositionD,
+// neiglist.cu:356-360: symplectic Euler in displacement form), then the
+// per-step checks.  Every operation is an explicitly rounded intrinsic, so
+// the per-step kernels and the free-particle window kernel give bit-identical
+// states.  FP64 form: the reference's F dt dt / m term by term; mixed form:
+// one reciprocal dt^2/m (FP64) and dt^2/I (FP32) per particle, fused
+// multiply-adds into the FP64 displacement and the FP32 rotation.
+template <typename Real>
+__device__ __forceinline__ void integrate(V3<Real> F, V3<Real> T, Real m, Real I, double dt, Real dtr,
+                                          float half_skin2, V3<double>& x, V3<double>& d, V3<Real>& a, float4& q,
+                                          uint& flags, double& mz) {
+    if constexpr (sizeof(Real) == 8) {
+        d.x = __dadd_rn(d.x, __ddiv_rn(__dmul_rn(__dmul_rn(F.x, dt), dt), m));
+        d.y = __dadd_rn(d.y, __ddiv_rn(__dmul_rn(__dmul_rn(F.y, dt), dt), m));
+        d.z = __dadd_rn(d.z, __ddiv_rn(__dmul_rn(__dmul_rn(F.z, dt), dt), m));
+        a.x = __dadd_rn(a.x, __ddiv_rn(__dmul_rn(__dmul_rn(T.x, dtr), dtr), I));
+        a.y = __dadd_rn(a.y, __ddiv_rn(__dmul_rn(__dmul_rn(T.y, dtr), dtr), I));
+        a.z = __dadd_rn(a.z, __ddiv_rn(__dmul_rn(__dmul_rn(T.z, dtr), dtr), I));
+    } else {
+        const double km = __ddiv_rn(__dmul_rn(dt, dt), (double)m);
+        const float kI = __fdiv_rn(__fmul_rn(dtr, dtr), I);
+        d.x = __fma_rn((double)F.x, km, d.x);
+        d.y = __fma_rn((double)F.y, km, d.y);
+        d.z = __fma_rn((double)F.z, km, d.z);
+        a.x = __fmaf_rn(T.x, kI, a.x);
+        a.y = __fmaf_rn(T.y, kI, a.y);
+        a.z = __fmaf_rn(T.z, kI, a.z);
+    }
+    x.x = __dadd_rn(x.x, d.x); x.y = __dadd_rn(x.y, d.y); x.z = __dadd_rn(x.z, d.z);
+    q.x = __fadd_rn(q.x, __double2float_rn(d.x));
+    q.y = __fadd_rn(q.y, __double2float_rn(d.y));
+    q.z = __fadd_rn(q.z, __double2float_rn(d.z));
+    const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
+    if (q2 > half_skin2) flags |= kStSkin;
+    if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
+    mz = x.z > 0.0 ? x.z : 0.0;
+}
+
+template <typename Real> __device__ __forceinline__ Real sphere_mass(Real density, Real r) {
+    return density * (Real)8 * r * r * r;
+}
 
 // Gravity + walls (calculateforceiwD, neiglist.cu:238-306) + integrator
 // (updatepositionD, neiglist.cu:308-409) for particle i whose pair sums are
@@ -464,7 +549,7 @@ __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real
                                                 Planes3<double> W, const LawParams<Real>& pw, const ParticleCommon& pc,
                                                 Real dtr, Real inv_dt, Real density, double& mz, uint& flags,
                                                 uint cnt, double* dbgF, double* dbgT, uint* dbgC) {
-    const Real m = density * (Real)8 * r * r * r;
+    const Real m = sphere_mass(density, r);
     const Real I = (Real)0.4 * m * (r * r);
     if (pc.first) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }   // displacement since the list (dempacking.cu:541)
     uint wflag = __float_as_uint(q.w);
@@ -486,37 +571,12 @@ __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real
         dbgT[3 * i] = T.x; dbgT[3 * i + 1] = T.y; dbgT[3 * i + 2] = T.z;
         dbgC[i] = cnt;
     }
-    // symplectic Euler in displacement form (neiglist.cu:356-360).  FP64 form:
-    // the reference's F dt dt / m term by term; mixed form: one reciprocal
-    // dt^2/m (FP64) and dt^2/I (FP32) per particle.
-    const double dt = pc.dt;
-    if (sizeof(Real) == 8) {
-        d.x = d.x + (double)F.x * dt * dt / (double)m;
-        d.y = d.y + (double)F.y * dt * dt / (double)m;
-        d.z = d.z + (double)F.z * dt * dt / (double)m;
-        a.x = a.x + T.x * dtr * dtr / I;
-        a.y = a.y + T.y * dtr * dtr / I;
-        a.z = a.z + T.z * dtr * dtr / I;
-    } else {
-        const double km = dt * dt / (double)m;
-        const Real kI = dtr * dtr / I;
-        d.x = d.x + (double)F.x * km;
-        d.y = d.y + (double)F.y * km;
-        d.z = d.z + (double)F.z * km;
-        a.x = a.x + T.x * kI;
-        a.y = a.y + T.y * kI;
-        a.z = a.z + T.z * kI;
-    }
-    x.x += d.x; x.y += d.y; x.z += d.z;
-    q.x += (float)d.x; q.y += (float)d.y; q.z += (float)d.z;
+    integrate<Real>(F, T, m, I, pc.dt, dtr, pc.half_skin2, x, d, a, q, flags, mz);
     q.w = __uint_as_float(wflag);
     Po.x[i] = x.x; Po.y[i] = x.y; Po.z[i] = x.z;
     Do.x[i] = d.x; Do.y[i] = d.y; Do.z[i] = d.z;
     Ao.x[i] = a.x; Ao.y[i] = a.y; Ao.z[i] = a.z;
     Q[i] = q;
-    if (q.x * q.x + q.y * q.y + q.z * q.z > pc.half_skin2) flags |= kStSkin;
-    if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
-    mz = x.z > 0.0 ? x.z : 0.0;
 }
 
 // Per-step observables: on the observed step (the last of a window, or of an
@@ -530,8 +590,8 @@ __device__ __forceinline__ void block_observables(double mz, uint cnt, uint flag
         if (flags && lane_id() == 0) atomicOr(&words->status, flags);
         return;
     }
-    __shared__ unsigned long long s_mz[8];
-    __shared__ uint s_cnt[8], s_fl[8];
+    __shared__ unsigned long long s_mz[32];   // one entry per warp, blocks of up to 1024 threads
+    __shared__ uint s_cnt[32], s_fl[32];
     unsigned long long mb = (unsigned long long)__double_as_longlong(mz);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -552,70 +612,251 @@ __device__ __forceinline__ void block_observables(double mz, uint cnt, uint flag
     }
 }
 
-// PCCP gather (sumallforceiD's role, through the CSR row and the reverse
-// row of the sphere, both read as contiguous ranges) + particle_finish, one
-// thread per particle.  State is updated in place.
+// Clears the partials [from, to) of an observed step that this kernel does
+// not write (they may hold another launch shape's partials).
+__device__ __forceinline__ void clear_partials(StepPartials part, size_t from, size_t to) {
+    if (threadIdx.x == 0)
+        for (size_t b = from + blockIdx.x; b < to; b += gridDim.x) {
+            part.maxhz_bits[b] = 0ull;
+            part.contacts[b] = 0u;
+        }
+}
+
+// Bound particle i (a listed pair or a wall candidacy this window): the PCCP
+// gather (sumallforceiD's role) through the CSR row and the reverse row of
+// the sphere, both read as contiguous ranges, gravity, the gathered wall
+// force, then particle_finish.  State is updated in place.
+template <typename Real, bool COH>
+__device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const ParticleCommon& pc, uint i, Real r, uint ws,
+                                           uint total, uint o0, uint o1, uint r0, uint r1, double& mz, uint& cnt,
+                                           uint& flags) {
+    const V3<double> x = ld3p<COH>(a.P, i);
+    const V3<double> d = ld3p<COH>(a.D, i);
+    const V3<Real> av = ld3p<COH>(a.A, i);
+    const float4 q = ldx<COH>(a.Q + i);
+    V3<Real> F = zero3<Real>(), T = zero3<Real>();
+    if ((long long)total <= a.cap) {
+        for (uint k = o0; k < o1; k++) {
+            const R4<Real> f = ld4<COH>(a.pf + k);
+            if (f.w != (Real)0) {
+                const R4<Real> tq = ld4<COH>(a.pti + k);
+                F.x += f.x; F.y += f.y; F.z += f.z;
+                T.x += tq.x; T.y += tq.y; T.z += tq.z;
+                cnt++;
+            }
+        }
+        for (uint u = r0; u < r1; u++) {
+            const R4<Real> f = ld4<COH>(a.rfj + u);
+            if (f.w != (Real)0) {
+                const R4<Real> tq = ld4<COH>(a.rtj + u);
+                F.x += f.x; F.y += f.y; F.z += f.z;
+                T.x += tq.x; T.y += tq.y; T.z += tq.z;
+                cnt++;
+            }
+        }
+    }
+    F.z += -sphere_mass(a.density, r);   // gravity, then the walls (calculateforceiwD's order)
+    if (ws != kEmpty) {
+        const R4<Real> fw = ld4<COH>(a.wf + 2 * ws), tw = ld4<COH>(a.wf + 2 * ws + 1);
+        F.x += fw.x; F.y += fw.y; F.z += fw.z;
+        T.x += tw.x; T.y += tw.y; T.z += tw.z;
+    }
+    particle_finish<Real, false>(i, F, T, r, x, d, av, q, a.P, a.D, a.A, a.Q, a.W, a.pw, pc, a.dtr, a.inv_dt,
+                                 a.density, mz, flags, cnt, a.dbgF, a.dbgT, a.dbgC);
+}
+
+// PCCP particle kernel: one thread per bound particle (blist[t], t < nB =
+// bpos[n]).
 template <typename Real>
-__global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(long long n, const uint* __restrict__ off,
-                                                  const uint* __restrict__ roff, long long cap,
-                                                  const R4<Real>* __restrict__ pf, const R4<Real>* __restrict__ pti,
-                                                  const R4<Real>* __restrict__ rfj, const R4<Real>* __restrict__ rtj,
-                                                  Planes3<double> P, Planes3<double> D, Planes3<Real> A,
-                                                  const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
-                                                  LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt,
-                                                  Real density, StepPartials part, EngineWords* words, double* dbgF,
-                                                  double* dbgT, uint* dbgC, const uint* __restrict__ wslot,
-                                                  const R4<Real>* __restrict__ wf) {
+__global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(StepArgs<Real> a, StepPartials part) {
     pdl_trigger();
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz = 0.0;
     uint cnt = 0, flags = 0;
     // list-time data and the radius: safe before pdl_wait
+    const bool live = t < (long long)a.bpos[a.n];
+    uint i = 0, ws = kEmpty, total = 0, o0 = 0, o1 = 0, r0 = 0, r1 = 0;
     Real r = (Real)0;
-    uint ws = kEmpty, total = 0, o0 = 0, o1 = 0, r0 = 0, r1 = 0;
-    if (i < n) {
-        r = R[i];
-        ws = wslot[i];
-        total = off[n];
-        o0 = off[i]; o1 = off[i + 1]; r0 = roff[i]; r1 = roff[i + 1];
+    if (live) {
+        i = a.blist[t];
+        r = a.R[i];
+        ws = a.wslot[i];
+        total = a.off[a.n];
+        o0 = a.off[i]; o1 = a.off[i + 1]; r0 = a.roff[i]; r1 = a.roff[i + 1];
     }
     pdl_wait();
-    if (i < n) {
-        const V3<double> x = mk(P.x[i], P.y[i], P.z[i]);
-        const V3<double> d = mk(D.x[i], D.y[i], D.z[i]);
-        const V3<Real> a = mk(A.x[i], A.y[i], A.z[i]);
-        const float4 q = Q[i];
+    if (live) bound_item<Real, false>(a, a.pc, i, r, ws, total, o0, o1, r0, r1, mz, cnt, flags);
+    block_observables(mz, cnt, flags, a.pc.observe, part, a.words);
+}
+
+// Free particle i (no listed pair and no wall candidacy in this window): until
+// the next re-list it moves under gravity alone, independent of every other
+// particle (the skin check guards that).  Steps slot0 .. slot0+nsteps-1 of the
+// window run in registers: the state is read once and written once, with the
+// per-step arithmetic of particle_finish.  mz_obs receives the height after
+// step observe_slot (if in range).
+template <typename Real>
+__device__ __forceinline__ void free_item(const StepArgs<Real>& a, uint i, int slot0, int nsteps, int observe_slot,
+                                          bool rec, double& mz_obs, uint& flags) {
+    const Real r = a.R[i];
+    V3<double> x = mk(a.P.x[i], a.P.y[i], a.P.z[i]);
+    V3<double> d = mk(a.D.x[i], a.D.y[i], a.D.z[i]);
+    V3<Real> av = mk(a.A.x[i], a.A.y[i], a.A.z[i]);
+    float4 q = a.Q[i];
+    const Real m = sphere_mass(a.density, r);
+    const Real I = (Real)0.4 * m * (r * r);
+    for (int s = slot0; s < slot0 + nsteps; s++) {
+        if (s == 0) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
-        if ((long long)total <= cap) {
-            for (uint k = o0; k < o1; k++) {
-                const R4<Real> f = pf[k];
-                if (f.w != (Real)0) {
-                    const R4<Real> t = pti[k];
-                    F.x += f.x; F.y += f.y; F.z += f.z;
-                    T.x += t.x; T.y += t.y; T.z += t.z;
-                    cnt++;
-                }
-            }
-            for (uint u = r0; u < r1; u++) {
-                const R4<Real> f = rfj[u];
-                if (f.w != (Real)0) {
-                    const R4<Real> t = rtj[u];
-                    F.x += f.x; F.y += f.y; F.z += f.z;
-                    T.x += t.x; T.y += t.y; T.z += t.z;
-                    cnt++;
-                }
-            }
+        F.z += -sphere_mass(a.density, r);
+        if (rec) {
+            a.dbgF[3 * i] = F.x; a.dbgF[3 * i + 1] = F.y; a.dbgF[3 * i + 2] = F.z;
+            a.dbgT[3 * i] = T.x; a.dbgT[3 * i + 1] = T.y; a.dbgT[3 * i + 2] = T.z;
+            a.dbgC[i] = 0;
         }
-        F.z += -density * (Real)8 * r * r * r;   // gravity, then the walls (calculateforceiwD's order)
-        if (ws != kEmpty) {
-            const R4<Real> fw = wf[2 * ws], tw = wf[2 * ws + 1];
-            F.x += fw.x; F.y += fw.y; F.z += fw.z;
-            T.x += tw.x; T.y += tw.y; T.z += tw.z;
-        }
-        particle_finish<Real, false>(i, F, T, r, x, d, a, q, P, D, A, Q, W, pw, pc, dtr, inv_dt, density, mz, flags,
-                                     cnt, dbgF, dbgT, dbgC);
+        double mz;
+        integrate<Real>(F, T, m, I, a.pc.dt, a.dtr, a.pc.half_skin2, x, d, av, q, flags, mz);
+        if (s == observe_slot) mz_obs = mz;
     }
-    block_observables(mz, cnt, flags, pc.observe, part, words);
+    a.P.x[i] = x.x; a.P.y[i] = x.y; a.P.z[i] = x.z;
+    a.D.x[i] = d.x; a.D.y[i] = d.y; a.D.z[i] = d.z;
+    a.A.x[i] = av.x; a.A.y[i] = av.y; a.A.z[i] = av.z;
+    a.Q[i] = q;
+}
+
+// Free particles (flist[t], t < n - nB), slots slot0 .. slot0+nsteps-1.
+template <typename Real>
+__global__ void __launch_bounds__(256) k_free_run(StepArgs<Real> a, int slot0, int nsteps, int observe_slot,
+                                                  StepPartials part, size_t clr0, size_t clr1) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double mz_obs = 0.0;
+    uint flags = 0;
+    if (t < a.n - (long long)a.bpos[a.n])
+        free_item<Real>(a, a.flist[t], slot0, nsteps, observe_slot, a.dbgF != nullptr && nsteps == 1, mz_obs, flags);
+    const int observe = observe_slot >= slot0 && observe_slot < slot0 + nsteps;
+    block_observables(mz_obs, 0u, flags, observe, part, a.words);
+    if (observe) clear_partials(part, clr0, clr1);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of the window kernel (all blocks co-resident: cooperative
+// launch).  Arrival counter + generation word; the waiting is bounded: after
+// kBarrierNs without release the block records kStBarrier in the status word
+// and goes on, and later barriers of the launch then do not wait at all, so
+// the launch always ends.
+constexpr unsigned long long kBarrierNs = 1000000000ull;   // 1 s
+
+__device__ __forceinline__ uint ld_acquire(const uint* p) {
+    uint v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add(uint* p, uint v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier number `k` (0, 1, ...) of a window-kernel launch: every
+// block adds 1 to the arrival counter (zeroed before the launch) with release
+// semantics and waits, with acquire loads, until it reaches (k+1) x blocks.
+// The wait is bounded: after kBarrierNs the block records kStBarrier in the
+// status word and goes on, and later barriers of the launch then do not wait
+// at all, so the launch always ends.
+__device__ __forceinline__ void grid_barrier(uint* count, uint k, EngineWords* words) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint target = (k + 1u) * gridDim.x;
+        red_release_add(count, 1u);
+        if (!(ld_acquire(&words->status) & kStBarrier)) {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire(count) < target) {
+                __nanosleep(20);
+                if (global_ns() - t0 > kBarrierNs) {
+                    atomicOr(&words->status, kStBarrier);
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// The whole window's steps in one cooperative launch (after the re-list):
+// per step, phase 1 = wall + pair items, barrier, phase 2 = bound particles
+// plus 1/K of the free particles (each run through all K steps in
+// registers), barrier.  Items and particles keep their thread for the whole
+// window; data written by other blocks is read with L2-coherent loads.  The
+// arithmetic is that of the per-step kernels (same device functions), so the
+// states are bit-identical.  Observables of the window's last step go to
+// `part` (one partial per block; the slot's remaining partials are cleared).
+constexpr int kWinThreads = 512;
+
+template <typename Real>
+__global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int K, StepPartials part, size_t npart,
+                                                           uint* bar) {
+    const long long nthr = (long long)gridDim.x * blockDim.x;
+    // work index: warps dealt round-robin over the blocks (SMs), lanes
+    // contiguous, so every phase spreads over the whole GPU
+    const long long tid =
+        ((long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x) * 32 + (threadIdx.x & 31);
+    uint nbar = 0;
+    const uint nw = *a.wcount;
+    const uint total = a.off[a.n];
+    const long long items = (long long)nw + ((long long)total <= a.cap ? (long long)total : 0ll);
+    const long long nb = a.bpos[a.n], nf = a.n - nb;
+    // this thread's first item and first bound particle: indices kept in
+    // registers for the whole window (further ones are reloaded per step)
+    uint i0 = 0, j0 = 0, s0 = 0;
+    item_indices(a, tid, nw, items, i0, j0, s0);
+    uint b0 = 0, ws0 = kEmpty, o00 = 0, o10 = 0, r00 = 0, r10 = 0;
+    Real rb0 = (Real)0;
+    if (tid < nb) {
+        b0 = a.blist[tid];
+        rb0 = a.R[b0];
+        ws0 = a.wslot[b0];
+        o00 = a.off[b0]; o10 = a.off[b0 + 1]; r00 = a.roff[b0]; r10 = a.roff[b0 + 1];
+    }
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    ParticleCommon pc = a.pc;
+    for (int s = 0; s < K; s++) {
+        // phase 1: wall and pair items
+        for (long long u = tid; u < items; u += nthr) {
+            uint i = i0, j = j0, rslot = s0;
+            if (u != tid) item_indices(a, u, nw, items, i, j, rslot);
+            if (u < (long long)nw) wall_item<Real, true>(a, u, i);
+            else pair_item<Real, true>(a, u - nw, i, j, rslot);
+        }
+        grid_barrier(bar, nbar++, a.words);
+        // phase 2: bound particles; this step's share of the free particles
+        // (each run through all K steps) from the other end of the work range
+        pc.first = s == 0 ? 1 : 0;
+        for (long long t = tid; t < nb; t += nthr) {
+            double mzi = 0.0;
+            uint ci = 0;
+            if (t == tid) {
+                bound_item<Real, true>(a, pc, b0, rb0, ws0, total, o00, o10, r00, r10, mzi, ci, flags);
+            } else {
+                const uint i = a.blist[t];
+                bound_item<Real, true>(a, pc, i, a.R[i], a.wslot[i], total, a.off[i], a.off[i + 1], a.roff[i],
+                                       a.roff[i + 1], mzi, ci, flags);
+            }
+            if (s == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
+        }
+        const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
+        for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
+            double mzi = 0.0;
+            free_item<Real>(a, a.flist[t], 0, K, K - 1, false, mzi, flags);
+            mz = fmax(mz, mzi);
+        }
+        if (s < K - 1) grid_barrier(bar, nbar++, a.words);
+    }
+    block_observables(mz, cnt, flags, 1, part, a.words);
+    clear_partials(part, gridDim.x, npart);
 }
 
 // PP (particle-parallel, the paper's Figure 1(b)): each particle evaluates all
@@ -631,7 +872,7 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     Planes3<Real> Ai, Planes3<double> Po, Planes3<double> Do, Planes3<Real> Ao, const Real* __restrict__ R,
     float4* __restrict__ Q, Planes3<double> W, Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp,
     LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt, Real density, StepPartials part,
-    EngineWords* words, double* dbgF, double* dbgT, uint* dbgC) {
+    EngineWords* words, double* dbgF, double* dbgT, uint* dbgC, size_t clr0, size_t clr1) {
     pdl_trigger();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz = 0.0;
@@ -678,6 +919,7 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
                                     cnt, dbgF, dbgT, dbgC);
     }
     block_observables(mz, cnt, flags, pc.observe, part, words);
+    if (pc.observe) clear_partials(part, clr0, clr1);
 }
 
 __global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned long long* out) {
@@ -750,8 +992,14 @@ ParticleCommon particle_common(const dem_ctx* c, int slot) {
     return pc;
 }
 
+// Per slot: nblk partials of the (bound-)particle kernel, then nblk of the
+// free-particle kernel.
 StepPartials partials(const dem_ctx* c, int slot) {
-    return StepPartials{c->part_mz + (size_t)slot * c->nblk, c->part_cnt + (size_t)slot * c->nblk};
+    return StepPartials{c->part_mz + (size_t)slot * c->npart, c->part_cnt + (size_t)slot * c->npart};
+}
+StepPartials free_partials(const dem_ctx* c, int slot) {
+    return StepPartials{c->part_mz + (size_t)slot * c->npart + c->nblk,
+                        c->part_cnt + (size_t)slot * c->npart + c->nblk};
 }
 
 // List build from the current state, carrying history from list buffer src
@@ -775,13 +1023,19 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
                                               c->skey, (R4<Real>*)c->spos);
     const Real skin = (Real)c->cfg.skin;
     k_nbr_walk<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin,
-                                                  c->njgi, c->njli, c->scr, c->words);
-    rc = exclusive_scan2_u32(c->njgi, c->off[dst], c->off[dst] + n, c->njli, c->roff, c->roff + n, n, c->scan_tmp, s);
-    if (rc) return rc;
+                                                  c->wslot, c->njgi, c->njli, c->bflag, c->scr, c->words);
+    {
+        const uint* in[3] = {c->njgi, c->njli, c->bflag};
+        uint* out[3] = {c->off[dst], c->roff, c->bpos};
+        uint* tot[3] = {c->off[dst] + n, c->roff + n, c->bpos + n};
+        rc = exclusive_scan_multi_u32(3, in, out, tot, n, c->scan_tmp, s);
+        if (rc) return rc;
+    }
     k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
         n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
         c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
-        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry, c->scr);
+        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry, c->scr,
+        c->bflag, c->bpos, c->blist, c->flist);
     k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->ru, c->off[dst], c->cap);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
@@ -794,32 +1048,77 @@ bool step_pdl(const dem_ctx* c, int slot, bool first_of_step) {
     return c->pdl && !c->profiling && !c->record && (slot > 0 || !first_of_step);
 }
 
-template <typename Real> int launch_pair(dem_ctx* c, int lst, int slot) {
+template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int slot) {
     const long long np = c->npad;
-    LawParams<Real> pp = make_law<Real>(c->mat.pp);
-    DEM_CUDA_TRY(launch_ex(k_pair<Real>, c->pair_grid, 256, c->stream, step_pdl(c, slot, true), c->off[lst], c->n,
-                           c->cap, c->lp, c->ln[lst], c->ru, planes<double>(c->pos[0], np),
-                           planes<double>(c->disp[0], np), planes<Real>(c->ang[0], np), (const Real*)c->rad,
-                           planes<double>(c->hist[lst][0], c->cap), pp, (Real)(1.0 / c->cfg.dt),
-                           (Real)c->cfg.density, (R4<Real>*)c->pf, (R4<Real>*)c->pti, (R4<Real>*)c->rfj,
-                           (R4<Real>*)c->rtj, c->wlist, c->wcount, planes<double>(c->wh, np),
-                           make_law<Real>(c->mat.pw), c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
-                           (R4<Real>*)c->wf));
+    StepArgs<Real> a;
+    a.n = c->n;
+    a.cap = c->cap;
+    a.off = c->off[lst]; a.lp = c->lp; a.ln = c->ln[lst]; a.ru = c->ru; a.roff = c->roff;
+    a.wlist = c->wlist; a.wcount = c->wcount; a.wslot = c->wslot;
+    a.bpos = c->bpos; a.blist = c->blist; a.flist = c->flist;
+    a.P = planes<double>(c->pos[0], np);
+    a.D = planes<double>(c->disp[0], np);
+    a.W = planes<double>(c->wh, np);
+    a.H = planes<double>(c->hist[lst][0], c->cap);
+    a.A = planes<Real>(c->ang[0], np);
+    a.R = (const Real*)c->rad;
+    a.Q = c->q;
+    a.pf = (R4<Real>*)c->pf; a.pti = (R4<Real>*)c->pti; a.rfj = (R4<Real>*)c->rfj; a.rtj = (R4<Real>*)c->rtj;
+    a.wf = (R4<Real>*)c->wf;
+    a.pp = make_law<Real>(c->mat.pp);
+    a.pw = make_law<Real>(c->mat.pw);
+    a.pc = particle_common(c, slot);
+    a.dtr = (Real)c->cfg.dt;
+    a.inv_dt = (Real)(1.0 / c->cfg.dt);
+    a.density = (Real)c->cfg.density;
+    a.words = c->words;
+    a.dbgF = c->record ? c->dbgF : nullptr;
+    a.dbgT = c->record ? c->dbgT : nullptr;
+    a.dbgC = c->record ? c->dbgC : nullptr;
+    return a;
+}
+
+template <typename Real> int launch_pair(dem_ctx* c, int lst, int slot) {
+    DEM_CUDA_TRY(launch_ex(k_pair<Real>, c->pair_grid, 256, c->stream, step_pdl(c, slot, true),
+                           step_args<Real>(c, lst, slot)));
     return DEM_OK;
 }
 
 template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
-    const long long n = c->n, np = c->npad;
-    LawParams<Real> pw = make_law<Real>(c->mat.pw);
-    const double dt = c->cfg.dt;
-    DEM_CUDA_TRY(launch_ex(
-        k_particle<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, false), n, c->off[lst], c->roff,
-        c->cap, (const R4<Real>*)c->pf, (const R4<Real>*)c->pti, (const R4<Real>*)c->rfj, (const R4<Real>*)c->rtj,
-        planes<double>(c->pos[0], np), planes<double>(c->disp[0], np), planes<Real>(c->ang[0], np),
-        (const Real*)c->rad, c->q, planes<double>(c->wh, np), pw, particle_common(c, slot), (Real)dt,
-        (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words, c->record ? c->dbgF : nullptr,
-        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, (const uint*)c->wslot,
-        (const R4<Real>*)c->wf));
+    DEM_CUDA_TRY(launch_ex(k_particle<Real>, grid_for(c->n, 256), 256, c->stream, step_pdl(c, slot, false),
+                           step_args<Real>(c, lst, slot), partials(c, slot)));
+    return DEM_OK;
+}
+
+// Free particles, window slots slot0 .. slot0+nsteps-1, on stream s.
+template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nsteps, cudaStream_t s) {
+    const int obs = c->observe_slot;
+    const int os = (obs >= slot0 && obs < slot0 + nsteps) ? obs : slot0;
+    StepArgs<Real> a = step_args<Real>(c, lst, slot0);
+    if (nsteps != 1) a.dbgF = a.dbgT = nullptr, a.dbgC = nullptr;
+    k_free_run<Real><<<grid_for(c->n, 256), 256, 0, s>>>(a, slot0, nsteps, obs, free_partials(c, os), c->nblk,
+                                                         c->npart - c->nblk);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+// The window kernel: all K steps of the window in one cooperative launch.
+template <typename Real> int launch_window(dem_ctx* c, int lst) {
+    const int K = c->cfg.relist_interval;
+    DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, sizeof(uint), c->stream));   // arrival counter
+    StepArgs<Real> a = step_args<Real>(c, lst, 0);
+    a.dbgF = a.dbgT = nullptr;
+    a.dbgC = nullptr;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c->win_grid);
+    cfg.blockDim = dim3(kWinThreads);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window<Real>, a, K, partials(c, K - 1), c->npart, c->bar));
     return DEM_OK;
 }
 
@@ -835,7 +1134,8 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
         planes<Real>(c->ang[1 - sb], np), (const Real*)c->rad, c->q, planes<double>(c->wh, np),
         planes<double>(c->hist[lst][hp], c->cap), planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw,
         particle_common(c, slot), (Real)dt, (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words,
-        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr));
+        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr,
+        (size_t)c->nblk, c->npart));
     return DEM_OK;
 }
 
@@ -867,6 +1167,10 @@ int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part
         if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2 + 2 * slot], c->stream, cudaEventRecordExternal));
         rc = mixed ? launch_particle<float>(c, lst, slot) : launch_particle<double>(c, lst, slot);
         if (rc) return rc;
+        if (!c->free_in_window) {   // eager step: the free particles' one step, same stream
+            rc = mixed ? launch_free<float>(c, lst, slot, 1, c->stream) : launch_free<double>(c, lst, slot, 1, c->stream);
+            if (rc) return rc;
+        }
     }
     if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[3 + 2 * slot], c->stream, cudaEventRecordExternal));
     if (c->profiling) {
@@ -887,18 +1191,47 @@ namespace {
 // Enqueue one full window (re-list from list `src`, then K steps).
 int enqueue_window(dem_ctx* c, int src) {
     const int K = c->cfg.relist_interval;
-    if (c->wtiming_capture) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[0], c->stream, cudaEventRecordExternal));
+    const bool wt = c->wtiming_capture;
+    if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[0], c->stream, cudaEventRecordExternal));
     int rc = relist(c, src);
     if (rc) return rc;
-    if (c->wtiming_capture) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[1], c->stream, cudaEventRecordExternal));
+    if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[1], c->stream, cudaEventRecordExternal));
     c->hph = 0;
     const int lst = 1 - src;
     c->observe_slot = K - 1;
+    const bool mixed = c->prec == DEM_PREC_MIXED;
+    if (c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel) {
+        // every step of the window in one cooperative launch
+        rc = mixed ? launch_window<float>(c, lst) : launch_window<double>(c, lst);
+        if (rc) return rc;
+        if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2], c->stream, cudaEventRecordExternal));
+        c->wtiming_path = 1;
+        return DEM_OK;
+    }
+    // per-step kernels.  PCCP: the free particles' whole window is one kernel
+    // on a forked branch, concurrent with the bound chain (pair + particle per
+    // step); the two touch disjoint particles and join before the next
+    // re-list.  While forces are recorded every step, the free particles step
+    // with the bound ones instead.
+    const bool fork = c->mode == DEM_FORCE_PCCP && !c->record;
+    if (fork) {
+        DEM_CUDA_TRY(cudaEventRecord(c->evfork, c->stream));
+        DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
+        if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2 + 2 * K], c->stream2, cudaEventRecordExternal));
+        rc = mixed ? launch_free<float>(c, lst, 0, K, c->stream2) : launch_free<double>(c, lst, 0, K, c->stream2);
+        if (rc) return rc;
+        if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[3 + 2 * K], c->stream2, cudaEventRecordExternal));
+        DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
+        c->free_in_window = true;
+    }
     double a, b;
     for (int s = 0; s < K; s++) {
         rc = step_kernels(c, lst, s, &a, &b);
-        if (rc) return rc;
+        if (rc) { c->free_in_window = false; return rc; }
     }
+    c->free_in_window = false;
+    if (fork) DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->evjoin, 0));
+    c->wtiming_path = fork ? 2 : 0;
     return DEM_OK;
 }
 
@@ -984,7 +1317,9 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
         (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->ru, cap)) || (rc = dalloc(&c->words, 1)) ||
         (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
-        (rc = dalloc(&c->wcount, 1)) || (rc = dalloc(&c->arrival, np)) || (rc = dalloc(&c->scr, np * kScr)))
+        (rc = dalloc(&c->wcount, 1)) || (rc = dalloc(&c->arrival, np)) || (rc = dalloc(&c->scr, np * kScr)) ||
+        (rc = dalloc(&c->bflag, np)) || (rc = dalloc(&c->bpos, np + 1)) || (rc = dalloc(&c->blist, np)) ||
+        (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, 64)))
         return bail(rc);
     e = cudaMalloc(&c->wf, 2 * np * 4 * rs);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (wall forces)", __FILE__, __LINE__));
@@ -1006,15 +1341,32 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
                                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair<double>, 256, 0);
         if (e != cudaSuccess) return bail(cuda_fail(e, "pair kernel occupancy", __FILE__, __LINE__));
         c->pair_grid = (unsigned)std::max(1, nsm * std::max(per, 1));
+        int wper = 0;   // the window kernel: every block co-resident (cooperative launch)
+        e = c->prec == DEM_PREC_MIXED ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<float>, kWinThreads, 0)
+                                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<double>, kWinThreads, 0);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "window kernel occupancy", __FILE__, __LINE__));
+        int coop = 0;
+        e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaDeviceGetAttribute", __FILE__, __LINE__));
+        c->win_grid = (unsigned)std::max(1, nsm * wper);
+        const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
+        c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
         const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches inside a window
         c->pdl = !(pdl && pdl[0] == '0');
     }
-    if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->nblk)) ||
-        (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->nblk)))
+    // partials per slot: particle-kernel blocks, free-kernel blocks, and at
+    // least as many as the window kernel has blocks
+    c->npart = std::max<size_t>(2 * (size_t)c->nblk, c->win_grid);
+    if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->npart)) ||
+        (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->npart)))
         return bail(rc);
-    c->scan_words = 2 * scan_scratch_words(std::max<long long>(np + 1, 1));
+    e = cudaMemset(c->part_mz, 0, (size_t)cfg->relist_interval * c->npart * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(c->part_cnt, 0, (size_t)cfg->relist_interval * c->npart * sizeof(uint));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (partials)", __FILE__, __LINE__));
+    c->scan_words = 3 * scan_scratch_words(std::max<long long>(np + 1, 1));
     if ((rc = dalloc(&c->scan_tmp, c->scan_words))) return bail(rc);
     e = cudaMemset(c->words, 0, sizeof(EngineWords));
+    if (e == cudaSuccess) e = cudaMemset(c->bar, 0, 64 * sizeof(uint));
     if (e == cudaSuccess) e = cudaMemset(c->off[0], 0, (np + 1) * sizeof(uint));
     if (e == cudaSuccess) e = cudaMemset(c->off[1], 0, (np + 1) * sizeof(uint));
     if (e == cudaSuccess) e = cudaMemset(c->roff, 0, (np + 1) * sizeof(uint));
@@ -1024,6 +1376,9 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         if (e != cudaSuccess) return bail(cuda_fail(e, "cudaEventCreate", __FILE__, __LINE__));
     }
     e = cudaEventCreateWithFlags(&c->ext_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evfork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evjoin, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__));
     c->stream = c->own_stream;
@@ -1042,14 +1397,17 @@ int dem_destroy(dem_ctx* c) {
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
-                    c->scr};
+                    c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
     for (int k = 0; k < 4; k++)
         if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->ext_ready) cudaEventDestroy(c->ext_ready);
+    if (c->evfork) cudaEventDestroy(c->evfork);
+    if (c->evjoin) cudaEventDestroy(c->evjoin);
     for (cudaEvent_t e : c->wev) cudaEventDestroy(e);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return DEM_OK;
@@ -1287,12 +1645,12 @@ int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
     std::vector<unsigned long long> pm;
     std::vector<uint> pc;
     if (c->last_slot >= 0) {
-        pm.resize(c->nblk);
-        pc.resize(c->nblk);
-        DEM_CUDA_TRY(cudaMemcpyAsync(pm.data(), c->part_mz + (size_t)c->last_slot * c->nblk,
-                                     c->nblk * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
-        DEM_CUDA_TRY(cudaMemcpyAsync(pc.data(), c->part_cnt + (size_t)c->last_slot * c->nblk, c->nblk * sizeof(uint),
-                                     cudaMemcpyDeviceToHost, c->stream));
+        pm.resize(c->npart);
+        pc.resize(c->npart);
+        DEM_CUDA_TRY(cudaMemcpyAsync(pm.data(), c->part_mz + (size_t)c->last_slot * c->npart,
+                                     c->npart * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        DEM_CUDA_TRY(cudaMemcpyAsync(pc.data(), c->part_cnt + (size_t)c->last_slot * c->npart,
+                                     c->npart * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     }
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     EngineWords w;
@@ -1317,7 +1675,8 @@ int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
     out->mean_cn = c->n > 0 ? (double)csum / (double)c->n : 0.0;
     out->packing_fraction = mz > 0.0 ? c->vol / (c->cfg.world[0] * c->cfg.world[1] * mz) : 0.0;
     int status = DEM_OK;
-    if (w.status & kStNonfinite) status = DEM_ERR_NONFINITE;
+    if (w.status & kStBarrier) status = DEM_ERR_TIMEOUT;
+    else if (w.status & kStNonfinite) status = DEM_ERR_NONFINITE;
     else if (w.status & kStCapacity) status = DEM_ERR_CAPACITY;
     else if (w.status & kStSkin) status = DEM_ERR_SKIN;
     out->status = status;
@@ -1432,7 +1791,7 @@ int dem_kernel_times(dem_ctx* c, double out[3]) {
 
 int dem_set_window_timing(dem_ctx* c, int on) {
     if (!c) return fail(DEM_ERR_ARG, "dem_set_window_timing: null ctx");
-    const size_t need = 2 + 2 * (size_t)c->cfg.relist_interval;
+    const size_t need = 4 + 2 * (size_t)c->cfg.relist_interval;
     if (on && c->wev.size() < need) {
         for (size_t k = c->wev.size(); k < need; k++) {
             cudaEvent_t e = nullptr;
@@ -1444,13 +1803,21 @@ int dem_set_window_timing(dem_ctx* c, int on) {
     return DEM_OK;
 }
 
-int dem_window_kernel_times(dem_ctx* c, double out[3]) {
+int dem_window_kernel_times(dem_ctx* c, double out[5]) {
     if (!c || !out) return fail(DEM_ERR_ARG, "dem_window_kernel_times: null argument");
-    out[0] = out[1] = out[2] = 0.0;
+    for (int k = 0; k < 5; k++) out[k] = 0.0;
     if (!c->wtiming_ran) return fail(DEM_ERR_STATE, "dem_window_kernel_times: no timed window has run");
     const int K = c->cfg.relist_interval;
-    DEM_CUDA_TRY(cudaEventSynchronize(c->wev[3 + 2 * (K - 1)]));
     float ms = 0.f;
+    if (c->wtiming_path == 1) {   // window kernel
+        DEM_CUDA_TRY(cudaEventSynchronize(c->wev[2]));
+        DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[0], c->wev[1]));
+        out[0] = ms;
+        DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[1], c->wev[2]));
+        out[4] = ms;
+        return DEM_OK;
+    }
+    DEM_CUDA_TRY(cudaEventSynchronize(c->wev[3 + 2 * (K - 1)]));
     DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[0], c->wev[1]));
     out[0] = ms;
     for (int s = 0; s < K; s++) {
@@ -1459,6 +1826,11 @@ int dem_window_kernel_times(dem_ctx* c, double out[3]) {
         out[1] += ms / K;
         DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[2 + 2 * s], c->wev[3 + 2 * s]));
         out[2] += ms / K;
+    }
+    if (c->wtiming_path == 2) {   // forked free-particle kernel
+        DEM_CUDA_TRY(cudaEventSynchronize(c->wev[3 + 2 * K]));
+        DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[2 + 2 * K], c->wev[3 + 2 * K]));
+        out[3] = ms;
     }
     return DEM_OK;
 }

@@ -11,6 +11,7 @@ enum : uint {
     kStCapacity = 1u,
     kStNonfinite = 2u,
     kStSkin = 4u,
+    kStBarrier = 8u,   // a window-kernel grid barrier ran out of time
 };
 
 // device words: [0] status bits, [1] max row count
@@ -83,6 +84,17 @@ struct dem_ctx {
     uint* njli = nullptr;
     uint* arrival = nullptr; // per particle: slot among its cell's members (hash order)
     uint* scr = nullptr;     // per sorted slot: the walk's first kScr row candidates
+    uint* bflag = nullptr;   // per particle: 1 = bound this window (a listed pair or a wall candidacy)
+    uint* bpos = nullptr;    // exclusive scan of bflag; bpos[n] = number of bound particles
+    uint* blist = nullptr;   // bound particle ids, ascending
+    uint* flist = nullptr;   // free particle ids, ascending
+    cudaStream_t stream2 = 0;        // free-particle branch of the window graph
+    cudaEvent_t evfork = nullptr, evjoin = nullptr;
+    bool free_in_window = false;     // capturing: the free particles run as one window kernel
+    uint* bar = nullptr;             // window-kernel grid barrier: [0] arrival counter
+    unsigned win_grid = 1;           // window-kernel blocks (all co-resident)
+    bool win_kernel = true;          // whole PCCP windows as one cooperative launch
+    int wtiming_path = 0;            // last timed window: 0 per-step, 1 window kernel, 2 per-step + forked free
     uint* off[2] = {nullptr, nullptr};
     uint* roff = nullptr;
     uint* ln[2] = {nullptr, nullptr};
@@ -106,9 +118,10 @@ struct dem_ctx {
     size_t scan_words = 0;
     // scalars
     EngineWords* words = nullptr;
-    unsigned long long* part_mz = nullptr;   // relist_interval x nblk
-    uint* part_cnt = nullptr;                // relist_interval x nblk
+    unsigned long long* part_mz = nullptr;   // relist_interval x npart
+    uint* part_cnt = nullptr;                // relist_interval x npart
     unsigned nblk = 0;                       // blocks of the particle kernel
+    size_t npart = 0;                        // partials per slot: 2 nblk (bound, free)
     unsigned long long* rmax_bits = nullptr;
     void* host_pinned = nullptr;     // mirror for scalars
     // debug force record

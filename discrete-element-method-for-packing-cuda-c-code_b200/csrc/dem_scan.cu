@@ -2,8 +2,8 @@
 // per-particle pair counts, radix digit histograms).  Three launches:
 // tile reduce -> scan of tile sums (one CTA per array) -> tile scan + offset.
 // 256 threads x 16 items per tile; items are loaded as uint4 when aligned.
-// Up to two arrays of the same length are scanned by the same three launches
-// (blockIdx.y selects the array).
+// Up to three arrays of the same length are scanned by the same three
+// launches (blockIdx.y selects the array).
 #include "dem_common.cuh"
 
 namespace dem {
@@ -57,11 +57,12 @@ __device__ __forceinline__ void load_items(const uint* in, long long n, long lon
     }
 }
 
+constexpr int kMaxArrays = 3;
 struct ScanSet {
-    const uint* in[2];
-    uint* out[2];
-    uint* total[2];
-    uint* sums[2];
+    const uint* in[kMaxArrays];
+    uint* out[kMaxArrays];
+    uint* total[kMaxArrays];
+    uint* sums[kMaxArrays];
 };
 
 __global__ void __launch_bounds__(kScanThreads) k_tile_reduce(ScanSet a, long long n) {
@@ -137,23 +138,29 @@ size_t scan_scratch_words(long long n) {
 }
 
 int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s) {
-    if (n <= 0) {
-        if (total) DEM_CUDA_TRY(cudaMemsetAsync(total, 0, sizeof(uint), s));
-        return DEM_OK;
-    }
-    ScanSet a = {{in, nullptr}, {out, nullptr}, {total, nullptr}, {tmp, nullptr}};
-    return scan_set(a, 1, n, s);
+    const uint* ins[1] = {in};
+    uint* outs[1] = {out};
+    uint* tots[1] = {total};
+    return exclusive_scan_multi_u32(1, ins, outs, tots, n, tmp, s);
 }
 
-int exclusive_scan2_u32(const uint* in0, uint* out0, uint* total0, const uint* in1, uint* out1, uint* total1,
-                        long long n, uint* tmp, cudaStream_t s) {
+int exclusive_scan_multi_u32(int narr, const uint* const* in, uint* const* out, uint* const* total, long long n,
+                             uint* tmp, cudaStream_t s) {
+    if (narr < 1 || narr > kMaxArrays) return fail(DEM_ERR_ARG, "exclusive_scan_multi_u32: %d arrays", narr);
     if (n <= 0) {
-        if (total0) DEM_CUDA_TRY(cudaMemsetAsync(total0, 0, sizeof(uint), s));
-        if (total1) DEM_CUDA_TRY(cudaMemsetAsync(total1, 0, sizeof(uint), s));
+        for (int a = 0; a < narr; a++)
+            if (total[a]) DEM_CUDA_TRY(cudaMemsetAsync(total[a], 0, sizeof(uint), s));
         return DEM_OK;
     }
-    ScanSet a = {{in0, in1}, {out0, out1}, {total0, total1}, {tmp, tmp + scan_scratch_words(n)}};
-    return scan_set(a, 2, n, s);
+    ScanSet set = {};
+    const size_t words = scan_scratch_words(n);
+    for (int a = 0; a < narr; a++) {
+        set.in[a] = in[a];
+        set.out[a] = out[a];
+        set.total[a] = total[a];
+        set.sums[a] = tmp + a * words;
+    }
+    return scan_set(set, narr, n, s);
 }
 
 }  // namespace dem

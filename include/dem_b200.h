@@ -45,6 +45,7 @@ extern "C" {
 #define DEM_ERR_SKIN        5  /* a particle moved more than skin/2 inside a window */
 #define DEM_ERR_IO          6  /* deck / output file error                          */
 #define DEM_ERR_STATE       7  /* call out of order (e.g. step before upload)       */
+#define DEM_ERR_TIMEOUT     8  /* a bounded device-side wait ran out (window kernel) */
 
 /* Text of the last error raised on the calling host thread. */
 const char* dem_last_error_string(void);
@@ -280,13 +281,15 @@ int dem_grid_info(dem_ctx* ctx, unsigned int grid[3], double* cell, long long* n
 int dem_set_profiling(dem_ctx* ctx, int on);
 int dem_kernel_times(dem_ctx* ctx, double out[3]);
 /* Event timing inside the window graphs: while on, whole windows replay a
- * second graph that also records CUDA events around the re-list and every
- * pair / particle launch (plain windows carry no event nodes).
- * dem_window_kernel_times gives the mean times (ms) of the last such window:
- * out[0]=re-list, out[1]=pair force per step, out[2]=particle update per step
- * (PP mode: out[1] ~ 0, out[2] the fused step). */
+ * second graph that also records CUDA events around the re-list and the step
+ * kernels (plain windows carry no event nodes).  dem_window_kernel_times
+ * gives the times (ms) of the last such window: out[0]=re-list; per-step
+ * path: out[1]=pair force per step, out[2]=bound-particle update per step,
+ * out[3]=the forked free-particle kernel (whole window); window-kernel path
+ * (PCCP default): out[4]=the window kernel (all steps).  PP mode: out[1] ~ 0,
+ * out[2] the fused step. */
 int dem_set_window_timing(dem_ctx* ctx, int on);
-int dem_window_kernel_times(dem_ctx* ctx, double out[3]);
+int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
 
 /* ---------------------------------------------------------------- adjoint --
  * Reverse mode of the step (force + walls + integrator) over a window; no

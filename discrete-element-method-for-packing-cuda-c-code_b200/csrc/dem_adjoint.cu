@@ -32,9 +32,7 @@ constexpr int kB = 256;
 constexpr int kPairB = 128;   // block size of k_adj_pairs; pbar holds one 12-slot row per block
 
 struct Ck {
-    double* pos = nullptr;   // 3 np
-    double* disp = nullptr;  // 3 np
-    void* ang = nullptr;     // 3 np Real
+    void* rec = nullptr;     // np particle records
     float4* q = nullptr;     // np
     double* wh = nullptr;    // 3 np
     uint* off = nullptr;     // np + 1 (previous list)
@@ -58,6 +56,7 @@ struct AdjWork {
     double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Fb = nullptr, *Tb = nullptr, *Rb = nullptr;
     double* Hb[2] = {nullptr, nullptr};
     double* pbar = nullptr;      // npb x 12 (one row per k_adj_pairs block)
+    double* Pobj = nullptr;      // 3 np: the final positions for the objective
     long long npb = 0;
     double* obj = nullptr;       // [0] value, [1..] scratch
     unsigned long long* zmax = nullptr;  // [0] max z bits, [1] argmax
@@ -68,13 +67,14 @@ struct AdjWork {
 namespace {
 
 void free_ck(Ck& k) {
-    void* p[] = {k.pos, k.disp, k.ang, k.q, k.wh, k.off, k.ln, k.hist};
+    void* p[] = {k.rec, k.q, k.wh, k.off, k.ln, k.hist};
     for (void* x : p)
         if (x) cudaFree(x);
     k = Ck();
 }
 
 size_t rsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(float) : sizeof(double); }
+size_t recsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>); }
 
 int ensure_work(dem_ctx* c, long long seg, long long nck) {
     AdjWork* w = c->adj;
@@ -90,7 +90,8 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
             (rc = dalloc(&w->Wb, 3 * np)) || (rc = dalloc(&w->Fb, 3 * np)) || (rc = dalloc(&w->Tb, 3 * np)) ||
             (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
             (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) || (rc = dalloc(&w->zmax, 2)) ||
-            (rc = dalloc(&w->save_mz, c->npart)) || (rc = dalloc(&w->save_cnt, c->npart)))
+            (rc = dalloc(&w->save_mz, c->npart)) || (rc = dalloc(&w->save_cnt, c->npart)) ||
+            (rc = dalloc(&w->Pobj, 3 * np)))
             return rc;
         w->npb = grid_for(c->n, kPairB);
     }
@@ -123,11 +124,10 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
         w->ck.resize(nck);
         for (size_t k = old; k < (size_t)nck; k++) {
             Ck& x = w->ck[k];
-            if ((rc = dalloc(&x.pos, 3 * np)) || (rc = dalloc(&x.disp, 3 * np)) || (rc = dalloc(&x.q, np)) ||
-                (rc = dalloc(&x.wh, 3 * np)) || (rc = dalloc(&x.off, np + 1)) || (rc = dalloc(&x.ln, cap)) ||
-                (rc = dalloc(&x.hist, 3 * cap)))
+            if ((rc = dalloc(&x.q, np)) || (rc = dalloc(&x.wh, 3 * np)) || (rc = dalloc(&x.off, np + 1)) ||
+                (rc = dalloc(&x.ln, cap)) || (rc = dalloc(&x.hist, 3 * cap)))
                 return rc;
-            DEM_CUDA_TRY(cudaMalloc(&x.ang, 3 * np * rsz(c)));
+            DEM_CUDA_TRY(cudaMalloc(&x.rec, np * recsz(c)));
         }
     }
     w->nck = nck;
@@ -145,9 +145,7 @@ int save_ck(dem_ctx* c, Ck& k) {
     const long long np = c->npad, cap = c->cap;
     cudaStream_t s = c->stream;
     int rc;
-    if ((rc = copy(k.pos, c->pos[c->sbuf], 3 * np * sizeof(double), s)) ||
-        (rc = copy(k.disp, c->disp[c->sbuf], 3 * np * sizeof(double), s)) ||
-        (rc = copy(k.ang, c->ang[c->sbuf], 3 * np * rsz(c), s)) || (rc = copy(k.q, c->q, np * sizeof(float4), s)) ||
+    if ((rc = copy(k.rec, c->rec[c->sbuf], np * recsz(c), s)) || (rc = copy(k.q, c->q, np * sizeof(float4), s)) ||
         (rc = copy(k.wh, c->wh, 3 * np * sizeof(double), s)) ||
         (rc = copy(k.off, c->off[c->cur], (np + 1) * sizeof(uint), s)) ||
         (rc = copy(k.ln, c->ln[c->cur], cap * sizeof(uint), s)) ||
@@ -166,9 +164,7 @@ int restore_ck(dem_ctx* c, const Ck& k) {
     c->sbuf = k.sbuf;
     c->hph = k.hph;
     int rc;
-    if ((rc = copy(c->pos[c->sbuf], k.pos, 3 * np * sizeof(double), s)) ||
-        (rc = copy(c->disp[c->sbuf], k.disp, 3 * np * sizeof(double), s)) ||
-        (rc = copy(c->ang[c->sbuf], k.ang, 3 * np * rsz(c), s)) || (rc = copy(c->q, k.q, np * sizeof(float4), s)) ||
+    if ((rc = copy(c->rec[c->sbuf], k.rec, np * recsz(c), s)) || (rc = copy(c->q, k.q, np * sizeof(float4), s)) ||
         (rc = copy(c->wh, k.wh, 3 * np * sizeof(double), s)) ||
         (rc = copy(c->off[c->cur], k.off, (np + 1) * sizeof(uint), s)) ||
         (rc = copy(c->ln[c->cur], k.ln, cap * sizeof(uint), s)) ||
@@ -324,19 +320,22 @@ __global__ void k_adj_carry(const uint* __restrict__ off, long long n, long long
 // Records the input of one recomputed step: state planes, wall history and
 // the pair history of the current list (count read on the device).
 template <typename Real>
-__global__ void k_tape(long long n, long long np, long long cap, const double* __restrict__ P,
-                       const double* __restrict__ D, const Real* __restrict__ A, const double* __restrict__ W,
-                       const uint* __restrict__ off, const double* __restrict__ H, double* __restrict__ tx,
-                       double* __restrict__ td, Real* __restrict__ ta, double* __restrict__ twh,
-                       double* __restrict__ th) {
+__global__ void k_tape(long long n, long long np, long long cap, const PRec<Real>* __restrict__ S,
+                       const double* __restrict__ W, const uint* __restrict__ off, const double* __restrict__ H,
+                       double* __restrict__ tx, double* __restrict__ td, Real* __restrict__ ta,
+                       double* __restrict__ twh, double* __restrict__ th) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    for (long long k = t0; k < 3 * np; k += stride) {
-        tx[k] = P[k];
-        td[k] = D[k];
-        ta[k] = A[k];
-        twh[k] = W[k];
+    for (long long i = t0; i < np; i += stride) {
+        V3<double> x, d;
+        V3<Real> a;
+        Real r;
+        ld_rec<false>(S + i, x, d, a, r);
+        st3(tx, np, i, x);
+        st3(td, np, i, d);
+        ta[i] = a.x; ta[np + i] = a.y; ta[2 * np + i] = a.z;
     }
+    for (long long k = t0; k < 3 * np; k += stride) twh[k] = W[k];
     long long total = off[n];
     if (total > cap) total = cap;
     for (long long k = t0; k < total; k += stride) {
@@ -477,11 +476,18 @@ template <typename Real> int adj_pairs(dem_ctx* c, long long t, const ListRec& l
     return DEM_OK;
 }
 
+template <typename Real>
+__global__ void k_rec_positions(long long np, const PRec<Real>* __restrict__ S, double* __restrict__ P) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < np) st3(P, np, i, ld_pos<false>(S + i));
+}
+
 template <typename Real> int objective(dem_ctx* c, int which) {
     AdjWork* w = c->adj;
     const long long n = c->n, np = c->npad, cap = c->cap;
-    const double* P = c->pos[c->sbuf];
     cudaStream_t s = c->stream;
+    double* P = w->Pobj;   // final positions as planes
+    k_rec_positions<Real><<<grid_for(np, kB), kB, 0, s>>>(np, (const PRec<Real>*)c->rec[c->sbuf], P);
     DEM_CUDA_TRY(cudaMemsetAsync(w->obj, 0, 16 * sizeof(double), s));
     if (which == DEM_OBJ_PACKING) {
         unsigned long long init[2] = {0ull, ~0ull};
@@ -585,14 +591,14 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
                 if ((rc = list_snapshot(c, w->lists[t / K]))) return rc;
             }
             if (mixed)
-                k_tape<float><<<148 * 4, kB, 0, s>>>(c->n, np, cap, c->pos[c->sbuf], c->disp[c->sbuf],
-                                                     (const float*)c->ang[c->sbuf], c->wh, c->off[c->cur],
+                k_tape<float><<<148 * 4, kB, 0, s>>>(c->n, np, cap, (const PRec<float>*)c->rec[c->sbuf], c->wh,
+                                                     c->off[c->cur],
                                                      c->hist[c->cur][c->hph], w->tx + 3 * np * t, w->td + 3 * np * t,
                                                      (float*)w->ta + 3 * np * t, w->twh + 3 * np * t,
                                                      w->th + 3 * cap * t);
             else
-                k_tape<double><<<148 * 4, kB, 0, s>>>(c->n, np, cap, c->pos[c->sbuf], c->disp[c->sbuf],
-                                                      (const double*)c->ang[c->sbuf], c->wh, c->off[c->cur],
+                k_tape<double><<<148 * 4, kB, 0, s>>>(c->n, np, cap, (const PRec<double>*)c->rec[c->sbuf], c->wh,
+                                                      c->off[c->cur],
                                                       c->hist[c->cur][c->hph], w->tx + 3 * np * t,
                                                       w->td + 3 * np * t, (double*)w->ta + 3 * np * t,
                                                       w->twh + 3 * np * t, w->th + 3 * cap * t);
@@ -673,7 +679,7 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (Ck& k : w->ck) free_ck(k);
     void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->Xb, w->Db, w->Ab, w->Wb, w->Fb, w->Tb,
-                 w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt};
+                 w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj};
     for (void* x : p)
         if (x) cudaFree(x);
     for (ListRec& l : w->lists) {

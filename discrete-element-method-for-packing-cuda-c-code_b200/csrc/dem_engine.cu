@@ -82,29 +82,32 @@ __device__ __forceinline__ uint lane_id() { return threadIdx.x & 31; }
 // ------------------------------------------------------------ state I/O
 template <typename Real>
 __global__ void k_from_aos(long long n, const double* __restrict__ pos, const double* __restrict__ pdis,
-                           const double* __restrict__ angv, const double* __restrict__ rad, Planes3<double> P,
-                           Planes3<double> D, Planes3<Real> A, Real* __restrict__ R, float4* __restrict__ Q,
-                           Planes3<double> W) {
+                           const double* __restrict__ angv, const double* __restrict__ rad, PRec<Real>* __restrict__ S,
+                           Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    P.x[i] = pos[3 * i]; P.y[i] = pos[3 * i + 1]; P.z[i] = pos[3 * i + 2];
-    D.x[i] = pdis ? pdis[3 * i] : 0.0; D.y[i] = pdis ? pdis[3 * i + 1] : 0.0; D.z[i] = pdis ? pdis[3 * i + 2] : 0.0;
-    A.x[i] = angv ? (Real)angv[3 * i] : (Real)0;
-    A.y[i] = angv ? (Real)angv[3 * i + 1] : (Real)0;
-    A.z[i] = angv ? (Real)angv[3 * i + 2] : (Real)0;
-    R[i] = (Real)rad[i];
+    const V3<double> x = mk(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    const V3<double> d = pdis ? mk(pdis[3 * i], pdis[3 * i + 1], pdis[3 * i + 2]) : zero3<double>();
+    const V3<Real> a = angv ? mk((Real)angv[3 * i], (Real)angv[3 * i + 1], (Real)angv[3 * i + 2]) : zero3<Real>();
+    const Real r = (Real)rad[i];
+    st_rec(S + i, x, d, a, r);
+    R[i] = r;
     Q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     W.x[i] = 0.0; W.y[i] = 0.0; W.z[i] = 0.0;
 }
 
 template <typename Real>
-__global__ void k_to_aos(long long n, Planes3<double> P, Planes3<double> D, Planes3<Real> A, double* __restrict__ pos,
+__global__ void k_to_aos(long long n, const PRec<Real>* __restrict__ S, double* __restrict__ pos,
                          double* __restrict__ pdis, double* __restrict__ angv) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (pos) { pos[3 * i] = P.x[i]; pos[3 * i + 1] = P.y[i]; pos[3 * i + 2] = P.z[i]; }
-    if (pdis) { pdis[3 * i] = D.x[i]; pdis[3 * i + 1] = D.y[i]; pdis[3 * i + 2] = D.z[i]; }
-    if (angv) { angv[3 * i] = (double)A.x[i]; angv[3 * i + 1] = (double)A.y[i]; angv[3 * i + 2] = (double)A.z[i]; }
+    V3<double> x, d;
+    V3<Real> a;
+    Real r;
+    ld_rec<false>(S + i, x, d, a, r);
+    if (pos) { pos[3 * i] = x.x; pos[3 * i + 1] = x.y; pos[3 * i + 2] = x.z; }
+    if (pdis) { pdis[3 * i] = d.x; pdis[3 * i + 1] = d.y; pdis[3 * i + 2] = d.z; }
+    if (angv) { angv[3 * i] = (double)a.x; angv[3 * i + 1] = (double)a.y; angv[3 * i + 2] = (double)a.z; }
 }
 
 // --------------------------------------------------------------- re-list
@@ -115,14 +118,15 @@ __global__ void k_to_aos(long long n, Planes3<double> P, Planes3<double> D, Plan
 // the step checks, so no other particle can touch a wall before the next
 // re-list -- the same guarantee as the pair list's).
 template <typename Real>
-__global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __restrict__ key, uint* __restrict__ count,
-                             uint* __restrict__ arrival, const Real* __restrict__ R, double hx, double hy,
-                             double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist,
-                             uint* __restrict__ wcount) {
+__global__ void k_hash_count(long long n, const PRec<Real>* __restrict__ S, GridC g, uint* __restrict__ key,
+                             uint* __restrict__ count, uint* __restrict__ arrival, const Real* __restrict__ R,
+                             double hx, double hy, double half_skin, uint* __restrict__ wslot,
+                             uint* __restrict__ wlist, uint* __restrict__ wcount) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const V3<double> p = ld_pos<false>(S + i);
     {
-        const double x = P.x[i], y = P.y[i], z = P.z[i];
+        const double x = p.x, y = p.y, z = p.z;
         const double mg = (double)R[i] + half_skin;
         const bool near = (z < mg) || (x + hx < mg) || (hx - x < mg) || (y + hy < mg) || (hy - y < mg);
         uint ws = kEmpty;
@@ -134,9 +138,9 @@ __global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __re
     }
     const Real csr = (Real)g.cs;
     Real xl;
-    int cx = cell_axis<Real>(P.x[i], g.ox, csr, g.gx, xl);
-    int cy = cell_axis<Real>(P.y[i], g.oy, csr, g.gy, xl);
-    int cz = cell_axis<Real>(P.z[i], g.oz, csr, g.gz, xl);
+    int cx = cell_axis<Real>(p.x, g.ox, csr, g.gx, xl);
+    int cy = cell_axis<Real>(p.y, g.oy, csr, g.gy, xl);
+    int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
     uint c = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
     key[i] = c;
     arrival[i] = atomicAdd(&count[c], 1u);   // the particle's slot among its cell's members (unordered)
@@ -148,16 +152,17 @@ __global__ void k_hash_count(long long n, Planes3<double> P, GridC g, uint* __re
 // coalesced by id.
 template <typename Real>
 __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint* __restrict__ arrival,
-                          const uint* __restrict__ cstart, uint* __restrict__ count, Planes3<double> P,
+                          const uint* __restrict__ cstart, uint* __restrict__ count, const PRec<Real>* __restrict__ S,
                           const Real* __restrict__ R, GridC g, uint* __restrict__ sidu, uint* __restrict__ skeyu,
                           R4<Real>* __restrict__ sposu) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint c = key[i];
+    const V3<double> p = ld_pos<false>(S + i);
     R4<Real> v;
-    v.x = (Real)(P.x[i] - g.ox);
-    v.y = (Real)(P.y[i] - g.oy);
-    v.z = (Real)(P.z[i] - g.oz);
+    v.x = (Real)(p.x - g.ox);
+    v.y = (Real)(p.y - g.oy);
+    v.z = (Real)(p.z - g.oz);
     v.w = R[i];
     const uint slot = cstart[c] + arrival[i];
     count[c] = 0u;
@@ -377,8 +382,8 @@ __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double
 template <typename Real> struct StepArgs {
     long long n, cap;
     const uint *off, *lp, *ln, *ru, *roff, *wlist, *wcount, *wslot, *bpos, *blist, *flist;
-    Planes3<double> P, D, W, H;   // position, displacement, wall history, pair history (in place)
-    Planes3<Real> A;              // rotation
+    PRec<Real>* S;                // particle records (in place)
+    Planes3<double> W, H;         // wall history, pair history (in place)
     const Real* R;
     float4* Q;                    // displacement since the list (xyz), wall flag (w)
     R4<Real> *pf, *pti, *rfj, *rtj, *wf;
@@ -414,12 +419,15 @@ template <bool COH, typename T> __device__ __forceinline__ V3<T> ld3p(Planes3<T>
 // wf[2c+1].
 template <typename Real, bool COH>
 __device__ __forceinline__ void wall_item(const StepArgs<Real>& a, long long c, uint i) {
-    const Real r = a.R[i];
+    V3<double> x, d;
+    V3<Real> av;
+    Real r;
+    ld_rec<COH>(a.S + i, x, d, av, r);
     const Real m = a.density * (Real)8 * r * r * r;
     V3<double> h = ld3p<COH>(a.W, i);
     V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
-    const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, ld3p<COH>(a.P, i), cvt<Real>(ld3p<COH>(a.D, i)),
-                                        ld3p<COH>(a.A, i), r, m, h, a.inv_dt, a.pw, Fw, Tw, (Real*)nullptr);
+    const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, x, cvt<Real>(d), av, r, m, h, a.inv_dt, a.pw, Fw, Tw,
+                                        (Real*)nullptr);
     a.W.x[i] = h.x; a.W.y[i] = h.y; a.W.z[i] = h.z;
     R4<Real> a4, b4;
     a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
@@ -436,10 +444,13 @@ __device__ __forceinline__ void wall_item(const StepArgs<Real>& a, long long c, 
 template <typename Real, bool COH>
 __device__ __forceinline__ void pair_item(const StepArgs<Real>& a, long long k, uint i, uint j, uint rslot) {
     V3<double> h = mk(ldx<COH>(a.H.x + k), ldx<COH>(a.H.y + k), ldx<COH>(a.H.z + k));
+    V3<double> xi, di, xj, dj;
+    V3<Real> ai, aj;
+    Real ri, rj;
+    ld_rec<COH>(a.S + i, xi, di, ai, ri);
+    ld_rec<COH>(a.S + j, xj, dj, aj, rj);
     V3<Real> Fi, Ti, Tj;
-    const int c = pair_eval<Real>(ld3p<COH>(a.P, i), ld3p<COH>(a.P, j), ld3p<COH>(a.D, i), ld3p<COH>(a.D, j),
-                                  ld3p<COH>(a.A, i), ld3p<COH>(a.A, j), a.R[i], a.R[j], h, a.pp, a.inv_dt, a.density,
-                                  Fi, Ti, Tj);
+    const int c = pair_eval<Real>(xi, xj, di, dj, ai, aj, ri, rj, h, a.pp, a.inv_dt, a.density, Fi, Ti, Tj);
     a.H.x[k] = h.x; a.H.y[k] = h.y; a.H.z[k] = h.z;
     R4<Real> fo, fr;
     if (c) {
@@ -544,8 +555,8 @@ template <typename Real> __device__ __forceinline__ Real sphere_mass(Real densit
 // in F/T; writes the new state to the output planes.
 template <typename Real, bool WALLS>
 __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real> T, Real r, V3<double> x,
-                                                V3<double> d, V3<Real> a, float4 q, Planes3<double> Po,
-                                                Planes3<double> Do, Planes3<Real> Ao, float4* __restrict__ Q,
+                                                V3<double> d, V3<Real> a, float4 q, PRec<Real>* So,
+                                                float4* __restrict__ Q,
                                                 Planes3<double> W, const LawParams<Real>& pw, const ParticleCommon& pc,
                                                 Real dtr, Real inv_dt, Real density, double& mz, uint& flags,
                                                 uint cnt, double* dbgF, double* dbgT, uint* dbgC) {
@@ -573,9 +584,7 @@ __device__ __forceinline__ void particle_finish(long long i, V3<Real> F, V3<Real
     }
     integrate<Real>(F, T, m, I, pc.dt, dtr, pc.half_skin2, x, d, a, q, flags, mz);
     q.w = __uint_as_float(wflag);
-    Po.x[i] = x.x; Po.y[i] = x.y; Po.z[i] = x.z;
-    Do.x[i] = d.x; Do.y[i] = d.y; Do.z[i] = d.z;
-    Ao.x[i] = a.x; Ao.y[i] = a.y; Ao.z[i] = a.z;
+    st_rec(So + i, x, d, a, r);
     Q[i] = q;
 }
 
@@ -630,9 +639,10 @@ template <typename Real, bool COH>
 __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const ParticleCommon& pc, uint i, Real r, uint ws,
                                            uint total, uint o0, uint o1, uint r0, uint r1, double& mz, uint& cnt,
                                            uint& flags) {
-    const V3<double> x = ld3p<COH>(a.P, i);
-    const V3<double> d = ld3p<COH>(a.D, i);
-    const V3<Real> av = ld3p<COH>(a.A, i);
+    V3<double> x, d;
+    V3<Real> av;
+    Real rr;
+    ld_rec<COH>(a.S + i, x, d, av, rr);
     const float4 q = ldx<COH>(a.Q + i);
     V3<Real> F = zero3<Real>(), T = zero3<Real>();
     if ((long long)total <= a.cap) {
@@ -661,8 +671,8 @@ __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const Partic
         F.x += fw.x; F.y += fw.y; F.z += fw.z;
         T.x += tw.x; T.y += tw.y; T.z += tw.z;
     }
-    particle_finish<Real, false>(i, F, T, r, x, d, av, q, a.P, a.D, a.A, a.Q, a.W, a.pw, pc, a.dtr, a.inv_dt,
-                                 a.density, mz, flags, cnt, a.dbgF, a.dbgT, a.dbgC);
+    particle_finish<Real, false>(i, F, T, r, x, d, av, q, a.S, a.Q, a.W, a.pw, pc, a.dtr, a.inv_dt, a.density, mz,
+                                 flags, cnt, a.dbgF, a.dbgT, a.dbgC);
 }
 
 // PCCP particle kernel: one thread per bound particle (blist[t], t < nB =
@@ -698,10 +708,10 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(StepArgs<Re
 template <typename Real>
 __device__ __forceinline__ void free_item(const StepArgs<Real>& a, uint i, int slot0, int nsteps, int observe_slot,
                                           bool rec, double& mz_obs, uint& flags) {
-    const Real r = a.R[i];
-    V3<double> x = mk(a.P.x[i], a.P.y[i], a.P.z[i]);
-    V3<double> d = mk(a.D.x[i], a.D.y[i], a.D.z[i]);
-    V3<Real> av = mk(a.A.x[i], a.A.y[i], a.A.z[i]);
+    V3<double> x, d;
+    V3<Real> av;
+    Real r;
+    ld_rec<false>(a.S + i, x, d, av, r);
     float4 q = a.Q[i];
     const Real m = sphere_mass(a.density, r);
     const Real I = (Real)0.4 * m * (r * r);
@@ -718,9 +728,7 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, uint i, int s
         integrate<Real>(F, T, m, I, a.pc.dt, a.dtr, a.pc.half_skin2, x, d, av, q, flags, mz);
         if (s == observe_slot) mz_obs = mz;
     }
-    a.P.x[i] = x.x; a.P.y[i] = x.y; a.P.z[i] = x.z;
-    a.D.x[i] = d.x; a.D.y[i] = d.y; a.D.z[i] = d.z;
-    a.A.x[i] = av.x; a.A.y[i] = av.y; a.A.z[i] = av.z;
+    st_rec(a.S + i, x, d, av, r);
     a.Q[i] = q;
 }
 
@@ -868,9 +876,8 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
 template <typename Real>
 __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     long long n, const uint* __restrict__ off, const uint* __restrict__ roff, const uint* __restrict__ rk,
-    const uint* __restrict__ lp, const uint* __restrict__ ln, long long cap, Planes3<double> Pi, Planes3<double> Di,
-    Planes3<Real> Ai, Planes3<double> Po, Planes3<double> Do, Planes3<Real> Ao, const Real* __restrict__ R,
-    float4* __restrict__ Q, Planes3<double> W, Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp,
+    const uint* __restrict__ lp, const uint* __restrict__ ln, long long cap, const PRec<Real>* __restrict__ Si,
+    PRec<Real>* __restrict__ So, const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W, Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp,
     LawParams<Real> pw, ParticleCommon pc, Real dtr, Real inv_dt, Real density, StepPartials part,
     EngineWords* words, double* dbgF, double* dbgT, uint* dbgC, size_t clr0, size_t clr1) {
     pdl_trigger();
@@ -887,19 +894,22 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     }
     pdl_wait();
     if (i < n) {
-        const V3<double> x = mk(Pi.x[i], Pi.y[i], Pi.z[i]);
-        const V3<double> d = mk(Di.x[i], Di.y[i], Di.z[i]);
-        const V3<Real> a = mk(Ai.x[i], Ai.y[i], Ai.z[i]);
+        V3<double> x, d;
+        V3<Real> a;
+        Real rr;
+        ld_rec<false>(Si + i, x, d, a, rr);
         const float4 q = Q[i];
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
         if ((long long)total <= cap) {
             for (uint k = o0; k < o1; k++) {
                 const uint j = ln[k];
                 V3<double> h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
+                V3<double> xj, dj;
+                V3<Real> aj;
+                Real rj;
+                ld_rec<false>(Si + j, xj, dj, aj, rj);
                 V3<Real> Fl, Tl, Th;
-                const int c = pair_eval<Real>(x, mk(Pi.x[j], Pi.y[j], Pi.z[j]), d, mk(Di.x[j], Di.y[j], Di.z[j]), a,
-                                              mk(Ai.x[j], Ai.y[j], Ai.z[j]), r, R[j], h, pp, inv_dt, density, Fl, Tl,
-                                              Th);
+                const int c = pair_eval<Real>(x, xj, d, dj, a, aj, r, rj, h, pp, inv_dt, density, Fl, Tl, Th);
                 Ho.x[k] = h.x; Ho.y[k] = h.y; Ho.z[k] = h.z;
                 if (c) { F += Fl; T += Tl; cnt++; }
             }
@@ -908,15 +918,17 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
                 if (k >= total) continue;
                 const uint j = lp[k];
                 V3<double> h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
+                V3<double> xj, dj;
+                V3<Real> aj;
+                Real rj;
+                ld_rec<false>(Si + j, xj, dj, aj, rj);
                 V3<Real> Fl, Tl, Th;
-                const int c = pair_eval<Real>(mk(Pi.x[j], Pi.y[j], Pi.z[j]), x, mk(Di.x[j], Di.y[j], Di.z[j]), d,
-                                              mk(Ai.x[j], Ai.y[j], Ai.z[j]), a, R[j], r, h, pp, inv_dt, density, Fl,
-                                              Tl, Th);
+                const int c = pair_eval<Real>(xj, x, dj, d, aj, a, rj, r, h, pp, inv_dt, density, Fl, Tl, Th);
                 if (c) { F -= Fl; T += Th; cnt++; }
             }
         }
-        particle_finish<Real, true>(i, F, T, r, x, d, a, q, Po, Do, Ao, Q, W, pw, pc, dtr, inv_dt, density, mz, flags,
-                                    cnt, dbgF, dbgT, dbgC);
+        particle_finish<Real, true>(i, F, T, r, x, d, a, q, So, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt,
+                                    dbgF, dbgT, dbgC);
     }
     block_observables(mz, cnt, flags, pc.observe, part, words);
     if (pc.observe) clear_partials(part, clr0, clr1);
@@ -1005,19 +1017,19 @@ StepPartials free_partials(const dem_ctx* c, int slot) {
 // List build from the current state, carrying history from list buffer src
 // (phase c->hph) into buffer 1-src (phase 0).
 template <typename Real> int launch_relist(dem_ctx* c, int src) {
-    const long long n = c->n, np = c->npad;
+    const long long n = c->n;
     const int dst = 1 - src;
     const int B = 256;
     cudaStream_t s = c->stream;
-    Planes3<double> P = planes<double>(c->pos[c->sbuf], np);
+    const PRec<Real>* S = (const PRec<Real>*)c->rec[c->sbuf];
     GridC g = c->grid;
     DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
-    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, P, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
+    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, S, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
                                                     c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
                                                     c->wslot, c->wlist, c->wcount);
     int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
     if (rc) return rc;
-    k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->arrival, c->cstart, c->ccount, P, (const Real*)c->rad,
+    k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->arrival, c->cstart, c->ccount, S, (const Real*)c->rad,
                                                  g, c->sid, c->skeyu, (R4<Real>*)c->sposu);
     k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->cstart, c->sid, c->skeyu, (const R4<Real>*)c->sposu, c->sid2,
                                               c->skey, (R4<Real>*)c->spos);
@@ -1056,11 +1068,9 @@ template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int
     a.off = c->off[lst]; a.lp = c->lp; a.ln = c->ln[lst]; a.ru = c->ru; a.roff = c->roff;
     a.wlist = c->wlist; a.wcount = c->wcount; a.wslot = c->wslot;
     a.bpos = c->bpos; a.blist = c->blist; a.flist = c->flist;
-    a.P = planes<double>(c->pos[0], np);
-    a.D = planes<double>(c->disp[0], np);
+    a.S = (PRec<Real>*)c->rec[0];
     a.W = planes<double>(c->wh, np);
     a.H = planes<double>(c->hist[lst][0], c->cap);
-    a.A = planes<Real>(c->ang[0], np);
     a.R = (const Real*)c->rad;
     a.Q = c->q;
     a.pf = (R4<Real>*)c->pf; a.pti = (R4<Real>*)c->pti; a.rfj = (R4<Real>*)c->rfj; a.rtj = (R4<Real>*)c->rtj;
@@ -1128,14 +1138,13 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
     LawParams<Real> pp = make_law<Real>(c->mat.pp), pw = make_law<Real>(c->mat.pw);
     const double dt = c->cfg.dt;
     DEM_CUDA_TRY(launch_ex(
-        k_step_pp<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, true), n, c->off[lst], c->roff,
-        c->rk, c->lp, c->ln[lst], c->cap, planes<double>(c->pos[sb], np), planes<double>(c->disp[sb], np),
-        planes<Real>(c->ang[sb], np), planes<double>(c->pos[1 - sb], np), planes<double>(c->disp[1 - sb], np),
-        planes<Real>(c->ang[1 - sb], np), (const Real*)c->rad, c->q, planes<double>(c->wh, np),
-        planes<double>(c->hist[lst][hp], c->cap), planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw,
-        particle_common(c, slot), (Real)dt, (Real)(1.0 / dt), (Real)c->cfg.density, partials(c, slot), c->words,
-        c->record ? c->dbgF : nullptr, c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr,
-        (size_t)c->nblk, c->npart));
+        k_step_pp<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, true), n, (const uint*)c->off[lst],
+        (const uint*)c->roff, (const uint*)c->rk, (const uint*)c->lp, (const uint*)c->ln[lst], c->cap,
+        (const PRec<Real>*)c->rec[sb], (PRec<Real>*)c->rec[1 - sb], (const Real*)c->rad, c->q,
+        planes<double>(c->wh, np), planes<double>(c->hist[lst][hp], c->cap),
+        planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw, particle_common(c, slot), (Real)dt, (Real)(1.0 / dt),
+        (Real)c->cfg.density, partials(c, slot), c->words, c->record ? c->dbgF : nullptr,
+        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, (size_t)c->nblk, c->npart));
     return DEM_OK;
 }
 
@@ -1302,9 +1311,10 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     const long long n = c->n, np = c->npad, cap = c->cap;
     const size_t rs = real_size(c->prec);
     const int nstate = c->mode == DEM_FORCE_PP ? 2 : 1;
+    const size_t recb = c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>);
     for (int b = 0; b < nstate; b++) {
-        if ((rc = dalloc(&c->pos[b], 3 * np)) || (rc = dalloc(&c->disp[b], 3 * np))) return bail(rc);
-        e = cudaMalloc(&c->ang[b], 3 * np * rs);
+        e = cudaMalloc(&c->rec[b], np * recb);
+        if (e == cudaSuccess) e = cudaMemset(c->rec[b], 0, np * recb);
         if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (state)", __FILE__, __LINE__));
     }
     for (int l = 0; l < 2; l++)
@@ -1392,7 +1402,7 @@ int dem_destroy(dem_ctx* c) {
     dem_adjoint_release(c);
     free_graphs(c);
     free_cells(c);
-    void* ptrs[] = {c->pos[0], c->pos[1], c->disp[0], c->disp[1], c->ang[0], c->ang[1], c->rad, c->q, c->wh,
+    void* ptrs[] = {c->rec[0], c->rec[1], c->rad, c->q, c->wh,
                     c->staging, c->key, c->sid, c->sid2, c->spos, c->skeyu, c->skey, c->sposu, c->njgi, c->njli,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
@@ -1529,13 +1539,12 @@ static int upload_common(dem_ctx* c, const double* pos, const double* pdis, cons
         if (!(c->rmax > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state_device: radii not positive");
     }
     if (c->prec == DEM_PREC_MIXED)
-        k_from_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(
-            n, ppos, ppd, ppa, prad, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
-            planes<float>(c->ang[0], np), (float*)c->rad, c->q, planes<double>(c->wh, np));
+        k_from_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, ppos, ppd, ppa, prad, (PRec<float>*)c->rec[0],
+                                                                  (float*)c->rad, c->q, planes<double>(c->wh, np));
     else
-        k_from_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(
-            n, ppos, ppd, ppa, prad, planes<double>(c->pos[0], np), planes<double>(c->disp[0], np),
-            planes<double>(c->ang[0], np), (double*)c->rad, c->q, planes<double>(c->wh, np));
+        k_from_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, ppos, ppd, ppa, prad,
+                                                                   (PRec<double>*)c->rec[0], (double*)c->rad, c->q,
+                                                                   planes<double>(c->wh, np));
     DEM_LAUNCH_CHECK();
     return finish_upload(c);
 }
@@ -1558,13 +1567,9 @@ static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, 
     if (!pdis) td = nullptr;
     if (!angv) ta = nullptr;
     if (c->prec == DEM_PREC_MIXED)
-        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos[sb], np),
-                                                                planes<double>(c->disp[sb], np),
-                                                                planes<float>(c->ang[sb], np), tp, td, ta);
+        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, (const PRec<float>*)c->rec[sb], tp, td, ta);
     else
-        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, planes<double>(c->pos[sb], np),
-                                                                 planes<double>(c->disp[sb], np),
-                                                                 planes<double>(c->ang[sb], np), tp, td, ta);
+        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, (const PRec<double>*)c->rec[sb], tp, td, ta);
     DEM_LAUNCH_CHECK();
     if (host) {
         if (pos) DEM_CUDA_TRY(cudaMemcpyAsync(pos, tp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

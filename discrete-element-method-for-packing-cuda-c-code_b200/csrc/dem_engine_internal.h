@@ -23,6 +23,69 @@ struct EngineWords {
 
 template <typename Real> struct Planes3 { Real* x; Real* y; Real* z; };
 
+// Particle record: FP64 position and per-step displacement, rotation (per-step
+// angle) and radius in the working precision.  One record per particle, so a
+// gathered particle costs 2 (mixed: 64 B) or 3 (FP64: 96 B) 32-byte sectors
+// instead of one per field.
+template <typename Real> struct PRec;
+template <> struct alignas(64) PRec<float> {
+    double x, y, z, dx, dy, dz;
+    float ax, ay, az, r;
+};
+template <> struct alignas(32) PRec<double> {
+    double x, y, z, dx, dy, dz;
+    double ax, ay, az, r, pad0, pad1;
+};
+static_assert(sizeof(PRec<float>) == 64 && sizeof(PRec<double>) == 96, "record layout");
+
+// Record access by 16-byte vectors; COH: L2-coherent loads (.cg) for data that
+// other blocks of the same launch write.
+template <bool COH, typename T> __device__ __forceinline__ T ldv(const T* p) {
+    if constexpr (COH) return __ldcg(p);
+    else return *p;
+}
+template <bool COH>
+__device__ __forceinline__ void ld_rec(const PRec<float>* p, V3<double>& x, V3<double>& d, V3<float>& a, float& r) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 v0 = ldv<COH>(q), v1 = ldv<COH>(q + 1), v2 = ldv<COH>(q + 2);
+    const float4 v3 = ldv<COH>(reinterpret_cast<const float4*>(p) + 3);
+    x = mk(v0.x, v0.y, v1.x);
+    d = mk(v1.y, v2.x, v2.y);
+    a = mk(v3.x, v3.y, v3.z);
+    r = v3.w;
+}
+template <bool COH>
+__device__ __forceinline__ void ld_rec(const PRec<double>* p, V3<double>& x, V3<double>& d, V3<double>& a,
+                                       double& r) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 v0 = ldv<COH>(q), v1 = ldv<COH>(q + 1), v2 = ldv<COH>(q + 2), v3 = ldv<COH>(q + 3),
+                  v4 = ldv<COH>(q + 4);
+    x = mk(v0.x, v0.y, v1.x);
+    d = mk(v1.y, v2.x, v2.y);
+    a = mk(v3.x, v3.y, v4.x);
+    r = v4.y;
+}
+template <bool COH, typename Real> __device__ __forceinline__ V3<double> ld_pos(const PRec<Real>* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 v0 = ldv<COH>(q), v1 = ldv<COH>(q + 1);
+    return mk(v0.x, v0.y, v1.x);
+}
+__device__ __forceinline__ void st_rec(PRec<float>* p, V3<double> x, V3<double> d, V3<float> a, float r) {
+    double2* q = reinterpret_cast<double2*>(p);
+    q[0] = make_double2(x.x, x.y);
+    q[1] = make_double2(x.z, d.x);
+    q[2] = make_double2(d.y, d.z);
+    reinterpret_cast<float4*>(p)[3] = make_float4(a.x, a.y, a.z, r);
+}
+__device__ __forceinline__ void st_rec(PRec<double>* p, V3<double> x, V3<double> d, V3<double> a, double r) {
+    double2* q = reinterpret_cast<double2*>(p);
+    q[0] = make_double2(x.x, x.y);
+    q[1] = make_double2(x.z, d.x);
+    q[2] = make_double2(d.y, d.z);
+    q[3] = make_double2(a.x, a.y);
+    q[4] = make_double2(a.z, r);
+}
+
 struct GridC {
     double ox, oy, oz;   // world origin
     double cs;
@@ -62,9 +125,7 @@ struct dem_ctx {
     double rmax = 0.0;
     double vol = 0.0;        // sum (4/3) pi r^3
     // state: [current buffer]; the second buffer exists in PP mode only
-    double* pos[2] = {nullptr, nullptr};   // 3 planes
-    double* disp[2] = {nullptr, nullptr};  // 3 planes
-    void* ang[2] = {nullptr, nullptr};     // 3 planes, Real
+    void* rec[2] = {nullptr, nullptr};     // PRec<Real>[npad] per state buffer
     int sbuf = 0;
     void* rad = nullptr;     // Real
     float4* q = nullptr;

@@ -38,7 +38,7 @@ BYTES_PER_PARTICLE = {"mixed": 172, "fp64": 200}   # per particle-step, all fiel
 BYTES_PER_PAIR = 56                                 # ids 8 + FP64 history r+w 48, per pair-step
 METRIC = "particle-steps/s @500K spheres"
 UNIT = "particle-steps/s"
-KERNELS_PER_WINDOW = 11 + 2 * 20   # re-list (incl. 2 scan passes x 3 launches) + 2 per step
+KERNELS_PER_WINDOW = 12 + 1   # re-list (incl. 2 scan passes x 3 launches) + the window kernel
 
 
 def load_pkg():
@@ -211,11 +211,18 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
     bp = BYTES_PER_PARTICLE[args.precision]
-    part_bytes = w.n * bp
-    achieved = part_bytes / (kt["particle_ms"] / 1e3) / 1e9 if kt["particle_ms"] > 0 else None
     pairs = sc["pairs"]
-    window_bytes = win * (w.n * bp + pairs * BYTES_PER_PAIR) + w.n * (24 + 8 + 16 + 4) + pairs * 64
-    traffic = profile_traffic(f"k_particle_rsa500k_{args.precision}")
+    # dominant kernel: the window kernel (every step of a window in one launch).
+    # Algorithmic bytes per launch: each particle-step and pair-step touches
+    # its fields once (B_p, B_pair per particle-step / pair-step).
+    win_bytes_kernel = win * (w.n * bp + pairs * BYTES_PER_PAIR)
+    if kt["window_kernel_ms"] > 0:
+        kname, kbytes, kms = "k_window", win_bytes_kernel, kt["window_kernel_ms"]
+    else:   # per-step kernels: the particle kernel per step
+        kname, kbytes, kms = "k_particle", w.n * bp, kt["particle_ms"]
+    achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else None
+    window_bytes = win_bytes_kernel + w.n * (24 + 8 + 16 + 4) + pairs * 64
+    traffic = profile_traffic(f"{kname}_rsa500k_{args.precision}")
 
     # --- FP64 plain form of the same step (throughput bar for mixed)
     fp64 = None
@@ -315,9 +322,12 @@ def run_ours(args):
                    "ms_per_dem_step": max_ms / dem_steps, "pairs_per_particle": pairs / w.n,
                    "contacts_per_particle": sc["contacts"] / w.n, "packing_fraction": sc["packing_fraction"],
                    "mean_cn": sc["mean_cn"]},
-        "roofline": {"bound": "hbm", "kernel": "k_particle", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": part_bytes,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": kbytes,
+                     "note": "algorithmic bytes count every particle-step's fields once; the window kernel "
+                             "keeps free particles in registers across its steps, so achieved can exceed the "
+                             "copy peak while DRAM traffic (traffic) stays far below the algorithmic bytes",
                      "kernel_ms": kt, "kernel_timing": "CUDA events inside the last timed window's graph "
                      "(mean over its 20 steps)", "step_bytes_per_window": window_bytes,
                      "step_achieved_gbs": window_bytes / (max_ms / K / 1e3) / 1e9},

@@ -53,6 +53,22 @@ def load_pkg():
     return mod
 
 
+def max_over_ranks(torch, dist, ms, device, ws):
+    """The job's time: the largest per-rank device time (every rank's timed
+    region ends at a barrier first)."""
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if ws > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(n_per_rank, dem_steps, ws, max_ms):
+    """Particle-steps/s of all replicas together (weak scaling: each rank
+    steps its own n_per_rank particles)."""
+    return n_per_rank * dem_steps * ws / (max_ms / 1e3)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -201,13 +217,9 @@ def run_ours(args):
     # dominant kernel duration: CUDA events inside the last timed window's graph
     kt = eng.window_kernel_times()
     sc = eng.scalars()
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(torch, dist, total_ms, dev, ws)
     dem_steps = K * win
-    value = w.n * dem_steps * ws / (max_ms / 1e3)
+    value = whole_job_rate(w.n, dem_steps, ws, max_ms)
 
     peak, peak_kind = measured_peak()
     bp = BYTES_PER_PARTICLE[args.precision]
@@ -290,14 +302,10 @@ def run_ours(args):
         stream.synchronize()
         wall = time.perf_counter() - t0
         ev_ms = a.elapsed_time(b)
-        e2e_s = max(wall, ev_ms / 1e3)
-        t2 = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        if ws > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        e2e_s = float(t2.item())
+        e2e_s = max_over_ranks(torch, dist, max(wall, ev_ms / 1e3) * 1e3, dev, ws) / 1e3
         h2d = 3 * w.n * 8 + w.n * 8
         d2h = 9 * w.n * 8 + ke * 64
-        e2e = {"value": w.n * ke * win * ws / e2e_s, "unit": UNIT, "windows": ke,
+        e2e = {"value": whole_job_rate(w.n, ke * win, ws, e2e_s * 1e3), "unit": UNIT, "windows": ke,
                "h2d_bytes_per_step": h2d / ke, "d2h_bytes_per_step": d2h / ke,
                "timing": "host wall clock and CUDA events, larger of the two"}
 

@@ -9,13 +9,17 @@
 //      sum (4/3) pi r^3 / (Wx Wy max z) or potential energy
 //      sum m z + sum (2/5) estar sqrt(R*) delta^2.5 (pairs and walls); its
 //      gradient seeds the adjoint state.
-//   3. for each segment, last first: restore the checkpoint, recompute the K
-//      steps recording per-step state, force, torque and pair history, and
-//      every re-list's list and carry map; then sweep the steps backwards:
-//        k_adj_prep   integrator reverse (one thread per particle)
-//        k_adj_pairs  pair + wall VJP (dem_law_adj.cuh), particle-parallel:
-//                     each particle evaluates the reverse of all its pairs
-//                     and keeps its own share -- no atomics, deterministic
+//   3. for each segment, last first: restore the checkpoint, recompute the
+//      segment (PCCP: re-list + window kernel per window, writing the tape of
+//      the bound particles -- state, force, torque, wall and pair history --
+//      and every re-list's list, carry map and bound/free lists; one CUDA
+//      graph per segment); then sweep the steps backwards (one CUDA graph
+//      per segment):
+//        k_adj_free   free particles of the window: integrator reverse only
+//        k_adj_step   bound particles: integrator reverse + pair + wall VJP
+//                     (dem_law_adj.cuh), particle-parallel: each particle
+//                     evaluates the reverse of all its pairs and keeps its
+//                     own share -- no atomics, deterministic
 //        k_adj_carry  at a re-list, the history adjoints of the new list go
 //                     back to the carried pairs of the previous list
 // The reverse runs in FP64 on the recorded FP64/FP32 trajectory.
@@ -29,7 +33,7 @@ namespace dem {
 
 namespace {
 constexpr int kB = 256;
-constexpr int kPairB = 128;   // block size of k_adj_pairs; pbar holds one 12-slot row per block
+constexpr int kPairB = 128;   // block size of k_adj_step; pbar holds one 12-slot row per block
 
 struct Ck {
     void* rec = nullptr;     // np particle records
@@ -43,7 +47,10 @@ struct Ck {
 
 struct ListRec {
     uint *off = nullptr, *ln = nullptr, *lp = nullptr, *roff = nullptr, *rk = nullptr, *carry = nullptr;
-    long long P = 0;
+    uint* bflag = nullptr;   // bound (1) / free (0) particles of the window
+    uint* blist = nullptr;   // bound particle ids (n)
+    uint* flist = nullptr;   // free particle ids (n)
+    uint* nb = nullptr;      // number of bound particles (device word)
 };
 }  // namespace
 
@@ -53,9 +60,14 @@ struct AdjWork {
     std::vector<ListRec> lists;
     double *tx = nullptr, *td = nullptr, *twh = nullptr, *tF = nullptr, *tT = nullptr, *th = nullptr;
     void* ta = nullptr;
-    double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Fb = nullptr, *Tb = nullptr, *Rb = nullptr;
+    // state adjoints, two sets (ping-pong per reversed step); the objective
+    // seeds set 0 (Xb, Db, Ab alias it)
+    double* Xb2[2] = {nullptr, nullptr};
+    double* Db2[2] = {nullptr, nullptr};
+    double* Ab2[2] = {nullptr, nullptr};
+    double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Rb = nullptr;
     double* Hb[2] = {nullptr, nullptr};
-    double* pbar = nullptr;      // npb x 12 (one row per k_adj_pairs block)
+    double* pbar = nullptr;      // npb x 12 (one row per k_adj_step block)
     double* Pobj = nullptr;      // 3 np: the final positions for the objective
     long long npb = 0;
     double* obj = nullptr;       // [0] value, [1..] scratch
@@ -86,21 +98,26 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
     const int K = c->cfg.relist_interval;
     int rc;
     if (!w->Xb) {
-        if ((rc = dalloc(&w->Xb, 3 * np)) || (rc = dalloc(&w->Db, 3 * np)) || (rc = dalloc(&w->Ab, 3 * np)) ||
-            (rc = dalloc(&w->Wb, 3 * np)) || (rc = dalloc(&w->Fb, 3 * np)) || (rc = dalloc(&w->Tb, 3 * np)) ||
+        if ((rc = dalloc(&w->Xb2[0], 3 * np)) || (rc = dalloc(&w->Db2[0], 3 * np)) ||
+            (rc = dalloc(&w->Ab2[0], 3 * np)) || (rc = dalloc(&w->Xb2[1], 3 * np)) ||
+            (rc = dalloc(&w->Db2[1], 3 * np)) || (rc = dalloc(&w->Ab2[1], 3 * np)) || (rc = dalloc(&w->Wb, 3 * np)) ||
             (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
-            (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) || (rc = dalloc(&w->zmax, 2)) ||
+            (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) ||
+            (rc = dalloc(&w->zmax, 2)) ||
             (rc = dalloc(&w->save_mz, c->npart)) || (rc = dalloc(&w->save_cnt, c->npart)) ||
             (rc = dalloc(&w->Pobj, 3 * np)))
             return rc;
         w->npb = grid_for(c->n, kPairB);
+        w->Xb = w->Xb2[0];
+        w->Db = w->Db2[0];
+        w->Ab = w->Ab2[0];
     }
     if (seg > w->seg) {
         void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta};
         for (void* x : p)
             if (x) cudaFree(x);
         for (ListRec& l : w->lists) {
-            void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry};
+            void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry, l.bflag, l.blist, l.flist, l.nb};
             for (void* x : q)
                 if (x) cudaFree(x);
         }
@@ -114,7 +131,9 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
         w->lists.resize(nw);
         for (ListRec& l : w->lists)
             if ((rc = dalloc(&l.off, np + 1)) || (rc = dalloc(&l.ln, cap)) || (rc = dalloc(&l.lp, cap)) ||
-                (rc = dalloc(&l.roff, np + 1)) || (rc = dalloc(&l.rk, cap)) || (rc = dalloc(&l.carry, cap)))
+                (rc = dalloc(&l.roff, np + 1)) || (rc = dalloc(&l.rk, cap)) || (rc = dalloc(&l.carry, cap)) ||
+                (rc = dalloc(&l.bflag, np)) || (rc = dalloc(&l.blist, np)) || (rc = dalloc(&l.flist, np)) ||
+                (rc = dalloc(&l.nb, 1)))
                 return rc;
         w->seg = seg;
         w->nwin = nw;
@@ -184,59 +203,107 @@ __device__ __forceinline__ void st3(double* a, long long np, long long i, V3d v)
     a[i] = v.x; a[np + i] = v.y; a[2 * np + i] = v.z;
 }
 
-// Integrator reverse (neiglist.cu:356-360 read backwards):
+// Integrator reverse of particle i (neiglist.cu:356-360 read backwards):
 //   d' = d + F dt^2/m,  x' = x + d',  a' = a + T dt^2/I,  F_z includes -m.
+// Given the adjoints (xb, db, ab) of the state after the step, returns the
+// adjoint of d' (dtot = db + xb) and of the step's force and torque, and
+// adds the mass / inertia terms to the radius adjoint.  A free particle of
+// the window (not taped) feels its weight only, in the working precision as
+// the forward computed it.
 template <typename Real>
-__global__ void k_adj_prep(long long n, long long np, const Real* __restrict__ R, const double* __restrict__ F,
-                           const double* __restrict__ T, double dt, double density, double* __restrict__ Xb,
-                           double* __restrict__ Db, const double* __restrict__ Ab, double* __restrict__ Fb,
-                           double* __restrict__ Tb, double* __restrict__ Rb) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double r = (double)R[i];
+__device__ __forceinline__ void integ_rev(Real rr, bool bound, const double* __restrict__ F,
+                                          const double* __restrict__ T, long long i, double dt, double density, V3d xb,
+                                          V3d db, V3d ab, V3d& dtot, V3d& fb, V3d& tb, double& rb) {
+    const double r = (double)rr;
     const double m = density * 8.0 * r * r * r, I = 0.4 * m * (r * r);
     const double dmdr = density * 24.0 * r * r, dIdr = 0.4 * (dmdr * r * r + 2.0 * m * r);
-    const V3d xb = ld3(Xb, np, i), ab = ld3(Ab, np, i);
-    const V3d dtot = ld3(Db, np, i) + xb;
-    const V3d f = mk(F[3 * i], F[3 * i + 1], F[3 * i + 2]), t = mk(T[3 * i], T[3 * i + 1], T[3 * i + 2]);
+    dtot = db + xb;
+    const V3d f = bound ? mk(F[3 * i], F[3 * i + 1], F[3 * i + 2])
+                        : mk(0.0, 0.0, (double)(-((Real)density * (Real)8 * rr * rr * rr)));
+    const V3d t = bound ? mk(T[3 * i], T[3 * i + 1], T[3 * i + 2]) : mk(0.0, 0.0, 0.0);
     const double k = dt * dt / m, kI = dt * dt / I;
-    const V3d fb = k * dtot;
-    st3(Fb, np, i, fb);
-    st3(Tb, np, i, kI * ab);
+    fb = k * dtot;
+    tb = kI * ab;
     double mb = -dot(dtot, f) * k / m;   // d/dm of F dt^2/m
     mb += -fb.z;                          // gravity F_z = ... - m
     const double Ib = -dot(ab, t) * kI / I;
-    Rb[i] += mb * dmdr + Ib * dIdr;
-    st3(Db, np, i, dtot);
+    rb += mb * dmdr + Ib * dIdr;
+}
+
+// Force / torque adjoints of partner j from the after-step adjoints (the
+// first half of integ_rev, no side effects).
+template <typename Real>
+__device__ __forceinline__ void partner_fb(Real rr, long long np, long long j, double dt, double density,
+                                           const double* __restrict__ Xa, const double* __restrict__ Da,
+                                           const double* __restrict__ Aa, V3d& fb, V3d& tb) {
+    const double r = (double)rr;
+    const double m = density * 8.0 * r * r * r, I = 0.4 * m * (r * r);
+    fb = (dt * dt / m) * (ld3(Da, np, j) + ld3(Xa, np, j));
+    tb = (dt * dt / I) * ld3(Aa, np, j);
 }
 
 struct AdjList {
     const uint *off, *ln, *lp, *roff, *rk;
 };
 
-// Pair and wall reverse, particle-parallel.  Each particle evaluates (forward
-// with tape, then reverse) every pair it belongs to and keeps its own share
-// of the input adjoints; the pair's history adjoint and its parameter
-// adjoints are kept by the lower index only.
+// One reversed step of the window's free particles (flist[t], t < n - nb):
+// they feel their weight only, so the step is the integrator reverse; their
+// wall-history adjoint is zero.
 template <typename Real>
-__global__ void __launch_bounds__(kPairB) k_adj_pairs(
-    long long n, long long np, long long cap, AdjList L, const double* __restrict__ tx, const double* __restrict__ td,
-    const Real* __restrict__ ta, const double* __restrict__ twh,
-    const double* __restrict__ th, const Real* __restrict__ R, LawParams<double> pp, LawParams<double> pw,
-    double inv_dt, double density, double hx, double hy, const double* __restrict__ Fb, const double* __restrict__ Tb,
-    const double* __restrict__ Hout, double* __restrict__ Hin, double* __restrict__ Xb, double* __restrict__ Db,
-    double* __restrict__ Ab, double* __restrict__ Wb, double* __restrict__ Rb, double* __restrict__ pbar) {
+__global__ void k_adj_free(long long n, long long np, const uint* __restrict__ flist, const uint* __restrict__ nbp,
+                           const Real* __restrict__ R, double dt, double density, const double* __restrict__ Xa,
+                           const double* __restrict__ Da, const double* __restrict__ Aa, double* __restrict__ Xo,
+                           double* __restrict__ Do, double* __restrict__ Ao, double* __restrict__ Wb,
+                           double* __restrict__ Rb) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n - (long long)*nbp) return;
+    const long long i = flist[t];
+    const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
+    V3d dtot, fb, tb;
+    double rb = 0.0;
+    integ_rev<Real>(R[i], false, nullptr, nullptr, i, dt, density, xa, ld3(Da, np, i), aa, dtot, fb, tb, rb);
+    st3(Xo, np, i, xa);
+    st3(Do, np, i, dtot);
+    st3(Ao, np, i, aa);
+    st3(Wb, np, i, zero3<double>());
+    Rb[i] += rb;
+}
+
+// One reversed step of the window's bound particles (blist[u], u < nb),
+// particle-parallel: the integrator reverse of particle i, then every pair it
+// belongs to and its walls, evaluated forward with tape and reversed; each
+// particle keeps its own share of the input adjoints, the pair's history
+// adjoint and its parameter adjoints are kept by the lower index only.  State
+// adjoints ping-pong: (Xa, Da, Aa) after the step are read (also for the
+// partners' force adjoints), (Xo, Do, Ao) before the step are written; no
+// atomics, deterministic.
+template <typename Real>
+__global__ void __launch_bounds__(kPairB) k_adj_step(
+    long long n, long long np, long long cap, AdjList L, const uint* __restrict__ blist, const uint* __restrict__ nbp,
+    const double* __restrict__ tx, const double* __restrict__ td, const Real* __restrict__ ta,
+    const double* __restrict__ twh, const double* __restrict__ th, const double* __restrict__ tF,
+    const double* __restrict__ tT, const Real* __restrict__ R, LawParams<double> pp, LawParams<double> pw,
+    double dt, double density, double hx, double hy, const double* __restrict__ Hout, double* __restrict__ Hin,
+    const double* __restrict__ Xa, const double* __restrict__ Da, const double* __restrict__ Aa,
+    double* __restrict__ Xo, double* __restrict__ Do, double* __restrict__ Ao, double* __restrict__ Wb,
+    double* __restrict__ Rb, double* __restrict__ pbar) {
     __shared__ double sp[12][kPairB / 32];
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const double inv_dt = 1.0 / dt;
+    const long long u0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     LawBar bp, bw;
     lawbar_zero(bp);
     lawbar_zero(bw);
-    if (i < n) {
+    if (u0 < (long long)*nbp) {
+        const long long i = blist[u0];
+        const Real rr = R[i];
+        const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
+        V3d dtot, fbi, tbi;
+        double rb = 0.0;
+        integ_rev<Real>(rr, true, tF, tT, i, dt, density, xa, ld3(Da, np, i), aa, dtot, fbi, tbi, rb);
+        V3d xb = zero3<double>(), dbv = zero3<double>(), ab = zero3<double>();
         const V3d xi = ld3(tx, np, i), di = ld3(td, np, i), ai = ldA<Real>(ta, np, i);
-        const double ri = (double)R[i];
-        const V3d fbi = ld3(Fb, np, i), tbi = ld3(Tb, np, i);
-        V3d xb = zero3<double>(), dbv = zero3<double>(), ab = zero3<double>(), dum3 = zero3<double>();
-        double rb = 0.0, dum = 0.0;
+        const double ri = (double)rr;
+        double dum = 0.0;
         const uint total = L.off[n];
         if ((long long)total <= cap) {
             for (uint k = L.off[i]; k < L.off[i + 1]; k++) {
@@ -249,9 +316,11 @@ __global__ void __launch_bounds__(kPairB) k_adj_pairs(
                     Hin[k] = 0.0; Hin[cap + k] = 0.0; Hin[2 * cap + k] = 0.0;
                     continue;
                 }
+                V3d fbj, tbj;
+                partner_fb<Real>(R[j], np, j, dt, density, Xa, Da, Aa, fbj, tbj);
                 V3d hinb = zero3<double>(), xjb = zero3<double>(), djb = zero3<double>(), ajb = zero3<double>();
-                pair_rev(t, pp, inv_dt, density, fbi - ld3(Fb, np, j), tbi, ld3(Tb, np, j),
-                         mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]), xb, xjb, dbv, djb, ab, ajb, rb, dum, hinb, bp);
+                pair_rev(t, pp, inv_dt, density, fbi - fbj, tbi, tbj, mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]), xb,
+                         xjb, dbv, djb, ab, ajb, rb, dum, hinb, bp);
                 Hin[k] = hinb.x; Hin[cap + k] = hinb.y; Hin[2 * cap + k] = hinb.z;
             }
             for (uint u = L.roff[i]; u < L.roff[i + 1]; u++) {
@@ -264,12 +333,13 @@ __global__ void __launch_bounds__(kPairB) k_adj_pairs(
                 if (!pair_fwd(ld3(tx, np, j), xi, ld3(td, np, j), di, ldA<Real>(ta, np, j), ai, (double)R[j], ri, hin,
                               pp, inv_dt, density, t, Fi, Ti, Tj, ho))
                     continue;
+                V3d fbj, tbj;
+                partner_fb<Real>(R[j], np, j, dt, density, Xa, Da, Aa, fbj, tbj);
                 LawBar scratch;
                 lawbar_zero(scratch);
                 V3d hinb = zero3<double>(), xlb = zero3<double>(), dlb = zero3<double>(), alb = zero3<double>();
-                pair_rev(t, pp, inv_dt, density, ld3(Fb, np, j) - fbi, ld3(Tb, np, j), tbi,
-                         mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]), xlb, xb, dlb, dbv, alb, ab, dum, rb, hinb,
-                         scratch);
+                pair_rev(t, pp, inv_dt, density, fbj - fbi, tbj, tbi, mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]),
+                         xlb, xb, dlb, dbv, alb, ab, dum, rb, hinb, scratch);
             }
         }
         // walls (the stored slot is the history input; it is zero whenever
@@ -278,10 +348,9 @@ __global__ void __launch_bounds__(kPairB) k_adj_pairs(
         V3d hwb = zero3<double>();
         wall_vjp(hx, hy, xi, di, ai, ri, density, hw, pw, inv_dt, fbi, tbi, ld3(Wb, np, i), xb, dbv, ab, rb, hwb, bw);
         st3(Wb, np, i, hwb);
-        (void)dum3;
-        st3(Xb, np, i, ld3(Xb, np, i) + xb);
-        st3(Db, np, i, ld3(Db, np, i) + dbv);
-        st3(Ab, np, i, ld3(Ab, np, i) + ab);
+        st3(Xo, np, i, xa + xb);
+        st3(Do, np, i, dtot + dbv);
+        st3(Ao, np, i, aa + ab);
         Rb[i] += rb;
     }
     // parameter adjoints: block sums accumulated into this block's slot
@@ -308,13 +377,14 @@ __global__ void k_adj_carry(const uint* __restrict__ off, long long n, long long
                             const double* __restrict__ Hnew, double* __restrict__ Hold) {
     const uint total = off[n];
     if ((long long)total > cap) return;
-    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= (long long)total) return;
-    const uint t = carry[k];
-    if (t == kEmpty || (long long)t >= cap) return;
-    Hold[t] = Hnew[k];
-    Hold[cap + t] = Hnew[cap + k];
-    Hold[2 * cap + t] = Hnew[2 * cap + k];
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total;
+         k += (long long)gridDim.x * blockDim.x) {
+        const uint t = carry[k];
+        if (t == kEmpty || (long long)t >= cap) continue;
+        Hold[t] = Hnew[k];
+        Hold[cap + t] = Hnew[cap + k];
+        Hold[2 * cap + t] = Hnew[2 * cap + k];
+    }
 }
 
 // Records the input of one recomputed step: state planes, wall history and
@@ -453,25 +523,23 @@ __global__ void k_obj_potential(long long n, long long np, long long cap, AdjLis
     }
 }
 
-template <typename Real> int adj_prep(dem_ctx* c, long long t) {
-    AdjWork* w = c->adj;
-    const long long np = c->npad;
-    k_adj_prep<Real><<<grid_for(c->n, kB), kB, 0, c->stream>>>(
-        c->n, np, (const Real*)c->rad, w->tF + 3 * np * t, w->tT + 3 * np * t, c->cfg.dt, c->cfg.density, w->Xb, w->Db,
-        w->Ab, w->Fb, w->Tb, w->Rb);
-    DEM_LAUNCH_CHECK();
-    return DEM_OK;
-}
-
-template <typename Real> int adj_pairs(dem_ctx* c, long long t, const ListRec& l, int hb) {
+// Reversed step t of the segment: state adjoints read from set `in` (after
+// the step), written to set 1 - in (before the step); free particles by
+// k_adj_free, bound ones by k_adj_step.
+template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l, int hb, int in) {
     AdjWork* w = c->adj;
     const long long np = c->npad, cap = c->cap;
     AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
-    k_adj_pairs<Real><<<(unsigned)w->npb, kPairB, 0, c->stream>>>(
-        c->n, np, cap, L, w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t,
-        w->twh + 3 * np * t, w->th + 3 * cap * t, (const Real*)c->rad, make_law<double>(c->mat.pp),
-        make_law<double>(c->mat.pw), 1.0 / c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
-        w->Fb, w->Tb, w->Hb[hb], w->Hb[1 - hb], w->Xb, w->Db, w->Ab, w->Wb, w->Rb, w->pbar);
+    k_adj_free<Real><<<grid_for(c->n, kB), kB, 0, c->stream>>>(
+        c->n, np, l.flist, l.nb, (const Real*)c->rad, c->cfg.dt, c->cfg.density, w->Xb2[in], w->Db2[in], w->Ab2[in],
+        w->Xb2[1 - in], w->Db2[1 - in], w->Ab2[1 - in], w->Wb, w->Rb);
+    DEM_LAUNCH_CHECK();
+    k_adj_step<Real><<<(unsigned)w->npb, kPairB, 0, c->stream>>>(
+        c->n, np, cap, L, l.blist, l.nb, w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t,
+        w->twh + 3 * np * t, w->th + 3 * cap * t, w->tF + 3 * np * t, w->tT + 3 * np * t, (const Real*)c->rad,
+        make_law<double>(c->mat.pp), make_law<double>(c->mat.pw), c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5,
+        c->cfg.world[1] * 0.5, w->Hb[hb], w->Hb[1 - hb], w->Xb2[in], w->Db2[in], w->Ab2[in], w->Xb2[1 - in],
+        w->Db2[1 - in], w->Ab2[1 - in], w->Wb, w->Rb, w->pbar);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -507,20 +575,105 @@ template <typename Real> int objective(dem_ctx* c, int which) {
     return DEM_OK;
 }
 
+// The list of the window just built (no host sync: the pair arrays are
+// copied at capacity; kernels read the pair count on the device) with its
+// bound / free particle lists.
 int list_snapshot(dem_ctx* c, ListRec& l) {
     cudaStream_t s = c->stream;
-    const long long np = c->npad;
-    uint P = 0;
-    DEM_CUDA_TRY(cudaMemcpyAsync(&P, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, s));
-    DEM_CUDA_TRY(cudaStreamSynchronize(s));
-    if ((long long)P > c->cap) return fail(DEM_ERR_CAPACITY, "adjoint: pair list exceeded capacity");
-    l.P = P;
+    const long long np = c->npad, cap = c->cap;
     int rc;
     if ((rc = copy(l.off, c->off[c->cur], (np + 1) * sizeof(uint), s)) ||
         (rc = copy(l.roff, c->roff, (np + 1) * sizeof(uint), s)) ||
-        (rc = copy(l.ln, c->ln[c->cur], P * sizeof(uint), s)) || (rc = copy(l.lp, c->lp, P * sizeof(uint), s)) ||
-        (rc = copy(l.rk, c->rk, P * sizeof(uint), s)))
+        (rc = copy(l.ln, c->ln[c->cur], cap * sizeof(uint), s)) || (rc = copy(l.lp, c->lp, cap * sizeof(uint), s)) ||
+        (rc = copy(l.rk, c->rk, cap * sizeof(uint), s)) || (rc = copy(l.bflag, c->bflag, np * sizeof(uint), s)) ||
+        (rc = copy(l.blist, c->blist, np * sizeof(uint), s)) || (rc = copy(l.flist, c->flist, np * sizeof(uint), s)) ||
+        (rc = copy(l.nb, c->bpos + c->n, sizeof(uint), s)))
         return rc;
+    return DEM_OK;
+}
+
+// The recompute of one segment with the window kernel: per window, the
+// re-list (recording the carry map), the list snapshot and the window kernel
+// writing the tape.  Advances c->cur as the re-lists do.
+int recompute_segment(dem_ctx* c, long long every) {
+    AdjWork* w = c->adj;
+    const int K = c->cfg.relist_interval;
+    int rc;
+    for (long long t = 0; t < every; t += K) {
+        c->carry = w->lists[t / K].carry;
+        rc = relist(c, c->cur);
+        c->carry = nullptr;
+        if (rc) return rc;
+        c->cur = 1 - c->cur;
+        c->hph = 0;
+        if ((rc = list_snapshot(c, w->lists[t / K]))) return rc;
+        WindowTape tape{w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, (int)t};
+        if ((rc = window_kernel(c, c->cur, &tape))) return rc;
+    }
+    return DEM_OK;
+}
+
+// The reversed steps of one segment (steps every-1 .. 0), enqueued on the
+// context's stream; hb / in advance as the steps swap their buffers.
+int reverse_segment(dem_ctx* c, long long every, int& hb, int& in) {
+    AdjWork* w = c->adj;
+    const int K = c->cfg.relist_interval;
+    const long long cap = c->cap;
+    const bool mixed = c->prec == DEM_PREC_MIXED;
+    cudaStream_t s = c->stream;
+    int rc;
+    for (long long t = every - 1; t >= 0; t--) {
+        const ListRec& l = w->lists[t / K];
+        rc = mixed ? adj_step<float>(c, t, l, hb, in) : adj_step<double>(c, t, l, hb, in);
+        if (rc) return rc;
+        in = 1 - in;   // set `in` now holds the adjoints of the state before the step
+        hb = 1 - hb;   // Hb[hb] now holds the adjoint of this step's input history
+        if (t % K == 0) {
+            // input history came from the re-list carry: route it to the
+            // previous list's output history
+            DEM_CUDA_TRY(cudaMemsetAsync(w->Hb[1 - hb], 0, 3 * cap * sizeof(double), s));
+            k_adj_carry<<<148 * 4, kB, 0, s>>>(l.off, c->n, cap, l.carry, w->Hb[hb], w->Hb[1 - hb]);
+            DEM_LAUNCH_CHECK();
+            hb = 1 - hb;
+        }
+    }
+    return DEM_OK;
+}
+
+void reverse_parities(long long every, int K, int& hb, int& in) {
+    for (long long t = every - 1; t >= 0; t--) {
+        in = 1 - in;
+        hb = 1 - hb;
+        if (t % K == 0) hb = 1 - hb;
+    }
+}
+
+// Graphs of one dem_adjoint_window call, indexed by parities at the segment
+// start (recompute: list buffer; reverse sweep: hb, in).
+struct SegmentGraphs {
+    cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    ~SegmentGraphs() {
+        for (auto& row : g)
+            for (cudaGraphExec_t& e : row)
+                if (e) cudaGraphExecDestroy(e);
+    }
+};
+
+// Captures what `enqueue` puts on the stream as a graph (once) and launches it.
+template <typename F> int run_captured(dem_ctx* c, cudaGraphExec_t& ge, F enqueue) {
+    cudaStream_t s = c->stream;
+    if (!ge) {
+        cudaGraph_t gr = nullptr;
+        DEM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue();
+        cudaError_t e = cudaStreamEndCapture(s, &gr);
+        if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (adjoint)", __FILE__, __LINE__);
+        e = cudaGraphInstantiate(&ge, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate (adjoint)", __FILE__, __LINE__);
+    }
+    DEM_CUDA_TRY(cudaGraphLaunch(ge, s));
     return DEM_OK;
 }
 
@@ -573,13 +726,31 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     rc = mixed ? objective<float>(c, which) : objective<double>(c, which);
     if (rc) return rc;
     // ------------------------------------------------------- reverse segments
-    dem_record_forces(c, 1);
+    // Recompute path: the window kernel writing the tape of the bound
+    // particles (PCCP), else per-step kernels with the force record.
+    const bool win_path = c->mode == DEM_FORCE_PCCP && c->win_kernel;
+    if (!win_path) dem_record_forces(c, 1);
     c->observe_slot = -1;   // the recompute writes no observables
     int hb = 0;   // Hb[hb]: adjoint of the pair history output by the step being reversed
+    int in = 0;   // state-adjoint set of the state after the step being reversed
+    SegmentGraphs fgraph, rgraph;
     for (long long g = nseg - 1; g >= 0; g--) {
         if ((rc = restore_ck(c, w->ck[g]))) return rc;
         // recompute the segment, recording what the reverse sweep needs
-        for (long long t = 0; t < every; t++) {
+        if (win_path) {
+            // one graph per list-buffer parity at the segment start (the
+            // capture only records: c->cur is advanced after the launch)
+            const int cur0 = c->cur;
+            rc = run_captured(c, fgraph.g[cur0][0], [&]() {
+                const int r = recompute_segment(c, every);
+                c->cur = cur0;
+                return r;
+            });
+            if (rc) return rc;
+            for (long long t = 0; t < every; t += K) c->cur = 1 - c->cur;
+            c->hph = 0;
+        }
+        for (long long t = 0; !win_path && t < every; t++) {
             const int slot = (int)(t % K);
             if (slot == 0) {
                 c->carry = w->lists[t / K].carry;
@@ -614,24 +785,14 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
             c->dbgT = keepT;
             if (rc) return rc;
         }
-        // reverse sweep
-        for (long long t = every - 1; t >= 0; t--) {
-            const ListRec& l = w->lists[t / K];
-            rc = mixed ? adj_prep<float>(c, t) : adj_prep<double>(c, t);
-            if (rc) return rc;
-            rc = mixed ? adj_pairs<float>(c, t, l, hb) : adj_pairs<double>(c, t, l, hb);
-            if (rc) return rc;
-            hb = 1 - hb;   // Hb[hb] now holds the adjoint of this step's input history
-            if (t % K == 0) {
-                // input history came from the re-list carry: route it to the
-                // previous list's output history
-                DEM_CUDA_TRY(cudaMemsetAsync(w->Hb[1 - hb], 0, 3 * cap * sizeof(double), s));
-                k_adj_carry<<<grid_for(std::max<long long>(l.P, 1), kB), kB, 0, s>>>(l.off, c->n, cap, l.carry,
-                                                                                      w->Hb[hb], w->Hb[1 - hb]);
-                DEM_LAUNCH_CHECK();
-                hb = 1 - hb;
-            }
-        }
+        // reverse sweep: one graph per (hb, in) parity at the segment start
+        const int hb0 = hb, in0 = in;
+        rc = run_captured(c, rgraph.g[hb0][in0], [&]() {
+            int h = hb0, i = in0;
+            return reverse_segment(c, every, h, i);
+        });
+        if (rc) return rc;
+        reverse_parities(every, K, hb, in);
     }
     DEM_CUDA_TRY(cudaEventRecord(c->ev[2], s));
     // ------------------------------------------------------------ results
@@ -678,12 +839,12 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     AdjWork* w = c->adj;
     cudaStreamSynchronize(c->stream);
     for (Ck& k : w->ck) free_ck(k);
-    void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->Xb, w->Db, w->Ab, w->Wb, w->Fb, w->Tb,
-                 w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj};
+    void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1],
+                 w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj};
     for (void* x : p)
         if (x) cudaFree(x);
     for (ListRec& l : w->lists) {
-        void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry};
+        void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry, l.bflag, l.blist, l.flist, l.nb};
         for (void* x : q)
             if (x) cudaFree(x);
     }

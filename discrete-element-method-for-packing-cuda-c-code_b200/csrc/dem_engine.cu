@@ -393,6 +393,15 @@ template <typename Real> struct StepArgs {
     EngineWords* words;
     double *dbgF, *dbgT;
     uint* dbgC;
+    // adjoint tape of the window kernel (tx == nullptr: none): per step, the
+    // state before the step of every bound particle (tx, td, ta: 3 planes of
+    // tnp), its wall history (twh), its total force and torque (tF, tT: xyz
+    // per particle), and every listed pair's history before the step (th: 3
+    // planes of cap); the window's first step is tape step tstep0.
+    double *tx, *td, *twh, *tF, *tT, *th;
+    Real* ta;
+    long long tnp;
+    int tstep0;
 };
 
 // Loads of data that other blocks of the same launch write (the window
@@ -418,13 +427,17 @@ template <bool COH, typename T> __device__ __forceinline__ V3<T> ld3p(Planes3<T>
 // W in place (zero when not touching), wall force and torque in wf[2c],
 // wf[2c+1].
 template <typename Real, bool COH>
-__device__ __forceinline__ void wall_item(const StepArgs<Real>& a, long long c, uint i) {
+__device__ __forceinline__ void wall_item(const StepArgs<Real>& a, long long c, uint i, long long ts = -1) {
     V3<double> x, d;
     V3<Real> av;
     Real r;
     ld_rec<COH>(a.S + i, x, d, av, r);
     const Real m = a.density * (Real)8 * r * r * r;
     V3<double> h = ld3p<COH>(a.W, i);
+    if (ts >= 0) {
+        double* t = a.twh + 3 * a.tnp * ts;
+        t[i] = h.x; t[a.tnp + i] = h.y; t[2 * a.tnp + i] = h.z;
+    }
     V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
     const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, x, cvt<Real>(d), av, r, m, h, a.inv_dt, a.pw, Fw, Tw,
                                         (Real*)nullptr);
@@ -442,8 +455,13 @@ __device__ __forceinline__ void wall_item(const StepArgs<Real>& a, long long c, 
 // u = ru[k], so the gather reads both of a sphere's row ranges directly.
 // .w = 1 marks a contact.
 template <typename Real, bool COH>
-__device__ __forceinline__ void pair_item(const StepArgs<Real>& a, long long k, uint i, uint j, uint rslot) {
+__device__ __forceinline__ void pair_item(const StepArgs<Real>& a, long long k, uint i, uint j, uint rslot,
+                                          long long ts = -1) {
     V3<double> h = mk(ldx<COH>(a.H.x + k), ldx<COH>(a.H.y + k), ldx<COH>(a.H.z + k));
+    if (ts >= 0) {
+        double* t = a.th + 3 * a.cap * ts;
+        t[k] = h.x; t[a.cap + k] = h.y; t[2 * a.cap + k] = h.z;
+    }
     V3<double> xi, di, xj, dj;
     V3<Real> ai, aj;
     Real ri, rj;
@@ -638,12 +656,18 @@ __device__ __forceinline__ void clear_partials(StepPartials part, size_t from, s
 template <typename Real, bool COH>
 __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const ParticleCommon& pc, uint i, Real r, uint ws,
                                            uint total, uint o0, uint o1, uint r0, uint r1, double& mz, uint& cnt,
-                                           uint& flags) {
+                                           uint& flags, long long ts = -1) {
     V3<double> x, d;
     V3<Real> av;
     Real rr;
     ld_rec<COH>(a.S + i, x, d, av, rr);
     const float4 q = ldx<COH>(a.Q + i);
+    if (ts >= 0) {   // state before the step
+        const long long np = a.tnp, o = 3 * np * ts;
+        a.tx[o + i] = x.x; a.tx[o + np + i] = x.y; a.tx[o + 2 * np + i] = x.z;
+        a.td[o + i] = d.x; a.td[o + np + i] = d.y; a.td[o + 2 * np + i] = d.z;
+        a.ta[o + i] = av.x; a.ta[o + np + i] = av.y; a.ta[o + 2 * np + i] = av.z;
+    }
     V3<Real> F = zero3<Real>(), T = zero3<Real>();
     if ((long long)total <= a.cap) {
         for (uint k = o0; k < o1; k++) {
@@ -670,6 +694,12 @@ __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const Partic
         const R4<Real> fw = ld4<COH>(a.wf + 2 * ws), tw = ld4<COH>(a.wf + 2 * ws + 1);
         F.x += fw.x; F.y += fw.y; F.z += fw.z;
         T.x += tw.x; T.y += tw.y; T.z += tw.z;
+    }
+    if (ts >= 0) {   // total force and torque of the step
+        double* f = a.tF + 3 * a.tnp * ts;
+        double* t = a.tT + 3 * a.tnp * ts;
+        f[3 * i] = F.x; f[3 * i + 1] = F.y; f[3 * i + 2] = F.z;
+        t[3 * i] = T.x; t[3 * i + 1] = T.y; t[3 * i + 2] = T.z;
     }
     particle_finish<Real, false>(i, F, T, r, x, d, av, q, a.S, a.Q, a.W, a.pw, pc, a.dtr, a.inv_dt, a.density, mz,
                                  flags, cnt, a.dbgF, a.dbgT, a.dbgC);
@@ -832,12 +862,13 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
     uint cnt = 0, flags = 0;
     ParticleCommon pc = a.pc;
     for (int s = 0; s < K; s++) {
+        const long long ts = a.tx ? (long long)a.tstep0 + s : -1ll;
         // phase 1: wall and pair items
         for (long long u = tid; u < items; u += nthr) {
             uint i = i0, j = j0, rslot = s0;
             if (u != tid) item_indices(a, u, nw, items, i, j, rslot);
-            if (u < (long long)nw) wall_item<Real, true>(a, u, i);
-            else pair_item<Real, true>(a, u - nw, i, j, rslot);
+            if (u < (long long)nw) wall_item<Real, true>(a, u, i, ts);
+            else pair_item<Real, true>(a, u - nw, i, j, rslot, ts);
         }
         grid_barrier(bar, nbar++, a.words);
         // phase 2: bound particles; this step's share of the free particles
@@ -847,11 +878,11 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
             double mzi = 0.0;
             uint ci = 0;
             if (t == tid) {
-                bound_item<Real, true>(a, pc, b0, rb0, ws0, total, o00, o10, r00, r10, mzi, ci, flags);
+                bound_item<Real, true>(a, pc, b0, rb0, ws0, total, o00, o10, r00, r10, mzi, ci, flags, ts);
             } else {
                 const uint i = a.blist[t];
                 bound_item<Real, true>(a, pc, i, a.R[i], a.wslot[i], total, a.off[i], a.off[i + 1], a.roff[i],
-                                       a.roff[i + 1], mzi, ci, flags);
+                                       a.roff[i + 1], mzi, ci, flags, ts);
             }
             if (s == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
         }
@@ -1085,6 +1116,10 @@ template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int
     a.dbgF = c->record ? c->dbgF : nullptr;
     a.dbgT = c->record ? c->dbgT : nullptr;
     a.dbgC = c->record ? c->dbgC : nullptr;
+    a.tx = a.td = a.twh = a.tF = a.tT = a.th = nullptr;
+    a.ta = nullptr;
+    a.tnp = np;
+    a.tstep0 = 0;
     return a;
 }
 
@@ -1113,12 +1148,17 @@ template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nst
 }
 
 // The window kernel: all K steps of the window in one cooperative launch.
-template <typename Real> int launch_window(dem_ctx* c, int lst) {
+template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape* tape) {
     const int K = c->cfg.relist_interval;
     DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, sizeof(uint), c->stream));   // arrival counter
     StepArgs<Real> a = step_args<Real>(c, lst, 0);
     a.dbgF = a.dbgT = nullptr;
     a.dbgC = nullptr;
+    if (tape) {
+        a.tx = tape->tx; a.td = tape->td; a.twh = tape->twh; a.tF = tape->tF; a.tT = tape->tT; a.th = tape->th;
+        a.ta = (Real*)tape->ta;
+        a.tstep0 = tape->step0;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->win_grid);
     cfg.blockDim = dim3(kWinThreads);
@@ -1151,6 +1191,10 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
 }  // namespace
 
 namespace dem {
+int window_kernel(dem_ctx* c, int lst, const WindowTape* tape) {
+    return c->prec == DEM_PREC_MIXED ? launch_window<float>(c, lst, tape) : launch_window<double>(c, lst, tape);
+}
+
 int relist(dem_ctx* c, int src) {
     return c->prec == DEM_PREC_MIXED ? launch_relist<float>(c, src) : launch_relist<double>(c, src);
 }
@@ -1211,7 +1255,7 @@ int enqueue_window(dem_ctx* c, int src) {
     const bool mixed = c->prec == DEM_PREC_MIXED;
     if (c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel) {
         // every step of the window in one cooperative launch
-        rc = mixed ? launch_window<float>(c, lst) : launch_window<double>(c, lst);
+        rc = mixed ? launch_window<float>(c, lst, nullptr) : launch_window<double>(c, lst, nullptr);
         if (rc) return rc;
         if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2], c->stream, cudaEventRecordExternal));
         c->wtiming_path = 1;

@@ -94,6 +94,14 @@ struct GridC {
 
 struct StepPartials { unsigned long long* maxhz_bits; uint* contacts; };
 
+// Tape written by the window kernel for the adjoint's recompute (see
+// StepArgs in dem_engine.cu); ta is Real.
+struct WindowTape {
+    double *tx, *td, *twh, *tF, *tT, *th;
+    void* ta;
+    int step0;
+};
+
 struct ParticleCommon {
     double dt, hx, hy;
     float half_skin2;
@@ -220,8 +228,11 @@ namespace dem {
 // carrying history from list buffer `src` into 1-src; when c->carry is set,
 // carry[k] receives the previous slot of new pair k (kEmpty if new).
 // step_kernels(): one DEM step on list buffer `lst`, window slot `slot`.
+// window_kernel(): all steps of a window on list buffer `lst` (PCCP, window
+// kernel enabled), optionally writing the adjoint tape.
 int relist(dem_ctx* c, int src);
 int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part);
+int window_kernel(dem_ctx* c, int lst, const WindowTape* tape);
 template <typename Real> Planes3<Real> planes(void* base, long long npad) {
     Real* b = (Real*)base;
     return Planes3<Real>{b, b + npad, b + 2 * npad};

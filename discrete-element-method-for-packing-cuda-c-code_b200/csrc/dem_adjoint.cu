@@ -15,7 +15,7 @@
 //      and every re-list's list, carry map and bound/free lists; one CUDA
 //      graph per segment); then sweep the steps backwards (one CUDA graph
 //      per segment):
-//        k_adj_free   free particles of the window: integrator reverse only
+//        k_adj_free_window  free particles: the window's steps in closed form
 //        k_adj_step   bound particles: integrator reverse + pair + wall VJP
 //                     (dem_law_adj.cuh), particle-parallel: each particle
 //                     evaluates the reverse of all its pairs and keeps its
@@ -246,27 +246,26 @@ struct AdjList {
     const uint *off, *ln, *lp, *roff, *rk;
 };
 
-// One reversed step of the window's free particles (flist[t], t < n - nb):
-// they feel their weight only, so the step is the integrator reverse; their
-// wall-history adjoint is zero.
-template <typename Real>
-__global__ void k_adj_free(long long n, long long np, const uint* __restrict__ flist, const uint* __restrict__ nbp,
-                           const Real* __restrict__ R, double dt, double density, const double* __restrict__ Xa,
-                           const double* __restrict__ Da, const double* __restrict__ Aa, double* __restrict__ Xo,
-                           double* __restrict__ Do, double* __restrict__ Ao, double* __restrict__ Wb,
-                           double* __restrict__ Rb) {
+// The window's free particles (flist[t], t < n - nb), all K steps of the
+// window reversed at once.  A free particle feels its weight only: per step
+// d' = d - g dt^2 and x' = x + d', so the reverse keeps the position and
+// rotation adjoints and adds the position adjoint to the displacement adjoint
+// once per step (d_bar += K x_bar); no parameter or radius depends on it
+// (F/m = -g) and its wall-history adjoint is zero.  No bound particle reads a
+// free particle's adjoints inside the window, so they are read from set `in`
+// at the window's end and written to the set current after its K reversed
+// steps.
+__global__ void k_adj_free_window(long long n, long long np, int K, const uint* __restrict__ flist,
+                                  const uint* __restrict__ nbp, const double* Xi, const double* Di, const double* Ai,
+                                  double* Xo, double* Do, double* Ao, double* __restrict__ Wb) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n - (long long)*nbp) return;
     const long long i = flist[t];
-    const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
-    V3d dtot, fb, tb;
-    double rb = 0.0;
-    integ_rev<Real>(R[i], false, nullptr, nullptr, i, dt, density, xa, ld3(Da, np, i), aa, dtot, fb, tb, rb);
-    st3(Xo, np, i, xa);
-    st3(Do, np, i, dtot);
-    st3(Ao, np, i, aa);
+    const V3d xb = ld3(Xi, np, i), db = ld3(Di, np, i), ab = ld3(Ai, np, i);
+    st3(Xo, np, i, xb);
+    st3(Do, np, i, db + (double)K * xb);
+    st3(Ao, np, i, ab);
     st3(Wb, np, i, zero3<double>());
-    Rb[i] += rb;
 }
 
 // One reversed step of the window's bound particles (blist[u], u < nb),
@@ -523,17 +522,12 @@ __global__ void k_obj_potential(long long n, long long np, long long cap, AdjLis
     }
 }
 
-// Reversed step t of the segment: state adjoints read from set `in` (after
-// the step), written to set 1 - in (before the step); free particles by
-// k_adj_free, bound ones by k_adj_step.
+// Reversed step t of the segment for the bound particles: state adjoints
+// read from set `in` (after the step), written to set 1 - in (before it).
 template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l, int hb, int in) {
     AdjWork* w = c->adj;
     const long long np = c->npad, cap = c->cap;
     AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
-    k_adj_free<Real><<<grid_for(c->n, kB), kB, 0, c->stream>>>(
-        c->n, np, l.flist, l.nb, (const Real*)c->rad, c->cfg.dt, c->cfg.density, w->Xb2[in], w->Db2[in], w->Ab2[in],
-        w->Xb2[1 - in], w->Db2[1 - in], w->Ab2[1 - in], w->Wb, w->Rb);
-    DEM_LAUNCH_CHECK();
     k_adj_step<Real><<<(unsigned)w->npb, kPairB, 0, c->stream>>>(
         c->n, np, cap, L, l.blist, l.nb, w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t,
         w->twh + 3 * np * t, w->th + 3 * cap * t, w->tF + 3 * np * t, w->tT + 3 * np * t, (const Real*)c->rad,
@@ -622,8 +616,16 @@ int reverse_segment(dem_ctx* c, long long every, int& hb, int& in) {
     const bool mixed = c->prec == DEM_PREC_MIXED;
     cudaStream_t s = c->stream;
     int rc;
+    const long long np = c->npad;
     for (long long t = every - 1; t >= 0; t--) {
         const ListRec& l = w->lists[t / K];
+        if (t % K == K - 1) {   // the window's free particles, all its steps at once
+            const int out = (K & 1) ? 1 - in : in;
+            k_adj_free_window<<<grid_for(c->n, kB), kB, 0, s>>>(c->n, np, K, l.flist, l.nb, w->Xb2[in], w->Db2[in],
+                                                                w->Ab2[in], w->Xb2[out], w->Db2[out], w->Ab2[out],
+                                                                w->Wb);
+            DEM_LAUNCH_CHECK();
+        }
         rc = mixed ? adj_step<float>(c, t, l, hb, in) : adj_step<double>(c, t, l, hb, in);
         if (rc) return rc;
         in = 1 - in;   // set `in` now holds the adjoints of the state before the step

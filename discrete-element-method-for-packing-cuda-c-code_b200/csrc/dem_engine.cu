@@ -381,7 +381,7 @@ __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double
 // particles) and of the window kernel that runs all of a window's steps.
 template <typename Real> struct StepArgs {
     long long n, cap;
-    const uint *off, *lp, *ln, *ru, *roff, *wlist, *wcount, *wslot, *bpos, *blist, *flist;
+    const uint *off, *lp, *ln, *ru, *roff, *rk, *wlist, *wcount, *wslot, *bpos, *blist, *flist;
     PRec<Real>* S;                // particle records (in place)
     Planes3<double> W, H;         // wall history, pair history (in place)
     const Real* R;
@@ -736,12 +736,13 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(StepArgs<Re
 // per-step arithmetic of particle_finish.  mz_obs receives the height after
 // step observe_slot (if in range).
 template <typename Real>
-__device__ __forceinline__ void free_item(const StepArgs<Real>& a, uint i, int slot0, int nsteps, int observe_slot,
-                                          bool rec, double& mz_obs, uint& flags) {
+__device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Real>* Sin, PRec<Real>* Sout, uint i,
+                                          int slot0, int nsteps, int observe_slot, bool rec, double& mz_obs,
+                                          uint& flags) {
     V3<double> x, d;
     V3<Real> av;
     Real r;
-    ld_rec<false>(a.S + i, x, d, av, r);
+    ld_rec<false>(Sin + i, x, d, av, r);
     float4 q = a.Q[i];
     const Real m = sphere_mass(a.density, r);
     const Real I = (Real)0.4 * m * (r * r);
@@ -758,7 +759,7 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, uint i, int s
         integrate<Real>(F, T, m, I, a.pc.dt, a.dtr, a.pc.half_skin2, x, d, av, q, flags, mz);
         if (s == observe_slot) mz_obs = mz;
     }
-    st_rec(a.S + i, x, d, av, r);
+    st_rec(Sout + i, x, d, av, r);
     a.Q[i] = q;
 }
 
@@ -770,7 +771,8 @@ __global__ void __launch_bounds__(256) k_free_run(StepArgs<Real> a, int slot0, i
     double mz_obs = 0.0;
     uint flags = 0;
     if (t < a.n - (long long)a.bpos[a.n])
-        free_item<Real>(a, a.flist[t], slot0, nsteps, observe_slot, a.dbgF != nullptr && nsteps == 1, mz_obs, flags);
+        free_item<Real>(a, a.S, a.S, a.flist[t], slot0, nsteps, observe_slot, a.dbgF != nullptr && nsteps == 1, mz_obs,
+                        flags);
     const int observe = observe_slot >= slot0 && observe_slot < slot0 + nsteps;
     block_observables(mz_obs, 0u, flags, observe, part, a.words);
     if (observe) clear_partials(part, clr0, clr1);
@@ -889,7 +891,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
         const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
         for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
             double mzi = 0.0;
-            free_item<Real>(a, a.flist[t], 0, K, K - 1, false, mzi, flags);
+            free_item<Real>(a, a.S, a.S, a.flist[t], 0, K, K - 1, false, mzi, flags);
             mz = fmax(mz, mzi);
         }
         if (s < K - 1) grid_barrier(bar, nbar++, a.words);
@@ -900,10 +902,55 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
 
 // PP (particle-parallel, the paper's Figure 1(b)): each particle evaluates all
 // of its pairs itself -- its own row (it is lo) and its reverse row (it is hi)
-// -- so one kernel does the whole step.  Each pair is evaluated by both of its
+// -- and its walls, then integrates.  Each pair is evaluated by both of its
 // particles with the same arguments in the same order, so the two results are
 // bit-identical; only lo writes the pair's new history.  State and history
 // are read from the "in" buffers and written to the "out" buffers (ping-pong).
+template <typename Real, bool COH>
+__device__ __forceinline__ void pp_item(long long i, Real r, uint total, uint o0, uint o1, uint r0, uint r1,
+                                        const uint* __restrict__ rk, const uint* __restrict__ lp,
+                                        const uint* __restrict__ ln, long long cap, const PRec<Real>* Si, PRec<Real>* So,
+                                        float4* Q, Planes3<double> W, Planes3<double> Hi, Planes3<double> Ho,
+                                        const LawParams<Real>& pp, const LawParams<Real>& pw, const ParticleCommon& pc,
+                                        Real dtr, Real inv_dt, Real density, double& mz, uint& cnt, uint& flags,
+                                        double* dbgF, double* dbgT, uint* dbgC) {
+    V3<double> x, d;
+    V3<Real> a;
+    Real rr;
+    ld_rec<COH>(Si + i, x, d, a, rr);
+    const float4 q = ldx<COH>(Q + i);
+    V3<Real> F = zero3<Real>(), T = zero3<Real>();
+    if ((long long)total <= cap) {
+        for (uint k = o0; k < o1; k++) {
+            const uint j = ln[k];
+            V3<double> h = mk(ldx<COH>(Hi.x + k), ldx<COH>(Hi.y + k), ldx<COH>(Hi.z + k));
+            V3<double> xj, dj;
+            V3<Real> aj;
+            Real rj;
+            ld_rec<COH>(Si + j, xj, dj, aj, rj);
+            V3<Real> Fl, Tl, Th;
+            const int c = pair_eval<Real>(x, xj, d, dj, a, aj, r, rj, h, pp, inv_dt, density, Fl, Tl, Th);
+            Ho.x[k] = h.x; Ho.y[k] = h.y; Ho.z[k] = h.z;
+            if (c) { F += Fl; T += Tl; cnt++; }
+        }
+        for (uint u = r0; u < r1; u++) {
+            const uint k = rk[u];
+            if (k >= total) continue;
+            const uint j = lp[k];
+            V3<double> h = mk(ldx<COH>(Hi.x + k), ldx<COH>(Hi.y + k), ldx<COH>(Hi.z + k));
+            V3<double> xj, dj;
+            V3<Real> aj;
+            Real rj;
+            ld_rec<COH>(Si + j, xj, dj, aj, rj);
+            V3<Real> Fl, Tl, Th;
+            const int c = pair_eval<Real>(xj, x, dj, d, aj, a, rj, r, h, pp, inv_dt, density, Fl, Tl, Th);
+            if (c) { F -= Fl; T += Th; cnt++; }
+        }
+    }
+    particle_finish<Real, true>(i, F, T, r, x, d, a, q, So, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt, dbgF,
+                                dbgT, dbgC);
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     long long n, const uint* __restrict__ off, const uint* __restrict__ roff, const uint* __restrict__ rk,
@@ -924,45 +971,71 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
         o0 = off[i]; o1 = off[i + 1]; r0 = roff[i]; r1 = roff[i + 1];
     }
     pdl_wait();
-    if (i < n) {
-        V3<double> x, d;
-        V3<Real> a;
-        Real rr;
-        ld_rec<false>(Si + i, x, d, a, rr);
-        const float4 q = Q[i];
-        V3<Real> F = zero3<Real>(), T = zero3<Real>();
-        if ((long long)total <= cap) {
-            for (uint k = o0; k < o1; k++) {
-                const uint j = ln[k];
-                V3<double> h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
-                V3<double> xj, dj;
-                V3<Real> aj;
-                Real rj;
-                ld_rec<false>(Si + j, xj, dj, aj, rj);
-                V3<Real> Fl, Tl, Th;
-                const int c = pair_eval<Real>(x, xj, d, dj, a, aj, r, rj, h, pp, inv_dt, density, Fl, Tl, Th);
-                Ho.x[k] = h.x; Ho.y[k] = h.y; Ho.z[k] = h.z;
-                if (c) { F += Fl; T += Tl; cnt++; }
-            }
-            for (uint u = r0; u < r1; u++) {
-                const uint k = rk[u];
-                if (k >= total) continue;
-                const uint j = lp[k];
-                V3<double> h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
-                V3<double> xj, dj;
-                V3<Real> aj;
-                Real rj;
-                ld_rec<false>(Si + j, xj, dj, aj, rj);
-                V3<Real> Fl, Tl, Th;
-                const int c = pair_eval<Real>(xj, x, dj, d, aj, a, rj, r, h, pp, inv_dt, density, Fl, Tl, Th);
-                if (c) { F -= Fl; T += Th; cnt++; }
-            }
-        }
-        particle_finish<Real, true>(i, F, T, r, x, d, a, q, So, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, cnt,
-                                    dbgF, dbgT, dbgC);
-    }
+    if (i < n)
+        pp_item<Real, false>(i, r, total, o0, o1, r0, r1, rk, lp, ln, cap, Si, So, Q, W, Hi, Ho, pp, pw, pc, dtr, inv_dt,
+                             density, mz, cnt, flags, dbgF, dbgT, dbgC);
     block_observables(mz, cnt, flags, pc.observe, part, words);
     if (pc.observe) clear_partials(part, clr0, clr1);
+}
+
+// PP window kernel (one cooperative launch per window, as k_window): per
+// step, every bound particle runs pp_item from the "in" buffers into the
+// "out" buffers, and 1/K of the free particles run all K steps in registers
+// (read from the window's first state buffer, written to its last); one grid
+// barrier per step, then the buffers swap.  Same device functions as the
+// per-step PP kernel, so the states are bit-identical.
+template <typename Real>
+__global__ void __launch_bounds__(kWinThreads, 1) k_window_pp(StepArgs<Real> a, PRec<Real>* S0, PRec<Real>* S1,
+                                                              Planes3<double> H0, Planes3<double> H1, int K,
+                                                              StepPartials part, size_t npart, uint* bar) {
+    const long long nthr = (long long)gridDim.x * blockDim.x;
+    const long long tid =
+        ((long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x) * 32 + (threadIdx.x & 31);
+    uint nbar = 0;
+    const uint total = a.off[a.n];
+    const long long nb = a.bpos[a.n], nf = a.n - nb;
+    // this thread's first bound particle: list data kept in registers
+    uint b0 = 0, o00 = 0, o10 = 0, r00 = 0, r10 = 0;
+    Real rb0 = (Real)0;
+    if (tid < nb) {
+        b0 = a.blist[tid];
+        rb0 = a.R[b0];
+        o00 = a.off[b0]; o10 = a.off[b0 + 1]; r00 = a.roff[b0]; r10 = a.roff[b0 + 1];
+    }
+    PRec<Real>* Sf = (K & 1) ? S1 : S0;   // the free particles' final buffer
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    ParticleCommon pc = a.pc;
+    for (int s = 0; s < K; s++) {
+        PRec<Real>* Si = (s & 1) ? S1 : S0;
+        PRec<Real>* So = (s & 1) ? S0 : S1;
+        const Planes3<double> Hi = (s & 1) ? H1 : H0, Ho = (s & 1) ? H0 : H1;
+        pc.first = s == 0 ? 1 : 0;
+        for (long long t = tid; t < nb; t += nthr) {
+            double mzi = 0.0;
+            uint ci = 0;
+            if (t == tid) {
+                pp_item<Real, true>(b0, rb0, total, o00, o10, r00, r10, a.rk, a.lp, a.ln, a.cap, Si, So, a.Q, a.W, Hi,
+                                    Ho, a.pp, a.pw, pc, a.dtr, a.inv_dt, a.density, mzi, ci, flags, nullptr, nullptr,
+                                    nullptr);
+            } else {
+                const uint i = a.blist[t];
+                pp_item<Real, true>(i, a.R[i], total, a.off[i], a.off[i + 1], a.roff[i], a.roff[i + 1], a.rk, a.lp,
+                                    a.ln, a.cap, Si, So, a.Q, a.W, Hi, Ho, a.pp, a.pw, pc, a.dtr, a.inv_dt, a.density,
+                                    mzi, ci, flags, nullptr, nullptr, nullptr);
+            }
+            if (s == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
+        }
+        const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
+        for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
+            double mzi = 0.0;
+            free_item<Real>(a, S0, Sf, a.flist[t], 0, K, K - 1, false, mzi, flags);
+            mz = fmax(mz, mzi);
+        }
+        if (s < K - 1) grid_barrier(bar, nbar++, a.words);
+    }
+    block_observables(mz, cnt, flags, 1, part, a.words);
+    clear_partials(part, gridDim.x, npart);
 }
 
 __global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned long long* out) {
@@ -1096,7 +1169,7 @@ template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int
     StepArgs<Real> a;
     a.n = c->n;
     a.cap = c->cap;
-    a.off = c->off[lst]; a.lp = c->lp; a.ln = c->ln[lst]; a.ru = c->ru; a.roff = c->roff;
+    a.off = c->off[lst]; a.lp = c->lp; a.ln = c->ln[lst]; a.ru = c->ru; a.roff = c->roff; a.rk = c->rk;
     a.wlist = c->wlist; a.wcount = c->wcount; a.wslot = c->wslot;
     a.bpos = c->bpos; a.blist = c->blist; a.flist = c->flist;
     a.S = (PRec<Real>*)c->rec[0];
@@ -1169,6 +1242,29 @@ template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape
     cfg.attrs = at;
     cfg.numAttrs = 1;
     DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window<Real>, a, K, partials(c, K - 1), c->npart, c->bar));
+    return DEM_OK;
+}
+
+// PP window kernel: state buffer sb and history phase hp at the window start.
+template <typename Real> int launch_window_pp(dem_ctx* c, int lst, int sb, int hp) {
+    const int K = c->cfg.relist_interval;
+    DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, sizeof(uint), c->stream));   // arrival counter
+    StepArgs<Real> a = step_args<Real>(c, lst, 0);
+    a.dbgF = a.dbgT = nullptr;
+    a.dbgC = nullptr;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c->win_grid);
+    cfg.blockDim = dim3(kWinThreads);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window_pp<Real>, a, (PRec<Real>*)c->rec[sb], (PRec<Real>*)c->rec[1 - sb],
+                                    planes<double>(c->hist[lst][hp], c->cap),
+                                    planes<double>(c->hist[lst][1 - hp], c->cap), K, partials(c, K - 1), c->npart,
+                                    c->bar));
     return DEM_OK;
 }
 
@@ -1256,6 +1352,15 @@ int enqueue_window(dem_ctx* c, int src) {
     if (c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel) {
         // every step of the window in one cooperative launch
         rc = mixed ? launch_window<float>(c, lst, nullptr) : launch_window<double>(c, lst, nullptr);
+        if (rc) return rc;
+        if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2], c->stream, cudaEventRecordExternal));
+        c->wtiming_path = 1;
+        return DEM_OK;
+    }
+    if (c->mode == DEM_FORCE_PP && !c->record && c->win_kernel) {
+        // PP: every step of the window in one cooperative launch
+        rc = mixed ? launch_window_pp<float>(c, lst, c->sbuf, c->hph)
+                   : launch_window_pp<double>(c, lst, c->sbuf, c->hph);
         if (rc) return rc;
         if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2], c->stream, cudaEventRecordExternal));
         c->wtiming_path = 1;
@@ -1396,8 +1501,13 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         if (e != cudaSuccess) return bail(cuda_fail(e, "pair kernel occupancy", __FILE__, __LINE__));
         c->pair_grid = (unsigned)std::max(1, nsm * std::max(per, 1));
         int wper = 0;   // the window kernel: every block co-resident (cooperative launch)
-        e = c->prec == DEM_PREC_MIXED ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<float>, kWinThreads, 0)
-                                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<double>, kWinThreads, 0);
+        const bool mx = c->prec == DEM_PREC_MIXED;
+        if (c->mode == DEM_FORCE_PP)
+            e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window_pp<float>, kWinThreads, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window_pp<double>, kWinThreads, 0);
+        else
+            e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<float>, kWinThreads, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<double>, kWinThreads, 0);
         if (e != cudaSuccess) return bail(cuda_fail(e, "window kernel occupancy", __FILE__, __LINE__));
         int coop = 0;
         e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);

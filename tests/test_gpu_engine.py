@@ -274,20 +274,23 @@ def test_window_timing_graphs_equal_plain_graphs(dem, wl, cuda):
         np.testing.assert_array_equal(x, y)
 
 
+@pytest.mark.parametrize("mode", ["pccp", "pp"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_window_kernel_equals_per_step_kernels(dem, wl, cuda, monkeypatch, prec):
+def test_window_kernel_equals_per_step_kernels(dem, wl, cuda, monkeypatch, prec, mode):
     """Whole windows as one cooperative launch (the default) and as per-step
-    pair / particle kernels with the forked free-particle kernel
-    (DEM_B200_WINDOW=0) agree bit for bit, dense bed included."""
+    kernels (DEM_B200_WINDOW=0: PCCP pair / particle kernels with the forked
+    free-particle kernel, or the PP step kernel) agree bit for bit, dense bed
+    included."""
     from _cases import dense_lattice
+    fm = dem.FORCE_PCCP if mode == "pccp" else dem.FORCE_PP
     for w in (wl.small_box(n=3000), dense_lattice(dem, nx=8, ny=8, nz=6)):
         p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
         rng = np.random.default_rng(3)
         pdis = rng.normal(0, 2e-6, 3 * w.n)
-        a = make_engine(dem, w, p)
+        a = make_engine(dem, w, p, force_mode=fm)
         a.upload(w.pos, w.rad, pdis, None)
         monkeypatch.setenv("DEM_B200_WINDOW", "0")
-        b = make_engine(dem, w, p)
+        b = make_engine(dem, w, p, force_mode=fm)
         b.upload(w.pos, w.rad, pdis, None)
         monkeypatch.delenv("DEM_B200_WINDOW")
         a.step(3 * w.relist_interval)

@@ -129,9 +129,17 @@ __global__ void k_hash_count(long long n, const PRec<Real>* __restrict__ S, Grid
         const double x = p.x, y = p.y, z = p.z;
         const double mg = (double)R[i] + half_skin;
         const bool near = (z < mg) || (x + hx < mg) || (hx - x < mg) || (y + hy < mg) || (hy - y < mg);
+        // one atomic per warp for its candidates (slot order within a warp
+        // follows the lanes; the slots only name the candidates)
+        const uint act = __activemask();
+        const uint m = __ballot_sync(act, near);
+        uint base = 0;
+        const int lead = __ffs(act) - 1;
+        if ((int)lane_id() == lead && m) base = atomicAdd(wcount, (uint)__popc(m));
+        base = __shfl_sync(act, base, lead);
         uint ws = kEmpty;
         if (near) {
-            ws = atomicAdd(wcount, 1u);
+            ws = base + (uint)__popc(m & ((1u << lane_id()) - 1u));
             wlist[ws] = (uint)i;
         }
         wslot[i] = ws;
@@ -176,7 +184,7 @@ __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint*
 template <typename Real>
 __global__ void k_rank(long long n, const uint* __restrict__ cstart, const uint* __restrict__ sidu,
                        const uint* __restrict__ skeyu, const R4<Real>* __restrict__ sposu, uint* __restrict__ sid2,
-                       uint* __restrict__ skey, R4<Real>* __restrict__ spos) {
+                       uint* __restrict__ skey, R4<Real>* __restrict__ spos, uint* __restrict__ tpos) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const uint i = sidu[t];
@@ -187,6 +195,7 @@ __global__ void k_rank(long long n, const uint* __restrict__ cstart, const uint*
     sid2[s + rank] = i;
     skey[s + rank] = c;
     spos[s + rank] = sposu[t];
+    tpos[i] = s + rank;
 }
 
 // Walk the 27 cells around sorted slot t and either count (FILL=false) or
@@ -233,7 +242,7 @@ __device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, 
 
 // The re-list walk: per sorted slot t, count the candidates j > i (row of i)
 // and j < i (reverse row of i) and keep the first kScr j > i candidates in
-// scr[t * kScr ...]; rows longer than kScr are walked again by the fill.
+// scr[i * kScr ...]; rows longer than kScr are walked again by the fill.
 // A particle with any candidate or a wall candidacy is BOUND for the window
 // (bflag = 1), otherwise FREE.
 constexpr uint kScr = 8;
@@ -248,7 +257,7 @@ __global__ void k_nbr_walk(long long n, const uint* __restrict__ sid2, const R4<
     if (t < n) {
         const uint i = sid2[t];
         uint nup;
-        walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, scr + (size_t)t * kScr,
+        walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, scr + (size_t)i * kScr,
                            kScr);
         njgi[i] = nup;
         njli[i] = nall - nup;
@@ -277,24 +286,27 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
                            const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
                            uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
                            uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,
-                           const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist) {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+                           const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist,
+                           const uint* __restrict__ tpos) {
+    const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // particle order
+    if (ii >= n) return;
+    const uint i = (uint)ii;
     {   // bound / free lists, ascending particle id
-        const uint i = sid2[t], b = bpos[i];
+        const uint b = bpos[i];
         if (bflag[i]) blist[b] = i;
         else flist[i - b] = i;
     }
     const uint total = off[n];
     if ((long long)total > cap) {
-        if (t == 0) atomicOr(&words->status, kStCapacity);
+        if (i == 0) atomicOr(&words->status, kStCapacity);
         return;
     }
-    const uint i = sid2[t];
     const uint b = off[i], e = off[i + 1];
+    if (e == b) return;
     if (e - b <= kScr) {
-        for (uint k = 0; k < e - b; k++) ln[b + k] = scr[(size_t)t * kScr + k];
-    } else {
+        for (uint k = 0; k < e - b; k++) ln[b + k] = scr[(size_t)i * kScr + k];
+    } else {   // a long row: walk again from the particle's sorted slot
+        const uint t = tpos[i];
         uint nup, nall;
         walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
     }
@@ -1136,7 +1148,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->arrival, c->cstart, c->ccount, S, (const Real*)c->rad,
                                                  g, c->sid, c->skeyu, (R4<Real>*)c->sposu);
     k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->cstart, c->sid, c->skeyu, (const R4<Real>*)c->sposu, c->sid2,
-                                              c->skey, (R4<Real>*)c->spos);
+                                              c->skey, (R4<Real>*)c->spos, c->tpos);
     const Real skin = (Real)c->cfg.skin;
     k_nbr_walk<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin,
                                                   c->wslot, c->njgi, c->njli, c->bflag, c->scr, c->words);
@@ -1151,7 +1163,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
         c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
         planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry, c->scr,
-        c->bflag, c->bpos, c->blist, c->flist);
+        c->bflag, c->bpos, c->blist, c->flist, c->tpos);
     k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->ru, c->off[dst], c->cap);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
@@ -1478,7 +1490,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
         (rc = dalloc(&c->wcount, 1)) || (rc = dalloc(&c->arrival, np)) || (rc = dalloc(&c->scr, np * kScr)) ||
         (rc = dalloc(&c->bflag, np)) || (rc = dalloc(&c->bpos, np + 1)) || (rc = dalloc(&c->blist, np)) ||
-        (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, 64)))
+        (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, 64)) || (rc = dalloc(&c->tpos, np)))
         return bail(rc);
     e = cudaMalloc(&c->wf, 2 * np * 4 * rs);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (wall forces)", __FILE__, __LINE__));
@@ -1561,7 +1573,8 @@ int dem_destroy(dem_ctx* c) {
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
-                    c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar};
+                    c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar,
+                    c->tpos};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);

@@ -152,7 +152,8 @@ struct dem_ctx {
     uint* njgi = nullptr;
     uint* njli = nullptr;
     uint* arrival = nullptr; // per particle: slot among its cell's members (hash order)
-    uint* scr = nullptr;     // per sorted slot: the walk's first kScr row candidates
+    uint* scr = nullptr;     // per particle: the walk's first kScr row candidates
+    uint* tpos = nullptr;    // per particle: its slot in the cell-sorted order
     uint* bflag = nullptr;   // per particle: 1 = bound this window (a listed pair or a wall candidacy)
     uint* bpos = nullptr;    // exclusive scan of bflag; bpos[n] = number of bound particles
     uint* blist = nullptr;   // bound particle ids, ascending

@@ -185,6 +185,11 @@ _SIGS = [
     ("dem_write_preflow", ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
                                          _vp, _vp, _vp]),
     ("dem_write_timesteps", ctypes.c_int, [ctypes.c_char_p, ctypes.c_double, ctypes.c_longlong]),
+    ("dem_read_preflow", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _vp, _vp,
+                                        _vp, ctypes.c_longlong]),
+    ("dem_save_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("dem_load_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("dem_write_finish", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p]),
 ]
 
@@ -487,6 +492,12 @@ class Engine:
         check(lib().dem_kernel_times(self._h, out), "dem_kernel_times")
         return {"relist_ms": out[0], "pair_ms": out[1], "particle_ms": out[2]}
 
+    def save_state(self, path):
+        check(lib().dem_save_state(self._h, str(path).encode()), "dem_save_state")
+
+    def load_state(self, path):
+        check(lib().dem_load_state(self._h, str(path).encode()), "dem_load_state")
+
     def set_window_timing(self, on=True):
         check(lib().dem_set_window_timing(self._h, 1 if on else 0), "dem_set_window_timing")
 
@@ -531,6 +542,16 @@ def gen_rsa(world, rad, seed):
     pos = np.empty(3 * rad.size)
     check(lib().dem_gen_rsa(int(rad.size), _d3(world), _ptr(rad), int(seed), _ptr(pos)), "dem_gen_rsa")
     return pos
+
+
+def read_preflow(path):
+    it, n, itime = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    check(lib().dem_read_preflow(str(path).encode(), ctypes.byref(it), ctypes.byref(n), ctypes.byref(itime), None,
+                                 None, None, 0), "dem_read_preflow")
+    pos, pdis, angv = np.empty(3 * n.value), np.empty(3 * n.value), np.empty(3 * n.value)
+    check(lib().dem_read_preflow(str(path).encode(), ctypes.byref(it), ctypes.byref(n), ctypes.byref(itime),
+                                 _ptr(pos), _ptr(pdis), _ptr(angv), n.value), "dem_read_preflow")
+    return it.value, itime.value, pos, pdis, angv
 
 
 def estar(E, nu, rho, dref):

@@ -799,9 +799,9 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     DEM_CUDA_TRY(cudaEventRecord(c->ev[2], s));
     // ------------------------------------------------------------ results
     std::vector<double> pb((size_t)w->npb * 12);
-    double obj[2];
+    double obj[3];   // value, and the elastic energy's direct d/d estar (pair, wall)
     DEM_CUDA_TRY(cudaMemcpyAsync(pb.data(), w->pbar, pb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (d_radii) DEM_CUDA_TRY(cudaMemcpyAsync(d_radii, w->Rb, c->n * sizeof(double), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
     double acc[12] = {0};
@@ -812,10 +812,8 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     out->d_pw = dem_contact{acc[6], acc[7], 0.0, acc[8], acc[9], acc[10], acc[11]};
     if (which == DEM_OBJ_POTENTIAL) {
         // direct dependence of the elastic energy on estar
-        double eb[2];
-        DEM_CUDA_TRY(cudaMemcpy(eb, w->obj + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost));
-        out->d_pp.estar += eb[0];
-        out->d_pw.estar += eb[1];
+        out->d_pp.estar += obj[1];
+        out->d_pw.estar += obj[2];
     }
     float f1 = 0.f, f2 = 0.f;
     DEM_CUDA_TRY(cudaEventElapsedTime(&f1, c->ev[0], c->ev[1]));

@@ -35,7 +35,8 @@ int compat_device(CompatDevice** out) {
     CompatDevice* c = new CompatDevice();
     c->device = dev;
     DEM_CUDA_TRY(cudaMalloc(&c->words, 16 * sizeof(uint)));
-    DEM_CUDA_TRY(cudaMemset(c->words, 0, 16 * sizeof(uint)));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->words, 0, 16 * sizeof(uint), g_stream));   // ordered before the wrappers
+    DEM_CUDA_TRY(cudaStreamSynchronize(g_stream));
     DEM_CUDA_TRY(cudaMallocHost(&c->host_words, 16 * sizeof(uint)));
     g_devs.push_back(c);
     *out = c;
@@ -434,15 +435,20 @@ int setMaterialProperties(const Matproperties* par, const Wallproperties* parw) 
     dem_contact a{par->estarp, par->ufricp, par->vpois, par->dampnp, par->damptp, par->upp, 0.0};
     dem_contact b{parw->estarw, parw->ufricw, parw->vpoisw, parw->dampnw, parw->damptw, parw->upw, 0.0};
     LawParams<double> pa = make_law<double>(a), pb = make_law<double>(b);
-    DEM_CUDA_TRY(cudaMemcpyToSymbol(c_pp, &pa, sizeof(pa)));
-    DEM_CUDA_TRY(cudaMemcpyToSymbol(c_pw, &pb, sizeof(pb)));
+    // on the wrappers' stream, after the kernels already queued there, and
+    // complete before returning (a pageable upload may still be in flight
+    // when a plain cudaMemcpyToSymbol returns)
+    DEM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_pp, &pa, sizeof(pa), 0, cudaMemcpyHostToDevice, g_stream));
+    DEM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_pw, &pb, sizeof(pb), 0, cudaMemcpyHostToDevice, g_stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(g_stream));
     return DEM_OK;
 }
 
 int setListCutoff(double cua, double cub) {
     if (!(cub > 0.0) || !(cua >= 0.0)) return fail(DEM_ERR_ARG, "setListCutoff: need cua >= 0, cub > 0");
-    DEM_CUDA_TRY(cudaMemcpyToSymbol(c_cua, &cua, sizeof(double)));
-    DEM_CUDA_TRY(cudaMemcpyToSymbol(c_cub, &cub, sizeof(double)));
+    DEM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_cua, &cua, sizeof(double), 0, cudaMemcpyHostToDevice, g_stream));
+    DEM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_cub, &cub, sizeof(double), 0, cudaMemcpyHostToDevice, g_stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(g_stream));
     return DEM_OK;
 }
 

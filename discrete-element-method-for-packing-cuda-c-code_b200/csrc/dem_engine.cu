@@ -790,18 +790,27 @@ __global__ void __launch_bounds__(256) k_free_run(StepArgs<Real> a, int slot0, i
     if (observe) clear_partials(part, clr0, clr1);
 }
 
+// Grid-wide barrier of the window kernel (all blocks co-resident: cooperative
+// launch).  bar[0] is the launch's arrival counter and bar[kBarGiveUp] its
+// give-up word, both zeroed before every launch.  The wait is bounded: a
+// block that waits longer than kBarrierNs of %globaltimer AND kBarrierMinPolls
+// polls (or kBarrierMaxPolls polls in any case) records kStBarrier in the
+// status word and raises the launch's give-up word, after which the launch's
+// remaining barriers do not wait, so it always ends.  The timer is restarted
+// if it steps backwards, and the poll floor keeps a forward step of the timer
+// (the driver recalibrates %globaltimer) from ending a healthy wait.  A later
+// launch starts with its own give-up word clear.
+constexpr unsigned long long kBarrierNs = 1000000000ull;   // 1 s
+constexpr uint kBarrierMinPolls = 200000u;                 // >= ~0.1 s of polling
+constexpr uint kBarrierMaxPolls = 20000000u;               // a few seconds at most
+constexpr int kBarGiveUp = 32;                             // bar[32]: own 128-byte line
+constexpr int kBarWords = 64;                              // words zeroed per launch
+
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
 }
-
-// Grid-wide barrier of the window kernel (all blocks co-resident: cooperative
-// launch).  Arrival counter + generation word; the waiting is bounded: after
-// kBarrierNs without release the block records kStBarrier in the status word
-// and goes on, and later barriers of the launch then do not wait at all, so
-// the launch always ends.
-constexpr unsigned long long kBarrierNs = 1000000000ull;   // 1 s
 
 __device__ __forceinline__ uint ld_acquire(const uint* p) {
     uint v;
@@ -813,22 +822,24 @@ __device__ __forceinline__ void red_release_add(uint* p, uint v) {
 }
 
 // Grid-wide barrier number `k` (0, 1, ...) of a window-kernel launch: every
-// block adds 1 to the arrival counter (zeroed before the launch) with release
-// semantics and waits, with acquire loads, until it reaches (k+1) x blocks.
-// The wait is bounded: after kBarrierNs the block records kStBarrier in the
-// status word and goes on, and later barriers of the launch then do not wait
-// at all, so the launch always ends.
-__device__ __forceinline__ void grid_barrier(uint* count, uint k, EngineWords* words) {
+// block adds 1 to the arrival counter with release semantics and waits, with
+// acquire loads, until it reaches (k+1) x blocks (bounded as above).
+__device__ __forceinline__ void grid_barrier(uint* bar, uint k, EngineWords* words) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint target = (k + 1u) * gridDim.x;
-        red_release_add(count, 1u);
-        if (!(ld_acquire(&words->status) & kStBarrier)) {
-            const unsigned long long t0 = global_ns();
-            while (ld_acquire(count) < target) {
+        red_release_add(bar, 1u);
+        if (!ld_acquire(bar + kBarGiveUp)) {
+            unsigned long long t0 = global_ns();
+            uint polls = 0;
+            while (ld_acquire(bar) < target) {
                 __nanosleep(20);
-                if (global_ns() - t0 > kBarrierNs) {
+                ++polls;
+                const unsigned long long now = global_ns();
+                if (now < t0) t0 = now;   // the timer stepped back: restart the clock
+                if ((now - t0 > kBarrierNs && polls > kBarrierMinPolls) || polls > kBarrierMaxPolls) {
                     atomicOr(&words->status, kStBarrier);
+                    atomicExch(bar + kBarGiveUp, 1u);
                     break;
                 }
             }
@@ -1235,7 +1246,7 @@ template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nst
 // The window kernel: all K steps of the window in one cooperative launch.
 template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape* tape) {
     const int K = c->cfg.relist_interval;
-    DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, sizeof(uint), c->stream));   // arrival counter
+    DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, kBarWords * sizeof(uint), c->stream));   // counter, give-up word
     StepArgs<Real> a = step_args<Real>(c, lst, 0);
     a.dbgF = a.dbgT = nullptr;
     a.dbgC = nullptr;
@@ -1260,7 +1271,7 @@ template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape
 // PP window kernel: state buffer sb and history phase hp at the window start.
 template <typename Real> int launch_window_pp(dem_ctx* c, int lst, int sb, int hp) {
     const int K = c->cfg.relist_interval;
-    DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, sizeof(uint), c->stream));   // arrival counter
+    DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, kBarWords * sizeof(uint), c->stream));   // counter, give-up word
     StepArgs<Real> a = step_args<Real>(c, lst, 0);
     a.dbgF = a.dbgT = nullptr;
     a.dbgC = nullptr;
@@ -1469,13 +1480,22 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     auto bail = [&](int code) { dem_destroy(c); return code; };
     cudaError_t e = cudaGetDevice(&c->device);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaGetDevice", __FILE__, __LINE__));
+    // The context's stream first: every initialising memset below is queued on
+    // it and complete before dem_create returns.  (A plain cudaMemset would go
+    // to the legacy stream, which the context's non-blocking streams do not
+    // wait for: on a GPU busy with other streams' kernels it could land after
+    // the context's first upload or state load.)
+    e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__));
+    c->stream = c->own_stream;
+    const cudaStream_t s0 = c->own_stream;
     const long long n = c->n, np = c->npad, cap = c->cap;
     const size_t rs = real_size(c->prec);
     const int nstate = c->mode == DEM_FORCE_PP ? 2 : 1;
     const size_t recb = c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>);
     for (int b = 0; b < nstate; b++) {
         e = cudaMalloc(&c->rec[b], np * recb);
-        if (e == cudaSuccess) e = cudaMemset(c->rec[b], 0, np * recb);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->rec[b], 0, np * recb, s0);
         if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (state)", __FILE__, __LINE__));
     }
     for (int l = 0; l < 2; l++)
@@ -1490,7 +1510,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
         (rc = dalloc(&c->wcount, 1)) || (rc = dalloc(&c->arrival, np)) || (rc = dalloc(&c->scr, np * kScr)) ||
         (rc = dalloc(&c->bflag, np)) || (rc = dalloc(&c->bpos, np + 1)) || (rc = dalloc(&c->blist, np)) ||
-        (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, 64)) || (rc = dalloc(&c->tpos, np)))
+        (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, kBarWords)) || (rc = dalloc(&c->tpos, np)))
         return bail(rc);
     e = cudaMalloc(&c->wf, 2 * np * 4 * rs);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (wall forces)", __FILE__, __LINE__));
@@ -1536,16 +1556,17 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->npart)) ||
         (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->npart)))
         return bail(rc);
-    e = cudaMemset(c->part_mz, 0, (size_t)cfg->relist_interval * c->npart * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(c->part_cnt, 0, (size_t)cfg->relist_interval * c->npart * sizeof(uint));
+    e = cudaMemsetAsync(c->part_mz, 0, (size_t)cfg->relist_interval * c->npart * sizeof(unsigned long long), s0);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(c->part_cnt, 0, (size_t)cfg->relist_interval * c->npart * sizeof(uint), s0);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (partials)", __FILE__, __LINE__));
     c->scan_words = 3 * scan_scratch_words(std::max<long long>(np + 1, 1));
     if ((rc = dalloc(&c->scan_tmp, c->scan_words))) return bail(rc);
-    e = cudaMemset(c->words, 0, sizeof(EngineWords));
-    if (e == cudaSuccess) e = cudaMemset(c->bar, 0, 64 * sizeof(uint));
-    if (e == cudaSuccess) e = cudaMemset(c->off[0], 0, (np + 1) * sizeof(uint));
-    if (e == cudaSuccess) e = cudaMemset(c->off[1], 0, (np + 1) * sizeof(uint));
-    if (e == cudaSuccess) e = cudaMemset(c->roff, 0, (np + 1) * sizeof(uint));
+    e = cudaMemsetAsync(c->words, 0, sizeof(EngineWords), s0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->bar, 0, kBarWords * sizeof(uint), s0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->off[0], 0, (np + 1) * sizeof(uint), s0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->off[1], 0, (np + 1) * sizeof(uint), s0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->roff, 0, (np + 1) * sizeof(uint), s0);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (engine init)", __FILE__, __LINE__));
     for (int k = 0; k < 4; k++) {
         e = cudaEventCreate(&c->ev[k]);
@@ -1555,9 +1576,9 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evfork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evjoin, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__));
-    c->stream = c->own_stream;
+    e = cudaStreamSynchronize(s0);   // the initialisation above is done
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamSynchronize", __FILE__, __LINE__));
     *out = c;
     return DEM_OK;
 }
@@ -2004,6 +2025,170 @@ int dem_window_kernel_times(dem_ctx* c, double out[5]) {
         DEM_CUDA_TRY(cudaEventElapsedTime(&ms, c->wev[2 + 2 * K], c->wev[3 + 2 * K]));
         out[3] = ms;
     }
+    return DEM_OK;
+}
+
+
+// ------------------------------------------------------ checkpoint / resume
+// The reference's restart path (dempacking.cu:361-367, commented out there)
+// would re-read preflow.dat, which has neither the pair nor the wall history.
+// This file holds the whole engine state at a re-list boundary: particle
+// state, displacement-since-list words, wall history and the previous pair
+// list with its FP64 tangential history (the next re-list carries from it),
+// the step counters and the material.  Native byte order, this library only.
+namespace {
+struct StateHeader {
+    char magic[8];
+    int version, precision, force_mode, relist_interval;
+    long long n, step, relists, npairs;
+    double dt, skin, cell, density, world[3], rmax, vol;
+    int have_mat, pad;
+    dem_material mat;
+};
+constexpr char kStateMagic[8] = {'D', 'E', 'M', 'B', '2', '0', '0', 'S'};
+
+int write_all(FILE* f, const void* p, size_t bytes) {
+    return fwrite(p, 1, bytes, f) == bytes ? DEM_OK : fail(DEM_ERR_IO, "dem_save_state: write failed");
+}
+int read_all(FILE* f, void* p, size_t bytes) {
+    return fread(p, 1, bytes, f) == bytes ? DEM_OK : fail(DEM_ERR_IO, "dem_load_state: truncated state file");
+}
+}  // namespace
+
+int dem_save_state(dem_ctx* c, const char* path) {
+    if (!c || !path) return fail(DEM_ERR_ARG, "dem_save_state: null argument");
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_save_state: no state uploaded");
+    if (c->in_window != 0)
+        return fail(DEM_ERR_STATE, "dem_save_state: save at a re-list boundary (step a multiple of relist_interval)");
+    const long long n = c->n, np = c->npad;
+    std::vector<double> pos(3 * n), pdis(3 * n), angv(3 * n), rad(n), wh(3 * n);
+    std::vector<float4> q(n);
+    int rc = dem_download_state(c, pos.data(), pdis.data(), angv.data());
+    if (rc) return rc;
+    uint P = 0;
+    cudaStream_t s = c->stream;
+    DEM_CUDA_TRY(cudaMemcpyAsync(&P, c->off[c->cur] + n, sizeof(uint), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((long long)P > c->cap) P = 0;   // an overflowed list carries nothing
+    std::vector<uint> off(n + 1), ln(P);
+    std::vector<double> hist(3 * (size_t)P);
+    if (c->prec == DEM_PREC_MIXED) {
+        std::vector<float> rf(n);
+        DEM_CUDA_TRY(cudaMemcpyAsync(rf.data(), c->rad, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        DEM_CUDA_TRY(cudaStreamSynchronize(s));
+        for (long long i = 0; i < n; i++) rad[i] = rf[i];
+    } else {
+        DEM_CUDA_TRY(cudaMemcpyAsync(rad.data(), c->rad, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    DEM_CUDA_TRY(cudaMemcpyAsync(q.data(), c->q, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    for (int a = 0; a < 3; a++)
+        DEM_CUDA_TRY(cudaMemcpyAsync(wh.data() + a * n, c->wh + a * np, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(off.data(), c->off[c->cur], (n + 1) * sizeof(uint), cudaMemcpyDeviceToHost, s));
+    if (P) {
+        DEM_CUDA_TRY(cudaMemcpyAsync(ln.data(), c->ln[c->cur], P * sizeof(uint), cudaMemcpyDeviceToHost, s));
+        const double* h = c->hist[c->cur][c->hph];
+        for (int a = 0; a < 3; a++)
+            DEM_CUDA_TRY(cudaMemcpyAsync(hist.data() + (size_t)a * P, h + a * c->cap, P * sizeof(double),
+                                         cudaMemcpyDeviceToHost, s));
+    } else {
+        std::fill(off.begin(), off.end(), 0u);
+    }
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    StateHeader hd = {};
+    memcpy(hd.magic, kStateMagic, 8);
+    hd.version = 1;
+    hd.precision = c->prec;
+    hd.force_mode = c->mode;
+    hd.relist_interval = c->cfg.relist_interval;
+    hd.n = n;
+    hd.step = c->step;
+    hd.relists = c->relists;
+    hd.npairs = P;
+    hd.dt = c->cfg.dt; hd.skin = c->cfg.skin; hd.cell = c->cfg.cell; hd.density = c->cfg.density;
+    for (int a = 0; a < 3; a++) hd.world[a] = c->cfg.world[a];
+    hd.rmax = c->rmax;
+    hd.vol = c->vol;
+    hd.have_mat = c->have_mat ? 1 : 0;
+    hd.mat = c->mat;
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
+    rc = write_all(f, &hd, sizeof(hd));
+    if (!rc) rc = write_all(f, pos.data(), pos.size() * sizeof(double));
+    if (!rc) rc = write_all(f, pdis.data(), pdis.size() * sizeof(double));
+    if (!rc) rc = write_all(f, angv.data(), angv.size() * sizeof(double));
+    if (!rc) rc = write_all(f, rad.data(), rad.size() * sizeof(double));
+    if (!rc) rc = write_all(f, q.data(), q.size() * sizeof(float4));
+    if (!rc) rc = write_all(f, wh.data(), wh.size() * sizeof(double));
+    if (!rc) rc = write_all(f, off.data(), off.size() * sizeof(uint));
+    if (!rc && P) rc = write_all(f, ln.data(), ln.size() * sizeof(uint));
+    if (!rc && P) rc = write_all(f, hist.data(), hist.size() * sizeof(double));
+    if (fclose(f) != 0 && !rc) rc = fail(DEM_ERR_IO, "dem_save_state: close failed");
+    return rc;
+}
+
+int dem_load_state(dem_ctx* c, const char* path) {
+    if (!c || !path) return fail(DEM_ERR_ARG, "dem_load_state: null argument");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
+    StateHeader hd;
+    int rc = read_all(f, &hd, sizeof(hd));
+    if (!rc && (memcmp(hd.magic, kStateMagic, 8) != 0 || hd.version != 1))
+        rc = fail(DEM_ERR_IO, "dem_load_state: %s is not a state file of this library", path);
+    if (!rc && (hd.n != c->n || hd.precision != c->prec || hd.force_mode != c->mode ||
+                hd.relist_interval != c->cfg.relist_interval))
+        rc = fail(DEM_ERR_ARG, "dem_load_state: the context differs from the saved one (n %lld/%lld, precision, "
+                  "force mode or relist_interval)", hd.n, c->n);
+    if (!rc && hd.npairs > c->cap)
+        rc = fail(DEM_ERR_CAPACITY, "dem_load_state: %lld saved pairs exceed the pair capacity", hd.npairs);
+    if (rc) { fclose(f); return rc; }
+    const long long n = c->n, np = c->npad, P = hd.npairs;
+    std::vector<double> pos(3 * n), pdis(3 * n), angv(3 * n), rad(n), wh(3 * n), hist(3 * (size_t)P);
+    std::vector<float4> q(n);
+    std::vector<uint> off(n + 1), ln(P);
+    rc = read_all(f, pos.data(), pos.size() * sizeof(double));
+    if (!rc) rc = read_all(f, pdis.data(), pdis.size() * sizeof(double));
+    if (!rc) rc = read_all(f, angv.data(), angv.size() * sizeof(double));
+    if (!rc) rc = read_all(f, rad.data(), rad.size() * sizeof(double));
+    if (!rc) rc = read_all(f, q.data(), q.size() * sizeof(float4));
+    if (!rc) rc = read_all(f, wh.data(), wh.size() * sizeof(double));
+    if (!rc) rc = read_all(f, off.data(), off.size() * sizeof(uint));
+    if (!rc && P) rc = read_all(f, ln.data(), ln.size() * sizeof(uint));
+    if (!rc && P) rc = read_all(f, hist.data(), hist.size() * sizeof(double));
+    fclose(f);
+    if (rc) return rc;
+    // the list drives device indexing: rows must be well formed (offsets from
+    // 0 to P, non-decreasing; partners j > i, ascending, below n)
+    bool ok = off[0] == 0u && (long long)off[n] == P;
+    for (long long i = 0; ok && i < n; i++) {
+        if (off[i + 1] < off[i]) { ok = false; break; }
+        for (uint k = off[i]; k < off[i + 1]; k++)
+            if (ln[k] <= (uint)i || (long long)ln[k] >= n || (k > off[i] && ln[k] <= ln[k - 1])) { ok = false; break; }
+    }
+    if (!ok) return fail(DEM_ERR_IO, "dem_load_state: %s holds a malformed pair list", path);
+    if (hd.have_mat && (rc = dem_set_material(c, &hd.mat))) return rc;
+    if ((rc = dem_upload_state(c, pos.data(), pdis.data(), angv.data(), rad.data()))) return rc;
+    // the upload started afresh (list buffer 0 current, empty); put back the
+    // rest of the saved state
+    cudaStream_t s = c->stream;
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->q, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    for (int a = 0; a < 3; a++)
+        DEM_CUDA_TRY(cudaMemcpyAsync(c->wh + a * np, wh.data() + a * n, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->off[0], off.data(), (n + 1) * sizeof(uint), cudaMemcpyHostToDevice, s));
+    std::vector<uint> lp(P);   // each pair's row (the lower particle), as a re-list writes it
+    for (long long i = 0; i < n; i++)
+        for (uint k = off[i]; k < off[i + 1]; k++) lp[k] = (uint)i;
+    if (P) {
+        DEM_CUDA_TRY(cudaMemcpyAsync(c->lp, lp.data(), P * sizeof(uint), cudaMemcpyHostToDevice, s));
+        DEM_CUDA_TRY(cudaMemcpyAsync(c->ln[0], ln.data(), P * sizeof(uint), cudaMemcpyHostToDevice, s));
+        for (int a = 0; a < 3; a++)
+            DEM_CUDA_TRY(cudaMemcpyAsync(c->hist[0][0] + a * c->cap, hist.data() + (size_t)a * P, P * sizeof(double),
+                                         cudaMemcpyHostToDevice, s));
+    }
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    c->step = hd.step;
+    c->relists = hd.relists;
+    c->rmax = hd.rmax;
+    c->vol = hd.vol;
     return DEM_OK;
 }
 

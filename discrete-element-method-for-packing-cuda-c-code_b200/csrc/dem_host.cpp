@@ -280,6 +280,38 @@ int dem_write_preflow(const char* path, long long it, long long n, long long iti
     return DEM_OK;
 }
 
+// preflow.dat reader: the format the writer above produces (the reference's
+// own reader is commented out, dempacking.cu:361-367).  With pos == NULL only
+// the header line is read (it, n, itime); otherwise n particles of 9 values
+// (position, per-step displacement, per-step rotation) into arrays holding
+// ncap particles.  The file keeps 6 decimals of each value.
+int dem_read_preflow(const char* path, long long* it, long long* n, long long* itime, double* pos, double* pdis,
+                     double* angv, long long ncap) {
+    if (!path || !it || !n || !itime) return fail(DEM_ERR_ARG, "dem_read_preflow: null argument");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
+    long long a = 0, b = 0, c = 0;
+    if (fscanf(f, " %lld , %lld , %lld", &a, &b, &c) != 3 || b < 0) {
+        fclose(f);
+        return fail(DEM_ERR_IO, "%s: malformed preflow header", path);
+    }
+    *it = a; *n = b; *itime = c;
+    if (!pos) { fclose(f); return DEM_OK; }
+    if (!pdis || !angv) { fclose(f); return fail(DEM_ERR_ARG, "dem_read_preflow: null array"); }
+    if (b > ncap) { fclose(f); return fail(DEM_ERR_ARG, "dem_read_preflow: %lld particles exceed the arrays (%lld)", b, ncap); }
+    for (long long i = 0; i < b; i++) {
+        double v[9];
+        if (fscanf(f, " %lf %lf %lf %lf %lf %lf %lf %lf %lf", v, v + 1, v + 2, v + 3, v + 4, v + 5, v + 6, v + 7,
+                   v + 8) != 9) {
+            fclose(f);
+            return fail(DEM_ERR_IO, "%s: truncated at particle %lld", path, i);
+        }
+        for (int k = 0; k < 3; k++) { pos[3 * i + k] = v[k]; pdis[3 * i + k] = v[3 + k]; angv[3 * i + k] = v[6 + k]; }
+    }
+    fclose(f);
+    return DEM_OK;
+}
+
 // timesteps.dat line of dempacking.cu:802.
 int dem_write_timesteps(const char* path, double tret, long long it) {
     FILE* f = fopen(path, "ab+");

@@ -291,6 +291,19 @@ int dem_kernel_times(dem_ctx* ctx, double out[3]);
 int dem_set_window_timing(dem_ctx* ctx, int on);
 int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
 
+/* Checkpoint / resume (row (f)2; the reference's restart reader is commented
+ * out, dempacking.cu:361-367, and its preflow.dat has no contact history).
+ * dem_save_state writes the whole engine state at a re-list boundary (step a
+ * multiple of relist_interval, else DEM_ERR_STATE): particle state, radii,
+ * displacement-since-list words, wall history, the previous pair list with
+ * its FP64 tangential history, step counters and material (binary, native
+ * byte order, this library only).  dem_load_state restores it into a
+ * context of the same n, precision, force mode and relist_interval
+ * (DEM_ERR_ARG otherwise); stepping on gives the same states bit for bit as
+ * the saved context would. */
+int dem_save_state(dem_ctx* ctx, const char* path);
+int dem_load_state(dem_ctx* ctx, const char* path);
+
 /* ---------------------------------------------------------------- adjoint --
  * Reverse mode of the step (force + walls + integrator) over a window; no
  * counterpart in the reference.  The forward runs nsteps from the current
@@ -376,6 +389,12 @@ int dem_write_particles(const char* path, int zone, long long n, const double* p
 int dem_write_preflow(const char* path, long long it, long long n, long long itime,
                       const double* pos, const double* pdis, const double* angv);
 int dem_write_timesteps(const char* path, double tret, long long it);
+/* Reads preflow.dat as dem_write_preflow writes it (the reference's reader is
+ * commented out, dempacking.cu:361-367).  pos == NULL: header only
+ * (it, n, itime); else n particles into arrays of ncap particles (6 decimals
+ * per value, as written). */
+int dem_read_preflow(const char* path, long long* it, long long* n, long long* itime, double* pos,
+                     double* pdis, double* angv, long long ncap);
 int dem_write_finish(const char* jobfinished_path, const char* restart_path);
 
 #ifdef __cplusplus

@@ -176,3 +176,28 @@ def test_output_files(dem, deck, tmp_path):
     assert rs.read_text().splitlines() == ["program comes to end!", "       1        1"]
     assert L.dem_write_ppor(str(tmp_path / "no" / "dir" / "x.dat").encode(), 1, 1, 0, 0.0, 0.0, 0.0, 0.0) \
         == dem.DEM_ERR_IO
+
+
+def test_preflow_reader_round_trip(dem, tmp_path):
+    rng = np.random.default_rng(4)
+    n = 50
+    pos, pdis, angv = rng.uniform(-5, 5, 3 * n), rng.normal(0, 1e-3, 3 * n), rng.normal(0, 1e-3, 3 * n)
+    pre = tmp_path / "preflow.dat"
+    assert dem.lib().dem_write_preflow(str(pre).encode(), 7000, n, 5, dem._ptr(pos), dem._ptr(pdis),
+                                       dem._ptr(angv)) == 0
+    it, itime, p2, d2, a2 = dem.read_preflow(pre)
+    assert (it, itime, p2.size) == (7000, 5, 3 * n)
+    # the file keeps 6 decimals
+    np.testing.assert_allclose(p2, pos, rtol=0, atol=5e-7)
+    np.testing.assert_allclose(d2, pdis, rtol=0, atol=5e-7)
+    np.testing.assert_allclose(a2, angv, rtol=0, atol=5e-7)
+    small = np.empty(3)
+    c = ctypes.c_longlong
+    rc = dem.lib().dem_read_preflow(str(pre).encode(), ctypes.byref(c()), ctypes.byref(c()), ctypes.byref(c()),
+                                    dem._ptr(small), dem._ptr(small), dem._ptr(small), 1)
+    assert rc == dem.DEM_ERR_ARG
+    bad = tmp_path / "bad.dat"
+    bad.write_text("7000, 2, 5\n1 2 3 4 5 6 7 8 9\n1 2 3\n")
+    with pytest.raises(dem.DemError) as e:
+        dem.read_preflow(bad)
+    assert e.value.code == dem.DEM_ERR_IO

@@ -190,6 +190,8 @@ _SIGS = [
                                         _vp, ctypes.c_longlong]),
     ("dem_save_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("dem_load_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("dem_set_pour", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_double, ctypes.c_longlong]),
+    ("dem_active_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     ("dem_write_finish", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p]),
 ]
 
@@ -497,6 +499,17 @@ class Engine:
 
     def load_state(self, path):
         check(lib().dem_load_state(self._h, str(path).encode()), "dem_load_state")
+
+    def set_pour(self, nplayer, tnewpar, n_active=0):
+        """Poured packing (dem_set_pour): the uploaded states are injection
+        states; n_active particles are in the system, and nplayer more join
+        before every step whose time dt*it passes N*tnewpar/nplayer."""
+        check(lib().dem_set_pour(self._h, int(nplayer), float(tnewpar), int(n_active)), "dem_set_pour")
+
+    def active_count(self):
+        v = ctypes.c_longlong(0)
+        check(lib().dem_active_count(self._h, ctypes.byref(v)), "dem_active_count")
+        return v.value
 
     def set_window_timing(self, on=True):
         check(lib().dem_set_window_timing(self._h, 1 if on else 0), "dem_set_window_timing")

@@ -696,6 +696,9 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
         return fail(DEM_ERR_ARG, "dem_adjoint_window: need nsteps %% every == 0 and every %% relist_interval == 0");
     if (c->in_window != 0) return fail(DEM_ERR_STATE, "dem_adjoint_window: start at a re-list boundary");
     if (c->profiling) return fail(DEM_ERR_STATE, "dem_adjoint_window: switch profiling off");
+    if (c->n != c->ntot)
+        return fail(DEM_ERR_STATE, "dem_adjoint_window: layers are still to be poured in (%lld of %lld in the system)",
+                    c->n, c->ntot);
     const long long nseg = nsteps / every;
     int rc = ensure_work(c, every, nseg + 1);
     if (rc) return rc;

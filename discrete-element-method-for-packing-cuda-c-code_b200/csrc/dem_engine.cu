@@ -96,18 +96,36 @@ __global__ void k_from_aos(long long n, const double* __restrict__ pos, const do
     W.x[i] = 0.0; W.y[i] = 0.0; W.z[i] = 0.0;
 }
 
+// Particles nact .. n-1 (not yet poured in) report their injection state.
 template <typename Real>
-__global__ void k_to_aos(long long n, const PRec<Real>* __restrict__ S, double* __restrict__ pos,
-                         double* __restrict__ pdis, double* __restrict__ angv) {
+__global__ void k_to_aos(long long n, long long nact, const PRec<Real>* __restrict__ S,
+                         const PRec<Real>* __restrict__ pour, double* __restrict__ pos, double* __restrict__ pdis,
+                         double* __restrict__ angv) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     V3<double> x, d;
     V3<Real> a;
     Real r;
-    ld_rec<false>(S + i, x, d, a, r);
+    ld_rec<false>((i < nact ? S : pour) + i, x, d, a, r);
     if (pos) { pos[3 * i] = x.x; pos[3 * i + 1] = x.y; pos[3 * i + 2] = x.z; }
     if (pdis) { pdis[3 * i] = d.x; pdis[3 * i + 1] = d.y; pdis[3 * i + 2] = d.z; }
     if (angv) { angv[3 * i] = (double)a.x; angv[3 * i + 1] = (double)a.y; angv[3 * i + 2] = (double)a.z; }
+}
+
+// Poured packing: particles nold .. nnew-1 join the system with their
+// injection records (dempacking.cu:459-460), zero displacement since the list
+// and no wall contact; their rows of the current (previous) list are empty,
+// so the coming re-list carries no history into them.
+template <typename Real>
+__global__ void k_pour_activate(long long nold, long long nnew, const PRec<Real>* __restrict__ pour,
+                                PRec<Real>* __restrict__ S, float4* __restrict__ Q, Planes3<double> W,
+                                uint* __restrict__ off) {
+    const long long i = nold + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnew) return;
+    S[i] = pour[i];
+    Q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    W.x[i] = 0.0; W.y[i] = 0.0; W.z[i] = 0.0;
+    off[i + 1] = off[nold];
 }
 
 // --------------------------------------------------------------- re-list
@@ -1448,6 +1466,35 @@ int launch_window_graph(dem_ctx* c) {
     return DEM_OK;
 }
 
+// Poured packing: is a layer due before the step with index s (0-based; the
+// reference's it = s + 1 and time = dt*it, dempacking.cu:375-381)?  The
+// threshold is the reference's (float)N*tnewpar/float(nplayer).
+bool pour_due(const dem_ctx* c, long long s) {
+    if (!c->pouring || c->n >= c->ntot) return false;
+    const double time = c->cfg.dt * (double)(s + 1);
+    return time > (double)(float)c->n * c->pour_tnewpar / (double)(float)c->pour_nplayer;
+}
+
+// The next layer joins (dempacking.cu:459-461): nplayer more particles (the
+// rest at the end), and the step re-lists.
+int pour_insert(dem_ctx* c) {
+    const long long nold = c->n, nnew = std::min(nold + c->pour_nplayer, c->ntot);
+    const unsigned g = grid_for(nnew - nold, 256);
+    const Planes3<double> W = planes<double>(c->wh, c->npad);
+    if (c->prec == DEM_PREC_MIXED)
+        k_pour_activate<float><<<g, 256, 0, c->stream>>>(nold, nnew, (const PRec<float>*)c->pour_rec,
+                                                         (PRec<float>*)c->rec[c->sbuf], c->q, W, c->off[c->cur]);
+    else
+        k_pour_activate<double><<<g, 256, 0, c->stream>>>(nold, nnew, (const PRec<double>*)c->pour_rec,
+                                                          (PRec<double>*)c->rec[c->sbuf], c->q, W, c->off[c->cur]);
+    DEM_LAUNCH_CHECK();
+    c->n = nnew;
+    c->vol = 4.0 / 3.0 * M_PI * c->r3sum[nnew];
+    c->in_window = 0;   // this step re-lists (m_hiall = 1)
+    free_graphs(c);     // the particle count is part of every captured launch
+    return DEM_OK;
+}
+
 size_t real_size(int prec) { return prec == DEM_PREC_MIXED ? sizeof(float) : sizeof(double); }
 
 }  // namespace
@@ -1473,6 +1520,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     c->prec = cfg->precision;
     c->mode = cfg->force_mode;
     c->n = cfg->n;
+    c->ntot = cfg->n;
     c->npad = (cfg->n + 63) / 64 * 64;
     c->cap = cfg->pair_capacity > 0 ? cfg->pair_capacity : 8 * cfg->n;
     if (c->cap > 0x7fffffffLL) c->cap = 0x7fffffffLL;
@@ -1595,7 +1643,7 @@ int dem_destroy(dem_ctx* c) {
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
                     c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar,
-                    c->tpos};
+                    c->tpos, c->pour_rec};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
@@ -1676,6 +1724,9 @@ static int finish_upload(dem_ctx* c) {
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[0], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[1], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->words, 0, sizeof(EngineWords), c->stream));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->part_mz, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(unsigned long long),
+                                 c->stream));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->part_cnt, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(uint), c->stream));
     c->cur = 0;
     c->sbuf = 0;
     c->hph = 0;
@@ -1690,6 +1741,11 @@ static int finish_upload(dem_ctx* c) {
 static int upload_common(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad,
                          bool host) {
     if (!c || !pos || !rad) return fail(DEM_ERR_ARG, "dem_upload_state: null argument");
+    // every particle the context holds is in the system again (a pour ends);
+    // graphs captured for fewer particles go
+    if (c->n != c->ntot) free_graphs(c);
+    c->n = c->ntot;
+    c->pouring = false;
     const long long n = c->n, np = c->npad;
     double* st = c->staging;
     double *spos = st, *sd = st + 3 * np, *sa = st + 6 * np, *sr = st + 9 * np;
@@ -1747,7 +1803,8 @@ int dem_upload_state_device(dem_ctx* c, const double* pos, const double* pdis, c
 static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, bool host) {
     if (!c) return fail(DEM_ERR_ARG, "dem_download_state: null ctx");
     if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_download_state: no state uploaded");
-    const long long n = c->n, np = c->npad;
+    // every particle the context holds; those not yet poured in as injected
+    const long long n = c->ntot, np = c->npad, nact = c->pouring ? c->n : c->ntot;
     const int sb = c->sbuf;
     double* st = c->staging;
     double *tp = host ? st : pos, *td = host ? st + 3 * np : pdis, *ta = host ? st + 6 * np : angv;
@@ -1755,9 +1812,11 @@ static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, 
     if (!pdis) td = nullptr;
     if (!angv) ta = nullptr;
     if (c->prec == DEM_PREC_MIXED)
-        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, (const PRec<float>*)c->rec[sb], tp, td, ta);
+        k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(
+            n, nact, (const PRec<float>*)c->rec[sb], (const PRec<float>*)c->pour_rec, tp, td, ta);
     else
-        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, (const PRec<double>*)c->rec[sb], tp, td, ta);
+        k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(
+            n, nact, (const PRec<double>*)c->rec[sb], (const PRec<double>*)c->pour_rec, tp, td, ta);
     DEM_LAUNCH_CHECK();
     if (host) {
         if (pos) DEM_CUDA_TRY(cudaMemcpyAsync(pos, tp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1783,7 +1842,10 @@ int dem_step_n(dem_ctx* c, long long nsteps) {
     const int K = c->cfg.relist_interval;
     int rc;
     while (nsteps > 0) {
-        if (c->in_window == 0 && nsteps >= K && !c->profiling) {
+        if (pour_due(c, c->step) && (rc = pour_insert(c))) return rc;
+        // a whole window replays its graph unless a layer joins inside it
+        // (the window then ends there: its steps run one by one)
+        if (c->in_window == 0 && nsteps >= K && !c->profiling && !pour_due(c, c->step + K - 1)) {
             // whole window: replay the captured graph
             rc = launch_window_graph(c);
             if (rc) return rc;
@@ -1825,6 +1887,50 @@ int dem_step_n(dem_ctx* c, long long nsteps) {
         c->in_window++;
         if (c->in_window == K) c->in_window = 0;
     }
+    return DEM_OK;
+}
+
+int dem_set_pour(dem_ctx* c, long long nplayer, double tnewpar, long long n_active) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_set_pour: null ctx");
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_set_pour: upload the injection states first");
+    if (c->pouring) return fail(DEM_ERR_STATE, "dem_set_pour: a pour is already set (upload again to start over)");
+    if (nplayer <= 0 || !(tnewpar > 0.0) || n_active < 0 || n_active > c->ntot)
+        return fail(DEM_ERR_ARG, "dem_set_pour: need nplayer > 0, tnewpar > 0 and 0 <= n_active <= n");
+    const long long ntot = c->ntot;
+    const size_t recb = c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>);
+    cudaStream_t s = c->stream;
+    if (!c->pour_rec) DEM_CUDA_TRY(cudaMalloc(&c->pour_rec, (size_t)c->npad * recb));
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->pour_rec, c->rec[c->sbuf], (size_t)ntot * recb, cudaMemcpyDeviceToDevice, s));
+    // r^3 prefix sums for the packing fraction of the particles in the system
+    std::vector<double> r(ntot);
+    if (c->prec == DEM_PREC_MIXED) {
+        std::vector<float> rf(ntot);
+        DEM_CUDA_TRY(cudaMemcpyAsync(rf.data(), c->rad, ntot * sizeof(float), cudaMemcpyDeviceToHost, s));
+        DEM_CUDA_TRY(cudaStreamSynchronize(s));
+        for (long long i = 0; i < ntot; i++) r[i] = rf[i];
+    } else {
+        DEM_CUDA_TRY(cudaMemcpyAsync(r.data(), c->rad, ntot * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    DEM_CUDA_TRY(cudaMemsetAsync(c->part_mz, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(unsigned long long),
+                                 s));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->part_cnt, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(uint), s));
+    DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    c->r3sum.assign(ntot + 1, 0.0);
+    for (long long i = 0; i < ntot; i++) c->r3sum[i + 1] = c->r3sum[i] + r[i] * r[i] * r[i];
+    if (n_active != c->n) free_graphs(c);
+    c->n = n_active;
+    c->vol = 4.0 / 3.0 * M_PI * c->r3sum[n_active];
+    c->pour_nplayer = nplayer;
+    c->pour_tnewpar = tnewpar;
+    c->pouring = true;
+    c->in_window = 0;   // the next step re-lists the particles in the system
+    c->last_slot = -1;
+    return DEM_OK;
+}
+
+int dem_active_count(dem_ctx* c, long long* n_active) {
+    if (!c || !n_active) return fail(DEM_ERR_ARG, "dem_active_count: null argument");
+    *n_active = c->n;
     return DEM_OK;
 }
 
@@ -2035,17 +2141,22 @@ int dem_window_kernel_times(dem_ctx* c, double out[5]) {
 // This file holds the whole engine state at a re-list boundary: particle
 // state, displacement-since-list words, wall history and the previous pair
 // list with its FP64 tangential history (the next re-list carries from it),
-// the step counters and the material.  Native byte order, this library only.
+// the step counters, the material and a pour in progress (particles not yet
+// in the system are stored with their injection states).  Native byte order,
+// this library only.
 namespace {
 struct StateHeader {
     char magic[8];
     int version, precision, force_mode, relist_interval;
     long long n, step, relists, npairs;
     double dt, skin, cell, density, world[3], rmax, vol;
-    int have_mat, pad;
+    int have_mat, pouring;
     dem_material mat;
+    long long n_active, pour_nplayer;
+    double pour_tnewpar;
 };
 constexpr char kStateMagic[8] = {'D', 'E', 'M', 'B', '2', '0', '0', 'S'};
+constexpr int kStateVersion = 2;
 
 int write_all(FILE* f, const void* p, size_t bytes) {
     return fwrite(p, 1, bytes, f) == bytes ? DEM_OK : fail(DEM_ERR_IO, "dem_save_state: write failed");
@@ -2060,17 +2171,18 @@ int dem_save_state(dem_ctx* c, const char* path) {
     if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_save_state: no state uploaded");
     if (c->in_window != 0)
         return fail(DEM_ERR_STATE, "dem_save_state: save at a re-list boundary (step a multiple of relist_interval)");
-    const long long n = c->n, np = c->npad;
+    // particle sections: every particle held; list: the particles in the system
+    const long long n = c->ntot, na = c->n, np = c->npad;
     std::vector<double> pos(3 * n), pdis(3 * n), angv(3 * n), rad(n), wh(3 * n);
     std::vector<float4> q(n);
     int rc = dem_download_state(c, pos.data(), pdis.data(), angv.data());
     if (rc) return rc;
     uint P = 0;
     cudaStream_t s = c->stream;
-    DEM_CUDA_TRY(cudaMemcpyAsync(&P, c->off[c->cur] + n, sizeof(uint), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(&P, c->off[c->cur] + na, sizeof(uint), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
     if ((long long)P > c->cap) P = 0;   // an overflowed list carries nothing
-    std::vector<uint> off(n + 1), ln(P);
+    std::vector<uint> off(na + 1), ln(P);
     std::vector<double> hist(3 * (size_t)P);
     if (c->prec == DEM_PREC_MIXED) {
         std::vector<float> rf(n);
@@ -2083,7 +2195,7 @@ int dem_save_state(dem_ctx* c, const char* path) {
     DEM_CUDA_TRY(cudaMemcpyAsync(q.data(), c->q, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
     for (int a = 0; a < 3; a++)
         DEM_CUDA_TRY(cudaMemcpyAsync(wh.data() + a * n, c->wh + a * np, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    DEM_CUDA_TRY(cudaMemcpyAsync(off.data(), c->off[c->cur], (n + 1) * sizeof(uint), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(off.data(), c->off[c->cur], (na + 1) * sizeof(uint), cudaMemcpyDeviceToHost, s));
     if (P) {
         DEM_CUDA_TRY(cudaMemcpyAsync(ln.data(), c->ln[c->cur], P * sizeof(uint), cudaMemcpyDeviceToHost, s));
         const double* h = c->hist[c->cur][c->hph];
@@ -2096,7 +2208,7 @@ int dem_save_state(dem_ctx* c, const char* path) {
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
     StateHeader hd = {};
     memcpy(hd.magic, kStateMagic, 8);
-    hd.version = 1;
+    hd.version = kStateVersion;
     hd.precision = c->prec;
     hd.force_mode = c->mode;
     hd.relist_interval = c->cfg.relist_interval;
@@ -2110,6 +2222,10 @@ int dem_save_state(dem_ctx* c, const char* path) {
     hd.vol = c->vol;
     hd.have_mat = c->have_mat ? 1 : 0;
     hd.mat = c->mat;
+    hd.pouring = c->pouring ? 1 : 0;
+    hd.n_active = na;
+    hd.pour_nplayer = c->pour_nplayer;
+    hd.pour_tnewpar = c->pour_tnewpar;
     FILE* f = fopen(path, "wb");
     if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
     rc = write_all(f, &hd, sizeof(hd));
@@ -2132,19 +2248,22 @@ int dem_load_state(dem_ctx* c, const char* path) {
     if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
     StateHeader hd;
     int rc = read_all(f, &hd, sizeof(hd));
-    if (!rc && (memcmp(hd.magic, kStateMagic, 8) != 0 || hd.version != 1))
+    if (!rc && (memcmp(hd.magic, kStateMagic, 8) != 0 || hd.version != kStateVersion))
         rc = fail(DEM_ERR_IO, "dem_load_state: %s is not a state file of this library", path);
-    if (!rc && (hd.n != c->n || hd.precision != c->prec || hd.force_mode != c->mode ||
+    if (!rc && (hd.n != c->ntot || hd.precision != c->prec || hd.force_mode != c->mode ||
                 hd.relist_interval != c->cfg.relist_interval))
         rc = fail(DEM_ERR_ARG, "dem_load_state: the context differs from the saved one (n %lld/%lld, precision, "
-                  "force mode or relist_interval)", hd.n, c->n);
-    if (!rc && hd.npairs > c->cap)
+                  "force mode or relist_interval)", hd.n, c->ntot);
+    if (!rc && (hd.n_active < 0 || hd.n_active > hd.n || (!hd.pouring && hd.n_active != hd.n) ||
+                (hd.pouring && (hd.pour_nplayer <= 0 || !(hd.pour_tnewpar > 0.0)))))
+        rc = fail(DEM_ERR_IO, "dem_load_state: %s holds an inconsistent pour", path);
+    if (!rc && (hd.npairs < 0 || hd.npairs > c->cap))
         rc = fail(DEM_ERR_CAPACITY, "dem_load_state: %lld saved pairs exceed the pair capacity", hd.npairs);
     if (rc) { fclose(f); return rc; }
-    const long long n = c->n, np = c->npad, P = hd.npairs;
+    const long long n = c->ntot, na = hd.n_active, np = c->npad, P = hd.npairs;
     std::vector<double> pos(3 * n), pdis(3 * n), angv(3 * n), rad(n), wh(3 * n), hist(3 * (size_t)P);
     std::vector<float4> q(n);
-    std::vector<uint> off(n + 1), ln(P);
+    std::vector<uint> off(na + 1), ln(P);
     rc = read_all(f, pos.data(), pos.size() * sizeof(double));
     if (!rc) rc = read_all(f, pdis.data(), pdis.size() * sizeof(double));
     if (!rc) rc = read_all(f, angv.data(), angv.size() * sizeof(double));
@@ -2157,25 +2276,28 @@ int dem_load_state(dem_ctx* c, const char* path) {
     fclose(f);
     if (rc) return rc;
     // the list drives device indexing: rows must be well formed (offsets from
-    // 0 to P, non-decreasing; partners j > i, ascending, below n)
-    bool ok = off[0] == 0u && (long long)off[n] == P;
-    for (long long i = 0; ok && i < n; i++) {
+    // 0 to P, non-decreasing; partners j > i, ascending, among the particles
+    // in the system)
+    bool ok = off[0] == 0u && (long long)off[na] == P;
+    for (long long i = 0; ok && i < na; i++) {
         if (off[i + 1] < off[i]) { ok = false; break; }
         for (uint k = off[i]; k < off[i + 1]; k++)
-            if (ln[k] <= (uint)i || (long long)ln[k] >= n || (k > off[i] && ln[k] <= ln[k - 1])) { ok = false; break; }
+            if (ln[k] <= (uint)i || (long long)ln[k] >= na || (k > off[i] && ln[k] <= ln[k - 1])) { ok = false; break; }
     }
     if (!ok) return fail(DEM_ERR_IO, "dem_load_state: %s holds a malformed pair list", path);
     if (hd.have_mat && (rc = dem_set_material(c, &hd.mat))) return rc;
     if ((rc = dem_upload_state(c, pos.data(), pdis.data(), angv.data(), rad.data()))) return rc;
+    // particles not yet poured in wait with the injection states just uploaded
+    if (hd.pouring && (rc = dem_set_pour(c, hd.pour_nplayer, hd.pour_tnewpar, na))) return rc;
     // the upload started afresh (list buffer 0 current, empty); put back the
     // rest of the saved state
     cudaStream_t s = c->stream;
     DEM_CUDA_TRY(cudaMemcpyAsync(c->q, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
     for (int a = 0; a < 3; a++)
         DEM_CUDA_TRY(cudaMemcpyAsync(c->wh + a * np, wh.data() + a * n, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    DEM_CUDA_TRY(cudaMemcpyAsync(c->off[0], off.data(), (n + 1) * sizeof(uint), cudaMemcpyHostToDevice, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->off[0], off.data(), (na + 1) * sizeof(uint), cudaMemcpyHostToDevice, s));
     std::vector<uint> lp(P);   // each pair's row (the lower particle), as a re-list writes it
-    for (long long i = 0; i < n; i++)
+    for (long long i = 0; i < na; i++)
         for (uint k = off[i]; k < off[i + 1]; k++) lp[k] = (uint)i;
     if (P) {
         DEM_CUDA_TRY(cudaMemcpyAsync(c->lp, lp.data(), P * sizeof(uint), cudaMemcpyHostToDevice, s));

@@ -120,7 +120,15 @@ struct dem_ctx {
     dem_config cfg{};
     int prec = DEM_PREC_MIXED;
     int mode = DEM_FORCE_PCCP;
-    long long n = 0, npad = 0, cap = 0;
+    long long n = 0, npad = 0, cap = 0;   // n: particles in the system (the first n of ntot)
+    long long ntot = 0;                    // particles the context holds (dem_config.n)
+    // poured packing: particles n .. ntot-1 wait in pour_rec (their injection
+    // records) and join nplayer at a time (dem_set_pour)
+    bool pouring = false;
+    long long pour_nplayer = 0;
+    double pour_tnewpar = 0.0;
+    void* pour_rec = nullptr;              // PRec<Real>[npad]
+    std::vector<double> r3sum;             // r3sum[k] = sum of r^3 over the first k particles
     int device = 0;
     cudaStream_t stream = 0;
     cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one

@@ -17,6 +17,13 @@ damping, normal and tangential), flat frictional walls, gravity -z, skin
                  5,000 steps, mu = 0.5, mu_r = 0.005 R*.  Mixed precision.
   settle_50k     50,000 lognormal (as rsa_500k) in 40x40x150 mm, dt = 5e-7 s,
                  pre-settled 20,000 steps, then a 2,000-step window.
+  pour_box       a poured packing (the reference's layer injection) at test
+                 size: 108 spheres r = 0.5 mm in 8x8 mm, 3 layers of 36 on a
+                 6x6 injection lattice 3 mm above the floor, initial speed 1.5
+                 (reduced) in the reference's random downward directions, a
+                 layer every 1507 steps (each layer has left the injection
+                 height before the next arrives), dt = 5e-4 (reduced), skin
+                 0.55 (the reference's cub - cua).
 """
 import math
 from dataclasses import dataclass, field
@@ -118,3 +125,35 @@ def small_box(n=3000, box=(16.0, 16.0, 40.0), seed=SEED, precision=PREC_FP64, co
         pos = p.reshape(-1).copy()
     pp, pw = material(mu=0.3, roll_rel=0.002)
     return Workload("small_box", n, pos, rad, tuple(box), reduced_dt(5e-7), 200, 20, 0.05, precision, pp, pw)
+
+
+def pour_box(seed=SEED, nx=6, ny=6, layers=3, box=(8.0, 8.0, 12.0), z_inject=3.0, vel0=1.5, dt=5e-4,
+             layer_steps=1507.0, precision=PREC_FP64):
+    """Poured packing at test size.  Injection states of all particles:
+    nx*ny lattice sites per layer (dempacking.cu:253-279), every layer at the
+    same height, speed vel0 at elevation pi*(u/3 + 1/3) below the horizontal
+    and a uniform azimuth (:302-309, seeded).  meta: pdis (displacement per
+    step), nplayer, tnewpar (one layer per layer_steps steps)."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * layers
+    W, T = box[0], box[1]
+    xs = ((np.arange(nx) + 0.5) / nx - 0.5) * W
+    ys = ((np.arange(ny) + 0.5) / ny - 0.5) * T
+    site = np.array([(x, y) for x in xs for y in ys])
+    pos = np.zeros((n, 3))
+    pos[:, :2] = np.tile(site, (layers, 1))
+    pos[:, 2] = z_inject
+    ang = np.pi * (rng.random(n) / 3.0 + 1.0 / 3.0)
+    az = 2.0 * np.pi * rng.random(n)
+    pdis = np.zeros((n, 3))
+    pdis[:, 2] = -vel0 * np.sin(ang) * dt
+    dxy = -vel0 * np.cos(ang) * dt
+    pdis[:, 0] = dxy * np.cos(az)
+    pdis[:, 1] = dxy * np.sin(az)
+    rad = np.full(n, 0.5)
+    pp, pw = material(mu=0.3, roll_rel=0.002)
+    w = Workload("pour_box", n, pos.reshape(-1), rad, tuple(box), dt, int(layer_steps * layers), 20, 0.55,
+                 precision, pp, pw,
+                 meta={"pdis": pdis.reshape(-1), "nplayer": nx * ny, "tnewpar": layer_steps * dt,
+                       "init": f"poured: {nx}x{ny} injection lattice, a layer every {layer_steps:g} steps"})
+    return w

@@ -291,18 +291,40 @@ int dem_kernel_times(dem_ctx* ctx, double out[3]);
 int dem_set_window_timing(dem_ctx* ctx, int on);
 int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
 
-/* Checkpoint / resume (row (f)2; the reference's restart reader is commented
- * out, dempacking.cu:361-367, and its preflow.dat has no contact history).
+/* Checkpoint / resume (the reference's restart reader is commented out,
+ * dempacking.cu:361-367, and its preflow.dat has no contact history).
  * dem_save_state writes the whole engine state at a re-list boundary (step a
  * multiple of relist_interval, else DEM_ERR_STATE): particle state, radii,
  * displacement-since-list words, wall history, the previous pair list with
- * its FP64 tangential history, step counters and material (binary, native
- * byte order, this library only).  dem_load_state restores it into a
- * context of the same n, precision, force mode and relist_interval
- * (DEM_ERR_ARG otherwise); stepping on gives the same states bit for bit as
- * the saved context would. */
+ * its FP64 tangential history, step counters, material and a pour in
+ * progress (binary, native byte order, this library only).  dem_load_state
+ * restores it into a context of the same n, precision, force mode and
+ * relist_interval (DEM_ERR_ARG otherwise; DEM_ERR_IO for a file that is not
+ * one, or whose pair list is malformed); stepping on gives the same states
+ * bit for bit as the saved context would. */
 int dem_save_state(dem_ctx* ctx, const char* path);
 int dem_load_state(dem_ctx* ctx, const char* path);
+
+/* Poured packing: the reference's layer injection (dempacking.cu:373-534),
+ * replacing its download / free / malloc / upload of every array per layer
+ * with buffers sized once for all particles.  The context's n particles are
+ * the run's ntot; the state uploaded last (dem_upload_state*) holds their
+ * injection states (position, displacement per step, rotation, radius).
+ * After dem_set_pour only the first n_active are in the system.  Before each
+ * step (reference step it = completed steps + 1, time = dt*it,
+ * dempacking.cu:375-376), while N < n and time > (float)N*tnewpar/float(nplayer)
+ * (:379-381), the next nplayer particles (the rest, at the end) join with
+ * their injection states, no wall or pair history and zero displacement
+ * since the list, and the step re-lists (:459-461): the re-list window
+ * restarts there.  Forces, observables (packing fraction over the particles
+ * in the system, mean CN = 2 contacts / N), dem_download_pairs and the window
+ * kernels cover the N particles in the system; dem_download_state* returns
+ * all n, those not yet poured in as injected.  A later upload ends the pour.
+ * DEM_ERR_STATE before an upload or when a pour is already set (upload again
+ * to start over); dem_adjoint_window refuses (DEM_ERR_STATE) until every
+ * particle is in.  dem_active_count: N (n when not pouring). */
+int dem_set_pour(dem_ctx* ctx, long long nplayer, double tnewpar, long long n_active);
+int dem_active_count(dem_ctx* ctx, long long* n_active);
 
 /* ---------------------------------------------------------------- adjoint --
  * Reverse mode of the step (force + walls + integrator) over a window; no

@@ -883,6 +883,82 @@ int orc_run_list(long long n, double* pos, double* pdis, double* angv, const dou
     return status;
 }
 
+/* Poured packing: the reference's layer injection (dempacking.cu:376-461).
+ * The arrays hold all ntot particles; entries from N on are the injection
+ * states of particles not yet in the system, N starting at n_active.  Before
+ * step it (1-based; time = dt*it, :375-376): while N < ntot and
+ * time > (float)N*tnewpar/float(nplayer) (:379-381) the next nplayer
+ * particles join (N += nplayer, capped at ntot: :459-460) and the step
+ * re-lists (m_hiall = 1: :461); the fixed re-list cadence restarts there.
+ * A new particle brings no tangential history: its rows of the previous list
+ * are empty (the reference re-uploads its old-list arrays with the new count,
+ * :522-533, leaving the new rows to whatever the host arrays held; empty rows
+ * are the physical reading).  out_nact (if not NULL): N of each step.
+ * Returns 0, 3 (pair capacity) or 5 (skin violation). */
+int orc_run_pour(long long ntot, double* pos, double* pdis, double* angv, const double* rad, double* whist,
+                 const double* world, const double* params, const double* mat, int fp32_list,
+                 long long nsteps, int interval, long long cap, long long nplayer, double tnewpar,
+                 long long n_active, long long* out_nact, double* out_scalars,
+                 uint* out_off, uint* out_ln, double* out_hist, long long* out_P)
+{
+    const double dt = params[0], skin = params[1], cs = params[2], density = params[3];
+    OContact pp{mat[0], mat[1], mat[2], mat[3], mat[4], mat[5], mat[6]};
+    OContact pw{mat[7], mat[8], mat[9], mat[10], mat[11], mat[12], mat[13]};
+    std::vector<double> q(3 * ntot, 0.0), F(3 * ntot), T(3 * ntot);
+    std::vector<uint> C(ntot);
+    std::vector<uint> off(ntot + 1, 0), ln, ooff(ntot + 1, 0), oln;
+    std::vector<double> hist, ohist;
+    long long P = 0, N = n_active;
+    int status = 0, win = 0;
+    bool have_old = false;
+    for (long long st = 0; st < nsteps; st++) {
+        const double time = dt * (double)(st + 1);
+        if (N < ntot && time > (double)(float)N * tnewpar / (double)(float)nplayer) {
+            const long long nn = std::min(N + nplayer, ntot);
+            for (long long i = N + 1; i <= nn; i++) ooff[i] = ooff[N];   /* empty old rows */
+            N = nn;
+            win = 0;
+        }
+        OState s{N, pos, pdis, angv, const_cast<double*>(rad), whist, q.data()};
+        if (win == 0) {
+            ln.assign(cap > 0 ? cap : 1, 0);
+            hist.assign(3 * (cap > 0 ? cap : 1), 0.0);
+            int mr;
+            long long got = orc_build_list(N, pos, rad, world, cs, skin, fp32_list,
+                                           have_old ? ooff.data() : nullptr, have_old ? oln.data() : nullptr,
+                                           have_old ? ohist.data() : nullptr,
+                                           off.data(), ln.data(), hist.data(), cap, &mr);
+            if (got < 0) return 3;
+            P = got;
+            std::fill(q.begin(), q.end(), 0.0);
+        }
+        engine_forces(s, world, dt, density, pp, pw, P, off.data(), ln.data(), hist.data(),
+                      F.data(), T.data(), C.data());
+        double mz;
+        int viol;
+        engine_integrate(s, dt, density, F.data(), T.data(), skin, &mz, &viol);
+        if (viol && !status) status = 5;
+        ooff = off;
+        oln.assign(ln.begin(), ln.begin() + P);
+        ohist.assign(hist.begin(), hist.begin() + 3 * P);
+        have_old = true;
+        win = (win + 1) % interval;
+        if (out_nact) out_nact[st] = N;
+        if (out_scalars) {
+            long long csum = 0;
+            for (long long i = 0; i < N; i++) csum += C[i];
+            out_scalars[3 * st] = mz;
+            out_scalars[3 * st + 1] = (double)(csum / 2);
+            out_scalars[3 * st + 2] = (double)P;
+        }
+    }
+    if (out_P) *out_P = P;
+    if (out_off) memcpy(out_off, off.data(), (N + 1) * sizeof(uint));
+    if (out_ln && P) memcpy(out_ln, ln.data(), P * sizeof(uint));
+    if (out_hist && P) memcpy(out_hist, hist.data(), 3 * P * sizeof(double));
+    return status;
+}
+
 /* One force evaluation (no integration) for a freshly built list: forces,
  * torques and contact counts per particle; wall history and pair history
  * start from zero.  Used for first-step force parity. */

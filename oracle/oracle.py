@@ -59,6 +59,8 @@ def lib():
             "orc_run": (_i, [_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _ll, _i, _ll, _vp, _vp, _vp, _vp]),
             "orc_run_list": (_i, [_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _ll, _i, _ll, _vp, _vp, _vp, _vp,
                                   _vp, _vp, _vp, _vp]),
+            "orc_run_pour": (_i, [_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _ll, _i, _ll, _ll, _d, _ll, _vp,
+                                  _vp, _vp, _vp, _vp, _vp]),
             "orc_forces_once": (_i, [_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _ll, _vp, _vp, _vp, _vp]),
             "orc_engine_new": (_vp, [_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _ll]),
             "orc_engine_step": (_i, [_vp, _ll, _vp]),
@@ -171,6 +173,37 @@ def run(pos, rad, world, dt, skin, cell, density, mat14, fp32_list, nsteps, inte
         s = sc.reshape(-1, 3)
         out.update(maxhz=s[:, 0].copy(), ncontacts=s[:, 1].copy(), npairs=s[:, 2].copy())
     return out
+
+
+def run_pour(pos, rad, world, dt, skin, cell, density, mat14, fp32_list, nsteps, interval, nplayer, tnewpar,
+             n_active=0, pdis=None, angv=None, cap=None):
+    """Poured packing (orc_run_pour): pos/pdis/angv/rad hold all ntot
+    particles, entries from the active count on being injection states.
+    Returns the final state, the active count and scalars of every step, and
+    the final list."""
+    pos = f64(pos).copy()
+    rad = f64(rad)
+    n = rad.size
+    pdis = np.zeros(3 * n) if pdis is None else f64(pdis).copy()
+    angv = np.zeros(3 * n) if angv is None else f64(angv).copy()
+    wh = np.zeros(3 * n)
+    cap = cap or 16 * n + 16
+    params = np.array([dt, skin, cell, density], dtype=np.float64)
+    sc = np.zeros(3 * nsteps)
+    nact = np.zeros(nsteps, dtype=np.int64)
+    off = np.zeros(n + 1, dtype=np.uint32)
+    ln = np.zeros(cap, dtype=np.uint32)
+    hist = np.zeros(3 * cap)
+    npairs = ctypes.c_longlong(0)
+    st = lib().orc_run_pour(n, P(pos), P(pdis), P(angv), P(rad), P(wh), P(f64(world)), P(params), P(f64(mat14)),
+                            int(fp32_list), int(nsteps), int(interval), int(cap), int(nplayer), float(tnewpar),
+                            int(n_active), P(nact), P(sc), P(off), P(ln), P(hist), ctypes.byref(npairs))
+    Pn = npairs.value
+    s = sc.reshape(-1, 3)
+    na = int(nact[-1]) if nsteps else int(n_active)
+    return dict(status=st, pos=pos, pdis=pdis, angv=angv, whist=wh, nact=nact, maxhz=s[:, 0].copy(),
+                ncontacts=s[:, 1].copy(), npairs=s[:, 2].copy(), list_off=off[:na + 1].copy(),
+                list_ln=ln[:Pn].copy(), list_hist=hist[:3 * Pn].copy())
 
 
 def forces_once(pos, rad, world, dt, skin, cell, density, mat14, fp32_list, pdis=None, angv=None, cap=None):

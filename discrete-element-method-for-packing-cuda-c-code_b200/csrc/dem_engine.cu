@@ -174,13 +174,15 @@ __global__ void k_hash_count(long long n, const PRec<Real>* __restrict__ S, Grid
 
 // Scatter each particle (id, cell, list coordinates x,y,z,r in the list
 // precision) into its cell's range at its arrival slot, unordered inside the
-// cell; the count array returns to zero for the next re-list.  Reads are
-// coalesced by id.
+// cell, and record each particle's slot (tpos); the count array returns to
+// zero for the next re-list.  Reads are coalesced by id.  The walk and the
+// fill work on this order directly: a row's candidate set does not depend on
+// the order inside a cell, and every row is sorted by j before use.
 template <typename Real>
 __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint* __restrict__ arrival,
                           const uint* __restrict__ cstart, uint* __restrict__ count, const PRec<Real>* __restrict__ S,
                           const Real* __restrict__ R, GridC g, uint* __restrict__ sidu, uint* __restrict__ skeyu,
-                          R4<Real>* __restrict__ sposu) {
+                          R4<Real>* __restrict__ sposu, uint* __restrict__ tpos) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint c = key[i];
@@ -195,14 +197,17 @@ __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint*
     sidu[slot] = (uint)i;
     skeyu[slot] = c;
     sposu[slot] = v;
+    tpos[i] = slot;
 }
 
 // Order each cell's members by id: together with the counting scatter this is
 // the stable sort by cell of calcHash + RadixSort (dempacking.cu:545-555).
+// Run on request only (dem_download_cells); the re-list needs no order inside
+// a cell.
 template <typename Real>
 __global__ void k_rank(long long n, const uint* __restrict__ cstart, const uint* __restrict__ sidu,
                        const uint* __restrict__ skeyu, const R4<Real>* __restrict__ sposu, uint* __restrict__ sid2,
-                       uint* __restrict__ skey, R4<Real>* __restrict__ spos, uint* __restrict__ tpos) {
+                       uint* __restrict__ skey, R4<Real>* __restrict__ spos) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const uint i = sidu[t];
@@ -213,7 +218,6 @@ __global__ void k_rank(long long n, const uint* __restrict__ cstart, const uint*
     sid2[s + rank] = i;
     skey[s + rank] = c;
     spos[s + rank] = sposu[t];
-    tpos[i] = s + rank;
 }
 
 // Walk the 27 cells around sorted slot t and either count (FILL=false) or
@@ -1175,11 +1179,9 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
     if (rc) return rc;
     k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->arrival, c->cstart, c->ccount, S, (const Real*)c->rad,
-                                                 g, c->sid, c->skeyu, (R4<Real>*)c->sposu);
-    k_rank<Real><<<grid_for(n, B), B, 0, s>>>(n, c->cstart, c->sid, c->skeyu, (const R4<Real>*)c->sposu, c->sid2,
-                                              c->skey, (R4<Real>*)c->spos, c->tpos);
+                                                 g, c->sid, c->skeyu, (R4<Real>*)c->sposu, c->tpos);
     const Real skin = (Real)c->cfg.skin;
-    k_nbr_walk<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin,
+    k_nbr_walk<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid, (const R4<Real>*)c->sposu, c->skeyu, c->cstart, g, skin,
                                                   c->wslot, c->njgi, c->njli, c->bflag, c->scr, c->words);
     {
         const uint* in[3] = {c->njgi, c->njli, c->bflag};
@@ -1189,7 +1191,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         if (rc) return rc;
     }
     k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
-        n, c->sid2, (const R4<Real>*)c->spos, c->skey, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
+        n, c->sid, (const R4<Real>*)c->sposu, c->skeyu, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
         c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
         planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry, c->scr,
         c->bflag, c->bpos, c->blist, c->flist, c->tpos);
@@ -2047,6 +2049,16 @@ int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsign
     if (!c) return fail(DEM_ERR_ARG, "dem_download_cells: null ctx");
     if (!c->uploaded || c->relists == 0) return fail(DEM_ERR_STATE, "dem_download_cells: no list built yet");
     const long long n = c->n, nc = c->ncells;
+    // the re-list left each cell's members in arrival order: order them by id
+    if (c->prec == DEM_PREC_MIXED)
+        k_rank<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->cstart, c->sid, c->skeyu,
+                                                               (const R4<float>*)c->sposu, c->sid2, c->skey,
+                                                               (R4<float>*)c->spos);
+    else
+        k_rank<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->cstart, c->sid, c->skeyu,
+                                                                (const R4<double>*)c->sposu, c->sid2, c->skey,
+                                                                (R4<double>*)c->spos);
+    DEM_LAUNCH_CHECK();
     if (ids) DEM_CUDA_TRY(cudaMemcpyAsync(ids, c->sid2, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     if (keys) DEM_CUDA_TRY(cudaMemcpyAsync(keys, c->skey, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     std::vector<uint> cs;

@@ -271,6 +271,26 @@ def run_ours(args):
         ppm = {"value": w.n * k3 * win / (ms3 / 1e3), "unit": UNIT, "windows": k3,
                "pccp_over_pp": (value / ws) / (w.n * k3 * win / (ms3 / 1e3))}
 
+    # --- the 4,000,000-sphere bidisperse workload (mixed): the step at scale
+    scale = None
+    if not args.skip_4m and args.precision == "mixed" and ws == 1:
+        import dem_b200.workloads as wmod
+        w4 = wmod.bidisperse_4m()
+        e4 = dem.Engine(**w4.engine_kwargs())
+        e4.set_stream(stream.cuda_stream)
+        e4.set_material(w4.pp, w4.pw)
+        e4.upload(w4.pos, w4.rad)
+        with torch.cuda.stream(stream):
+            e4.step(3 * win)
+        e4.upload(w4.pos, w4.rad)
+        k4 = max(10, K // 20)
+        ms4 = time_windows(torch, e4, stream, k4, flush, win)
+        s4 = e4.scalars()
+        e4.close()
+        scale = {"workload": "bidisperse_4m", "n_particles": w4.n, "value": w4.n * k4 * win / (ms4 / 1e3),
+                 "unit": UNIT, "windows": k4, "ms_per_dem_step": ms4 / (k4 * win),
+                 "pairs_per_particle": s4["pairs"] / w4.n, "status": s4["status"]}
+
     # --- adjoint window cost on the pre-settled 50,000-sphere workload
     adj = None
     if not args.skip_adjoint:
@@ -343,6 +363,7 @@ def run_ours(args):
         "gpu_launches": KERNELS_PER_WINDOW * K,
         "fp64_plain": fp64,
         "pp_mode": ppm,
+        "scale_4m": scale,
         "adjoint": adj,
         "e2e": e2e,
         "cpu_baseline": cpu,
@@ -448,6 +469,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-pp", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-4m", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -186,6 +186,36 @@ def test_full_size_rsa_500k_list_bit_exact(dem, orc, wl, cuda):
     assert np.all(np.diff(key) > 0)
 
 
+def test_full_size_bidisperse_4m(dem, orc, wl, cuda):
+    """The 4,000,000-sphere bidisperse workload (radii 0.4/0.6 mm, 200x200x600
+    mm): the canonical pair set at full size matches the oracle exactly, ten
+    windows run clean, and the mixed form's packing fraction is the FP64
+    form's within 1e-3."""
+    w = wl.bidisperse_4m()
+    e = make_engine(dem, w)
+    e.step(1)
+    keys, ids, st, en = e.cells()
+    cell = e.grid_info()[1]
+    g, sk, si, cs, ce = oracle_cells(orc, w, cell, True)
+    np.testing.assert_array_equal(keys, sk)
+    np.testing.assert_array_equal(ids, si)
+    lp, ln, _ = e.pairs()
+    off, oln, _, _ = orc.build_list(w.pos, w.rad, w.world, cell, w.skin, True)
+    np.testing.assert_array_equal(ln, oln)
+    np.testing.assert_array_equal(lp, np.repeat(np.arange(w.n, dtype=np.uint32), np.diff(off)))
+    e.step(10 * w.relist_interval - 1)
+    s = e.scalars()
+    assert s["status"] == 0 and s["relists"] == 10
+    lp, ln, _ = e.pairs()
+    key = lp.astype(np.uint64) << np.uint64(32) | ln.astype(np.uint64)
+    assert np.all(lp < ln) and np.all(np.diff(key) > 0)
+    f = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_FP64})
+    f.set_material(w.pp, w.pw)
+    f.upload(w.pos, w.rad)
+    f.step(10 * w.relist_interval)
+    assert abs(f.scalars()["packing_fraction"] - s["packing_fraction"]) <= 1e-3
+
+
 def test_mixed_vs_fp64_oracle_packing_fraction(dem, orc, wl, cuda):
     """Mixed-precision run of a reduced rsa workload (20,000 spheres, 1,000
     steps) against the FP64 oracle: packing fraction within 1e-3."""

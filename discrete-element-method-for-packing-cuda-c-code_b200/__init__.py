@@ -191,6 +191,7 @@ _SIGS = [
     ("dem_save_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("dem_load_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("dem_set_pour", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_double, ctypes.c_longlong]),
+    ("dem_check_barrier_timeout", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("dem_active_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     ("dem_write_finish", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p]),
 ]
@@ -505,6 +506,13 @@ class Engine:
         states; n_active particles are in the system, and nplayer more join
         before every step whose time dt*it passes N*tnewpar/nplayer."""
         check(lib().dem_set_pour(self._h, int(nplayer), float(tnewpar), int(n_active)), "dem_set_pour")
+
+    def check_barrier_timeout(self):
+        """Run one grid-barrier wait that cannot complete (dem_check_barrier_timeout):
+        it must give up and report DEM_ERR_TIMEOUT; returns the ms waited."""
+        ms = ctypes.c_double(0.0)
+        check(lib().dem_check_barrier_timeout(self._h, ctypes.byref(ms)), "dem_check_barrier_timeout")
+        return ms.value
 
     def active_count(self):
         v = ctypes.c_longlong(0)

@@ -846,11 +846,13 @@ __device__ __forceinline__ void red_release_add(uint* p, uint v) {
 // Grid-wide barrier number `k` (0, 1, ...) of a window-kernel launch: every
 // block adds 1 to the arrival counter with release semantics and waits, with
 // acquire loads, until it reaches (k+1) x blocks (bounded as above).
-__device__ __forceinline__ void grid_barrier(uint* bar, uint k, EngineWords* words) {
+__device__ __forceinline__ void grid_arrive(uint* bar) {
     __syncthreads();
+    if (threadIdx.x == 0) red_release_add(bar, 1u);
+}
+__device__ __forceinline__ void grid_wait(uint* bar, uint k, EngineWords* words) {
     if (threadIdx.x == 0) {
         const uint target = (k + 1u) * gridDim.x;
-        red_release_add(bar, 1u);
         if (!ld_acquire(bar + kBarGiveUp)) {
             unsigned long long t0 = global_ns();
             uint polls = 0;
@@ -868,6 +870,21 @@ __device__ __forceinline__ void grid_barrier(uint* bar, uint k, EngineWords* wor
         }
     }
     __syncthreads();
+}
+__device__ __forceinline__ void grid_barrier(uint* bar, uint k, EngineWords* words) {
+    grid_arrive(bar);
+    grid_wait(bar, k, words);
+}
+
+// Check of the bounded wait: the launch's one block arrives once and waits
+// for barrier 1, which needs a second arrival that never comes; the wait must
+// give up, record kStBarrier and raise the give-up word.  `spent` receives
+// the nanoseconds waited.
+__global__ void k_barrier_check(uint* bar, EngineWords* words, unsigned long long* spent) {
+    const unsigned long long t0 = global_ns();
+    grid_arrive(bar);          // the counter reaches 1
+    grid_wait(bar, 1, words);  // waits for 2 (one block): gives up
+    if (threadIdx.x == 0) *spent = global_ns() - t0;
 }
 
 // The whole window's steps in one cooperative launch (after the re-list):
@@ -2111,6 +2128,33 @@ int dem_set_window_timing(dem_ctx* c, int on) {
         }
     }
     c->wtiming = on != 0;
+    return DEM_OK;
+}
+
+int dem_check_barrier_timeout(dem_ctx* c, double* waited_ms) {
+    if (!c || !waited_ms) return fail(DEM_ERR_ARG, "dem_check_barrier_timeout: null argument");
+    *waited_ms = 0.0;
+    if (c->in_window != 0) return fail(DEM_ERR_STATE, "dem_check_barrier_timeout: call at a re-list boundary");
+    unsigned long long* spent = nullptr;
+    int rc = dalloc(&spent, 1);
+    if (rc) return rc;
+    cudaStream_t s = c->stream;
+    cudaError_t e = cudaMemsetAsync(c->bar, 0, kBarWords * sizeof(uint), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(spent, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) {
+        k_barrier_check<<<1, 32, 0, s>>>(c->bar, c->words, spent);
+        e = cudaGetLastError();
+    }
+    unsigned long long ns = 0;
+    EngineWords w{};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ns, spent, sizeof(ns), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&w, c->words, sizeof(w), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(spent);
+    if (e != cudaSuccess) return cuda_fail(e, "dem_check_barrier_timeout", __FILE__, __LINE__);
+    *waited_ms = (double)ns * 1e-6;
+    if (!(w.status & kStBarrier))
+        return fail(DEM_ERR_STATE, "dem_check_barrier_timeout: the wait did not report its timeout");
     return DEM_OK;
 }
 

@@ -288,6 +288,14 @@ int dem_kernel_times(dem_ctx* ctx, double out[3]);
  * out[3]=the forked free-particle kernel (whole window); window-kernel path
  * (PCCP default): out[4]=the window kernel (all steps).  PP mode: out[1] ~ 0,
  * out[2] the fused step. */
+/* Check of the window kernel's bounded grid-barrier wait (no fault, no
+ * hang): on the context's stream, one block waits for a barrier arrival that
+ * never comes; the wait gives up after about 1 s, records the timeout in the
+ * status word (dem_get_scalars then reports DEM_ERR_TIMEOUT until the next
+ * upload) and the launch ends.  DEM_OK when the timeout was reported;
+ * *waited_ms receives the time the block waited.  At a re-list boundary
+ * (DEM_ERR_STATE otherwise). */
+int dem_check_barrier_timeout(dem_ctx* ctx, double* waited_ms);
 int dem_set_window_timing(dem_ctx* ctx, int on);
 int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
 

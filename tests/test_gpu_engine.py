@@ -410,3 +410,23 @@ def test_pp_mode_trajectory_vs_oracle(dem, orc, wl, cuda):
     o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, dem.material_array(w.pp, w.pw), False, steps,
                 w.relist_interval)
     assert np.sqrt(np.mean((pos - o["pos"]) ** 2)) <= 1e-9
+
+
+def test_barrier_wait_gives_up_and_context_stays_usable(dem, wl, cuda):
+    """The window kernel's grid-barrier wait is bounded: a wait for an arrival
+    that never comes gives up after about a second, the status word reports
+    DEM_ERR_TIMEOUT, and after a new upload the context steps exactly as a
+    fresh one does (no fault, no hang, nothing left behind)."""
+    w = wl.small_box(n=2000)
+    e = make_engine(dem, w)
+    e.step(w.relist_interval)
+    ms = e.check_barrier_timeout()
+    assert 900.0 <= ms <= 30000.0, ms
+    assert e.scalars()["status"] == dem.DEM_ERR_TIMEOUT
+    e.upload(w.pos, w.rad)
+    e.step(3 * w.relist_interval)
+    assert e.scalars()["status"] == 0
+    f = make_engine(dem, w)
+    f.step(3 * w.relist_interval)
+    for x, y in zip(e.download(), f.download()):
+        np.testing.assert_array_equal(x, y)

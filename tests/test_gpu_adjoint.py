@@ -174,3 +174,37 @@ def test_adjoint_settle_50k_window(dem, wl, cuda):
     vm = value(w.pp, w.pw, w.rad - v)["value"]
     g_fd = (vp - vm) / 2.0
     assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd), (g_ad, g_fd)
+
+
+def test_autograd_function_matches_finite_differences(dem, wl, cuda):
+    """The adjoint through a torch.autograd.Function of the physical
+    parameters (tests/_adjoint_torch.py): torch.autograd.grad of the
+    potential energy after the window with respect to Young's modulus,
+    restitution, sliding and rolling friction and the radii, against central
+    differences of the same window.  Tolerance 1e-3 relative plus the FD noise
+    floor (1e-8 of the objective)."""
+    import torch
+    from _adjoint_torch import DemWindow, WindowSetup, window_value
+    w, pdis, angv = case(dem)
+    s = WindowSetup(dem, wl, w, w.pos, pdis, angv, STEPS, EVERY, dem.OBJ_POTENTIAL, dem.PREC_FP64, w.cell() + 0.01)
+    p0 = {"E": 1e7, "e": 0.5, "mu": 0.3, "mu_r": 0.002}
+    xs = {k: torch.tensor(v, dtype=torch.float64, requires_grad=True) for k, v in p0.items()}
+    rad = torch.tensor(w.rad, dtype=torch.float64, requires_grad=True)
+    val = DemWindow.apply(xs["E"], xs["e"], xs["mu"], xs["mu_r"], rad, s)
+    g = torch.autograd.grad(val, [xs["E"], xs["e"], xs["mu"], xs["mu_r"], rad])
+    base = float(val.detach())
+    assert np.isfinite(base) and base > 0
+    floor = 1e-8 * abs(base)
+    for idx, k in enumerate(("E", "e", "mu", "mu_r")):
+        h = 1e-5 * p0[k] if k != "e" else 1e-5
+        vp = window_value(s, **{**p0, k: p0[k] + h}, rad=w.rad)
+        vm = window_value(s, **{**p0, k: p0[k] - h}, rad=w.rad)
+        g_fd = (vp - vm) / (2 * h) * (p0[k] if k != "e" else 1.0)
+        g_ad = float(g[idx]) * (p0[k] if k != "e" else 1.0)
+        assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd) + floor, (k, g_ad, g_fd)
+    rng = np.random.default_rng(7)
+    v = rng.normal(size=w.n)
+    hr = 1e-9
+    g_fd = (window_value(s, **p0, rad=w.rad + hr * v) - window_value(s, **p0, rad=w.rad - hr * v)) / (2 * hr)
+    g_ad = float(g[4].numpy() @ v)
+    assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd), (g_ad, g_fd)

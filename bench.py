@@ -38,7 +38,8 @@ BYTES_PER_PARTICLE = {"mixed": 172, "fp64": 200}   # per particle-step, all fiel
 BYTES_PER_PAIR = 56                                 # ids 8 + FP64 history r+w 48, per pair-step
 METRIC = "particle-steps/s @500K spheres"
 UNIT = "particle-steps/s"
-KERNELS_PER_WINDOW = 12 + 1   # re-list (incl. 2 scan passes x 3 launches) + the window kernel
+KERNELS_PER_WINDOW = 11 + 1   # re-list: hash, 3-launch cell scan, scatter, walk, 3-launch triple scan, fill,
+                              # reverse sort; + the window kernel
 
 
 def load_pkg():

@@ -154,6 +154,10 @@ _SIGS = [
     ("dem_download_state_device", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("dem_step_n", ctypes.c_int, [_vp, ctypes.c_longlong]),
     ("dem_get_scalars", ctypes.c_int, [_vp, ctypes.POINTER(Scalars)]),
+    ("dem_scalars_raw_bytes", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    ("dem_scalars_enqueue", ctypes.c_int, [_vp, _vp]),
+    ("dem_scalars_from_raw", ctypes.c_int, [_vp, _vp, ctypes.POINTER(Scalars)]),
+    ("dem_synchronize", ctypes.c_int, [_vp]),
     ("dem_record_forces", ctypes.c_int, [_vp, ctypes.c_int]),
     ("dem_download_forces", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("dem_download_pairs", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
@@ -421,6 +425,27 @@ class Engine:
         if raise_on_status:
             check(rc, "dem_get_scalars")
         return s.as_dict()
+
+    def scalars_raw_bytes(self):
+        v = ctypes.c_longlong(0)
+        check(lib().dem_scalars_raw_bytes(self._h, ctypes.byref(v)), "dem_scalars_raw_bytes")
+        return v.value
+
+    def scalars_enqueue(self, raw_addr):
+        """Queue the observables' copy into host memory at raw_addr (pinned
+        for an asynchronous copy; scalars_raw_bytes() bytes); no wait."""
+        check(lib().dem_scalars_enqueue(self._h, ctypes.c_void_p(raw_addr)), "dem_scalars_enqueue")
+
+    def scalars_from_raw(self, raw_addr, raise_on_status=True):
+        """Observables from a buffer filled by scalars_enqueue (after a sync)."""
+        s = Scalars()
+        rc = lib().dem_scalars_from_raw(self._h, ctypes.c_void_p(raw_addr), ctypes.byref(s))
+        if raise_on_status:
+            check(rc, "dem_scalars_from_raw")
+        return s.as_dict()
+
+    def synchronize(self):
+        check(lib().dem_synchronize(self._h), "dem_synchronize")
 
     def download(self):
         pos = np.empty(3 * self.n)

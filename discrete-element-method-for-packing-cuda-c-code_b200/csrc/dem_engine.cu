@@ -1953,45 +1953,89 @@ int dem_active_count(dem_ctx* c, long long* n_active) {
     return DEM_OK;
 }
 
-int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
-    if (!c || !out) return fail(DEM_ERR_ARG, "dem_get_scalars: null argument");
-    memset(out, 0, sizeof(*out));
-    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_get_scalars: no state uploaded");
-    char* hp = (char*)c->host_pinned;
-    DEM_CUDA_TRY(cudaMemcpyAsync(hp, c->words, sizeof(EngineWords), cudaMemcpyDeviceToHost, c->stream));
-    DEM_CUDA_TRY(cudaMemcpyAsync(hp + 64, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    std::vector<unsigned long long> pm;
-    std::vector<uint> pc;
+// Raw observables of the last step, as dem_scalars_enqueue leaves them in
+// host memory: a header of host-side counters taken at enqueue time, the
+// status words, the current list's pair count and the last step's per-block
+// partials (max height, contact count).
+namespace {
+struct RawHead {
+    long long step, relists, n, last_slot;
+    double vol;
+    unsigned long long npart;
+    long long pad[2];
+};
+static_assert(sizeof(RawHead) == 64, "raw header");
+constexpr size_t kRawWords = 64, kRawPairs = 80, kRawMz = 96;
+size_t raw_bytes(const dem_ctx* c) { return kRawMz + c->npart * (sizeof(unsigned long long) + sizeof(uint)); }
+}  // namespace
+
+int dem_scalars_raw_bytes(dem_ctx* c, long long* bytes) {
+    if (!c || !bytes) return fail(DEM_ERR_ARG, "dem_scalars_raw_bytes: null argument");
+    *bytes = (long long)raw_bytes(c);
+    return DEM_OK;
+}
+
+int dem_scalars_enqueue(dem_ctx* c, void* raw) {
+    if (!c || !raw) return fail(DEM_ERR_ARG, "dem_scalars_enqueue: null argument");
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_scalars_enqueue: no state uploaded");
+    char* r = (char*)raw;
+    RawHead h{};
+    h.step = c->step;
+    h.relists = c->relists;
+    h.n = c->n;
+    h.last_slot = c->last_slot;
+    h.vol = c->vol;
+    h.npart = c->npart;
+    memcpy(r, &h, sizeof(h));
+    cudaStream_t s = c->stream;
+    DEM_CUDA_TRY(cudaMemcpyAsync(r + kRawWords, c->words, sizeof(EngineWords), cudaMemcpyDeviceToHost, s));
+    DEM_CUDA_TRY(cudaMemcpyAsync(r + kRawPairs, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, s));
     if (c->last_slot >= 0) {
-        pm.resize(c->npart);
-        pc.resize(c->npart);
-        DEM_CUDA_TRY(cudaMemcpyAsync(pm.data(), c->part_mz + (size_t)c->last_slot * c->npart,
-                                     c->npart * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
-        DEM_CUDA_TRY(cudaMemcpyAsync(pc.data(), c->part_cnt + (size_t)c->last_slot * c->npart,
-                                     c->npart * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+        DEM_CUDA_TRY(cudaMemcpyAsync(r + kRawMz, c->part_mz + (size_t)c->last_slot * c->npart,
+                                     c->npart * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        DEM_CUDA_TRY(cudaMemcpyAsync(r + kRawMz + c->npart * sizeof(unsigned long long),
+                                     c->part_cnt + (size_t)c->last_slot * c->npart, c->npart * sizeof(uint),
+                                     cudaMemcpyDeviceToHost, s));
     }
-    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DEM_OK;
+}
+
+int dem_scalars_from_raw(dem_ctx* c, const void* raw, dem_scalars* out) {
+    if (!c || !raw || !out) return fail(DEM_ERR_ARG, "dem_scalars_from_raw: null argument");
+    memset(out, 0, sizeof(*out));
+    const char* r = (const char*)raw;
+    RawHead h;
+    memcpy(&h, r, sizeof(h));
+    if (h.npart != (unsigned long long)c->npart) return fail(DEM_ERR_ARG, "dem_scalars_from_raw: not this context's");
     EngineWords w;
-    memcpy(&w, hp, sizeof(w));
+    memcpy(&w, r + kRawWords, sizeof(w));
     uint P;
-    memcpy(&P, hp + 64, sizeof(P));
+    memcpy(&P, r + kRawPairs, sizeof(P));
     unsigned long long mzb = 0, csum = 0;
-    for (size_t b = 0; b < pm.size(); b++) {
-        mzb = std::max(mzb, pm[b]);
-        csum += pc[b];
+    if (h.last_slot >= 0) {
+        const char* pm = r + kRawMz;
+        const char* pc = pm + h.npart * sizeof(unsigned long long);
+        for (size_t b = 0; b < (size_t)h.npart; b++) {
+            unsigned long long m;
+            uint k;
+            memcpy(&m, pm + b * sizeof(m), sizeof(m));
+            memcpy(&k, pc + b * sizeof(k), sizeof(k));
+            mzb = std::max(mzb, m);
+            csum += k;
+        }
     }
     double mz;
     memcpy(&mz, &mzb, sizeof(mz));
-    out->step = c->step;
-    out->pairs = c->relists ? (long long)P : 0;
+    out->step = h.step;
+    out->pairs = h.relists ? (long long)P : 0;
     out->contacts = (long long)(csum / 2);
     out->maxhz = mz;
-    out->relists = c->relists;
+    out->relists = h.relists;
     out->max_row = (int)w.max_row;
     // packing fraction sum (4/3) pi r^3 / (Wx Wy maxhz): dempacking.cu:768-771
     // with the monodisperse N pi/6 generalised; mean CN = pcntot/N (:768).
-    out->mean_cn = c->n > 0 ? (double)csum / (double)c->n : 0.0;
-    out->packing_fraction = mz > 0.0 ? c->vol / (c->cfg.world[0] * c->cfg.world[1] * mz) : 0.0;
+    out->mean_cn = h.n > 0 ? (double)csum / (double)h.n : 0.0;
+    out->packing_fraction = mz > 0.0 ? h.vol / (c->cfg.world[0] * c->cfg.world[1] * mz) : 0.0;
     int status = DEM_OK;
     if (w.status & kStBarrier) status = DEM_ERR_TIMEOUT;
     else if (w.status & kStNonfinite) status = DEM_ERR_NONFINITE;
@@ -2004,6 +2048,23 @@ int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
     if (status == DEM_ERR_SKIN)
         return fail(DEM_ERR_SKIN, "a particle moved more than skin/2 = %g within a re-list window", 0.5 * c->cfg.skin);
     return DEM_OK;
+}
+
+int dem_synchronize(dem_ctx* c) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_synchronize: null ctx");
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DEM_OK;
+}
+
+int dem_get_scalars(dem_ctx* c, dem_scalars* out) {
+    if (!c || !out) return fail(DEM_ERR_ARG, "dem_get_scalars: null argument");
+    memset(out, 0, sizeof(*out));
+    if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_get_scalars: no state uploaded");
+    std::vector<unsigned long long> raw((raw_bytes(c) + 7) / 8);
+    int rc = dem_scalars_enqueue(c, raw.data());
+    if (rc) return rc;
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return dem_scalars_from_raw(c, raw.data(), out);
 }
 
 int dem_record_forces(dem_ctx* c, int on) {

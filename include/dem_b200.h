@@ -261,6 +261,18 @@ int dem_download_state_device(dem_ctx* ctx, double* pos, double* pdis, double* a
 int dem_step_n(dem_ctx* ctx, long long nsteps);
 /* Synchronises; observables of the last step and the sticky status. */
 int dem_get_scalars(dem_ctx* ctx, dem_scalars* out);
+/* Observables without a host wait.  dem_scalars_enqueue queues, on the
+ * context's stream, the device-to-host copy of what dem_get_scalars reads
+ * (status, pair count, the last step's per-block partials) into `raw`, host
+ * memory of dem_scalars_raw_bytes bytes (pinned memory makes the copy
+ * asynchronous), and returns at once; once the stream has passed the copy
+ * (dem_synchronize or any call that waits), dem_scalars_from_raw reduces it
+ * to the dem_scalars of that moment, with dem_get_scalars' return codes.
+ * Each enqueue needs its own buffer until it has been reduced. */
+int dem_scalars_raw_bytes(dem_ctx* ctx, long long* bytes);
+int dem_scalars_enqueue(dem_ctx* ctx, void* raw);
+int dem_scalars_from_raw(dem_ctx* ctx, const void* raw, dem_scalars* out);
+int dem_synchronize(dem_ctx* ctx);
 /* Record per-particle force/torque/contact count of each step into device
  * buffers (off by default; costs 52 bytes per particle-step of writes). */
 int dem_record_forces(dem_ctx* ctx, int on);

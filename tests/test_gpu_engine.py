@@ -430,3 +430,29 @@ def test_barrier_wait_gives_up_and_context_stays_usable(dem, wl, cuda):
     f.step(3 * w.relist_interval)
     for x, y in zip(e.download(), f.download()):
         np.testing.assert_array_equal(x, y)
+
+
+def test_observables_without_a_host_wait(dem, wl, cuda):
+    """dem_scalars_enqueue after every window (pinned buffers, no wait), one
+    synchronisation, then dem_scalars_from_raw: the same observables, step by
+    step, as dem_get_scalars on a second context; a buffer is refused by a
+    context of another size."""
+    import torch
+    w = wl.small_box(n=3000)
+    K = w.relist_interval
+    a, b = make_engine(dem, w), make_engine(dem, w)
+    rb = a.scalars_raw_bytes()
+    raws = torch.empty((6, rb), dtype=torch.uint8).pin_memory()
+    sync = []
+    for k in range(6):
+        a.step(K + (k == 3) * 7)                      # one call ends inside a window
+        a.scalars_enqueue(raws[k].data_ptr())
+        b.step(K + (k == 3) * 7)
+        sync.append(b.scalars())
+    a.synchronize()
+    for k in range(6):
+        assert a.scalars_from_raw(raws[k].data_ptr()) == sync[k], k
+    other = make_engine(dem, wl.rsa_500k(precision=dem.PREC_MIXED, n=30_000, box=(40.0, 40.0, 120.0)))
+    with pytest.raises(dem.DemError) as e:
+        other.scalars_from_raw(raws[0].data_ptr())
+    assert e.value.code == dem.DEM_ERR_ARG

@@ -34,6 +34,7 @@ namespace dem {
 namespace {
 constexpr int kB = 256;
 constexpr int kPairB = 128;   // block size of k_adj_step; pbar holds one 12-slot row per block
+constexpr long long kScatterPrime = 2654435761ll;
 
 struct Ck {
     void* rec = nullptr;     // np particle records
@@ -289,11 +290,17 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
     __shared__ double sp[12][kPairB / 32];
     const double inv_dt = 1.0 / dt;
     const long long u0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nb = (long long)*nbp;
     LawBar bp, bw;
     lawbar_zero(bp);
     lawbar_zero(bw);
-    if (u0 < (long long)*nbp) {
-        const long long i = blist[u0];
+    if (u0 < nb) {
+        // bound particles in a scattered order (u0 -> u0 * p mod nb, p a
+        // prime above any particle count: a bijection): with the particles
+        // stored in cell order, neighbours with many contacts -- long FP64
+        // chains -- would otherwise fill the same warps (measured: 25 % longer
+        // reverse sweeps); scattered, every warp gets a mix
+        const long long i = blist[(u0 * kScatterPrime) % nb];
         const Real rr = R[i];
         const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
         V3d dtot, fbi, tbi;
@@ -807,6 +814,10 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (d_radii) DEM_CUDA_TRY(cudaMemcpyAsync(d_radii, w->Rb, c->n * sizeof(double), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
+    if (d_radii && c->ordered) {   // into the caller's particle order
+        std::vector<double> t(d_radii, d_radii + c->n);
+        for (long long i = 0; i < c->n; i++) d_radii[c->hperm[i]] = t[i];
+    }
     double acc[12] = {0};
     for (size_t b = 0; b < (size_t)w->npb; b++)
         for (int k = 0; k < 12; k++) acc[k] += pb[b * 12 + k];

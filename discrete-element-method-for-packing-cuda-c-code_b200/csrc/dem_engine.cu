@@ -80,16 +80,20 @@ template <typename Real> __device__ __forceinline__ bool cand_test(const R4<Real
 __device__ __forceinline__ uint lane_id() { return threadIdx.x & 31; }
 
 // ------------------------------------------------------------ state I/O
+// Internal slot i takes the caller's particle perm[i] (identity when perm is
+// null).
 template <typename Real>
 __global__ void k_from_aos(long long n, const double* __restrict__ pos, const double* __restrict__ pdis,
                            const double* __restrict__ angv, const double* __restrict__ rad, PRec<Real>* __restrict__ S,
-                           Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W) {
+                           Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
+                           const uint* __restrict__ perm) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const V3<double> x = mk(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
-    const V3<double> d = pdis ? mk(pdis[3 * i], pdis[3 * i + 1], pdis[3 * i + 2]) : zero3<double>();
-    const V3<Real> a = angv ? mk((Real)angv[3 * i], (Real)angv[3 * i + 1], (Real)angv[3 * i + 2]) : zero3<Real>();
-    const Real r = (Real)rad[i];
+    const long long u = perm ? (long long)perm[i] : i;
+    const V3<double> x = mk(pos[3 * u], pos[3 * u + 1], pos[3 * u + 2]);
+    const V3<double> d = pdis ? mk(pdis[3 * u], pdis[3 * u + 1], pdis[3 * u + 2]) : zero3<double>();
+    const V3<Real> a = angv ? mk((Real)angv[3 * u], (Real)angv[3 * u + 1], (Real)angv[3 * u + 2]) : zero3<Real>();
+    const Real r = (Real)rad[u];
     st_rec(S + i, x, d, a, r);
     R[i] = r;
     Q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -97,19 +101,22 @@ __global__ void k_from_aos(long long n, const double* __restrict__ pos, const do
 }
 
 // Particles nact .. n-1 (not yet poured in) report their injection state.
+// Internal slot i goes to the caller's particle perm[i] (identity when perm is
+// null).
 template <typename Real>
 __global__ void k_to_aos(long long n, long long nact, const PRec<Real>* __restrict__ S,
                          const PRec<Real>* __restrict__ pour, double* __restrict__ pos, double* __restrict__ pdis,
-                         double* __restrict__ angv) {
+                         double* __restrict__ angv, const uint* __restrict__ perm) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     V3<double> x, d;
     V3<Real> a;
     Real r;
     ld_rec<false>((i < nact ? S : pour) + i, x, d, a, r);
-    if (pos) { pos[3 * i] = x.x; pos[3 * i + 1] = x.y; pos[3 * i + 2] = x.z; }
-    if (pdis) { pdis[3 * i] = d.x; pdis[3 * i + 1] = d.y; pdis[3 * i + 2] = d.z; }
-    if (angv) { angv[3 * i] = (double)a.x; angv[3 * i + 1] = (double)a.y; angv[3 * i + 2] = (double)a.z; }
+    const long long u = perm ? (long long)perm[i] : i;
+    if (pos) { pos[3 * u] = x.x; pos[3 * u + 1] = x.y; pos[3 * u + 2] = x.z; }
+    if (pdis) { pdis[3 * u] = d.x; pdis[3 * u + 1] = d.y; pdis[3 * u + 2] = d.z; }
+    if (angv) { angv[3 * u] = (double)a.x; angv[3 * u + 1] = (double)a.y; angv[3 * u + 2] = (double)a.z; }
 }
 
 // Poured packing: particles nold .. nnew-1 join the system with their
@@ -1616,6 +1623,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
         const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches inside a window
         c->pdl = !(pdl && pdl[0] == '0');
+        const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order
+        c->reorder = !(ro && ro[0] == '0');
     }
     // partials per slot: particle-kernel blocks, free-kernel blocks, and at
     // least as many as the window kernel has blocks
@@ -1662,7 +1671,7 @@ int dem_destroy(dem_ctx* c) {
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
                     c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar,
-                    c->tpos, c->pour_rec};
+                    c->tpos, c->pour_rec, c->perm};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
@@ -1757,8 +1766,42 @@ static int finish_upload(dem_ctx* c) {
     return setup_grid(c);
 }
 
-static int upload_common(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad,
-                         bool host) {
+// The order of a host upload: internal slot t holds the caller's particle
+// perm[t], ascending (cell key, id) on the context's cell grid (any order
+// that keeps neighbours together serves; this one is the re-list's).  Empty
+// when the grid is too large for the host count.
+static void cell_order(const dem_ctx* c, const double* pos, long long n, std::vector<uint>& perm) {
+    perm.clear();
+    const double cs = c->cfg.cell > 0.0 ? c->cfg.cell : 2.0 * c->rmax + c->cfg.skin + 1e-4;
+    const long long gx = (long long)(c->cfg.world[0] / cs) + 1, gy = (long long)(c->cfg.world[1] / cs) + 1,
+                    gz = (long long)(c->cfg.world[2] / cs) + 1;
+    const long long nc = gx * gy * gz;
+    if (!(cs > 0.0) || nc > (1ll << 27)) return;
+    auto cell = [cs](double v, long long g) -> long long {
+        const double f = v / cs;
+        if (!(f >= 0.0)) return 0;           // below the origin, or not a number
+        return f >= (double)g ? g - 1 : (long long)f;
+    };
+    std::vector<uint> key(n), cnt(nc + 1, 0u);
+    for (long long i = 0; i < n; i++) {
+        const long long cx = cell(pos[3 * i] + 0.5 * c->cfg.world[0], gx);
+        const long long cy = cell(pos[3 * i + 1] + 0.5 * c->cfg.world[1], gy);
+        const long long cz = cell(pos[3 * i + 2], gz);
+        key[i] = (uint)((cz * gy + cy) * gx + cx);
+        cnt[key[i] + 1]++;
+    }
+    for (long long k = 0; k < nc; k++) cnt[k + 1] += cnt[k];
+    perm.resize(n);
+    for (long long i = 0; i < n; i++) perm[cnt[key[i]]++] = (uint)i;
+}
+
+enum UploadOrder { kOrderCaller = 0, kOrderCells = 1, kOrderGiven = 2 };
+
+// kOrderCells (host buffers only): sort by cell; kOrderCaller: keep the
+// caller's order; kOrderGiven: the buffers are already in internal order and
+// `given` is its permutation (a state file's).
+static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad,
+                       bool host, int order, const uint* given) {
     if (!c || !pos || !rad) return fail(DEM_ERR_ARG, "dem_upload_state: null argument");
     // every particle the context holds is in the system again (a pour ends);
     // graphs captured for fewer particles go
@@ -1769,6 +1812,8 @@ static int upload_common(dem_ctx* c, const double* pos, const double* pdis, cons
     double* st = c->staging;
     double *spos = st, *sd = st + 3 * np, *sa = st + 6 * np, *sr = st + 9 * np;
     const double *ppos = pos, *ppd = pdis, *ppa = angv, *prad = rad;
+    c->ordered = false;
+    c->hperm.clear();
     if (host) {
         DEM_CUDA_TRY(cudaMemcpyAsync(spos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (pdis) DEM_CUDA_TRY(cudaMemcpyAsync(sd, pdis, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -1783,6 +1828,17 @@ static int upload_common(dem_ctx* c, const double* pos, const double* pdis, cons
         }
         c->rmax = rm;
         c->vol = 4.0 / 3.0 * M_PI * v3;
+        if (order == kOrderCells && c->reorder) cell_order(c, pos, n, c->hperm);
+        else if (order == kOrderGiven && given) c->hperm.assign(given, given + n);
+        c->ordered = !c->hperm.empty();
+        if (c->ordered) {
+            if (!c->perm) {
+                int rc = dalloc(&c->perm, np);
+                if (rc) return rc;
+            }
+            DEM_CUDA_TRY(cudaMemcpyAsync(c->perm, c->hperm.data(), n * sizeof(uint), cudaMemcpyHostToDevice,
+                                         c->stream));
+        }
     } else {
         // the caller's buffers may have been written on the legacy stream
         DEM_CUDA_TRY(cudaEventRecord(c->ext_ready, 0));
@@ -1801,25 +1857,29 @@ static int upload_common(dem_ctx* c, const double* pos, const double* pdis, cons
         c->vol = 4.0 / 3.0 * M_PI * v3;
         if (!(c->rmax > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state_device: radii not positive");
     }
+    // kOrderGiven: the data are internal already (no gather), the order is recorded
+    const uint* gather = (c->ordered && order == kOrderCells) ? c->perm : nullptr;
     if (c->prec == DEM_PREC_MIXED)
         k_from_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, ppos, ppd, ppa, prad, (PRec<float>*)c->rec[0],
-                                                                  (float*)c->rad, c->q, planes<double>(c->wh, np));
+                                                                  (float*)c->rad, c->q, planes<double>(c->wh, np),
+                                                                  gather);
     else
         k_from_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, ppos, ppd, ppa, prad,
                                                                    (PRec<double>*)c->rec[0], (double*)c->rad, c->q,
-                                                                   planes<double>(c->wh, np));
+                                                                   planes<double>(c->wh, np), gather);
     DEM_LAUNCH_CHECK();
     return finish_upload(c);
 }
 
 int dem_upload_state(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
-    return upload_common(c, pos, pdis, angv, rad, true);
+    return upload_impl(c, pos, pdis, angv, rad, true, kOrderCells, nullptr);
 }
 int dem_upload_state_device(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
-    return upload_common(c, pos, pdis, angv, rad, false);
+    return upload_impl(c, pos, pdis, angv, rad, false, kOrderCaller, nullptr);
 }
 
-static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, bool host) {
+// internal: in the internal particle order (state files); else the caller's.
+static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, bool host, bool internal = false) {
     if (!c) return fail(DEM_ERR_ARG, "dem_download_state: null ctx");
     if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_download_state: no state uploaded");
     // every particle the context holds; those not yet poured in as injected
@@ -1830,12 +1890,13 @@ static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, 
     if (!pos) tp = nullptr;
     if (!pdis) td = nullptr;
     if (!angv) ta = nullptr;
+    const uint* scatter = (c->ordered && !internal) ? c->perm : nullptr;
     if (c->prec == DEM_PREC_MIXED)
         k_to_aos<float><<<grid_for(n, 256), 256, 0, c->stream>>>(
-            n, nact, (const PRec<float>*)c->rec[sb], (const PRec<float>*)c->pour_rec, tp, td, ta);
+            n, nact, (const PRec<float>*)c->rec[sb], (const PRec<float>*)c->pour_rec, tp, td, ta, scatter);
     else
         k_to_aos<double><<<grid_for(n, 256), 256, 0, c->stream>>>(
-            n, nact, (const PRec<double>*)c->rec[sb], (const PRec<double>*)c->pour_rec, tp, td, ta);
+            n, nact, (const PRec<double>*)c->rec[sb], (const PRec<double>*)c->pour_rec, tp, td, ta, scatter);
     DEM_LAUNCH_CHECK();
     if (host) {
         if (pos) DEM_CUDA_TRY(cudaMemcpyAsync(pos, tp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1918,6 +1979,28 @@ int dem_set_pour(dem_ctx* c, long long nplayer, double tnewpar, long long n_acti
     const long long ntot = c->ntot;
     const size_t recb = c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>);
     cudaStream_t s = c->stream;
+    if (c->ordered) {
+        // layers join in the caller's order: put the particles back into it
+        // (the state is kept, the contact history restarts)
+        std::vector<double> pos(3 * ntot), pdis(3 * ntot), angv(3 * ntot), rad(ntot), ri(ntot);
+        int rc = download_common(c, pos.data(), pdis.data(), angv.data(), true);
+        if (rc) return rc;
+        if (c->prec == DEM_PREC_MIXED) {
+            std::vector<float> rf(ntot);
+            DEM_CUDA_TRY(cudaMemcpyAsync(rf.data(), c->rad, ntot * sizeof(float), cudaMemcpyDeviceToHost, s));
+            DEM_CUDA_TRY(cudaStreamSynchronize(s));
+            for (long long t = 0; t < ntot; t++) ri[t] = rf[t];
+        } else {
+            DEM_CUDA_TRY(cudaMemcpyAsync(ri.data(), c->rad, ntot * sizeof(double), cudaMemcpyDeviceToHost, s));
+            DEM_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        for (long long t = 0; t < ntot; t++) rad[c->hperm[t]] = ri[t];
+        const long long step = c->step, relists = c->relists;
+        if ((rc = upload_impl(c, pos.data(), pdis.data(), angv.data(), rad.data(), true, kOrderCaller, nullptr)))
+            return rc;
+        c->step = step;
+        c->relists = relists;
+    }
     if (!c->pour_rec) DEM_CUDA_TRY(cudaMalloc(&c->pour_rec, (size_t)c->npad * recb));
     DEM_CUDA_TRY(cudaMemcpyAsync(c->pour_rec, c->rec[c->sbuf], (size_t)ntot * recb, cudaMemcpyDeviceToDevice, s));
     // r^3 prefix sums for the packing fraction of the particles in the system
@@ -2088,6 +2171,19 @@ int dem_download_forces(dem_ctx* c, double* force, double* torque, unsigned int*
     if (torque) DEM_CUDA_TRY(cudaMemcpyAsync(torque, c->dbgT, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (contacts) DEM_CUDA_TRY(cudaMemcpyAsync(contacts, c->dbgC, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->ordered) {   // into the caller's order
+        const std::vector<uint>& pm = c->hperm;
+        for (double* a : {force, torque}) {
+            if (!a) continue;
+            std::vector<double> t(a, a + 3 * n);
+            for (long long i = 0; i < n; i++)
+                for (int q = 0; q < 3; q++) a[3 * (size_t)pm[i] + q] = t[3 * (size_t)i + q];
+        }
+        if (contacts) {
+            std::vector<uint> t(contacts, contacts + n);
+            for (long long i = 0; i < n; i++) contacts[pm[i]] = t[i];
+        }
+    }
     return DEM_OK;
 }
 
@@ -2119,6 +2215,30 @@ int dem_download_pairs(dem_ctx* c, unsigned int* lp, unsigned int* ln, double* h
     cudaFree(dln);
     cudaFree(dh);
     if (e != cudaSuccess) return cuda_fail(e, "dem_download_pairs", __FILE__, __LINE__);
+    if (c->ordered) {
+        // in the caller's particle ids: each pair (lower id, higher id), the
+        // history in that pair's orientation (it changes sign when the two
+        // swap roles), sorted by (lower, higher)
+        const std::vector<uint>& pm = c->hperm;
+        std::vector<uint> a(P), b(P), idx(P);
+        std::vector<double> h;
+        if (hist) h.assign(hist, hist + 3 * (size_t)P);
+        for (uint k = 0; k < P; k++) {
+            const uint u = pm[lp[k]], v = pm[ln[k]];
+            a[k] = std::min(u, v);
+            b[k] = std::max(u, v);
+            if (hist && u > v)
+                for (int q = 0; q < 3; q++) h[3 * (size_t)k + q] = -h[3 * (size_t)k + q];
+            idx[k] = k;
+        }
+        std::sort(idx.begin(), idx.end(), [&](uint x, uint y) { return a[x] != a[y] ? a[x] < a[y] : b[x] < b[y]; });
+        for (uint k = 0; k < P; k++) {
+            lp[k] = a[idx[k]];
+            ln[k] = b[idx[k]];
+            if (hist)
+                for (int q = 0; q < 3; q++) hist[3 * (size_t)k + q] = h[3 * (size_t)idx[k] + q];
+        }
+    }
     return DEM_OK;
 }
 
@@ -2140,12 +2260,19 @@ int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsign
     if (ids) DEM_CUDA_TRY(cudaMemcpyAsync(ids, c->sid2, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     if (keys) DEM_CUDA_TRY(cudaMemcpyAsync(keys, c->skey, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     std::vector<uint> cs;
-    if (cell_start || cell_end) {
-        if (ncells_cap < nc) return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
+    const bool remap = c->ordered && ids;
+    if (cell_start || cell_end || remap) {
+        if ((cell_start || cell_end) && ncells_cap < nc)
+            return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
         cs.resize(nc + 1);
         DEM_CUDA_TRY(cudaMemcpyAsync(cs.data(), c->cstart, (nc + 1) * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     }
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (remap) {   // the caller's ids, ascending inside each cell
+        for (long long t = 0; t < n; t++) ids[t] = c->hperm[ids[t]];
+        for (long long cc = 0; cc < nc; cc++)
+            if (cs[cc + 1] - cs[cc] > 1) std::sort(ids + cs[cc], ids + cs[cc + 1]);
+    }
     if (cell_start || cell_end) {
         for (long long cc = 0; cc < nc; cc++) {
             bool empty = cs[cc] == cs[cc + 1];
@@ -2271,9 +2398,10 @@ struct StateHeader {
     dem_material mat;
     long long n_active, pour_nplayer;
     double pour_tnewpar;
+    long long ordered;   // the particle order follows (n uint32 after the header)
 };
 constexpr char kStateMagic[8] = {'D', 'E', 'M', 'B', '2', '0', '0', 'S'};
-constexpr int kStateVersion = 2;
+constexpr int kStateVersion = 3;
 
 int write_all(FILE* f, const void* p, size_t bytes) {
     return fwrite(p, 1, bytes, f) == bytes ? DEM_OK : fail(DEM_ERR_IO, "dem_save_state: write failed");
@@ -2292,7 +2420,7 @@ int dem_save_state(dem_ctx* c, const char* path) {
     const long long n = c->ntot, na = c->n, np = c->npad;
     std::vector<double> pos(3 * n), pdis(3 * n), angv(3 * n), rad(n), wh(3 * n);
     std::vector<float4> q(n);
-    int rc = dem_download_state(c, pos.data(), pdis.data(), angv.data());
+    int rc = download_common(c, pos.data(), pdis.data(), angv.data(), true, true);   // internal order
     if (rc) return rc;
     uint P = 0;
     cudaStream_t s = c->stream;
@@ -2343,9 +2471,11 @@ int dem_save_state(dem_ctx* c, const char* path) {
     hd.n_active = na;
     hd.pour_nplayer = c->pour_nplayer;
     hd.pour_tnewpar = c->pour_tnewpar;
+    hd.ordered = c->ordered ? 1 : 0;
     FILE* f = fopen(path, "wb");
     if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
     rc = write_all(f, &hd, sizeof(hd));
+    if (!rc && c->ordered) rc = write_all(f, c->hperm.data(), n * sizeof(uint));
     if (!rc) rc = write_all(f, pos.data(), pos.size() * sizeof(double));
     if (!rc) rc = write_all(f, pdis.data(), pdis.size() * sizeof(double));
     if (!rc) rc = write_all(f, angv.data(), angv.size() * sizeof(double));
@@ -2372,7 +2502,7 @@ int dem_load_state(dem_ctx* c, const char* path) {
         rc = fail(DEM_ERR_ARG, "dem_load_state: the context differs from the saved one (n %lld/%lld, precision, "
                   "force mode or relist_interval)", hd.n, c->ntot);
     if (!rc && (hd.n_active < 0 || hd.n_active > hd.n || (!hd.pouring && hd.n_active != hd.n) ||
-                (hd.pouring && (hd.pour_nplayer <= 0 || !(hd.pour_tnewpar > 0.0)))))
+                (hd.pouring && (hd.pour_nplayer <= 0 || !(hd.pour_tnewpar > 0.0) || hd.ordered))))
         rc = fail(DEM_ERR_IO, "dem_load_state: %s holds an inconsistent pour", path);
     if (!rc && (hd.npairs < 0 || hd.npairs > c->cap))
         rc = fail(DEM_ERR_CAPACITY, "dem_load_state: %lld saved pairs exceed the pair capacity", hd.npairs);
@@ -2380,7 +2510,20 @@ int dem_load_state(dem_ctx* c, const char* path) {
     const long long n = c->ntot, na = hd.n_active, np = c->npad, P = hd.npairs;
     std::vector<double> pos(3 * n), pdis(3 * n), angv(3 * n), rad(n), wh(3 * n), hist(3 * (size_t)P);
     std::vector<float4> q(n);
-    std::vector<uint> off(na + 1), ln(P);
+    std::vector<uint> off(na + 1), ln(P), order;
+    if (hd.ordered) {   // the particle order: a permutation of 0 .. n-1
+        order.resize(n);
+        rc = read_all(f, order.data(), n * sizeof(uint));
+        std::vector<unsigned char> seen(n, 0);
+        for (long long t = 0; !rc && t < n; t++) {
+            if ((long long)order[t] >= n || seen[order[t]]) {
+                rc = fail(DEM_ERR_IO, "dem_load_state: %s holds a malformed particle order", path);
+                break;
+            }
+            seen[order[t]] = 1;
+        }
+        if (rc) { fclose(f); return rc; }
+    }
     rc = read_all(f, pos.data(), pos.size() * sizeof(double));
     if (!rc) rc = read_all(f, pdis.data(), pdis.size() * sizeof(double));
     if (!rc) rc = read_all(f, angv.data(), angv.size() * sizeof(double));
@@ -2403,7 +2546,10 @@ int dem_load_state(dem_ctx* c, const char* path) {
     }
     if (!ok) return fail(DEM_ERR_IO, "dem_load_state: %s holds a malformed pair list", path);
     if (hd.have_mat && (rc = dem_set_material(c, &hd.mat))) return rc;
-    if ((rc = dem_upload_state(c, pos.data(), pdis.data(), angv.data(), rad.data()))) return rc;
+    // the sections are in the saved context's internal order
+    if ((rc = upload_impl(c, pos.data(), pdis.data(), angv.data(), rad.data(), true,
+                          hd.ordered ? kOrderGiven : kOrderCaller, hd.ordered ? order.data() : nullptr)))
+        return rc;
     // particles not yet poured in wait with the injection states just uploaded
     if (hd.pouring && (rc = dem_set_pour(c, hd.pour_nplayer, hd.pour_tnewpar, na))) return rc;
     // the upload started afresh (list buffer 0 current, empty); put back the

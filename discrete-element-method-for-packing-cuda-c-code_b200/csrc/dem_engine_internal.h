@@ -129,6 +129,13 @@ struct dem_ctx {
     double pour_tnewpar = 0.0;
     void* pour_rec = nullptr;              // PRec<Real>[npad]
     std::vector<double> r3sum;             // r3sum[k] = sum of r^3 over the first k particles
+    // particle order: the host upload sorts the particles by cell (locality of
+    // every gather and scatter); internal slot t holds the caller's particle
+    // perm[t].  Results leave in the caller's order.
+    bool reorder = true;                   // host uploads sort by cell (DEM_B200_REORDER=0: off)
+    bool ordered = false;
+    uint* perm = nullptr;                  // device copy (npad)
+    std::vector<uint> hperm;               // host copy (n)
     int device = 0;
     cudaStream_t stream = 0;
     cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one

@@ -249,7 +249,11 @@ int dem_destroy(dem_ctx* ctx);
 int dem_set_stream(dem_ctx* ctx, void* cuda_stream);
 int dem_set_material(dem_ctx* ctx, const dem_material* mat);
 /* Host AoS (xyz-interleaved) double arrays of length 3n (rad: n).  pdis/angv
- * may be NULL (zero).  Resets histories and forces a re-list. */
+ * may be NULL (zero).  Resets histories and forces a re-list.  The context
+ * stores the particles sorted by cell (locality of every gather and scatter;
+ * environment DEM_B200_REORDER=0 keeps the caller's order); every result --
+ * states, forces, pairs, cells, radius gradients -- is returned in the
+ * caller's order and ids.  The _device form keeps the caller's order. */
 int dem_upload_state(dem_ctx* ctx, const double* pos, const double* pdis,
                      const double* angv, const double* rad);
 /* Same with device pointers (AoS double), no host copy. */
@@ -340,6 +344,9 @@ int dem_load_state(dem_ctx* ctx, const char* path);
  * in the system, mean CN = 2 contacts / N), dem_download_pairs and the window
  * kernels cover the N particles in the system; dem_download_state* returns
  * all n, those not yet poured in as injected.  A later upload ends the pour.
+ * Layers join in the caller's order: on a context whose upload sorted the
+ * particles by cell, dem_set_pour first puts them back (the state is kept,
+ * the contact history restarts).
  * DEM_ERR_STATE before an upload or when a pour is already set (upload again
  * to start over); dem_adjoint_window refuses (DEM_ERR_STATE) until every
  * particle is in.  dem_active_count: N (n when not pouring). */

@@ -456,3 +456,37 @@ def test_observables_without_a_host_wait(dem, wl, cuda):
     with pytest.raises(dem.DemError) as e:
         other.scalars_from_raw(raws[0].data_ptr())
     assert e.value.code == dem.DEM_ERR_ARG
+
+
+def test_cell_order_is_invisible(dem, wl, cuda, monkeypatch):
+    """A host upload sorts the particles by cell inside the context; every
+    result leaves in the caller's order: the state round-trips exactly, and a
+    run agrees with one in the caller's order (DEM_B200_REORDER=0) -- same
+    canonical pair set, histories and positions to rounding."""
+    w = dense_lattice(dem, nx=9, ny=9, nz=6)
+    rng = np.random.default_rng(17)
+    perm = rng.permutation(w.n)           # the caller's order: spatially scrambled
+    pos = w.pos.reshape(-1, 3)[perm].reshape(-1).copy()
+    rad = w.rad[perm].copy()
+    pdis = rng.normal(0, 2e-6, 3 * w.n)
+    angv = rng.normal(0, 2e-5, 3 * w.n)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("DEM_B200_REORDER", flag)
+        e = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_FP64})
+        e.set_material(w.pp, w.pw)
+        e.upload(pos, rad, pdis, angv)
+        p0, d0, a0 = e.download()
+        np.testing.assert_array_equal(p0, pos)
+        np.testing.assert_array_equal(d0, pdis)
+        np.testing.assert_array_equal(a0, angv)
+        e.step(5 * w.relist_interval + 3)
+        out.append((e.download(), e.pairs(), e.scalars()))
+    (sa, pa, ca), (sb, pb, cb) = out
+    assert ca["status"] == cb["status"] == 0
+    assert ca["contacts"] == cb["contacts"] > 100 and ca["pairs"] == cb["pairs"]
+    np.testing.assert_array_equal(pa[0], pb[0])
+    np.testing.assert_array_equal(pa[1], pb[1])
+    np.testing.assert_allclose(pa[2], pb[2], rtol=0, atol=1e-12 * np.abs(pb[2]).max())
+    for x, y in zip(sa, sb):
+        np.testing.assert_allclose(x, y, rtol=0, atol=1e-12 * max(np.abs(y).max(), 1e-30))

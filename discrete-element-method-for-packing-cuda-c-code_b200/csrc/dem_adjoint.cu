@@ -33,7 +33,7 @@ namespace dem {
 
 namespace {
 constexpr int kB = 256;
-constexpr int kPairB = 128;   // block size of k_adj_step; pbar holds one 12-slot row per block
+constexpr int kPairB = 32;    // block size of k_adj_step; pbar holds one 12-slot row per block
 constexpr long long kScatterPrime = 2654435761ll;
 
 struct Ck {
@@ -60,6 +60,7 @@ struct AdjWork {
     std::vector<Ck> ck;
     std::vector<ListRec> lists;
     double *tx = nullptr, *td = nullptr, *twh = nullptr, *tF = nullptr, *tT = nullptr, *th = nullptr;
+    uint* tc = nullptr;   // per step and particle: its pair contacts in the forward
     void* ta = nullptr;
     // state adjoints, two sets (ping-pong per reversed step); the objective
     // seeds set 0 (Xb, Db, Ab alias it)
@@ -114,7 +115,7 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
         w->Ab = w->Ab2[0];
     }
     if (seg > w->seg) {
-        void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta};
+        void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->tc};
         for (void* x : p)
             if (x) cudaFree(x);
         for (ListRec& l : w->lists) {
@@ -125,7 +126,8 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
         w->lists.clear();
         if ((rc = dalloc(&w->tx, 3 * np * seg)) || (rc = dalloc(&w->td, 3 * np * seg)) ||
             (rc = dalloc(&w->twh, 3 * np * seg)) || (rc = dalloc(&w->tF, 3 * np * seg)) ||
-            (rc = dalloc(&w->tT, 3 * np * seg)) || (rc = dalloc(&w->th, 3 * cap * seg)))
+            (rc = dalloc(&w->tT, 3 * np * seg)) || (rc = dalloc(&w->th, 3 * cap * seg)) ||
+            (rc = dalloc(&w->tc, np * seg)))
             return rc;
         DEM_CUDA_TRY(cudaMalloc(&w->ta, 3 * np * seg * rsz(c)));
         const long long nw = (seg + K - 1) / K;
@@ -206,22 +208,17 @@ __device__ __forceinline__ void st3(double* a, long long np, long long i, V3d v)
 
 // Integrator reverse of particle i (neiglist.cu:356-360 read backwards):
 //   d' = d + F dt^2/m,  x' = x + d',  a' = a + T dt^2/I,  F_z includes -m.
-// Given the adjoints (xb, db, ab) of the state after the step, returns the
-// adjoint of d' (dtot = db + xb) and of the step's force and torque, and
-// adds the mass / inertia terms to the radius adjoint.  A free particle of
-// the window (not taped) feels its weight only, in the working precision as
-// the forward computed it.
+// Given the step's taped total force f and torque t and the adjoints (xb,
+// db, ab) of the state after the step, returns the adjoint of d' (dtot = db +
+// xb) and of the step's force and torque, and adds the mass / inertia terms
+// to the radius adjoint.
 template <typename Real>
-__device__ __forceinline__ void integ_rev(Real rr, bool bound, const double* __restrict__ F,
-                                          const double* __restrict__ T, long long i, double dt, double density, V3d xb,
-                                          V3d db, V3d ab, V3d& dtot, V3d& fb, V3d& tb, double& rb) {
+__device__ __forceinline__ void integ_rev(Real rr, V3d f, V3d t, double dt, double density, V3d xb, V3d db, V3d ab,
+                                          V3d& dtot, V3d& fb, V3d& tb, double& rb) {
     const double r = (double)rr;
     const double m = density * 8.0 * r * r * r, I = 0.4 * m * (r * r);
     const double dmdr = density * 24.0 * r * r, dIdr = 0.4 * (dmdr * r * r + 2.0 * m * r);
     dtot = db + xb;
-    const V3d f = bound ? mk(F[3 * i], F[3 * i + 1], F[3 * i + 2])
-                        : mk(0.0, 0.0, (double)(-((Real)density * (Real)8 * rr * rr * rr)));
-    const V3d t = bound ? mk(T[3 * i], T[3 * i + 1], T[3 * i + 2]) : mk(0.0, 0.0, 0.0);
     const double k = dt * dt / m, kI = dt * dt / I;
     fb = k * dtot;
     tb = kI * ab;
@@ -282,7 +279,8 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
     long long n, long long np, long long cap, AdjList L, const uint* __restrict__ blist, const uint* __restrict__ nbp,
     const double* __restrict__ tx, const double* __restrict__ td, const Real* __restrict__ ta,
     const double* __restrict__ twh, const double* __restrict__ th, const double* __restrict__ tF,
-    const double* __restrict__ tT, const Real* __restrict__ R, LawParams<double> pp, LawParams<double> pw,
+    const double* __restrict__ tT, const uint* __restrict__ tc, const Real* __restrict__ R, LawParams<double> pp,
+    LawParams<double> pw,
     double dt, double density, double hx, double hy, const double* __restrict__ Hout, double* __restrict__ Hin,
     const double* __restrict__ Xa, const double* __restrict__ Da, const double* __restrict__ Aa,
     double* __restrict__ Xo, double* __restrict__ Do, double* __restrict__ Ao, double* __restrict__ Wb,
@@ -294,25 +292,49 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
     LawBar bp, bw;
     lawbar_zero(bp);
     lawbar_zero(bw);
+    // Before pdl_wait: what the recompute wrote (list, tape) -- the particle,
+    // its taped state, force, torque, wall history and pair-contact count,
+    // and its row bounds.  The previous reversed step (the predecessor)
+    // writes only adjoints, and it triggers this launch only after its own
+    // wait, so everything older than it is complete.
+    // Bound particles in a scattered order (u0 -> u0 * p mod nb, p a prime
+    // above any particle count: a bijection): with the particles stored in
+    // cell order, neighbours with many contacts -- long FP64 chains -- would
+    // otherwise fill the same warps (measured: 25 % longer reverse sweeps);
+    // scattered, every warp gets a mix.
+    long long i = 0;
+    Real rr = (Real)0;
+    V3d xi = zero3<double>(), di = zero3<double>(), ai = zero3<double>(), fi = zero3<double>(), ti = zero3<double>(),
+        hw = zero3<double>();
+    uint total = 0, o0 = 0, o1 = 0, q0 = 0, q1 = 0, nc = 0;
     if (u0 < nb) {
-        // bound particles in a scattered order (u0 -> u0 * p mod nb, p a
-        // prime above any particle count: a bijection): with the particles
-        // stored in cell order, neighbours with many contacts -- long FP64
-        // chains -- would otherwise fill the same warps (measured: 25 % longer
-        // reverse sweeps); scattered, every warp gets a mix
-        const long long i = blist[(u0 * kScatterPrime) % nb];
-        const Real rr = R[i];
+        i = blist[(u0 * kScatterPrime) % nb];
+        rr = R[i];
+        xi = ld3(tx, np, i); di = ld3(td, np, i); ai = ldA<Real>(ta, np, i);
+        fi = mk(tF[3 * i], tF[3 * i + 1], tF[3 * i + 2]);
+        ti = mk(tT[3 * i], tT[3 * i + 1], tT[3 * i + 2]);
+        hw = ld3(twh, np, i);
+        nc = tc[i];
+        total = L.off[n];
+        o0 = L.off[i]; o1 = L.off[i + 1]; q0 = L.roff[i]; q1 = L.roff[i + 1];
+    }
+    pdl_wait();
+    pdl_trigger();
+    if (u0 < nb) {
         const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
         V3d dtot, fbi, tbi;
         double rb = 0.0;
-        integ_rev<Real>(rr, true, tF, tT, i, dt, density, xa, ld3(Da, np, i), aa, dtot, fbi, tbi, rb);
+        integ_rev<Real>(rr, fi, ti, dt, density, xa, ld3(Da, np, i), aa, dtot, fbi, tbi, rb);
         V3d xb = zero3<double>(), dbv = zero3<double>(), ab = zero3<double>();
-        const V3d xi = ld3(tx, np, i), di = ld3(td, np, i), ai = ldA<Real>(ta, np, i);
         const double ri = (double)rr;
         double dum = 0.0;
-        const uint total = L.off[n];
-        if ((long long)total <= cap) {
-            for (uint k = L.off[i]; k < L.off[i + 1]; k++) {
+        if ((long long)total <= cap && nc == 0) {
+            // no pair contact in the forward step: every listed pair of the
+            // sphere was inert (zero force, history reset), so only the
+            // history adjoints of its own row are cleared; no partner is read
+            for (uint k = o0; k < o1; k++) { Hin[k] = 0.0; Hin[cap + k] = 0.0; Hin[2 * cap + k] = 0.0; }
+        } else if ((long long)total <= cap) {
+            for (uint k = o0; k < o1; k++) {
                 const uint j = L.ln[k];
                 const V3d hin = mk(th[k], th[cap + k], th[2 * cap + k]);
                 PairTape t;
@@ -329,7 +351,7 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
                          xjb, dbv, djb, ab, ajb, rb, dum, hinb, bp);
                 Hin[k] = hinb.x; Hin[cap + k] = hinb.y; Hin[2 * cap + k] = hinb.z;
             }
-            for (uint u = L.roff[i]; u < L.roff[i + 1]; u++) {
+            for (uint u = q0; u < q1; u++) {
                 const uint k = L.rk[u];
                 if (k >= total) continue;
                 const uint j = L.lp[k];
@@ -350,7 +372,6 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
         }
         // walls (the stored slot is the history input; it is zero whenever
         // the particle did not touch a wall at the previous step)
-        const V3d hw = ld3(twh, np, i);
         V3d hwb = zero3<double>();
         wall_vjp(hx, hy, xi, di, ai, ri, density, hw, pw, inv_dt, fbi, tbi, ld3(Wb, np, i), xb, dbv, ab, rb, hwb, bw);
         st3(Wb, np, i, hwb);
@@ -535,13 +556,18 @@ template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l,
     AdjWork* w = c->adj;
     const long long np = c->npad, cap = c->cap;
     AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
-    k_adj_step<Real><<<(unsigned)w->npb, kPairB, 0, c->stream>>>(
-        c->n, np, cap, L, l.blist, l.nb, w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t,
-        w->twh + 3 * np * t, w->th + 3 * cap * t, w->tF + 3 * np * t, w->tT + 3 * np * t, (const Real*)c->rad,
+    // a reversed step that directly follows another is launched programmatic
+    // (its tape loads overlap the predecessor's tail); the first step of a
+    // window follows the free-particle kernel and is launched plainly
+    const bool pdl = c->pdl && (t % c->cfg.relist_interval) != c->cfg.relist_interval - 1;
+    DEM_CUDA_TRY(launch_ex(
+        k_adj_step<Real>, (unsigned)w->npb, kPairB, c->stream, pdl, c->n, np, cap, L, l.blist, l.nb,
+        w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t, w->twh + 3 * np * t,
+        w->th + 3 * cap * t, w->tF + 3 * np * t, w->tT + 3 * np * t, (const uint*)w->tc + np * t, (const Real*)c->rad,
         make_law<double>(c->mat.pp), make_law<double>(c->mat.pw), c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5,
-        c->cfg.world[1] * 0.5, w->Hb[hb], w->Hb[1 - hb], w->Xb2[in], w->Db2[in], w->Ab2[in], w->Xb2[1 - in],
-        w->Db2[1 - in], w->Ab2[1 - in], w->Wb, w->Rb, w->pbar);
-    DEM_LAUNCH_CHECK();
+        c->cfg.world[1] * 0.5, (const double*)w->Hb[hb], w->Hb[1 - hb], (const double*)w->Xb2[in],
+        (const double*)w->Db2[in], (const double*)w->Ab2[in], w->Xb2[1 - in], w->Db2[1 - in], w->Ab2[1 - in], w->Wb,
+        w->Rb, w->pbar));
     return DEM_OK;
 }
 
@@ -608,7 +634,7 @@ int recompute_segment(dem_ctx* c, long long every) {
         c->cur = 1 - c->cur;
         c->hph = 0;
         if ((rc = list_snapshot(c, w->lists[t / K]))) return rc;
-        WindowTape tape{w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, (int)t};
+        WindowTape tape{w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, (int)t, w->tc};
         if ((rc = window_kernel(c, c->cur, &tape))) return rc;
     }
     return DEM_OK;
@@ -789,12 +815,15 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
             // the step writes its total force and torque straight into the tape
             double* keepF = c->dbgF;
             double* keepT = c->dbgT;
+            uint* keepC = c->dbgC;
             c->dbgF = w->tF + 3 * np * t;
             c->dbgT = w->tT + 3 * np * t;
+            c->dbgC = w->tc + np * t;   // per-particle pair contacts
             double a, b;
             rc = step_kernels(c, c->cur, slot, &a, &b);
             c->dbgF = keepF;
             c->dbgT = keepT;
+            c->dbgC = keepC;
             if (rc) return rc;
         }
         // reverse sweep: one graph per (hb, in) parity at the segment start
@@ -853,7 +882,7 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     AdjWork* w = c->adj;
     cudaStreamSynchronize(c->stream);
     for (Ck& k : w->ck) free_ck(k);
-    void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1],
+    void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->tc, w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1],
                  w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj};
     for (void* x : p)
         if (x) cudaFree(x);

@@ -68,11 +68,10 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <typename... KArgs, typename... Args>
-cudaError_t launch_ex(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, bool pdl,
-                      Args... args) {
+cudaError_t launch_ex(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, bool pdl, Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -87,10 +86,11 @@ cudaError_t launch_ex(void (*kernel)(KArgs...), unsigned grid, unsigned block, c
 // out[i] = sum_{t<i} in[i]; if total != nullptr, *total (device) = full sum.
 // out may alias in.  Scratch: tmp with scan_scratch_words(n) uint32.
 size_t scan_scratch_words(long long n);
-int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s);
+int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s,
+                       bool pdl = false);
 // Up to three arrays of length n in the same three launches; tmp holds
 // narr * scan_scratch_words(n) uint32.  Outputs may alias their inputs.
 int exclusive_scan_multi_u32(int narr, const uint* const* in, uint* const* out, uint* const* total, long long n,
-                             uint* tmp, cudaStream_t s);
+                             uint* tmp, cudaStream_t s, bool pdl = false);
 
 }  // namespace dem

@@ -28,6 +28,7 @@
 #include <vector>
 #include <algorithm>
 #include "dem_engine_internal.h"
+#include "dem_compat_state.h"
 
 namespace dem {
 
@@ -190,6 +191,8 @@ __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint*
                           const uint* __restrict__ cstart, uint* __restrict__ count, const PRec<Real>* __restrict__ S,
                           const Real* __restrict__ R, GridC g, uint* __restrict__ sidu, uint* __restrict__ skeyu,
                           R4<Real>* __restrict__ sposu, uint* __restrict__ tpos) {
+    pdl_wait();
+    pdl_trigger();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint c = key[i];
@@ -281,6 +284,8 @@ __global__ void k_nbr_walk(long long n, const uint* __restrict__ sid2, const R4<
                            const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
                            const uint* __restrict__ wslot, uint* __restrict__ njgi, uint* __restrict__ njli,
                            uint* __restrict__ bflag, uint* __restrict__ scr, EngineWords* words) {
+    pdl_wait();
+    pdl_trigger();
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     uint nall = 0;
     if (t < n) {
@@ -317,6 +322,8 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
                            uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,
                            const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist,
                            const uint* __restrict__ tpos) {
+    pdl_wait();
+    pdl_trigger();
     const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // particle order
     if (ii >= n) return;
     const uint i = (uint)ii;
@@ -374,6 +381,8 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
 // the gather) and record each pair's reverse slot ru[k].
 __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,
                            const uint* __restrict__ off, long long cap) {
+    pdl_wait();
+    pdl_trigger();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if ((long long)off[n] > cap) return;
@@ -438,8 +447,10 @@ template <typename Real> struct StepArgs {
     // state before the step of every bound particle (tx, td, ta: 3 planes of
     // tnp), its wall history (twh), its total force and torque (tF, tT: xyz
     // per particle), and every listed pair's history before the step (th: 3
-    // planes of cap); the window's first step is tape step tstep0.
+    // planes of cap), and its pair-contact count (tc: per particle); the
+    // window's first step is tape step tstep0.
     double *tx, *td, *twh, *tF, *tT, *th;
+    uint* tc;
     Real* ta;
     long long tnp;
     int tstep0;
@@ -698,6 +709,7 @@ template <typename Real, bool COH>
 __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const ParticleCommon& pc, uint i, Real r, uint ws,
                                            uint total, uint o0, uint o1, uint r0, uint r1, double& mz, uint& cnt,
                                            uint& flags, long long ts = -1) {
+    const uint cnt0 = cnt;
     V3<double> x, d;
     V3<Real> av;
     Real rr;
@@ -736,11 +748,12 @@ __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const Partic
         F.x += fw.x; F.y += fw.y; F.z += fw.z;
         T.x += tw.x; T.y += tw.y; T.z += tw.z;
     }
-    if (ts >= 0) {   // total force and torque of the step
+    if (ts >= 0) {   // total force and torque of the step, and its pair contacts
         double* f = a.tF + 3 * a.tnp * ts;
         double* t = a.tT + 3 * a.tnp * ts;
         f[3 * i] = F.x; f[3 * i + 1] = F.y; f[3 * i + 2] = F.z;
         t[3 * i] = T.x; t[3 * i + 1] = T.y; t[3 * i + 2] = T.z;
+        a.tc[a.tnp * ts + i] = cnt - cnt0;
     }
     particle_finish<Real, false>(i, F, T, r, x, d, av, q, a.S, a.Q, a.W, a.pw, pc, a.dtr, a.inv_dt, a.density, mz,
                                  flags, cnt, a.dbgF, a.dbgT, a.dbgC);
@@ -1200,27 +1213,34 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, S, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
                                                     c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
                                                     c->wslot, c->wlist, c->wcount);
-    int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s);
+    // every launch after the first is programmatic: each kernel waits for its
+    // predecessor before it touches memory, so only the launch latency overlaps
+    const bool pdl = c->pdl && !c->profiling;
+    int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s, pdl);
     if (rc) return rc;
-    k_scatter<Real><<<grid_for(n, B), B, 0, s>>>(n, c->key, c->arrival, c->cstart, c->ccount, S, (const Real*)c->rad,
-                                                 g, c->sid, c->skeyu, (R4<Real>*)c->sposu, c->tpos);
+    DEM_CUDA_TRY(launch_ex(k_scatter<Real>, grid_for(n, B), B, s, pdl, n, (const uint*)c->key, (const uint*)c->arrival,
+                           (const uint*)c->cstart, c->ccount, S, (const Real*)c->rad, g, c->sid, c->skeyu,
+                           (R4<Real>*)c->sposu, c->tpos));
     const Real skin = (Real)c->cfg.skin;
-    k_nbr_walk<Real><<<grid_for(n, B), B, 0, s>>>(n, c->sid, (const R4<Real>*)c->sposu, c->skeyu, c->cstart, g, skin,
-                                                  c->wslot, c->njgi, c->njli, c->bflag, c->scr, c->words);
+    DEM_CUDA_TRY(launch_ex(k_nbr_walk<Real>, grid_for(n, B), B, s, pdl, n, (const uint*)c->sid,
+                           (const R4<Real>*)c->sposu, (const uint*)c->skeyu, (const uint*)c->cstart, g, skin,
+                           (const uint*)c->wslot, c->njgi, c->njli, c->bflag, c->scr, c->words));
     {
         const uint* in[3] = {c->njgi, c->njli, c->bflag};
         uint* out[3] = {c->off[dst], c->roff, c->bpos};
         uint* tot[3] = {c->off[dst] + n, c->roff + n, c->bpos + n};
-        rc = exclusive_scan_multi_u32(3, in, out, tot, n, c->scan_tmp, s);
+        rc = exclusive_scan_multi_u32(3, in, out, tot, n, c->scan_tmp, s, pdl);
         if (rc) return rc;
     }
-    k_nbr_fill<Real><<<grid_for(n, B), B, 0, s>>>(
-        n, c->sid, (const R4<Real>*)c->sposu, c->skeyu, c->cstart, g, skin, c->off[dst], c->roff, c->njli, c->ln[dst],
-        c->lp, planes<double>(c->hist[dst][0], c->cap), c->off[src], c->ln[src],
-        planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap, c->words, c->carry, c->scr,
-        c->bflag, c->bpos, c->blist, c->flist, c->tpos);
-    k_rev_sort<<<grid_for(n, B), B, 0, s>>>(n, c->roff, c->rk, c->ru, c->off[dst], c->cap);
-    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(launch_ex(
+        k_nbr_fill<Real>, grid_for(n, B), B, s, pdl, n, (const uint*)c->sid, (const R4<Real>*)c->sposu,
+        (const uint*)c->skeyu, (const uint*)c->cstart, g, skin, (const uint*)c->off[dst], (const uint*)c->roff,
+        c->njli, c->ln[dst], c->lp, planes<double>(c->hist[dst][0], c->cap), (const uint*)c->off[src],
+        (const uint*)c->ln[src], planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap,
+        c->words, c->carry, (const uint*)c->scr, (const uint*)c->bflag, (const uint*)c->bpos, c->blist, c->flist,
+        (const uint*)c->tpos));
+    DEM_CUDA_TRY(launch_ex(k_rev_sort, grid_for(n, B), B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
+                           (const uint*)c->off[dst], c->cap));
     return DEM_OK;
 }
 
@@ -1257,6 +1277,7 @@ template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int
     a.dbgT = c->record ? c->dbgT : nullptr;
     a.dbgC = c->record ? c->dbgC : nullptr;
     a.tx = a.td = a.twh = a.tF = a.tT = a.th = nullptr;
+    a.tc = nullptr;
     a.ta = nullptr;
     a.tnp = np;
     a.tstep0 = 0;
@@ -1296,6 +1317,7 @@ template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape
     a.dbgC = nullptr;
     if (tape) {
         a.tx = tape->tx; a.td = tape->td; a.twh = tape->twh; a.tF = tape->tF; a.tT = tape->tT; a.th = tape->th;
+        a.tc = tape->tc;
         a.ta = (Real*)tape->ta;
         a.tstep0 = tape->step0;
     }
@@ -1621,7 +1643,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_grid = (unsigned)std::max(1, nsm * wper);
         const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
-        const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches inside a window
+        const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches everywhere
         c->pdl = !(pdl && pdl[0] == '0');
         const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order
         c->reorder = !(ro && ro[0] == '0');
@@ -1766,33 +1788,64 @@ static int finish_upload(dem_ctx* c) {
     return setup_grid(c);
 }
 
+// Cell key of every particle for the upload order, (key, id) pairs: the
+// cell of each coordinate is floor((p - origin) / cs) clamped to the grid
+// (below the origin or not a number: cell 0), as the host computes it.
+__global__ void k_cell_keys(long long n, const double* __restrict__ pos, double cs, double hx, double hy, long long gx,
+                            long long gy, long long gz, uint2* __restrict__ kv) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    auto cell = [cs](double v, long long g) -> long long {
+        const double f = v / cs;
+        if (!(f >= 0.0)) return 0;
+        return f >= (double)g ? g - 1 : (long long)f;
+    };
+    const long long cx = cell(pos[3 * i] + hx, gx), cy = cell(pos[3 * i + 1] + hy, gy), cz = cell(pos[3 * i + 2], gz);
+    kv[i] = make_uint2((uint)((cz * gy + cy) * gx + cx), (uint)i);
+}
+
+__global__ void k_perm_of(long long n, const uint2* __restrict__ kv, uint* __restrict__ perm) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) perm[t] = kv[t].y;
+}
+
 // The order of a host upload: internal slot t holds the caller's particle
 // perm[t], ascending (cell key, id) on the context's cell grid (any order
-// that keeps neighbours together serves; this one is the re-list's).  Empty
-// when the grid is too large for the host count.
-static void cell_order(const dem_ctx* c, const double* pos, long long n, std::vector<uint>& perm) {
-    perm.clear();
+// that keeps neighbours together serves; this one is the re-list's).
+// Computed on the device from the uploaded positions (pos: device AoS): a
+// stable radix sort of (key, id) in the walk's scratch (free between
+// re-lists), then the permutation goes to c->perm and, for the downloads that
+// map ids, to the host (c->hperm; the call waits for it).  Leaves hperm empty
+// (the caller's order) when the grid is too large (over 2^27 cells).
+static int device_cell_order(dem_ctx* c, const double* pos, long long n) {
+    c->hperm.clear();
     const double cs = c->cfg.cell > 0.0 ? c->cfg.cell : 2.0 * c->rmax + c->cfg.skin + 1e-4;
+    if (!(cs > 0.0)) return DEM_OK;
     const long long gx = (long long)(c->cfg.world[0] / cs) + 1, gy = (long long)(c->cfg.world[1] / cs) + 1,
                     gz = (long long)(c->cfg.world[2] / cs) + 1;
     const long long nc = gx * gy * gz;
-    if (!(cs > 0.0) || nc > (1ll << 27)) return;
-    auto cell = [cs](double v, long long g) -> long long {
-        const double f = v / cs;
-        if (!(f >= 0.0)) return 0;           // below the origin, or not a number
-        return f >= (double)g ? g - 1 : (long long)f;
-    };
-    std::vector<uint> key(n), cnt(nc + 1, 0u);
-    for (long long i = 0; i < n; i++) {
-        const long long cx = cell(pos[3 * i] + 0.5 * c->cfg.world[0], gx);
-        const long long cy = cell(pos[3 * i + 1] + 0.5 * c->cfg.world[1], gy);
-        const long long cz = cell(pos[3 * i + 2], gz);
-        key[i] = (uint)((cz * gy + cy) * gx + cx);
-        cnt[key[i] + 1]++;
-    }
-    for (long long k = 0; k < nc; k++) cnt[k + 1] += cnt[k];
-    perm.resize(n);
-    for (long long i = 0; i < n; i++) perm[cnt[key[i]]++] = (uint)i;
+    if (nc > (1ll << 27)) return DEM_OK;
+    const long long np = c->npad;
+    uint2* kv = reinterpret_cast<uint2*>(c->scr);   // 2 np words
+    uint2* kv2 = kv + np;                            // 2 np words
+    uint* scratch = c->scr + 4 * np;                 // (kScr - 4) np words
+    // the sort's histograms fit the rest of the scratch from 65 particles on;
+    // fewer keep the caller's order
+    if (radix_scratch_words((uint)n) > (size_t)(kScr - 4) * (size_t)np) return DEM_OK;
+    int rc;
+    if (!c->perm && (rc = dalloc(&c->perm, np))) return rc;
+    k_cell_keys<<<grid_for(n, 256), 256, 0, c->stream>>>(n, pos, cs, 0.5 * c->cfg.world[0], 0.5 * c->cfg.world[1],
+                                                         gx, gy, gz, kv);
+    DEM_LAUNCH_CHECK();
+    uint bits = 1;
+    while (bits < 32 && (1ull << bits) < (unsigned long long)nc) bits++;
+    if ((rc = radix_sort_pairs(kv, kv2, (uint)n, bits, scratch, c->stream))) return rc;
+    k_perm_of<<<grid_for(n, 256), 256, 0, c->stream>>>(n, kv, c->perm);
+    DEM_LAUNCH_CHECK();
+    c->hperm.resize(n);
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->hperm.data(), c->perm, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DEM_OK;
 }
 
 enum UploadOrder { kOrderCaller = 0, kOrderCells = 1, kOrderGiven = 2 };
@@ -1828,10 +1881,11 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
         }
         c->rmax = rm;
         c->vol = 4.0 / 3.0 * M_PI * v3;
-        if (order == kOrderCells && c->reorder) cell_order(c, pos, n, c->hperm);
-        else if (order == kOrderGiven && given) c->hperm.assign(given, given + n);
-        c->ordered = !c->hperm.empty();
-        if (c->ordered) {
+        if (order == kOrderCells && c->reorder) {
+            int rc = device_cell_order(c, spos, n);
+            if (rc) return rc;
+        } else if (order == kOrderGiven && given) {
+            c->hperm.assign(given, given + n);
             if (!c->perm) {
                 int rc = dalloc(&c->perm, np);
                 if (rc) return rc;
@@ -1839,6 +1893,7 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
             DEM_CUDA_TRY(cudaMemcpyAsync(c->perm, c->hperm.data(), n * sizeof(uint), cudaMemcpyHostToDevice,
                                          c->stream));
         }
+        c->ordered = !c->hperm.empty();
     } else {
         // the caller's buffers may have been written on the legacy stream
         DEM_CUDA_TRY(cudaEventRecord(c->ext_ready, 0));

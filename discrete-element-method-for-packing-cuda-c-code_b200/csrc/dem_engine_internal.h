@@ -100,6 +100,7 @@ struct WindowTape {
     double *tx, *td, *twh, *tF, *tT, *th;
     void* ta;
     int step0;
+    uint* tc;   // per particle and step: its pair contacts
 };
 
 struct ParticleCommon {
@@ -198,7 +199,7 @@ struct dem_ctx {
     void* rfj = nullptr;     // per reverse slot: force on hi, .w = contact
     void* rtj = nullptr;     // per reverse slot: torque on hi
     unsigned pair_grid = 1;  // one wave of the pair kernel
-    bool pdl = true;         // programmatic launches inside a window
+    bool pdl = true;         // programmatic launches: window steps, re-list, reverse sweep
     uint* scan_tmp = nullptr;
     size_t scan_words = 0;
     // scalars

@@ -67,6 +67,8 @@ struct ScanSet {
 
 __global__ void __launch_bounds__(kScanThreads) k_tile_reduce(ScanSet a, long long n) {
     __shared__ uint sw[kScanThreads / 32 + 1];
+    pdl_wait();
+    pdl_trigger();
     const int y = blockIdx.y;
     uint it[kScanItems];
     load_items(a.in[y], n, (long long)blockIdx.x * kScanTile, it);
@@ -81,6 +83,8 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_reduce(ScanSet a, long lo
 // One CTA per array scans its tile sums in chunks of 256.
 __global__ void __launch_bounds__(kScanThreads) k_scan_sums(ScanSet a, long long nt) {
     __shared__ uint sw[kScanThreads / 32 + 1];
+    pdl_wait();
+    pdl_trigger();
     uint* sums = a.sums[blockIdx.y];
     uint carry = 0;
     for (long long base = 0; base < nt; base += kScanThreads) {
@@ -96,6 +100,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_sums(ScanSet a, long long
 
 __global__ void __launch_bounds__(kScanThreads) k_tile_scan(ScanSet a, long long n) {
     __shared__ uint sw[kScanThreads / 32 + 1];
+    pdl_wait();
+    pdl_trigger();
     const int y = blockIdx.y;
     const uint* in = a.in[y];
     uint* out = a.out[y];
@@ -122,12 +128,14 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_scan(ScanSet a, long long
     }
 }
 
-int scan_set(ScanSet a, int narr, long long n, cudaStream_t s) {
+// pdl: the three launches are programmatic (each kernel waits for its
+// predecessor before it touches memory, so only the launch latency overlaps);
+// for a scan that follows a kernel on the stream
+int scan_set(ScanSet a, int narr, long long n, cudaStream_t s, bool pdl) {
     const long long nt = (n + kScanTile - 1) / kScanTile;
-    k_tile_reduce<<<dim3((unsigned)nt, narr), kScanThreads, 0, s>>>(a, n);
-    k_scan_sums<<<dim3(1, narr), kScanThreads, 0, s>>>(a, nt);
-    k_tile_scan<<<dim3((unsigned)nt, narr), kScanThreads, 0, s>>>(a, n);
-    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(launch_ex(k_tile_reduce, dim3((unsigned)nt, narr), dim3(kScanThreads), s, pdl, a, n));
+    DEM_CUDA_TRY(launch_ex(k_scan_sums, dim3(1, narr), dim3(kScanThreads), s, pdl, a, nt));
+    DEM_CUDA_TRY(launch_ex(k_tile_scan, dim3((unsigned)nt, narr), dim3(kScanThreads), s, pdl, a, n));
     return DEM_OK;
 }
 }  // namespace
@@ -137,15 +145,15 @@ size_t scan_scratch_words(long long n) {
     return (size_t)(nt < 1 ? 1 : nt) + 4;
 }
 
-int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s) {
+int exclusive_scan_u32(const uint* in, uint* out, long long n, uint* total, uint* tmp, cudaStream_t s, bool pdl) {
     const uint* ins[1] = {in};
     uint* outs[1] = {out};
     uint* tots[1] = {total};
-    return exclusive_scan_multi_u32(1, ins, outs, tots, n, tmp, s);
+    return exclusive_scan_multi_u32(1, ins, outs, tots, n, tmp, s, pdl);
 }
 
 int exclusive_scan_multi_u32(int narr, const uint* const* in, uint* const* out, uint* const* total, long long n,
-                             uint* tmp, cudaStream_t s) {
+                             uint* tmp, cudaStream_t s, bool pdl) {
     if (narr < 1 || narr > kMaxArrays) return fail(DEM_ERR_ARG, "exclusive_scan_multi_u32: %d arrays", narr);
     if (n <= 0) {
         for (int a = 0; a < narr; a++)
@@ -160,7 +168,7 @@ int exclusive_scan_multi_u32(int narr, const uint* const* in, uint* const* out, 
         set.total[a] = total[a];
         set.sums[a] = tmp + a * words;
     }
-    return scan_set(set, narr, n, s);
+    return scan_set(set, narr, n, s, pdl);
 }
 
 }  // namespace dem

@@ -251,9 +251,11 @@ int dem_set_material(dem_ctx* ctx, const dem_material* mat);
 /* Host AoS (xyz-interleaved) double arrays of length 3n (rad: n).  pdis/angv
  * may be NULL (zero).  Resets histories and forces a re-list.  The context
  * stores the particles sorted by cell (locality of every gather and scatter;
- * environment DEM_B200_REORDER=0 keeps the caller's order); every result --
- * states, forces, pairs, cells, radius gradients -- is returned in the
- * caller's order and ids.  The _device form keeps the caller's order. */
+ * the order is computed on the device and the call waits for it; 64
+ * particles or fewer, or environment DEM_B200_REORDER=0, keep the caller's
+ * order); every result -- states, forces, pairs, cells, radius gradients --
+ * is returned in the caller's order and ids.  The _device form keeps the
+ * caller's order. */
 int dem_upload_state(dem_ctx* ctx, const double* pos, const double* pdis,
                      const double* angv, const double* rad);
 /* Same with device pointers (AoS double), no host copy. */

@@ -136,6 +136,21 @@ def test_adjoint_leaves_forward_state(dem, cuda):
     assert a.scalars()["status"] == 0
 
 
+def test_plain_and_programmatic_reverse_sweeps_agree(dem, cuda, monkeypatch):
+    """The reverse steps launched programmatically (the default: each loads
+    its tape before waiting for its predecessor) and plainly (DEM_B200_PDL=0)
+    give the same objective and gradients bit for bit."""
+    w, pdis, angv = case(dem)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("DEM_B200_PDL", flag)
+        out.append(run_adjoint(dem, w, pdis, angv, w.pp, w.pw, w.rad, dem.OBJ_POTENTIAL))
+    a, b = out
+    assert a["value"] == b["value"]
+    assert a["d_pp"] == b["d_pp"] and a["d_pw"] == b["d_pw"]
+    np.testing.assert_array_equal(a["d_radii"], b["d_radii"])
+
+
 def test_adjoint_settle_50k_window(dem, wl, cuda):
     """The 50,000-sphere configuration: pre-settled 20,000 steps, then a
     2,000-step mixed-precision window with checkpoints every 100; gradients of

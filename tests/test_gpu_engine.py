@@ -335,16 +335,24 @@ def test_window_kernel_equals_per_step_kernels(dem, wl, cuda, monkeypatch, prec,
 
 
 def test_plain_launches_equal_programmatic_launches(dem, wl, cuda, monkeypatch):
-    """Step kernels launched programmatically inside a window (the default)
-    and launched plainly (DEM_B200_PDL=0) agree bit for bit."""
+    """Re-list and step kernels launched programmatically (the default) and
+    launched plainly (DEM_B200_PDL=0) agree bit for bit, with the per-step
+    kernels and with the window kernel."""
     w = wl.small_box(n=3000)
-    a = make_engine(dem, w)
-    monkeypatch.setenv("DEM_B200_PDL", "0")
-    b = make_engine(dem, w)
-    a.step(45)
-    b.step(45)
-    for x, y in zip(a.download(), b.download()):
-        np.testing.assert_array_equal(x, y)
+    for window in ("0", "1"):
+        monkeypatch.setenv("DEM_B200_WINDOW", window)
+        monkeypatch.setenv("DEM_B200_PDL", "1")
+        a = make_engine(dem, w)
+        monkeypatch.setenv("DEM_B200_PDL", "0")
+        b = make_engine(dem, w)
+        a.step(45)
+        b.step(45)
+        for x, y in zip(a.download(), b.download()):
+            np.testing.assert_array_equal(x, y)
+        for x, y in zip(a.pairs(), b.pairs()):
+            np.testing.assert_array_equal(x, y)
+        a.close()
+        b.close()
 
 
 def test_device_upload_download_roundtrip(dem, wl, cuda):
@@ -456,6 +464,58 @@ def test_observables_without_a_host_wait(dem, wl, cuda):
     with pytest.raises(dem.DemError) as e:
         other.scalars_from_raw(raws[0].data_ptr())
     assert e.value.code == dem.DEM_ERR_ARG
+
+
+def _state_header(dem):
+    import ctypes
+
+    class StateHeader(ctypes.Structure):   # the state file's header (dem_save_state)
+        _fields_ = [("magic", ctypes.c_char * 8), ("version", ctypes.c_int), ("precision", ctypes.c_int),
+                    ("force_mode", ctypes.c_int), ("relist_interval", ctypes.c_int), ("n", ctypes.c_longlong),
+                    ("step", ctypes.c_longlong), ("relists", ctypes.c_longlong), ("npairs", ctypes.c_longlong),
+                    ("dt", ctypes.c_double), ("skin", ctypes.c_double), ("cell", ctypes.c_double),
+                    ("density", ctypes.c_double), ("world", ctypes.c_double * 3), ("rmax", ctypes.c_double),
+                    ("vol", ctypes.c_double), ("have_mat", ctypes.c_int), ("pouring", ctypes.c_int),
+                    ("mat", dem.Material), ("n_active", ctypes.c_longlong), ("pour_nplayer", ctypes.c_longlong),
+                    ("pour_tnewpar", ctypes.c_double), ("ordered", ctypes.c_longlong)]
+    return StateHeader
+
+
+@pytest.mark.parametrize("n_side", [2, 9])
+def test_upload_order_is_the_cell_order(dem, wl, cuda, tmp_path, n_side):
+    """The order a host upload gives the particles, computed on the device, is
+    the stable (cell key, id) order on the context's grid (read back from a
+    state file); 64 particles or fewer keep the caller's order."""
+    w = dense_lattice(dem, nx=n_side, ny=n_side, nz=6)
+    rng = np.random.default_rng(23)
+    perm = rng.permutation(w.n)
+    pos = w.pos.reshape(-1, 3)[perm].reshape(-1).copy()
+    rad = w.rad[perm].copy()
+    e = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_MIXED})
+    e.set_material(w.pp, w.pw)
+    e.upload(pos, rad)
+    e.save_state(tmp_path / "s.bin")
+    cs = e.grid_info()[1]
+    e.close()
+    H = _state_header(dem)
+    raw = (tmp_path / "s.bin").read_bytes()
+    h = H.from_buffer_copy(raw[:__import__("ctypes").sizeof(H)])
+    assert h.magic == b"DEMB200S" and h.n == w.n
+    if w.n <= 64:
+        assert h.ordered == 0
+        return
+    assert h.ordered == 1
+    got = np.frombuffer(raw, dtype=np.uint32, count=w.n, offset=__import__("ctypes").sizeof(H))
+    g = [int(x / cs) + 1 for x in w.world]
+    p = pos.reshape(-1, 3)
+
+    def cell(v, gn):
+        f = v / cs
+        return np.where(~(f >= 0.0), 0, np.where(f >= gn, gn - 1, np.floor(np.maximum(f, 0.0)))).astype(np.int64)
+
+    key = (cell(p[:, 2], g[2]) * g[1] + cell(p[:, 1] + 0.5 * w.world[1], g[1])) * g[0] + \
+        cell(p[:, 0] + 0.5 * w.world[0], g[0])
+    np.testing.assert_array_equal(got, np.argsort(key, kind="stable"))
 
 
 def test_cell_order_is_invisible(dem, wl, cuda, monkeypatch):

@@ -115,6 +115,46 @@ def test_adjoint_matches_finite_differences(dem, orc, cuda, objective):
     assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd), (g_ad, g_fd)
 
 
+def sparse_case(dem):
+    """Spheres pressed into the floor (wall contacts and no pair contact, one
+    with a listed non-touching neighbour), a pair overlapping mid-air and
+    approaching (a pair contact through the whole window), and a falling
+    sphere listed with both of the pair but touching neither: the reverse
+    step's paths for spheres with and without pair contacts side by side."""
+    import dem_b200.workloads as wm
+    pos = [1.2, 1.2, 0.4995, -1.2, 1.2, 0.4995, 1.2, -1.2, 0.4995, -1.2, -1.2, 0.4995, 2.24, 1.2, 0.4995,
+           -0.4999, 0.0, 8.0, 0.4999, 0.0, 8.0, 0.0, 0.9, 8.0]
+    rad = np.full(8, 0.5)
+    pp, pw = wm.material(mu=0.3, roll_rel=0.002)
+    w = wm.Workload("sparse", 8, np.array(pos), rad, (6.0, 6.0, 20.0), wm.reduced_dt(5e-7), 0, 20, 0.05,
+                    dem.PREC_FP64, pp, pw)
+    rng = np.random.default_rng(8)
+    pdis = rng.normal(0, 2e-6, 24)
+    pdis[15], pdis[18] = 0.05 * w.dt, -0.05 * w.dt
+    angv = rng.normal(0, 2e-5, 24)
+    return w, pdis, angv
+
+
+def test_adjoint_spheres_with_and_without_pair_contacts(dem, cuda):
+    """Bound spheres without pair contacts (wall contacts only; the forward's
+    taped contact count lets their reverse step skip the pair loops) beside a
+    pair in contact, against central differences of the potential energy in
+    every contact parameter."""
+    w, pdis, angv = sparse_case(dem)
+    base = run_adjoint(dem, w, pdis, angv, w.pp, w.pw, w.rad, dem.OBJ_POTENTIAL)
+    assert base["value"] > 0
+    h = 1e-5
+    floor = 1e-8 * abs(base["value"])
+    for key in KEYS:
+        g_ad = sum(grad_from_adjoint(base, key)) * w.pp[KEYS[key][0]]
+        vp = run_adjoint(dem, w, pdis, angv, scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h), w.rad,
+                         dem.OBJ_POTENTIAL)
+        vm = run_adjoint(dem, w, pdis, angv, scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h), w.rad,
+                         dem.OBJ_POTENTIAL)
+        g_fd = (vp["value"] - vm["value"]) / (2 * h)
+        assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd) + floor, (key, g_ad, g_fd)
+
+
 def test_adjoint_leaves_forward_state(dem, cuda):
     """After dem_adjoint_window the context holds the state of a plain
     forward run of the same window, and its observables."""

@@ -70,6 +70,7 @@ struct AdjWork {
     double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Rb = nullptr;
     double* Hb[2] = {nullptr, nullptr};
     double* pbar = nullptr;      // npb x 12 (one row per k_adj_step block)
+    double* objp = nullptr;      // 3 per k_obj_potential block: energy, d/d estar (pair, wall)
     double* Pobj = nullptr;      // 3 np: the final positions for the objective
     long long npb = 0;
     double* obj = nullptr;       // [0] value, [1..] scratch
@@ -105,6 +106,7 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
             (rc = dalloc(&w->Db2[1], 3 * np)) || (rc = dalloc(&w->Ab2[1], 3 * np)) || (rc = dalloc(&w->Wb, 3 * np)) ||
             (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
             (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) ||
+            (rc = dalloc(&w->objp, 3 * (size_t)grid_for(c->n, kB))) ||
             (rc = dalloc(&w->zmax, 2)) ||
             (rc = dalloc(&w->save_mz, c->npart)) || (rc = dalloc(&w->save_cnt, c->npart)) ||
             (rc = dalloc(&w->Pobj, 3 * np)))
@@ -274,6 +276,24 @@ __global__ void k_adj_free_window(long long n, long long np, int K, const uint* 
 // adjoints ping-pong: (Xa, Da, Aa) after the step are read (also for the
 // partners' force adjoints), (Xo, Do, Ao) before the step are written; no
 // atomics, deterministic.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+// L2 prefetch of partner j's taped state and radius and of pair k's history.
+template <typename Real>
+__device__ __forceinline__ void prefetch_partner(uint j, uint k, long long np, long long cap,
+                                                 const double* __restrict__ tx, const double* __restrict__ td,
+                                                 const Real* __restrict__ ta, const double* __restrict__ th,
+                                                 const Real* __restrict__ R) {
+    for (int c = 0; c < 3; c++) {
+        prefetch_l2(tx + c * np + j);
+        prefetch_l2(td + c * np + j);
+        prefetch_l2(ta + c * np + j);
+        prefetch_l2(th + c * cap + k);
+    }
+    prefetch_l2(R + j);
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(kPairB) k_adj_step(
     long long n, long long np, long long cap, AdjList L, const uint* __restrict__ blist, const uint* __restrict__ nbp,
@@ -317,6 +337,16 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
         nc = tc[i];
         total = L.off[n];
         o0 = L.off[i]; o1 = L.off[i + 1]; q0 = L.roff[i]; q1 = L.roff[i + 1];
+        if (nc != 0 && (long long)total <= cap) {
+            // a sphere in contact: the first partner of each row has its taped
+            // state and the pair's history brought into L2 while the
+            // predecessor finishes (tape data only; no registers held)
+            if (o1 > o0) prefetch_partner(L.ln[o0], o0, np, cap, tx, td, ta, th, R);
+            if (q1 > q0) {
+                const uint k = L.rk[q0];
+                if (k < total) prefetch_partner(L.lp[k], k, np, cap, tx, td, ta, th, R);
+            }
+        }
     }
     pdl_wait();
     pdl_trigger();
@@ -487,7 +517,7 @@ __global__ void k_obj_packing(long long n, long long np, const Real* __restrict_
 template <typename Real>
 __global__ void k_obj_potential(long long n, long long np, long long cap, AdjList L, const double* __restrict__ P,
                                 const Real* __restrict__ R, double estar, double estar_w, double density, double hx,
-                                double hy, double* Xb, double* Rb, double* obj, double* pbar_est) {
+                                double hy, double* Xb, double* Rb, double* part) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double U = 0.0, eb = 0.0, ebw = 0.0;
     if (i < n) {
@@ -537,16 +567,22 @@ __global__ void k_obj_potential(long long n, long long np, long long cap, AdjLis
         st3(Xb, np, i, ld3(Xb, np, i) + xb);
         Rb[i] += rb;
     }
+    // block sums in a fixed order (no atomics: the same bits on every run),
+    // summed over the blocks on the host
+    __shared__ double sw[3][kB / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         U += __shfl_xor_sync(0xffffffffu, U, o);
         eb += __shfl_xor_sync(0xffffffffu, eb, o);
         ebw += __shfl_xor_sync(0xffffffffu, ebw, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        if (U != 0.0) atomicAdd(&obj[0], U);
-        if (eb != 0.0) atomicAdd(&pbar_est[0], eb);
-        if (ebw != 0.0) atomicAdd(&pbar_est[1], ebw);
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sw[0][warp] = U; sw[1][warp] = eb; sw[2][warp] = ebw; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double x = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sw[threadIdx.x][q];
+        part[3 * (size_t)blockIdx.x + threadIdx.x] = x;
     }
 }
 
@@ -596,7 +632,7 @@ template <typename Real> int objective(dem_ctx* c, int which) {
         AdjList L{c->off[c->cur], c->ln[c->cur], c->lp, c->roff, c->rk};
         k_obj_potential<Real><<<grid_for(n, kB), kB, 0, s>>>(n, np, cap, L, P, (const Real*)c->rad, c->mat.pp.estar,
                                                              c->mat.pw.estar, c->cfg.density, c->cfg.world[0] * 0.5,
-                                                             c->cfg.world[1] * 0.5, w->Xb, w->Rb, w->obj, w->obj + 1);
+                                                             c->cfg.world[1] * 0.5, w->Xb, w->Rb, w->objp);
     }
     DEM_LAUNCH_CHECK();
     return DEM_OK;
@@ -838,15 +874,22 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     DEM_CUDA_TRY(cudaEventRecord(c->ev[2], s));
     // ------------------------------------------------------------ results
     std::vector<double> pb((size_t)w->npb * 12);
-    double obj[3];   // value, and the elastic energy's direct d/d estar (pair, wall)
+    double obj[3] = {0.0, 0.0, 0.0};   // value, and the elastic energy's direct d/d estar (pair, wall)
+    const size_t nob = (size_t)grid_for(c->n, kB);
+    std::vector<double> op(which == DEM_OBJ_POTENTIAL ? 3 * nob : 0);
     DEM_CUDA_TRY(cudaMemcpyAsync(pb.data(), w->pbar, pb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (which == DEM_OBJ_POTENTIAL)
+        DEM_CUDA_TRY(cudaMemcpyAsync(op.data(), w->objp, op.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    else
+        DEM_CUDA_TRY(cudaMemcpyAsync(obj, w->obj, sizeof(double), cudaMemcpyDeviceToHost, s));
     if (d_radii) DEM_CUDA_TRY(cudaMemcpyAsync(d_radii, w->Rb, c->n * sizeof(double), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
     if (d_radii && c->ordered) {   // into the caller's particle order
         std::vector<double> t(d_radii, d_radii + c->n);
         for (long long i = 0; i < c->n; i++) d_radii[c->hperm[i]] = t[i];
     }
+    for (size_t b = 0; b < op.size() / 3; b++)   // block sums of the energy objective, in block order
+        for (int q = 0; q < 3; q++) obj[q] += op[3 * b + q];
     double acc[12] = {0};
     for (size_t b = 0; b < (size_t)w->npb; b++)
         for (int k = 0; k < 12; k++) acc[k] += pb[b * 12 + k];
@@ -883,7 +926,8 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (Ck& k : w->ck) free_ck(k);
     void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->tc, w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1],
-                 w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj};
+                 w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj,
+                 w->objp};
     for (void* x : p)
         if (x) cudaFree(x);
     for (ListRec& l : w->lists) {

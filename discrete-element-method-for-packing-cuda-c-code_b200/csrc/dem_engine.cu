@@ -1132,13 +1132,24 @@ __global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned lon
     if (lane_id() == 0 && b) atomicMax(out, b);
 }
 
-__global__ void k_vol(long long n, const double* __restrict__ rad, double* out) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Sum of r^3 over the radii, one block in a fixed order (no atomics: the
+// same bits on every run); launch with 1024 threads.
+__global__ void __launch_bounds__(1024) k_vol(long long n, const double* __restrict__ rad, double* out) {
+    __shared__ double sw[32];
     double v = 0.0;
-    if (i < n) { const double r = rad[i]; v = r * r * r; }
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        const double r = rad[i];
+        v += r * r * r;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane_id() == 0 && v != 0.0) atomicAdd(out, v);
+    if (lane_id() == 0) sw[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sw[w];
+        *out = t;
+    }
 }
 
 __global__ void k_pairs_out(const uint* __restrict__ off, long long n, long long cap, const uint* __restrict__ lp,
@@ -1900,7 +1911,7 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
         DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ext_ready, 0));
         DEM_CUDA_TRY(cudaMemsetAsync(c->rmax_bits, 0, 2 * sizeof(unsigned long long), c->stream));
         k_rmax<<<grid_for(n, 256), 256, 0, c->stream>>>(n, rad, c->rmax_bits);
-        k_vol<<<grid_for(n, 256), 256, 0, c->stream>>>(n, rad, reinterpret_cast<double*>(c->rmax_bits + 1));
+        k_vol<<<1, 1024, 0, c->stream>>>(n, rad, reinterpret_cast<double*>(c->rmax_bits + 1));
         DEM_LAUNCH_CHECK();
         unsigned long long b[2] = {0, 0};
         DEM_CUDA_TRY(cudaMemcpyAsync(c->host_pinned, c->rmax_bits, sizeof(b), cudaMemcpyDeviceToHost, c->stream));

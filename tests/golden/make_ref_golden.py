@@ -34,4 +34,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/ref_golden")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_ref_golden.py <directory written by oracle/_ref/ref_golden>")
+    main(sys.argv[1])

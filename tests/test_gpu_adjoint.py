@@ -191,6 +191,44 @@ def test_plain_and_programmatic_reverse_sweeps_agree(dem, cuda, monkeypatch):
     np.testing.assert_array_equal(a["d_radii"], b["d_radii"])
 
 
+@pytest.mark.parametrize("which", ["dense", "sparse"])
+def test_recompute_paths_agree(dem, cuda, monkeypatch, which):
+    """The reverse sweep's recompute through the per-step kernels (window
+    kernel off: tape from the force record, contact counts included) gives
+    the window kernel's gradients bit for bit; the particle-parallel force
+    mode (its own per-step kernel, whose forward agrees with the pair-parallel
+    one to rounding) agrees within the gradient tolerance, 1e-3."""
+    w, pdis, angv = case(dem) if which == "dense" else sparse_case(dem)
+
+    def run(**env):
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        e = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_FP64, "cell": w.cell() + 0.01,
+                          "force_mode": dem.FORCE_PP if env.get("PP") else dem.FORCE_PCCP})
+        e.set_material(w.pp, w.pw)
+        e.upload(w.pos, w.rad, pdis, angv)
+        r = e.adjoint(STEPS, EVERY, dem.OBJ_POTENTIAL)
+        assert e.scalars()["status"] == 0
+        e.close()
+        return r
+
+    a = run(DEM_B200_WINDOW="1")
+    b = run(DEM_B200_WINDOW="0")
+    assert a["value"] == b["value"]
+    assert a["d_pp"] == b["d_pp"] and a["d_pw"] == b["d_pw"]
+    np.testing.assert_array_equal(a["d_radii"], b["d_radii"])
+    monkeypatch.setenv("DEM_B200_WINDOW", "1")
+    c = run(PP="1")
+    assert c["value"] == pytest.approx(a["value"], rel=1e-9)
+    floor = 1e-8 * abs(a["value"])
+    for key in KEYS:
+        x, y = sum(grad_from_adjoint(a, key)), sum(grad_from_adjoint(c, key))
+        assert abs(x - y) <= 1e-3 * abs(x) + floor, (key, x, y)
+    v = np.random.default_rng(4).normal(size=w.n)
+    x, y = float(a["d_radii"] @ v), float(c["d_radii"] @ v)
+    assert abs(x - y) <= 1e-3 * abs(x), (x, y)
+
+
 def test_adjoint_settle_50k_window(dem, wl, cuda):
     """The 50,000-sphere configuration: pre-settled 20,000 steps, then a
     2,000-step mixed-precision window with checkpoints every 100; gradients of

@@ -129,6 +129,40 @@ def test_trajectory_lattice_2k(dem, orc, wl, cuda, prec):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_config1_full_run(dem, orc, wl, cuda, prec):
+    """The 2,000-sphere lattice configuration at its full length, 20,000
+    steps (1,000 re-lists; the spheres fall, collide and settle into a bed
+    with ~1,650 contacts), stepped in ten calls: the FP64 engine tracks the
+    FP64 oracle to 1e-10 d with the same contact count, the mixed engine to
+    1e-5 d with the packing fraction within 1e-3 and the mean coordination
+    number within 0.02."""
+    w = wl.lattice_2k()
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    e = make_engine(dem, w, p)
+    for _ in range(10):
+        e.step(w.steps // 10)
+    s = e.scalars()
+    pos, _, _ = e.download()
+    cell = e.grid_info()[1]
+    e.close()
+    o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, cell, w.density, dem.material_array(w.pp, w.pw), prec == "mixed",
+                w.steps, w.relist_interval)
+    assert s["status"] == 0 and o["status"] == 0
+    assert s["relists"] == w.steps // w.relist_interval
+    oc = int(o["ncontacts"][-1])
+    assert oc > 1000                                   # a settled bed, not a free fall
+    rms = np.sqrt(np.mean((pos - o["pos"]) ** 2))
+    pf_o = np.sum(4.0 / 3.0 * np.pi * w.rad ** 3) / (w.world[0] * w.world[1] * o["maxhz"][-1])
+    if prec == "fp64":
+        assert rms <= 1e-10, rms
+        assert s["contacts"] == oc
+    else:
+        assert rms <= 1e-5, rms
+    assert abs(s["packing_fraction"] - pf_o) <= 1e-3
+    assert abs(s["mean_cn"] - 2.0 * oc / w.n) <= 0.02
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_dense_trajectory_and_history_carry(dem, orc, wl, cuda, prec):
     """A bed with ~3,500 persistent contacts, 401 steps (21 re-lists): every
     pair's carried FP64 tangential history, the positions and the contact

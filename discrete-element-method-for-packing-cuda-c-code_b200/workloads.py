@@ -30,8 +30,9 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (PREC_FP64, PREC_MIXED, RADII_BIDISPERSE, RADII_LOGNORMAL, contact, damp_from_restitution, estar,
-               gen_lattice, gen_radii, gen_rsa)
+from . import PREC_FP64, PREC_MIXED, RADII_BIDISPERSE, RADII_LOGNORMAL, contact
+# host-only generators (libdem_gen.so): a workload never loads the GPU library
+from .gen import damp_from_restitution, estar, gen_lattice, gen_radii, gen_rsa
 
 D_REF = 1e-3                       # m
 G = 9.81

@@ -10,6 +10,14 @@ full 10,000 steps from its initial state.  L2 is flushed (256 MiB write)
 between bench steps, outside the timed events; within a window the state
 stays as hot as it is in a real run.
 
+Besides the headline the JSON line carries: the FP64 plain form and the
+particle-parallel force mode on the same workload; the same 500,000 spheres
+as a settled bed (every sphere in contact: the contact path under load) with
+its window kernel's HBM roofline; the 4,000,000-sphere bidisperse workload;
+the adjoint window's cost; the end-to-end figure through the public API with
+host buffers; and the FP64 oracle on the host cores, whose sample also gives
+the mixed form's error against it.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 (under torchrun): independent replicas, one per GPU (the step has no
@@ -98,59 +106,91 @@ def profile_traffic(name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 50 ms while running."""
+    """SM clocks and clock-event (throttle) reasons of one GPU, polled through
+    NVML every ~1 ms by a background thread while running, so that a timed
+    region of a few milliseconds still holds samples; nvidia-smi at 50 ms
+    when NVML is unavailable.  Reads settings only."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+        self.samples = []        # (mhz, reasons bitmask)
+        self.smax = None
+        self.source = None
+        self._stop = threading.Event()
+        self._t = None
 
     def start(self):
+        self.samples = []
+        self._stop.clear()
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.source = "nvml, ~1 ms polling"
+
+            def poll():
+                while not self._stop.is_set():
+                    mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(mhz), int(rs)))
+                    time.sleep(0.001)
+            self._t = threading.Thread(target=poll, daemon=True)
+            self._t.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 2.0:   # polling before the timed region starts
+                time.sleep(0.001)
+        except Exception:
+            self._t = None
+            self._start_smi()
+
+    def _start_smi(self):
+        fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={fields}",
                                           "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-            t0 = time.time()
-            while not self.lines and time.time() - t0 < 3.0:   # sampler running before timing starts
-                time.sleep(0.02)
-            self.lines.clear()
+            self.source = "nvidia-smi, 50 ms"
+
+            def read():
+                for ln in self.proc.stdout:
+                    parts = [x.strip() for x in ln.split(",")]
+                    try:
+                        self.smax = float(parts[1])
+                        bits = 0
+                        for (nm, b), v in zip(self.REASONS, parts[2:6]):
+                            if v.lower().startswith("active"):
+                                bits |= b
+                        self.samples.append((float(parts[0]), bits))
+                    except (ValueError, IndexError):
+                        continue
+            self._t = threading.Thread(target=read, daemon=True)
+            self._t.start()
         except Exception:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 9:
-                continue
+        self._stop.set()
+        if getattr(self, "proc", None) is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=2.0)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": [], "samples": 0, "source": self.source}
+        mhz = [m for m, _ in self.samples]
+        bits = 0
+        for _, b in self.samples:
+            bits |= b
+        return {"sm_mhz": statistics.median(mhz), "sm_min_mhz": min(mhz), "sm_max_mhz": self.smax,
+                "reasons": [nm for nm, b in self.REASONS if bits & b], "samples": len(mhz), "source": self.source}
 
 
 def workload(dem, precision, rank):
@@ -162,7 +202,7 @@ def time_windows(torch, eng, stream, K, flush_buf, win, time_kernels=False):
     """Per-window CUDA events on the engine's stream; L2 flush between windows
     outside the events.  Returns total ms.  With time_kernels, the last timed
     window replays the engine's window graph variant that records CUDA events
-    around the re-list and each pair / particle launch (captured beforehand)."""
+    around the re-list and the window kernel (captured beforehand)."""
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     with torch.cuda.stream(stream):
         for k in range(K):
@@ -176,6 +216,32 @@ def time_windows(torch, eng, stream, K, flush_buf, win, time_kernels=False):
                 eng.set_window_timing(False)
     stream.synchronize()
     return sum(a.elapsed_time(b) for a, b in evs)
+
+
+def window_bytes(n, work, win, bp, ncells):
+    """Algorithmic bytes of one window (the byte model of the scope table:
+    every field of a particle touched once per step it is stepped, B_p per
+    particle-step, 56 B per pair-step), split into the window kernel's and the
+    re-list's.  A bound particle (a listed pair or a wall candidacy) is
+    stepped with the pair phase every step: win x B_p.  A free particle meets
+    nothing before the next re-list, so the window kernel reads and writes
+    its fields once and runs its steps in registers: B_p per window.  The
+    re-list: N (24 pos + 8 key/val + 16 sort + 4 cell start) + 8 C + 64 P
+    (the new list's ids and history written, the old list's read)."""
+    nb, P = work["bound"], work["pairs"]
+    kernel = win * (nb * bp + P * BYTES_PER_PAIR) + (n - nb) * bp
+    relist = n * (24 + 8 + 16 + 4) + 8 * ncells + 64 * P
+    return kernel, relist
+
+
+def roofline(kname, kbytes, kms, peak, peak_kind, workload, traffic=None, note=None):
+    achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else None
+    r = {"bound": "hbm", "kernel": kname, "workload": workload, "achieved": achieved, "peak": peak, "unit": "GB/s",
+         "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind, "traffic": traffic,
+         "algorithmic_bytes_per_launch": kbytes, "kernel_ms": kms}
+    if note:
+        r["note"] = note
+    return r
 
 
 def run_ours(args):
@@ -217,25 +283,29 @@ def run_ours(args):
     clk = clocks.stop()
     # dominant kernel duration: CUDA events inside the last timed window's graph
     kt = eng.window_kernel_times()
+    work = eng.window_work()
     sc = eng.scalars()
     max_ms = max_over_ranks(torch, dist, total_ms, dev, ws)
     dem_steps = K * win
     value = whole_job_rate(w.n, dem_steps, ws, max_ms)
+    ncells = eng.grid_info()[2]
 
     peak, peak_kind = measured_peak()
     bp = BYTES_PER_PARTICLE[args.precision]
-    pairs = sc["pairs"]
-    # dominant kernel: the window kernel (every step of a window in one launch).
-    # Algorithmic bytes per launch: each particle-step and pair-step touches
-    # its fields once (B_p, B_pair per particle-step / pair-step).
-    win_bytes_kernel = win * (w.n * bp + pairs * BYTES_PER_PAIR)
+    kbytes, rbytes = window_bytes(w.n, work, win, bp, ncells)
     if kt["window_kernel_ms"] > 0:
-        kname, kbytes, kms = "k_window", win_bytes_kernel, kt["window_kernel_ms"]
-    else:   # per-step kernels: the particle kernel per step
-        kname, kbytes, kms = "k_particle", w.n * bp, kt["particle_ms"]
-    achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else None
-    window_bytes = win_bytes_kernel + w.n * (24 + 8 + 16 + 4) + pairs * 64
-    traffic = profile_traffic(f"{kname}_rsa500k_{args.precision}")
+        kname, kms = "k_window", kt["window_kernel_ms"]
+    else:   # per-step kernels
+        kname, kms = "k_pair+k_particle", kt["pair_ms"] + kt["particle_ms"]
+    head_roof = roofline(kname, kbytes, kms, peak, peak_kind, w.name,
+                         traffic=profile_traffic(f"{kname}_rsa500k_{args.precision}"),
+                         note="free flight: ~5 % of the spheres are bound (a listed pair or a wall), the rest "
+                              "step in registers; the launch is latency-bound (grid barriers, dependent loads)")
+    head_roof.update({"kernel_timing": "CUDA events inside the last timed window's graph; window_kernel_ms is one "
+                                       "launch = the window's 20 steps, relist_ms one re-list",
+                      "kernel_ms_all": kt, "window_work": work,
+                      "step_bytes_per_window": kbytes + rbytes,
+                      "step_achieved_gbs": (kbytes + rbytes) / (max_ms / K / 1e3) / 1e9})
 
     # --- FP64 plain form of the same step (throughput bar for mixed)
     fp64 = None
@@ -272,6 +342,11 @@ def run_ours(args):
         ppm = {"value": w.n * k3 * win / (ms3 / 1e3), "unit": UNIT, "windows": k3,
                "pccp_over_pp": (value / ws) / (w.n * k3 * win / (ms3 / 1e3))}
 
+    # --- the same spheres as a settled bed: the contact path under load
+    bed = None
+    if not args.skip_bed and ws == 1:
+        bed = settled_bed(dem, torch, stream, flush, args, peak, peak_kind)
+
     # --- the 4,000,000-sphere bidisperse workload (mixed): the step at scale
     scale = None
     if not args.skip_4m and args.precision == "mixed" and ws == 1:
@@ -297,49 +372,19 @@ def run_ours(args):
     if not args.skip_adjoint:
         adj = adjoint_cost(dem, torch, stream)
 
-    # --- end to end through the public API with host buffers: pinned host
-    # state -> dem_upload_state -> K windows with a scalar read-back each
-    # (dem_get_scalars, a host sync) -> final dem_download_state to pinned host
+    # --- end to end through the public API with host buffers, the same K
+    # windows as the headline: pinned host state -> dem_upload_state -> K
+    # windows, each window's observables copied to pinned host memory as it
+    # ends (dem_scalars_enqueue) -> dem_download_state of the final state
     e2e = None
     if not args.skip_e2e:
-        hp = torch.from_numpy(w.pos).pin_memory()
-        hr = torch.from_numpy(w.rad).pin_memory()
-        out = torch.empty(3 * w.n, dtype=torch.float64).pin_memory()
-        outd = torch.empty(3 * w.n, dtype=torch.float64).pin_memory()
-        outa = torch.empty(3 * w.n, dtype=torch.float64).pin_memory()
-        ke = max(10, K // 5)
-        rawb = eng.scalars_raw_bytes()
-        raws = torch.empty((ke, rawb), dtype=torch.uint8).pin_memory()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0 = time.perf_counter()
-        a.record(stream)
-        eng.upload(hp.numpy(), hr.numpy())
-        # every window's observables go to pinned host memory as it ends
-        # (dem_scalars_enqueue: queued copies, no host wait between windows)
-        for k in range(ke):
-            eng.step(win)
-            eng.scalars_enqueue(raws[k].data_ptr())
-        pos_o, pdis_o, angv_o = out.numpy(), outd.numpy(), outa.numpy()
-        from dem_b200 import _ptr, check, lib
-        check(lib().dem_download_state(eng.handle, _ptr(pos_o), _ptr(pdis_o), _ptr(angv_o)), "download")
-        b.record(stream)
-        stream.synchronize()
-        e2e_status = max(eng.scalars_from_raw(raws[k].data_ptr())["status"] for k in range(ke))
-        wall = time.perf_counter() - t0
-        ev_ms = a.elapsed_time(b)
-        e2e_s = max_over_ranks(torch, dist, max(wall, ev_ms / 1e3) * 1e3, dev, ws) / 1e3
-        h2d = 3 * w.n * 8 + w.n * 8
-        d2h = 9 * w.n * 8 + ke * rawb
-        e2e = {"value": whole_job_rate(w.n, ke * win, ws, e2e_s * 1e3), "unit": UNIT, "windows": ke,
-               "h2d_bytes_per_step": h2d / ke, "d2h_bytes_per_step": d2h / ke, "status": e2e_status,
-               "timing": "host wall clock and CUDA events, larger of the two; every window's observables "
-                         "copied to pinned host memory as it ends and reduced on the host before the clock stops"}
+        e2e = end_to_end(dem, torch, dist, eng, w, stream, dev, ws, K, win)
 
-    # --- CPU baseline: the FP64 oracle on this host's cores, bounded sample
+    # --- CPU baseline: the FP64 oracle on this host's cores, bounded sample;
+    # the GPU's state after the same steps gives the mixed form's error
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
-        cpu = cpu_baseline(dem, w, args.cpu_steps)
+        cpu = cpu_baseline(dem, w, args.cpu_steps, stream)
     eng.close()
     if ws > 1:
         dist.barrier()
@@ -354,22 +399,15 @@ def run_ours(args):
                    "dem_steps_per_bench_step": win, "dem_steps_timed": dem_steps, "precision": args.precision,
                    "relist_interval": win, "skin_d": w.skin, "parallelism": f"replicas x{ws}",
                    "l2": "flushed between bench steps (256 MiB write, outside the timed events)",
-                   "ms_per_dem_step": max_ms / dem_steps, "pairs_per_particle": pairs / w.n,
+                   "ms_per_dem_step": max_ms / dem_steps, "pairs_per_particle": sc["pairs"] / w.n,
                    "contacts_per_particle": sc["contacts"] / w.n, "packing_fraction": sc["packing_fraction"],
                    "mean_cn": sc["mean_cn"]},
-        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": kbytes,
-                     "note": "algorithmic bytes count every particle-step's fields once; the window kernel "
-                             "keeps free particles in registers across its steps, so achieved can exceed the "
-                             "copy peak while DRAM traffic (traffic) stays far below the algorithmic bytes",
-                     "kernel_ms": kt, "kernel_timing": "CUDA events inside the last timed window's graph "
-                     "(mean over its 20 steps)", "step_bytes_per_window": window_bytes,
-                     "step_achieved_gbs": window_bytes / (max_ms / K / 1e3) / 1e9},
+        "roofline": head_roof,
         "clocks": clk,
         "gpu_launches": KERNELS_PER_WINDOW * K,
         "fp64_plain": fp64,
         "pp_mode": ppm,
+        "settled_bed": bed,
         "scale_4m": scale,
         "adjoint": adj,
         "e2e": e2e,
@@ -378,11 +416,113 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
+def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
+    """bed_500k: the 500,000 spheres compacted into a bed (velocity
+    proportional to height, then gravity) and settled on the GPU, untimed;
+    then windows of the production cadence on it, timed: the mixed form (the
+    default force mode, with the window kernel's time and roofline) and the
+    FP64 plain form, with the bed's pairs, contacts and packing fraction."""
+    import dem_b200.workloads as wmod
+    t0 = time.perf_counter()
+    w0 = wmod.bed_500k_initial()
+    w = wmod.dense_bed(dem, w0, w0.meta["compact_steps"] + args.bed_settle_steps, stream=stream.cuda_stream)
+    settle_s = time.perf_counter() - t0
+    pdis, angv = w.meta["pdis"], w.meta["angv"]
+    win = w.relist_interval
+    kb = args.bed_windows
+    out = {"workload": w.name, "n_particles": w.n, "box_mm": list(w.world),
+           "init": w.meta["init"], "settle_steps": w.meta["settle_steps"], "settle_s": settle_s,
+           "settle_status": w.meta["settled"]["status"]}
+    for prec, key in ((dem.PREC_MIXED, "mixed"), (dem.PREC_FP64, "fp64")):
+        e = dem.Engine(**{**w.engine_kwargs(), "precision": prec})
+        e.set_stream(stream.cuda_stream)
+        e.set_material(w.pp, w.pw)
+        e.upload(w.pos, w.rad, pdis, angv)
+        with torch.cuda.stream(stream):
+            e.step(2 * win)
+            e.set_window_timing(True)
+            e.step(2 * win)
+            e.set_window_timing(False)
+        ms = time_windows(torch, e, stream, kb, flush, win, time_kernels=True)
+        kt = e.window_kernel_times()
+        work = e.window_work()
+        s = e.scalars(raise_on_status=False)
+        ncells = e.grid_info()[2]
+        e.close()
+        bp = BYTES_PER_PARTICLE[key]
+        kbytes, rbytes = window_bytes(w.n, work, win, bp, ncells)
+        r = {"value": w.n * kb * win / (ms / 1e3), "unit": UNIT, "windows": kb, "ms_per_dem_step": ms / (kb * win),
+             "pairs_per_particle": s["pairs"] / w.n, "contacts_per_particle": s["contacts"] / w.n,
+             "mean_cn": s["mean_cn"], "packing_fraction": s["packing_fraction"], "status": s["status"],
+             "window_work": work, "kernel_ms": kt}
+        if kt["window_kernel_ms"] > 0:
+            r["roofline"] = roofline("k_window", kbytes, kt["window_kernel_ms"], peak, peak_kind, w.name,
+                                     traffic=profile_traffic(f"k_window_bed500k_{key}"),
+                                     note="every sphere bound: B_p x 20 per sphere + 56 B x 20 per pair")
+        r["step_achieved_gbs"] = (kbytes + rbytes) / (ms / kb / 1e3) / 1e9
+        out[key] = r
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["roofline"] = out["mixed"].get("roofline")
+    return out
+
+
+def end_to_end(dem, torch, dist, eng, w, stream, dev, ws, K, win):
+    """K windows end to end through the public API with host buffers (the
+    headline's K), timed by the host clock and by CUDA events (the larger
+    counts), and the same with every phase bracketed by events."""
+    from dem_b200 import _ptr, check, lib
+    hp = torch.from_numpy(w.pos).pin_memory()
+    hr = torch.from_numpy(w.rad).pin_memory()
+    outs = [torch.empty(3 * w.n, dtype=torch.float64).pin_memory() for _ in range(3)]
+    rawb = eng.scalars_raw_bytes()
+    raws = torch.empty((K, rawb), dtype=torch.uint8).pin_memory()
+
+    def job(phases=None):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev[0].record(stream)
+        eng.upload(hp.numpy(), hr.numpy())
+        if phases is not None:
+            ev[1].record(stream)
+        for k in range(K):
+            eng.step(win)
+            eng.scalars_enqueue(raws[k].data_ptr())
+        if phases is not None:
+            ev[2].record(stream)
+        check(lib().dem_download_state(eng.handle, _ptr(outs[0].numpy()), _ptr(outs[1].numpy()),
+                                       _ptr(outs[2].numpy())), "download")
+        ev[3].record(stream)
+        stream.synchronize()
+        status = max(eng.scalars_from_raw(raws[k].data_ptr())["status"] for k in range(K))
+        wall = time.perf_counter() - t0
+        if phases is not None:
+            phases.update(upload_ms=ev[0].elapsed_time(ev[1]), windows_ms=ev[1].elapsed_time(ev[2]),
+                          download_ms=ev[2].elapsed_time(ev[3]))
+        return max(wall * 1e3, ev[0].elapsed_time(ev[3])), status
+
+    job()                      # warm: pinned buffers touched, graphs of this context captured
+    ms, status = job()
+    phases = {}
+    job(phases)
+    e2e_ms = max_over_ranks(torch, dist, ms, dev, ws)
+    h2d = 3 * w.n * 8 + w.n * 8
+    d2h = 9 * w.n * 8 + K * rawb
+    return {"value": whole_job_rate(w.n, K * win, ws, e2e_ms), "unit": UNIT, "windows": K,
+            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K, "status": status, "ms": e2e_ms,
+            "phases_ms": phases,
+            "timing": "host wall clock and CUDA events around upload -> K windows -> download, larger of the two; "
+                      "every window's observables copied to pinned host memory as it ends and reduced on the host "
+                      "before the clock stops; phases_ms from a second job with events between the phases"}
+
+
 def adjoint_cost(dem, torch, stream):
     """settle_50k: 50,000 lognormal spheres (40x40x150 mm) pre-settled for
-    20,000 steps, then a 2,000-step window, checkpoints every 100: time of
-    the reverse sweep (objective + recompute + reverse) against the plain
-    forward window, packing-fraction objective."""
+    20,000 steps, then a 2,000-step window, checkpoints every 100, potential
+    energy objective (whose friction gradients are not zero: the packing
+    fraction's max height belongs to a sphere in free fall).  The whole call
+    (checkpointed forward + objective + recompute + reverse) and the reverse
+    part alone against the plain forward window."""
     import dem_b200.workloads as wm
     w = wm.settle_50k()
     e = dem.Engine(**w.engine_kwargs())
@@ -399,31 +539,65 @@ def adjoint_cost(dem, torch, stream):
     stream.synchronize()
     fwd_ms = a.elapsed_time(b)
     e.upload(pos, w.rad, pdis, angv)
-    e.adjoint(w.steps, 100, dem.OBJ_PACKING)           # warm-up (allocates the tape)
+    e.adjoint(w.steps, 100, dem.OBJ_POTENTIAL)           # warm-up (allocates the tape)
     e.upload(pos, w.rad, pdis, angv)
-    r = e.adjoint(w.steps, 100, dem.OBJ_PACKING)
+    c, d = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c.record(stream)
+    r = e.adjoint(w.steps, 100, dem.OBJ_POTENTIAL)
+    d.record(stream)
+    stream.synchronize()
+    call_ms = c.elapsed_time(d)
     e.close()
     return {"workload": w.name, "n_particles": w.n, "window_steps": w.steps, "checkpoint_every": 100,
-            "objective": "packing fraction", "forward_window_ms": fwd_ms,
-            "checkpointed_forward_ms": r["forward_ms"], "reverse_ms": r["adjoint_ms"],
-            "adjoint_over_forward": r["adjoint_ms"] / fwd_ms,
-            "d_mu": r["d_pp"]["mu"] + r["d_pw"]["mu"], "d_roll_rel": r["d_pp"]["roll_rel"] + r["d_pw"]["roll_rel"]}
+            "objective": "potential energy", "forward_window_ms": fwd_ms,
+            "checkpointed_forward_ms": r["forward_ms"], "reverse_ms": r["adjoint_ms"], "call_ms": call_ms,
+            "call_over_forward": call_ms / fwd_ms,
+            "forward_plus_reverse_over_forward": (r["forward_ms"] + r["adjoint_ms"]) / fwd_ms,
+            "reverse_over_forward": r["adjoint_ms"] / fwd_ms,
+            "d_log_mu": r["d_pp"]["mu"] * w.pp["mu"] + r["d_pw"]["mu"] * w.pw["mu"],
+            "d_log_roll_rel": r["d_pp"]["roll_rel"] * w.pp["roll_rel"] + r["d_pw"]["roll_rel"] * w.pw["roll_rel"],
+            "objective_value": r["value"]}
 
 
-def cpu_baseline(dem, w, steps):
+def cpu_baseline(dem, w, steps, stream):
+    """The FP64 oracle (OpenMP, all host threads) on `steps` DEM steps of the
+    workload from its initial state; the mixed GPU form's state after the
+    same steps against it: packing fraction, mean coordination number and
+    per-particle position RMS (the observables of dempacking.cu:766-776)."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as orc
     threads = orc.num_threads()
     mat = dem.material_array(w.pp, w.pw)
-    st = orc.Stepper(w.pos, w.rad, w.world, w.dt, w.skin, w.cell(), w.density, mat,
-                     w.precision == dem.PREC_MIXED, w.relist_interval)
     t0 = time.perf_counter()
-    st.step(steps)
+    o = orc.run(w.pos, w.rad, w.world, w.dt, w.skin, w.cell(), w.density, mat, False, steps, w.relist_interval)
     dt = time.perf_counter() - t0
-    st.close()
+    e = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_MIXED})
+    e.set_stream(stream.cuda_stream)
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad)
+    e.step(steps)
+    s = e.scalars()
+    pos, _, _ = e.download()
+    e.close()
+    phi_o = float(np.sum(4.0 / 3.0 * np.pi * w.rad ** 3) / (w.world[0] * w.world[1] * o["maxhz"][-1]))
+    cn_o = 2.0 * float(o["ncontacts"][-1]) / w.n
+    err = {"steps": steps, "packing_fraction_abs": abs(s["packing_fraction"] - phi_o),
+           "mean_cn_abs": abs(s["mean_cn"] - cn_o), "position_rms_d": float(np.sqrt(np.mean((pos - o["pos"]) ** 2))),
+           "oracle_status": int(o["status"]), "max_contacts_seen": int(np.max(o["ncontacts"]))}
     return {"value": w.n * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{steps} DEM steps ({steps // w.relist_interval} re-lists) of {w.name} from its initial "
-                      f"state, FP64 oracle, OpenMP {threads} threads"}
+                      f"state, FP64 oracle, OpenMP {threads} threads",
+            "mixed_error_vs_oracle": err}
+
+
+def mapped_libraries():
+    """This repository's shared libraries mapped into the process."""
+    try:
+        maps = pathlib.Path("/proc/self/maps").read_text()
+    except OSError:
+        return None
+    names = sorted({ln.split()[-1] for ln in maps.splitlines() if ln.endswith(".so") and str(ROOT) in ln})
+    return [str(pathlib.Path(x).relative_to(ROOT)) for x in names]
 
 
 def run_reference(args):
@@ -459,6 +633,7 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} DEM steps of {w.name} after {args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_mapped": mapped_libraries(),
     }
     print(json.dumps(line), flush=True)
 
@@ -466,15 +641,19 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--cpu-steps", type=int, default=1000)
+    ap.add_argument("--bed-settle-steps", type=int, default=10000,
+                    help="settling steps of the bed after its 25,000 compaction steps")
+    ap.add_argument("--bed-windows", type=int, default=10)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-pp", action="store_true")
+    ap.add_argument("--skip-bed", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-4m", action="store_true")
     args = ap.parse_args()

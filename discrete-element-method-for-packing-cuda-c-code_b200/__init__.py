@@ -167,6 +167,8 @@ _SIGS = [
     ("dem_kernel_times", ctypes.c_int, [_vp, _c_double_p]),
     ("dem_set_window_timing", ctypes.c_int, [_vp, ctypes.c_int]),
     ("dem_window_kernel_times", ctypes.c_int, [_vp, _c_double_p]),
+    ("dem_window_work", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
     ("dem_adjoint_window", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(AdjointResult), _vp]),
     ("dem_adjoint_release", ctypes.c_int, [_vp]),
@@ -546,6 +548,13 @@ class Engine:
 
     def set_window_timing(self, on=True):
         check(lib().dem_set_window_timing(self._h, 1 if on else 0), "dem_set_window_timing")
+
+    def window_work(self):
+        """Bound particles, wall candidates and listed pairs of the current
+        list's window (dem_window_work)."""
+        b, w, p = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
+        check(lib().dem_window_work(self._h, ctypes.byref(b), ctypes.byref(w), ctypes.byref(p)), "dem_window_work")
+        return {"bound": b.value, "wall_candidates": w.value, "pairs": p.value}
 
     def window_kernel_times(self):
         out = (ctypes.c_double * 5)()

@@ -885,6 +885,8 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     if (d_radii) DEM_CUDA_TRY(cudaMemcpyAsync(d_radii, w->Rb, c->n * sizeof(double), cudaMemcpyDeviceToHost, s));
     DEM_CUDA_TRY(cudaStreamSynchronize(s));
     if (d_radii && c->ordered) {   // into the caller's particle order
+        const int rp = host_perm(c);
+        if (rp) return rp;
         std::vector<double> t(d_radii, d_radii + c->n);
         for (long long i = 0; i < c->n; i++) d_radii[c->hperm[i]] = t[i];
     }

@@ -440,6 +440,7 @@ template <typename Real> struct StepArgs {
     LawParams<Real> pp, pw;
     ParticleCommon pc;
     Real dtr, inv_dt, density;
+    int split;                    // window kernels: bound items per thread of the bound blocks (0: all blocks)
     EngineWords* words;
     double *dbgF, *dbgT;
     uint* dbgC;
@@ -863,16 +864,17 @@ __device__ __forceinline__ void red_release_add(uint* p, uint v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Grid-wide barrier number `k` (0, 1, ...) of a window-kernel launch: every
-// block adds 1 to the arrival counter with release semantics and waits, with
-// acquire loads, until it reaches (k+1) x blocks (bounded as above).
+// Barrier number `k` (0, 1, ...) among the first `nblk` blocks of a
+// window-kernel launch (the blocks that hold bound work): every one adds 1 to
+// the arrival counter with release semantics and waits, with acquire loads,
+// until it reaches (k+1) x nblk (bounded as above).
 __device__ __forceinline__ void grid_arrive(uint* bar) {
     __syncthreads();
     if (threadIdx.x == 0) red_release_add(bar, 1u);
 }
-__device__ __forceinline__ void grid_wait(uint* bar, uint k, EngineWords* words) {
+__device__ __forceinline__ void grid_wait(uint* bar, uint k, uint nblk, EngineWords* words) {
     if (threadIdx.x == 0) {
-        const uint target = (k + 1u) * gridDim.x;
+        const uint target = (k + 1u) * nblk;
         if (!ld_acquire(bar + kBarGiveUp)) {
             unsigned long long t0 = global_ns();
             uint polls = 0;
@@ -891,9 +893,9 @@ __device__ __forceinline__ void grid_wait(uint* bar, uint k, EngineWords* words)
     }
     __syncthreads();
 }
-__device__ __forceinline__ void grid_barrier(uint* bar, uint k, EngineWords* words) {
+__device__ __forceinline__ void grid_barrier(uint* bar, uint k, uint nblk, EngineWords* words) {
     grid_arrive(bar);
-    grid_wait(bar, k, words);
+    grid_wait(bar, k, nblk, words);
 }
 
 // Check of the bounded wait: the launch's one block arrives once and waits
@@ -902,34 +904,77 @@ __device__ __forceinline__ void grid_barrier(uint* bar, uint k, EngineWords* wor
 // the nanoseconds waited.
 __global__ void k_barrier_check(uint* bar, EngineWords* words, unsigned long long* spent) {
     const unsigned long long t0 = global_ns();
-    grid_arrive(bar);          // the counter reaches 1
-    grid_wait(bar, 1, words);  // waits for 2 (one block): gives up
+    grid_arrive(bar);                    // the counter reaches 1
+    grid_wait(bar, 1, gridDim.x, words);  // waits for 2 (one block): gives up
     if (threadIdx.x == 0) *spent = global_ns() - t0;
 }
 
-// The whole window's steps in one cooperative launch (after the re-list):
-// per step, phase 1 = wall + pair items, barrier, phase 2 = bound particles
-// plus 1/K of the free particles (each run through all K steps in
-// registers), barrier.  Items and particles keep their thread for the whole
-// window; data written by other blocks is read with L2-coherent loads.  The
-// arithmetic is that of the per-step kernels (same device functions), so the
-// states are bit-identical.  Observables of the window's last step go to
-// `part` (one partial per block; the slot's remaining partials are cleared).
+// The whole window's steps in one cooperative launch (after the re-list).
+// The launch's blocks are split by the window's work: the first `nbb` blocks
+// (bound_blocks) hold the bound work and step it together -- per step, phase
+// 1 = wall + pair items, barrier among them, phase 2 = bound particles,
+// barrier -- while the other blocks run every free particle through all K
+// steps in registers, without any barrier (a free particle meets nothing
+// before the next re-list, so its steps need no other particle).  When the
+// bound work needs every block (a dense bed), the free particles are dealt
+// over the steps instead: 1/K of them in each phase 2.  Items and particles
+// keep their thread for the whole window; data written by other blocks is
+// read with L2-coherent loads.  The arithmetic is that of the per-step
+// kernels (same device functions), so the states are bit-identical whatever
+// the split.  Observables of the window's last step go to `part` (one
+// partial per block; the slot's remaining partials are cleared).
 constexpr int kWinThreads = 512;
+
+// Blocks of a window launch of `grid` blocks that take the bound work:
+// `split` bound items (or bound particles, whichever are more) per thread,
+// ceil(max(items, nb) / (kWinThreads * split)) blocks; all of them when split
+// <= 0 or when every particle is bound; none when there is no bound work.
+__device__ __forceinline__ uint bound_blocks(long long items, long long nb, long long nf, uint grid, int split) {
+    if (split <= 0 || nf == 0) return grid;
+    const long long need = items > nb ? items : nb;
+    const long long per = (long long)kWinThreads * split;
+    const long long b = (need + per - 1) / per;
+    return (uint)(b < (long long)grid ? b : (long long)grid);
+}
+
+// Free particles flist[fid], flist[fid + stride], ... through all K steps
+// (the free-only blocks of a split window launch).
+template <typename Real>
+__device__ __forceinline__ void free_sweep(const StepArgs<Real>& a, const PRec<Real>* Sin, PRec<Real>* Sout,
+                                           long long fid, long long stride, long long nf, int K, double& mz,
+                                           uint& flags) {
+    for (long long t = fid; t < nf; t += stride) {
+        double mzi = 0.0;
+        free_item<Real>(a, Sin, Sout, a.flist[t], 0, K, K - 1, false, mzi, flags);
+        mz = fmax(mz, mzi);
+    }
+}
 
 template <typename Real>
 __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int K, StepPartials part, size_t npart,
                                                            uint* bar) {
-    const long long nthr = (long long)gridDim.x * blockDim.x;
-    // work index: warps dealt round-robin over the blocks (SMs), lanes
-    // contiguous, so every phase spreads over the whole GPU
-    const long long tid =
-        ((long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x) * 32 + (threadIdx.x & 31);
     uint nbar = 0;
     const uint nw = *a.wcount;
     const uint total = a.off[a.n];
     const long long items = (long long)nw + ((long long)total <= a.cap ? (long long)total : 0ll);
     const long long nb = a.bpos[a.n], nf = a.n - nb;
+    const uint nbb = bound_blocks(items, nb, nf, gridDim.x, a.split);
+    const long long warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    if (blockIdx.x >= nbb) {   // free-only block
+        const uint nfb = gridDim.x - nbb;
+        free_sweep<Real>(a, a.S, a.S, (warp * nfb + (blockIdx.x - nbb)) * 32 + lane, (long long)nfb * kWinThreads, nf,
+                         K, mz, flags);
+        block_observables(mz, cnt, flags, 1, part, a.words);
+        clear_partials(part, gridDim.x, npart);
+        return;
+    }
+    const bool deal_free = nbb == gridDim.x;   // no free-only blocks: free particles go with the steps
+    const long long nthr = (long long)nbb * blockDim.x;
+    // work index: warps dealt round-robin over the bound blocks (SMs), lanes
+    // contiguous, so every phase spreads over all of them
+    const long long tid = (warp * nbb + blockIdx.x) * 32 + lane;
     // this thread's first item and first bound particle: indices kept in
     // registers for the whole window (further ones are reloaded per step)
     uint i0 = 0, j0 = 0, s0 = 0;
@@ -942,8 +987,6 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
         ws0 = a.wslot[b0];
         o00 = a.off[b0]; o10 = a.off[b0 + 1]; r00 = a.roff[b0]; r10 = a.roff[b0 + 1];
     }
-    double mz = 0.0;
-    uint cnt = 0, flags = 0;
     ParticleCommon pc = a.pc;
     for (int s = 0; s < K; s++) {
         const long long ts = a.tx ? (long long)a.tstep0 + s : -1ll;
@@ -954,9 +997,10 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
             if (u < (long long)nw) wall_item<Real, true>(a, u, i, ts);
             else pair_item<Real, true>(a, u - nw, i, j, rslot, ts);
         }
-        grid_barrier(bar, nbar++, a.words);
-        // phase 2: bound particles; this step's share of the free particles
-        // (each run through all K steps) from the other end of the work range
+        grid_barrier(bar, nbar++, nbb, a.words);
+        // phase 2: bound particles; with no free-only blocks, this step's
+        // share of the free particles (each run through all K steps) from the
+        // other end of the work range
         pc.first = s == 0 ? 1 : 0;
         for (long long t = tid; t < nb; t += nthr) {
             double mzi = 0.0;
@@ -970,13 +1014,15 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
             }
             if (s == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
         }
-        const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
-        for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
-            double mzi = 0.0;
-            free_item<Real>(a, a.S, a.S, a.flist[t], 0, K, K - 1, false, mzi, flags);
-            mz = fmax(mz, mzi);
+        if (deal_free) {
+            const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
+            for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
+                double mzi = 0.0;
+                free_item<Real>(a, a.S, a.S, a.flist[t], 0, K, K - 1, false, mzi, flags);
+                mz = fmax(mz, mzi);
+            }
         }
-        if (s < K - 1) grid_barrier(bar, nbar++, a.words);
+        if (s < K - 1) grid_barrier(bar, nbar++, nbb, a.words);
     }
     block_observables(mz, cnt, flags, 1, part, a.words);
     clear_partials(part, gridDim.x, npart);
@@ -1060,22 +1106,36 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     if (pc.observe) clear_partials(part, clr0, clr1);
 }
 
-// PP window kernel (one cooperative launch per window, as k_window): per
-// step, every bound particle runs pp_item from the "in" buffers into the
-// "out" buffers, and 1/K of the free particles run all K steps in registers
-// (read from the window's first state buffer, written to its last); one grid
-// barrier per step, then the buffers swap.  Same device functions as the
-// per-step PP kernel, so the states are bit-identical.
+// PP window kernel (one cooperative launch per window, as k_window, with the
+// same split of its blocks): per step, every bound particle runs pp_item from
+// the "in" buffers into the "out" buffers, one barrier among the bound blocks
+// per step, then the buffers swap; the free particles run all K steps in
+// registers (read from the window's first state buffer, written to its last),
+// in the free-only blocks or, with none, 1/K of them per step.  Same device
+// functions as the per-step PP kernel, so the states are bit-identical.
 template <typename Real>
 __global__ void __launch_bounds__(kWinThreads, 1) k_window_pp(StepArgs<Real> a, PRec<Real>* S0, PRec<Real>* S1,
                                                               Planes3<double> H0, Planes3<double> H1, int K,
                                                               StepPartials part, size_t npart, uint* bar) {
-    const long long nthr = (long long)gridDim.x * blockDim.x;
-    const long long tid =
-        ((long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x) * 32 + (threadIdx.x & 31);
     uint nbar = 0;
     const uint total = a.off[a.n];
     const long long nb = a.bpos[a.n], nf = a.n - nb;
+    const uint nbb = bound_blocks(nb, nb, nf, gridDim.x, a.split);
+    const long long warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    PRec<Real>* Sf = (K & 1) ? S1 : S0;   // the free particles' final buffer
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    if (blockIdx.x >= nbb) {   // free-only block
+        const uint nfb = gridDim.x - nbb;
+        free_sweep<Real>(a, S0, Sf, (warp * nfb + (blockIdx.x - nbb)) * 32 + lane, (long long)nfb * kWinThreads, nf, K,
+                         mz, flags);
+        block_observables(mz, cnt, flags, 1, part, a.words);
+        clear_partials(part, gridDim.x, npart);
+        return;
+    }
+    const bool deal_free = nbb == gridDim.x;
+    const long long nthr = (long long)nbb * blockDim.x;
+    const long long tid = (warp * nbb + blockIdx.x) * 32 + lane;
     // this thread's first bound particle: list data kept in registers
     uint b0 = 0, o00 = 0, o10 = 0, r00 = 0, r10 = 0;
     Real rb0 = (Real)0;
@@ -1084,9 +1144,6 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window_pp(StepArgs<Real> a, 
         rb0 = a.R[b0];
         o00 = a.off[b0]; o10 = a.off[b0 + 1]; r00 = a.roff[b0]; r10 = a.roff[b0 + 1];
     }
-    PRec<Real>* Sf = (K & 1) ? S1 : S0;   // the free particles' final buffer
-    double mz = 0.0;
-    uint cnt = 0, flags = 0;
     ParticleCommon pc = a.pc;
     for (int s = 0; s < K; s++) {
         PRec<Real>* Si = (s & 1) ? S1 : S0;
@@ -1108,13 +1165,15 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window_pp(StepArgs<Real> a, 
             }
             if (s == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
         }
-        const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
-        for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
-            double mzi = 0.0;
-            free_item<Real>(a, S0, Sf, a.flist[t], 0, K, K - 1, false, mzi, flags);
-            mz = fmax(mz, mzi);
+        if (deal_free) {
+            const long long f0 = nf * s / K, f1 = nf * (s + 1) / K;
+            for (long long t = f0 + (nthr - 1 - tid); t < f1; t += nthr) {
+                double mzi = 0.0;
+                free_item<Real>(a, S0, Sf, a.flist[t], 0, K, K - 1, false, mzi, flags);
+                mz = fmax(mz, mzi);
+            }
         }
-        if (s < K - 1) grid_barrier(bar, nbar++, a.words);
+        if (s < K - 1) grid_barrier(bar, nbar++, nbb, a.words);
     }
     block_observables(mz, cnt, flags, 1, part, a.words);
     clear_partials(part, gridDim.x, npart);
@@ -1283,6 +1342,7 @@ template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int
     a.dtr = (Real)c->cfg.dt;
     a.inv_dt = (Real)(1.0 / c->cfg.dt);
     a.density = (Real)c->cfg.density;
+    a.split = c->win_split;
     a.words = c->words;
     a.dbgF = c->record ? c->dbgF : nullptr;
     a.dbgT = c->record ? c->dbgT : nullptr;
@@ -1558,6 +1618,18 @@ size_t real_size(int prec) { return prec == DEM_PREC_MIXED ? sizeof(float) : siz
 
 }  // namespace
 
+namespace dem {
+int host_perm(dem_ctx* c) {
+    if (!c->hperm_stale) return DEM_OK;
+    const long long n = c->ntot;
+    c->hperm.resize(n);
+    DEM_CUDA_TRY(cudaMemcpyAsync(c->hperm.data(), c->perm, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->hperm_stale = false;
+    return DEM_OK;
+}
+}  // namespace dem
+
 extern "C" {
 
 int dem_create(const dem_config* cfg, dem_ctx** out) {
@@ -1658,6 +1730,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->pdl = !(pdl && pdl[0] == '0');
         const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order
         c->reorder = !(ro && ro[0] == '0');
+        const char* sp = getenv("DEM_B200_SPLIT");   // window kernels' bound items per thread (0: no split)
+        if (sp && sp[0]) c->win_split = atoi(sp);
     }
     // partials per slot: particle-kernel blocks, free-kernel blocks, and at
     // least as many as the window kernel has blocks
@@ -1682,6 +1756,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         if (e != cudaSuccess) return bail(cuda_fail(e, "cudaEventCreate", __FILE__, __LINE__));
     }
     e = cudaEventCreateWithFlags(&c->ext_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->h2d_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evfork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evjoin, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
@@ -1711,6 +1786,7 @@ int dem_destroy(dem_ctx* c) {
     for (int k = 0; k < 4; k++)
         if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->ext_ready) cudaEventDestroy(c->ext_ready);
+    if (c->h2d_done) cudaEventDestroy(c->h2d_done);
     if (c->evfork) cudaEventDestroy(c->evfork);
     if (c->evjoin) cudaEventDestroy(c->evjoin);
     for (cudaEvent_t e : c->wev) cudaEventDestroy(e);
@@ -1825,11 +1901,14 @@ __global__ void k_perm_of(long long n, const uint2* __restrict__ kv, uint* __res
 // that keeps neighbours together serves; this one is the re-list's).
 // Computed on the device from the uploaded positions (pos: device AoS): a
 // stable radix sort of (key, id) in the walk's scratch (free between
-// re-lists), then the permutation goes to c->perm and, for the downloads that
-// map ids, to the host (c->hperm; the call waits for it).  Leaves hperm empty
-// (the caller's order) when the grid is too large (over 2^27 cells).
-static int device_cell_order(dem_ctx* c, const double* pos, long long n) {
+// re-lists), then the permutation goes to c->perm; the host copy that the
+// id-mapping downloads use is fetched on first use (host_perm), so the
+// upload does not wait for the sort.  *ordered = false (the caller's order)
+// when the grid is too large (over 2^27 cells) or the particles too few.
+static int device_cell_order(dem_ctx* c, const double* pos, long long n, bool* ordered) {
     c->hperm.clear();
+    c->hperm_stale = false;
+    *ordered = false;
     const double cs = c->cfg.cell > 0.0 ? c->cfg.cell : 2.0 * c->rmax + c->cfg.skin + 1e-4;
     if (!(cs > 0.0)) return DEM_OK;
     const long long gx = (long long)(c->cfg.world[0] / cs) + 1, gy = (long long)(c->cfg.world[1] / cs) + 1,
@@ -1853,11 +1932,11 @@ static int device_cell_order(dem_ctx* c, const double* pos, long long n) {
     if ((rc = radix_sort_pairs(kv, kv2, (uint)n, bits, scratch, c->stream))) return rc;
     k_perm_of<<<grid_for(n, 256), 256, 0, c->stream>>>(n, kv, c->perm);
     DEM_LAUNCH_CHECK();
-    c->hperm.resize(n);
-    DEM_CUDA_TRY(cudaMemcpyAsync(c->hperm.data(), c->perm, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->hperm_stale = true;
+    *ordered = true;
     return DEM_OK;
 }
+
 
 enum UploadOrder { kOrderCaller = 0, kOrderCells = 1, kOrderGiven = 2 };
 
@@ -1878,11 +1957,15 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
     const double *ppos = pos, *ppd = pdis, *ppa = angv, *prad = rad;
     c->ordered = false;
     c->hperm.clear();
+    c->hperm_stale = false;
     if (host) {
         DEM_CUDA_TRY(cudaMemcpyAsync(spos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (pdis) DEM_CUDA_TRY(cudaMemcpyAsync(sd, pdis, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (angv) DEM_CUDA_TRY(cudaMemcpyAsync(sa, angv, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         DEM_CUDA_TRY(cudaMemcpyAsync(sr, rad, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        // the call returns once the copies have read the caller's buffers
+        // (not after the device work that follows them)
+        DEM_CUDA_TRY(cudaEventRecord(c->h2d_done, c->stream));
         ppos = spos; ppd = pdis ? sd : nullptr; ppa = angv ? sa : nullptr; prad = sr;
         double rm = 0.0, v3 = 0.0;
         for (long long i = 0; i < n; i++) {
@@ -1892,8 +1975,9 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
         }
         c->rmax = rm;
         c->vol = 4.0 / 3.0 * M_PI * v3;
+        bool cell_ordered = false;
         if (order == kOrderCells && c->reorder) {
-            int rc = device_cell_order(c, spos, n);
+            int rc = device_cell_order(c, spos, n, &cell_ordered);
             if (rc) return rc;
         } else if (order == kOrderGiven && given) {
             c->hperm.assign(given, given + n);
@@ -1904,7 +1988,7 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
             DEM_CUDA_TRY(cudaMemcpyAsync(c->perm, c->hperm.data(), n * sizeof(uint), cudaMemcpyHostToDevice,
                                          c->stream));
         }
-        c->ordered = !c->hperm.empty();
+        c->ordered = cell_ordered || !c->hperm.empty();
     } else {
         // the caller's buffers may have been written on the legacy stream
         DEM_CUDA_TRY(cudaEventRecord(c->ext_ready, 0));
@@ -1934,7 +2018,10 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
                                                                    (PRec<double>*)c->rec[0], (double*)c->rad, c->q,
                                                                    planes<double>(c->wh, np), gather);
     DEM_LAUNCH_CHECK();
-    return finish_upload(c);
+    int rc = finish_upload(c);
+    if (rc) return rc;
+    if (host) DEM_CUDA_TRY(cudaEventSynchronize(c->h2d_done));   // the caller may reuse its buffers
+    return DEM_OK;
 }
 
 int dem_upload_state(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
@@ -2050,6 +2137,7 @@ int dem_set_pour(dem_ctx* c, long long nplayer, double tnewpar, long long n_acti
         // (the state is kept, the contact history restarts)
         std::vector<double> pos(3 * ntot), pdis(3 * ntot), angv(3 * ntot), rad(ntot), ri(ntot);
         int rc = download_common(c, pos.data(), pdis.data(), angv.data(), true);
+        if (!rc) rc = host_perm(c);
         if (rc) return rc;
         if (c->prec == DEM_PREC_MIXED) {
             std::vector<float> rf(ntot);
@@ -2238,6 +2326,8 @@ int dem_download_forces(dem_ctx* c, double* force, double* torque, unsigned int*
     if (contacts) DEM_CUDA_TRY(cudaMemcpyAsync(contacts, c->dbgC, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (c->ordered) {   // into the caller's order
+        const int rc = host_perm(c);
+        if (rc) return rc;
         const std::vector<uint>& pm = c->hperm;
         for (double* a : {force, torque}) {
             if (!a) continue;
@@ -2282,6 +2372,8 @@ int dem_download_pairs(dem_ctx* c, unsigned int* lp, unsigned int* ln, double* h
     cudaFree(dh);
     if (e != cudaSuccess) return cuda_fail(e, "dem_download_pairs", __FILE__, __LINE__);
     if (c->ordered) {
+        const int rp = host_perm(c);
+        if (rp) return rp;
         // in the caller's particle ids: each pair (lower id, higher id), the
         // history in that pair's orientation (it changes sign when the two
         // swap roles), sorted by (lower, higher)
@@ -2335,6 +2427,8 @@ int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsign
     }
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (remap) {   // the caller's ids, ascending inside each cell
+        const int rp = host_perm(c);
+        if (rp) return rp;
         for (long long t = 0; t < n; t++) ids[t] = c->hperm[ids[t]];
         for (long long cc = 0; cc < nc; cc++)
             if (cs[cc + 1] - cs[cc] > 1) std::sort(ids + cs[cc], ids + cs[cc + 1]);
@@ -2409,6 +2503,25 @@ int dem_check_barrier_timeout(dem_ctx* c, double* waited_ms) {
     *waited_ms = (double)ns * 1e-6;
     if (!(w.status & kStBarrier))
         return fail(DEM_ERR_STATE, "dem_check_barrier_timeout: the wait did not report its timeout");
+    return DEM_OK;
+}
+
+int dem_window_work(dem_ctx* c, long long* bound, long long* wall_candidates, long long* pairs) {
+    if (!c) return fail(DEM_ERR_ARG, "dem_window_work: null ctx");
+    if (bound) *bound = 0;
+    if (wall_candidates) *wall_candidates = 0;
+    if (pairs) *pairs = 0;
+    if (!c->uploaded || c->relists == 0) return DEM_OK;
+    uint v[3] = {0, 0, 0};
+    uint* hp = (uint*)c->host_pinned;
+    DEM_CUDA_TRY(cudaMemcpyAsync(hp, c->bpos + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaMemcpyAsync(hp + 1, c->wcount, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaMemcpyAsync(hp + 2, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    memcpy(v, hp, sizeof(v));
+    if (bound) *bound = v[0];
+    if (wall_candidates) *wall_candidates = v[1];
+    if (pairs) *pairs = (long long)v[2] <= c->cap ? v[2] : 0;
     return DEM_OK;
 }
 
@@ -2538,6 +2651,7 @@ int dem_save_state(dem_ctx* c, const char* path) {
     hd.pour_nplayer = c->pour_nplayer;
     hd.pour_tnewpar = c->pour_tnewpar;
     hd.ordered = c->ordered ? 1 : 0;
+    if (c->ordered && (rc = host_perm(c))) return rc;
     FILE* f = fopen(path, "wb");
     if (!f) return fail(DEM_ERR_IO, "Cannot open file %s", path);
     rc = write_all(f, &hd, sizeof(hd));

@@ -136,7 +136,9 @@ struct dem_ctx {
     bool reorder = true;                   // host uploads sort by cell (DEM_B200_REORDER=0: off)
     bool ordered = false;
     uint* perm = nullptr;                  // device copy (npad)
-    std::vector<uint> hperm;               // host copy (n)
+    std::vector<uint> hperm;               // host copy (n), fetched on first use after an upload
+    bool hperm_stale = false;              // the device copy is newer than hperm
+    cudaEvent_t h2d_done = nullptr;        // a host upload's copies have read the caller's buffers
     int device = 0;
     cudaStream_t stream = 0;
     cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one
@@ -180,6 +182,7 @@ struct dem_ctx {
     uint* bar = nullptr;             // window-kernel grid barrier: [0] arrival counter
     unsigned win_grid = 1;           // window-kernel blocks (all co-resident)
     bool win_kernel = true;          // whole PCCP windows as one cooperative launch
+    int win_split = 1;               // window kernels: bound items per thread of the bound blocks (0: no split)
     int wtiming_path = 0;            // last timed window: 0 per-step, 1 window kernel, 2 per-step + forked free
     uint* off[2] = {nullptr, nullptr};
     uint* roff = nullptr;
@@ -250,6 +253,9 @@ namespace dem {
 int relist(dem_ctx* c, int src);
 int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part);
 int window_kernel(dem_ctx* c, int lst, const WindowTape* tape);
+// The host copy of the particle order (c->hperm), fetched from the device
+// (one copy and a stream wait) when an upload computed a new one.
+int host_perm(dem_ctx* c);
 template <typename Real> Planes3<Real> planes(void* base, long long npad) {
     Real* b = (Real*)base;
     return Planes3<Real>{b, b + npad, b + 2 * npad};

@@ -17,6 +17,11 @@ damping, normal and tangential), flat frictional walls, gravity -z, skin
                  5,000 steps, mu = 0.5, mu_r = 0.005 R*.  Mixed precision.
   settle_50k     50,000 lognormal (as rsa_500k) in 40x40x150 mm, dt = 5e-7 s,
                  pre-settled 20,000 steps, then a 2,000-step window.
+  bed_500k       the rsa_500k spheres as a settled bed (every sphere in
+                 contact): RSA largest first at solid fraction 0.32 in a
+                 100x100 mm base, compacted by a downward velocity
+                 proportional to height and gravity (dense_bed()), then
+                 stepped as rsa_500k.
   pour_box       a poured packing (the reference's layer injection) at test
                  size: 108 spheres r = 0.5 mm in 8x8 mm, 3 layers of 36 on a
                  6x6 injection lattice 3 mm above the floor, initial speed 1.5
@@ -158,3 +163,52 @@ def pour_box(seed=SEED, nx=6, ny=6, layers=3, box=(8.0, 8.0, 12.0), z_inject=3.0
                  meta={"pdis": pdis.reshape(-1), "nplayer": nx * ny, "tnewpar": layer_steps * dt,
                        "init": f"poured: {nx}x{ny} injection lattice, a layer every {layer_steps:g} steps"})
     return w
+
+
+def bed_500k_initial(seed=SEED, precision=PREC_MIXED, n=500_000, base=(100.0, 100.0), phi0=0.32, phi_bed=0.58,
+                     compact_s=0.0125):
+    """Initial state of the settled 500,000-sphere bed: the rsa_500k radii
+    placed by random sequential addition largest first (which reaches solid
+    fraction phi0 = 0.32; in random order RSA stops near 0.25) in a
+    base[0] x base[1] box of height V / (phi0 A), with a downward velocity
+    proportional to height, z (1 - phi0/phi_bed) / compact_s, so that the
+    column closes to about phi_bed in compact_s seconds with gentle
+    neighbour impacts (relative speeds ~ gap x 46/s).  meta["pdis"]: the
+    per-step displacement (velocity x dt) of that motion at dt = 5e-7 s."""
+    rad = gen_radii(n, RADII_LOGNORMAL, 0.5, 0.2, 0.3, 0.8, seed)
+    V = float(np.sum(4.0 / 3.0 * np.pi * rad ** 3))
+    H = V / (phi0 * base[0] * base[1])
+    order = np.argsort(-rad, kind="stable")
+    ps = gen_rsa((base[0], base[1], H), rad[order], seed + 1).reshape(-1, 3)
+    pos = np.empty_like(ps)
+    pos[order] = ps
+    dt = reduced_dt(5e-7)
+    vz = -pos[:, 2] * (1.0 - phi0 / phi_bed) / (compact_s / TAU)     # reduced velocity
+    pdis = np.zeros_like(pos)
+    pdis[:, 2] = vz * dt
+    pp, pw = material(mu=0.3, roll_rel=0.002)
+    world = (base[0], base[1], float(np.ceil(H + 5.0)))
+    return Workload("bed_500k", n, pos.reshape(-1).copy(), rad, world, dt, 10000, 20, 0.05, precision, pp, pw,
+                    meta={"init": f"RSA largest first at phi {phi0} in {base[0]:g}x{base[1]:g}x{H:.1f} mm, "
+                                  f"compacted in {compact_s * 1e3:g} ms then settled",
+                          "pdis": pdis.reshape(-1).copy(), "compact_steps": int(round(compact_s / 5e-7))})
+
+
+def dense_bed(dem, w, settle_steps, relist=10, stream=None):
+    """Settles bed_500k_initial's column on the GPU (mixed precision, re-list
+    every `relist` steps so that the fastest spheres stay inside the skin
+    guard), and returns the bed as a Workload at the production cadence
+    (re-list every 20 steps) with its state: pos, and pdis/angv in meta."""
+    e = dem.Engine(**{**w.engine_kwargs(), "precision": PREC_MIXED, "relist_interval": relist})
+    if stream is not None:
+        e.set_stream(stream)
+    e.set_material(w.pp, w.pw)
+    e.upload(w.pos, w.rad, w.meta["pdis"], None)
+    e.step(settle_steps)
+    s = e.scalars()
+    pos, pdis, angv = e.download()
+    e.close()
+    meta = dict(w.meta)
+    meta.update(pdis=pdis, angv=angv, settle_steps=settle_steps, settled=s)
+    return Workload(w.name, w.n, pos, w.rad, w.world, w.dt, w.steps, 20, w.skin, w.precision, w.pp, w.pw,
+                    meta=meta)

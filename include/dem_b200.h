@@ -316,6 +316,12 @@ int dem_kernel_times(dem_ctx* ctx, double out[3]);
 int dem_check_barrier_timeout(dem_ctx* ctx, double* waited_ms);
 int dem_set_window_timing(dem_ctx* ctx, int on);
 int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
+/* Work of the current list's window (waits for the context's stream):
+ * *bound = particles with a listed pair or a wall candidacy (stepped with the
+ * pair phase), *wall_candidates = particles near a wall, *pairs = listed
+ * pairs; the others step under gravity alone until the next re-list.  No
+ * counterpart in the reference (it steps every particle the same way). */
+int dem_window_work(dem_ctx* ctx, long long* bound, long long* wall_candidates, long long* pairs);
 
 /* Checkpoint / resume (the reference's restart reader is commented out,
  * dempacking.cu:361-367, and its preflow.dat has no contact history).

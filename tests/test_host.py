@@ -201,3 +201,25 @@ def test_preflow_reader_round_trip(dem, tmp_path):
     with pytest.raises(dem.DemError) as e:
         dem.read_preflow(bad)
     assert e.value.code == dem.DEM_ERR_IO
+
+
+def test_host_only_generators_match_and_leave_the_gpu_library_unloaded(dem, tmp_path):
+    """The workloads generate their initial states with libdem_gen.so (the
+    generators' source built host only): bit for bit the library's own
+    generators, and a process that only generates a workload (the CPU timing
+    of the reference step) never maps libdem_b200.so."""
+    import subprocess
+    import sys
+    from dem_b200 import gen
+    rad_g = gen.gen_radii(5000, dem.RADII_LOGNORMAL, 0.5, 0.2, 0.3, 0.8, seed=11)
+    np.testing.assert_array_equal(rad_g, dem.gen_radii(5000, dem.RADII_LOGNORMAL, 0.5, 0.2, 0.3, 0.8, seed=11))
+    np.testing.assert_array_equal(gen.gen_rsa((30.0, 30.0, 30.0), rad_g, 12),
+                                  dem.gen_rsa((30.0, 30.0, 30.0), rad_g, 12))
+    assert gen.estar(1e7, 0.29, 2500.0, 1e-3) == dem.estar(1e7, 0.29, 2500.0, 1e-3)
+    code = ("import sys, pathlib; sys.path.insert(0, 'tests'); from _load import load_pkg; dem = load_pkg(); "
+            "import dem_b200.workloads as wl; w = wl.rsa_500k(n=3000, box=(30.0, 30.0, 60.0)); "
+            "maps = pathlib.Path('/proc/self/maps').read_text(); "
+            "print('gpu-lib' if 'libdem_b200.so' in maps else 'host-only', dem._LIB is None)")
+    root = __import__("pathlib").Path(__file__).resolve().parents[1]
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, check=True).stdout
+    assert out.split() == ["host-only", "True"], out

@@ -24,6 +24,7 @@
 //                     back to the carried pairs of the previous list
 // The reverse runs in FP64 on the recorded FP64/FP32 trajectory.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 #include "dem_engine_internal.h"
@@ -34,6 +35,8 @@ namespace dem {
 namespace {
 constexpr int kB = 256;
 constexpr int kPairB = 32;    // block size of k_adj_step; pbar holds one 12-slot row per block
+constexpr int kAB = 128;      // block size of k_adj_pairs and k_adj_bound
+constexpr int kPC = 20;       // doubles per pair of the two-phase reverse step's shares
 constexpr long long kScatterPrime = 2654435761ll;
 
 struct Ck {
@@ -69,7 +72,11 @@ struct AdjWork {
     double* Ab2[2] = {nullptr, nullptr};
     double *Xb = nullptr, *Db = nullptr, *Ab = nullptr, *Wb = nullptr, *Rb = nullptr;
     double* Hb[2] = {nullptr, nullptr};
-    double* pbar = nullptr;      // npb x 12 (one row per k_adj_step block)
+    double* pbar = nullptr;      // npb x 12 (one row per reverse-step block: pair params 0-5, wall params 6-11)
+    double* PC = nullptr;        // kPC per pair slot: the shares a pair's reverse sends to lo and hi
+    uint* pon = nullptr;         // per pair slot: 1 if PC holds this step's shares
+    unsigned grid_pairs = 1, grid_bound = 1;   // blocks of k_adj_pairs / k_adj_bound
+    bool pair_parallel = true;   // two-phase reverse step (DEM_B200_ADJ=pp: k_adj_step)
     double* objp = nullptr;      // 3 per k_obj_potential block: energy, d/d estar (pair, wall)
     double* Pobj = nullptr;      // 3 np: the final positions for the objective
     long long npb = 0;
@@ -105,13 +112,19 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
             (rc = dalloc(&w->Ab2[0], 3 * np)) || (rc = dalloc(&w->Xb2[1], 3 * np)) ||
             (rc = dalloc(&w->Db2[1], 3 * np)) || (rc = dalloc(&w->Ab2[1], 3 * np)) || (rc = dalloc(&w->Wb, 3 * np)) ||
             (rc = dalloc(&w->Rb, np)) || (rc = dalloc(&w->Hb[0], 3 * cap)) || (rc = dalloc(&w->Hb[1], 3 * cap)) ||
-            (rc = dalloc(&w->pbar, (size_t)grid_for(c->n, kPairB) * 12)) || (rc = dalloc(&w->obj, 16)) ||
+            (rc = dalloc(&w->obj, 16)) ||
             (rc = dalloc(&w->objp, 3 * (size_t)grid_for(c->n, kB))) ||
             (rc = dalloc(&w->zmax, 2)) ||
             (rc = dalloc(&w->save_mz, c->npart)) || (rc = dalloc(&w->save_cnt, c->npart)) ||
             (rc = dalloc(&w->Pobj, 3 * np)))
             return rc;
-        w->npb = grid_for(c->n, kPairB);
+        const char* ap = getenv("DEM_B200_ADJ");   // "pp": the particle-parallel reverse step
+        w->pair_parallel = !(ap && ap[0] == 'p');
+        w->grid_pairs = std::min<unsigned>(grid_for(cap, kAB), 2048u);
+        w->grid_bound = grid_for(c->n, kAB);
+        w->npb = std::max<long long>(grid_for(c->n, kPairB), std::max(w->grid_pairs, w->grid_bound));
+        if ((rc = dalloc(&w->pbar, (size_t)w->npb * 12))) return rc;
+        if (w->pair_parallel && ((rc = dalloc(&w->PC, (size_t)kPC * cap)) || (rc = dalloc(&w->pon, cap)))) return rc;
         w->Xb = w->Xb2[0];
         w->Db = w->Db2[0];
         w->Ab = w->Ab2[0];
@@ -429,6 +442,161 @@ __global__ void __launch_bounds__(kPairB) k_adj_step(
     }
 }
 
+// One reversed step of the bound particles in two pair-parallel phases (the
+// default; k_adj_step above is the particle-parallel form, DEM_B200_ADJ=pp).
+//
+// Phase A (k_adj_pairs), one thread per listed pair (lo, hi): the pair law is
+// evaluated forward from the tape and reversed once, with the force adjoint
+// of each side taken from the after-step state adjoints (the first half of
+// the integrator reverse); the pair's input-history adjoint goes to Hin, its
+// parameter adjoints into this block's row of pbar (slots 0-5), and the
+// adjoints it sends to lo and hi into PC (kPC doubles per pair: lo's x, d, a
+// and radius, then hi's), with pon[k] = 1.  A pair whose two spheres had no
+// pair contact in the forward step (taped count 0 on either side) only clears
+// its history adjoint.  Phase B (k_adj_bound), one thread per bound particle:
+// the integrator reverse, the sum of its pairs' shares (own row, then reverse
+// row, in list order: deterministic), the walls (parameter adjoints into
+// slots 6-11 of its block's row), and the state adjoints before the step.
+// The chain of one thread is one pair's law instead of all of a sphere's
+// pairs twice over; no atomics.
+__device__ __forceinline__ void block_sum6(const double v[6], double* row) {
+    __shared__ double sp[6][kAB / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sp[k][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double x = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) x += sp[threadIdx.x][w];
+        row[threadIdx.x] += x;
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kAB) k_adj_pairs(
+    long long n, long long np, long long cap, AdjList L, const double* __restrict__ tx, const double* __restrict__ td,
+    const Real* __restrict__ ta, const double* __restrict__ th, const uint* __restrict__ tc, const Real* __restrict__ R,
+    LawParams<double> pp, double dt, double density, const double* __restrict__ Hout, double* __restrict__ Hin,
+    const double* __restrict__ Xa, const double* __restrict__ Da, const double* __restrict__ Aa,
+    double* __restrict__ PC, uint* __restrict__ pon, double* __restrict__ pbar) {
+    const double inv_dt = 1.0 / dt;
+    LawBar bp;
+    lawbar_zero(bp);
+    // the list and the tape (the recompute's) may be read before the wait;
+    // the state and history adjoints are the predecessors'
+    const uint total = L.off[n];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    pdl_wait();
+    pdl_trigger();
+    if ((long long)total <= cap) {
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total; k += stride) {
+            const uint lo = L.lp[k], hi = L.ln[k];
+            bool on = tc[lo] != 0 && tc[hi] != 0;
+            PairTape t;
+            if (on) {
+                const V3d hin = mk(th[k], th[cap + k], th[2 * cap + k]);
+                V3d Fi, Ti, Tj, ho;
+                on = pair_fwd(ld3(tx, np, lo), ld3(tx, np, hi), ld3(td, np, lo), ld3(td, np, hi), ldA<Real>(ta, np, lo),
+                              ldA<Real>(ta, np, hi), (double)R[lo], (double)R[hi], hin, pp, inv_dt, density, t, Fi,
+                              Ti, Tj, ho) != 0;
+            }
+            if (!on) {
+                Hin[k] = 0.0; Hin[cap + k] = 0.0; Hin[2 * cap + k] = 0.0;
+                pon[k] = 0u;
+                continue;
+            }
+            V3d fbl, tbl, fbh, tbh;
+            partner_fb<Real>(R[lo], np, lo, dt, density, Xa, Da, Aa, fbl, tbl);
+            partner_fb<Real>(R[hi], np, hi, dt, density, Xa, Da, Aa, fbh, tbh);
+            V3d xl = zero3<double>(), xh = zero3<double>(), dl = zero3<double>(), dh = zero3<double>(),
+                al = zero3<double>(), ah = zero3<double>(), hinb = zero3<double>();
+            double rl = 0.0, rh = 0.0;
+            pair_rev(t, pp, inv_dt, density, fbl - fbh, tbl, tbh, mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]), xl, xh,
+                     dl, dh, al, ah, rl, rh, hinb, bp);
+            Hin[k] = hinb.x; Hin[cap + k] = hinb.y; Hin[2 * cap + k] = hinb.z;
+            double* c = PC + (size_t)kPC * k;
+            c[0] = xl.x; c[1] = xl.y; c[2] = xl.z; c[3] = dl.x; c[4] = dl.y; c[5] = dl.z;
+            c[6] = al.x; c[7] = al.y; c[8] = al.z; c[9] = rl;
+            c[10] = xh.x; c[11] = xh.y; c[12] = xh.z; c[13] = dh.x; c[14] = dh.y; c[15] = dh.z;
+            c[16] = ah.x; c[17] = ah.y; c[18] = ah.z; c[19] = rh;
+            pon[k] = 1u;
+        }
+    }
+    const double v[6] = {bp.estar, bp.mu, bp.cn, bp.ct, bp.roll, bp.roll_rel};
+    block_sum6(v, pbar + (size_t)blockIdx.x * 12);
+}
+
+__device__ __forceinline__ void add_share(const double* __restrict__ c, V3d& xb, V3d& db, V3d& ab, double& rb) {
+    xb += mk(c[0], c[1], c[2]);
+    db += mk(c[3], c[4], c[5]);
+    ab += mk(c[6], c[7], c[8]);
+    rb += c[9];
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kAB) k_adj_bound(
+    long long n, long long np, long long cap, AdjList L, const uint* __restrict__ blist, const uint* __restrict__ nbp,
+    const double* __restrict__ tx, const double* __restrict__ td, const Real* __restrict__ ta,
+    const double* __restrict__ twh, const double* __restrict__ tF, const double* __restrict__ tT,
+    const Real* __restrict__ R, LawParams<double> pw, double dt, double density, double hx, double hy,
+    const double* __restrict__ PC, const uint* __restrict__ pon, const double* __restrict__ Xa,
+    const double* __restrict__ Da, const double* __restrict__ Aa, double* __restrict__ Xo, double* __restrict__ Do,
+    double* __restrict__ Ao, double* __restrict__ Wb, double* __restrict__ Rb, double* __restrict__ pbar) {
+    const double inv_dt = 1.0 / dt;
+    LawBar bw;
+    lawbar_zero(bw);
+    const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nb = (long long)*nbp;
+    // before the wait: the list and the tape of the particle
+    long long i = 0;
+    Real rr = (Real)0;
+    V3d xi = zero3<double>(), di = zero3<double>(), ai = zero3<double>(), fi = zero3<double>(), ti = zero3<double>(),
+        hw = zero3<double>();
+    uint total = 0, o0 = 0, o1 = 0, q0 = 0, q1 = 0;
+    if (u < nb) {
+        i = blist[u];
+        rr = R[i];
+        xi = ld3(tx, np, i); di = ld3(td, np, i); ai = ldA<Real>(ta, np, i);
+        fi = mk(tF[3 * i], tF[3 * i + 1], tF[3 * i + 2]);
+        ti = mk(tT[3 * i], tT[3 * i + 1], tT[3 * i + 2]);
+        hw = ld3(twh, np, i);
+        total = L.off[n];
+        o0 = L.off[i]; o1 = L.off[i + 1]; q0 = L.roff[i]; q1 = L.roff[i + 1];
+    }
+    pdl_wait();
+    pdl_trigger();
+    if (u < nb) {
+        const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
+        V3d dtot, fbi, tbi;
+        double rb = 0.0;
+        integ_rev<Real>(rr, fi, ti, dt, density, xa, ld3(Da, np, i), aa, dtot, fbi, tbi, rb);
+        V3d xb = zero3<double>(), dbv = zero3<double>(), ab = zero3<double>();
+        if ((long long)total <= cap) {
+            for (uint k = o0; k < o1; k++)
+                if (pon[k]) add_share(PC + (size_t)kPC * k, xb, dbv, ab, rb);
+            for (uint q = q0; q < q1; q++) {
+                const uint k = L.rk[q];
+                if (k < total && pon[k]) add_share(PC + (size_t)kPC * k + 10, xb, dbv, ab, rb);
+            }
+        }
+        V3d hwb = zero3<double>();
+        wall_vjp(hx, hy, xi, di, ai, (double)rr, density, hw, pw, inv_dt, fbi, tbi, ld3(Wb, np, i), xb, dbv, ab, rb,
+                 hwb, bw);
+        st3(Wb, np, i, hwb);
+        st3(Xo, np, i, xa + xb);
+        st3(Do, np, i, dtot + dbv);
+        st3(Ao, np, i, aa + ab);
+        Rb[i] += rb;
+    }
+    const double v[6] = {bw.estar, bw.mu, bw.cn, bw.ct, bw.roll, bw.roll_rel};
+    block_sum6(v, pbar + (size_t)blockIdx.x * 12 + 6);
+}
+
 // History adjoint across a re-list: new pair k carried old pair carry[k].
 __global__ void k_adj_carry(const uint* __restrict__ off, long long n, long long cap, const uint* __restrict__ carry,
                             const double* __restrict__ Hnew, double* __restrict__ Hold) {
@@ -592,6 +760,27 @@ template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l,
     AdjWork* w = c->adj;
     const long long np = c->npad, cap = c->cap;
     AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
+    if (w->pair_parallel) {
+        // both phases programmatic: each waits for its predecessor before it
+        // reads an adjoint (tape and list loads overlap the predecessor's tail)
+        const bool pdl = c->pdl;
+        const double* tx = w->tx + 3 * np * t;
+        const double* td = w->td + 3 * np * t;
+        const Real* ta = (const Real*)w->ta + 3 * np * t;
+        DEM_CUDA_TRY(launch_ex(k_adj_pairs<Real>, w->grid_pairs, kAB, c->stream, pdl, c->n, np, cap, L, tx, td, ta,
+                               (const double*)w->th + 3 * cap * t, (const uint*)w->tc + np * t, (const Real*)c->rad,
+                               make_law<double>(c->mat.pp), c->cfg.dt, c->cfg.density, (const double*)w->Hb[hb],
+                               w->Hb[1 - hb], (const double*)w->Xb2[in], (const double*)w->Db2[in],
+                               (const double*)w->Ab2[in], w->PC, w->pon, w->pbar));
+        DEM_CUDA_TRY(launch_ex(k_adj_bound<Real>, w->grid_bound, kAB, c->stream, pdl, c->n, np, cap, L, l.blist, l.nb,
+                               tx, td, ta, (const double*)w->twh + 3 * np * t, (const double*)w->tF + 3 * np * t,
+                               (const double*)w->tT + 3 * np * t, (const Real*)c->rad, make_law<double>(c->mat.pw),
+                               c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
+                               (const double*)w->PC, (const uint*)w->pon, (const double*)w->Xb2[in],
+                               (const double*)w->Db2[in], (const double*)w->Ab2[in], w->Xb2[1 - in], w->Db2[1 - in],
+                               w->Ab2[1 - in], w->Wb, w->Rb, w->pbar));
+        return DEM_OK;
+    }
     // a reversed step that directly follows another is launched programmatic
     // (its tape loads overlap the predecessor's tail); the first step of a
     // window follows the free-particle kernel and is launched plainly
@@ -779,9 +968,12 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     // ---------------------------------------------------- forward + checkpoints
     DEM_CUDA_TRY(cudaEventRecord(c->ev[0], s));
     const long long step0 = c->step, relists0 = c->relists;
-    for (long long g = 0; g < nseg; g++) {
-        if ((rc = save_ck(c, w->ck[g]))) return rc;
-        if ((rc = dem_step_n(c, every))) return rc;
+    {
+        NvtxRange fwd_range("dem adjoint forward");
+        for (long long g = 0; g < nseg; g++) {
+            if ((rc = save_ck(c, w->ck[g]))) return rc;
+            if ((rc = dem_step_n(c, every))) return rc;
+        }
     }
     if ((rc = save_ck(c, w->ck[nseg]))) return rc;
     const size_t last = (size_t)(K - 1) * c->npart;
@@ -810,6 +1002,7 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     SegmentGraphs fgraph, rgraph;
     for (long long g = nseg - 1; g >= 0; g--) {
         if ((rc = restore_ck(c, w->ck[g]))) return rc;
+        NvtxRange seg_range("dem adjoint segment (recompute + reverse)");
         // recompute the segment, recording what the reverse sweep needs
         if (win_path) {
             // one graph per list-buffer parity at the segment start (the
@@ -929,7 +1122,7 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     for (Ck& k : w->ck) free_ck(k);
     void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->tc, w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1],
                  w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj,
-                 w->objp};
+                 w->objp, w->PC, w->pon};
     for (void* x : p)
         if (x) cudaFree(x);
     for (ListRec& l : w->lists) {

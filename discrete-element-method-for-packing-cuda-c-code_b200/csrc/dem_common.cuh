@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cmath>
+#include <nvtx3/nvToolsExt.h>
 #include "dem_b200.h"
 
 #define DEM_HD __host__ __device__ __forceinline__
@@ -51,6 +52,16 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
         if (e_ != cudaSuccess) return ::dem::cuda_fail(e_, #call, __FILE__, __LINE__); \
     } while (0)
 #define DEM_LAUNCH_CHECK() DEM_CUDA_TRY(cudaGetLastError())
+
+// NVTX range over a host scope (re-list, window, upload, adjoint phases):
+// a profiler attached to the process shows where the host enqueues each
+// phase; without one the calls do nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 inline unsigned grid_for(long long n, int block) {
     long long g = (n + block - 1) / block;

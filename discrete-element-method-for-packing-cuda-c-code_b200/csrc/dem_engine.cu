@@ -1448,10 +1448,12 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
 
 namespace dem {
 int window_kernel(dem_ctx* c, int lst, const WindowTape* tape) {
+    NvtxRange r("dem window kernel");
     return c->prec == DEM_PREC_MIXED ? launch_window<float>(c, lst, tape) : launch_window<double>(c, lst, tape);
 }
 
 int relist(dem_ctx* c, int src) {
+    NvtxRange r("dem re-list");
     return c->prec == DEM_PREC_MIXED ? launch_relist<float>(c, src) : launch_relist<double>(c, src);
 }
 
@@ -1555,6 +1557,7 @@ int enqueue_window(dem_ctx* c, int src) {
 
 // Capture (once) and launch the window graph for the current buffers.
 int launch_window_graph(dem_ctx* c) {
+    NvtxRange r("dem window graph");
     const int src = c->cur, sb = c->sbuf, hp = c->hph;
     const int tm = c->wtiming ? 1 : 0;
     cudaGraphExec_t& ge = c->gexec[src][sb][hp][tm];
@@ -2025,6 +2028,7 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
 }
 
 int dem_upload_state(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
+    NvtxRange r("dem upload");
     return upload_impl(c, pos, pdis, angv, rad, true, kOrderCells, nullptr);
 }
 int dem_upload_state_device(dem_ctx* c, const double* pos, const double* pdis, const double* angv, const double* rad) {
@@ -2061,6 +2065,7 @@ static int download_common(dem_ctx* c, double* pos, double* pdis, double* angv, 
 }
 
 int dem_download_state(dem_ctx* c, double* pos, double* pdis, double* angv) {
+    NvtxRange r("dem download");
     return download_common(c, pos, pdis, angv, true);
 }
 int dem_download_state_device(dem_ctx* c, double* pos, double* pdis, double* angv) {
@@ -2068,6 +2073,7 @@ int dem_download_state_device(dem_ctx* c, double* pos, double* pdis, double* ang
 }
 
 int dem_step_n(dem_ctx* c, long long nsteps) {
+    NvtxRange r("dem_step_n");
     if (!c) return fail(DEM_ERR_ARG, "dem_step_n: null ctx");
     if (!c->uploaded) return fail(DEM_ERR_STATE, "dem_step_n: no state uploaded");
     if (!c->have_mat) return fail(DEM_ERR_STATE, "dem_step_n: material not set");

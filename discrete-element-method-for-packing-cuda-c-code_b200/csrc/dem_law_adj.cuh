@@ -329,6 +329,7 @@ DEM_HD int wall_fwd(double hx, double hy, V3d x, V3d d, V3d a, double r, double 
     F = T = h_out = zero3<double>();
     if (prim < 0) return 0;
     const double m = density * 8.0 * r * r * r;
+#pragma unroll 1
     for (int w = 0; w < 5; w++) {
         if (!(dl[w] > 0.0)) continue;
         const V3d n = wall_normal(w);
@@ -354,6 +355,10 @@ DEM_HD int wall_vjp(double hx, double hy, V3d x, V3d d, V3d a, double r, double 
     const int prim = wall_prim(hx, hy, x, r, dl);
     if (prim < 0) return 0;
     const double m = density * 8.0 * r * r * r;
+    // one copy of the law's forward and reverse for all five walls (touching
+    // a wall is the rare path; unrolled, the copies would crowd out the
+    // registers of the rest of the reverse step)
+#pragma unroll 1
     for (int w = 0; w < 5; w++) {
         if (!(dl[w] > 0.0)) continue;
         const V3d n = wall_normal(w);

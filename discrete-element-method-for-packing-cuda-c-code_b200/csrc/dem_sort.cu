@@ -124,8 +124,10 @@ extern "C" int RadixSort(KeyValuePair* pData0, KeyValuePair* pData1, unsigned in
 //
 // The first call on a device resolves the array's device address with
 // cudaGetSymbolAddress while that device is current (host code cannot use the
-// symbol itself: on the host it names a stand-in, not device memory); make
-// that first call before any stream capture.  All calls share the one array,
+// symbol itself: on the host it names a stand-in, not device memory).  Under
+// CUDA's lazy module loading that call may be the one that loads this
+// library's device code, which reserves device memory: make the first call
+// during set-up, before any stream capture; later calls allocate nothing.  All calls share the one array,
 // which keeps the contents of the last call: every histogram word is written
 // before it is read, so nothing needs clearing, but two calls that overlap on
 // the GPU (different streams, or different host threads on the same device)

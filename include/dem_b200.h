@@ -98,8 +98,11 @@ int RadixSort(KeyValuePair* pData0, KeyValuePair* pData1,
  * library instead of cudaMalloc'd memory.  At most 4,194,304 records (larger
  * requests return DEM_ERR_ARG); the array (about 2 MiB) is held on every GPU
  * that loads the library until exit.  The first call on each device sets up
- * the array's address (make it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race and must be serialised. */
+ * the array's address, which may also load the library's device code (and
+ * with it reserve device memory) under CUDA's lazy module loading: make that
+ * first call during set-up, before any stream capture; later calls allocate
+ * nothing.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised. */
 int RadixSortNoAlloc(KeyValuePair* pData0, KeyValuePair* pData1,
                      unsigned int elements, unsigned int keybits);
 

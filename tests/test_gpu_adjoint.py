@@ -301,3 +301,30 @@ def test_autograd_function_matches_finite_differences(dem, wl, cuda):
     g_fd = (window_value(s, **p0, rad=w.rad + hr * v) - window_value(s, **p0, rad=w.rad - hr * v)) / (2 * hr)
     g_ad = float(g[4].numpy() @ v)
     assert abs(g_ad - g_fd) <= 1e-3 * abs(g_fd), (g_ad, g_fd)
+
+
+@pytest.mark.parametrize("which", ["dense", "sparse"])
+def test_pair_parallel_and_particle_parallel_reverse_agree(dem, cuda, monkeypatch, which):
+    """The reverse step in its two pair-parallel phases (the default: one
+    thread per pair's law, then one per bound sphere gathering the shares)
+    and in its particle-parallel form (DEM_B200_ADJ=pp: each sphere reverses
+    all its pairs) compute the same adjoint with the additions in another
+    order: objective equal, gradients within 1e-9 relative (plus 1e-12 of
+    the objective for gradients near zero)."""
+    w, pdis, angv = case(dem) if which == "dense" else sparse_case(dem)
+    out = []
+    for flag in ("pairs", "pp"):
+        monkeypatch.setenv("DEM_B200_ADJ", flag)
+        e = dem.Engine(**{**w.engine_kwargs(), "precision": dem.PREC_FP64, "cell": w.cell() + 0.01})
+        e.set_material(w.pp, w.pw)
+        e.upload(w.pos, w.rad, pdis, angv)
+        out.append(e.adjoint(STEPS, EVERY, dem.OBJ_POTENTIAL))
+        assert e.scalars()["status"] == 0
+        e.close()
+    a, b = out
+    assert a["value"] == b["value"]
+    floor = 1e-12 * abs(a["value"])
+    for side in ("d_pp", "d_pw"):
+        for k, x in a[side].items():
+            assert abs(x - b[side][k]) <= 1e-9 * abs(x) + floor, (side, k, x, b[side][k])
+    np.testing.assert_allclose(a["d_radii"], b["d_radii"], rtol=1e-9, atol=1e-12 * np.abs(a["d_radii"]).max())

@@ -40,6 +40,31 @@ def test_no_alloc_sort_matches_allocating_sort_on_two_calls(dem, cuda):
         assert np.all(np.diff(got[0::2].astype(np.int64)) >= 0)
 
 
+def test_no_alloc_sort_at_its_limit_is_the_stable_order_and_allocates_nothing(dem, cuda):
+    """Exactly 4,194,304 records (the fixed array at its fullest), twice: the
+    result is numpy's stable order of the keys, and the second call leaves
+    the device's free memory unchanged (the first may load the library's
+    device code, which is why a caller makes it during set-up)."""
+    torch = cuda
+    n, bits = 1 << 22, 24
+    kv = _keys(n, bits, 21)
+    order = np.argsort(kv[0::2], kind="stable")
+    want = np.empty_like(kv)
+    want[0::2], want[1::2] = kv[0::2][order], kv[1::2][order]
+    d0 = torch.from_numpy(kv.view(np.int32).copy()).cuda()
+    d1 = torch.zeros_like(d0)
+    dem.compat.RadixSortNoAlloc(d0, d1, n, bits)          # set-up call
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d0.cpu().numpy().view(np.uint32), want)
+    d0.copy_(torch.from_numpy(kv.view(np.int32).copy()))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    dem.compat.RadixSortNoAlloc(d0, d1, n, bits)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    np.testing.assert_array_equal(d0.cpu().numpy().view(np.uint32), want)
+
+
 def test_no_alloc_sort_rejects_sizes_above_its_limit(dem, cuda):
     with pytest.raises(dem.DemError) as ei:
         dem.compat.RadixSortNoAlloc(0, 0, (1 << 22) + 1, 32)

@@ -201,3 +201,101 @@ def test_deck_driver_pours_layers(dem, cuda, tmp_path):
     assert [(int(a[0]), int(a[1])) for a in rows] == [(1000, 98), (2000, 196), (3000, 294)]
     assert all(0.0 <= float(a[4]) < 1.0 for a in rows)
     assert (tmp_path / "particle.dat").exists() and (tmp_path / "jobfinished").exists()
+
+
+def _driver_injection(deck, seed=20261203):
+    """The deck driver's injection states (driver/dempacking.cpp, after
+    dempacking.cu:243-309): ntot spheres of radius 0.5 on the deck's
+    (W-3) x (T-3) injection lattice at hopzt - 5, speed vel0 at elevation
+    pi (u/3 + 1/3) below the horizontal and a uniform azimuth, u from
+    SplitMix64 seeded with `seed`; the same libm sin/cos as the driver."""
+    import math
+    n = deck.ntot
+    W, T, H = deck.world[0], deck.world[1], deck.world[2]
+    nx, ny = int(W) - 3, int(T) - 3
+    if not (0.5 * W > 1.99) or nx < 1 or ny < 1:
+        nx = ny = 1
+    ax, ay = W / nx, T / ny
+    mask = (1 << 64) - 1
+    state = [seed]
+
+    def urand():
+        state[0] = (state[0] + 0x9E3779B97F4A7C15) & mask
+        z = state[0]
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z ^= z >> 31
+        return float(z >> 11) * (1.0 / 9007199254740992.0)
+
+    pi = 4.0 * math.atan(1.0)
+    pos = np.zeros((n, 3))
+    pdis = np.zeros((n, 3))
+    nplayer = nx * ny
+    for i in range(n):
+        site = i % nplayer
+        ix, iy = site // ny, site % ny
+        pos[i, 0] = (ix + 0.5) * ax - 0.5 * W if nx > 1 else 0.0
+        pos[i, 1] = (iy + 0.5) * ay - 0.5 * T if ny > 1 else 0.0
+        pos[i, 2] = H - 5.0
+        ang = pi * (urand() * .33333 + .33333)
+        pdis[i, 2] = -deck.vel0 * math.sin(ang) * deck.dt
+        dxy = -deck.vel0 * math.cos(ang) * deck.dt
+        ang = 2.0 * pi * urand()
+        pdis[i, 0] = dxy * math.cos(ang)
+        pdis[i, 1] = dxy * math.sin(ang)
+    return pos.reshape(-1), pdis.reshape(-1), nplayer, (W, T, H)
+
+
+def _ppor_rows(path):
+    return [[float(x) for x in line.split()] for line in path.read_text().splitlines() if line.strip()]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_shipped_deck_through_the_driver_against_the_oracle(dem, orc, cuda, tmp_path, prec):
+    """The reference's own deck (hopp3d.inp: 10,000 spheres of 1 cm poured
+    in layers of 2,209 into a 50 x 50 (reduced) box from 55 diameters up,
+    40,000 steps) through the deck driver, its ppor.dat rows (particles in
+    the system, contacts, packing fraction, mean coordination number, max
+    height, every 1,000 steps) against the oracle's poured loop from the same
+    injection states.  FP64: the particle and contact counts exact, the
+    written values to their 6 decimals; mixed: the same particle counts, and
+    the final packing fraction within 1e-3 of the oracle's."""
+    import pathlib
+    import shutil
+    import subprocess
+    src = pathlib.Path(__file__).resolve().parent / "golden" / "hopp3d.inp"
+    shutil.copy(src, tmp_path / "hopp3d.inp")
+    deck = dem.read_deck(str(src))
+    exe = pathlib.Path(dem.__file__).resolve().parent / "dempacking"
+    r = subprocess.run([str(exe), "hopp3d.inp", "--precision", prec], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    rows = _ppor_rows(tmp_path / "ppor.dat")
+    assert [int(a[0]) for a in rows] == list(range(1000, deck.tstop + 1, 1000))
+    pos, pdis, nplayer, world = _driver_injection(deck)
+    rad = np.full(deck.ntot, 0.5)
+    pp, pw = dem.deck_material(deck)
+    o = orc.run_pour(pos, rad, world, deck.dt, 0.55, 1.55, 1.0, dem.material_array(pp, pw), prec == "mixed",
+                     deck.tstop, 20, nplayer, 0.5, 0, pdis=pdis)
+    assert o["status"] == 0
+    worst = {"phi": 0.0, "cn": 0.0, "maxhz": 0.0}
+    for a in rows:
+        it = int(a[0])
+        na = int(o["nact"][it - 1])
+        contacts = int(o["ncontacts"][it - 1])
+        mz = float(o["maxhz"][it - 1])
+        phi = na * (np.pi / 6.0) / (world[0] * world[1] * mz)
+        cn = 2.0 * contacts / na
+        assert int(a[1]) == na, (it, a[1], na)
+        worst["phi"] = max(worst["phi"], abs(a[4] - phi))
+        worst["cn"] = max(worst["cn"], abs(a[5] - cn))
+        worst["maxhz"] = max(worst["maxhz"], abs(a[6] - mz))
+        if prec == "fp64":
+            assert int(a[2]) == contacts, (it, a[2], contacts)
+            assert abs(a[4] - phi) <= 2e-6 and abs(a[5] - cn) <= 2e-6 and abs(a[6] - mz) <= 2e-6, (it, a, phi, cn, mz)
+    last = rows[-1]
+    phi_end = int(o["nact"][-1]) * (np.pi / 6.0) / (world[0] * world[1] * float(o["maxhz"][-1]))
+    print(f"\nshipped deck {prec}: final phi {last[4]:.6f} (oracle {phi_end:.6f}), CN {last[5]:.4f} "
+          f"(oracle {2.0 * o['ncontacts'][-1] / o['nact'][-1]:.4f}); worst over the rows {worst}")
+    assert int(last[1]) == deck.ntot
+    assert abs(last[4] - phi_end) <= 1e-3

@@ -646,8 +646,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--cpu-steps", type=int, default=1000)
-    ap.add_argument("--bed-settle-steps", type=int, default=10000,
-                    help="settling steps of the bed after its 25,000 compaction steps")
+    ap.add_argument("--bed-settle-steps", type=int, default=5000,
+                    help="steps of the bed after its 25,000 compaction steps, before its ten quenches")
     ap.add_argument("--bed-windows", type=int, default=10)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")

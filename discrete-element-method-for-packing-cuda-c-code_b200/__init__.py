@@ -168,7 +168,7 @@ _SIGS = [
     ("dem_set_window_timing", ctypes.c_int, [_vp, ctypes.c_int]),
     ("dem_window_kernel_times", ctypes.c_int, [_vp, _c_double_p]),
     ("dem_window_work", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
-                                       ctypes.POINTER(ctypes.c_longlong)]),
+                                       ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]),
     ("dem_adjoint_window", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(AdjointResult), _vp]),
     ("dem_adjoint_release", ctypes.c_int, [_vp]),
@@ -551,10 +551,12 @@ class Engine:
 
     def window_work(self):
         """Bound particles, wall candidates and listed pairs of the current
-        list's window (dem_window_work)."""
-        b, w, p = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
-        check(lib().dem_window_work(self._h, ctypes.byref(b), ctypes.byref(w), ctypes.byref(p)), "dem_window_work")
-        return {"bound": b.value, "wall_candidates": w.value, "pairs": p.value}
+        list's window, and whether its bound particles were stepped as cluster
+        batches (dem_window_work)."""
+        b, w, p, bt = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_int(0)
+        check(lib().dem_window_work(self._h, ctypes.byref(b), ctypes.byref(w), ctypes.byref(p), ctypes.byref(bt)),
+              "dem_window_work")
+        return {"bound": b.value, "wall_candidates": w.value, "pairs": p.value, "batched": bt.value}
 
     def window_kernel_times(self):
         out = (ctypes.c_double * 5)()

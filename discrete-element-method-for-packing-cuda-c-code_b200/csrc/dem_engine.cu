@@ -147,9 +147,14 @@ template <typename Real>
 __global__ void k_hash_count(long long n, const PRec<Real>* __restrict__ S, GridC g, uint* __restrict__ key,
                              uint* __restrict__ count, uint* __restrict__ arrival, const Real* __restrict__ R,
                              double hx, double hy, double half_skin, uint* __restrict__ wslot,
-                             uint* __restrict__ wlist, uint* __restrict__ wcount) {
+                             uint* __restrict__ wlist, uint* __restrict__ wcount, uint* __restrict__ cc_parent,
+                             uint* __restrict__ cc_zero, long long np) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (cc_parent) {   // the coming re-list's components start as singletons
+        cc_parent[i] = (uint)i;
+        cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u; cc_zero[3 * np + i] = 0u;
+    }
     const V3<double> p = ld_pos<false>(S + i);
     {
         const double x = p.x, y = p.y, z = p.z;
@@ -391,6 +396,140 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
     for (uint u = b; u < e; u++) ru[rk[u]] = u;
 }
 
+// ------------------------------------------------------- cluster batches
+// The window's interaction graph is the pair list: two spheres without a
+// listed pair cannot touch before the next re-list (the skin guard checks
+// it).  Its connected components are therefore independent for the whole
+// window.  The re-list finds them with a lock-free union-find over the pairs
+// (hooking the larger root under the smaller, the scheme of ECL-CC,
+// Jaiganesh & Burtscher 2018), groups the bound particles by component into
+// slots (component order by atomics: any order gives the same states, every
+// particle's sums keep their list order), and cuts the slots into batches of
+// whole components of about kBatchTarget particles that one block of k_batch
+// steps through the window in shared memory.  A batch above the block's
+// capacity (a bed of touching spheres is one component) sends the whole
+// window to the grid-barrier window kernel instead.
+constexpr uint kBatchTarget = 256;       // particles per batch (components are not split)
+constexpr int kBatchThreads = 256;
+template <typename Real> struct BatchCap;
+template <> struct BatchCap<float> { static constexpr uint P = 512, Q = 1024; };
+template <> struct BatchCap<double> { static constexpr uint P = 384, Q = 640; };
+
+// Root of x (parent[x] <= x everywhere; a root is its own parent), halving
+// the path on the way (plain stores touch only non-roots, the hooking CAS only
+// roots).
+__device__ __forceinline__ uint cc_find(uint* parent, uint x) {
+    uint cur = __ldcg(parent + x);
+    if (cur == x) return x;
+    uint prev = x, next;
+    while (cur > (next = __ldcg(parent + cur))) {
+        parent[prev] = next;
+        prev = cur;
+        cur = next;
+    }
+    return cur;
+}
+
+__global__ void k_cc_union(long long n, long long cap, const uint* __restrict__ off, const uint* __restrict__ lp,
+                           const uint* __restrict__ ln, uint* parent) {
+    pdl_wait();
+    pdl_trigger();
+    const uint total = off[n];
+    if ((long long)total > cap) return;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total;
+         k += (long long)gridDim.x * blockDim.x) {
+        uint ra = cc_find(parent, lp[k]), rb = cc_find(parent, ln[k]);
+        while (ra != rb) {
+            if (ra < rb) { const uint t = ra; ra = rb; rb = t; }
+            const uint old = atomicCAS(parent + ra, ra, rb);
+            if (old == ra) break;
+            ra = cc_find(parent, old);   // ra was hooked meanwhile: go on from its new root
+            rb = cc_find(parent, rb);
+        }
+    }
+}
+
+// Root of every bound particle (stored as its parent), component sizes and
+// pair counts (pairs counted by their lower particle).
+__global__ void k_cc_count(long long n, long long cap, const uint* __restrict__ blist, const uint* __restrict__ bpos,
+                           const uint* __restrict__ off, uint* parent, uint* __restrict__ size,
+                           uint* __restrict__ pairs, uint* __restrict__ ccw) {
+    pdl_wait();
+    pdl_trigger();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint total = off[n];
+    if (t == 0 && (long long)total > cap) atomicOr(ccw + 1, 1u);
+    if (t >= (long long)bpos[n]) return;
+    const uint i = blist[t];
+    const uint r = cc_find(parent, i);
+    parent[i] = r;
+    atomicAdd(size + r, 1u);
+    if ((long long)total <= cap) atomicAdd(pairs + r, off[i + 1] - off[i]);
+}
+
+// A slot range per component (roots only), marked at its first slot.
+__global__ void k_cc_base(long long n, const uint* __restrict__ blist, const uint* __restrict__ bpos,
+                          const uint* __restrict__ parent, const uint* __restrict__ size, uint* __restrict__ base,
+                          uint* __restrict__ start, uint* __restrict__ ccw) {
+    pdl_wait();
+    pdl_trigger();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)bpos[n]) return;
+    const uint i = blist[t];
+    if (parent[i] != i) return;
+    const uint b = atomicAdd(ccw, size[i]);
+    base[i] = b;
+    start[b] = 1u;
+}
+
+__global__ void k_cc_slot(long long n, const uint* __restrict__ blist, const uint* __restrict__ bpos,
+                          const uint* __restrict__ parent, const uint* __restrict__ base, uint* __restrict__ fill,
+                          uint* __restrict__ order) {
+    pdl_wait();
+    pdl_trigger();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)bpos[n]) return;
+    const uint i = blist[t];
+    const uint r = parent[i];
+    order[base[r] + atomicAdd(fill + r, 1u)] = i;
+}
+
+// First slot of batch b: the first component start at or after b *
+// kBatchTarget (all bound particles when none follows); the batch's particles
+// and pairs against the block's capacity (P particles, Q pairs).
+__device__ __forceinline__ uint cc_batch_start(uint b, uint nb, const uint* __restrict__ start, uint P, bool& ok) {
+    const unsigned long long s0 = (unsigned long long)b * kBatchTarget;
+    if (s0 >= nb) return nb;
+    uint s = (uint)s0;
+    for (uint k = 0; s < nb && !start[s]; k++, s++)
+        if (k >= P) { ok = false; return s; }   // a component larger than a block holds
+    return s;
+}
+__global__ void k_cc_batches(long long n, long long nbmax, uint P, uint Q, const uint* __restrict__ bpos,
+                             const uint* __restrict__ start, const uint* __restrict__ order,
+                             const uint* __restrict__ off, uint* __restrict__ batch, uint* __restrict__ ccw) {
+    pdl_wait();
+    pdl_trigger();
+    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nbmax) return;
+    const uint nb = bpos[n];
+    bool ok = true;
+    const uint s0 = cc_batch_start((uint)b, nb, start, P, ok);
+    batch[b] = s0;
+    if (!ok || s0 >= nb) {
+        if (!ok) atomicOr(ccw + 1, 1u);
+        return;
+    }
+    const uint s1 = cc_batch_start((uint)b + 1, nb, start, P, ok);
+    uint np = 0;
+    if (ok && s1 - s0 <= P)
+        for (uint s = s0; s < s1; s++) {
+            const uint i = order[s];
+            np += off[i + 1] - off[i];
+        }
+    if (!ok || s1 - s0 > P || np > Q) atomicOr(ccw + 1, 1u);
+}
+
 // ------------------------------------------------------------ pair force
 // Contact of one listed pair (lo, hi) = (Lp, Ln), the body of
 // calculateforcepairD (neiglist.cu:156-233) with the law of dem_law.cuh.
@@ -441,6 +580,11 @@ template <typename Real> struct StepArgs {
     ParticleCommon pc;
     Real dtr, inv_dt, density;
     int split;                    // window kernels: bound items per thread of the bound blocks (0: all blocks)
+    // cluster batches: when batch != 0 the window's bound particles are
+    // stepped by k_batch unless ccw[1] (a component or batch too large) is
+    // set, in which case the grid-barrier window kernel steps the window
+    int batch;
+    const uint* ccw;
     EngineWords* words;
     double *dbgF, *dbgT;
     uint* dbgC;
@@ -822,6 +966,7 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Re
 template <typename Real>
 __global__ void __launch_bounds__(256) k_free_run(StepArgs<Real> a, int slot0, int nsteps, int observe_slot,
                                                   StepPartials part, size_t clr0, size_t clr1) {
+    if (a.batch && a.ccw[1]) return;   // the grid-barrier window kernel steps this window's free particles too
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz_obs = 0.0;
     uint flags = 0;
@@ -953,6 +1098,7 @@ __device__ __forceinline__ void free_sweep(const StepArgs<Real>& a, const PRec<R
 template <typename Real>
 __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int K, StepPartials part, size_t npart,
                                                            uint* bar) {
+    if (a.batch && !a.ccw[1]) return;   // the cluster batches (k_batch, k_free_run) step this window
     uint nbar = 0;
     const uint nw = *a.wcount;
     const uint total = a.off[a.n];
@@ -1026,6 +1172,258 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
     }
     block_observables(mz, cnt, flags, 1, part, a.words);
     clear_partials(part, gridDim.x, npart);
+}
+
+// Exclusive scan of in[0, m) into out over the block (m <= a few thousand);
+// returns the total to every thread.  tmp: 33 words of shared memory.
+__device__ __forceinline__ uint block_exscan(const uint* in, uint* out, uint m, uint* tmp) {
+    const uint per = (m + blockDim.x - 1) / blockDim.x;
+    const uint b = threadIdx.x * per, e = min(b + per, m);
+    uint sum = 0;
+    for (uint k = b; k < e; k++) sum += in[k];
+    const uint lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint v = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)lane >= o) inc += v;
+    }
+    if (lane == 31) tmp[warp] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint acc = 0;
+        for (uint w = 0; w < (blockDim.x >> 5); w++) { const uint t = tmp[w]; tmp[w] = acc; acc += t; }
+        tmp[32] = acc;
+    }
+    __syncthreads();
+    uint run = tmp[warp] + inc - sum;
+    for (uint k = b; k < e; k++) { const uint v = in[k]; out[k] = run; run += v; }
+    const uint total = tmp[32];
+    __syncthreads();
+    return total;
+}
+
+// One block steps whole batches of small components through all K steps of
+// the window in shared memory: per step, the batch's pair items (pair_eval)
+// and wall items (wall_contacts), a block barrier, the batch's particles
+// (gather in list order: own row, then reverse row; gravity, walls,
+// integrate), a block barrier.  The operations and their order are those of
+// pair_item / wall_item / bound_item, so the states are those of the
+// grid-barrier window kernel and of the per-step kernels, bit for bit.  The
+// free particles run concurrently in k_free_run.  Observables of the window's
+// last step go to `part` (one partial per block; [gridDim.x, clr1) cleared).
+template <typename Real> struct BatchSmem {
+    V3<double>* x; V3<double>* d; V3<Real>* a; Real* r; float4* q; V3<double>* wh;
+    uint *gid, *ws, *pb, *pl, *rb, *rl;
+    R4<Real>* wf; R4<Real>* wt;
+    uint *plo, *phi, *pk, *prv;
+    V3<double>* ph;
+    R4<Real> *fo, *ti, *tj;
+    uint* scan;
+};
+template <typename Real> __host__ __device__ inline size_t batch_smem_layout(unsigned char* base, BatchSmem<Real>* L) {
+    constexpr uint P = BatchCap<Real>::P, Q = BatchCap<Real>::Q;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
+    BatchSmem<Real> l;
+    l.x = (V3<double>*)take(P * sizeof(V3<double>));
+    l.d = (V3<double>*)take(P * sizeof(V3<double>));
+    l.wh = (V3<double>*)take(P * sizeof(V3<double>));
+    l.q = (float4*)take(P * sizeof(float4));
+    l.wf = (R4<Real>*)take(P * sizeof(R4<Real>));
+    l.wt = (R4<Real>*)take(P * sizeof(R4<Real>));
+    l.a = (V3<Real>*)take(P * sizeof(V3<Real>));
+    l.r = (Real*)take(P * sizeof(Real));
+    l.gid = (uint*)take(P * 4); l.ws = (uint*)take(P * 4); l.pb = (uint*)take(P * 4);
+    l.pl = (uint*)take(P * 4); l.rb = (uint*)take(P * 4); l.rl = (uint*)take(P * 4);
+    l.ph = (V3<double>*)take(Q * sizeof(V3<double>));
+    l.fo = (R4<Real>*)take(Q * sizeof(R4<Real>));
+    l.ti = (R4<Real>*)take(Q * sizeof(R4<Real>));
+    l.tj = (R4<Real>*)take(Q * sizeof(R4<Real>));
+    l.plo = (uint*)take(Q * 4); l.phi = (uint*)take(Q * 4); l.pk = (uint*)take(Q * 4); l.prv = (uint*)take(Q * 4);
+    l.scan = (uint*)take(34 * 4);
+    if (L) *L = l;
+    return o;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kBatchThreads) k_batch(StepArgs<Real> a, int K, const uint* __restrict__ corder,
+                                                         const uint* __restrict__ cbatch, uint* cloc,
+                                                         StepPartials part, size_t clr1) {
+    if (a.ccw[1]) return;   // a component or a batch too large: the grid-barrier window kernel has the window
+    extern __shared__ __align__(16) unsigned char smem[];
+    BatchSmem<Real> L;
+    batch_smem_layout<Real>(smem, &L);
+    const long long nb = a.bpos[a.n];
+    const uint nbatch = (uint)((nb + kBatchTarget - 1) / kBatchTarget);
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    ParticleCommon pc = a.pc;
+    for (uint bi = blockIdx.x; bi < nbatch; bi += gridDim.x) {
+        const uint s0 = cbatch[bi], m = cbatch[bi + 1] - s0;
+        // the batch's particles into shared memory
+        for (uint p = threadIdx.x; p < m; p += blockDim.x) {
+            const uint i = corder[s0 + p];
+            cloc[i] = p;
+            L.gid[p] = i;
+            V3<double> x, d;
+            V3<Real> av;
+            Real r;
+            ld_rec<false>(a.S + i, x, d, av, r);
+            L.x[p] = x; L.d[p] = d; L.a[p] = av; L.r[p] = r;
+            L.q[p] = a.Q[i];
+            L.wh[p] = mk(a.W.x[i], a.W.y[i], a.W.z[i]);
+            L.ws[p] = a.wslot[i];
+            L.pl[p] = a.off[i + 1] - a.off[i];
+            L.rl[p] = a.roff[i + 1] - a.roff[i];
+        }
+        __syncthreads();
+        const uint npairs = block_exscan(L.pl, L.pb, m, L.scan);
+        block_exscan(L.rl, L.rb, m, L.scan);
+        // the batch's pairs: own rows in list order, reverse rows as pair slots
+        for (uint p = threadIdx.x; p < m; p += blockDim.x) {
+            const uint i = L.gid[p], o0 = a.off[i], b0 = L.pb[p];
+            for (uint e = 0; e < L.pl[p]; e++) {
+                const uint k = o0 + e;
+                L.plo[b0 + e] = p;
+                L.phi[b0 + e] = __ldcg(cloc + a.ln[k]);
+                L.pk[b0 + e] = k;
+                L.ph[b0 + e] = mk(a.H.x[k], a.H.y[k], a.H.z[k]);
+            }
+            const uint r0 = a.roff[i], rb = L.rb[p];
+            for (uint u = 0; u < L.rl[p]; u++) {
+                const uint k = a.rk[r0 + u];
+                const uint lo = a.lp[k];
+                L.prv[rb + u] = L.pb[__ldcg(cloc + lo)] + (k - a.off[lo]);
+            }
+        }
+        __syncthreads();
+        for (int st = 0; st < K; st++) {
+            const long long ts = a.tx ? (long long)a.tstep0 + st : -1ll;
+            // pair items and wall items (pair_item, wall_item)
+            for (uint e = threadIdx.x; e < npairs; e += blockDim.x) {
+                const uint lo = L.plo[e], hi = L.phi[e];
+                V3<double> h = L.ph[e];
+                if (ts >= 0) {
+                    double* t = a.th + 3 * a.cap * ts;
+                    const uint k = L.pk[e];
+                    t[k] = h.x; t[a.cap + k] = h.y; t[2 * a.cap + k] = h.z;
+                }
+                V3<Real> Fi, Ti, Tj;
+                const int c = pair_eval<Real>(L.x[lo], L.x[hi], L.d[lo], L.d[hi], L.a[lo], L.a[hi], L.r[lo], L.r[hi], h,
+                                              a.pp, a.inv_dt, a.density, Fi, Ti, Tj);
+                L.ph[e] = h;
+                R4<Real> fo;
+                if (c) {
+                    fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
+                    R4<Real> t4;
+                    t4.x = Ti.x; t4.y = Ti.y; t4.z = Ti.z; t4.w = (Real)0;
+                    L.ti[e] = t4;
+                    t4.x = Tj.x; t4.y = Tj.y; t4.z = Tj.z;
+                    L.tj[e] = t4;
+                } else {
+                    fo.x = fo.y = fo.z = fo.w = (Real)0;
+                }
+                L.fo[e] = fo;
+            }
+            for (uint p = threadIdx.x; p < m; p += blockDim.x) {
+                if (L.ws[p] == kEmpty) continue;
+                const Real r = L.r[p];
+                const Real mass = a.density * (Real)8 * r * r * r;
+                V3<double> h = L.wh[p];
+                if (ts >= 0) {
+                    double* t = a.twh + 3 * a.tnp * ts;
+                    const uint i = L.gid[p];
+                    t[i] = h.x; t[a.tnp + i] = h.y; t[2 * a.tnp + i] = h.z;
+                }
+                V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
+                const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, L.x[p], cvt<Real>(L.d[p]), L.a[p], r, mass, h,
+                                                    a.inv_dt, a.pw, Fw, Tw, (Real*)nullptr);
+                L.wh[p] = h;
+                R4<Real> a4, b4;
+                a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
+                b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
+                L.wf[p] = a4;
+                L.wt[p] = b4;
+            }
+            __syncthreads();
+            // particles (bound_item, particle_finish)
+            pc.first = st == 0 ? 1 : 0;
+            for (uint p = threadIdx.x; p < m; p += blockDim.x) {
+                V3<double> x = L.x[p], d = L.d[p];
+                V3<Real> av = L.a[p];
+                const Real r = L.r[p];
+                float4 q = L.q[p];
+                const uint i = L.gid[p];
+                if (ts >= 0) {
+                    const long long np = a.tnp, o = 3 * np * ts;
+                    a.tx[o + i] = x.x; a.tx[o + np + i] = x.y; a.tx[o + 2 * np + i] = x.z;
+                    a.td[o + i] = d.x; a.td[o + np + i] = d.y; a.td[o + 2 * np + i] = d.z;
+                    a.ta[o + i] = av.x; a.ta[o + np + i] = av.y; a.ta[o + 2 * np + i] = av.z;
+                }
+                V3<Real> F = zero3<Real>(), T = zero3<Real>();
+                uint ci = 0;
+                for (uint e = L.pb[p], e1 = L.pb[p] + L.pl[p]; e < e1; e++) {
+                    const R4<Real> f = L.fo[e];
+                    if (f.w != (Real)0) {
+                        const R4<Real> tq = L.ti[e];
+                        F.x += f.x; F.y += f.y; F.z += f.z;
+                        T.x += tq.x; T.y += tq.y; T.z += tq.z;
+                        ci++;
+                    }
+                }
+                for (uint v = L.rb[p], v1 = L.rb[p] + L.rl[p]; v < v1; v++) {
+                    const uint e = L.prv[v];
+                    const R4<Real> f = L.fo[e];
+                    if (f.w != (Real)0) {
+                        const R4<Real> tq = L.tj[e];
+                        F.x += -f.x; F.y += -f.y; F.z += -f.z;
+                        T.x += tq.x; T.y += tq.y; T.z += tq.z;
+                        ci++;
+                    }
+                }
+                F.z += -sphere_mass(a.density, r);
+                if (L.ws[p] != kEmpty) {
+                    const R4<Real> fw = L.wf[p], tw = L.wt[p];
+                    F.x += fw.x; F.y += fw.y; F.z += fw.z;
+                    T.x += tw.x; T.y += tw.y; T.z += tw.z;
+                }
+                if (ts >= 0) {
+                    double* f = a.tF + 3 * a.tnp * ts;
+                    double* t = a.tT + 3 * a.tnp * ts;
+                    f[3 * i] = F.x; f[3 * i + 1] = F.y; f[3 * i + 2] = F.z;
+                    t[3 * i] = T.x; t[3 * i + 1] = T.y; t[3 * i + 2] = T.z;
+                    a.tc[a.tnp * ts + i] = ci;
+                }
+                const Real mass = sphere_mass(a.density, r);
+                const Real I = (Real)0.4 * mass * (r * r);
+                if (pc.first) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }
+                const uint wflag = __float_as_uint(q.w);
+                double mzi;
+                integrate<Real>(F, T, mass, I, pc.dt, a.dtr, pc.half_skin2, x, d, av, q, flags, mzi);
+                q.w = __uint_as_float(wflag);
+                L.x[p] = x; L.d[p] = d; L.a[p] = av; L.q[p] = q;
+                if (st == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
+            }
+            __syncthreads();
+        }
+        // back to global memory
+        for (uint p = threadIdx.x; p < m; p += blockDim.x) {
+            const uint i = L.gid[p];
+            st_rec(a.S + i, L.x[p], L.d[p], L.a[p], L.r[p]);
+            a.Q[i] = L.q[p];
+            const V3<double> h = L.wh[p];
+            a.W.x[i] = h.x; a.W.y[i] = h.y; a.W.z[i] = h.z;
+        }
+        for (uint e = threadIdx.x; e < npairs; e += blockDim.x) {
+            const uint k = L.pk[e];
+            const V3<double> h = L.ph[e];
+            a.H.x[k] = h.x; a.H.y[k] = h.y; a.H.z[k] = h.z;
+        }
+        __syncthreads();   // the shared arrays are refilled by the next batch
+    }
+    block_observables(mz, cnt, flags, 1, part, a.words);
+    clear_partials(part, gridDim.x, clr1);
 }
 
 // PP (particle-parallel, the paper's Figure 1(b)): each particle evaluates all
@@ -1280,9 +1678,12 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     const PRec<Real>* S = (const PRec<Real>*)c->rec[c->sbuf];
     GridC g = c->grid;
     DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
+    const bool cc = c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent;
+    if (cc) DEM_CUDA_TRY(cudaMemsetAsync(c->cc_words, 0, 4 * sizeof(uint), s));
     k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, S, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
                                                     c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
-                                                    c->wslot, c->wlist, c->wcount);
+                                                    c->wslot, c->wlist, c->wcount, cc ? c->cc_parent : nullptr,
+                                                    c->cc_size, c->npad);
     // every launch after the first is programmatic: each kernel waits for its
     // predecessor before it touches memory, so only the launch latency overlaps
     const bool pdl = c->pdl && !c->profiling;
@@ -1311,6 +1712,21 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         (const uint*)c->tpos));
     DEM_CUDA_TRY(launch_ex(k_rev_sort, grid_for(n, B), B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
                            (const uint*)c->off[dst], c->cap));
+    if (cc) {   // the window's components and batches (cluster-batched window path)
+        const uint* off = c->off[dst];
+        DEM_CUDA_TRY(launch_ex(k_cc_union, (unsigned)std::min<long long>(grid_for(c->cap, B), 148LL * 16), B, s, pdl, n,
+                               c->cap, off, (const uint*)c->lp, (const uint*)c->ln[dst], c->cc_parent));
+        DEM_CUDA_TRY(launch_ex(k_cc_count, grid_for(n, B), B, s, pdl, n, c->cap, (const uint*)c->blist,
+                               (const uint*)c->bpos, off, c->cc_parent, c->cc_size, c->cc_pairs, c->cc_words));
+        DEM_CUDA_TRY(launch_ex(k_cc_base, grid_for(n, B), B, s, pdl, n, (const uint*)c->blist, (const uint*)c->bpos,
+                               (const uint*)c->cc_parent, (const uint*)c->cc_size, c->cc_base, c->cc_start,
+                               c->cc_words));
+        DEM_CUDA_TRY(launch_ex(k_cc_slot, grid_for(n, B), B, s, pdl, n, (const uint*)c->blist, (const uint*)c->bpos,
+                               (const uint*)c->cc_parent, (const uint*)c->cc_base, c->cc_fill, c->cc_order));
+        DEM_CUDA_TRY(launch_ex(k_cc_batches, grid_for(c->nbatch_max + 1, B), B, s, pdl, n, c->nbatch_max,
+                               BatchCap<Real>::P, BatchCap<Real>::Q, (const uint*)c->bpos, (const uint*)c->cc_start,
+                               (const uint*)c->cc_order, off, c->cc_batch, c->cc_words));
+    }
     return DEM_OK;
 }
 
@@ -1343,6 +1759,8 @@ template <typename Real> StepArgs<Real> step_args(const dem_ctx* c, int lst, int
     a.inv_dt = (Real)(1.0 / c->cfg.dt);
     a.density = (Real)c->cfg.density;
     a.split = c->win_split;
+    a.batch = 0;
+    a.ccw = c->cc_words;
     a.words = c->words;
     a.dbgF = c->record ? c->dbgF : nullptr;
     a.dbgT = c->record ? c->dbgT : nullptr;
@@ -1368,10 +1786,11 @@ template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
 }
 
 // Free particles, window slots slot0 .. slot0+nsteps-1, on stream s.
-template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nsteps, cudaStream_t s) {
+template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nsteps, cudaStream_t s, int batch = 0) {
     const int obs = c->observe_slot;
     const int os = (obs >= slot0 && obs < slot0 + nsteps) ? obs : slot0;
     StepArgs<Real> a = step_args<Real>(c, lst, slot0);
+    a.batch = batch;
     if (nsteps != 1) a.dbgF = a.dbgT = nullptr, a.dbgC = nullptr;
     k_free_run<Real><<<grid_for(c->n, 256), 256, 0, s>>>(a, slot0, nsteps, obs, free_partials(c, os), c->nblk,
                                                          c->npart - c->nblk);
@@ -1380,10 +1799,11 @@ template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nst
 }
 
 // The window kernel: all K steps of the window in one cooperative launch.
-template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape* tape) {
+template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape* tape, int batch = 0) {
     const int K = c->cfg.relist_interval;
     DEM_CUDA_TRY(cudaMemsetAsync(c->bar, 0, kBarWords * sizeof(uint), c->stream));   // counter, give-up word
     StepArgs<Real> a = step_args<Real>(c, lst, 0);
+    a.batch = batch;
     a.dbgF = a.dbgT = nullptr;
     a.dbgC = nullptr;
     if (tape) {
@@ -1428,6 +1848,37 @@ template <typename Real> int launch_window_pp(dem_ctx* c, int lst, int sb, int h
     return DEM_OK;
 }
 
+// The cluster-batched window: the grid-barrier window kernel (it steps the
+// window only when a component or batch is too large for a block), then the
+// free particles (forked stream) beside the batches, joined.
+template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const WindowTape* tape) {
+    const int K = c->cfg.relist_interval;
+    int rc = launch_window<Real>(c, lst, tape, 1);
+    if (rc) return rc;
+    DEM_CUDA_TRY(cudaEventRecord(c->evfork, c->stream));
+    DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
+    rc = launch_free<Real>(c, lst, 0, K, c->stream2, 1);
+    if (rc) return rc;
+    DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
+    StepArgs<Real> a = step_args<Real>(c, lst, 0);
+    a.batch = 1;
+    a.dbgF = a.dbgT = nullptr;
+    a.dbgC = nullptr;
+    if (tape) {
+        a.tx = tape->tx; a.td = tape->td; a.twh = tape->twh; a.tF = tape->tF; a.tT = tape->tT; a.th = tape->th;
+        a.tc = tape->tc;
+        a.ta = (Real*)tape->ta;
+        a.tstep0 = tape->step0;
+    }
+    k_batch<Real><<<c->batch_grid, kBatchThreads, c->batch_smem, c->stream>>>(
+        a, K, (const uint*)c->cc_order, (const uint*)c->cc_batch, c->cc_loc, partials(c, K - 1), (size_t)c->nblk);
+    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->evjoin, 0));
+    return DEM_OK;
+}
+
+bool use_batches(const dem_ctx* c) { return c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent != nullptr; }
+
 // PP step: reads state buffer sbuf and history phase hph, writes the others.
 template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, int hp) {
     const long long n = c->n, np = c->npad;
@@ -1449,6 +1900,9 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
 namespace dem {
 int window_kernel(dem_ctx* c, int lst, const WindowTape* tape) {
     NvtxRange r("dem window kernel");
+    if (use_batches(c))
+        return c->prec == DEM_PREC_MIXED ? launch_batched_window<float>(c, lst, tape)
+                                         : launch_batched_window<double>(c, lst, tape);
     return c->prec == DEM_PREC_MIXED ? launch_window<float>(c, lst, tape) : launch_window<double>(c, lst, tape);
 }
 
@@ -1512,8 +1966,9 @@ int enqueue_window(dem_ctx* c, int src) {
     c->observe_slot = K - 1;
     const bool mixed = c->prec == DEM_PREC_MIXED;
     if (c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel) {
-        // every step of the window in one cooperative launch
-        rc = mixed ? launch_window<float>(c, lst, nullptr) : launch_window<double>(c, lst, nullptr);
+        // every step of the window in one cooperative launch, or the cluster
+        // batches beside the free particles
+        rc = window_kernel(c, lst, nullptr);
         if (rc) return rc;
         if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2], c->stream, cudaEventRecordExternal));
         c->wtiming_path = 1;
@@ -1735,6 +2190,24 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->reorder = !(ro && ro[0] == '0');
         const char* sp = getenv("DEM_B200_SPLIT");   // window kernels' bound items per thread (0: no split)
         if (sp && sp[0]) c->win_split = atoi(sp);
+        const char* bt = getenv("DEM_B200_BATCH");   // "0": no cluster batches (grid-barrier window kernel)
+        c->batching = c->mode == DEM_FORCE_PCCP && c->win_kernel && !(bt && bt[0] == '0');
+        if (c->batching) {
+            const bool mx = c->prec == DEM_PREC_MIXED;
+            c->batch_smem = mx ? batch_smem_layout<float>(nullptr, nullptr) : batch_smem_layout<double>(nullptr, nullptr);
+            e = mx ? cudaFuncSetAttribute(k_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->batch_smem)
+                   : cudaFuncSetAttribute(k_batch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)c->batch_smem);
+            int bper = 0;
+            if (e == cudaSuccess)
+                e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bper, k_batch<float>, kBatchThreads, c->batch_smem)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bper, k_batch<double>, kBatchThreads,
+                                                                       c->batch_smem);
+            if (e != cudaSuccess) return bail(cuda_fail(e, "batch kernel set-up", __FILE__, __LINE__));
+            c->batching = bper > 0;
+            c->batch_grid = (unsigned)std::max<long long>(1, std::min<long long>((long long)nsm * bper, grid_for(n, 256)));
+            c->nbatch_max = (np + kBatchTarget - 1) / kBatchTarget + 1;
+        }
     }
     // partials per slot: particle-kernel blocks, free-kernel blocks, and at
     // least as many as the window kernel has blocks
@@ -1746,6 +2219,17 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     if (e == cudaSuccess)
         e = cudaMemsetAsync(c->part_cnt, 0, (size_t)cfg->relist_interval * c->npart * sizeof(uint), s0);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (partials)", __FILE__, __LINE__));
+    if (c->batching) {
+        if ((rc = dalloc(&c->cc_parent, np)) || (rc = dalloc(&c->cc_size, 4 * np)) || (rc = dalloc(&c->cc_base, np)) ||
+            (rc = dalloc(&c->cc_order, np)) || (rc = dalloc(&c->cc_batch, c->nbatch_max + 2)) ||
+            (rc = dalloc(&c->cc_loc, np)) || (rc = dalloc(&c->cc_words, 4)))
+            return bail(rc);
+        c->cc_pairs = c->cc_size + np;
+        c->cc_fill = c->cc_size + 2 * np;
+        c->cc_start = c->cc_size + 3 * np;
+        e = cudaMemsetAsync(c->cc_words, 0, 4 * sizeof(uint), s0);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (batch words)", __FILE__, __LINE__));
+    }
     c->scan_words = 3 * scan_scratch_words(std::max<long long>(np + 1, 1));
     if ((rc = dalloc(&c->scan_tmp, c->scan_words))) return bail(rc);
     e = cudaMemsetAsync(c->words, 0, sizeof(EngineWords), s0);
@@ -1782,7 +2266,8 @@ int dem_destroy(dem_ctx* c) {
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
                     c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar,
-                    c->tpos, c->pour_rec, c->perm};
+                    c->tpos, c->pour_rec, c->perm, c->cc_parent, c->cc_size, c->cc_base, c->cc_order,
+                    c->cc_batch, c->cc_loc, c->cc_words};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
@@ -2512,22 +2997,28 @@ int dem_check_barrier_timeout(dem_ctx* c, double* waited_ms) {
     return DEM_OK;
 }
 
-int dem_window_work(dem_ctx* c, long long* bound, long long* wall_candidates, long long* pairs) {
+int dem_window_work(dem_ctx* c, long long* bound, long long* wall_candidates, long long* pairs, int* batched) {
     if (!c) return fail(DEM_ERR_ARG, "dem_window_work: null ctx");
     if (bound) *bound = 0;
     if (wall_candidates) *wall_candidates = 0;
     if (pairs) *pairs = 0;
+    if (batched) *batched = 0;
     if (!c->uploaded || c->relists == 0) return DEM_OK;
-    uint v[3] = {0, 0, 0};
+    uint v[4] = {0, 0, 0, 1};
     uint* hp = (uint*)c->host_pinned;
     DEM_CUDA_TRY(cudaMemcpyAsync(hp, c->bpos + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaMemcpyAsync(hp + 1, c->wcount, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaMemcpyAsync(hp + 2, c->off[c->cur] + c->n, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    if (use_batches(c))
+        DEM_CUDA_TRY(cudaMemcpyAsync(hp + 3, c->cc_words + 1, sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
+    else
+        hp[3] = 1u;
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     memcpy(v, hp, sizeof(v));
     if (bound) *bound = v[0];
     if (wall_candidates) *wall_candidates = v[1];
     if (pairs) *pairs = (long long)v[2] <= c->cap ? v[2] : 0;
+    if (batched) *batched = v[3] == 0u ? 1 : 0;
     return DEM_OK;
 }
 

@@ -182,7 +182,7 @@ struct dem_ctx {
     uint* bar = nullptr;             // window-kernel grid barrier: [0] arrival counter
     unsigned win_grid = 1;           // window-kernel blocks (all co-resident)
     bool win_kernel = true;          // whole PCCP windows as one cooperative launch
-    int win_split = 1;               // window kernels: bound items per thread of the bound blocks (0: no split)
+    int win_split = 0;               // window kernels: bound items per thread of the bound blocks (0: no split)
     int wtiming_path = 0;            // last timed window: 0 per-step, 1 window kernel, 2 per-step + forked free
     uint* off[2] = {nullptr, nullptr};
     uint* roff = nullptr;
@@ -192,6 +192,23 @@ struct dem_ctx {
     int hph = 0;             // history phase of the current list (PP ping-pong)
     uint* rk = nullptr;
     uint* carry = nullptr;   // optional carry-map output of relist (adjoint recompute)
+    // cluster batches (PCCP windows): the window's bound particles grouped by
+    // connected component of the pair list; small components are packed into
+    // batches that one block steps through the whole window in shared memory
+    bool batching = true;            // DEM_B200_BATCH=0: the grid-barrier window kernel for every window
+    uint* cc_parent = nullptr;       // np: union-find parent, then the component root (its smallest id)
+    uint* cc_size = nullptr;         // np: per root: bound particles of the component
+    uint* cc_pairs = nullptr;        // np: per root: listed pairs of the component
+    uint* cc_fill = nullptr;         // np: per root: slots handed out so far
+    uint* cc_base = nullptr;         // np: per root: the component's first slot
+    uint* cc_start = nullptr;        // np + 1: 1 at each component's first slot
+    uint* cc_order = nullptr;        // np: bound particle ids, grouped by component
+    uint* cc_batch = nullptr;        // nbatch_max + 1: first slot of each batch
+    uint* cc_loc = nullptr;          // np: a batch particle's index inside its block
+    uint* cc_words = nullptr;        // [0] slots handed out, [1] 1 = a component or batch too large
+    long long nbatch_max = 0;
+    unsigned batch_grid = 1;         // blocks of the batch kernel
+    size_t batch_smem = 0;           // its dynamic shared memory
     uint* wslot = nullptr;   // per particle: wall-candidate slot of this window or kEmpty
     uint* wlist = nullptr;   // wall candidates (particle ids)
     uint* wcount = nullptr;  // number of wall candidates (device)

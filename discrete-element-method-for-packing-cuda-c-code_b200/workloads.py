@@ -20,8 +20,9 @@ damping, normal and tangential), flat frictional walls, gravity -z, skin
   bed_500k       the rsa_500k spheres as a settled bed (every sphere in
                  contact): RSA largest first at solid fraction 0.32 in a
                  100x100 mm base, compacted by a downward velocity
-                 proportional to height and gravity (dense_bed()), then
-                 stepped as rsa_500k.
+                 proportional to height and gravity with restitution 0.1,
+                 then quenched (velocities zeroed) ten times 500 steps apart
+                 (dense_bed()); then stepped as rsa_500k.
   pour_box       a poured packing (the reference's layer injection) at test
                  size: 108 spheres r = 0.5 mm in 8x8 mm, 3 layers of 36 on a
                  6x6 injection lattice 3 mm above the floor, initial speed 1.5
@@ -165,7 +166,7 @@ def pour_box(seed=SEED, nx=6, ny=6, layers=3, box=(8.0, 8.0, 12.0), z_inject=3.0
     return w
 
 
-def bed_500k_initial(seed=SEED, precision=PREC_MIXED, n=500_000, base=(100.0, 100.0), phi0=0.32, phi_bed=0.58,
+def bed_500k_initial(seed=SEED, precision=PREC_MIXED, n=500_000, base=(100.0, 100.0), phi0=0.32, phi_bed=0.55,
                      compact_s=0.0125):
     """Initial state of the settled 500,000-sphere bed: the rsa_500k radii
     placed by random sequential addition largest first (which reaches solid
@@ -194,21 +195,36 @@ def bed_500k_initial(seed=SEED, precision=PREC_MIXED, n=500_000, base=(100.0, 10
                           "pdis": pdis.reshape(-1).copy(), "compact_steps": int(round(compact_s / 5e-7))})
 
 
-def dense_bed(dem, w, settle_steps, relist=10, stream=None):
-    """Settles bed_500k_initial's column on the GPU (mixed precision, re-list
-    every `relist` steps so that the fastest spheres stay inside the skin
-    guard), and returns the bed as a Workload at the production cadence
-    (re-list every 20 steps) with its state: pos, and pdis/angv in meta."""
+def dense_bed(dem, w, settle_steps, relist=10, stream=None, e_settle=0.1, quench_cycles=10, quench_every=500,
+              log=None):
+    """Settles bed_500k_initial's column on the GPU and returns the bed as a
+    Workload at the production cadence (re-list every 20 steps) with its
+    state: pos, and pdis/angv in meta.  Mixed precision, re-list every
+    `relist` steps (the compaction's fastest spheres stay inside the skin
+    guard), restitution e_settle (the returned workload keeps its own
+    material): `settle_steps` of compaction, then `quench_cycles` times the
+    velocities set to zero (an upload of the positions alone) and
+    `quench_every` steps, which drains the kinetic and elastic energy the
+    compaction left, so that the bed rests under gravity instead of
+    rebounding.  log(stage, scalars) is called after each stage."""
     e = dem.Engine(**{**w.engine_kwargs(), "precision": PREC_MIXED, "relist_interval": relist})
     if stream is not None:
         e.set_stream(stream)
-    e.set_material(w.pp, w.pw)
+    e.set_material(*material(mu=0.3, roll_rel=0.002, e=e_settle))
     e.upload(w.pos, w.rad, w.meta["pdis"], None)
     e.step(settle_steps)
+    if log:
+        log("compaction", e.scalars(raise_on_status=False))
+    for q in range(quench_cycles):
+        pos, _, _ = e.download()
+        e.upload(pos, w.rad)
+        e.step(quench_every)
+        if log:
+            log(f"quench {q + 1}", e.scalars(raise_on_status=False))
     s = e.scalars()
     pos, pdis, angv = e.download()
     e.close()
     meta = dict(w.meta)
-    meta.update(pdis=pdis, angv=angv, settle_steps=settle_steps, settled=s)
+    meta.update(pdis=pdis, angv=angv, settle_steps=settle_steps + quench_cycles * quench_every, settled=s)
     return Workload(w.name, w.n, pos, w.rad, w.world, w.dt, w.steps, 20, w.skin, w.precision, w.pp, w.pw,
                     meta=meta)

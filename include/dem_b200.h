@@ -322,9 +322,13 @@ int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
 /* Work of the current list's window (waits for the context's stream):
  * *bound = particles with a listed pair or a wall candidacy (stepped with the
  * pair phase), *wall_candidates = particles near a wall, *pairs = listed
- * pairs; the others step under gravity alone until the next re-list.  No
+ * pairs; the others step under gravity alone until the next re-list.
+ * *batched = 1 when the bound particles' connected components (through the
+ * pair list) were small enough to be stepped as cluster batches, one block
+ * per batch in shared memory, 0 when the grid-barrier window kernel stepped
+ * them (a dense bed is one large component).  Any pointer may be NULL.  No
  * counterpart in the reference (it steps every particle the same way). */
-int dem_window_work(dem_ctx* ctx, long long* bound, long long* wall_candidates, long long* pairs);
+int dem_window_work(dem_ctx* ctx, long long* bound, long long* wall_candidates, long long* pairs, int* batched);
 
 /* Checkpoint / resume (the reference's restart reader is commented out,
  * dempacking.cu:361-367, and its preflow.dat has no contact history).

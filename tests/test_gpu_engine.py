@@ -368,6 +368,46 @@ def test_window_kernel_equals_per_step_kernels(dem, wl, cuda, monkeypatch, prec,
         b.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_cluster_batches_equal_grid_barrier_window(dem, wl, cuda, monkeypatch, prec):
+    """The cluster-batched window (the default for PCCP: the bound particles'
+    connected components packed into batches that one block steps through
+    the window in shared memory, the free particles beside them) and the
+    grid-barrier window kernel (DEM_B200_BATCH=0) agree bit for bit -- states,
+    pair histories, observables -- on a sparse bed, a compressed bed with
+    chains of contacts, and a dense lattice that is one component too large
+    for a block (which the batched context hands to the grid-barrier kernel)."""
+    from _cases import dense_lattice
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    cases = [(wl.small_box(n=3000), 1), (wl.small_box(n=4000, compress=0.85), None),
+             (dense_lattice(dem, nx=10, ny=10, nz=8), 0)]
+    for w, batched in cases:
+        rng = np.random.default_rng(9)
+        pdis = rng.normal(0, 2e-6, 3 * w.n)
+        angv = rng.normal(0, 2e-5, 3 * w.n)
+        a = make_engine(dem, w, p)
+        a.upload(w.pos, w.rad, pdis, angv)
+        monkeypatch.setenv("DEM_B200_BATCH", "0")
+        b = make_engine(dem, w, p)
+        b.upload(w.pos, w.rad, pdis, angv)
+        monkeypatch.delenv("DEM_B200_BATCH")
+        a.step(4 * w.relist_interval)
+        b.step(4 * w.relist_interval)
+        wa, wb = a.window_work(), b.window_work()
+        assert wb["batched"] == 0 and (batched is None or wa["batched"] == batched), (w.name, wa, wb)
+        print(f"\n{w.name} n={w.n}: {wa}")
+        assert wa["bound"] == wb["bound"] > 0
+        for x, y in zip(a.download(), b.download()):
+            np.testing.assert_array_equal(x, y)
+        for x, y in zip(a.pairs(), b.pairs()):
+            np.testing.assert_array_equal(x, y)
+        sa, sb = a.scalars(), b.scalars()
+        assert sa["status"] == 0 and sb["status"] == 0
+        assert sa["maxhz"] == sb["maxhz"] and sa["contacts"] == sb["contacts"]
+        a.close()
+        b.close()
+
+
 def test_plain_launches_equal_programmatic_launches(dem, wl, cuda, monkeypatch):
     """Re-list and step kernels launched programmatically (the default) and
     launched plainly (DEM_B200_PDL=0) agree bit for bit, with the per-step

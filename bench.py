@@ -46,8 +46,9 @@ BYTES_PER_PARTICLE = {"mixed": 172, "fp64": 200}   # per particle-step, all fiel
 BYTES_PER_PAIR = 56                                 # ids 8 + FP64 history r+w 48, per pair-step
 METRIC = "particle-steps/s @500K spheres"
 UNIT = "particle-steps/s"
-KERNELS_PER_WINDOW = 11 + 1   # re-list: hash, 3-launch cell scan, scatter, walk, 3-launch triple scan, fill,
-                              # reverse sort; + the window kernel
+KERNELS_RELIST = 11           # hash, 3-launch cell scan, scatter, walk, 3-launch triple scan, fill, reverse sort
+KERNELS_BATCHES = 3 + 3       # with cluster batches: component slots, particle slots, batches; the window
+                              # kernel (exits unless a batch is too large), the free particles, the batches
 
 
 def load_pkg():
@@ -198,13 +199,15 @@ def workload(dem, precision, rank):
     return w.rsa_500k(seed=w.SEED + rank, precision=precision)
 
 
-def time_windows(torch, eng, stream, K, flush_buf, win, time_kernels=False):
+def time_windows(torch, eng, stream, K, flush_buf, win, time_kernels=False, label="windows"):
     """Per-window CUDA events on the engine's stream; L2 flush between windows
     outside the events.  Returns total ms.  With time_kernels, the last timed
     window replays the engine's window graph variant that records CUDA events
-    around the re-list and the window kernel (captured beforehand)."""
+    around the re-list and the window kernel (captured beforehand).  The
+    windows run inside the NVTX range `label` (a profiler can select them:
+    ncu --nvtx --nvtx-include "<label>/")."""
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    with torch.cuda.stream(stream):
+    with torch.cuda.stream(stream), torch.cuda.nvtx.range(label):
         for k in range(K):
             flush_buf.zero_()
             if time_kernels and k == K - 1:
@@ -278,7 +281,7 @@ def run_ours(args):
     clocks = ClockSampler(local)
     clocks.start()
     torch.cuda.synchronize()
-    total_ms = time_windows(torch, eng, stream, K, flush, win, time_kernels=True)
+    total_ms = time_windows(torch, eng, stream, K, flush, win, time_kernels=True, label="headline")
     torch.cuda.synchronize()
     clk = clocks.stop()
     # dominant kernel duration: CUDA events inside the last timed window's graph
@@ -293,16 +296,24 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     bp = BYTES_PER_PARTICLE[args.precision]
     kbytes, rbytes = window_bytes(w.n, work, win, bp, ncells)
-    if kt["window_kernel_ms"] > 0:
+    note = ("free flight: ~10 % of the spheres are bound (a listed pair or a wall), the rest step in registers; "
+            "latency-bound (grid barriers, dependent loads)")
+    if kt["window_kernel_ms"] > 0 and work.get("batched") == 1:
+        kname, kms = "k_batch+k_free_run", kt["window_kernel_ms"]
+        note = ("free flight: ~10 % of the spheres are bound (a listed pair or a wall), stepped as cluster batches "
+                "(k_batch: one block per batch of whole components, all the window's steps in shared memory); the "
+                "free ones run in registers (k_free_run) on a concurrent stream; latency-bound (block barriers, "
+                "one round of batches)")
+    elif kt["window_kernel_ms"] > 0:
         kname, kms = "k_window", kt["window_kernel_ms"]
     else:   # per-step kernels
         kname, kms = "k_pair+k_particle", kt["pair_ms"] + kt["particle_ms"]
     head_roof = roofline(kname, kbytes, kms, peak, peak_kind, w.name,
-                         traffic=profile_traffic(f"{kname}_rsa500k_{args.precision}"),
-                         note="free flight: ~5 % of the spheres are bound (a listed pair or a wall), the rest "
-                              "step in registers; the launch is latency-bound (grid barriers, dependent loads)")
-    head_roof.update({"kernel_timing": "CUDA events inside the last timed window's graph; window_kernel_ms is one "
-                                       "launch = the window's 20 steps, relist_ms one re-list",
+                         traffic=profile_traffic(f"{kname.replace('+', '_')}_rsa500k_{args.precision}"), note=note)
+    head_roof.update({"kernel_timing": "CUDA events inside the last timed window's graph; window_kernel_ms is the "
+                                       "window's stepping (one launch of the window kernel, or the batched window: "
+                                       "its exiting window kernel, k_free_run beside k_batch, joined) = the window's "
+                                       "20 steps, relist_ms one re-list",
                       "kernel_ms_all": kt, "window_work": work,
                       "step_bytes_per_window": kbytes + rbytes,
                       "step_achieved_gbs": (kbytes + rbytes) / (max_ms / K / 1e3) / 1e9})
@@ -404,7 +415,7 @@ def run_ours(args):
                    "mean_cn": sc["mean_cn"]},
         "roofline": head_roof,
         "clocks": clk,
-        "gpu_launches": KERNELS_PER_WINDOW * K,
+        "gpu_launches": (KERNELS_RELIST + (KERNELS_BATCHES if work.get("batched") is not None else 1)) * K,
         "fp64_plain": fp64,
         "pp_mode": ppm,
         "settled_bed": bed,
@@ -425,7 +436,17 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
     import dem_b200.workloads as wmod
     t0 = time.perf_counter()
     w0 = wmod.bed_500k_initial()
-    w = wmod.dense_bed(dem, w0, w0.meta["compact_steps"] + args.bed_settle_steps, stream=stream.cuda_stream)
+    if args.bed_load:   # a bed settled and saved by an earlier run (--bed-save)
+        z = np.load(args.bed_load)
+        meta = dict(w0.meta, pdis=z["pdis"], angv=z["angv"], settle_steps=int(z["settle_steps"]),
+                    settled={"status": int(z["status"])})
+        w = wmod.Workload(w0.name, w0.n, z["pos"], w0.rad, w0.world, w0.dt, w0.steps, 20, w0.skin, w0.precision,
+                          w0.pp, w0.pw, meta=meta)
+    else:
+        w = wmod.dense_bed(dem, w0, w0.meta["compact_steps"] + args.bed_settle_steps, stream=stream.cuda_stream)
+        if args.bed_save:
+            np.savez(args.bed_save, pos=w.pos, pdis=w.meta["pdis"], angv=w.meta["angv"],
+                     settle_steps=w.meta["settle_steps"], status=w.meta["settled"]["status"])
     settle_s = time.perf_counter() - t0
     pdis, angv = w.meta["pdis"], w.meta["angv"]
     win = w.relist_interval
@@ -434,6 +455,8 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
            "init": w.meta["init"], "settle_steps": w.meta["settle_steps"], "settle_s": settle_s,
            "settle_status": w.meta["settled"]["status"]}
     for prec, key in ((dem.PREC_MIXED, "mixed"), (dem.PREC_FP64, "fp64")):
+        if key not in args.bed_precisions.split(","):
+            continue
         e = dem.Engine(**{**w.engine_kwargs(), "precision": prec})
         e.set_stream(stream.cuda_stream)
         e.set_material(w.pp, w.pw)
@@ -443,7 +466,7 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
             e.set_window_timing(True)
             e.step(2 * win)
             e.set_window_timing(False)
-        ms = time_windows(torch, e, stream, kb, flush, win, time_kernels=True)
+        ms = time_windows(torch, e, stream, kb, flush, win, time_kernels=True, label=f"bed {key}")
         kt = e.window_kernel_times()
         work = e.window_work()
         s = e.scalars(raise_on_status=False)
@@ -461,8 +484,9 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
                                      note="every sphere bound: B_p x 20 per sphere + 56 B x 20 per pair")
         r["step_achieved_gbs"] = (kbytes + rbytes) / (ms / kb / 1e3) / 1e9
         out[key] = r
-    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
-    out["roofline"] = out["mixed"].get("roofline")
+    if "mixed" in out and "fp64" in out:
+        out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["roofline"] = out.get("mixed", {}).get("roofline")
     return out
 
 
@@ -638,6 +662,15 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_bed_only(args):
+    import torch
+    dem = load_pkg()
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    peak, peak_kind = measured_peak()
+    print(json.dumps({"settled_bed": settled_bed(dem, torch, stream, flush, args, peak, peak_kind)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -649,6 +682,9 @@ def main():
     ap.add_argument("--bed-settle-steps", type=int, default=5000,
                     help="steps of the bed after its 25,000 compaction steps, before its ten quenches")
     ap.add_argument("--bed-windows", type=int, default=10)
+    ap.add_argument("--bed-save", default="", help="save the settled bed (npz) for later --bed-load runs")
+    ap.add_argument("--bed-load", default="", help="time a bed saved by --bed-save instead of settling one")
+    ap.add_argument("--bed-precisions", default="mixed,fp64", help="bed rows to time (mixed, fp64)")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -656,7 +692,12 @@ def main():
     ap.add_argument("--skip-bed", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-4m", action="store_true")
+    ap.add_argument("--only-bed", action="store_true",
+                    help="the settled bed alone (for profiling its windows: NVTX ranges 'bed mixed', 'bed fp64')")
     args = ap.parse_args()
+    if args.only_bed:
+        run_bed_only(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -80,6 +80,47 @@ template <typename Real> __device__ __forceinline__ bool cand_test(const R4<Real
 
 __device__ __forceinline__ uint lane_id() { return threadIdx.x & 31; }
 
+// Root of x (parent[x] <= x everywhere; a root is its own parent), halving
+// the path on the way (plain stores touch only non-roots, the hooking CAS only
+// roots).
+__device__ __forceinline__ uint cc_find(uint* parent, uint x) {
+    uint cur = __ldcg(parent + x);
+    if (cur == x) return x;
+    uint prev = x, next;
+    while (cur > (next = __ldcg(parent + cur))) {
+        parent[prev] = next;
+        prev = cur;
+        cur = next;
+    }
+    return cur;
+}
+
+// Root of x by a walk without stores, for use once all unions are made:
+// other threads may meanwhile store roots into parent, which only shortens
+// the walk (parent[x] < x for every non-root, so it ends).  A find with path
+// halving there could overwrite a root just stored for another particle with
+// a mere ancestor.
+__device__ __forceinline__ uint cc_root(const uint* parent, uint x) {
+    uint p;
+    while ((p = __ldcg(parent + x)) != x) x = p;
+    return x;
+}
+
+// Joins the components of a and b: the larger root is hooked under the
+// smaller one by a compare-and-swap on the root, retried from the new roots
+// when another thread hooked it first.
+__device__ __forceinline__ void cc_union(uint* parent, uint a, uint b) {
+    uint ra = cc_find(parent, a), rb = cc_find(parent, b);
+    while (ra != rb) {
+        if (ra < rb) { const uint t = ra; ra = rb; rb = t; }
+        const uint old = atomicCAS(parent + ra, ra, rb);
+        if (old == ra) break;
+        ra = cc_find(parent, old);
+        rb = cc_find(parent, rb);
+    }
+}
+
+
 // ------------------------------------------------------------ state I/O
 // Internal slot i takes the caller's particle perm[i] (identity when perm is
 // null).
@@ -153,7 +194,7 @@ __global__ void k_hash_count(long long n, const PRec<Real>* __restrict__ S, Grid
     if (i >= n) return;
     if (cc_parent) {   // the coming re-list's components start as singletons
         cc_parent[i] = (uint)i;
-        cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u; cc_zero[3 * np + i] = 0u;
+        cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
     }
     const V3<double> p = ld_pos<false>(S + i);
     {
@@ -326,11 +367,12 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
                            uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
                            uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,
                            const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist,
-                           const uint* __restrict__ tpos) {
+                           const uint* __restrict__ tpos, uint* cc_parent, const uint* __restrict__ cc_skip) {
     pdl_wait();
     pdl_trigger();
     const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // particle order
     if (ii >= n) return;
+    if (cc_parent && *cc_skip) cc_parent = nullptr;   // a dense bed: no component pass this re-list
     const uint i = (uint)ii;
     {   // bound / free lists, ascending particle id
         const uint b = bpos[i];
@@ -379,21 +421,33 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
             continue;
         }
         rk[roff[j] + left - 1u] = k;
+        if (cc_parent) cc_union(cc_parent, i, j);   // the window's components (cluster batches)
     }
 }
 
 // Sort each reverse row (pair indices ascending: a deterministic order for
 // the gather) and record each pair's reverse slot ru[k].
+// With cluster batches (parent != nullptr): every bound particle also takes
+// its component's root (all unions were made by the fill) and adds itself and
+// its row's pairs to the root's counts.
 __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,
-                           const uint* __restrict__ off, long long cap) {
+                           const uint* __restrict__ off, long long cap, uint* parent, const uint* __restrict__ bflag,
+                           uint* __restrict__ csize, uint* __restrict__ cpairs, const uint* __restrict__ cc_skip) {
     pdl_wait();
     pdl_trigger();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (parent && *cc_skip) parent = nullptr;
     if ((long long)off[n] > cap) return;
     const uint b = roff[i], e = roff[i + 1];
     isort_u32(rk + b, e - b);
     for (uint u = b; u < e; u++) ru[rk[u]] = u;
+    if (parent && bflag[i]) {
+        const uint r = cc_root(parent, (uint)i);
+        parent[i] = r;
+        atomicAdd(csize + r, 1u);
+        atomicAdd(cpairs + r, off[i + 1] - off[i]);
+    }
 }
 
 // ------------------------------------------------------- cluster batches
@@ -405,137 +459,139 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
 // Jaiganesh & Burtscher 2018), groups the bound particles by component into
 // slots (component order by atomics: any order gives the same states, every
 // particle's sums keep their list order), and cuts the slots into batches of
-// whole components of about kBatchTarget particles that one block of k_batch
-// steps through the window in shared memory.  A batch above the block's
-// capacity (a bed of touching spheres is one component) sends the whole
-// window to the grid-barrier window kernel instead.
-constexpr uint kBatchTarget = 256;       // particles per batch (components are not split)
-constexpr int kBatchThreads = 256;
-template <typename Real> struct BatchCap;
-template <> struct BatchCap<float> { static constexpr uint P = 512, Q = 1024; };
-template <> struct BatchCap<double> { static constexpr uint P = 384, Q = 640; };
+// whole components, one per resident block of k_batch where they fit (the
+// batch window, cc_target), that one block steps through the window in
+// shared memory.  A batch above the block's capacity (a bed of touching
+// spheres is one component) sends the whole window to the grid-barrier window
+// kernel instead.
 
-// Root of x (parent[x] <= x everywhere; a root is its own parent), halving
-// the path on the way (plain stores touch only non-roots, the hooking CAS only
-// roots).
-__device__ __forceinline__ uint cc_find(uint* parent, uint x) {
-    uint cur = __ldcg(parent + x);
-    if (cur == x) return x;
-    uint prev = x, next;
-    while (cur > (next = __ldcg(parent + cur))) {
-        parent[prev] = next;
-        prev = cur;
-        cur = next;
+// A slot range per component (roots only; one atomic per warp for the slot
+// counter), and the largest component.
+__global__ void k_cc_base(long long n, long long cap, const uint* __restrict__ blist, const uint* __restrict__ bpos,
+                          const uint* __restrict__ off, const uint* __restrict__ parent,
+                          const uint* __restrict__ size, uint* __restrict__ base, uint* __restrict__ ccw,
+                          const uint* __restrict__ cc_skip) {
+    pdl_wait();
+    pdl_trigger();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (*cc_skip) {   // no components this re-list: the grid-barrier window kernel has the window
+        if (t == 0) atomicOr(ccw + 1, 1u);
+        return;
     }
-    return cur;
-}
-
-__global__ void k_cc_union(long long n, long long cap, const uint* __restrict__ off, const uint* __restrict__ lp,
-                           const uint* __restrict__ ln, uint* parent) {
-    pdl_wait();
-    pdl_trigger();
-    const uint total = off[n];
-    if ((long long)total > cap) return;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total;
-         k += (long long)gridDim.x * blockDim.x) {
-        uint ra = cc_find(parent, lp[k]), rb = cc_find(parent, ln[k]);
-        while (ra != rb) {
-            if (ra < rb) { const uint t = ra; ra = rb; rb = t; }
-            const uint old = atomicCAS(parent + ra, ra, rb);
-            if (old == ra) break;
-            ra = cc_find(parent, old);   // ra was hooked meanwhile: go on from its new root
-            rb = cc_find(parent, rb);
-        }
+    if (t == 0 && (long long)off[n] > cap) atomicOr(ccw + 1, 1u);
+    uint i = 0, sz = 0;
+    if (t < (long long)bpos[n]) {
+        i = blist[t];
+        if (parent[i] == i) sz = size[i];
     }
+    uint inc = sz;
+    const uint lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint v = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)lane >= o) inc += v;
+    }
+    const uint wtot = __shfl_sync(0xffffffffu, inc, 31);
+    uint wmax = sz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+    uint wbase = 0;
+    if (lane == 31 && wtot) {
+        wbase = atomicAdd(ccw, wtot);
+        atomicMax(ccw + 2, wmax);
+    }
+    wbase = __shfl_sync(0xffffffffu, wbase, 31);
+    if (sz) base[i] = wbase + inc - sz;
 }
 
-// Root of every bound particle (stored as its parent), component sizes and
-// pair counts (pairs counted by their lower particle).
-__global__ void k_cc_count(long long n, long long cap, const uint* __restrict__ blist, const uint* __restrict__ bpos,
-                           const uint* __restrict__ off, uint* parent, uint* __restrict__ size,
-                           uint* __restrict__ pairs, uint* __restrict__ ccw) {
+// The batch window: the bound particles spread over the batch kernel's
+// resident blocks G, at least kBatchMin, at most P minus the largest component
+// (so that a window's components and the tail of its last one fit a block).
+__device__ __forceinline__ uint cc_target(uint nb, uint G, uint P, uint maxc) {
+    uint t = (nb + G - 1) / G;
+    const uint hi = P > maxc ? P - maxc : 0u;
+    t = min(t, hi);
+    return max(t, kBatchMin);
+}
+
+// Each bound particle's slot inside its component's range; each root adds its
+// component to the batch window its first slot falls in: the window's first
+// slot (minimum), particles and pairs.  bw: [0, nbb) first slots, [nbb, 2 nbb)
+// particles, [2 nbb, 3 nbb) pairs.
+__global__ void k_cc_slot(long long n, long long nbb, uint G, uint P, const uint* __restrict__ blist,
+                          const uint* __restrict__ bpos, const uint* __restrict__ parent, const uint* __restrict__ base,
+                          const uint* __restrict__ size, const uint* __restrict__ pairs, uint* __restrict__ fill,
+                          uint* __restrict__ order, uint* __restrict__ bw, uint* __restrict__ ccw) {
     pdl_wait();
     pdl_trigger();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint total = off[n];
-    if (t == 0 && (long long)total > cap) atomicOr(ccw + 1, 1u);
-    if (t >= (long long)bpos[n]) return;
-    const uint i = blist[t];
-    const uint r = cc_find(parent, i);
-    parent[i] = r;
-    atomicAdd(size + r, 1u);
-    if ((long long)total <= cap) atomicAdd(pairs + r, off[i + 1] - off[i]);
-}
-
-// A slot range per component (roots only), marked at its first slot.
-__global__ void k_cc_base(long long n, const uint* __restrict__ blist, const uint* __restrict__ bpos,
-                          const uint* __restrict__ parent, const uint* __restrict__ size, uint* __restrict__ base,
-                          uint* __restrict__ start, uint* __restrict__ ccw) {
-    pdl_wait();
-    pdl_trigger();
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)bpos[n]) return;
-    const uint i = blist[t];
-    if (parent[i] != i) return;
-    const uint b = atomicAdd(ccw, size[i]);
-    base[i] = b;
-    start[b] = 1u;
-}
-
-__global__ void k_cc_slot(long long n, const uint* __restrict__ blist, const uint* __restrict__ bpos,
-                          const uint* __restrict__ parent, const uint* __restrict__ base, uint* __restrict__ fill,
-                          uint* __restrict__ order) {
-    pdl_wait();
-    pdl_trigger();
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)bpos[n]) return;
+    if (ccw[1]) return;   // the window goes to the grid-barrier kernel already
+    const uint nb = bpos[n];
+    const uint tgt = cc_target(nb, G, P, ccw[2]);
+    if (t == 0) ccw[3] = tgt;
+    if (t >= (long long)nb) return;
     const uint i = blist[t];
     const uint r = parent[i];
-    order[base[r] + atomicAdd(fill + r, 1u)] = i;
+    if (r >= (uint)n || parent[r] != r) {   // not a root: the window goes to the grid-barrier kernel
+        atomicOr(ccw + 1, 1u);
+        return;
+    }
+    const uint s = base[r] + atomicAdd(fill + r, 1u);
+    if (s >= nb) {
+        atomicOr(ccw + 1, 1u);
+        return;
+    }
+    order[s] = i;
+    if (r == i) {
+        const uint b0 = base[i], bt = b0 / tgt;
+        if ((long long)bt >= nbb) {
+            atomicOr(ccw + 1, 1u);
+            return;
+        }
+        atomicMin(bw + bt, b0);
+        atomicAdd(bw + nbb + bt, size[i]);
+        atomicAdd(bw + 2 * nbb + bt, pairs[i]);
+    }
 }
 
-// First slot of batch b: the first component start at or after b *
-// kBatchTarget (all bound particles when none follows); the batch's particles
-// and pairs against the block's capacity (P particles, Q pairs).
-__device__ __forceinline__ uint cc_batch_start(uint b, uint nb, const uint* __restrict__ start, uint P, bool& ok) {
-    const unsigned long long s0 = (unsigned long long)b * kBatchTarget;
-    if (s0 >= nb) return nb;
-    uint s = (uint)s0;
-    for (uint k = 0; s < nb && !start[s]; k++, s++)
-        if (k >= P) { ok = false; return s; }   // a component larger than a block holds
-    return s;
-}
-__global__ void k_cc_batches(long long n, long long nbmax, uint P, uint Q, const uint* __restrict__ bpos,
-                             const uint* __restrict__ start, const uint* __restrict__ order,
-                             const uint* __restrict__ off, uint* __restrict__ batch, uint* __restrict__ ccw) {
+// First slot of batch b (the first component whose first slot is b * target
+// or later; all bound particles when none is), and the batch's particles and
+// pairs against the block's capacity (P, Q).
+__global__ void k_cc_batches(long long n, long long nbmax, long long nbb, uint P, uint Q, const uint* __restrict__ bpos,
+                             const uint* __restrict__ bw, uint* __restrict__ batch, uint* __restrict__ ccw,
+                             uint* __restrict__ cc_skip) {
     pdl_wait();
     pdl_trigger();
     const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b > nbmax) return;
-    const uint nb = bpos[n];
-    bool ok = true;
-    const uint s0 = cc_batch_start((uint)b, nb, start, P, ok);
-    batch[b] = s0;
-    if (!ok || s0 >= nb) {
-        if (!ok) atomicOr(ccw + 1, 1u);
-        return;
+    if (b == 0) {
+        // a component larger than a block (a dense bed): the next kDenseSkip
+        // re-lists skip the component pass (union-find on one giant
+        // component costs more than the window it would batch), then it is
+        // tried again
+        const uint k = *cc_skip;
+        if (k) *cc_skip = k - 1u;
+        else if (ccw[2] > P) *cc_skip = kDenseSkip;
     }
-    const uint s1 = cc_batch_start((uint)b + 1, nb, start, P, ok);
-    uint np = 0;
-    if (ok && s1 - s0 <= P)
-        for (uint s = s0; s < s1; s++) {
-            const uint i = order[s];
-            np += off[i + 1] - off[i];
-        }
-    if (!ok || s1 - s0 > P || np > Q) atomicOr(ccw + 1, 1u);
+    if (b > nbmax || ccw[1]) return;
+    const uint nb = bpos[n], tgt = ccw[3];
+    uint s0 = bw[b];
+    long long k = b;
+    // a window with no first slot lies inside a component that started
+    // earlier (longer than a block if the search runs out: its batch's count
+    // is over P already)
+    while (s0 == 0xffffffffu && k < nbmax && k - b <= (long long)(P / tgt) + 1) s0 = bw[++k];
+    if (s0 == 0xffffffffu || s0 > nb) s0 = nb;
+    batch[b] = s0;
+    if (bw[nbb + b] > P || bw[2 * nbb + b] > Q) atomicOr(ccw + 1, 1u);
 }
 
 // ------------------------------------------------------------ pair force
 // Contact of one listed pair (lo, hi) = (Lp, Ln), the body of
 // calculateforcepairD (neiglist.cu:156-233) with the law of dem_law.cuh.
-// Geometry from FP64 positions; in the mixed form the overlap is formed as
-// (s^2 - d^2)/(s + d) in FP64 and rounded once, the rest of the law is FP32
-// except the FP64 history update.  Returns 1 when touching; Fi is the force
+// Geometry from FP64 positions; in the mixed form the overlap is
+// (s^2 - d^2)/(s + d) with the numerator formed in FP64 (no cancellation)
+// and rounded once, the distance, the division and the rest of the law in
+// FP32 except the FP64 history update.  Returns 1 when touching; Fi is the force
 // on lo, Ti/Tj the torques on lo/hi; h is the pair's history (in/out).
 template <typename Real>
 __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double> di, V3<double> dj, V3<Real> ai,
@@ -544,16 +600,30 @@ __device__ __forceinline__ int pair_eval(V3<double> xi, V3<double> xj, V3<double
     const V3<double> Dv = xj - xi;
     const double d2 = dot(Dv, Dv);
     const double s = (double)ri + (double)rj;
-    const double dist = sqrt(d2);
     Real delta;
-    if (sizeof(Real) == 4) delta = (Real)((s * s - d2) / (s + dist));
-    else delta = (Real)(s - dist);
-    if (!(delta > (Real)0 && dist > 0.0)) {
-        h = zero3<double>();
-        return 0;
+    V3<Real> nn;
+    if constexpr (sizeof(Real) == 4) {
+        // the overlap's numerator s^2 - d^2 in FP64 (no cancellation), the
+        // rest in FP32: delta = (s^2 - d^2) / (s + d), n = D / d
+        const float d2f = (float)d2;
+        const float dist = sqrtf(d2f);
+        delta = (float)(s * s - d2) / ((float)s + dist);
+        if (!(delta > 0.f && d2f > 0.f)) {
+            h = zero3<double>();
+            return 0;
+        }
+        const float inv = 1.f / dist;
+        nn = mk((float)Dv.x * inv, (float)Dv.y * inv, (float)Dv.z * inv);
+    } else {
+        const double dist = sqrt(d2);
+        delta = (Real)(s - dist);
+        if (!(delta > (Real)0 && dist > 0.0)) {
+            h = zero3<double>();
+            return 0;
+        }
+        const double inv = 1.0 / dist;
+        nn = cvt<Real>(Dv * inv);
     }
-    const double inv = 1.0 / dist;
-    const V3<Real> nn = cvt<Real>(Dv * inv);
     const Real rstar = ri * rj / (ri + rj);
     const Real mi = density * (Real)8 * ri * ri * ri, mj = density * (Real)8 * rj * rj * rj;
     const Real mstar = mi * mj / (mi + mj);
@@ -730,6 +800,31 @@ __global__ void __launch_bounds__(256) k_pair(StepArgs<Real> a) {
 // states.  FP64 form: the reference's F dt dt / m term by term; mixed form:
 // one reciprocal dt^2/m (FP64) and dt^2/I (FP32) per particle, fused
 // multiply-adds into the FP64 displacement and the FP32 rotation.
+// The mixed integrator's per-particle factors dt^2/m (FP64) and dt^2/I
+// (FP32): constant through a window, so window-long loops compute them once.
+__device__ __forceinline__ double mixed_km(double dt, float m) { return __ddiv_rn(__dmul_rn(dt, dt), (double)m); }
+__device__ __forceinline__ float mixed_ki(float dtr, float I) { return __fdiv_rn(__fmul_rn(dtr, dtr), I); }
+
+// Mixed step with the factors given (the same operations as integrate<float>).
+__device__ __forceinline__ void integrate_k(V3<float> F, V3<float> T, double km, float kI, float half_skin2,
+                                            V3<double>& x, V3<double>& d, V3<float>& a, float4& q, uint& flags,
+                                            double& mz) {
+    d.x = __fma_rn((double)F.x, km, d.x);
+    d.y = __fma_rn((double)F.y, km, d.y);
+    d.z = __fma_rn((double)F.z, km, d.z);
+    a.x = __fmaf_rn(T.x, kI, a.x);
+    a.y = __fmaf_rn(T.y, kI, a.y);
+    a.z = __fmaf_rn(T.z, kI, a.z);
+    x.x = __dadd_rn(x.x, d.x); x.y = __dadd_rn(x.y, d.y); x.z = __dadd_rn(x.z, d.z);
+    q.x = __fadd_rn(q.x, __double2float_rn(d.x));
+    q.y = __fadd_rn(q.y, __double2float_rn(d.y));
+    q.z = __fadd_rn(q.z, __double2float_rn(d.z));
+    const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
+    if (q2 > half_skin2) flags |= kStSkin;
+    if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
+    mz = x.z > 0.0 ? x.z : 0.0;
+}
+
 template <typename Real>
 __device__ __forceinline__ void integrate(V3<Real> F, V3<Real> T, Real m, Real I, double dt, Real dtr,
                                           float half_skin2, V3<double>& x, V3<double>& d, V3<Real>& a, float4& q,
@@ -742,8 +837,8 @@ __device__ __forceinline__ void integrate(V3<Real> F, V3<Real> T, Real m, Real I
         a.y = __dadd_rn(a.y, __ddiv_rn(__dmul_rn(__dmul_rn(T.y, dtr), dtr), I));
         a.z = __dadd_rn(a.z, __ddiv_rn(__dmul_rn(__dmul_rn(T.z, dtr), dtr), I));
     } else {
-        const double km = __ddiv_rn(__dmul_rn(dt, dt), (double)m);
-        const float kI = __fdiv_rn(__fmul_rn(dtr, dtr), I);
+        const double km = mixed_km(dt, (float)m);
+        const float kI = mixed_ki((float)dtr, (float)I);
         d.x = __fma_rn((double)F.x, km, d.x);
         d.y = __fma_rn((double)F.y, km, d.y);
         d.z = __fma_rn((double)F.z, km, d.z);
@@ -945,6 +1040,8 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Re
     float4 q = a.Q[i];
     const Real m = sphere_mass(a.density, r);
     const Real I = (Real)0.4 * m * (r * r);
+    const double km = mixed_km(a.pc.dt, (float)m);
+    const float kI = mixed_ki((float)a.dtr, (float)I);
     for (int s = slot0; s < slot0 + nsteps; s++) {
         if (s == 0) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
@@ -955,7 +1052,10 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Re
             a.dbgC[i] = 0;
         }
         double mz;
-        integrate<Real>(F, T, m, I, a.pc.dt, a.dtr, a.pc.half_skin2, x, d, av, q, flags, mz);
+        if constexpr (sizeof(Real) == 4)   // the factors computed once (the same values integrate computes)
+            integrate_k(F, T, km, kI, a.pc.half_skin2, x, d, av, q, flags, mz);
+        else
+            integrate<Real>(F, T, m, I, a.pc.dt, a.dtr, a.pc.half_skin2, x, d, av, q, flags, mz);
         if (s == observe_slot) mz_obs = mz;
     }
     st_rec(Sout + i, x, d, av, r);
@@ -1174,35 +1274,6 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int
     clear_partials(part, gridDim.x, npart);
 }
 
-// Exclusive scan of in[0, m) into out over the block (m <= a few thousand);
-// returns the total to every thread.  tmp: 33 words of shared memory.
-__device__ __forceinline__ uint block_exscan(const uint* in, uint* out, uint m, uint* tmp) {
-    const uint per = (m + blockDim.x - 1) / blockDim.x;
-    const uint b = threadIdx.x * per, e = min(b + per, m);
-    uint sum = 0;
-    for (uint k = b; k < e; k++) sum += in[k];
-    const uint lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint inc = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint v = __shfl_up_sync(0xffffffffu, inc, o);
-        if ((int)lane >= o) inc += v;
-    }
-    if (lane == 31) tmp[warp] = inc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint acc = 0;
-        for (uint w = 0; w < (blockDim.x >> 5); w++) { const uint t = tmp[w]; tmp[w] = acc; acc += t; }
-        tmp[32] = acc;
-    }
-    __syncthreads();
-    uint run = tmp[warp] + inc - sum;
-    for (uint k = b; k < e; k++) { const uint v = in[k]; out[k] = run; run += v; }
-    const uint total = tmp[32];
-    __syncthreads();
-    return total;
-}
-
 // One block steps whole batches of small components through all K steps of
 // the window in shared memory: per step, the batch's pair items (pair_eval)
 // and wall items (wall_contacts), a block barrier, the batch's particles
@@ -1214,7 +1285,8 @@ __device__ __forceinline__ uint block_exscan(const uint* in, uint* out, uint m, 
 // last step go to `part` (one partial per block; [gridDim.x, clr1) cleared).
 template <typename Real> struct BatchSmem {
     V3<double>* x; V3<double>* d; V3<Real>* a; Real* r; float4* q; V3<double>* wh;
-    uint *gid, *ws, *pb, *pl, *rb, *rl;
+    double* km; float* ki;       // the mixed integrator's factors dt^2/m, dt^2/I
+    uint *gid, *ws, *pb, *pl, *rb, *rl, *wl, *wli;   // wl: wall-candidate flags then slots; wli: their list
     R4<Real>* wf; R4<Real>* wt;
     uint *plo, *phi, *pk, *prv;
     V3<double>* ph;
@@ -1234,8 +1306,11 @@ template <typename Real> __host__ __device__ inline size_t batch_smem_layout(uns
     l.wt = (R4<Real>*)take(P * sizeof(R4<Real>));
     l.a = (V3<Real>*)take(P * sizeof(V3<Real>));
     l.r = (Real*)take(P * sizeof(Real));
+    l.km = (double*)take(P * sizeof(double));
+    l.ki = (float*)take(P * sizeof(float));
     l.gid = (uint*)take(P * 4); l.ws = (uint*)take(P * 4); l.pb = (uint*)take(P * 4);
     l.pl = (uint*)take(P * 4); l.rb = (uint*)take(P * 4); l.rl = (uint*)take(P * 4);
+    l.wl = (uint*)take(P * 4); l.wli = (uint*)take(P * 4);
     l.ph = (V3<double>*)take(Q * sizeof(V3<double>));
     l.fo = (R4<Real>*)take(Q * sizeof(R4<Real>));
     l.ti = (R4<Real>*)take(Q * sizeof(R4<Real>));
@@ -1255,15 +1330,27 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch(StepArgs<Real> a, int K
     BatchSmem<Real> L;
     batch_smem_layout<Real>(smem, &L);
     const long long nb = a.bpos[a.n];
-    const uint nbatch = (uint)((nb + kBatchTarget - 1) / kBatchTarget);
+    const uint tgt = a.ccw[3];
+    const uint nbatch = (uint)((nb + tgt - 1) / tgt);
     double mz = 0.0;
     uint cnt = 0, flags = 0;
     ParticleCommon pc = a.pc;
+    constexpr uint P = BatchCap<Real>::P, Q = BatchCap<Real>::Q;
     for (uint bi = blockIdx.x; bi < nbatch; bi += gridDim.x) {
-        const uint s0 = cbatch[bi], m = cbatch[bi + 1] - s0;
+        const uint s0 = cbatch[bi], s1 = cbatch[bi + 1];
+        // a batch that is not whole components (a re-list that cut it wrongly)
+        // is skipped and reported (capacity status), never stepped; every
+        // test below ends in a block-wide vote, so all threads skip together
+        if (s1 < s0 || s1 > (uint)nb || s1 - s0 > P) {
+            if (threadIdx.x == 0) atomicOr(&a.words->status, kStCapacity);
+            continue;
+        }
+        const uint m = s1 - s0;
+        uint bad = 0;
         // the batch's particles into shared memory
         for (uint p = threadIdx.x; p < m; p += blockDim.x) {
             const uint i = corder[s0 + p];
+            if (i >= (uint)a.n) { bad = 1u; continue; }
             cloc[i] = p;
             L.gid[p] = i;
             V3<double> x, d;
@@ -1274,77 +1361,106 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch(StepArgs<Real> a, int K
             L.q[p] = a.Q[i];
             L.wh[p] = mk(a.W.x[i], a.W.y[i], a.W.z[i]);
             L.ws[p] = a.wslot[i];
+            L.wl[p] = a.wslot[i] != kEmpty ? 1u : 0u;
             L.pl[p] = a.off[i + 1] - a.off[i];
             L.rl[p] = a.roff[i + 1] - a.roff[i];
+            const Real mass = sphere_mass(a.density, r);
+            L.km[p] = mixed_km(a.pc.dt, (float)mass);
+            L.ki[p] = mixed_ki((float)a.dtr, (float)((Real)0.4 * mass * (r * r)));
         }
-        __syncthreads();
+        if (__syncthreads_or(bad)) {
+            if (threadIdx.x == 0) atomicOr(&a.words->status, kStCapacity);
+            continue;
+        }
         const uint npairs = block_exscan(L.pl, L.pb, m, L.scan);
-        block_exscan(L.rl, L.rb, m, L.scan);
-        // the batch's pairs: own rows in list order, reverse rows as pair slots
+        const uint nrev = block_exscan(L.rl, L.rb, m, L.scan);
+        if (npairs > Q || nrev != npairs) {   // not whole components: skipped, reported
+            if (threadIdx.x == 0) atomicOr(&a.words->status, kStCapacity);
+            continue;
+        }
+        const uint nwall = block_exscan(L.wl, L.wl, m, L.scan);   // the batch's wall candidates, listed
+        for (uint p = threadIdx.x; p < m; p += blockDim.x)
+            if (L.ws[p] != kEmpty) L.wli[L.wl[p]] = p;
+        // the batch's pairs: own rows in list order, reverse rows as pair
+        // slots; each partner must be a particle of this batch (and each
+        // particle once in it)
         for (uint p = threadIdx.x; p < m; p += blockDim.x) {
             const uint i = L.gid[p], o0 = a.off[i], b0 = L.pb[p];
+            if (__ldcg(cloc + i) != p) bad = 1u;
             for (uint e = 0; e < L.pl[p]; e++) {
                 const uint k = o0 + e;
+                const uint j = a.ln[k];
+                const uint hi = j < (uint)a.n ? __ldcg(cloc + j) : 0xffffffffu;
+                if (hi >= m || L.gid[hi] != j) { bad = 1u; break; }
                 L.plo[b0 + e] = p;
-                L.phi[b0 + e] = __ldcg(cloc + a.ln[k]);
+                L.phi[b0 + e] = hi;
                 L.pk[b0 + e] = k;
                 L.ph[b0 + e] = mk(a.H.x[k], a.H.y[k], a.H.z[k]);
             }
             const uint r0 = a.roff[i], rb = L.rb[p];
-            for (uint u = 0; u < L.rl[p]; u++) {
+            for (uint u = 0; u < L.rl[p] && !bad; u++) {
                 const uint k = a.rk[r0 + u];
                 const uint lo = a.lp[k];
-                L.prv[rb + u] = L.pb[__ldcg(cloc + lo)] + (k - a.off[lo]);
+                const uint q = lo < (uint)a.n ? __ldcg(cloc + lo) : 0xffffffffu;
+                if (q >= m || L.gid[q] != lo) { bad = 1u; break; }
+                const uint slot = L.pb[q] + (k - a.off[lo]);
+                if (slot >= npairs) { bad = 1u; break; }
+                L.prv[rb + u] = slot;
             }
         }
-        __syncthreads();
+        if (__syncthreads_or(bad)) {
+            if (threadIdx.x == 0) atomicOr(&a.words->status, kStCapacity);
+            continue;
+        }
         for (int st = 0; st < K; st++) {
             const long long ts = a.tx ? (long long)a.tstep0 + st : -1ll;
-            // pair items and wall items (pair_item, wall_item)
-            for (uint e = threadIdx.x; e < npairs; e += blockDim.x) {
-                const uint lo = L.plo[e], hi = L.phi[e];
-                V3<double> h = L.ph[e];
-                if (ts >= 0) {
-                    double* t = a.th + 3 * a.cap * ts;
-                    const uint k = L.pk[e];
-                    t[k] = h.x; t[a.cap + k] = h.y; t[2 * a.cap + k] = h.z;
-                }
-                V3<Real> Fi, Ti, Tj;
-                const int c = pair_eval<Real>(L.x[lo], L.x[hi], L.d[lo], L.d[hi], L.a[lo], L.a[hi], L.r[lo], L.r[hi], h,
-                                              a.pp, a.inv_dt, a.density, Fi, Ti, Tj);
-                L.ph[e] = h;
-                R4<Real> fo;
-                if (c) {
-                    fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
-                    R4<Real> t4;
-                    t4.x = Ti.x; t4.y = Ti.y; t4.z = Ti.z; t4.w = (Real)0;
-                    L.ti[e] = t4;
-                    t4.x = Tj.x; t4.y = Tj.y; t4.z = Tj.z;
-                    L.tj[e] = t4;
+            // pair items and wall items (pair_item, wall_item), one item per thread
+            for (uint u = threadIdx.x; u < npairs + nwall; u += blockDim.x) {
+                if (u < npairs) {
+                    const uint e = u;
+                    const uint lo = L.plo[e], hi = L.phi[e];
+                    V3<double> h = L.ph[e];
+                    if (ts >= 0) {
+                        double* t = a.th + 3 * a.cap * ts;
+                        const uint k = L.pk[e];
+                        t[k] = h.x; t[a.cap + k] = h.y; t[2 * a.cap + k] = h.z;
+                    }
+                    V3<Real> Fi, Ti, Tj;
+                    const int c = pair_eval<Real>(L.x[lo], L.x[hi], L.d[lo], L.d[hi], L.a[lo], L.a[hi], L.r[lo],
+                                                  L.r[hi], h, a.pp, a.inv_dt, a.density, Fi, Ti, Tj);
+                    L.ph[e] = h;
+                    R4<Real> fo;
+                    if (c) {
+                        fo.x = Fi.x; fo.y = Fi.y; fo.z = Fi.z; fo.w = (Real)1;
+                        R4<Real> t4;
+                        t4.x = Ti.x; t4.y = Ti.y; t4.z = Ti.z; t4.w = (Real)0;
+                        L.ti[e] = t4;
+                        t4.x = Tj.x; t4.y = Tj.y; t4.z = Tj.z;
+                        L.tj[e] = t4;
+                    } else {
+                        fo.x = fo.y = fo.z = fo.w = (Real)0;
+                    }
+                    L.fo[e] = fo;
                 } else {
-                    fo.x = fo.y = fo.z = fo.w = (Real)0;
+                    const uint p = L.wli[u - npairs];
+                    const Real r = L.r[p];
+                    const Real mass = a.density * (Real)8 * r * r * r;
+                    V3<double> h = L.wh[p];
+                    if (ts >= 0) {
+                        double* t = a.twh + 3 * a.tnp * ts;
+                        const uint i = L.gid[p];
+                        t[i] = h.x; t[a.tnp + i] = h.y; t[2 * a.tnp + i] = h.z;
+                    }
+                    V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
+                    const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, L.x[p], cvt<Real>(L.d[p]), L.a[p], r, mass,
+                                                        h, a.inv_dt, a.pw, Fw, Tw, (Real*)nullptr);
+                    L.wh[p] = h;
+                    R4<Real> a4, b4;
+                    a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
+                    b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
+                    L.wf[p] = a4;
+                    L.wt[p] = b4;
                 }
-                L.fo[e] = fo;
-            }
-            for (uint p = threadIdx.x; p < m; p += blockDim.x) {
-                if (L.ws[p] == kEmpty) continue;
-                const Real r = L.r[p];
-                const Real mass = a.density * (Real)8 * r * r * r;
-                V3<double> h = L.wh[p];
-                if (ts >= 0) {
-                    double* t = a.twh + 3 * a.tnp * ts;
-                    const uint i = L.gid[p];
-                    t[i] = h.x; t[a.tnp + i] = h.y; t[2 * a.tnp + i] = h.z;
-                }
-                V3<Real> Fw = zero3<Real>(), Tw = zero3<Real>();
-                const int hit = wall_contacts<Real>(a.pc.hx, a.pc.hy, L.x[p], cvt<Real>(L.d[p]), L.a[p], r, mass, h,
-                                                    a.inv_dt, a.pw, Fw, Tw, (Real*)nullptr);
-                L.wh[p] = h;
-                R4<Real> a4, b4;
-                a4.x = Fw.x; a4.y = Fw.y; a4.z = Fw.z; a4.w = hit ? (Real)1 : (Real)0;
-                b4.x = Tw.x; b4.y = Tw.y; b4.z = Tw.z; b4.w = (Real)0;
-                L.wf[p] = a4;
-                L.wt[p] = b4;
             }
             __syncthreads();
             // particles (bound_item, particle_finish)
@@ -1400,7 +1516,10 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch(StepArgs<Real> a, int K
                 if (pc.first) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }
                 const uint wflag = __float_as_uint(q.w);
                 double mzi;
-                integrate<Real>(F, T, mass, I, pc.dt, a.dtr, pc.half_skin2, x, d, av, q, flags, mzi);
+                if constexpr (sizeof(Real) == 4)
+                    integrate_k(F, T, L.km[p], L.ki[p], pc.half_skin2, x, d, av, q, flags, mzi);
+                else
+                    integrate<Real>(F, T, mass, I, pc.dt, a.dtr, pc.half_skin2, x, d, av, q, flags, mzi);
                 q.w = __uint_as_float(wflag);
                 L.x[p] = x; L.d[p] = d; L.a[p] = av; L.q[p] = q;
                 if (st == K - 1) { mz = fmax(mz, mzi); cnt += ci; }
@@ -1500,6 +1619,107 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     if (i < n)
         pp_item<Real, false>(i, r, total, o0, o1, r0, r1, rk, lp, ln, cap, Si, So, Q, W, Hi, Ho, pp, pw, pc, dtr, inv_dt,
                              density, mz, cnt, flags, dbgF, dbgT, dbgC);
+    block_observables(mz, cnt, flags, pc.observe, part, words);
+    if (pc.observe) clear_partials(part, clr0, clr1);
+}
+
+// PP step with G lanes per particle (the default PP step): the lanes of a
+// group evaluate the particle's pairs side by side -- own row then reverse
+// row, entry e on lane e mod G -- and the group's first lane adds the results
+// in list order (ordered shuffles), then runs particle_finish.  The same
+// pair_eval calls with the same arguments and the same sums in the same order
+// as pp_item, so the states are bit-identical to k_step_pp's; only the
+// latency of a particle's pair chain is spread over its lanes (the serial
+// loop of k_step_pp holds a dense bed's step at ~6 dependent laws).  Groups
+// stride over the particles (the grid has as many blocks as k_step_pp, so the
+// per-block partials keep their count); each warp loops while its first
+// group has a particle, so every shuffle sees all 32 lanes.
+template <typename Real, int G>
+__global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_ppg(
+    long long n, const uint* __restrict__ off, const uint* __restrict__ roff, const uint* __restrict__ rk,
+    const uint* __restrict__ lp, const uint* __restrict__ ln, long long cap, const PRec<Real>* __restrict__ Si,
+    PRec<Real>* __restrict__ So, const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
+    Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp, LawParams<Real> pw, ParticleCommon pc, Real dtr,
+    Real inv_dt, Real density, StepPartials part, EngineWords* words, double* dbgF, double* dbgT, uint* dbgC,
+    size_t clr0, size_t clr1) {
+    static_assert(32 % G == 0, "a group lies inside a warp");
+    pdl_trigger();
+    const uint lane = threadIdx.x & 31, g = lane % G;
+    const long long gid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const long long stride = (long long)gridDim.x * blockDim.x / G;
+    const long long wfirst = gid - lane / G;   // the warp's first group
+    double mz = 0.0;
+    uint cnt = 0, flags = 0;
+    pdl_wait();
+    const uint total = off[n];
+    const bool listed = (long long)total <= cap;
+    for (long long i = gid, w0 = wfirst; w0 < n; i += stride, w0 += stride) {
+        const bool act = i < n;
+        V3<double> x = zero3<double>(), d = zero3<double>();
+        V3<Real> a = zero3<Real>();
+        Real r = (Real)0, rr;
+        uint o0 = 0, no = 0, r0 = 0, nr = 0;
+        if (act) {
+            r = R[i];
+            ld_rec<false>(Si + i, x, d, a, rr);
+            if (listed) {
+                o0 = off[i]; no = off[i + 1] - o0;
+                r0 = roff[i]; nr = roff[i + 1] - r0;
+            }
+        }
+        const uint ne = no + nr;
+        const uint nch = __reduce_max_sync(0xffffffffu, (ne + G - 1) / G);
+        V3<Real> F = zero3<Real>(), T = zero3<Real>();
+        uint ci = 0;
+        for (uint ch = 0; ch < nch; ch++) {
+            const uint e = ch * G + g;
+            V3<Real> Fe = zero3<Real>(), Te = zero3<Real>();
+            uint ce = 0;
+            if (e < ne) {
+                V3<double> xj, dj, h;
+                V3<Real> aj, Fl, Tl, Th;
+                Real rj;
+                if (e < no) {   // own row: this particle is lo
+                    const uint k = o0 + e;
+                    const uint j = ln[k];
+                    h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
+                    ld_rec<false>(Si + j, xj, dj, aj, rj);
+                    ce = pair_eval<Real>(x, xj, d, dj, a, aj, r, rj, h, pp, inv_dt, density, Fl, Tl, Th);
+                    Ho.x[k] = h.x; Ho.y[k] = h.y; Ho.z[k] = h.z;
+                    if (ce) { Fe = Fl; Te = Tl; }
+                } else {        // reverse row: this particle is hi
+                    const uint k = rk[r0 + (e - no)];
+                    if (k < total) {
+                        const uint j = lp[k];
+                        h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
+                        ld_rec<false>(Si + j, xj, dj, aj, rj);
+                        ce = pair_eval<Real>(xj, x, dj, d, aj, a, rj, r, h, pp, inv_dt, density, Fl, Tl, Th);
+                        if (ce) { Fe = mk(-Fl.x, -Fl.y, -Fl.z); Te = Th; }
+                    }
+                }
+            }
+            // the group's first lane adds the entries in list order
+#pragma unroll
+            for (int l = 0; l < G; l++) {
+                const uint cl = __shfl_sync(0xffffffffu, ce, l, G);
+                const Real fx = __shfl_sync(0xffffffffu, Fe.x, l, G), fy = __shfl_sync(0xffffffffu, Fe.y, l, G),
+                           fz = __shfl_sync(0xffffffffu, Fe.z, l, G);
+                const Real tx = __shfl_sync(0xffffffffu, Te.x, l, G), ty = __shfl_sync(0xffffffffu, Te.y, l, G),
+                           tz = __shfl_sync(0xffffffffu, Te.z, l, G);
+                if (cl) {
+                    F.x += fx; F.y += fy; F.z += fz;
+                    T.x += tx; T.y += ty; T.z += tz;
+                    ci++;
+                }
+            }
+        }
+        if (act && g == 0) {
+            const float4 q = Q[i];
+            particle_finish<Real, true>(i, F, T, r, x, d, a, q, So, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, ci,
+                                        dbgF, dbgT, dbgC);
+            cnt += ci;
+        }
+    }
     block_observables(mz, cnt, flags, pc.observe, part, words);
     if (pc.observe) clear_partials(part, clr0, clr1);
 }
@@ -1679,7 +1899,12 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     GridC g = c->grid;
     DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
     const bool cc = c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent;
-    if (cc) DEM_CUDA_TRY(cudaMemsetAsync(c->cc_words, 0, 4 * sizeof(uint), s));
+    if (cc) {
+        const size_t nbb = (size_t)c->nbatch_max + 2;
+        DEM_CUDA_TRY(cudaMemsetAsync(c->cc_words, 0, 4 * sizeof(uint), s));
+        DEM_CUDA_TRY(cudaMemsetAsync(c->cc_bw, 0xff, nbb * sizeof(uint), s));
+        DEM_CUDA_TRY(cudaMemsetAsync(c->cc_bw + nbb, 0, 2 * nbb * sizeof(uint), s));
+    }
     k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, S, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
                                                     c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
                                                     c->wslot, c->wlist, c->wcount, cc ? c->cc_parent : nullptr,
@@ -1709,23 +1934,23 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         c->njli, c->ln[dst], c->lp, planes<double>(c->hist[dst][0], c->cap), (const uint*)c->off[src],
         (const uint*)c->ln[src], planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap,
         c->words, c->carry, (const uint*)c->scr, (const uint*)c->bflag, (const uint*)c->bpos, c->blist, c->flist,
-        (const uint*)c->tpos));
+        (const uint*)c->tpos, cc ? c->cc_parent : nullptr, (const uint*)c->cc_skip));
     DEM_CUDA_TRY(launch_ex(k_rev_sort, grid_for(n, B), B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
-                           (const uint*)c->off[dst], c->cap));
+                           (const uint*)c->off[dst], c->cap, cc ? c->cc_parent : nullptr, (const uint*)c->bflag,
+                           c->cc_size, c->cc_pairs, (const uint*)c->cc_skip));
     if (cc) {   // the window's components and batches (cluster-batched window path)
         const uint* off = c->off[dst];
-        DEM_CUDA_TRY(launch_ex(k_cc_union, (unsigned)std::min<long long>(grid_for(c->cap, B), 148LL * 16), B, s, pdl, n,
-                               c->cap, off, (const uint*)c->lp, (const uint*)c->ln[dst], c->cc_parent));
-        DEM_CUDA_TRY(launch_ex(k_cc_count, grid_for(n, B), B, s, pdl, n, c->cap, (const uint*)c->blist,
-                               (const uint*)c->bpos, off, c->cc_parent, c->cc_size, c->cc_pairs, c->cc_words));
-        DEM_CUDA_TRY(launch_ex(k_cc_base, grid_for(n, B), B, s, pdl, n, (const uint*)c->blist, (const uint*)c->bpos,
-                               (const uint*)c->cc_parent, (const uint*)c->cc_size, c->cc_base, c->cc_start,
-                               c->cc_words));
-        DEM_CUDA_TRY(launch_ex(k_cc_slot, grid_for(n, B), B, s, pdl, n, (const uint*)c->blist, (const uint*)c->bpos,
-                               (const uint*)c->cc_parent, (const uint*)c->cc_base, c->cc_fill, c->cc_order));
-        DEM_CUDA_TRY(launch_ex(k_cc_batches, grid_for(c->nbatch_max + 1, B), B, s, pdl, n, c->nbatch_max,
-                               BatchCap<Real>::P, BatchCap<Real>::Q, (const uint*)c->bpos, (const uint*)c->cc_start,
-                               (const uint*)c->cc_order, off, c->cc_batch, c->cc_words));
+        const long long nbb = c->nbatch_max + 2;
+        DEM_CUDA_TRY(launch_ex(k_cc_base, grid_for(n, B), B, s, pdl, n, c->cap, (const uint*)c->blist,
+                               (const uint*)c->bpos, off, (const uint*)c->cc_parent, (const uint*)c->cc_size,
+                               c->cc_base, c->cc_words, (const uint*)c->cc_skip));
+        DEM_CUDA_TRY(launch_ex(k_cc_slot, grid_for(n, B), B, s, pdl, n, nbb, c->batch_grid, BatchCap<Real>::P,
+                               (const uint*)c->blist, (const uint*)c->bpos, (const uint*)c->cc_parent,
+                               (const uint*)c->cc_base, (const uint*)c->cc_size, (const uint*)c->cc_pairs, c->cc_fill,
+                               c->cc_order, c->cc_bw, c->cc_words));
+        DEM_CUDA_TRY(launch_ex(k_cc_batches, grid_for(c->nbatch_max + 1, B), B, s, pdl, n, c->nbatch_max, nbb,
+                               BatchCap<Real>::P, BatchCap<Real>::Q, (const uint*)c->bpos, (const uint*)c->cc_bw,
+                               c->cc_batch, c->cc_words, c->cc_skip));
     }
     return DEM_OK;
 }
@@ -1877,7 +2102,6 @@ template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const Wi
     return DEM_OK;
 }
 
-bool use_batches(const dem_ctx* c) { return c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent != nullptr; }
 
 // PP step: reads state buffer sbuf and history phase hph, writes the others.
 template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, int hp) {
@@ -1885,7 +2109,8 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
     LawParams<Real> pp = make_law<Real>(c->mat.pp), pw = make_law<Real>(c->mat.pw);
     const double dt = c->cfg.dt;
     DEM_CUDA_TRY(launch_ex(
-        k_step_pp<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, true), n, (const uint*)c->off[lst],
+        c->pp_group ? k_step_ppg<Real, kPPLanes> : k_step_pp<Real>, grid_for(n, 256), 256, c->stream,
+        step_pdl(c, slot, true), n, (const uint*)c->off[lst],
         (const uint*)c->roff, (const uint*)c->rk, (const uint*)c->lp, (const uint*)c->ln[lst], c->cap,
         (const PRec<Real>*)c->rec[sb], (PRec<Real>*)c->rec[1 - sb], (const Real*)c->rad, c->q,
         planes<double>(c->wh, np), planes<double>(c->hist[lst][hp], c->cap),
@@ -1898,6 +2123,8 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
 }  // namespace
 
 namespace dem {
+bool use_batches(const dem_ctx* c) { return c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent != nullptr; }
+
 int window_kernel(dem_ctx* c, int lst, const WindowTape* tape) {
     NvtxRange r("dem window kernel");
     if (use_batches(c))
@@ -2184,6 +2411,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_grid = (unsigned)std::max(1, nsm * wper);
         const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
+        const char* ppg = getenv("DEM_B200_PPG");   // "0": the PP step with one thread per particle
+        c->pp_group = !(ppg && ppg[0] == '0');
         const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches everywhere
         c->pdl = !(pdl && pdl[0] == '0');
         const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order
@@ -2206,7 +2435,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
             if (e != cudaSuccess) return bail(cuda_fail(e, "batch kernel set-up", __FILE__, __LINE__));
             c->batching = bper > 0;
             c->batch_grid = (unsigned)std::max<long long>(1, std::min<long long>((long long)nsm * bper, grid_for(n, 256)));
-            c->nbatch_max = (np + kBatchTarget - 1) / kBatchTarget + 1;
+            c->nbatch_max = (np + kBatchMin - 1) / kBatchMin + 1;
         }
     }
     // partials per slot: particle-kernel blocks, free-kernel blocks, and at
@@ -2220,14 +2449,15 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         e = cudaMemsetAsync(c->part_cnt, 0, (size_t)cfg->relist_interval * c->npart * sizeof(uint), s0);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (partials)", __FILE__, __LINE__));
     if (c->batching) {
-        if ((rc = dalloc(&c->cc_parent, np)) || (rc = dalloc(&c->cc_size, 4 * np)) || (rc = dalloc(&c->cc_base, np)) ||
+        if ((rc = dalloc(&c->cc_parent, np)) || (rc = dalloc(&c->cc_size, 3 * np)) || (rc = dalloc(&c->cc_base, np)) ||
             (rc = dalloc(&c->cc_order, np)) || (rc = dalloc(&c->cc_batch, c->nbatch_max + 2)) ||
-            (rc = dalloc(&c->cc_loc, np)) || (rc = dalloc(&c->cc_words, 4)))
+            (rc = dalloc(&c->cc_loc, np)) || (rc = dalloc(&c->cc_words, 4)) || (rc = dalloc(&c->cc_skip, 2)) ||
+            (rc = dalloc(&c->cc_bw, 3 * (c->nbatch_max + 2))))
             return bail(rc);
         c->cc_pairs = c->cc_size + np;
         c->cc_fill = c->cc_size + 2 * np;
-        c->cc_start = c->cc_size + 3 * np;
         e = cudaMemsetAsync(c->cc_words, 0, 4 * sizeof(uint), s0);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->cc_skip, 0, 2 * sizeof(uint), s0);
         if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMemset (batch words)", __FILE__, __LINE__));
     }
     c->scan_words = 3 * scan_scratch_words(std::max<long long>(np + 1, 1));
@@ -2267,7 +2497,7 @@ int dem_destroy(dem_ctx* c) {
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
                     c->scr, c->bflag, c->bpos, c->blist, c->flist, c->bar,
                     c->tpos, c->pour_rec, c->perm, c->cc_parent, c->cc_size, c->cc_base, c->cc_order,
-                    c->cc_batch, c->cc_loc, c->cc_words};
+                    c->cc_batch, c->cc_loc, c->cc_words, c->cc_bw, c->cc_skip};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
@@ -2349,6 +2579,7 @@ static int finish_upload(dem_ctx* c) {
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[0], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[1], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->words, 0, sizeof(EngineWords), c->stream));
+    if (c->cc_skip) DEM_CUDA_TRY(cudaMemsetAsync(c->cc_skip, 0, 2 * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->part_mz, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(unsigned long long),
                                  c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->part_cnt, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(uint), c->stream));

@@ -110,6 +110,50 @@ struct ParticleCommon {
     int observe;   // write this step's per-block observables (max height, contacts)
 };
 
+// Cluster batches: batches of whole components, at most BatchCap<Real>::P
+// particles and ::Q listed pairs each (what one block holds in shared memory,
+// forward and reverse).  A batch takes the components whose first slot falls
+// in one window of `target` slots; the re-list chooses target per window as
+// the bound particles over the batch kernel's resident blocks (one round of
+// blocks), at least kBatchMin and at most P minus the largest component.
+constexpr uint kBatchMin = 32;
+constexpr int kPPLanes = 8;
+constexpr uint kDenseSkip = 32;          // re-lists without the component pass after one larger than a block              // lanes per particle of the grouped PP step (k_step_ppg)
+constexpr int kBatchThreads = 512;       // k_batch: one particle per thread
+constexpr int kAdjBatchThreads = 256;    // k_adj_batch (its FP64 reverse needs the registers)
+template <typename Real> struct BatchCap;
+template <> struct BatchCap<float> { static constexpr uint P = 512, Q = 640; };
+template <> struct BatchCap<double> { static constexpr uint P = 384, Q = 640; };
+
+// Exclusive scan of in[0, m) into out over the block (m <= a few thousand);
+// returns the total to every thread.  tmp: 33 words of shared memory.
+__device__ __forceinline__ uint block_exscan(const uint* in, uint* out, uint m, uint* tmp) {
+    const uint per = (m + blockDim.x - 1) / blockDim.x;
+    const uint b = threadIdx.x * per, e = min(b + per, m);
+    uint sum = 0;
+    for (uint k = b; k < e; k++) sum += in[k];
+    const uint lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint v = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)lane >= o) inc += v;
+    }
+    if (lane == 31) tmp[warp] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint acc = 0;
+        for (uint w = 0; w < (blockDim.x >> 5); w++) { const uint t = tmp[w]; tmp[w] = acc; acc += t; }
+        tmp[32] = acc;
+    }
+    __syncthreads();
+    uint run = tmp[warp] + inc - sum;
+    for (uint k = b; k < e; k++) { const uint v = in[k]; out[k] = run; run += v; }
+    const uint total = tmp[32];
+    __syncthreads();
+    return total;
+}
+
 }  // namespace dem
 
 using dem::EngineWords;
@@ -196,16 +240,19 @@ struct dem_ctx {
     // connected component of the pair list; small components are packed into
     // batches that one block steps through the whole window in shared memory
     bool batching = true;            // DEM_B200_BATCH=0: the grid-barrier window kernel for every window
+    bool pp_group = true;            // PP step with kPPLanes lanes per particle (DEM_B200_PPG=0: one thread)
     uint* cc_parent = nullptr;       // np: union-find parent, then the component root (its smallest id)
     uint* cc_size = nullptr;         // np: per root: bound particles of the component
     uint* cc_pairs = nullptr;        // np: per root: listed pairs of the component
     uint* cc_fill = nullptr;         // np: per root: slots handed out so far
     uint* cc_base = nullptr;         // np: per root: the component's first slot
-    uint* cc_start = nullptr;        // np + 1: 1 at each component's first slot
+    uint* cc_bw = nullptr;           // 3 (nbatch_max + 2): per batch first slot, particles, pairs
     uint* cc_order = nullptr;        // np: bound particle ids, grouped by component
     uint* cc_batch = nullptr;        // nbatch_max + 1: first slot of each batch
     uint* cc_loc = nullptr;          // np: a batch particle's index inside its block
-    uint* cc_words = nullptr;        // [0] slots handed out, [1] 1 = a component or batch too large
+    uint* cc_skip = nullptr;         // [0] re-lists left that skip the component pass (a dense bed)
+    uint* cc_words = nullptr;        // [0] slots handed out, [1] 1 = a batch too large (or the list overflowed),
+                                     // [2] largest component, [3] batch window (slots)
     long long nbatch_max = 0;
     unsigned batch_grid = 1;         // blocks of the batch kernel
     size_t batch_smem = 0;           // its dynamic shared memory
@@ -270,6 +317,8 @@ namespace dem {
 int relist(dem_ctx* c, int src);
 int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part);
 int window_kernel(dem_ctx* c, int lst, const WindowTape* tape);
+// Whether PCCP windows run as cluster batches (set at dem_create).
+bool use_batches(const dem_ctx* c);
 // The host copy of the particle order (c->hperm), fetched from the device
 // (one copy and a stream wait) when an upload computed a new one.
 int host_perm(dem_ctx* c);

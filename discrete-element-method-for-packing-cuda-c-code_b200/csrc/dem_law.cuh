@@ -56,7 +56,10 @@ DEM_HD void contact_law(F delta, V3<F> n, F rstar, F mstar, V3<F> U, V3<F> Wr, V
     xi = (xi - xn * nd) + cvt<double>(Ut);
     if (p.mu > F(0)) {
         const F xmax = p.xfac * delta;
-        const double xim_d = sqrt(dot(xi, xi));
+        // |xi| in the force's precision (FP32 in the mixed form: the history
+        // itself stays FP64, its length and the slip rescale are FP32-exact)
+        const double xx = dot(xi, xi);
+        const double xim_d = sizeof(F) == 4 ? (double)dsqrt((F)xx) : sqrt(xx);
         const F xim = (F)xim_d;
         const F s = (xim < xmax ? xim : xmax) / xmax;
         const F oms = F(1) - s;
@@ -68,7 +71,7 @@ DEM_HD void contact_law(F delta, V3<F> n, F rstar, F mstar, V3<F> U, V3<F> Wr, V
         const F ftm = dsqrt(dot(Ft, Ft));
         const F cap = p.mu * fn_e;
         if (ftm > cap) Ft = Ft * (cap / ftm);
-        if (xim_d > (double)xmax) xi = xi * ((double)xmax / xim_d);
+        if (xim_d > (double)xmax) xi = xi * (sizeof(F) == 4 ? (double)(xmax / xim) : (double)xmax / xim_d);
     } else {
         Ft = zero3<F>();
         xi = zero3<double>();

@@ -13,7 +13,7 @@ oracle (the CPU restatement of the reference step), with the errors stated.
 * 50,000 lognormal spheres pre-settled 20,000 steps, then the 2,000-step
   mixed window with checkpoints every 100: gradients of the potential energy
   with respect to sliding and rolling friction against central differences
-  (step 1e-4 relative) of the GPU forward and of the FP64 oracle.
+  of the GPU forward and of the FP64 oracle.
 
 The packing-fraction objective has zero friction gradients on that window:
 it is sum (4/3) pi r^3 / (Wx Wy max z), and the highest sphere is in free
@@ -144,11 +144,13 @@ def test_config5_friction_gradients(dem, orc, wl, cuda):
     precision) and of the FP64 oracle (from the same pre-settled state).  The
     differences subtract the two runs' energies particle by particle (the
     gravity term is ~1e6 times the gradient).  Tolerance 1e-3 relative for
-    the sliding friction; the rolling-friction gradient is 2e-6 of the
-    sliding one here (only the few spheres that bounced off the floor roll),
-    and its FP32 forward differences carry the torques' rounding, so it is
-    held to 1e-2 relative against the FP64 oracle and 5e-2 against the mixed
-    forward."""
+    the sliding friction.  The rolling-friction gradient is 5e-4 of the
+    sliding one here (only the few spheres that bounced off the floor roll):
+    against the FP64 oracle's differences (step 1e-4) it is held to 1e-2
+    relative; the mixed forward's differences at step 1e-4 are dominated by
+    the FP32 torques' rounding (the energy change is ~1e-8 of a 4e6
+    objective), so the GPU differences for it take the step 1e-2 and the
+    tolerance 5e-2."""
     w = wl.settle_50k()
     s0, (pos, pdis, angv), cell = run_engine(dem, w, dem.PREC_MIXED, w.meta["presettle_steps"])
     assert s0["status"] == 0
@@ -183,14 +185,17 @@ def test_config5_friction_gradients(dem, orc, wl, cuda):
 
     base = adjoint(w.pp, w.pw)
     assert base["value"] > 0
-    h = 1e-4
+    h_or = 1e-4
+    h_gpu = {"mu": 1e-4, "roll_rel": 1e-2}
     rows = []
     for key in ("mu", "roll_rel"):
         g_ad = (base["d_pp"][key] * w.pp[key] + base["d_pw"][key] * w.pw[key])   # d/d(log parameter)
-        pp_p, pw_p = scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h)
-        pp_m, pw_m = scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h)
-        g_fd = central_difference(gpu_parts(pp_p, pw_p), gpu_parts(pp_m, pw_m), h)
-        g_or = central_difference(oracle_parts(pp_p, pw_p), oracle_parts(pp_m, pw_m), h)
+        h = h_gpu[key]
+        g_fd = central_difference(gpu_parts(scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h)),
+                                  gpu_parts(scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h)), h)
+        h = h_or
+        g_or = central_difference(oracle_parts(scaled(w.pp, key, 1 + h), scaled(w.pw, key, 1 + h)),
+                                  oracle_parts(scaled(w.pp, key, 1 - h), scaled(w.pw, key, 1 - h)), h)
         print(f"\nconfig5 d U / d log {key}: adjoint {g_ad:.6e}  GPU FD {g_fd:.6e}  oracle FD {g_or:.6e}  "
               f"(U {base['value']:.6e})")
         rows.append((key, g_ad, g_fd, g_or))

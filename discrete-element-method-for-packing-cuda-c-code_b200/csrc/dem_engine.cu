@@ -1623,107 +1623,6 @@ __global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_pp(
     if (pc.observe) clear_partials(part, clr0, clr1);
 }
 
-// PP step with G lanes per particle (the default PP step): the lanes of a
-// group evaluate the particle's pairs side by side -- own row then reverse
-// row, entry e on lane e mod G -- and the group's first lane adds the results
-// in list order (ordered shuffles), then runs particle_finish.  The same
-// pair_eval calls with the same arguments and the same sums in the same order
-// as pp_item, so the states are bit-identical to k_step_pp's; only the
-// latency of a particle's pair chain is spread over its lanes (the serial
-// loop of k_step_pp holds a dense bed's step at ~6 dependent laws).  Groups
-// stride over the particles (the grid has as many blocks as k_step_pp, so the
-// per-block partials keep their count); each warp loops while its first
-// group has a particle, so every shuffle sees all 32 lanes.
-template <typename Real, int G>
-__global__ void __launch_bounds__(256, DEM_PP_MINB) k_step_ppg(
-    long long n, const uint* __restrict__ off, const uint* __restrict__ roff, const uint* __restrict__ rk,
-    const uint* __restrict__ lp, const uint* __restrict__ ln, long long cap, const PRec<Real>* __restrict__ Si,
-    PRec<Real>* __restrict__ So, const Real* __restrict__ R, float4* __restrict__ Q, Planes3<double> W,
-    Planes3<double> Hi, Planes3<double> Ho, LawParams<Real> pp, LawParams<Real> pw, ParticleCommon pc, Real dtr,
-    Real inv_dt, Real density, StepPartials part, EngineWords* words, double* dbgF, double* dbgT, uint* dbgC,
-    size_t clr0, size_t clr1) {
-    static_assert(32 % G == 0, "a group lies inside a warp");
-    pdl_trigger();
-    const uint lane = threadIdx.x & 31, g = lane % G;
-    const long long gid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-    const long long stride = (long long)gridDim.x * blockDim.x / G;
-    const long long wfirst = gid - lane / G;   // the warp's first group
-    double mz = 0.0;
-    uint cnt = 0, flags = 0;
-    pdl_wait();
-    const uint total = off[n];
-    const bool listed = (long long)total <= cap;
-    for (long long i = gid, w0 = wfirst; w0 < n; i += stride, w0 += stride) {
-        const bool act = i < n;
-        V3<double> x = zero3<double>(), d = zero3<double>();
-        V3<Real> a = zero3<Real>();
-        Real r = (Real)0, rr;
-        uint o0 = 0, no = 0, r0 = 0, nr = 0;
-        if (act) {
-            r = R[i];
-            ld_rec<false>(Si + i, x, d, a, rr);
-            if (listed) {
-                o0 = off[i]; no = off[i + 1] - o0;
-                r0 = roff[i]; nr = roff[i + 1] - r0;
-            }
-        }
-        const uint ne = no + nr;
-        const uint nch = __reduce_max_sync(0xffffffffu, (ne + G - 1) / G);
-        V3<Real> F = zero3<Real>(), T = zero3<Real>();
-        uint ci = 0;
-        for (uint ch = 0; ch < nch; ch++) {
-            const uint e = ch * G + g;
-            V3<Real> Fe = zero3<Real>(), Te = zero3<Real>();
-            uint ce = 0;
-            if (e < ne) {
-                V3<double> xj, dj, h;
-                V3<Real> aj, Fl, Tl, Th;
-                Real rj;
-                if (e < no) {   // own row: this particle is lo
-                    const uint k = o0 + e;
-                    const uint j = ln[k];
-                    h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
-                    ld_rec<false>(Si + j, xj, dj, aj, rj);
-                    ce = pair_eval<Real>(x, xj, d, dj, a, aj, r, rj, h, pp, inv_dt, density, Fl, Tl, Th);
-                    Ho.x[k] = h.x; Ho.y[k] = h.y; Ho.z[k] = h.z;
-                    if (ce) { Fe = Fl; Te = Tl; }
-                } else {        // reverse row: this particle is hi
-                    const uint k = rk[r0 + (e - no)];
-                    if (k < total) {
-                        const uint j = lp[k];
-                        h = mk(Hi.x[k], Hi.y[k], Hi.z[k]);
-                        ld_rec<false>(Si + j, xj, dj, aj, rj);
-                        ce = pair_eval<Real>(xj, x, dj, d, aj, a, rj, r, h, pp, inv_dt, density, Fl, Tl, Th);
-                        if (ce) { Fe = mk(-Fl.x, -Fl.y, -Fl.z); Te = Th; }
-                    }
-                }
-            }
-            // the group's first lane adds the entries in list order
-#pragma unroll
-            for (int l = 0; l < G; l++) {
-                const uint cl = __shfl_sync(0xffffffffu, ce, l, G);
-                const Real fx = __shfl_sync(0xffffffffu, Fe.x, l, G), fy = __shfl_sync(0xffffffffu, Fe.y, l, G),
-                           fz = __shfl_sync(0xffffffffu, Fe.z, l, G);
-                const Real tx = __shfl_sync(0xffffffffu, Te.x, l, G), ty = __shfl_sync(0xffffffffu, Te.y, l, G),
-                           tz = __shfl_sync(0xffffffffu, Te.z, l, G);
-                if (cl) {
-                    F.x += fx; F.y += fy; F.z += fz;
-                    T.x += tx; T.y += ty; T.z += tz;
-                    ci++;
-                }
-            }
-        }
-        if (act && g == 0) {
-            const float4 q = Q[i];
-            particle_finish<Real, true>(i, F, T, r, x, d, a, q, So, Q, W, pw, pc, dtr, inv_dt, density, mz, flags, ci,
-                                        dbgF, dbgT, dbgC);
-            cnt += ci;
-        }
-    }
-    block_observables(mz, cnt, flags, pc.observe, part, words);
-    if (pc.observe) clear_partials(part, clr0, clr1);
-}
-
 // PP window kernel (one cooperative launch per window, as k_window, with the
 // same split of its blocks): per step, every bound particle runs pp_item from
 // the "in" buffers into the "out" buffers, one barrier among the bound blocks
@@ -2109,8 +2008,7 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
     LawParams<Real> pp = make_law<Real>(c->mat.pp), pw = make_law<Real>(c->mat.pw);
     const double dt = c->cfg.dt;
     DEM_CUDA_TRY(launch_ex(
-        c->pp_group ? k_step_ppg<Real, kPPLanes> : k_step_pp<Real>, grid_for(n, 256), 256, c->stream,
-        step_pdl(c, slot, true), n, (const uint*)c->off[lst],
+        k_step_pp<Real>, grid_for(n, 256), 256, c->stream, step_pdl(c, slot, true), n, (const uint*)c->off[lst],
         (const uint*)c->roff, (const uint*)c->rk, (const uint*)c->lp, (const uint*)c->ln[lst], c->cap,
         (const PRec<Real>*)c->rec[sb], (PRec<Real>*)c->rec[1 - sb], (const Real*)c->rad, c->q,
         planes<double>(c->wh, np), planes<double>(c->hist[lst][hp], c->cap),
@@ -2411,8 +2309,6 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_grid = (unsigned)std::max(1, nsm * wper);
         const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
-        const char* ppg = getenv("DEM_B200_PPG");   // "0": the PP step with one thread per particle
-        c->pp_group = !(ppg && ppg[0] == '0');
         const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches everywhere
         c->pdl = !(pdl && pdl[0] == '0');
         const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order

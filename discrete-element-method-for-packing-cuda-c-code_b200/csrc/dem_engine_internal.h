@@ -117,8 +117,7 @@ struct ParticleCommon {
 // the bound particles over the batch kernel's resident blocks (one round of
 // blocks), at least kBatchMin and at most P minus the largest component.
 constexpr uint kBatchMin = 32;
-constexpr int kPPLanes = 8;
-constexpr uint kDenseSkip = 32;          // re-lists without the component pass after one larger than a block              // lanes per particle of the grouped PP step (k_step_ppg)
+constexpr uint kDenseSkip = 32;          // re-lists without the component pass after one larger than a block
 constexpr int kBatchThreads = 512;       // k_batch: one particle per thread
 constexpr int kAdjBatchThreads = 256;    // k_adj_batch (its FP64 reverse needs the registers)
 template <typename Real> struct BatchCap;
@@ -240,7 +239,6 @@ struct dem_ctx {
     // connected component of the pair list; small components are packed into
     // batches that one block steps through the whole window in shared memory
     bool batching = true;            // DEM_B200_BATCH=0: the grid-barrier window kernel for every window
-    bool pp_group = true;            // PP step with kPPLanes lanes per particle (DEM_B200_PPG=0: one thread)
     uint* cc_parent = nullptr;       // np: union-find parent, then the component root (its smallest id)
     uint* cc_size = nullptr;         // np: per root: bound particles of the component
     uint* cc_pairs = nullptr;        // np: per root: listed pairs of the component

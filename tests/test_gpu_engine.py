@@ -369,41 +369,6 @@ def test_window_kernel_equals_per_step_kernels(dem, wl, cuda, monkeypatch, prec,
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_grouped_pp_step_equals_one_thread_pp_step(dem, wl, cuda, monkeypatch, prec):
-    """The PP step with a group of lanes per particle (the default: the
-    particle's pairs evaluated side by side, added in list order by the
-    group's first lane) and with one thread per particle (DEM_B200_PPG=0)
-    agree bit for bit -- states, pair histories, observables -- per-step
-    kernels on a sparse bed and on a dense lattice (rows longer than a
-    group)."""
-    from _cases import dense_lattice
-    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
-    monkeypatch.setenv("DEM_B200_WINDOW", "0")
-    for w, dense in ((wl.small_box(n=3000), False), (dense_lattice(dem, nx=10, ny=10, nz=8), True)):
-        rng = np.random.default_rng(5)
-        pdis = rng.normal(0, 2e-6, 3 * w.n)
-        angv = rng.normal(0, 2e-5, 3 * w.n)
-        a = make_engine(dem, w, p, force_mode=dem.FORCE_PP)
-        a.upload(w.pos, w.rad, pdis, angv)
-        monkeypatch.setenv("DEM_B200_PPG", "0")
-        b = make_engine(dem, w, p, force_mode=dem.FORCE_PP)
-        b.upload(w.pos, w.rad, pdis, angv)
-        monkeypatch.delenv("DEM_B200_PPG")
-        a.step(3 * w.relist_interval + 7)
-        b.step(3 * w.relist_interval + 7)
-        for x, y in zip(a.download(), b.download()):
-            np.testing.assert_array_equal(x, y)
-        for x, y in zip(a.pairs(), b.pairs()):
-            np.testing.assert_array_equal(x, y)
-        sa, sb = a.scalars(), b.scalars()
-        assert sa["status"] == 0 and sb["status"] == 0
-        assert sa["maxhz"] == sb["maxhz"] and sa["contacts"] == sb["contacts"]
-        assert sa["contacts"] > 0 or not dense
-        a.close()
-        b.close()
-
-
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_cluster_batches_equal_grid_barrier_window(dem, wl, cuda, monkeypatch, prec):
     """The cluster-batched window (the default for PCCP: the bound particles'
     connected components packed into batches that one block steps through

@@ -14,14 +14,18 @@
 //      the bound particles -- state, force, torque, wall and pair history --
 //      and every re-list's list, carry map and bound/free lists; one CUDA
 //      graph per segment); then sweep the steps backwards (one CUDA graph
-//      per segment):
+//      per segment, on its own stream):
 //        k_adj_free_window  free particles: the window's steps in closed form
-//        k_adj_step   bound particles: integrator reverse + pair + wall VJP
-//                     (dem_law_adj.cuh), particle-parallel: each particle
-//                     evaluates the reverse of all its pairs and keeps its
-//                     own share -- no atomics, deterministic
+//        k_adj_pairs + k_adj_bound  bound particles, per step: each listed
+//                     pair's law reversed once, then each particle's
+//                     integrator reverse with its pairs' shares in list
+//                     order and its walls' VJP (dem_law_adj.cuh) -- no
+//                     atomics, deterministic (k_adj_step: the same in one
+//                     particle-parallel kernel, DEM_B200_ADJ=pp)
 //        k_adj_carry  at a re-list, the history adjoints of the new list go
 //                     back to the carried pairs of the previous list
+//      Two tape sets: segment g-1 is recomputed into one while segment g is
+//      reversed from the other.
 // The reverse runs in FP64 on the recorded FP64/FP32 trajectory.
 #include <algorithm>
 #include <cstdlib>
@@ -55,20 +59,33 @@ struct ListRec {
     uint* blist = nullptr;   // bound particle ids (n)
     uint* flist = nullptr;   // free particle ids (n)
     uint* nb = nullptr;      // number of bound particles (device word)
-    // cluster batches of the window (forward path): components in slot
-    // order, batch starts, and the word that is 1 when they overflowed
-    uint* cc_order = nullptr;
-    uint* cc_batch = nullptr;
-    uint* cc_over = nullptr;    // the re-list's batch words: [1] window not batched, [3] batch window
 };
 }  // namespace
+
+// The tape of one segment's recompute: per step the bound particles' state
+// before the step, wall history, total force and torque, pair contacts and
+// every listed pair's history; per window its list.
+struct TapeSet {
+    std::vector<ListRec> lists;
+    double *tx = nullptr, *td = nullptr, *twh = nullptr, *tF = nullptr, *tT = nullptr, *th = nullptr;
+    uint* tc = nullptr;   // per step and particle: its pair contacts in the forward
+    void* ta = nullptr;
+};
 
 struct AdjWork {
     long long seg = 0, nck = 0, nwin = 0;
     std::vector<Ck> ck;
-    std::vector<ListRec> lists;
+    // two tape sets: the recompute of segment g-1 (context stream) fills one
+    // while the reverse of segment g (reverse stream) reads the other
+    TapeSet set[2];
+    cudaStream_t rs = nullptr;                       // the reverse sweep's stream
+    cudaEvent_t filled[2] = {nullptr, nullptr};      // set k's recompute done
+    cudaEvent_t freed[2] = {nullptr, nullptr};       // set k's reverse done
+    cudaEvent_t joined = nullptr;
+    // the set selected for the code below (select_set)
+    ListRec* lists = nullptr;
     double *tx = nullptr, *td = nullptr, *twh = nullptr, *tF = nullptr, *tT = nullptr, *th = nullptr;
-    uint* tc = nullptr;   // per step and particle: its pair contacts in the forward
+    uint* tc = nullptr;
     void* ta = nullptr;
     // state adjoints, two sets (ping-pong per reversed step); the objective
     // seeds set 0 (Xb, Db, Ab alias it)
@@ -82,9 +99,6 @@ struct AdjWork {
     uint* pon = nullptr;         // per pair slot: 1 if PC holds this step's shares
     unsigned grid_pairs = 1, grid_bound = 1;   // blocks of k_adj_pairs / k_adj_bound
     bool pair_parallel = true;   // two-phase reverse step (DEM_B200_ADJ=pp: k_adj_step)
-    unsigned grid_adjb = 1;      // blocks of k_adj_batch (windows stepped as cluster batches)
-    size_t adjb_smem = 0;
-    double* gbar = nullptr;      // np x 12: parameter adjoints of the batched windows, per particle (k_adj_batch)
     double* objp = nullptr;      // 3 per k_obj_potential block: energy, d/d estar (pair, wall)
     double* Pobj = nullptr;      // 3 np: the final positions for the objective
     long long npb = 0;
@@ -104,9 +118,25 @@ void free_ck(Ck& k) {
 }
 
 size_t rsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(float) : sizeof(double); }
-size_t recsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>); }
 
-int adjb_setup(dem_ctx* c);
+void select_set(AdjWork* w, int k) {
+    TapeSet& t = w->set[k];
+    w->lists = t.lists.data();
+    w->tx = t.tx; w->td = t.td; w->twh = t.twh; w->tF = t.tF; w->tT = t.tT; w->th = t.th; w->tc = t.tc; w->ta = t.ta;
+}
+
+void free_set(TapeSet& t) {
+    void* p[] = {t.tx, t.td, t.twh, t.tF, t.tT, t.th, t.ta, t.tc};
+    for (void* x : p)
+        if (x) cudaFree(x);
+    for (ListRec& l : t.lists) {
+        void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry, l.bflag, l.blist, l.flist, l.nb};
+        for (void* x : q)
+            if (x) cudaFree(x);
+    }
+    t = TapeSet();
+}
+size_t recsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>); }
 
 int ensure_work(dem_ctx* c, long long seg, long long nck) {
     AdjWork* w = c->adj;
@@ -132,44 +162,40 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
         w->pair_parallel = !(ap && ap[0] == 'p');
         w->grid_pairs = std::min<unsigned>(grid_for(cap, kAB), 2048u);
         w->grid_bound = grid_for(c->n, kAB);
-        if (use_batches(c) && (rc = adjb_setup(c))) return rc;
         w->npb = std::max<long long>(grid_for(c->n, kPairB), std::max(w->grid_pairs, w->grid_bound));
-        w->npb = std::max<long long>(w->npb, w->grid_adjb);
         if ((rc = dalloc(&w->pbar, (size_t)w->npb * 12))) return rc;
-        if (use_batches(c) && (rc = dalloc(&w->gbar, (size_t)np * 12))) return rc;
         if (w->pair_parallel && ((rc = dalloc(&w->PC, (size_t)kPC * cap)) || (rc = dalloc(&w->pon, cap)))) return rc;
         w->Xb = w->Xb2[0];
         w->Db = w->Db2[0];
         w->Ab = w->Ab2[0];
     }
-    if (seg > w->seg) {
-        void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->tc};
-        for (void* x : p)
-            if (x) cudaFree(x);
-        for (ListRec& l : w->lists) {
-            void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry, l.bflag, l.blist, l.flist, l.nb, l.cc_order,
-                         l.cc_batch, l.cc_over};
-            for (void* x : q)
-                if (x) cudaFree(x);
+    if (!w->rs) {
+        DEM_CUDA_TRY(cudaStreamCreateWithFlags(&w->rs, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; k++) {
+            DEM_CUDA_TRY(cudaEventCreateWithFlags(&w->filled[k], cudaEventDisableTiming));
+            DEM_CUDA_TRY(cudaEventCreateWithFlags(&w->freed[k], cudaEventDisableTiming));
         }
-        w->lists.clear();
-        if ((rc = dalloc(&w->tx, 3 * np * seg)) || (rc = dalloc(&w->td, 3 * np * seg)) ||
-            (rc = dalloc(&w->twh, 3 * np * seg)) || (rc = dalloc(&w->tF, 3 * np * seg)) ||
-            (rc = dalloc(&w->tT, 3 * np * seg)) || (rc = dalloc(&w->th, 3 * cap * seg)) ||
-            (rc = dalloc(&w->tc, np * seg)))
-            return rc;
-        DEM_CUDA_TRY(cudaMalloc(&w->ta, 3 * np * seg * rsz(c)));
+        DEM_CUDA_TRY(cudaEventCreateWithFlags(&w->joined, cudaEventDisableTiming));
+    }
+    if (seg > w->seg) {
+        cudaStreamSynchronize(w->rs);
         const long long nw = (seg + K - 1) / K;
-        w->lists.resize(nw);
-        for (ListRec& l : w->lists)
-            if ((rc = dalloc(&l.off, np + 1)) || (rc = dalloc(&l.ln, cap)) || (rc = dalloc(&l.lp, cap)) ||
-                (rc = dalloc(&l.roff, np + 1)) || (rc = dalloc(&l.rk, cap)) || (rc = dalloc(&l.carry, cap)) ||
-                (rc = dalloc(&l.bflag, np)) || (rc = dalloc(&l.blist, np)) || (rc = dalloc(&l.flist, np)) ||
-                (rc = dalloc(&l.nb, 1)) || (rc = dalloc(&l.cc_over, 4)))
+        for (TapeSet& t : w->set) {
+            free_set(t);
+            if ((rc = dalloc(&t.tx, 3 * np * seg)) || (rc = dalloc(&t.td, 3 * np * seg)) ||
+                (rc = dalloc(&t.twh, 3 * np * seg)) || (rc = dalloc(&t.tF, 3 * np * seg)) ||
+                (rc = dalloc(&t.tT, 3 * np * seg)) || (rc = dalloc(&t.th, 3 * cap * seg)) ||
+                (rc = dalloc(&t.tc, np * seg)))
                 return rc;
-        if (use_batches(c))
-            for (ListRec& l : w->lists)
-                if ((rc = dalloc(&l.cc_order, np)) || (rc = dalloc(&l.cc_batch, c->nbatch_max + 2))) return rc;
+            DEM_CUDA_TRY(cudaMalloc(&t.ta, 3 * np * seg * rsz(c)));
+            t.lists.resize(nw);
+            for (ListRec& l : t.lists)
+                if ((rc = dalloc(&l.off, np + 1)) || (rc = dalloc(&l.ln, cap)) || (rc = dalloc(&l.lp, cap)) ||
+                    (rc = dalloc(&l.roff, np + 1)) || (rc = dalloc(&l.rk, cap)) || (rc = dalloc(&l.carry, cap)) ||
+                    (rc = dalloc(&l.bflag, np)) || (rc = dalloc(&l.blist, np)) || (rc = dalloc(&l.flist, np)) ||
+                    (rc = dalloc(&l.nb, 1)))
+                    return rc;
+        }
         w->seg = seg;
         w->nwin = nw;
     }
@@ -615,245 +641,6 @@ __global__ void __launch_bounds__(kAB) k_adj_bound(
     block_sum6(v, pbar + (size_t)blockIdx.x * 12 + 6);
 }
 
-// The reverse of a whole window for its cluster batches (the components
-// the forward stepped as batches): one block per batch runs the window's K
-// reversed steps in shared memory -- per step the pair phase of k_adj_pairs
-// (each pair's law forward from the tape and reversed once), a block barrier,
-// the particle phase of k_adj_bound (integrator reverse, the pairs' shares in
-// list order, walls), a block barrier -- with the same operations in the same
-// order per particle, so the state, wall-history and radius adjoints equal
-// those of the per-step reverse bit for bit.  The parameter adjoints are
-// summed per pair over the window's steps (in shared memory), then per
-// particle over its own row's pairs in list order plus its wall contacts,
-// into the particle's row of gbar: sums whose order does not depend on how
-// the re-list grouped the components into batches (its slot order comes from
-// atomics), so a run gives the same bits every time.  State adjoints are read
-// from set `in` (after the window) and written to set `outs` (before it), the
-// pair history adjoints from Hout (of the window's last step's output) to Hin
-// (of its first step's input), which may be the same array.
-template <typename Real> struct AdjBatchSmem {
-    V3d *xa, *da, *aa, *wb;
-    double* rb;
-    uint *gid, *pb, *pl, *rb0, *rl;
-    double* sh;       // kPC per pair
-    double* pacc;     // 6 per pair: its parameter adjoints summed over the window's steps
-    V3d* hc;          // per pair: the history adjoint being carried backwards
-    uint *plo, *phi, *pk, *prv, *on;
-    uint* scan;
-};
-template <typename Real> __host__ __device__ inline size_t adj_batch_layout(unsigned char* base, AdjBatchSmem<Real>* L) {
-    constexpr uint P = BatchCap<Real>::P, Q = BatchCap<Real>::Q;
-    size_t o = 0;
-    auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
-    AdjBatchSmem<Real> l;
-    l.xa = (V3d*)take(P * sizeof(V3d)); l.da = (V3d*)take(P * sizeof(V3d));
-    l.aa = (V3d*)take(P * sizeof(V3d)); l.wb = (V3d*)take(P * sizeof(V3d));
-    l.rb = (double*)take(P * sizeof(double));
-    l.gid = (uint*)take(P * 4); l.pb = (uint*)take(P * 4); l.pl = (uint*)take(P * 4);
-    l.rb0 = (uint*)take(P * 4); l.rl = (uint*)take(P * 4);
-    l.sh = (double*)take((size_t)Q * kPC * sizeof(double));
-    l.pacc = (double*)take((size_t)Q * 6 * sizeof(double));
-    l.hc = (V3d*)take(Q * sizeof(V3d));
-    l.plo = (uint*)take(Q * 4); l.phi = (uint*)take(Q * 4); l.pk = (uint*)take(Q * 4);
-    l.prv = (uint*)take(Q * 4); l.on = (uint*)take(Q * 4);
-    l.scan = (uint*)take(34 * 4);
-    if (L) *L = l;
-    return o;
-}
-
-template <typename Real>
-__global__ void __launch_bounds__(kAdjBatchThreads) k_adj_batch(
-    long long n, long long np, long long cap, int K, AdjList L, const uint* __restrict__ corder,
-    const uint* __restrict__ cbatch, const uint* __restrict__ nbp, const uint* __restrict__ ccw,
-    const double* __restrict__ tx, const double* __restrict__ td, const Real* __restrict__ ta,
-    const double* __restrict__ twh, const double* __restrict__ th, const double* __restrict__ tF,
-    const double* __restrict__ tT, const uint* __restrict__ tc, const Real* __restrict__ R, LawParams<double> pp,
-    LawParams<double> pw, double dt, double density, double hx, double hy, const double* Hout, double* Hin,
-    const double* Xa, const double* Da, const double* Aa, double* Xo, double* Do, double* Ao, double* Wb,
-    double* Rb, double* __restrict__ gbar, uint* cloc) {
-    if (ccw[1]) return;   // the window was stepped by the grid-barrier kernel: the per-step reverse has it
-    extern __shared__ __align__(16) unsigned char smem[];
-    AdjBatchSmem<Real> S;
-    adj_batch_layout<Real>(smem, &S);
-    const double inv_dt = 1.0 / dt;
-    const long long nb = *nbp;
-    const uint tgt = ccw[3];
-    const uint nbatch = (uint)((nb + tgt - 1) / tgt);
-    const uint total = L.off[n];
-    constexpr uint P = BatchCap<Real>::P, Q = BatchCap<Real>::Q;
-    for (uint bi = blockIdx.x; bi < nbatch; bi += gridDim.x) {
-        const uint s0 = cbatch[bi], s1 = cbatch[bi + 1];
-        if (s1 < s0 || s1 > (uint)nb || s1 - s0 > P) continue;   // the forward reported it (capacity status)
-        const uint m = s1 - s0;
-        uint bad = 0;
-        for (uint p = threadIdx.x; p < m; p += blockDim.x) {
-            const uint i = corder[s0 + p];
-            if (i >= (uint)n) { bad = 1u; continue; }
-            cloc[i] = p;
-            S.gid[p] = i;
-            S.xa[p] = ld3(Xa, np, i); S.da[p] = ld3(Da, np, i); S.aa[p] = ld3(Aa, np, i);
-            S.wb[p] = ld3(Wb, np, i);
-            S.rb[p] = Rb[i];
-            const bool lst = (long long)total <= cap;
-            S.pl[p] = lst ? L.off[i + 1] - L.off[i] : 0u;
-            S.rl[p] = lst ? L.roff[i + 1] - L.roff[i] : 0u;
-        }
-        if (__syncthreads_or(bad)) continue;   // as in the forward (block-wide vote)
-        const uint npairs = block_exscan(S.pl, S.pb, m, S.scan);
-        const uint nrev = block_exscan(S.rl, S.rb0, m, S.scan);
-        if (npairs > Q || nrev != npairs) continue;   // as in the forward
-        for (uint p = threadIdx.x; p < m; p += blockDim.x) {
-            const uint i = S.gid[p], o0 = L.off[i], b0 = S.pb[p];
-            if (__ldcg(cloc + i) != p) bad = 1u;
-            for (uint e = 0; e < S.pl[p]; e++) {
-                const uint k = o0 + e;
-                const uint j = L.ln[k];
-                const uint hi = j < (uint)n ? __ldcg(cloc + j) : 0xffffffffu;
-                if (hi >= m || S.gid[hi] != j) { bad = 1u; break; }
-                S.plo[b0 + e] = p;
-                S.phi[b0 + e] = hi;
-                S.pk[b0 + e] = k;
-                S.hc[b0 + e] = mk(Hout[k], Hout[cap + k], Hout[2 * cap + k]);
-                double* acc = S.pacc + 6 * (size_t)(b0 + e);
-                acc[0] = acc[1] = acc[2] = acc[3] = acc[4] = acc[5] = 0.0;
-            }
-            const uint r0 = L.roff[i], q0 = S.rb0[p];
-            for (uint u = 0; u < S.rl[p] && !bad; u++) {
-                const uint k = L.rk[r0 + u];
-                const uint lo = L.lp[k];
-                const uint q = lo < (uint)n ? __ldcg(cloc + lo) : 0xffffffffu;
-                if (q >= m || S.gid[q] != lo) { bad = 1u; break; }
-                const uint slot = S.pb[q] + (k - L.off[lo]);
-                if (slot >= npairs) { bad = 1u; break; }
-                S.prv[q0 + u] = slot;
-            }
-        }
-        if (__syncthreads_or(bad)) continue;
-        for (int t = K - 1; t >= 0; t--) {
-            const double* txs = tx + 3 * np * t;
-            const double* tds = td + 3 * np * t;
-            const Real* tas = ta + 3 * np * t;
-            const double* ths = th + 3 * cap * t;
-            const uint* tcs = tc + np * t;
-            // pairs (k_adj_pairs)
-            for (uint e = threadIdx.x; e < npairs; e += blockDim.x) {
-                const uint lo = S.plo[e], hi = S.phi[e], k = S.pk[e];
-                const uint il = S.gid[lo], ih = S.gid[hi];
-                bool on = tcs[il] != 0 && tcs[ih] != 0;
-                PairTape pt;
-                if (on) {
-                    const V3d hin = mk(ths[k], ths[cap + k], ths[2 * cap + k]);
-                    V3d Fi, Ti, Tj, ho;
-                    on = pair_fwd(ld3(txs, np, il), ld3(txs, np, ih), ld3(tds, np, il), ld3(tds, np, ih),
-                                  ldA<Real>(tas, np, il), ldA<Real>(tas, np, ih), (double)R[il], (double)R[ih], hin, pp,
-                                  inv_dt, density, pt, Fi, Ti, Tj, ho) != 0;
-                }
-                if (!on) {
-                    S.hc[e] = zero3<double>();
-                    S.on[e] = 0u;
-                    continue;
-                }
-                const double rl = (double)R[il], rh = (double)R[ih];
-                const double ml = density * 8.0 * rl * rl * rl, Il = 0.4 * ml * (rl * rl);
-                const double mh = density * 8.0 * rh * rh * rh, Ih = 0.4 * mh * (rh * rh);
-                const V3d fbl = (dt * dt / ml) * (S.da[lo] + S.xa[lo]), tbl = (dt * dt / Il) * S.aa[lo];
-                const V3d fbh = (dt * dt / mh) * (S.da[hi] + S.xa[hi]), tbh = (dt * dt / Ih) * S.aa[hi];
-                V3d xl = zero3<double>(), xh = zero3<double>(), dl = zero3<double>(), dh = zero3<double>(),
-                    al = zero3<double>(), ah = zero3<double>(), hinb = zero3<double>();
-                double rlb = 0.0, rhb = 0.0;
-                LawBar lb;
-                lawbar_zero(lb);
-                pair_rev(pt, pp, inv_dt, density, fbl - fbh, tbl, tbh, S.hc[e], xl, xh, dl, dh, al, ah, rlb, rhb, hinb,
-                         lb);
-                S.hc[e] = hinb;
-                double* acc = S.pacc + 6 * (size_t)e;
-                acc[0] += lb.estar; acc[1] += lb.mu; acc[2] += lb.cn;
-                acc[3] += lb.ct; acc[4] += lb.roll; acc[5] += lb.roll_rel;
-                double* c = S.sh + (size_t)kPC * e;
-                c[0] = xl.x; c[1] = xl.y; c[2] = xl.z; c[3] = dl.x; c[4] = dl.y; c[5] = dl.z;
-                c[6] = al.x; c[7] = al.y; c[8] = al.z; c[9] = rlb;
-                c[10] = xh.x; c[11] = xh.y; c[12] = xh.z; c[13] = dh.x; c[14] = dh.y; c[15] = dh.z;
-                c[16] = ah.x; c[17] = ah.y; c[18] = ah.z; c[19] = rhb;
-                S.on[e] = 1u;
-            }
-            __syncthreads();
-            // particles (k_adj_bound)
-            for (uint p = threadIdx.x; p < m; p += blockDim.x) {
-                const uint i = S.gid[p];
-                const Real rr = R[i];
-                const V3d fi = mk(tF[3 * np * t + 3 * i], tF[3 * np * t + 3 * i + 1], tF[3 * np * t + 3 * i + 2]);
-                const V3d ti = mk(tT[3 * np * t + 3 * i], tT[3 * np * t + 3 * i + 1], tT[3 * np * t + 3 * i + 2]);
-                const V3d xa = S.xa[p], aa = S.aa[p];
-                V3d dtot, fbi, tbi;
-                double rb = 0.0;
-                integ_rev<Real>(rr, fi, ti, dt, density, xa, S.da[p], aa, dtot, fbi, tbi, rb);
-                V3d xb = zero3<double>(), dbv = zero3<double>(), ab = zero3<double>();
-                for (uint e = S.pb[p], e1 = S.pb[p] + S.pl[p]; e < e1; e++)
-                    if (S.on[e]) add_share(S.sh + (size_t)kPC * e, xb, dbv, ab, rb);
-                for (uint v = S.rb0[p], v1 = S.rb0[p] + S.rl[p]; v < v1; v++) {
-                    const uint e = S.prv[v];
-                    if (S.on[e]) add_share(S.sh + (size_t)kPC * e + 10, xb, dbv, ab, rb);
-                }
-                V3d hwb = zero3<double>();
-                LawBar lw;
-                lawbar_zero(lw);
-                if (wall_vjp(hx, hy, ld3(txs, np, i), ld3(tds, np, i), ldA<Real>(tas, np, i), (double)rr, density,
-                             ld3(twh + 3 * np * t, np, i), pw, inv_dt, fbi, tbi, S.wb[p], xb, dbv, ab, rb, hwb, lw)) {
-                    double* g = gbar + 12 * (size_t)i + 6;   // this particle's row: only this thread writes it
-                    g[0] += lw.estar; g[1] += lw.mu; g[2] += lw.cn;
-                    g[3] += lw.ct; g[4] += lw.roll; g[5] += lw.roll_rel;
-                }
-                S.wb[p] = hwb;
-                S.xa[p] = xa + xb;
-                S.da[p] = dtot + dbv;
-                S.aa[p] = aa + ab;
-                S.rb[p] += rb;
-            }
-            __syncthreads();
-        }
-        for (uint p = threadIdx.x; p < m; p += blockDim.x) {
-            const uint i = S.gid[p];
-            st3(Xo, np, i, S.xa[p]); st3(Do, np, i, S.da[p]); st3(Ao, np, i, S.aa[p]);
-            st3(Wb, np, i, S.wb[p]);
-            Rb[i] = S.rb[p];
-            double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // own row's pairs, list order
-            for (uint e = S.pb[p], e1 = S.pb[p] + S.pl[p]; e < e1; e++)
-                for (int j = 0; j < 6; j++) v[j] += S.pacc[6 * (size_t)e + j];
-            double* g = gbar + 12 * (size_t)i;
-            for (int j = 0; j < 6; j++) g[j] += v[j];
-        }
-        for (uint e = threadIdx.x; e < npairs; e += blockDim.x) {
-            const uint k = S.pk[e];
-            const V3d h = S.hc[e];
-            Hin[k] = h.x; Hin[cap + k] = h.y; Hin[2 * cap + k] = h.z;
-        }
-        __syncthreads();
-    }
-}
-
-// The batched windows' per-particle parameter adjoints (gbar) summed into
-// pbar's first rows: block b sums particles [b kB, (b + 1) kB) in a fixed
-// order, so the result does not depend on the run.
-__global__ void __launch_bounds__(kB) k_adj_gbar(long long n, const double* __restrict__ gbar,
-                                                 double* __restrict__ pbar) {
-    __shared__ double sp[12][kB / 32];
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 12; k++) {
-        double x = i < n ? gbar[12 * i + k] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) sp[k][warp] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x < 12) {
-        double x = 0.0;
-        for (int w = 0; w < kB / 32; w++) x += sp[threadIdx.x][w];
-        pbar[(size_t)blockIdx.x * 12 + threadIdx.x] += x;
-    }
-}
-
 // History adjoint across a re-list: new pair k carried old pair carry[k].
 __global__ void k_adj_carry(const uint* __restrict__ off, long long n, long long cap, const uint* __restrict__ carry,
                             const double* __restrict__ Hnew, double* __restrict__ Hold) {
@@ -1024,12 +811,12 @@ template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l,
         const double* tx = w->tx + 3 * np * t;
         const double* td = w->td + 3 * np * t;
         const Real* ta = (const Real*)w->ta + 3 * np * t;
-        DEM_CUDA_TRY(launch_ex(k_adj_pairs<Real>, w->grid_pairs, kAB, c->stream, pdl, c->n, np, cap, L, tx, td, ta,
+        DEM_CUDA_TRY(launch_ex(k_adj_pairs<Real>, w->grid_pairs, kAB, w->rs, pdl, c->n, np, cap, L, tx, td, ta,
                                (const double*)w->th + 3 * cap * t, (const uint*)w->tc + np * t, (const Real*)c->rad,
                                make_law<double>(c->mat.pp), c->cfg.dt, c->cfg.density, (const double*)w->Hb[hb],
                                w->Hb[1 - hb], (const double*)w->Xb2[in], (const double*)w->Db2[in],
                                (const double*)w->Ab2[in], w->PC, w->pon, w->pbar));
-        DEM_CUDA_TRY(launch_ex(k_adj_bound<Real>, w->grid_bound, kAB, c->stream, pdl, c->n, np, cap, L, l.blist, l.nb,
+        DEM_CUDA_TRY(launch_ex(k_adj_bound<Real>, w->grid_bound, kAB, w->rs, pdl, c->n, np, cap, L, l.blist, l.nb,
                                tx, td, ta, (const double*)w->twh + 3 * np * t, (const double*)w->tF + 3 * np * t,
                                (const double*)w->tT + 3 * np * t, (const Real*)c->rad, make_law<double>(c->mat.pw),
                                c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
@@ -1043,55 +830,13 @@ template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l,
     // window follows the free-particle kernel and is launched plainly
     const bool pdl = c->pdl && (t % c->cfg.relist_interval) != c->cfg.relist_interval - 1;
     DEM_CUDA_TRY(launch_ex(
-        k_adj_step<Real>, (unsigned)w->npb, kPairB, c->stream, pdl, c->n, np, cap, L, l.blist, l.nb,
+        k_adj_step<Real>, (unsigned)w->npb, kPairB, w->rs, pdl, c->n, np, cap, L, l.blist, l.nb,
         w->tx + 3 * np * t, w->td + 3 * np * t, (const Real*)w->ta + 3 * np * t, w->twh + 3 * np * t,
         w->th + 3 * cap * t, w->tF + 3 * np * t, w->tT + 3 * np * t, (const uint*)w->tc + np * t, (const Real*)c->rad,
         make_law<double>(c->mat.pp), make_law<double>(c->mat.pw), c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5,
         c->cfg.world[1] * 0.5, (const double*)w->Hb[hb], w->Hb[1 - hb], (const double*)w->Xb2[in],
         (const double*)w->Db2[in], (const double*)w->Ab2[in], w->Xb2[1 - in], w->Db2[1 - in], w->Ab2[1 - in], w->Wb,
         w->Rb, w->pbar));
-    return DEM_OK;
-}
-
-// All K reversed steps of the window that starts at segment step t0, for
-// its cluster batches (k_adj_batch); state adjoints from set `in` to set
-// `out`.
-template <typename Real>
-int adj_batch(dem_ctx* c, long long t0, const AdjList& L, const ListRec& l, const double* Hout, double* Hin, int in,
-              int out) {
-    AdjWork* w = c->adj;
-    const long long np = c->npad, cap = c->cap;
-    const int K = c->cfg.relist_interval;
-    k_adj_batch<Real><<<w->grid_adjb, kAdjBatchThreads, w->adjb_smem, c->stream>>>(
-        c->n, np, cap, K, L, l.cc_order, l.cc_batch, l.nb, l.cc_over, w->tx + 3 * np * t0, w->td + 3 * np * t0,
-        (const Real*)w->ta + 3 * np * t0, w->twh + 3 * np * t0, w->th + 3 * cap * t0, w->tF + 3 * np * t0,
-        w->tT + 3 * np * t0, (const uint*)w->tc + np * t0, (const Real*)c->rad, make_law<double>(c->mat.pp),
-        make_law<double>(c->mat.pw), c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, Hout, Hin,
-        (const double*)w->Xb2[in], (const double*)w->Db2[in], (const double*)w->Ab2[in], w->Xb2[out], w->Db2[out],
-        w->Ab2[out], w->Wb, w->Rb, w->gbar, c->cc_loc);
-    DEM_LAUNCH_CHECK();
-    return DEM_OK;
-}
-
-// Shared memory and grid of k_adj_batch (once per workspace).
-int adjb_setup(dem_ctx* c) {
-    AdjWork* w = c->adj;
-    const bool mx = c->prec == DEM_PREC_MIXED;
-    w->adjb_smem = mx ? adj_batch_layout<float>(nullptr, nullptr) : adj_batch_layout<double>(nullptr, nullptr);
-    cudaError_t e = mx ? cudaFuncSetAttribute(k_adj_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)w->adjb_smem)
-                       : cudaFuncSetAttribute(k_adj_batch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)w->adjb_smem);
-    int per = 0, nsm = 0;
-    if (e == cudaSuccess)
-        e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_adj_batch<float>, kAdjBatchThreads,
-                                                               w->adjb_smem)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_adj_batch<double>, kAdjBatchThreads,
-                                                               w->adjb_smem);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    if (e != cudaSuccess) return cuda_fail(e, "adjoint batch kernel set-up", __FILE__, __LINE__);
-    if (per < 1) return fail(DEM_ERR_CUDA, "adjoint batch kernel does not fit an SM");
-    w->grid_adjb = (unsigned)std::max<long long>(1, std::min<long long>((long long)nsm * per, c->nbatch_max));
     return DEM_OK;
 }
 
@@ -1140,14 +885,6 @@ int list_snapshot(dem_ctx* c, ListRec& l) {
         (rc = copy(l.blist, c->blist, np * sizeof(uint), s)) || (rc = copy(l.flist, c->flist, np * sizeof(uint), s)) ||
         (rc = copy(l.nb, c->bpos + c->n, sizeof(uint), s)))
         return rc;
-    if (l.cc_order) {
-        if ((rc = copy(l.cc_order, c->cc_order, np * sizeof(uint), s)) ||
-            (rc = copy(l.cc_batch, c->cc_batch, (c->nbatch_max + 1) * sizeof(uint), s)) ||
-            (rc = copy(l.cc_over, c->cc_words, 4 * sizeof(uint), s)))
-            return rc;
-    } else {
-        DEM_CUDA_TRY(cudaMemsetAsync(l.cc_over, 0xff, 4 * sizeof(uint), s));   // no batches: the per-step reverse
-    }
     return DEM_OK;
 }
 
@@ -1172,19 +909,15 @@ int recompute_segment(dem_ctx* c, long long every) {
     return DEM_OK;
 }
 
-// The reversed steps of one segment (steps every-1 .. 0), enqueued on the
-// context's stream; hb / in advance as the steps swap their buffers.
-// The reversed steps of one segment (steps every-1 .. 0), enqueued on the
-// context's stream; hb / in advance as the steps swap their buffers.  A
-// window whose bound particles the forward stepped as cluster batches
-// (batched[window], known on the host) is reversed by one k_adj_batch
-// launch for all its steps; the others step by step.
-int reverse_segment(dem_ctx* c, long long every, int& hb, int& in, const std::vector<char>& batched) {
+// The reversed steps of one segment (steps every-1 .. 0) from the selected
+// tape set, enqueued on the reverse stream; hb / in advance as the steps swap
+// their buffers.
+int reverse_segment(dem_ctx* c, long long every, int& hb, int& in) {
     AdjWork* w = c->adj;
     const int K = c->cfg.relist_interval;
     const long long cap = c->cap;
     const bool mixed = c->prec == DEM_PREC_MIXED;
-    cudaStream_t s = c->stream;
+    cudaStream_t s = w->rs;
     int rc;
     const long long np = c->npad;
     for (long long t = every - 1; t >= 0; t--) {
@@ -1195,26 +928,11 @@ int reverse_segment(dem_ctx* c, long long every, int& hb, int& in, const std::ve
                                                                 w->Ab2[in], w->Xb2[out], w->Db2[out], w->Ab2[out],
                                                                 w->Wb);
             DEM_LAUNCH_CHECK();
-            if (batched[t / K]) {   // the window's bound particles, all its steps at once
-                const long long t0 = t - (K - 1);
-                const int hout = hb, hin = hb ^ (K & 1);
-                AdjList L{l.off, l.ln, l.lp, l.roff, l.rk};
-                if (mixed)
-                    rc = adj_batch<float>(c, t0, L, l, w->Hb[hout], w->Hb[hin], in, out);
-                else
-                    rc = adj_batch<double>(c, t0, L, l, w->Hb[hout], w->Hb[hin], in, out);
-                if (rc) return rc;
-                in = out;
-                hb = hin;
-                t = t0;
-            }
         }
-        if (!batched[t / K]) {
-            rc = mixed ? adj_step<float>(c, t, l, hb, in) : adj_step<double>(c, t, l, hb, in);
-            if (rc) return rc;
-            in = 1 - in;   // set `in` now holds the adjoints of the state before the step
-            hb = 1 - hb;   // Hb[hb] now holds the adjoint of this step's input history
-        }
+        rc = mixed ? adj_step<float>(c, t, l, hb, in) : adj_step<double>(c, t, l, hb, in);
+        if (rc) return rc;
+        in = 1 - in;   // set `in` now holds the adjoints of the state before the step
+        hb = 1 - hb;   // Hb[hb] now holds the adjoint of this step's input history
         if (t % K == 0) {
             // input history came from the re-list carry: route it to the
             // previous list's output history
@@ -1235,20 +953,21 @@ void reverse_parities(long long every, int K, int& hb, int& in) {
     }
 }
 
-// Graphs of one dem_adjoint_window call, indexed by parities at the segment
-// start (recompute: list buffer; reverse sweep: hb, in).
+// Graphs of one dem_adjoint_window call, indexed by the tape set and the
+// parities at the segment start (recompute: list buffer; reverse sweep: hb,
+// in): a graph holds the set's addresses.
 struct SegmentGraphs {
-    cudaGraphExec_t g[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaGraphExec_t g[2][2][2] = {};
     ~SegmentGraphs() {
-        for (auto& row : g)
-            for (cudaGraphExec_t& e : row)
-                if (e) cudaGraphExecDestroy(e);
+        for (auto& set : g)
+            for (auto& row : set)
+                for (cudaGraphExec_t& e : row)
+                    if (e) cudaGraphExecDestroy(e);
     }
 };
 
-// Captures what `enqueue` puts on the stream as a graph (once) and launches it.
-template <typename F> int run_captured(dem_ctx* c, cudaGraphExec_t& ge, F enqueue) {
-    cudaStream_t s = c->stream;
+// Captures what `enqueue` puts on stream s as a graph (once) and launches it.
+template <typename F> int run_captured(cudaStream_t s, cudaGraphExec_t& ge, F enqueue) {
     if (!ge) {
         cudaGraph_t gr = nullptr;
         DEM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1316,7 +1035,6 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     DEM_CUDA_TRY(cudaMemsetAsync(w->Rb, 0, np * sizeof(double), s));
     DEM_CUDA_TRY(cudaMemsetAsync(w->Hb[0], 0, 3 * cap * sizeof(double), s));
     DEM_CUDA_TRY(cudaMemsetAsync(w->pbar, 0, (size_t)w->npb * 12 * sizeof(double), s));
-    if (w->gbar) DEM_CUDA_TRY(cudaMemsetAsync(w->gbar, 0, (size_t)np * 12 * sizeof(double), s));
     rc = mixed ? objective<float>(c, which) : objective<double>(c, which);
     if (rc) return rc;
     // ------------------------------------------------------- reverse segments
@@ -1328,15 +1046,24 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     int hb = 0;   // Hb[hb]: adjoint of the pair history output by the step being reversed
     int in = 0;   // state-adjoint set of the state after the step being reversed
     SegmentGraphs fgraph, rgraph;
+    // Segment g is recomputed into tape set g & 1 on the context's stream and
+    // reversed from it on the reverse stream, so the recompute of segment g-1
+    // (into the other set) runs beside the reverse of segment g: the two are
+    // independent (the reverse reads only its tape and the adjoints).
     for (long long g = nseg - 1; g >= 0; g--) {
-        if ((rc = restore_ck(c, w->ck[g]))) return rc;
+        const int k = (int)(g & 1);
         NvtxRange seg_range("dem adjoint segment (recompute + reverse)");
+        // the set's previous reader, the reverse of segment g + 2, is done
+        if (g + 2 <= nseg - 1) DEM_CUDA_TRY(cudaStreamWaitEvent(s, w->freed[k], 0));
+        if ((rc = restore_ck(c, w->ck[g]))) return rc;
+        select_set(w, k);
         // recompute the segment, recording what the reverse sweep needs
         if (win_path) {
-            // one graph per list-buffer parity at the segment start (the
-            // capture only records: c->cur is advanced after the launch)
+            // one graph per tape set and list-buffer parity at the segment
+            // start (the capture only records: c->cur is advanced after the
+            // launch)
             const int cur0 = c->cur;
-            rc = run_captured(c, fgraph.g[cur0][0], [&]() {
+            rc = run_captured(s, fgraph.g[k][cur0][0], [&]() {
                 const int r = recompute_segment(c, every);
                 c->cur = cur0;
                 return r;
@@ -1383,35 +1110,21 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
             c->dbgC = keepC;
             if (rc) return rc;
         }
-        // which of the segment's windows the forward stepped as cluster batches
-        const long long nwin = every / K;
-        std::vector<char> batched(nwin, 0);
-        bool any = false;
-        if (use_batches(c) && win_path) {
-            std::vector<uint> over(nwin, 1u);
-            for (long long k = 0; k < nwin; k++)
-                DEM_CUDA_TRY(
-                    cudaMemcpyAsync(&over[k], w->lists[k].cc_over + 1, sizeof(uint), cudaMemcpyDeviceToHost, s));
-            DEM_CUDA_TRY(cudaStreamSynchronize(s));
-            for (long long k = 0; k < nwin; k++) any |= (batched[k] = over[k] == 0u) != 0;
-        }
-        if (!any) {
-            // reverse sweep step by step: one graph per (hb, in) parity at the segment start
-            const int hb0 = hb, in0 = in;
-            rc = run_captured(c, rgraph.g[hb0][in0], [&]() {
-                int h = hb0, i = in0;
-                return reverse_segment(c, every, h, i, batched);
-            });
-            if (rc) return rc;
-            reverse_parities(every, K, hb, in);
-        } else if ((rc = reverse_segment(c, every, hb, in, batched))) {
-            return rc;
-        }
+        DEM_CUDA_TRY(cudaEventRecord(w->filled[k], s));
+        // the reverse sweep step by step, after the recompute: one graph per
+        // tape set and (hb, in) parity at the segment start
+        DEM_CUDA_TRY(cudaStreamWaitEvent(w->rs, w->filled[k], 0));
+        const int hb0 = hb, in0 = in;
+        rc = run_captured(w->rs, rgraph.g[k][hb0][in0], [&]() {
+            int h = hb0, i = in0;
+            return reverse_segment(c, every, h, i);
+        });
+        if (rc) return rc;
+        reverse_parities(every, K, hb, in);
+        DEM_CUDA_TRY(cudaEventRecord(w->freed[k], w->rs));
     }
-    if (w->gbar) {   // the batched windows' parameter adjoints, in a fixed order
-        k_adj_gbar<<<grid_for(c->n, kB), kB, 0, s>>>(c->n, w->gbar, w->pbar);
-        DEM_LAUNCH_CHECK();
-    }
+    DEM_CUDA_TRY(cudaEventRecord(w->joined, w->rs));
+    DEM_CUDA_TRY(cudaStreamWaitEvent(s, w->joined, 0));
     DEM_CUDA_TRY(cudaEventRecord(c->ev[2], s));
     // ------------------------------------------------------------ results
     std::vector<double> pb((size_t)w->npb * 12);
@@ -1468,17 +1181,15 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     AdjWork* w = c->adj;
     cudaStreamSynchronize(c->stream);
     for (Ck& k : w->ck) free_ck(k);
-    void* p[] = {w->tx, w->td, w->twh, w->tF, w->tT, w->th, w->ta, w->tc, w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1],
-                 w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1], w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj,
-                 w->objp, w->PC, w->pon, w->gbar};
+    if (w->rs) cudaStreamSynchronize(w->rs);
+    void* p[] = {w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1], w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1],
+                 w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj, w->objp, w->PC, w->pon};
     for (void* x : p)
         if (x) cudaFree(x);
-    for (ListRec& l : w->lists) {
-        void* q[] = {l.off, l.ln, l.lp, l.roff, l.rk, l.carry, l.bflag, l.blist, l.flist, l.nb, l.cc_order,
-                     l.cc_batch, l.cc_over};
-        for (void* x : q)
-            if (x) cudaFree(x);
-    }
+    for (TapeSet& t : w->set) free_set(t);
+    for (cudaEvent_t e : {w->filled[0], w->filled[1], w->freed[0], w->freed[1], w->joined})
+        if (e) cudaEventDestroy(e);
+    if (w->rs) cudaStreamDestroy(w->rs);
     delete w;
     c->adj = nullptr;
     return DEM_OK;

@@ -111,15 +111,14 @@ struct ParticleCommon {
 };
 
 // Cluster batches: batches of whole components, at most BatchCap<Real>::P
-// particles and ::Q listed pairs each (what one block holds in shared memory,
-// forward and reverse).  A batch takes the components whose first slot falls
+// particles and ::Q listed pairs each (what one block of k_batch holds in
+// shared memory).  A batch takes the components whose first slot falls
 // in one window of `target` slots; the re-list chooses target per window as
 // the bound particles over the batch kernel's resident blocks (one round of
 // blocks), at least kBatchMin and at most P minus the largest component.
 constexpr uint kBatchMin = 32;
 constexpr uint kDenseSkip = 32;          // re-lists without the component pass after one larger than a block
 constexpr int kBatchThreads = 512;       // k_batch: one particle per thread
-constexpr int kAdjBatchThreads = 256;    // k_adj_batch (its FP64 reverse needs the registers)
 template <typename Real> struct BatchCap;
 template <> struct BatchCap<float> { static constexpr uint P = 512, Q = 640; };
 template <> struct BatchCap<double> { static constexpr uint P = 384, Q = 640; };

@@ -196,12 +196,10 @@ def test_recompute_paths_agree(dem, cuda, monkeypatch, which):
     """The reverse sweep's recompute through the per-step kernels (window
     kernel off: tape from the force record, contact counts included) and
     through the window path (cluster batches where the components fit a
-    block, whose windows reverse as batches too) give the same objective and
-    radius gradients bit for bit, and the same parameter gradients to 1e-12
-    relative (the batched reverse sums the same terms per particle, the
-    per-step one per block); the particle-parallel force mode (its own
-    per-step kernel, whose forward agrees with the pair-parallel one to
-    rounding) agrees within the gradient tolerance, 1e-3."""
+    block, else the grid-barrier window kernel, writing the tape) give the
+    same objective and gradients bit for bit; the particle-parallel force
+    mode (its own per-step kernel, whose forward agrees with the pair-parallel
+    one to rounding) agrees within the gradient tolerance, 1e-3."""
     w, pdis, angv = case(dem) if which == "dense" else sparse_case(dem)
 
     def run(**env):
@@ -219,10 +217,7 @@ def test_recompute_paths_agree(dem, cuda, monkeypatch, which):
     a = run(DEM_B200_WINDOW="1")
     b = run(DEM_B200_WINDOW="0")
     assert a["value"] == b["value"]
-    for side in ("d_pp", "d_pw"):
-        for k, x in a[side].items():
-            y = b[side][k]
-            assert abs(x - y) <= 1e-12 * max(abs(x), abs(y)), (side, k, x, y)
+    assert a["d_pp"] == b["d_pp"] and a["d_pw"] == b["d_pw"]
     np.testing.assert_array_equal(a["d_radii"], b["d_radii"])
     monkeypatch.setenv("DEM_B200_WINDOW", "1")
     c = run(PP="1")

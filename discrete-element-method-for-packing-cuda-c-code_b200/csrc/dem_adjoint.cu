@@ -62,6 +62,25 @@ struct ListRec {
 };
 }  // namespace
 
+// Graphs of the adjoint, indexed by the tape set and the parities at the
+// segment start (recompute: list buffer; reverse sweep: hb, in): a graph
+// holds the set's addresses and the material.  Kept across calls of the same
+// segment length; dropped with the engine's graphs (material, particle count,
+// grid) and when the tape is reallocated.
+struct SegmentGraphs {
+    cudaGraphExec_t g[2][2][2] = {};
+    void drop() {
+        for (auto& set : g)
+            for (auto& row : set)
+                for (cudaGraphExec_t& e : row)
+                    if (e) {
+                        cudaGraphExecDestroy(e);
+                        e = nullptr;
+                    }
+    }
+    ~SegmentGraphs() { drop(); }
+};
+
 // The tape of one segment's recompute: per step the bound particles' state
 // before the step, wall history, total force and torque, pair contacts and
 // every listed pair's history; per window its list.
@@ -82,6 +101,8 @@ struct AdjWork {
     cudaEvent_t filled[2] = {nullptr, nullptr};      // set k's recompute done
     cudaEvent_t freed[2] = {nullptr, nullptr};       // set k's reverse done
     cudaEvent_t joined = nullptr;
+    SegmentGraphs fgraph, rgraph;    // recompute and reverse graphs
+    long long graph_every = 0;       // the segment length they were captured for
     // the set selected for the code below (select_set)
     ListRec* lists = nullptr;
     double *tx = nullptr, *td = nullptr, *twh = nullptr, *tF = nullptr, *tT = nullptr, *th = nullptr;
@@ -97,6 +118,8 @@ struct AdjWork {
     double* pbar = nullptr;      // npb x 12 (one row per reverse-step block: pair params 0-5, wall params 6-11)
     double* PC = nullptr;        // kPC per pair slot: the shares a pair's reverse sends to lo and hi
     uint* pon = nullptr;         // per pair slot: 1 if PC holds this step's shares
+    double* WS = nullptr;        // 10 per particle: its walls' shares (pair phase)
+    uint* wson = nullptr;        // per particle: 1 if WS holds this step's shares
     unsigned grid_pairs = 1, grid_bound = 1;   // blocks of k_adj_pairs / k_adj_bound
     bool pair_parallel = true;   // two-phase reverse step (DEM_B200_ADJ=pp: k_adj_step)
     double* objp = nullptr;      // 3 per k_obj_potential block: energy, d/d estar (pair, wall)
@@ -138,6 +161,8 @@ void free_set(TapeSet& t) {
 }
 size_t recsz(const dem_ctx* c) { return c->prec == DEM_PREC_MIXED ? sizeof(PRec<float>) : sizeof(PRec<double>); }
 
+int adj_grids(dem_ctx* c);
+
 int ensure_work(dem_ctx* c, long long seg, long long nck) {
     AdjWork* w = c->adj;
     if (!w) {
@@ -160,11 +185,12 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
             return rc;
         const char* ap = getenv("DEM_B200_ADJ");   // "pp": the particle-parallel reverse step
         w->pair_parallel = !(ap && ap[0] == 'p');
-        w->grid_pairs = std::min<unsigned>(grid_for(cap, kAB), 2048u);
-        w->grid_bound = grid_for(c->n, kAB);
+        if ((rc = adj_grids(c))) return rc;
         w->npb = std::max<long long>(grid_for(c->n, kPairB), std::max(w->grid_pairs, w->grid_bound));
         if ((rc = dalloc(&w->pbar, (size_t)w->npb * 12))) return rc;
-        if (w->pair_parallel && ((rc = dalloc(&w->PC, (size_t)kPC * cap)) || (rc = dalloc(&w->pon, cap)))) return rc;
+        if (w->pair_parallel && ((rc = dalloc(&w->PC, (size_t)kPC * cap)) || (rc = dalloc(&w->pon, cap)) ||
+                                 (rc = dalloc(&w->WS, 10 * (size_t)np)) || (rc = dalloc(&w->wson, np))))
+            return rc;
         w->Xb = w->Xb2[0];
         w->Db = w->Db2[0];
         w->Ab = w->Ab2[0];
@@ -179,6 +205,8 @@ int ensure_work(dem_ctx* c, long long seg, long long nck) {
     }
     if (seg > w->seg) {
         cudaStreamSynchronize(w->rs);
+        w->fgraph.drop();
+        w->rgraph.drop();
         const long long nw = (seg + K - 1) / K;
         for (TapeSet& t : w->set) {
             free_set(t);
@@ -527,18 +555,44 @@ __global__ void __launch_bounds__(kAB) k_adj_pairs(
     const Real* __restrict__ ta, const double* __restrict__ th, const uint* __restrict__ tc, const Real* __restrict__ R,
     LawParams<double> pp, double dt, double density, const double* __restrict__ Hout, double* __restrict__ Hin,
     const double* __restrict__ Xa, const double* __restrict__ Da, const double* __restrict__ Aa,
-    double* __restrict__ PC, uint* __restrict__ pon, double* __restrict__ pbar) {
+    double* __restrict__ PC, uint* __restrict__ pon, double* __restrict__ pbar, const uint* __restrict__ blist,
+    const uint* __restrict__ nbp, const double* __restrict__ twh, LawParams<double> pw, double hx, double hy,
+    double* __restrict__ WS, uint* __restrict__ wson, double* __restrict__ Wb) {
     const double inv_dt = 1.0 / dt;
-    LawBar bp;
+    LawBar bp, bw;
     lawbar_zero(bp);
+    lawbar_zero(bw);
     // the list and the tape (the recompute's) may be read before the wait;
     // the state and history adjoints are the predecessors'
     const uint total = L.off[n];
+    const long long nb = (long long)*nbp;
     const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long npr = (long long)total <= cap ? (long long)total : 0ll;
     pdl_wait();
     pdl_trigger();
-    if ((long long)total <= cap) {
-        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < (long long)total; k += stride) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < npr + nb; k += stride) {
+        if (k >= npr) {
+            // a bound particle's walls: their VJP needs only the particle's
+            // force adjoints, so it runs beside the pairs; its shares go to
+            // WS for the particle phase, its history adjoint to Wb
+            const uint i = blist[k - npr];
+            V3d fbi, tbi;
+            partner_fb<Real>(R[i], np, i, dt, density, Xa, Da, Aa, fbi, tbi);
+            V3d xw = zero3<double>(), dw = zero3<double>(), aw = zero3<double>(), hwb = zero3<double>();
+            double rw = 0.0;
+            const int hit = wall_vjp(hx, hy, ld3(tx, np, i), ld3(td, np, i), ldA<Real>(ta, np, i), (double)R[i],
+                                     density, ld3(twh, np, i), pw, inv_dt, fbi, tbi, ld3(Wb, np, i), xw, dw, aw, rw,
+                                     hwb, bw);
+            st3(Wb, np, i, hwb);
+            if (hit) {
+                double* c = WS + 10 * (size_t)i;
+                c[0] = xw.x; c[1] = xw.y; c[2] = xw.z; c[3] = dw.x; c[4] = dw.y; c[5] = dw.z;
+                c[6] = aw.x; c[7] = aw.y; c[8] = aw.z; c[9] = rw;
+            }
+            wson[i] = hit ? 1u : 0u;
+            continue;
+        }
+        {
             const uint lo = L.lp[k], hi = L.ln[k];
             bool on = tc[lo] != 0 && tc[hi] != 0;
             PairTape t;
@@ -573,6 +627,8 @@ __global__ void __launch_bounds__(kAB) k_adj_pairs(
     }
     const double v[6] = {bp.estar, bp.mu, bp.cn, bp.ct, bp.roll, bp.roll_rel};
     block_sum6(v, pbar + (size_t)blockIdx.x * 12);
+    const double vw[6] = {bw.estar, bw.mu, bw.cn, bw.ct, bw.roll, bw.roll_rel};
+    block_sum6(vw, pbar + (size_t)blockIdx.x * 12 + 6);
 }
 
 __device__ __forceinline__ void add_share(const double* __restrict__ c, V3d& xb, V3d& db, V3d& ab, double& rb) {
@@ -585,36 +641,32 @@ __device__ __forceinline__ void add_share(const double* __restrict__ c, V3d& xb,
 template <typename Real>
 __global__ void __launch_bounds__(kAB) k_adj_bound(
     long long n, long long np, long long cap, AdjList L, const uint* __restrict__ blist, const uint* __restrict__ nbp,
-    const double* __restrict__ tx, const double* __restrict__ td, const Real* __restrict__ ta,
-    const double* __restrict__ twh, const double* __restrict__ tF, const double* __restrict__ tT,
-    const Real* __restrict__ R, LawParams<double> pw, double dt, double density, double hx, double hy,
-    const double* __restrict__ PC, const uint* __restrict__ pon, const double* __restrict__ Xa,
-    const double* __restrict__ Da, const double* __restrict__ Aa, double* __restrict__ Xo, double* __restrict__ Do,
-    double* __restrict__ Ao, double* __restrict__ Wb, double* __restrict__ Rb, double* __restrict__ pbar) {
-    const double inv_dt = 1.0 / dt;
-    LawBar bw;
-    lawbar_zero(bw);
-    const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const double* __restrict__ tF, const double* __restrict__ tT, const Real* __restrict__ R, double dt,
+    double density, const double* __restrict__ PC, const uint* __restrict__ pon, const double* __restrict__ WS,
+    const uint* __restrict__ wson, const double* __restrict__ Xa, const double* __restrict__ Da,
+    const double* __restrict__ Aa, double* __restrict__ Xo, double* __restrict__ Do, double* __restrict__ Ao,
+    double* __restrict__ Rb) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nb = (long long)*nbp;
-    // before the wait: the list and the tape of the particle
+    const uint total = L.off[n];
+    // the list and the tape of a particle (the first one before the wait)
     long long i = 0;
     Real rr = (Real)0;
-    V3d xi = zero3<double>(), di = zero3<double>(), ai = zero3<double>(), fi = zero3<double>(), ti = zero3<double>(),
-        hw = zero3<double>();
-    uint total = 0, o0 = 0, o1 = 0, q0 = 0, q1 = 0;
-    if (u < nb) {
+    V3d fi, ti;
+    uint o0 = 0, o1 = 0, q0 = 0, q1 = 0;
+    auto load = [&]() {
         i = blist[u];
         rr = R[i];
-        xi = ld3(tx, np, i); di = ld3(td, np, i); ai = ldA<Real>(ta, np, i);
         fi = mk(tF[3 * i], tF[3 * i + 1], tF[3 * i + 2]);
         ti = mk(tT[3 * i], tT[3 * i + 1], tT[3 * i + 2]);
-        hw = ld3(twh, np, i);
-        total = L.off[n];
         o0 = L.off[i]; o1 = L.off[i + 1]; q0 = L.roff[i]; q1 = L.roff[i + 1];
-    }
+    };
+    if (u < nb) load();
     pdl_wait();
     pdl_trigger();
-    if (u < nb) {
+    for (bool first = true; u < nb; u += stride, first = false) {
+        if (!first) load();
         const V3d xa = ld3(Xa, np, i), aa = ld3(Aa, np, i);
         V3d dtot, fbi, tbi;
         double rb = 0.0;
@@ -628,17 +680,33 @@ __global__ void __launch_bounds__(kAB) k_adj_bound(
                 if (k < total && pon[k]) add_share(PC + (size_t)kPC * k + 10, xb, dbv, ab, rb);
             }
         }
-        V3d hwb = zero3<double>();
-        wall_vjp(hx, hy, xi, di, ai, (double)rr, density, hw, pw, inv_dt, fbi, tbi, ld3(Wb, np, i), xb, dbv, ab, rb,
-                 hwb, bw);
-        st3(Wb, np, i, hwb);
+        if (wson[i]) add_share(WS + 10 * (size_t)i, xb, dbv, ab, rb);   // its walls (the pair phase's items)
         st3(Xo, np, i, xa + xb);
         st3(Do, np, i, dtot + dbv);
         st3(Ao, np, i, aa + ab);
         Rb[i] += rb;
     }
-    const double v[6] = {bw.estar, bw.mu, bw.cn, bw.ct, bw.roll, bw.roll_rel};
-    block_sum6(v, pbar + (size_t)blockIdx.x * 12 + 6);
+}
+
+// Grids of the two-phase reverse step: one round of resident blocks,
+// striding over the pairs / bound particles (a grid sized for the capacity
+// is mostly blocks without work, each of which still takes a slot on an SM
+// every step).
+int adj_grids(dem_ctx* c) {
+    AdjWork* w = c->adj;
+    const bool mx = c->prec == DEM_PREC_MIXED;
+    int nsm = 0, bp = 0, bb = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    if (e == cudaSuccess)
+        e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_adj_pairs<float>, kAB, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_adj_pairs<double>, kAB, 0);
+    if (e == cudaSuccess)
+        e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_adj_bound<float>, kAB, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_adj_bound<double>, kAB, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint kernel set-up", __FILE__, __LINE__);
+    w->grid_pairs = (unsigned)std::max(1, nsm * std::max(bp, 1));
+    w->grid_bound = (unsigned)std::max(1, nsm * std::max(bb, 1));
+    return DEM_OK;
 }
 
 // History adjoint across a re-list: new pair k carried old pair carry[k].
@@ -815,14 +883,15 @@ template <typename Real> int adj_step(dem_ctx* c, long long t, const ListRec& l,
                                (const double*)w->th + 3 * cap * t, (const uint*)w->tc + np * t, (const Real*)c->rad,
                                make_law<double>(c->mat.pp), c->cfg.dt, c->cfg.density, (const double*)w->Hb[hb],
                                w->Hb[1 - hb], (const double*)w->Xb2[in], (const double*)w->Db2[in],
-                               (const double*)w->Ab2[in], w->PC, w->pon, w->pbar));
+                               (const double*)w->Ab2[in], w->PC, w->pon, w->pbar, l.blist, l.nb,
+                               (const double*)w->twh + 3 * np * t, make_law<double>(c->mat.pw), c->cfg.world[0] * 0.5,
+                               c->cfg.world[1] * 0.5, w->WS, w->wson, w->Wb));
         DEM_CUDA_TRY(launch_ex(k_adj_bound<Real>, w->grid_bound, kAB, w->rs, pdl, c->n, np, cap, L, l.blist, l.nb,
-                               tx, td, ta, (const double*)w->twh + 3 * np * t, (const double*)w->tF + 3 * np * t,
-                               (const double*)w->tT + 3 * np * t, (const Real*)c->rad, make_law<double>(c->mat.pw),
-                               c->cfg.dt, c->cfg.density, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5,
-                               (const double*)w->PC, (const uint*)w->pon, (const double*)w->Xb2[in],
-                               (const double*)w->Db2[in], (const double*)w->Ab2[in], w->Xb2[1 - in], w->Db2[1 - in],
-                               w->Ab2[1 - in], w->Wb, w->Rb, w->pbar));
+                               (const double*)w->tF + 3 * np * t, (const double*)w->tT + 3 * np * t,
+                               (const Real*)c->rad, c->cfg.dt, c->cfg.density, (const double*)w->PC,
+                               (const uint*)w->pon, (const double*)w->WS, (const uint*)w->wson,
+                               (const double*)w->Xb2[in], (const double*)w->Db2[in], (const double*)w->Ab2[in],
+                               w->Xb2[1 - in], w->Db2[1 - in], w->Ab2[1 - in], w->Rb));
         return DEM_OK;
     }
     // a reversed step that directly follows another is launched programmatic
@@ -953,19 +1022,6 @@ void reverse_parities(long long every, int K, int& hb, int& in) {
     }
 }
 
-// Graphs of one dem_adjoint_window call, indexed by the tape set and the
-// parities at the segment start (recompute: list buffer; reverse sweep: hb,
-// in): a graph holds the set's addresses.
-struct SegmentGraphs {
-    cudaGraphExec_t g[2][2][2] = {};
-    ~SegmentGraphs() {
-        for (auto& set : g)
-            for (auto& row : set)
-                for (cudaGraphExec_t& e : row)
-                    if (e) cudaGraphExecDestroy(e);
-    }
-};
-
 // Captures what `enqueue` puts on stream s as a graph (once) and launches it.
 template <typename F> int run_captured(cudaStream_t s, cudaGraphExec_t& ge, F enqueue) {
     if (!ge) {
@@ -1045,7 +1101,13 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     c->observe_slot = -1;   // the recompute writes no observables
     int hb = 0;   // Hb[hb]: adjoint of the pair history output by the step being reversed
     int in = 0;   // state-adjoint set of the state after the step being reversed
-    SegmentGraphs fgraph, rgraph;
+    if (w->graph_every != every) {
+        w->fgraph.drop();
+        w->rgraph.drop();
+        w->graph_every = every;
+    }
+    SegmentGraphs& fgraph = w->fgraph;
+    SegmentGraphs& rgraph = w->rgraph;
     // Segment g is recomputed into tape set g & 1 on the context's stream and
     // reversed from it on the reverse stream, so the recompute of segment g-1
     // (into the other set) runs beside the reverse of segment g: the two are
@@ -1176,6 +1238,14 @@ extern "C" int dem_adjoint_window(dem_ctx* c, long long nsteps, int every, int w
     return DEM_OK;
 }
 
+namespace dem {
+void adjoint_drop_graphs(dem_ctx* c) {
+    if (!c->adj) return;
+    c->adj->fgraph.drop();
+    c->adj->rgraph.drop();
+}
+}  // namespace dem
+
 extern "C" int dem_adjoint_release(dem_ctx* c) {
     if (!c || !c->adj) return DEM_OK;
     AdjWork* w = c->adj;
@@ -1183,7 +1253,7 @@ extern "C" int dem_adjoint_release(dem_ctx* c) {
     for (Ck& k : w->ck) free_ck(k);
     if (w->rs) cudaStreamSynchronize(w->rs);
     void* p[] = {w->Xb2[0], w->Db2[0], w->Ab2[0], w->Xb2[1], w->Db2[1], w->Ab2[1], w->Wb, w->Rb, w->Hb[0], w->Hb[1],
-                 w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj, w->objp, w->PC, w->pon};
+                 w->pbar, w->obj, w->zmax, w->save_mz, w->save_cnt, w->Pobj, w->objp, w->PC, w->pon, w->WS, w->wson};
     for (void* x : p)
         if (x) cudaFree(x);
     for (TapeSet& t : w->set) free_set(t);

@@ -1757,6 +1757,7 @@ void free_graphs(dem_ctx* c) {
                         cudaGraphExecDestroy(c->gexec[a][b][h][t]);
                         c->gexec[a][b][h][t] = nullptr;
                     }
+    adjoint_drop_graphs(c);
 }
 
 void free_cells(dem_ctx* c) {

@@ -316,6 +316,8 @@ int step_kernels(dem_ctx* c, int lst, int slot, double* ms_pair, double* ms_part
 int window_kernel(dem_ctx* c, int lst, const WindowTape* tape);
 // Whether PCCP windows run as cluster batches (set at dem_create).
 bool use_batches(const dem_ctx* c);
+// Drops the adjoint's cached graphs (with the engine's: they hold its parameters).
+void adjoint_drop_graphs(dem_ctx* c);
 // The host copy of the particle order (c->hperm), fetched from the device
 // (one copy and a stream wait) when an upload computed a new one.
 int host_perm(dem_ctx* c);

@@ -176,6 +176,37 @@ def test_adjoint_leaves_forward_state(dem, cuda):
     assert a.scalars()["status"] == 0
 
 
+def test_repeated_calls_and_material_change(dem, cuda):
+    """One context, several calls: the adjoint's graphs are kept across calls
+    of the same segment length, so a second call from the same state gives
+    the same bits; after a material change (the graphs hold the contact
+    parameters) it gives the new material's gradients, bit for bit those of
+    a fresh context; another checkpoint interval recaptures."""
+    w, pdis, angv = case(dem)
+    kw = {**w.engine_kwargs(), "precision": dem.PREC_FP64, "cell": w.cell() + 0.01}
+    e = dem.Engine(**kw)
+    e.set_material(w.pp, w.pw)
+
+    def call(every=EVERY):
+        e.upload(w.pos, w.rad, pdis, angv)
+        r = e.adjoint(STEPS, every, dem.OBJ_POTENTIAL)
+        assert e.scalars()["status"] == 0
+        return r
+
+    r1, r2 = call(), call()
+    assert r1["value"] == r2["value"] and r1["d_pp"] == r2["d_pp"] and r1["d_pw"] == r2["d_pw"]
+    np.testing.assert_array_equal(r1["d_radii"], r2["d_radii"])
+    pp2, pw2 = scaled(w.pp, "mu", 1.5), scaled(w.pw, "mu", 1.5)
+    e.set_material(pp2, pw2)
+    r3 = call()
+    fresh = run_adjoint(dem, w, pdis, angv, pp2, pw2, w.rad, dem.OBJ_POTENTIAL)
+    assert r3["d_pp"] == fresh["d_pp"] and r3["d_pw"] == fresh["d_pw"] and r3["value"] == fresh["value"]
+    assert r3["d_pp"] != r1["d_pp"]
+    r4 = call(every=2 * EVERY if STEPS % (2 * EVERY) == 0 else STEPS)
+    assert abs(r4["value"] - r3["value"]) <= 1e-12 * abs(r3["value"])
+    e.close()
+
+
 def test_plain_and_programmatic_reverse_sweeps_agree(dem, cuda, monkeypatch):
     """The reverse steps launched programmatically (the default: each loads
     its tape before waiting for its predecessor) and plainly (DEM_B200_PDL=0)

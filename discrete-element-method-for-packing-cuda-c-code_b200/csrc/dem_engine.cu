@@ -178,54 +178,6 @@ __global__ void k_pour_activate(long long nold, long long nnew, const PRec<Real>
 }
 
 // --------------------------------------------------------------- re-list
-// Cell key per particle (calcHashD's role, neiglist.cu:77-97) and per-cell
-// counts; resets the displacement-since-list q (dempacking.cu:541).
-// Also lists the wall candidates of the coming window: particles closer to a
-// wall than r + skin/2 (a particle moves less than skin/2 per window, which
-// the step checks, so no other particle can touch a wall before the next
-// re-list -- the same guarantee as the pair list's).
-template <typename Real>
-__global__ void k_hash_count(long long n, const PRec<Real>* __restrict__ S, GridC g, uint* __restrict__ key,
-                             uint* __restrict__ count, uint* __restrict__ arrival, const Real* __restrict__ R,
-                             double hx, double hy, double half_skin, uint* __restrict__ wslot,
-                             uint* __restrict__ wlist, uint* __restrict__ wcount, uint* __restrict__ cc_parent,
-                             uint* __restrict__ cc_zero, long long np) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (cc_parent) {   // the coming re-list's components start as singletons
-        cc_parent[i] = (uint)i;
-        cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
-    }
-    const V3<double> p = ld_pos<false>(S + i);
-    {
-        const double x = p.x, y = p.y, z = p.z;
-        const double mg = (double)R[i] + half_skin;
-        const bool near = (z < mg) || (x + hx < mg) || (hx - x < mg) || (y + hy < mg) || (hy - y < mg);
-        // one atomic per warp for its candidates (slot order within a warp
-        // follows the lanes; the slots only name the candidates)
-        const uint act = __activemask();
-        const uint m = __ballot_sync(act, near);
-        uint base = 0;
-        const int lead = __ffs(act) - 1;
-        if ((int)lane_id() == lead && m) base = atomicAdd(wcount, (uint)__popc(m));
-        base = __shfl_sync(act, base, lead);
-        uint ws = kEmpty;
-        if (near) {
-            ws = base + (uint)__popc(m & ((1u << lane_id()) - 1u));
-            wlist[ws] = (uint)i;
-        }
-        wslot[i] = ws;
-    }
-    const Real csr = (Real)g.cs;
-    Real xl;
-    int cx = cell_axis<Real>(p.x, g.ox, csr, g.gx, xl);
-    int cy = cell_axis<Real>(p.y, g.oy, csr, g.gy, xl);
-    int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
-    uint c = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
-    key[i] = c;
-    arrival[i] = atomicAdd(&count[c], 1u);   // the particle's slot among its cell's members (unordered)
-}
-
 // Scatter each particle (id, cell, list coordinates x,y,z,r in the list
 // precision) into its cell's range at its arrival slot, unordered inside the
 // cell, and record each particle's slot (tpos); the count array returns to
@@ -256,92 +208,203 @@ __global__ void k_scatter(long long n, const uint* __restrict__ key, const uint*
     tpos[i] = slot;
 }
 
-// Order each cell's members by id: together with the counting scatter this is
-// the stable sort by cell of calcHash + RadixSort (dempacking.cu:545-555).
-// Run on request only (dem_download_cells); the re-list needs no order inside
-// a cell.
+// Row candidates kept per particle by the candidate pass; longer rows are
+// filtered again by the fill.
+constexpr uint kScr = 8;
+
+// ------------------------------------------------------------- outer list
+// The re-list searches candidates in an outer list: per particle every other
+// particle within r_i + r_j + oskin (both directions; oskin = skin + ext,
+// ext = min(skin, r_max / 10)) at the outer build, found by the cell walk on
+// a grid of cells >= 2 r_max + oskin.  The list is kept while no particle is
+// farther than odelta = 0.4 ext from its position at the build: a pair within
+// r_i + r_j + skin now was within r_i + r_j + skin + 2 odelta < r_i + r_j +
+// oskin then (with room for the rounding of the FP32 tests), so filtering the
+// outer rows with the exact candidate test gives exactly the pairs the cell
+// walk would give.  In a window graph the build is the body of a conditional
+// node that the check kernel switches on; an eager re-list always builds.
+
+// A particle's list coordinates (as k_scatter writes them): position relative
+// to the grid origin and radius, in the list precision.
 template <typename Real>
-__global__ void k_rank(long long n, const uint* __restrict__ cstart, const uint* __restrict__ sidu,
-                       const uint* __restrict__ skeyu, const R4<Real>* __restrict__ sposu, uint* __restrict__ sid2,
-                       uint* __restrict__ skey, R4<Real>* __restrict__ spos) {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const uint i = sidu[t];
-    const uint c = skeyu[t];
-    const uint s = cstart[c], e = cstart[c + 1];
-    uint rank = 0;
-    for (uint u = s; u < e; u++) rank += (sidu[u] < i) ? 1u : 0u;
-    sid2[s + rank] = i;
-    skey[s + rank] = c;
-    spos[s + rank] = sposu[t];
+__device__ __forceinline__ R4<Real> rec_r4(const PRec<Real>* __restrict__ S, const Real* __restrict__ R, uint i,
+                                           const GridC& g) {
+    const V3<double> p = ld_pos<false>(S + i);
+    R4<Real> v;
+    v.x = (Real)(p.x - g.ox);
+    v.y = (Real)(p.y - g.oy);
+    v.z = (Real)(p.z - g.oz);
+    v.w = R[i];
+    return v;
 }
 
-// Walk the 27 cells around sorted slot t and either count (FILL=false) or
-// write (FILL=true) candidates.  Returns (count of j>i, count of all).
+// Switches the build on when the outer list is invalid (oflag) or a particle
+// moved more than odelta since the build.
+template <typename Real>
+__global__ void k_outer_check(long long n, const PRec<Real>* __restrict__ S, Planes3<double> xo, double odelta2,
+                              const uint* __restrict__ oflag, cudaGraphConditionalHandle h) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool need = i == 0 && *oflag != 0u;
+    if (i < n) {
+        const V3<double> p = ld_pos<false>(S + i);
+        const double dx = p.x - xo.x[i], dy = p.y - xo.y[i], dz = p.z - xo.z[i];
+        need = need || !(dx * dx + dy * dy + dz * dz <= odelta2);
+    }
+    if (__any_sync(0xffffffffu, need) && lane_id() == 0) cudaGraphSetConditional(h, 1u);
+}
+
+// Cell key of each particle on the outer grid (calcHashD's role,
+// neiglist.cu:77-97), and its slot among the cell's members (the counting
+// sort of k_scatter).
+template <typename Real>
+__global__ void k_cell_hash(long long n, const PRec<Real>* __restrict__ S, GridC g, uint* __restrict__ key,
+                            uint* __restrict__ count, uint* __restrict__ arrival) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3<double> p = ld_pos<false>(S + i);
+    const Real csr = (Real)g.cs;
+    Real xl;
+    const int cx = cell_axis<Real>(p.x, g.ox, csr, g.gx, xl);
+    const int cy = cell_axis<Real>(p.y, g.oy, csr, g.gy, xl);
+    const int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
+    const uint c = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
+    key[i] = c;
+    arrival[i] = atomicAdd(&count[c], 1u);
+}
+
+// The outer walk from sorted slot t: every candidate within r_i + r_j + oskin
+// in the 27 cells (both directions); FILL writes them at out (capacity cap).
 template <typename Real, bool FILL>
-__device__ __forceinline__ void walk27(long long t, uint i, const R4<Real>& me, uint c, GridC g,
-                                       const uint* __restrict__ cstart, const uint* __restrict__ sid2,
-                                       const R4<Real>* __restrict__ spos, Real skin, uint& nup, uint& nall,
-                                       uint* __restrict__ out, uint outcap) {
+__device__ __forceinline__ uint walk27_all(long long t, const R4<Real>& me, uint c, const GridC& g,
+                                           const uint* __restrict__ cstart, const uint* __restrict__ sid2,
+                                           const R4<Real>* __restrict__ spos, Real oskin, uint* __restrict__ out,
+                                           uint outcap) {
     const int cx = (int)(c % (uint)g.gx);
     const int cy = (int)((c / (uint)g.gx) % (uint)g.gy);
     const int cz = (int)(c / ((uint)g.gx * (uint)g.gy));
-    nup = 0;
-    nall = 0;
-    // The cells x-1..x+1 of one (y, z) row are contiguous in the sorted order:
-    // 9 ranges instead of 27 cells.  All 18 range bounds are loaded up front
-    // (independent loads), then the candidates are tested.
     const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < g.gx - 1 ? cx + 1 : g.gx - 1;
-    uint rs[9], re[9];
-#pragma unroll
+    uint nall = 0;
     for (int r = 0; r < 9; r++) {
         const int z = cz - 1 + r / 3, y = cy - 1 + r % 3;
-        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) { rs[r] = 0; re[r] = 0; continue; }
+        if (z < 0 || z >= g.gz || y < 0 || y >= g.gy) continue;
         const uint rowc = ((uint)z * (uint)g.gy + (uint)y) * (uint)g.gx;
-        rs[r] = cstart[rowc + x0];
-        re[r] = cstart[rowc + x1 + 1];
-    }
-#pragma unroll
-    for (int r = 0; r < 9; r++) {
-        for (uint u = rs[r]; u < re[r]; u++) {
+        const uint u0 = cstart[rowc + x0], u1 = cstart[rowc + x1 + 1];
+        for (uint u = u0; u < u1; u++) {
             if ((long long)u == t) continue;
-            const R4<Real> o = spos[u];
-            if (cand_test<Real>(me, o, skin)) {
+            if (cand_test<Real>(me, spos[u], oskin)) {
+                if (FILL && nall < outcap) out[nall] = sid2[u];
                 nall++;
-                const uint j = sid2[u];
-                if (j > i) {
-                    if (FILL && nup < outcap) out[nup] = j;
-                    nup++;
-                }
             }
         }
     }
+    return nall;
 }
 
-// The re-list walk: per sorted slot t, count the candidates j > i (row of i)
-// and j < i (reverse row of i) and keep the first kScr j > i candidates in
-// scr[i * kScr ...]; rows longer than kScr are walked again by the fill.
-// A particle with any candidate or a wall candidacy is BOUND for the window
-// (bflag = 1), otherwise FREE.
-constexpr uint kScr = 8;
-
+// Outer build, count pass: each particle's outer row length.
 template <typename Real>
-__global__ void k_nbr_walk(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
-                           const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
-                           const uint* __restrict__ wslot, uint* __restrict__ njgi, uint* __restrict__ njli,
-                           uint* __restrict__ bflag, uint* __restrict__ scr, EngineWords* words) {
-    pdl_wait();
+__global__ void k_outer_count(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
+                              const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real oskin,
+                              uint* __restrict__ ocnt) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    ocnt[sid2[t]] = walk27_all<Real, false>(t, spos[t], skey[t], g, cstart, sid2, spos, oskin, nullptr, 0);
+}
+
+// Outer build, fill pass: the rows, each particle's position at the build,
+// and the list marked valid (or, beyond the capacity, the capacity status and
+// the list left invalid).
+template <typename Real>
+__global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
+                             const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real oskin,
+                             const uint* __restrict__ coff, uint* __restrict__ cln, long long ccap,
+                             const PRec<Real>* __restrict__ S, Planes3<double> xo, uint* __restrict__ oflag,
+                             EngineWords* words) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool over = (long long)coff[n] > ccap;
+    if (t == 0) {
+        *oflag = over ? 1u : 0u;
+        if (over) atomicOr(&words->status, kStCapacity);
+    }
+    if (t >= n || over) return;
+    const uint i = sid2[t];
+    const uint b = coff[i];
+    walk27_all<Real, true>(t, spos[t], skey[t], g, cstart, sid2, spos, oskin, cln + b, coff[i + 1] - b);
+    const V3<double> p = ld_pos<false>(S + i);
+    xo.x[i] = p.x; xo.y[i] = p.y; xo.z[i] = p.z;
+}
+
+// The re-list's candidate pass on the outer list, per particle i (id order):
+// the cluster-batch arrays start the re-list as singletons, the wall
+// candidacy takes a slot (within r + skin/2 of a wall: a particle moves less
+// than skin/2 per window, which the step checks, so no other particle can
+// touch a wall before the next re-list -- the pair list's guarantee), the
+// particle's cell on the configured grid is kept (dem_download_cells), and
+// the outer row is
+// filtered with the exact candidate test on the list coordinates: the counts
+// of the row (j > i) and of the reverse row (j < i), the first kScr row
+// candidates, and the bound flag (any candidate or a wall candidacy).
+template <typename Real>
+__global__ void k_filter(long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g,
+                         Real skin, const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap,
+                         double hx, double hy, double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist,
+                         uint* __restrict__ wcount, uint* __restrict__ cc_parent, uint* __restrict__ cc_zero,
+                         long long np, uint* __restrict__ ikey, uint* __restrict__ njgi, uint* __restrict__ njli,
+                         uint* __restrict__ bflag, uint* __restrict__ scr, EngineWords* words) {
     pdl_trigger();
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     uint nall = 0;
-    if (t < n) {
-        const uint i = sid2[t];
-        uint nup;
-        walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, scr + (size_t)i * kScr,
-                           kScr);
+    if (ii < n) {
+        const uint i = (uint)ii;
+        if (cc_parent) {   // the coming re-list's components start as singletons
+            cc_parent[i] = i;
+            cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
+        }
+        const V3<double> p = ld_pos<false>(S + i);
+        const double mg = (double)R[i] + half_skin;
+        const bool near = (p.z < mg) || (p.x + hx < mg) || (hx - p.x < mg) || (p.y + hy < mg) || (hy - p.y < mg);
+        {
+            const Real csr = (Real)g.cs;
+            Real xl;
+            const int cx = cell_axis<Real>(p.x, g.ox, csr, g.gx, xl);
+            const int cy = cell_axis<Real>(p.y, g.oy, csr, g.gy, xl);
+            const int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
+            ikey[i] = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
+        }
+        uint nup = 0;
+        if ((long long)coff[n] <= ccap) {
+            R4<Real> me;
+            me.x = (Real)(p.x - g.ox);
+            me.y = (Real)(p.y - g.oy);
+            me.z = (Real)(p.z - g.oz);
+            me.w = R[i];
+            uint* out = scr + (size_t)i * kScr;
+            for (uint k = coff[i], k1 = coff[i + 1]; k < k1; k++) {
+                const uint j = cln[k];
+                if (cand_test<Real>(me, rec_r4<Real>(S, R, j, g), skin)) {
+                    nall++;
+                    if (j > i) {
+                        if (nup < kScr) out[nup] = j;
+                        nup++;
+                    }
+                }
+            }
+        }
         njgi[i] = nup;
         njli[i] = nall - nup;
-        bflag[i] = (nall > 0 || wslot[i] != kEmpty) ? 1u : 0u;
+        // one atomic per warp for its wall candidates (slots only name them)
+        const uint act = __activemask();
+        const uint m = __ballot_sync(act, near);
+        uint base = 0;
+        const int lead = __ffs(act) - 1;
+        if ((int)lane_id() == lead && m) base = atomicAdd(wcount, (uint)__popc(m));
+        base = __shfl_sync(act, base, lead);
+        uint ws = kEmpty;
+        if (near) {
+            ws = base + (uint)__popc(m & ((1u << lane_id()) - 1u));
+            wlist[ws] = i;
+        }
+        wslot[i] = ws;
+        bflag[i] = (nall > 0 || near) ? 1u : 0u;
     }
     nall = __reduce_max_sync(0xffffffffu, nall);
     if (lane_id() == 0 && nall) atomicMax(&words->max_row, nall);
@@ -359,15 +422,15 @@ __device__ __forceinline__ void isort_u32(uint* a, uint len) {
 // Fill the CSR row of i (j>i ascending), carry the FP64 tangential history
 // from the previous list, record the reverse slots.
 template <typename Real>
-__global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<Real>* __restrict__ spos,
-                           const uint* __restrict__ skey, const uint* __restrict__ cstart, GridC g, Real skin,
+__global__ void k_nbr_fill(long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g,
+                           Real skin, const uint* __restrict__ coff, const uint* __restrict__ cln,
                            const uint* __restrict__ off, const uint* __restrict__ roff, uint* __restrict__ njli,
                            uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
                            const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
                            uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
                            uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,
                            const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist,
-                           const uint* __restrict__ tpos, uint* cc_parent, const uint* __restrict__ cc_skip) {
+                           uint* cc_parent, const uint* __restrict__ cc_skip) {
     pdl_wait();
     pdl_trigger();
     const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // particle order
@@ -388,10 +451,13 @@ __global__ void k_nbr_fill(long long n, const uint* __restrict__ sid2, const R4<
     if (e == b) return;
     if (e - b <= kScr) {
         for (uint k = 0; k < e - b; k++) ln[b + k] = scr[(size_t)i * kScr + k];
-    } else {   // a long row: walk again from the particle's sorted slot
-        const uint t = tpos[i];
-        uint nup, nall;
-        walk27<Real, true>(t, i, spos[t], skey[t], g, cstart, sid2, spos, skin, nup, nall, ln + b, e - b);
+    } else {   // a long row: filter the particle's outer row again
+        const R4<Real> me = rec_r4<Real>(S, R, i, g);
+        uint w = 0;
+        for (uint k = coff[i], k1 = coff[i + 1]; k < k1 && w < e - b; k++) {
+            const uint j = cln[k];
+            if (j > i && cand_test<Real>(me, rec_r4<Real>(S, R, j, g), skin)) ln[b + w++] = j;
+        }
     }
     isort_u32(ln + b, e - b);
     const bool old_ok = (long long)ooff[n] <= cap;   // an overflowed old list carries nothing
@@ -1790,6 +1856,69 @@ StepPartials free_partials(const dem_ctx* c, int slot) {
 
 // List build from the current state, carrying history from list buffer src
 // (phase c->hph) into buffer 1-src (phase 0).
+// The outer build on stream st (plain launches: in a graph it is the body of
+// a conditional node): cells of the outer grid, their scan, the counting
+// scatter, the row lengths, their scan, the rows.
+template <typename Real> int outer_build(dem_ctx* c, const PRec<Real>* S, cudaStream_t st) {
+    const long long n = c->n;
+    const int B = 256;
+    const GridC og = c->ogrid;
+    k_cell_hash<Real><<<grid_for(n, B), B, 0, st>>>(n, S, og, c->key, c->ccount, c->arrival);
+    DEM_LAUNCH_CHECK();
+    int rc = exclusive_scan_u32(c->ccount, c->cstart, c->oncells, c->cstart + c->oncells, c->scan_tmp, st, false);
+    if (rc) return rc;
+    k_scatter<Real><<<grid_for(n, B), B, 0, st>>>(n, (const uint*)c->key, (const uint*)c->arrival,
+                                                  (const uint*)c->cstart, c->ccount, S, (const Real*)c->rad, og,
+                                                  c->sid, c->skeyu, (R4<Real>*)c->sposu, c->tpos);
+    DEM_LAUNCH_CHECK();
+    const Real oskin = (Real)c->oskin;
+    k_outer_count<Real><<<grid_for(n, B), B, 0, st>>>(n, (const uint*)c->sid, (const R4<Real>*)c->sposu,
+                                                      (const uint*)c->skeyu, (const uint*)c->cstart, og, oskin,
+                                                      c->ocnt);
+    DEM_LAUNCH_CHECK();
+    if ((rc = exclusive_scan_u32(c->ocnt, c->coff, n, c->coff + n, c->scan_tmp, st, false))) return rc;
+    k_outer_fill<Real><<<grid_for(n, B), B, 0, st>>>(n, (const uint*)c->sid, (const R4<Real>*)c->sposu,
+                                                     (const uint*)c->skeyu, (const uint*)c->cstart, og, oskin,
+                                                     (const uint*)c->coff, c->cln, c->ccap, S,
+                                                     planes<double>(c->xo, c->npad), c->oflag, c->words);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
+// In a capture: k_outer_check, then a conditional node whose body (captured
+// on the context's build stream) is the outer build; the capture goes on
+// after the node.
+template <typename Real> int outer_build_conditional(dem_ctx* c, const PRec<Real>* S) {
+    cudaStream_t s = c->stream;
+    cudaStreamCaptureStatus st;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    DEM_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    DEM_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+    k_outer_check<Real><<<grid_for(c->n, 256), 256, 0, s>>>(c->n, S, planes<double>(c->xo, c->npad), c->odelta2,
+                                                            (const uint*)c->oflag, h);
+    DEM_LAUNCH_CHECK();
+    DEM_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    DEM_CUDA_TRY(cudaGraphAddNode(&node, cg, deps, nd, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    DEM_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    DEM_CUDA_TRY(cudaStreamBeginCaptureToGraph(c->cstream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const int rc = outer_build<Real>(c, S, c->cstream);
+    cudaGraph_t got = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->cstream, &got);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (outer build)", __FILE__, __LINE__);
+    return DEM_OK;
+}
+
 template <typename Real> int launch_relist(dem_ctx* c, int src) {
     const long long n = c->n;
     const int dst = 1 - src;
@@ -1805,22 +1934,27 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         DEM_CUDA_TRY(cudaMemsetAsync(c->cc_bw, 0xff, nbb * sizeof(uint), s));
         DEM_CUDA_TRY(cudaMemsetAsync(c->cc_bw + nbb, 0, 2 * nbb * sizeof(uint), s));
     }
-    k_hash_count<Real><<<grid_for(n, B), B, 0, s>>>(n, S, g, c->key, c->ccount, c->arrival, (const Real*)c->rad,
-                                                    c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
-                                                    c->wslot, c->wlist, c->wcount, cc ? c->cc_parent : nullptr,
-                                                    c->cc_size, c->npad);
     // every launch after the first is programmatic: each kernel waits for its
     // predecessor before it touches memory, so only the launch latency overlaps
     const bool pdl = c->pdl && !c->profiling;
-    int rc = exclusive_scan_u32(c->ccount, c->cstart, c->ncells, c->cstart + c->ncells, c->scan_tmp, s, pdl);
+    // the outer list: rebuilt when needed (a graph's conditional node, switched
+    // by k_outer_check), always in an eager re-list
+    cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+    DEM_CUDA_TRY(cudaStreamIsCapturing(s, &cst));
+    int rc;
+    if (cst == cudaStreamCaptureStatusActive) {
+        rc = outer_build_conditional<Real>(c, S);
+    } else {
+        rc = outer_build<Real>(c, S, s);
+    }
     if (rc) return rc;
-    DEM_CUDA_TRY(launch_ex(k_scatter<Real>, grid_for(n, B), B, s, pdl, n, (const uint*)c->key, (const uint*)c->arrival,
-                           (const uint*)c->cstart, c->ccount, S, (const Real*)c->rad, g, c->sid, c->skeyu,
-                           (R4<Real>*)c->sposu, c->tpos));
     const Real skin = (Real)c->cfg.skin;
-    DEM_CUDA_TRY(launch_ex(k_nbr_walk<Real>, grid_for(n, B), B, s, pdl, n, (const uint*)c->sid,
-                           (const R4<Real>*)c->sposu, (const uint*)c->skeyu, (const uint*)c->cstart, g, skin,
-                           (const uint*)c->wslot, c->njgi, c->njli, c->bflag, c->scr, c->words));
+    k_filter<Real><<<grid_for(n, B), B, 0, s>>>(n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
+                                                (const uint*)c->cln, c->ccap, c->cfg.world[0] * 0.5,
+                                                c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin, c->wslot, c->wlist,
+                                                c->wcount, cc ? c->cc_parent : nullptr, c->cc_size, c->npad, c->ikey,
+                                                c->njgi, c->njli, c->bflag, c->scr, c->words);
+    DEM_LAUNCH_CHECK();
     {
         const uint* in[3] = {c->njgi, c->njli, c->bflag};
         uint* out[3] = {c->off[dst], c->roff, c->bpos};
@@ -1829,12 +1963,12 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         if (rc) return rc;
     }
     DEM_CUDA_TRY(launch_ex(
-        k_nbr_fill<Real>, grid_for(n, B), B, s, pdl, n, (const uint*)c->sid, (const R4<Real>*)c->sposu,
-        (const uint*)c->skeyu, (const uint*)c->cstart, g, skin, (const uint*)c->off[dst], (const uint*)c->roff,
+        k_nbr_fill<Real>, grid_for(n, B), B, s, pdl, n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
+        (const uint*)c->cln, (const uint*)c->off[dst], (const uint*)c->roff,
         c->njli, c->ln[dst], c->lp, planes<double>(c->hist[dst][0], c->cap), (const uint*)c->off[src],
         (const uint*)c->ln[src], planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap,
         c->words, c->carry, (const uint*)c->scr, (const uint*)c->bflag, (const uint*)c->bpos, c->blist, c->flist,
-        (const uint*)c->tpos, cc ? c->cc_parent : nullptr, (const uint*)c->cc_skip));
+        cc ? c->cc_parent : nullptr, (const uint*)c->cc_skip));
     DEM_CUDA_TRY(launch_ex(k_rev_sort, grid_for(n, B), B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
                            (const uint*)c->off[dst], c->cap, cc ? c->cc_parent : nullptr, (const uint*)c->bflag,
                            c->cc_size, c->cc_pairs, (const uint*)c->cc_skip));
@@ -2195,6 +2329,8 @@ int pour_insert(dem_ctx* c) {
     c->vol = 4.0 / 3.0 * M_PI * c->r3sum[nnew];
     c->in_window = 0;   // this step re-lists (m_hiall = 1)
     free_graphs(c);     // the particle count is part of every captured launch
+    // the new particles have no outer rows yet
+    DEM_CUDA_TRY(cudaMemsetAsync(c->oflag, 0x01, sizeof(uint), c->stream));
     return DEM_OK;
 }
 
@@ -2265,8 +2401,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         for (int h = 0; h < nstate; h++)
             if ((rc = dalloc(&c->hist[l][h], 3 * cap))) return bail(rc);
     if ((rc = dalloc(&c->wh, 3 * np)) || (rc = dalloc(&c->q, np)) || (rc = dalloc(&c->staging, 10 * np)) ||
-        (rc = dalloc(&c->key, np)) || (rc = dalloc(&c->sid, np)) || (rc = dalloc(&c->sid2, np)) ||
-        (rc = dalloc(&c->skeyu, np)) || (rc = dalloc(&c->skey, np)) || (rc = dalloc(&c->njgi, np)) ||
+        (rc = dalloc(&c->key, np)) || (rc = dalloc(&c->sid, np)) ||
+        (rc = dalloc(&c->skeyu, np)) || (rc = dalloc(&c->njgi, np)) ||
         (rc = dalloc(&c->njli, np)) || (rc = dalloc(&c->off[0], np + 1)) || (rc = dalloc(&c->off[1], np + 1)) ||
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
         (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->ru, cap)) || (rc = dalloc(&c->words, 1)) ||
@@ -2275,10 +2411,19 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->bflag, np)) || (rc = dalloc(&c->bpos, np + 1)) || (rc = dalloc(&c->blist, np)) ||
         (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, kBarWords)) || (rc = dalloc(&c->tpos, np)))
         return bail(rc);
+    // the outer candidate list (rows in both directions; its skin is set
+    // with the grid, from r_max): four times the pair capacity
+    c->ccap = std::min<long long>(4 * cap, 0x7fffffffLL);
+    if ((rc = dalloc(&c->coff, np + 1)) || (rc = dalloc(&c->cln, c->ccap)) || (rc = dalloc(&c->ocnt, np)) ||
+        (rc = dalloc(&c->xo, 3 * np)) || (rc = dalloc(&c->oflag, 2)) || (rc = dalloc(&c->ikey, np)))
+        return bail(rc);
+    e = cudaMemsetAsync(c->oflag, 0x01, sizeof(uint), s0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->coff, 0, (np + 1) * sizeof(uint), s0);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "outer list set-up", __FILE__, __LINE__));
     e = cudaMalloc(&c->wf, 2 * np * 4 * rs);
     if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc (wall forces)", __FILE__, __LINE__));
     e = cudaMalloc(&c->rad, np * rs);
-    if (e == cudaSuccess) e = cudaMalloc(&c->spos, np * 4 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->sposu, np * 4 * rs);
     if (e == cudaSuccess) e = cudaMalloc(&c->pf, cap * 4 * rs);
     if (e == cudaSuccess && c->mode == DEM_FORCE_PCCP) e = cudaMalloc(&c->pti, cap * 4 * rs);
@@ -2388,7 +2533,8 @@ int dem_destroy(dem_ctx* c) {
     free_graphs(c);
     free_cells(c);
     void* ptrs[] = {c->rec[0], c->rec[1], c->rad, c->q, c->wh,
-                    c->staging, c->key, c->sid, c->sid2, c->spos, c->skeyu, c->skey, c->sposu, c->njgi, c->njli,
+                    c->staging, c->key, c->sid, c->skeyu, c->sposu, c->njgi, c->njli, c->coff, c->cln, c->ocnt,
+                    c->xo, c->oflag, c->ikey,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
@@ -2406,6 +2552,7 @@ int dem_destroy(dem_ctx* c) {
     if (c->evjoin) cudaEventDestroy(c->evjoin);
     for (cudaEvent_t e : c->wev) cudaEventDestroy(e);
     if (c->stream2) cudaStreamDestroy(c->stream2);
+    if (c->cstream) cudaStreamDestroy(c->cstream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return DEM_OK;
@@ -2450,14 +2597,26 @@ static int setup_grid(dem_ctx* c) {
     g.gz = (int)(c->cfg.world[2] / cs) + 1;
     const long long nc = (long long)g.gx * g.gy * g.gz;
     if (nc > 0x7fffffffLL) return fail(DEM_ERR_ARG, "grid of %lld cells too large", nc);
-    if (nc != c->ncells) {
+    // the outer list: skin + ext, ext = min(skin, r_max / 10), kept while no
+    // particle has moved 0.4 ext; its grid: cells of at least 2 r_max + oskin,
+    // same origin
+    const double ext = std::min(c->cfg.skin, 0.1 * c->rmax);
+    c->oskin = c->cfg.skin + ext;
+    c->odelta2 = (0.4 * ext) * (0.4 * ext);
+    GridC og = g;
+    og.cs = std::max(cs, 2.0 * c->rmax + c->oskin + 1e-4);
+    og.gx = (int)(c->cfg.world[0] / og.cs) + 1;
+    og.gy = (int)(c->cfg.world[1] / og.cs) + 1;
+    og.gz = (int)(c->cfg.world[2] / og.cs) + 1;
+    const long long onc = (long long)og.gx * og.gy * og.gz;
+    if (onc != c->oncells) {
         free_graphs(c);
         free_cells(c);
         int rc;
-        if ((rc = dalloc(&c->ccount, nc)) || (rc = dalloc(&c->cstart, nc + 1))) return rc;
-        DEM_CUDA_TRY(cudaMemsetAsync(c->ccount, 0, nc * sizeof(uint), c->stream));
-        c->ncells = nc;
-        size_t need = scan_scratch_words(std::max<long long>(nc, c->npad + 1));
+        if ((rc = dalloc(&c->ccount, onc)) || (rc = dalloc(&c->cstart, onc + 1))) return rc;
+        DEM_CUDA_TRY(cudaMemsetAsync(c->ccount, 0, onc * sizeof(uint), c->stream));
+        c->oncells = onc;
+        size_t need = scan_scratch_words(std::max<long long>(onc, c->npad + 1));
         if (need > c->scan_words) {
             DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
             cudaFree(c->scan_tmp);
@@ -2466,8 +2625,13 @@ static int setup_grid(dem_ctx* c) {
             c->scan_words = need;
         }
     }
-    if (g.cs != c->grid.cs || g.gx != c->grid.gx || g.gy != c->grid.gy || g.gz != c->grid.gz) free_graphs(c);
+    const auto same = [](const GridC& a, const GridC& b) {
+        return a.cs == b.cs && a.gx == b.gx && a.gy == b.gy && a.gz == b.gz;
+    };
+    if (!same(g, c->grid) || !same(og, c->ogrid)) free_graphs(c);
     c->grid = g;
+    c->ncells = nc;
+    c->ogrid = og;
     return DEM_OK;
 }
 
@@ -2477,6 +2641,8 @@ static int finish_upload(dem_ctx* c) {
     DEM_CUDA_TRY(cudaMemsetAsync(c->off[1], 0, (c->npad + 1) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->words, 0, sizeof(EngineWords), c->stream));
     if (c->cc_skip) DEM_CUDA_TRY(cudaMemsetAsync(c->cc_skip, 0, 2 * sizeof(uint), c->stream));
+    // the outer list is rebuilt at the first re-list (new positions, radii)
+    DEM_CUDA_TRY(cudaMemsetAsync(c->oflag, 0x01, sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->part_mz, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(unsigned long long),
                                  c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->part_cnt, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(uint), c->stream));
@@ -3024,39 +3190,39 @@ int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsign
     if (!c) return fail(DEM_ERR_ARG, "dem_download_cells: null ctx");
     if (!c->uploaded || c->relists == 0) return fail(DEM_ERR_STATE, "dem_download_cells: no list built yet");
     const long long n = c->n, nc = c->ncells;
-    // the re-list left each cell's members in arrival order: order them by id
-    if (c->prec == DEM_PREC_MIXED)
-        k_rank<float><<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->cstart, c->sid, c->skeyu,
-                                                               (const R4<float>*)c->sposu, c->sid2, c->skey,
-                                                               (R4<float>*)c->spos);
-    else
-        k_rank<double><<<grid_for(n, 256), 256, 0, c->stream>>>(n, c->cstart, c->sid, c->skeyu,
-                                                                (const R4<double>*)c->sposu, c->sid2, c->skey,
-                                                                (R4<double>*)c->spos);
-    DEM_LAUNCH_CHECK();
-    if (ids) DEM_CUDA_TRY(cudaMemcpyAsync(ids, c->sid2, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    if (keys) DEM_CUDA_TRY(cudaMemcpyAsync(keys, c->skey, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    std::vector<uint> cs;
-    const bool remap = c->ordered && ids;
-    if (cell_start || cell_end || remap) {
-        if ((cell_start || cell_end) && ncells_cap < nc)
-            return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
-        cs.resize(nc + 1);
-        DEM_CUDA_TRY(cudaMemcpyAsync(cs.data(), c->cstart, (nc + 1) * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
-    }
+    if ((cell_start || cell_end) && ncells_cap < nc)
+        return fail(DEM_ERR_ARG, "dem_download_cells: cell capacity %lld < %lld", ncells_cap, nc);
+    // each particle's cell on the configured grid at the last re-list, sorted
+    // here by (cell, caller's id): the stable sort of calcHash + RadixSort
+    std::vector<uint> key(n);
+    DEM_CUDA_TRY(cudaMemcpyAsync(key.data(), c->ikey, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    if (remap) {   // the caller's ids, ascending inside each cell
+    if (c->ordered) {
         const int rp = host_perm(c);
         if (rp) return rp;
-        for (long long t = 0; t < n; t++) ids[t] = c->hperm[ids[t]];
-        for (long long cc = 0; cc < nc; cc++)
-            if (cs[cc + 1] - cs[cc] > 1) std::sort(ids + cs[cc], ids + cs[cc + 1]);
+    }
+    std::vector<unsigned long long> kv(n);
+    for (long long t = 0; t < n; t++) {
+        const uint id = c->ordered ? c->hperm[t] : (uint)t;
+        kv[t] = ((unsigned long long)key[t] << 32) | id;
+    }
+    std::sort(kv.begin(), kv.end());
+    for (long long t = 0; t < n; t++) {
+        if (keys) keys[t] = (uint)(kv[t] >> 32);
+        if (ids) ids[t] = (uint)(kv[t] & 0xffffffffu);
     }
     if (cell_start || cell_end) {
         for (long long cc = 0; cc < nc; cc++) {
-            bool empty = cs[cc] == cs[cc + 1];
-            if (cell_start) cell_start[cc] = empty ? kEmpty : cs[cc];
-            if (cell_end) cell_end[cc] = empty ? kEmpty : cs[cc + 1];
+            if (cell_start) cell_start[cc] = kEmpty;
+            if (cell_end) cell_end[cc] = kEmpty;
+        }
+        for (long long t = 0; t < n; t++) {
+            const uint k = (uint)(kv[t] >> 32);
+            if (k >= (uint)nc) return fail(DEM_ERR_STATE, "dem_download_cells: cell key %u outside the grid", k);
+            if (t == 0 || (uint)(kv[t - 1] >> 32) != k)
+                if (cell_start) cell_start[k] = (uint)t;
+            if (t == n - 1 || (uint)(kv[t + 1] >> 32) != k)
+                if (cell_end) cell_end[k] = (uint)(t + 1);
         }
     }
     return DEM_OK;

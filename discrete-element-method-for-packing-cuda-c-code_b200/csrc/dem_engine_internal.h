@@ -187,9 +187,12 @@ struct dem_ctx {
     cudaEvent_t ext_ready = nullptr;  // orders legacy-stream work before device uploads
     dem_material mat{};
     bool have_mat = false;
-    // grid
+    // grid: the configured one (cell keys of dem_download_cells), and the
+    // outer list's (cells >= 2 r_max + oskin), whose cell arrays the re-list uses
     GridC grid{};
     long long ncells = 0;
+    GridC ogrid{};
+    long long oncells = 0;
     double rmax = 0.0;
     double vol = 0.0;        // sum (4/3) pi r^3
     // state: [current buffer]; the second buffer exists in PP mode only
@@ -199,14 +202,11 @@ struct dem_ctx {
     float4* q = nullptr;
     double* wh = nullptr;    // 3 planes
     double* staging = nullptr;   // 10n doubles
-    // list
+    // list: the outer build's cell arrays (outer grid)
     uint* key = nullptr;
     uint* sid = nullptr;     // unordered within cells (scatter)
-    uint* sid2 = nullptr;    // sorted by (cell, id)
     uint* skeyu = nullptr;
-    uint* skey = nullptr;
     void* sposu = nullptr;
-    void* spos = nullptr;
     uint* ccount = nullptr;
     uint* cstart = nullptr;
     uint* njgi = nullptr;
@@ -218,6 +218,18 @@ struct dem_ctx {
     uint* bpos = nullptr;    // exclusive scan of bflag; bpos[n] = number of bound particles
     uint* blist = nullptr;   // bound particle ids, ascending
     uint* flist = nullptr;   // free particle ids, ascending
+    // outer candidate list: rows of every particle within r_i + r_j + oskin
+    // at the build (both directions), kept while every particle stays within
+    // odelta of its position then (oskin, odelta: set with the grid)
+    double oskin = 0.0, odelta2 = 0.0;
+    uint* coff = nullptr;    // np + 1: row offsets
+    uint* cln = nullptr;     // ccap: candidates
+    long long ccap = 0;
+    uint* ocnt = nullptr;    // np: row lengths (build)
+    double* xo = nullptr;    // 3 planes: positions at the build
+    uint* oflag = nullptr;   // [0] nonzero: the list is invalid (rebuild at the next re-list)
+    uint* ikey = nullptr;    // np: each particle's cell on the configured grid at the last re-list
+    cudaStream_t cstream = 0;        // captures the outer build into its conditional node
     cudaStream_t stream2 = 0;        // free-particle branch of the window graph
     cudaEvent_t evfork = nullptr, evjoin = nullptr;
     bool free_in_window = false;     // capturing: the free particles run as one window kernel

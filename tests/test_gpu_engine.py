@@ -68,6 +68,33 @@ def test_cells_and_pairs_bit_exact(dem, orc, wl, cuda, prec, case):
     assert lp.size > 0
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_lists_from_the_outer_list_equal_fresh_lists(dem, orc, wl, cuda, prec):
+    """The re-list filters an outer candidate list (built at twice the skin
+    and rebuilt once a particle has moved 0.4 skin): after hundreds of
+    windows of falling, colliding spheres -- many rebuilds and many windows
+    between them -- each window's list equals the oracle's fresh cell-walk
+    list at the positions of its re-list, bit for bit."""
+    w = wl.lattice_2k()
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    e = make_engine(dem, w, p)
+    cell = e.grid_info()[1]
+    K = w.relist_interval
+    for m, windows in enumerate((1, 60, 200, 37, 400)):
+        e.step(windows * K)
+        pos = e.download()[0]
+        e.step(1)   # the re-list at these positions
+        lp, ln, _ = e.pairs()
+        off, oln, _, _ = orc.build_list(pos, w.rad, w.world, cell, w.skin, prec == "mixed")
+        olp = np.repeat(np.arange(w.n, dtype=np.uint32), np.diff(off))
+        np.testing.assert_array_equal(lp, olp)
+        np.testing.assert_array_equal(ln, oln)
+        assert e.scalars()["status"] == 0
+        e.step(K - 1)
+    assert lp.size > 1000   # a bed with contacts by the end
+    e.close()
+
+
 @pytest.mark.parametrize("case", ["small", "dense"])
 @pytest.mark.parametrize("prec,rtol", [("fp64", 1e-9), ("mixed", 2e-4)])
 def test_first_step_forces(dem, orc, wl, cuda, prec, rtol, case):

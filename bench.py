@@ -12,8 +12,9 @@ stays as hot as it is in a real run.
 
 Besides the headline the JSON line carries: the FP64 plain form and the
 particle-parallel force mode on the same workload; the same 500,000 spheres
-as a settled bed (every sphere in contact: the contact path under load) with
-its window kernel's HBM roofline; the 4,000,000-sphere bidisperse workload;
+as a settled bed (every sphere bound, ~3 contacts per sphere: the contact
+path under load) with its window kernel's HBM roofline; the
+4,000,000-sphere bidisperse workload;
 the adjoint window's cost; the end-to-end figure through the public API with
 host buffers; and the FP64 oracle on the host cores, whose sample also gives
 the mixed form's error against it.
@@ -46,9 +47,17 @@ BYTES_PER_PARTICLE = {"mixed": 172, "fp64": 200}   # per particle-step, all fiel
 BYTES_PER_PAIR = 56                                 # ids 8 + FP64 history r+w 48, per pair-step
 METRIC = "particle-steps/s @500K spheres"
 UNIT = "particle-steps/s"
-KERNELS_RELIST = 11           # hash, 3-launch cell scan, scatter, walk, 3-launch triple scan, fill, reverse sort
-KERNELS_BATCHES = 3 + 3       # with cluster batches: component slots, particle slots, batches; the window
-                              # kernel (exits unless a batch is too large), the free particles, the batches
+def launches_per_window(work, coop):
+    """Kernels a window graph launches when its outer candidate list stays
+    valid (a rebuild adds the 10 launches of the conditional node's body):
+    the outer check, then the cooperative re-list (or, one kernel per pass:
+    filter, 3-launch triple scan, fill, reverse rows, and with cluster
+    batches the component slots, particle slots and batches); then the window
+    kernel, which with cluster batches exits unless a batch is too large, the
+    free particles and the batches."""
+    batching = work.get("batched", -1) >= 0
+    relist = 2 if coop else 7 + (3 if batching else 0)
+    return relist + (3 if batching else 1)
 
 
 def load_pkg():
@@ -415,7 +424,7 @@ def run_ours(args):
                    "mean_cn": sc["mean_cn"]},
         "roofline": head_roof,
         "clocks": clk,
-        "gpu_launches": (KERNELS_RELIST + (KERNELS_BATCHES if work.get("batched") is not None else 1)) * K,
+        "gpu_launches": launches_per_window(work, os.environ.get("DEM_B200_RELIST_COOP", "1") != "0") * K,
         "fp64_plain": fp64,
         "pp_mode": ppm,
         "settled_bed": bed,

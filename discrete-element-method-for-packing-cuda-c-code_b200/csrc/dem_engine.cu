@@ -343,15 +343,22 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
 // filtered with the exact candidate test on the list coordinates: the counts
 // of the row (j > i) and of the reverse row (j < i), the first kScr row
 // candidates, and the bound flag (any candidate or a wall candidacy).
-template <typename Real>
-__global__ void k_filter(long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g,
-                         Real skin, const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap,
-                         double hx, double hy, double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist,
-                         uint* __restrict__ wcount, uint* __restrict__ cc_parent, uint* __restrict__ cc_zero,
-                         long long np, uint* __restrict__ ikey, uint* __restrict__ njgi, uint* __restrict__ njli,
-                         uint* __restrict__ bflag, uint* __restrict__ scr, EngineWords* words) {
-    pdl_trigger();
-    const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Each re-list pass is a device function of one index, called by its own
+// kernel (the per-kernel re-list: DEM_B200_RELIST_COOP=0, or no cooperative
+// launch) and by a phase of the cooperative re-list; DEM_*_PARAMS /
+// DEM_*_ARGS spell its parameters once for both.
+#define DEM_FILTER_PARAMS                                                                                      \
+    long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                   \
+        const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap, double hx, double hy,        \
+        double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist, uint* __restrict__ wcount,          \
+        uint* __restrict__ cc_parent, uint* __restrict__ cc_zero, long long np, uint* __restrict__ ikey,           \
+        uint* __restrict__ njgi, uint* __restrict__ njli, uint* __restrict__ bflag, uint* __restrict__ scr
+#define DEM_FILTER_ARGS \
+    n, S, R, g, skin, coff, cln, ccap, hx, hy, half_skin, wslot, wlist, wcount, cc_parent, cc_zero, np, ikey, njgi, \
+        njli, bflag, scr
+// One particle of the candidate pass; returns its candidate count (row and
+// reverse row).
+template <typename Real> __device__ __forceinline__ uint filter_item(long long ii, DEM_FILTER_PARAMS) {
     uint nall = 0;
     if (ii < n) {
         const uint i = (uint)ii;
@@ -406,6 +413,12 @@ __global__ void k_filter(long long n, const PRec<Real>* __restrict__ S, const Re
         wslot[i] = ws;
         bflag[i] = (nall > 0 || near) ? 1u : 0u;
     }
+    return nall;
+}
+
+template <typename Real> __global__ void k_filter(DEM_FILTER_PARAMS, EngineWords* words) {
+    pdl_trigger();
+    uint nall = filter_item<Real>((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_FILTER_ARGS);
     nall = __reduce_max_sync(0xffffffffu, nall);
     if (lane_id() == 0 && nall) atomicMax(&words->max_row, nall);
 }
@@ -421,19 +434,19 @@ __device__ __forceinline__ void isort_u32(uint* a, uint len) {
 
 // Fill the CSR row of i (j>i ascending), carry the FP64 tangential history
 // from the previous list, record the reverse slots.
-template <typename Real>
-__global__ void k_nbr_fill(long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g,
-                           Real skin, const uint* __restrict__ coff, const uint* __restrict__ cln,
-                           const uint* __restrict__ off, const uint* __restrict__ roff, uint* __restrict__ njli,
-                           uint* __restrict__ ln, uint* __restrict__ lp, Planes3<double> H,
-                           const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,
-                           uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,
-                           uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,
-                           const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist,
-                           uint* cc_parent, const uint* __restrict__ cc_skip) {
-    pdl_wait();
-    pdl_trigger();
-    const long long ii = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // particle order
+#define DEM_FILL_PARAMS                                                                                               \
+    long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                    \
+    const uint* __restrict__ coff, const uint* __restrict__ cln, const uint* __restrict__ off,                        \
+    const uint* __restrict__ roff, uint* __restrict__ njli, uint* __restrict__ ln, uint* __restrict__ lp,             \
+    Planes3<double> H, const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,               \
+    uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,                              \
+    uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,                           \
+    const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist, uint* cc_parent,               \
+    const uint* __restrict__ cc_skip
+#define DEM_FILL_ARGS                                                                                                 \
+    n, S, R, g, skin, coff, cln, off, roff, njli, ln, lp, H, ooff, oln, OH, rk, pf, cap, words, carry,                \
+    scr, bflag, bpos, blist, flist, cc_parent, cc_skip
+template <typename Real> __device__ __forceinline__ void fill_item(long long ii, DEM_FILL_PARAMS) {
     if (ii >= n) return;
     if (cc_parent && *cc_skip) cc_parent = nullptr;   // a dense bed: no component pass this re-list
     const uint i = (uint)ii;
@@ -491,17 +504,23 @@ __global__ void k_nbr_fill(long long n, const PRec<Real>* __restrict__ S, const 
     }
 }
 
+template <typename Real> __global__ void k_nbr_fill(DEM_FILL_PARAMS) {
+    pdl_wait();
+    pdl_trigger();
+    fill_item<Real>((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_FILL_ARGS);
+}
+
 // Sort each reverse row (pair indices ascending: a deterministic order for
 // the gather) and record each pair's reverse slot ru[k].
 // With cluster batches (parent != nullptr): every bound particle also takes
 // its component's root (all unions were made by the fill) and adds itself and
 // its row's pairs to the root's counts.
-__global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,
-                           const uint* __restrict__ off, long long cap, uint* parent, const uint* __restrict__ bflag,
-                           uint* __restrict__ csize, uint* __restrict__ cpairs, const uint* __restrict__ cc_skip) {
-    pdl_wait();
-    pdl_trigger();
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#define DEM_REVSORT_PARAMS                                                                                            \
+    long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,                         \
+    const uint* __restrict__ off, long long cap, uint* parent, const uint* __restrict__ bflag,                        \
+    uint* __restrict__ csize, uint* __restrict__ cpairs, const uint* __restrict__ cc_skip
+#define DEM_REVSORT_ARGS n, roff, rk, ru, off, cap, parent, bflag, csize, cpairs, cc_skip
+__device__ __forceinline__ void revsort_item(long long i, DEM_REVSORT_PARAMS) {
     if (i >= n) return;
     if (parent && *cc_skip) parent = nullptr;
     if ((long long)off[n] > cap) return;
@@ -514,6 +533,12 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
         atomicAdd(csize + r, 1u);
         atomicAdd(cpairs + r, off[i + 1] - off[i]);
     }
+}
+
+__global__ void k_rev_sort(DEM_REVSORT_PARAMS) {
+    pdl_wait();
+    pdl_trigger();
+    revsort_item((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_REVSORT_ARGS);
 }
 
 // ------------------------------------------------------- cluster batches
@@ -533,13 +558,12 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
 
 // A slot range per component (roots only; one atomic per warp for the slot
 // counter), and the largest component.
-__global__ void k_cc_base(long long n, long long cap, const uint* __restrict__ blist, const uint* __restrict__ bpos,
-                          const uint* __restrict__ off, const uint* __restrict__ parent,
-                          const uint* __restrict__ size, uint* __restrict__ base, uint* __restrict__ ccw,
-                          const uint* __restrict__ cc_skip) {
-    pdl_wait();
-    pdl_trigger();
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#define DEM_CCBASE_PARAMS                                                                                             \
+    long long n, long long cap, const uint* __restrict__ blist, const uint* __restrict__ bpos,                        \
+    const uint* __restrict__ off, const uint* __restrict__ parent, const uint* __restrict__ size,                     \
+    uint* __restrict__ base, uint* __restrict__ ccw, const uint* __restrict__ cc_skip
+#define DEM_CCBASE_ARGS n, cap, blist, bpos, off, parent, size, base, ccw, cc_skip
+__device__ __forceinline__ void cc_base_warp(long long t, DEM_CCBASE_PARAMS) {
     if (*cc_skip) {   // no components this re-list: the grid-barrier window kernel has the window
         if (t == 0) atomicOr(ccw + 1, 1u);
         return;
@@ -570,6 +594,12 @@ __global__ void k_cc_base(long long n, long long cap, const uint* __restrict__ b
     if (sz) base[i] = wbase + inc - sz;
 }
 
+__global__ void k_cc_base(DEM_CCBASE_PARAMS) {
+    pdl_wait();
+    pdl_trigger();
+    cc_base_warp((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_CCBASE_ARGS);
+}
+
 // The batch window: the bound particles spread over the batch kernel's
 // resident blocks G, at least kBatchMin, at most P minus the largest component
 // (so that a window's components and the tail of its last one fit a block).
@@ -584,13 +614,13 @@ __device__ __forceinline__ uint cc_target(uint nb, uint G, uint P, uint maxc) {
 // component to the batch window its first slot falls in: the window's first
 // slot (minimum), particles and pairs.  bw: [0, nbb) first slots, [nbb, 2 nbb)
 // particles, [2 nbb, 3 nbb) pairs.
-__global__ void k_cc_slot(long long n, long long nbb, uint G, uint P, const uint* __restrict__ blist,
-                          const uint* __restrict__ bpos, const uint* __restrict__ parent, const uint* __restrict__ base,
-                          const uint* __restrict__ size, const uint* __restrict__ pairs, uint* __restrict__ fill,
-                          uint* __restrict__ order, uint* __restrict__ bw, uint* __restrict__ ccw) {
-    pdl_wait();
-    pdl_trigger();
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#define DEM_CCSLOT_PARAMS                                                                                             \
+    long long n, long long nbb, uint G, uint P, const uint* __restrict__ blist,                                       \
+    const uint* __restrict__ bpos, const uint* __restrict__ parent, const uint* __restrict__ base,                    \
+    const uint* __restrict__ size, const uint* __restrict__ pairs, uint* __restrict__ fill,                           \
+    uint* __restrict__ order, uint* __restrict__ bw, uint* __restrict__ ccw
+#define DEM_CCSLOT_ARGS n, nbb, G, P, blist, bpos, parent, base, size, pairs, fill, order, bw, ccw
+__device__ __forceinline__ void cc_slot_item(long long t, DEM_CCSLOT_PARAMS) {
     if (ccw[1]) return;   // the window goes to the grid-barrier kernel already
     const uint nb = bpos[n];
     const uint tgt = cc_target(nb, G, P, ccw[2]);
@@ -620,15 +650,21 @@ __global__ void k_cc_slot(long long n, long long nbb, uint G, uint P, const uint
     }
 }
 
+__global__ void k_cc_slot(DEM_CCSLOT_PARAMS) {
+    pdl_wait();
+    pdl_trigger();
+    cc_slot_item((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_CCSLOT_ARGS);
+}
+
 // First slot of batch b (the first component whose first slot is b * target
 // or later; all bound particles when none is), and the batch's particles and
 // pairs against the block's capacity (P, Q).
-__global__ void k_cc_batches(long long n, long long nbmax, long long nbb, uint P, uint Q, const uint* __restrict__ bpos,
-                             const uint* __restrict__ bw, uint* __restrict__ batch, uint* __restrict__ ccw,
-                             uint* __restrict__ cc_skip) {
-    pdl_wait();
-    pdl_trigger();
-    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#define DEM_CCBATCH_PARAMS                                                                                            \
+    long long n, long long nbmax, long long nbb, uint P, uint Q, const uint* __restrict__ bpos,                       \
+    const uint* __restrict__ bw, uint* __restrict__ batch, uint* __restrict__ ccw,                                    \
+    uint* __restrict__ cc_skip
+#define DEM_CCBATCH_ARGS n, nbmax, nbb, P, Q, bpos, bw, batch, ccw, cc_skip
+__device__ __forceinline__ void cc_batches_item(long long b, DEM_CCBATCH_PARAMS) {
     if (b == 0) {
         // a component larger than a block (a dense bed): the next kDenseSkip
         // re-lists skip the component pass (union-find on one giant
@@ -649,6 +685,12 @@ __global__ void k_cc_batches(long long n, long long nbmax, long long nbb, uint P
     if (s0 == 0xffffffffu || s0 > nb) s0 = nb;
     batch[b] = s0;
     if (bw[nbb + b] > P || bw[2 * nbb + b] > Q) atomicOr(ccw + 1, 1u);
+}
+
+__global__ void k_cc_batches(DEM_CCBATCH_PARAMS) {
+    pdl_wait();
+    pdl_trigger();
+    cc_batches_item((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_CCBATCH_ARGS);
 }
 
 // ------------------------------------------------------------ pair force
@@ -1856,6 +1898,152 @@ StepPartials free_partials(const dem_ctx* c, int slot) {
 
 // List build from the current state, carrying history from list buffer src
 // (phase c->hph) into buffer 1-src (phase 0).
+// ------------------------------------------------------ cooperative re-list
+// The re-list after the outer list's check (and build) as one cooperative
+// launch: the candidate filter, the scan of the row / reverse-row / bound
+// counts, the fill, the reverse rows, and the component pass, as phases
+// separated by the bounded grid barrier (a kernel boundary per phase cost
+// its launch, its tail and its ramp: each of these passes is a few
+// microseconds of work over all particles).  Every phase calls the device
+// functions of the per-kernel re-list (used by eager re-lists), so the lists
+// are the same bits.
+constexpr int kRelistThreads = 256;
+
+template <typename Real> struct RelistCoop {
+    long long n, np, cap, ccap, nbb, nbmax;
+    const PRec<Real>* S;
+    const Real* R;
+    GridC g;
+    Real skin;
+    double hx, hy, half_skin;
+    const uint *coff, *cln, *ooff, *oln;
+    uint *wslot, *wlist, *wcount, *cc_parent, *cc_zero, *ikey, *njgi, *njli, *bflag, *scr;
+    uint *off, *roff, *ln, *lp, *rk, *ru, *carry, *bpos, *blist, *flist, *cc_skip;
+    Planes3<double> H, OH;
+    R4<Real>* pf;
+    EngineWords* words;
+    uint *csize, *cpairs, *base, *ccw, *fill, *order, *bw, *batch;
+    uint G, P, Q;
+    int cc;                  // the component pass runs (cluster batches)
+    uint* part;              // 3 per block: the scan's block totals
+    uint* bar;               // grid barrier (zeroed before the launch)
+};
+
+// Exclusive scans of njgi, njli, bflag into off, roff, bpos (totals at [n]):
+// block totals, a barrier, each block's prefix from the totals before it,
+// then the elements.  Block b scans the contiguous chunk [b C, (b+1) C).
+template <typename Real> __device__ __forceinline__ void coop_scan3(const RelistCoop<Real>& A, uint& nbar) {
+    const long long n = A.n;
+    const long long C = (n + gridDim.x - 1) / gridDim.x;
+    const long long lo = (long long)blockIdx.x * C, hi = min(n, lo + C);
+    const long long per = (C + blockDim.x - 1) / blockDim.x;
+    const long long t0 = lo + (long long)threadIdx.x * per, t1 = min(hi, t0 + per);
+    const uint* in[3] = {A.njgi, A.njli, A.bflag};
+    uint* out[3] = {A.off, A.roff, A.bpos};
+    __shared__ uint s_w[3][kRelistThreads / 32];
+    __shared__ uint s_blk[3];
+    uint sum[3] = {0u, 0u, 0u};
+    for (long long k = t0; k < t1; k++)
+        for (int a = 0; a < 3; a++) sum[a] += in[a][k];
+    // block exclusive scan of the thread sums
+    const uint lane = lane_id(), warp = threadIdx.x >> 5;
+    uint inc[3];
+    for (int a = 0; a < 3; a++) {
+        inc[a] = sum[a];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint v = __shfl_up_sync(0xffffffffu, inc[a], o);
+            if ((int)lane >= o) inc[a] += v;
+        }
+        if (lane == 31) s_w[a][warp] = inc[a];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        uint acc = 0;
+        for (uint w = 0; w < blockDim.x / 32; w++) { const uint v = s_w[threadIdx.x][w]; s_w[threadIdx.x][w] = acc; acc += v; }
+        A.part[3 * blockIdx.x + threadIdx.x] = acc;
+    }
+    __syncthreads();
+    uint run[3];
+    for (int a = 0; a < 3; a++) run[a] = s_w[a][warp] + inc[a] - sum[a];
+    grid_barrier(A.bar, nbar++, gridDim.x, A.words);
+    // this block's prefix: the totals of the blocks before it
+    uint pre[3] = {0u, 0u, 0u};
+    for (uint b = threadIdx.x; b < blockIdx.x; b += blockDim.x)
+        for (int a = 0; a < 3; a++) pre[a] += __ldcg(A.part + 3 * b + a);
+    for (int a = 0; a < 3; a++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pre[a] += __shfl_xor_sync(0xffffffffu, pre[a], o);
+    }
+    __syncthreads();   // s_w is reused for the prefix
+    if (lane == 0)
+        for (int a = 0; a < 3; a++) s_w[a][warp] = pre[a];
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        uint acc = 0;
+        for (uint w = 0; w < blockDim.x / 32; w++) acc += s_w[threadIdx.x][w];
+        s_blk[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    for (int a = 0; a < 3; a++) run[a] += s_blk[a];
+    for (long long k = t0; k < t1; k++)
+        for (int a = 0; a < 3; a++) {
+            const uint v = in[a][k];
+            out[a][k] = run[a];
+            run[a] += v;
+        }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x < 3)
+        out[threadIdx.x][n] = s_blk[threadIdx.x] + __ldcg(A.part + 3 * blockIdx.x + threadIdx.x);
+}
+
+template <typename Real> __global__ void __launch_bounds__(kRelistThreads) k_relist_coop(RelistCoop<Real> A) {
+    // the names of the per-kernel re-list's parameters
+    const long long n = A.n, np = A.np, cap = A.cap, ccap = A.ccap, nbb = A.nbb, nbmax = A.nbmax;
+    const PRec<Real>* S = A.S;
+    const Real* R = A.R;
+    const GridC g = A.g;
+    const Real skin = A.skin;
+    const double hx = A.hx, hy = A.hy, half_skin = A.half_skin;
+    const uint *coff = A.coff, *cln = A.cln, *ooff = A.ooff, *oln = A.oln;
+    uint *wslot = A.wslot, *wlist = A.wlist, *wcount = A.wcount, *cc_zero = A.cc_zero, *ikey = A.ikey;
+    uint *njgi = A.njgi, *njli = A.njli, *bflag = A.bflag, *scr = A.scr;
+    uint *off = A.off, *roff = A.roff, *ln = A.ln, *lp = A.lp, *rk = A.rk, *ru = A.ru, *carry = A.carry;
+    uint *bpos = A.bpos, *blist = A.blist, *flist = A.flist, *cc_skip = A.cc_skip;
+    uint* cc_parent = A.cc ? A.cc_parent : nullptr;
+    uint* parent = cc_parent;
+    const Planes3<double> H = A.H, OH = A.OH;
+    R4<Real>* pf = A.pf;
+    EngineWords* words = A.words;
+    uint *csize = A.csize, *cpairs = A.cpairs, *size = A.csize, *pairs = A.cpairs, *base = A.base, *ccw = A.ccw;
+    uint *fill = A.fill, *order = A.order, *bw = A.bw, *batch = A.batch;
+    const uint G = A.G, P = A.P, Q = A.Q;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nthr = (long long)gridDim.x * blockDim.x;
+    uint nbar = 0;
+    // candidate filter
+    uint mrow = 0;
+    for (long long ii = tid; ii < n; ii += nthr) mrow = max(mrow, filter_item<Real>(ii, DEM_FILTER_ARGS));
+    mrow = __reduce_max_sync(0xffffffffu, mrow);
+    if (lane_id() == 0 && mrow) atomicMax(&words->max_row, mrow);
+    grid_barrier(A.bar, nbar++, gridDim.x, words);
+    // row, reverse-row and bound counts: scans
+    coop_scan3<Real>(A, nbar);
+    grid_barrier(A.bar, nbar++, gridDim.x, words);
+    // rows, history carry, reverse slots, bound / free lists, unions
+    for (long long ii = tid; ii < n; ii += nthr) fill_item<Real>(ii, DEM_FILL_ARGS);
+    grid_barrier(A.bar, nbar++, gridDim.x, words);
+    // reverse rows in order; component roots and counts
+    for (long long i = tid; i < n; i += nthr) revsort_item(i, DEM_REVSORT_ARGS);
+    if (!A.cc) return;
+    grid_barrier(A.bar, nbar++, gridDim.x, words);
+    // components: slot ranges (whole warps), slots, batches
+    for (long long t = tid - lane_id(); t < n; t += nthr) cc_base_warp(t + lane_id(), DEM_CCBASE_ARGS);
+    grid_barrier(A.bar, nbar++, gridDim.x, words);
+    for (long long t = tid; t < n; t += nthr) cc_slot_item(t, DEM_CCSLOT_ARGS);
+    grid_barrier(A.bar, nbar++, gridDim.x, words);
+    for (long long b = tid; b <= nbmax; b += nthr) cc_batches_item(b, DEM_CCBATCH_ARGS);
+}
+
 // The outer build on stream st (plain launches: in a graph it is the body of
 // a conditional node): cells of the outer grid, their scan, the counting
 // scatter, the row lengths, their scan, the rows.
@@ -1942,13 +2130,46 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
     DEM_CUDA_TRY(cudaStreamIsCapturing(s, &cst));
     int rc;
-    if (cst == cudaStreamCaptureStatusActive) {
+    if (cst == cudaStreamCaptureStatusActive && c->outer_cond) {
         rc = outer_build_conditional<Real>(c, S);
     } else {
         rc = outer_build<Real>(c, S, s);
     }
     if (rc) return rc;
     const Real skin = (Real)c->cfg.skin;
+    if (c->coop_grid > 0) {   // the rest of the re-list in one cooperative launch
+        DEM_CUDA_TRY(cudaMemsetAsync(c->rbar, 0, kBarWords * sizeof(uint), s));
+        RelistCoop<Real> A;
+        A.n = n; A.np = c->npad; A.cap = c->cap; A.ccap = c->ccap;
+        A.nbb = c->nbatch_max + 2; A.nbmax = c->nbatch_max;
+        A.S = S; A.R = (const Real*)c->rad; A.g = g; A.skin = skin;
+        A.hx = c->cfg.world[0] * 0.5; A.hy = c->cfg.world[1] * 0.5; A.half_skin = 0.5 * c->cfg.skin;
+        A.coff = c->coff; A.cln = c->cln; A.ooff = c->off[src]; A.oln = c->ln[src];
+        A.wslot = c->wslot; A.wlist = c->wlist; A.wcount = c->wcount; A.cc_parent = c->cc_parent;
+        A.cc_zero = c->cc_size; A.ikey = c->ikey; A.njgi = c->njgi; A.njli = c->njli; A.bflag = c->bflag;
+        A.scr = c->scr; A.off = c->off[dst]; A.roff = c->roff; A.ln = c->ln[dst]; A.lp = c->lp; A.rk = c->rk;
+        A.ru = c->ru; A.carry = c->carry; A.bpos = c->bpos; A.blist = c->blist; A.flist = c->flist;
+        A.cc_skip = c->cc_skip;
+        A.H = planes<double>(c->hist[dst][0], c->cap);
+        A.OH = planes<double>(c->hist[src][c->hph], c->cap);
+        A.pf = (R4<Real>*)c->pf; A.words = c->words;
+        A.csize = c->cc_size; A.cpairs = c->cc_pairs; A.base = c->cc_base; A.ccw = c->cc_words;
+        A.fill = c->cc_fill; A.order = c->cc_order; A.bw = c->cc_bw; A.batch = c->cc_batch;
+        A.G = c->batch_grid; A.P = BatchCap<Real>::P; A.Q = BatchCap<Real>::Q;
+        A.cc = cc ? 1 : 0;
+        A.part = c->coop_part; A.bar = c->rbar;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c->coop_grid);
+        cfg.blockDim = dim3(kRelistThreads);
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_relist_coop<Real>, A));
+        return DEM_OK;
+    }
     k_filter<Real><<<grid_for(n, B), B, 0, s>>>(n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
                                                 (const uint*)c->cln, c->ccap, c->cfg.world[0] * 0.5,
                                                 c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin, c->wslot, c->wlist,
@@ -2415,7 +2636,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     // with the grid, from r_max): four times the pair capacity
     c->ccap = std::min<long long>(4 * cap, 0x7fffffffLL);
     if ((rc = dalloc(&c->coff, np + 1)) || (rc = dalloc(&c->cln, c->ccap)) || (rc = dalloc(&c->ocnt, np)) ||
-        (rc = dalloc(&c->xo, 3 * np)) || (rc = dalloc(&c->oflag, 2)) || (rc = dalloc(&c->ikey, np)))
+        (rc = dalloc(&c->xo, 3 * np)) || (rc = dalloc(&c->oflag, 2)) || (rc = dalloc(&c->ikey, np)) ||
+        (rc = dalloc(&c->rbar, kBarWords)))
         return bail(rc);
     e = cudaMemsetAsync(c->oflag, 0x01, sizeof(uint), s0);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->coff, 0, (np + 1) * sizeof(uint), s0);
@@ -2455,6 +2677,22 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_grid = (unsigned)std::max(1, nsm * wper);
         const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
+        // the cooperative re-list: one round of resident blocks
+        // (DEM_B200_RELIST_COOP=0: the per-kernel re-list)
+        {
+            int rper = 0;
+            e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, k_relist_coop<float>, kRelistThreads, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, k_relist_coop<double>, kRelistThreads, 0);
+            if (e != cudaSuccess) return bail(cuda_fail(e, "re-list kernel occupancy", __FILE__, __LINE__));
+            const char* rcoop = getenv("DEM_B200_RELIST_COOP");
+            const bool on = coop && rper > 0 && !(rcoop && rcoop[0] == '0');
+            c->coop_grid = on ? (unsigned)(nsm * rper) : 0u;
+            if (c->coop_grid && (rc = dalloc(&c->coop_part, 3 * (size_t)c->coop_grid))) return bail(rc);
+        }
+        // "0": the outer build in every re-list, no conditional node (a profiler
+        // does not see the kernel nodes of a graph that has conditional nodes)
+        const char* oc = getenv("DEM_B200_OUTER_COND");
+        c->outer_cond = !(oc && oc[0] == '0');
         const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches everywhere
         c->pdl = !(pdl && pdl[0] == '0');
         const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order
@@ -2534,7 +2772,7 @@ int dem_destroy(dem_ctx* c) {
     free_cells(c);
     void* ptrs[] = {c->rec[0], c->rec[1], c->rad, c->q, c->wh,
                     c->staging, c->key, c->sid, c->skeyu, c->sposu, c->njgi, c->njli, c->coff, c->cln, c->ocnt,
-                    c->xo, c->oflag, c->ikey,
+                    c->xo, c->oflag, c->ikey, c->rbar, c->coop_part,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
@@ -3312,7 +3550,7 @@ int dem_window_work(dem_ctx* c, long long* bound, long long* wall_candidates, lo
     if (bound) *bound = v[0];
     if (wall_candidates) *wall_candidates = v[1];
     if (pairs) *pairs = (long long)v[2] <= c->cap ? v[2] : 0;
-    if (batched) *batched = v[3] == 0u ? 1 : 0;
+    if (batched) *batched = !use_batches(c) ? -1 : (v[3] == 0u ? 1 : 0);
     return DEM_OK;
 }
 

@@ -230,6 +230,10 @@ struct dem_ctx {
     uint* oflag = nullptr;   // [0] nonzero: the list is invalid (rebuild at the next re-list)
     uint* ikey = nullptr;    // np: each particle's cell on the configured grid at the last re-list
     cudaStream_t cstream = 0;        // captures the outer build into its conditional node
+    bool outer_cond = true;          // DEM_B200_OUTER_COND=0: build in every re-list
+    unsigned coop_grid = 0;          // blocks of the cooperative re-list (0: the per-kernel re-list)
+    uint* coop_part = nullptr;       // 3 per block: its scan totals
+    uint* rbar = nullptr;            // its grid barrier
     cudaStream_t stream2 = 0;        // free-particle branch of the window graph
     cudaEvent_t evfork = nullptr, evjoin = nullptr;
     bool free_in_window = false;     // capturing: the free particles run as one window kernel

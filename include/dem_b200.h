@@ -326,7 +326,9 @@ int dem_window_kernel_times(dem_ctx* ctx, double out[5]);
  * *batched = 1 when the bound particles' connected components (through the
  * pair list) were small enough to be stepped as cluster batches, one block
  * per batch in shared memory, 0 when the grid-barrier window kernel stepped
- * them (a dense bed is one large component).  Any pointer may be NULL.  No
+ * them (a dense bed is one large component), -1 when the context does not
+ * batch (PP mode, DEM_B200_BATCH=0, per-step kernels).  Any pointer may be
+ * NULL.  No
  * counterpart in the reference (it steps every particle the same way). */
 int dem_window_work(dem_ctx* ctx, long long* bound, long long* wall_candidates, long long* pairs, int* batched);
 

@@ -70,8 +70,9 @@ def test_cells_and_pairs_bit_exact(dem, orc, wl, cuda, prec, case):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_lists_from_the_outer_list_equal_fresh_lists(dem, orc, wl, cuda, prec):
-    """The re-list filters an outer candidate list (built at twice the skin
-    and rebuilt once a particle has moved 0.4 skin): after hundreds of
+    """The re-list filters an outer candidate list (built at skin + ext,
+    ext = min(skin, r_max / 10), and rebuilt once a particle has moved 0.4
+    ext): after hundreds of
     windows of falling, colliding spheres -- many rebuilds and many windows
     between them -- each window's list equals the oracle's fresh cell-walk
     list at the positions of its re-list, bit for bit."""
@@ -93,6 +94,41 @@ def test_lists_from_the_outer_list_equal_fresh_lists(dem, orc, wl, cuda, prec):
         e.step(K - 1)
     assert lp.size > 1000   # a bed with contacts by the end
     e.close()
+
+
+@pytest.mark.parametrize("mode", ["pccp", "pp"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_cooperative_relist_equals_per_kernel_relist(dem, wl, cuda, monkeypatch, prec, mode):
+    """The re-list after the outer list as one cooperative launch (the
+    default: filter, scans, fill, reverse rows and component pass as phases
+    between grid barriers) and as one kernel per pass
+    (DEM_B200_RELIST_COOP=0) give the same lists, batches and states bit for
+    bit, on a sparse bed (cluster batches) and a dense lattice."""
+    from _cases import dense_lattice
+    p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
+    fm = dem.FORCE_PCCP if mode == "pccp" else dem.FORCE_PP
+    for w in (wl.small_box(n=3000), dense_lattice(dem, nx=10, ny=10, nz=8)):
+        rng = np.random.default_rng(11)
+        pdis = rng.normal(0, 2e-6, 3 * w.n)
+        a = make_engine(dem, w, p, force_mode=fm)
+        a.upload(w.pos, w.rad, pdis, None)
+        monkeypatch.setenv("DEM_B200_RELIST_COOP", "0")
+        b = make_engine(dem, w, p, force_mode=fm)
+        b.upload(w.pos, w.rad, pdis, None)
+        monkeypatch.delenv("DEM_B200_RELIST_COOP")
+        for steps in (4 * w.relist_interval, 3):
+            a.step(steps)
+            b.step(steps)
+            assert a.window_work() == b.window_work()
+            for x, y in zip(a.download(), b.download()):
+                np.testing.assert_array_equal(x, y)
+            for x, y in zip(a.pairs(), b.pairs()):
+                np.testing.assert_array_equal(x, y)
+        sa, sb = a.scalars(), b.scalars()
+        assert sa["status"] == 0 and sb["status"] == 0
+        assert sa["maxhz"] == sb["maxhz"] and sa["contacts"] == sb["contacts"] and sa["pairs"] == sb["pairs"]
+        a.close()
+        b.close()
 
 
 @pytest.mark.parametrize("case", ["small", "dense"])
@@ -423,7 +459,7 @@ def test_cluster_batches_equal_grid_barrier_window(dem, wl, cuda, monkeypatch, p
         a.step(4 * w.relist_interval)
         b.step(4 * w.relist_interval)
         wa, wb = a.window_work(), b.window_work()
-        assert wb["batched"] == 0 and (batched is None or wa["batched"] == batched), (w.name, wa, wb)
+        assert wb["batched"] == -1 and (batched is None or wa["batched"] == batched), (w.name, wa, wb)
         print(f"\n{w.name} n={w.n}: {wa}")
         assert wa["bound"] == wb["bound"] > 0
         for x, y in zip(a.download(), b.download()):

@@ -50,9 +50,10 @@ UNIT = "particle-steps/s"
 def launches_per_window(work, coop):
     """Kernels a window graph launches when its outer candidate list stays
     valid (a rebuild adds the 10 launches of the conditional node's body):
-    the outer check, then the cooperative re-list (or, one kernel per pass:
-    filter, 3-launch triple scan, fill, reverse rows, and with cluster
-    batches the component slots, particle slots and batches); then the window
+    the outer check, then one kernel per pass (filter, 3-launch triple scan,
+    fill, reverse rows, and with cluster batches the component slots,
+    particle slots and batches), or with DEM_B200_RELIST_COOP=1 the
+    cooperative re-list; then the window
     kernel, which with cluster batches exits unless a batch is too large, the
     free particles and the batches."""
     batching = work.get("batched", -1) >= 0
@@ -424,7 +425,7 @@ def run_ours(args):
                    "mean_cn": sc["mean_cn"]},
         "roofline": head_roof,
         "clocks": clk,
-        "gpu_launches": launches_per_window(work, os.environ.get("DEM_B200_RELIST_COOP", "1") != "0") * K,
+        "gpu_launches": launches_per_window(work, os.environ.get("DEM_B200_RELIST_COOP", "0") == "1") * K,
         "fp64_plain": fp64,
         "pp_mode": ppm,
         "settled_bed": bed,

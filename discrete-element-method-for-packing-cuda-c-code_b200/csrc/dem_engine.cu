@@ -344,8 +344,8 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
 // of the row (j > i) and of the reverse row (j < i), the first kScr row
 // candidates, and the bound flag (any candidate or a wall candidacy).
 // Each re-list pass is a device function of one index, called by its own
-// kernel (the per-kernel re-list: DEM_B200_RELIST_COOP=0, or no cooperative
-// launch) and by a phase of the cooperative re-list; DEM_*_PARAMS /
+// kernel (the per-kernel re-list, the default) and by a phase of the
+// cooperative re-list (DEM_B200_RELIST_COOP=1); DEM_*_PARAMS /
 // DEM_*_ARGS spell its parameters once for both.
 #define DEM_FILTER_PARAMS                                                                                      \
     long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                   \
@@ -2677,15 +2677,17 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_grid = (unsigned)std::max(1, nsm * wper);
         const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
-        // the cooperative re-list: one round of resident blocks
-        // (DEM_B200_RELIST_COOP=0: the per-kernel re-list)
+        // the cooperative re-list (DEM_B200_RELIST_COOP=1): one round of
+        // resident blocks; off by default, since in a graph its six grid
+        // barriers cost more than the launches they replace (108 us against
+        // 94 us per re-list of 500K spheres)
         {
             int rper = 0;
             e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, k_relist_coop<float>, kRelistThreads, 0)
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, k_relist_coop<double>, kRelistThreads, 0);
             if (e != cudaSuccess) return bail(cuda_fail(e, "re-list kernel occupancy", __FILE__, __LINE__));
             const char* rcoop = getenv("DEM_B200_RELIST_COOP");
-            const bool on = coop && rper > 0 && !(rcoop && rcoop[0] == '0');
+            const bool on = coop && rper > 0 && rcoop && rcoop[0] == '1';
             c->coop_grid = on ? (unsigned)(nsm * rper) : 0u;
             if (c->coop_grid && (rc = dalloc(&c->coop_part, 3 * (size_t)c->coop_grid))) return bail(rc);
         }

@@ -99,11 +99,11 @@ def test_lists_from_the_outer_list_equal_fresh_lists(dem, orc, wl, cuda, prec):
 @pytest.mark.parametrize("mode", ["pccp", "pp"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_cooperative_relist_equals_per_kernel_relist(dem, wl, cuda, monkeypatch, prec, mode):
-    """The re-list after the outer list as one cooperative launch (the
-    default: filter, scans, fill, reverse rows and component pass as phases
-    between grid barriers) and as one kernel per pass
-    (DEM_B200_RELIST_COOP=0) give the same lists, batches and states bit for
-    bit, on a sparse bed (cluster batches) and a dense lattice."""
+    """The re-list after the outer list as one kernel per pass (the default)
+    and as one cooperative launch (DEM_B200_RELIST_COOP=1: filter, scans,
+    fill, reverse rows and component pass as phases between grid barriers)
+    give the same lists, batches and states bit for bit, on a sparse bed
+    (cluster batches) and a dense lattice."""
     from _cases import dense_lattice
     p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
     fm = dem.FORCE_PCCP if mode == "pccp" else dem.FORCE_PP
@@ -112,7 +112,7 @@ def test_cooperative_relist_equals_per_kernel_relist(dem, wl, cuda, monkeypatch,
         pdis = rng.normal(0, 2e-6, 3 * w.n)
         a = make_engine(dem, w, p, force_mode=fm)
         a.upload(w.pos, w.rad, pdis, None)
-        monkeypatch.setenv("DEM_B200_RELIST_COOP", "0")
+        monkeypatch.setenv("DEM_B200_RELIST_COOP", "1")
         b = make_engine(dem, w, p, force_mode=fm)
         b.upload(w.pos, w.rad, pdis, None)
         monkeypatch.delenv("DEM_B200_RELIST_COOP")

@@ -47,17 +47,15 @@ BYTES_PER_PARTICLE = {"mixed": 172, "fp64": 200}   # per particle-step, all fiel
 BYTES_PER_PAIR = 56                                 # ids 8 + FP64 history r+w 48, per pair-step
 METRIC = "particle-steps/s @500K spheres"
 UNIT = "particle-steps/s"
-def launches_per_window(work, coop):
+def launches_per_window(work):
     """Kernels a window graph launches when its outer candidate list stays
     valid (a rebuild adds the 10 launches of the conditional node's body):
-    the outer check, then one kernel per pass (filter, 3-launch triple scan,
-    fill, reverse rows, and with cluster batches the component slots,
-    particle slots and batches), or with DEM_B200_RELIST_COOP=1 the
-    cooperative re-list; then the window
-    kernel, which with cluster batches exits unless a batch is too large, the
-    free particles and the batches."""
+    the outer check, the candidate pass with its scans, the fill, the reverse
+    rows, and with cluster batches the component slots, particle slots and
+    batches; then the window kernel, which with cluster batches exits unless
+    a batch is too large, the free particles and the batches."""
     batching = work.get("batched", -1) >= 0
-    relist = 2 if coop else 7 + (3 if batching else 0)
+    relist = 4 + (3 if batching else 0)
     return relist + (3 if batching else 1)
 
 
@@ -425,7 +423,7 @@ def run_ours(args):
                    "mean_cn": sc["mean_cn"]},
         "roofline": head_roof,
         "clocks": clk,
-        "gpu_launches": launches_per_window(work, os.environ.get("DEM_B200_RELIST_COOP", "0") == "1") * K,
+        "gpu_launches": launches_per_window(work) * K,
         "fp64_plain": fp64,
         "pp_mode": ppm,
         "settled_bed": bed,

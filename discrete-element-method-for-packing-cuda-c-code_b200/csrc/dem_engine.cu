@@ -334,19 +334,16 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
 }
 
 // The re-list's candidate pass on the outer list, per particle i (id order):
-// the cluster-batch arrays start the re-list as singletons, the wall
-// candidacy takes a slot (within r + skin/2 of a wall: a particle moves less
-// than skin/2 per window, which the step checks, so no other particle can
-// touch a wall before the next re-list -- the pair list's guarantee), the
-// particle's cell on the configured grid is kept (dem_download_cells), and
-// the outer row is
-// filtered with the exact candidate test on the list coordinates: the counts
-// of the row (j > i) and of the reverse row (j < i), the first kScr row
-// candidates, and the bound flag (any candidate or a wall candidacy).
-// Each re-list pass is a device function of one index, called by its own
-// kernel (the per-kernel re-list, the default) and by a phase of the
-// cooperative re-list (DEM_B200_RELIST_COOP=1); DEM_*_PARAMS /
-// DEM_*_ARGS spell its parameters once for both.
+// the wall candidacy takes a slot (within r + skin/2 of a wall: a particle
+// moves less than skin/2 per window, which the step checks, so no other
+// particle can touch a wall before the next re-list -- the pair list's
+// guarantee), the particle's cell on the configured grid is kept
+// (dem_download_cells), and the outer row is filtered with the exact
+// candidate test on the list coordinates: the counts of the row (j > i) and
+// of the reverse row (j < i), the first kScr row candidates, and the bound
+// flag (any candidate or a wall candidacy).  A bound particle starts the
+// re-list's components (cluster batches) as a singleton; free particles take
+// no part in them.
 #define DEM_FILTER_PARAMS                                                                                      \
     long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                   \
         const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap, double hx, double hy,        \
@@ -356,16 +353,12 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
 #define DEM_FILTER_ARGS \
     n, S, R, g, skin, coff, cln, ccap, hx, hy, half_skin, wslot, wlist, wcount, cc_parent, cc_zero, np, ikey, njgi, \
         njli, bflag, scr
-// One particle of the candidate pass; returns its candidate count (row and
-// reverse row).
-template <typename Real> __device__ __forceinline__ uint filter_item(long long ii, DEM_FILTER_PARAMS) {
-    uint nall = 0;
+// The three counts of one particle: row (j > i), reverse row (j < i), bound.
+struct FilterCounts { uint up, down, bound; };
+template <typename Real> __device__ __forceinline__ FilterCounts filter_item(long long ii, DEM_FILTER_PARAMS) {
+    FilterCounts o = {0u, 0u, 0u};
     if (ii < n) {
         const uint i = (uint)ii;
-        if (cc_parent) {   // the coming re-list's components start as singletons
-            cc_parent[i] = i;
-            cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
-        }
         const V3<double> p = ld_pos<false>(S + i);
         const double mg = (double)R[i] + half_skin;
         const bool near = (p.z < mg) || (p.x + hx < mg) || (hx - p.x < mg) || (p.y + hy < mg) || (hy - p.y < mg);
@@ -377,7 +370,7 @@ template <typename Real> __device__ __forceinline__ uint filter_item(long long i
             const int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
             ikey[i] = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
         }
-        uint nup = 0;
+        uint nup = 0, nall = 0;
         if ((long long)coff[n] <= ccap) {
             R4<Real> me;
             me.x = (Real)(p.x - g.ox);
@@ -411,16 +404,150 @@ template <typename Real> __device__ __forceinline__ uint filter_item(long long i
             wlist[ws] = i;
         }
         wslot[i] = ws;
-        bflag[i] = (nall > 0 || near) ? 1u : 0u;
+        const bool bound = nall > 0 || near;
+        bflag[i] = bound ? 1u : 0u;
+        if (cc_parent && bound) {   // the coming re-list's components start as singletons
+            cc_parent[i] = i;
+            cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
+        }
+        o.up = nup;
+        o.down = nall - nup;
+        o.bound = bound ? 1u : 0u;
     }
-    return nall;
+    return o;
 }
 
-template <typename Real> __global__ void k_filter(DEM_FILTER_PARAMS, EngineWords* words) {
+// The candidate pass fused with the exclusive scans of its three counts
+// (row offsets off, reverse-row offsets roff, bound positions bpos; totals
+// at [n]) by a single-pass scan with decoupled look-back (Merrill & Garland,
+// "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016): tiles
+// of kFilterThreads particles take tickets in the order they start, publish
+// their totals, and add up the published words of the tiles before them, so
+// no tile waits on one that has not started.  The tile also writes the bound
+// list (ascending id) and the free list.  Look-back words (lb): [0] the tile
+// ticket, then per tile and count a 64-bit word, the value in the low 32 bits
+// and the kind above (1: the tile's own total, 2: the total through the
+// tile); the fill clears them for the next re-list.
+constexpr int kFilterThreads = 256;
+constexpr unsigned long long kLbAgg = 1ull << 32, kLbIncl = 2ull << 32;
+constexpr int kLbSpin = 1 << 22;   // a look-back word not published after this many polls: kStBarrier
+inline size_t lb_words(long long np) { return 2 + 6 * (size_t)grid_for(np, kFilterThreads); }
+
+__device__ __forceinline__ void lb_store(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long lb_load(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint pick3(const uint (&v)[3], uint k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+
+// One look-back round for one count: the lanes hold the words of 32
+// consecutive earlier tiles, nearest first; adds the values up to the
+// nearest inclusive word (all 32 when there is none).
+__device__ __forceinline__ void lb_round(unsigned long long w, uint& pre, bool& done) {
+    if (done) return;   // uniform over the warp
+    const uint m = __ballot_sync(0xffffffffu, (w >> 32) == 2ull);
+    const int lim = m ? __ffs(m) - 1 : 31;
+    pre += __reduce_add_sync(0xffffffffu, (int)lane_id() <= lim ? (uint)w : 0u);
+    done = m != 0u;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAMS, EngineWords* words, uint* lb,
+                                                                uint* __restrict__ off, uint* __restrict__ roff,
+                                                                uint* __restrict__ bpos, uint* __restrict__ blist,
+                                                                uint* __restrict__ flist) {
+    __shared__ uint s_tile;
+    __shared__ uint s_w[3][kFilterThreads / 32];
+    __shared__ uint s_pre[3];
     pdl_trigger();
-    uint nall = filter_item<Real>((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_FILTER_ARGS);
-    nall = __reduce_max_sync(0xffffffffu, nall);
-    if (lane_id() == 0 && nall) atomicMax(&words->max_row, nall);
+    if (threadIdx.x == 0) s_tile = atomicAdd(lb, 1u);
+    __syncthreads();
+    const uint tile = s_tile;
+    if (tile >= gridDim.x) {   // a ticket left over (the words were not cleared): nothing out of range
+        if (threadIdx.x == 0) atomicOr(&words->status, kStBarrier);
+        return;
+    }
+    const long long ii = (long long)tile * kFilterThreads + threadIdx.x;
+    const FilterCounts o = filter_item<Real>(ii, DEM_FILTER_ARGS);
+    const uint mrow = __reduce_max_sync(0xffffffffu, o.up + o.down);
+    const uint lane = lane_id(), warp = threadIdx.x >> 5;
+    if (lane == 0 && mrow) atomicMax(&words->max_row, mrow);
+    const uint v[3] = {o.up, o.down, o.bound};
+    uint inc[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        inc[a] = v[a];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint t = __shfl_up_sync(0xffffffffu, inc[a], d);
+            if ((int)lane >= d) inc[a] += t;
+        }
+        if (lane == 31) s_w[a][warp] = inc[a];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int W = kFilterThreads / 32;
+        uint agg[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {   // warp totals -> warp offsets; the tile's totals
+            const uint w = (int)lane < W ? s_w[a][lane] : 0u;
+            uint wi = w;
+#pragma unroll
+            for (int d = 1; d < W; d <<= 1) {
+                const uint t = __shfl_up_sync(0xffffffffu, wi, d);
+                if ((int)lane >= d) wi += t;
+            }
+            if ((int)lane < W) s_w[a][lane] = wi - w;
+            agg[a] = __shfl_sync(0xffffffffu, wi, W - 1);
+        }
+        unsigned long long* st = reinterpret_cast<unsigned long long*>(lb + 2);
+        uint pre[3] = {0u, 0u, 0u};
+        if (tile == 0) {
+            if (lane < 3) lb_store(st + lane, kLbIncl | pick3(agg, lane));
+        } else {
+            if (lane < 3) lb_store(st + 3 * (size_t)tile + lane, kLbAgg | pick3(agg, lane));
+            bool d0 = false, d1 = false, d2 = false;
+            for (long long base = (long long)tile - 1; !(d0 && d1 && d2); base -= 32) {
+                const long long t = base - (long long)lane;
+                unsigned long long w0 = kLbIncl, w1 = kLbIncl, w2 = kLbIncl;   // before tile 0: zero
+                if (t >= 0) {
+                    const unsigned long long* q = st + 3 * t;
+                    for (int spin = 0;; spin++) {
+                        w0 = lb_load(q); w1 = lb_load(q + 1); w2 = lb_load(q + 2);
+                        if ((w0 >> 32) && (w1 >> 32) && (w2 >> 32)) break;
+                        if (spin >= kLbSpin) {   // never published: record it, count the tile as zero
+                            atomicOr(&words->status, kStBarrier);
+                            w0 = w1 = w2 = kLbIncl;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                lb_round(w0, pre[0], d0);
+                lb_round(w1, pre[1], d1);
+                lb_round(w2, pre[2], d2);
+            }
+            if (lane < 3) lb_store(st + 3 * (size_t)tile + lane, kLbIncl | (pick3(pre, lane) + pick3(agg, lane)));
+        }
+        if (lane < 3) s_pre[lane] = pick3(pre, lane);
+        if (tile == gridDim.x - 1 && lane < 3) {   // the totals
+            uint* tot = lane == 0 ? off : (lane == 1 ? roff : bpos);
+            tot[n] = pick3(pre, lane) + pick3(agg, lane);
+        }
+    }
+    __syncthreads();
+    if (ii < n) {
+        const uint i = (uint)ii;
+        off[i] = s_pre[0] + s_w[0][warp] + inc[0] - v[0];
+        roff[i] = s_pre[1] + s_w[1][warp] + inc[1] - v[1];
+        const uint b = s_pre[2] + s_w[2][warp] + inc[2] - v[2];
+        bpos[i] = b;
+        if (o.bound) blist[b] = i;
+        else flist[i - b] = i;
+    }
 }
 
 __device__ __forceinline__ void isort_u32(uint* a, uint len) {
@@ -433,33 +560,18 @@ __device__ __forceinline__ void isort_u32(uint* a, uint len) {
 }
 
 // Fill the CSR row of i (j>i ascending), carry the FP64 tangential history
-// from the previous list, record the reverse slots.
+// from the previous list, record the reverse slots.  Every particle with a
+// row is bound, so the pass strides over the bound list only.
 #define DEM_FILL_PARAMS                                                                                               \
     long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                    \
     const uint* __restrict__ coff, const uint* __restrict__ cln, const uint* __restrict__ off,                        \
     const uint* __restrict__ roff, uint* __restrict__ njli, uint* __restrict__ ln, uint* __restrict__ lp,             \
     Planes3<double> H, const uint* __restrict__ ooff, const uint* __restrict__ oln, Planes3<double> OH,               \
     uint* __restrict__ rk, R4<Real>* __restrict__ pf, long long cap, EngineWords* words,                              \
-    uint* __restrict__ carry, const uint* __restrict__ scr, const uint* __restrict__ bflag,                           \
-    const uint* __restrict__ bpos, uint* __restrict__ blist, uint* __restrict__ flist, uint* cc_parent,               \
-    const uint* __restrict__ cc_skip
+    uint* __restrict__ carry, const uint* __restrict__ scr, uint* cc_parent
 #define DEM_FILL_ARGS                                                                                                 \
-    n, S, R, g, skin, coff, cln, off, roff, njli, ln, lp, H, ooff, oln, OH, rk, pf, cap, words, carry,                \
-    scr, bflag, bpos, blist, flist, cc_parent, cc_skip
-template <typename Real> __device__ __forceinline__ void fill_item(long long ii, DEM_FILL_PARAMS) {
-    if (ii >= n) return;
-    if (cc_parent && *cc_skip) cc_parent = nullptr;   // a dense bed: no component pass this re-list
-    const uint i = (uint)ii;
-    {   // bound / free lists, ascending particle id
-        const uint b = bpos[i];
-        if (bflag[i]) blist[b] = i;
-        else flist[i - b] = i;
-    }
-    const uint total = off[n];
-    if ((long long)total > cap) {
-        if (i == 0) atomicOr(&words->status, kStCapacity);
-        return;
-    }
+    n, S, R, g, skin, coff, cln, off, roff, njli, ln, lp, H, ooff, oln, OH, rk, pf, cap, words, carry, scr, cc_parent
+template <typename Real> __device__ __forceinline__ void fill_item(uint i, DEM_FILL_PARAMS) {
     const uint b = off[i], e = off[i + 1];
     if (e == b) return;
     if (e - b <= kScr) {
@@ -504,41 +616,52 @@ template <typename Real> __device__ __forceinline__ void fill_item(long long ii,
     }
 }
 
-template <typename Real> __global__ void k_nbr_fill(DEM_FILL_PARAMS) {
+// The fill over the bound list (grid-stride); it also clears the candidate
+// pass's look-back words (lbw of them) for the next re-list.
+template <typename Real>
+__global__ void k_nbr_fill(DEM_FILL_PARAMS, const uint* __restrict__ bpos, const uint* __restrict__ blist,
+                           const uint* __restrict__ cc_skip, uint* __restrict__ lb, long long lbw) {
     pdl_wait();
     pdl_trigger();
-    fill_item<Real>((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_FILL_ARGS);
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nthr = (long long)gridDim.x * blockDim.x;
+    for (long long k = tid; k < lbw; k += nthr) lb[k] = 0u;
+    if ((long long)off[n] > cap) {
+        if (tid == 0) atomicOr(&words->status, kStCapacity);
+        return;
+    }
+    if (cc_parent && *cc_skip) cc_parent = nullptr;   // a dense bed: no component pass this re-list
+    const long long nb = bpos[n];
+    for (long long t = tid; t < nb; t += nthr) fill_item<Real>(blist[t], DEM_FILL_ARGS);
 }
 
 // Sort each reverse row (pair indices ascending: a deterministic order for
-// the gather) and record each pair's reverse slot ru[k].
-// With cluster batches (parent != nullptr): every bound particle also takes
-// its component's root (all unions were made by the fill) and adds itself and
+// the gather) and record each pair's reverse slot ru[k]; every particle with
+// a reverse row is bound (the pass strides over the bound list).  With
+// cluster batches (parent != nullptr): every bound particle also takes its
+// component's root (all unions were made by the fill) and adds itself and
 // its row's pairs to the root's counts.
-#define DEM_REVSORT_PARAMS                                                                                            \
-    long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,                         \
-    const uint* __restrict__ off, long long cap, uint* parent, const uint* __restrict__ bflag,                        \
-    uint* __restrict__ csize, uint* __restrict__ cpairs, const uint* __restrict__ cc_skip
-#define DEM_REVSORT_ARGS n, roff, rk, ru, off, cap, parent, bflag, csize, cpairs, cc_skip
-__device__ __forceinline__ void revsort_item(long long i, DEM_REVSORT_PARAMS) {
-    if (i >= n) return;
-    if (parent && *cc_skip) parent = nullptr;
-    if ((long long)off[n] > cap) return;
-    const uint b = roff[i], e = roff[i + 1];
-    isort_u32(rk + b, e - b);
-    for (uint u = b; u < e; u++) ru[rk[u]] = u;
-    if (parent && bflag[i]) {
-        const uint r = cc_root(parent, (uint)i);
-        parent[i] = r;
-        atomicAdd(csize + r, 1u);
-        atomicAdd(cpairs + r, off[i + 1] - off[i]);
-    }
-}
-
-__global__ void k_rev_sort(DEM_REVSORT_PARAMS) {
+__global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,
+                           const uint* __restrict__ off, long long cap, uint* parent, const uint* __restrict__ bpos,
+                           const uint* __restrict__ blist, uint* __restrict__ csize, uint* __restrict__ cpairs,
+                           const uint* __restrict__ cc_skip) {
     pdl_wait();
     pdl_trigger();
-    revsort_item((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_REVSORT_ARGS);
+    if ((long long)off[n] > cap) return;
+    if (parent && *cc_skip) parent = nullptr;
+    const long long nb = bpos[n];
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+         t += (long long)gridDim.x * blockDim.x) {
+        const uint i = blist[t];
+        const uint b = roff[i], e = roff[i + 1];
+        isort_u32(rk + b, e - b);
+        for (uint u = b; u < e; u++) ru[rk[u]] = u;
+        if (parent) {
+            const uint r = cc_root(parent, i);
+            parent[i] = r;
+            atomicAdd(csize + r, 1u);
+            atomicAdd(cpairs + r, off[i + 1] - off[i]);
+        }
+    }
 }
 
 // ------------------------------------------------------- cluster batches
@@ -594,10 +717,15 @@ __device__ __forceinline__ void cc_base_warp(long long t, DEM_CCBASE_PARAMS) {
     if (sz) base[i] = wbase + inc - sz;
 }
 
+// Grid-stride over whole warps of the bound list (the first warp always runs:
+// it makes the checks of t == 0).
 __global__ void k_cc_base(DEM_CCBASE_PARAMS) {
     pdl_wait();
     pdl_trigger();
-    cc_base_warp((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_CCBASE_ARGS);
+    const long long nthr = (long long)gridDim.x * blockDim.x;
+    const long long nb = max((long long)bpos[n], 1ll);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t - (long long)lane_id() < nb; t += nthr)
+        cc_base_warp(t, DEM_CCBASE_ARGS);
 }
 
 // The batch window: the bound particles spread over the batch kernel's
@@ -653,7 +781,10 @@ __device__ __forceinline__ void cc_slot_item(long long t, DEM_CCSLOT_PARAMS) {
 __global__ void k_cc_slot(DEM_CCSLOT_PARAMS) {
     pdl_wait();
     pdl_trigger();
-    cc_slot_item((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_CCSLOT_ARGS);
+    const long long nthr = (long long)gridDim.x * blockDim.x;
+    const long long nb = max((long long)bpos[n], 1ll);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += nthr)
+        cc_slot_item(t, DEM_CCSLOT_ARGS);
 }
 
 // First slot of batch b (the first component whose first slot is b * target
@@ -1898,152 +2029,6 @@ StepPartials free_partials(const dem_ctx* c, int slot) {
 
 // List build from the current state, carrying history from list buffer src
 // (phase c->hph) into buffer 1-src (phase 0).
-// ------------------------------------------------------ cooperative re-list
-// The re-list after the outer list's check (and build) as one cooperative
-// launch: the candidate filter, the scan of the row / reverse-row / bound
-// counts, the fill, the reverse rows, and the component pass, as phases
-// separated by the bounded grid barrier (a kernel boundary per phase cost
-// its launch, its tail and its ramp: each of these passes is a few
-// microseconds of work over all particles).  Every phase calls the device
-// functions of the per-kernel re-list (used by eager re-lists), so the lists
-// are the same bits.
-constexpr int kRelistThreads = 256;
-
-template <typename Real> struct RelistCoop {
-    long long n, np, cap, ccap, nbb, nbmax;
-    const PRec<Real>* S;
-    const Real* R;
-    GridC g;
-    Real skin;
-    double hx, hy, half_skin;
-    const uint *coff, *cln, *ooff, *oln;
-    uint *wslot, *wlist, *wcount, *cc_parent, *cc_zero, *ikey, *njgi, *njli, *bflag, *scr;
-    uint *off, *roff, *ln, *lp, *rk, *ru, *carry, *bpos, *blist, *flist, *cc_skip;
-    Planes3<double> H, OH;
-    R4<Real>* pf;
-    EngineWords* words;
-    uint *csize, *cpairs, *base, *ccw, *fill, *order, *bw, *batch;
-    uint G, P, Q;
-    int cc;                  // the component pass runs (cluster batches)
-    uint* part;              // 3 per block: the scan's block totals
-    uint* bar;               // grid barrier (zeroed before the launch)
-};
-
-// Exclusive scans of njgi, njli, bflag into off, roff, bpos (totals at [n]):
-// block totals, a barrier, each block's prefix from the totals before it,
-// then the elements.  Block b scans the contiguous chunk [b C, (b+1) C).
-template <typename Real> __device__ __forceinline__ void coop_scan3(const RelistCoop<Real>& A, uint& nbar) {
-    const long long n = A.n;
-    const long long C = (n + gridDim.x - 1) / gridDim.x;
-    const long long lo = (long long)blockIdx.x * C, hi = min(n, lo + C);
-    const long long per = (C + blockDim.x - 1) / blockDim.x;
-    const long long t0 = lo + (long long)threadIdx.x * per, t1 = min(hi, t0 + per);
-    const uint* in[3] = {A.njgi, A.njli, A.bflag};
-    uint* out[3] = {A.off, A.roff, A.bpos};
-    __shared__ uint s_w[3][kRelistThreads / 32];
-    __shared__ uint s_blk[3];
-    uint sum[3] = {0u, 0u, 0u};
-    for (long long k = t0; k < t1; k++)
-        for (int a = 0; a < 3; a++) sum[a] += in[a][k];
-    // block exclusive scan of the thread sums
-    const uint lane = lane_id(), warp = threadIdx.x >> 5;
-    uint inc[3];
-    for (int a = 0; a < 3; a++) {
-        inc[a] = sum[a];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint v = __shfl_up_sync(0xffffffffu, inc[a], o);
-            if ((int)lane >= o) inc[a] += v;
-        }
-        if (lane == 31) s_w[a][warp] = inc[a];
-    }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-        uint acc = 0;
-        for (uint w = 0; w < blockDim.x / 32; w++) { const uint v = s_w[threadIdx.x][w]; s_w[threadIdx.x][w] = acc; acc += v; }
-        A.part[3 * blockIdx.x + threadIdx.x] = acc;
-    }
-    __syncthreads();
-    uint run[3];
-    for (int a = 0; a < 3; a++) run[a] = s_w[a][warp] + inc[a] - sum[a];
-    grid_barrier(A.bar, nbar++, gridDim.x, A.words);
-    // this block's prefix: the totals of the blocks before it
-    uint pre[3] = {0u, 0u, 0u};
-    for (uint b = threadIdx.x; b < blockIdx.x; b += blockDim.x)
-        for (int a = 0; a < 3; a++) pre[a] += __ldcg(A.part + 3 * b + a);
-    for (int a = 0; a < 3; a++) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) pre[a] += __shfl_xor_sync(0xffffffffu, pre[a], o);
-    }
-    __syncthreads();   // s_w is reused for the prefix
-    if (lane == 0)
-        for (int a = 0; a < 3; a++) s_w[a][warp] = pre[a];
-    __syncthreads();
-    if (threadIdx.x < 3) {
-        uint acc = 0;
-        for (uint w = 0; w < blockDim.x / 32; w++) acc += s_w[threadIdx.x][w];
-        s_blk[threadIdx.x] = acc;
-    }
-    __syncthreads();
-    for (int a = 0; a < 3; a++) run[a] += s_blk[a];
-    for (long long k = t0; k < t1; k++)
-        for (int a = 0; a < 3; a++) {
-            const uint v = in[a][k];
-            out[a][k] = run[a];
-            run[a] += v;
-        }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x < 3)
-        out[threadIdx.x][n] = s_blk[threadIdx.x] + __ldcg(A.part + 3 * blockIdx.x + threadIdx.x);
-}
-
-template <typename Real> __global__ void __launch_bounds__(kRelistThreads) k_relist_coop(RelistCoop<Real> A) {
-    // the names of the per-kernel re-list's parameters
-    const long long n = A.n, np = A.np, cap = A.cap, ccap = A.ccap, nbb = A.nbb, nbmax = A.nbmax;
-    const PRec<Real>* S = A.S;
-    const Real* R = A.R;
-    const GridC g = A.g;
-    const Real skin = A.skin;
-    const double hx = A.hx, hy = A.hy, half_skin = A.half_skin;
-    const uint *coff = A.coff, *cln = A.cln, *ooff = A.ooff, *oln = A.oln;
-    uint *wslot = A.wslot, *wlist = A.wlist, *wcount = A.wcount, *cc_zero = A.cc_zero, *ikey = A.ikey;
-    uint *njgi = A.njgi, *njli = A.njli, *bflag = A.bflag, *scr = A.scr;
-    uint *off = A.off, *roff = A.roff, *ln = A.ln, *lp = A.lp, *rk = A.rk, *ru = A.ru, *carry = A.carry;
-    uint *bpos = A.bpos, *blist = A.blist, *flist = A.flist, *cc_skip = A.cc_skip;
-    uint* cc_parent = A.cc ? A.cc_parent : nullptr;
-    uint* parent = cc_parent;
-    const Planes3<double> H = A.H, OH = A.OH;
-    R4<Real>* pf = A.pf;
-    EngineWords* words = A.words;
-    uint *csize = A.csize, *cpairs = A.cpairs, *size = A.csize, *pairs = A.cpairs, *base = A.base, *ccw = A.ccw;
-    uint *fill = A.fill, *order = A.order, *bw = A.bw, *batch = A.batch;
-    const uint G = A.G, P = A.P, Q = A.Q;
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nthr = (long long)gridDim.x * blockDim.x;
-    uint nbar = 0;
-    // candidate filter
-    uint mrow = 0;
-    for (long long ii = tid; ii < n; ii += nthr) mrow = max(mrow, filter_item<Real>(ii, DEM_FILTER_ARGS));
-    mrow = __reduce_max_sync(0xffffffffu, mrow);
-    if (lane_id() == 0 && mrow) atomicMax(&words->max_row, mrow);
-    grid_barrier(A.bar, nbar++, gridDim.x, words);
-    // row, reverse-row and bound counts: scans
-    coop_scan3<Real>(A, nbar);
-    grid_barrier(A.bar, nbar++, gridDim.x, words);
-    // rows, history carry, reverse slots, bound / free lists, unions
-    for (long long ii = tid; ii < n; ii += nthr) fill_item<Real>(ii, DEM_FILL_ARGS);
-    grid_barrier(A.bar, nbar++, gridDim.x, words);
-    // reverse rows in order; component roots and counts
-    for (long long i = tid; i < n; i += nthr) revsort_item(i, DEM_REVSORT_ARGS);
-    if (!A.cc) return;
-    grid_barrier(A.bar, nbar++, gridDim.x, words);
-    // components: slot ranges (whole warps), slots, batches
-    for (long long t = tid - lane_id(); t < n; t += nthr) cc_base_warp(t + lane_id(), DEM_CCBASE_ARGS);
-    grid_barrier(A.bar, nbar++, gridDim.x, words);
-    for (long long t = tid; t < n; t += nthr) cc_slot_item(t, DEM_CCSLOT_ARGS);
-    grid_barrier(A.bar, nbar++, gridDim.x, words);
-    for (long long b = tid; b <= nbmax; b += nthr) cc_batches_item(b, DEM_CCBATCH_ARGS);
-}
-
 // The outer build on stream st (plain launches: in a graph it is the body of
 // a conditional node): cells of the outer grid, their scan, the counting
 // scatter, the row lengths, their scan, the rows.
@@ -2137,69 +2122,31 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     }
     if (rc) return rc;
     const Real skin = (Real)c->cfg.skin;
-    if (c->coop_grid > 0) {   // the rest of the re-list in one cooperative launch
-        DEM_CUDA_TRY(cudaMemsetAsync(c->rbar, 0, kBarWords * sizeof(uint), s));
-        RelistCoop<Real> A;
-        A.n = n; A.np = c->npad; A.cap = c->cap; A.ccap = c->ccap;
-        A.nbb = c->nbatch_max + 2; A.nbmax = c->nbatch_max;
-        A.S = S; A.R = (const Real*)c->rad; A.g = g; A.skin = skin;
-        A.hx = c->cfg.world[0] * 0.5; A.hy = c->cfg.world[1] * 0.5; A.half_skin = 0.5 * c->cfg.skin;
-        A.coff = c->coff; A.cln = c->cln; A.ooff = c->off[src]; A.oln = c->ln[src];
-        A.wslot = c->wslot; A.wlist = c->wlist; A.wcount = c->wcount; A.cc_parent = c->cc_parent;
-        A.cc_zero = c->cc_size; A.ikey = c->ikey; A.njgi = c->njgi; A.njli = c->njli; A.bflag = c->bflag;
-        A.scr = c->scr; A.off = c->off[dst]; A.roff = c->roff; A.ln = c->ln[dst]; A.lp = c->lp; A.rk = c->rk;
-        A.ru = c->ru; A.carry = c->carry; A.bpos = c->bpos; A.blist = c->blist; A.flist = c->flist;
-        A.cc_skip = c->cc_skip;
-        A.H = planes<double>(c->hist[dst][0], c->cap);
-        A.OH = planes<double>(c->hist[src][c->hph], c->cap);
-        A.pf = (R4<Real>*)c->pf; A.words = c->words;
-        A.csize = c->cc_size; A.cpairs = c->cc_pairs; A.base = c->cc_base; A.ccw = c->cc_words;
-        A.fill = c->cc_fill; A.order = c->cc_order; A.bw = c->cc_bw; A.batch = c->cc_batch;
-        A.G = c->batch_grid; A.P = BatchCap<Real>::P; A.Q = BatchCap<Real>::Q;
-        A.cc = cc ? 1 : 0;
-        A.part = c->coop_part; A.bar = c->rbar;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(c->coop_grid);
-        cfg.blockDim = dim3(kRelistThreads);
-        cfg.stream = s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_relist_coop<Real>, A));
-        return DEM_OK;
-    }
-    k_filter<Real><<<grid_for(n, B), B, 0, s>>>(n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
-                                                (const uint*)c->cln, c->ccap, c->cfg.world[0] * 0.5,
-                                                c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin, c->wslot, c->wlist,
-                                                c->wcount, cc ? c->cc_parent : nullptr, c->cc_size, c->npad, c->ikey,
-                                                c->njgi, c->njli, c->bflag, c->scr, c->words);
+    // candidates, their counts' scans, bound and free lists: one pass
+    k_filter_scan<Real><<<grid_for(n, kFilterThreads), kFilterThreads, 0, s>>>(
+        n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff, (const uint*)c->cln, c->ccap,
+        c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin, c->wslot, c->wlist, c->wcount,
+        cc ? c->cc_parent : nullptr, c->cc_size, c->npad, c->ikey, c->njgi, c->njli, c->bflag, c->scr, c->words, c->lb,
+        c->off[dst], c->roff, c->bpos, c->blist, c->flist);
     DEM_LAUNCH_CHECK();
-    {
-        const uint* in[3] = {c->njgi, c->njli, c->bflag};
-        uint* out[3] = {c->off[dst], c->roff, c->bpos};
-        uint* tot[3] = {c->off[dst] + n, c->roff + n, c->bpos + n};
-        rc = exclusive_scan_multi_u32(3, in, out, tot, n, c->scan_tmp, s, pdl);
-        if (rc) return rc;
-    }
+    const unsigned BG = c->bound_grid;
     DEM_CUDA_TRY(launch_ex(
-        k_nbr_fill<Real>, grid_for(n, B), B, s, pdl, n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
+        k_nbr_fill<Real>, BG, B, s, pdl, n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
         (const uint*)c->cln, (const uint*)c->off[dst], (const uint*)c->roff,
         c->njli, c->ln[dst], c->lp, planes<double>(c->hist[dst][0], c->cap), (const uint*)c->off[src],
         (const uint*)c->ln[src], planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap,
-        c->words, c->carry, (const uint*)c->scr, (const uint*)c->bflag, (const uint*)c->bpos, c->blist, c->flist,
-        cc ? c->cc_parent : nullptr, (const uint*)c->cc_skip));
-    DEM_CUDA_TRY(launch_ex(k_rev_sort, grid_for(n, B), B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
-                           (const uint*)c->off[dst], c->cap, cc ? c->cc_parent : nullptr, (const uint*)c->bflag,
-                           c->cc_size, c->cc_pairs, (const uint*)c->cc_skip));
+        c->words, c->carry, (const uint*)c->scr, cc ? c->cc_parent : nullptr, (const uint*)c->bpos,
+        (const uint*)c->blist, (const uint*)c->cc_skip, c->lb, (long long)lb_words(n)));
+    DEM_CUDA_TRY(launch_ex(k_rev_sort, BG, B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
+                           (const uint*)c->off[dst], c->cap, cc ? c->cc_parent : nullptr, (const uint*)c->bpos,
+                           (const uint*)c->blist, c->cc_size, c->cc_pairs, (const uint*)c->cc_skip));
     if (cc) {   // the window's components and batches (cluster-batched window path)
         const uint* off = c->off[dst];
         const long long nbb = c->nbatch_max + 2;
-        DEM_CUDA_TRY(launch_ex(k_cc_base, grid_for(n, B), B, s, pdl, n, c->cap, (const uint*)c->blist,
+        DEM_CUDA_TRY(launch_ex(k_cc_base, BG, B, s, pdl, n, c->cap, (const uint*)c->blist,
                                (const uint*)c->bpos, off, (const uint*)c->cc_parent, (const uint*)c->cc_size,
                                c->cc_base, c->cc_words, (const uint*)c->cc_skip));
-        DEM_CUDA_TRY(launch_ex(k_cc_slot, grid_for(n, B), B, s, pdl, n, nbb, c->batch_grid, BatchCap<Real>::P,
+        DEM_CUDA_TRY(launch_ex(k_cc_slot, BG, B, s, pdl, n, nbb, c->batch_grid, BatchCap<Real>::P,
                                (const uint*)c->blist, (const uint*)c->bpos, (const uint*)c->cc_parent,
                                (const uint*)c->cc_base, (const uint*)c->cc_size, (const uint*)c->cc_pairs, c->cc_fill,
                                c->cc_order, c->cc_bw, c->cc_words));
@@ -2637,9 +2584,10 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     c->ccap = std::min<long long>(4 * cap, 0x7fffffffLL);
     if ((rc = dalloc(&c->coff, np + 1)) || (rc = dalloc(&c->cln, c->ccap)) || (rc = dalloc(&c->ocnt, np)) ||
         (rc = dalloc(&c->xo, 3 * np)) || (rc = dalloc(&c->oflag, 2)) || (rc = dalloc(&c->ikey, np)) ||
-        (rc = dalloc(&c->rbar, kBarWords)))
+        (rc = dalloc(&c->lb, lb_words(np))))
         return bail(rc);
     e = cudaMemsetAsync(c->oflag, 0x01, sizeof(uint), s0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->lb, 0, lb_words(np) * sizeof(uint), s0);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->coff, 0, (np + 1) * sizeof(uint), s0);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(e, "outer list set-up", __FILE__, __LINE__));
@@ -2677,20 +2625,10 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->win_grid = (unsigned)std::max(1, nsm * wper);
         const char* wk = getenv("DEM_B200_WINDOW");   // "0": per-step kernels for whole windows too
         c->win_kernel = coop && wper > 0 && !(wk && wk[0] == '0');
-        // the cooperative re-list (DEM_B200_RELIST_COOP=1): one round of
-        // resident blocks; off by default, since in a graph its six grid
-        // barriers cost more than the launches they replace (108 us against
-        // 94 us per re-list of 500K spheres)
-        {
-            int rper = 0;
-            e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, k_relist_coop<float>, kRelistThreads, 0)
-                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, k_relist_coop<double>, kRelistThreads, 0);
-            if (e != cudaSuccess) return bail(cuda_fail(e, "re-list kernel occupancy", __FILE__, __LINE__));
-            const char* rcoop = getenv("DEM_B200_RELIST_COOP");
-            const bool on = coop && rper > 0 && rcoop && rcoop[0] == '1';
-            c->coop_grid = on ? (unsigned)(nsm * rper) : 0u;
-            if (c->coop_grid && (rc = dalloc(&c->coop_part, 3 * (size_t)c->coop_grid))) return bail(rc);
-        }
+        // the re-list passes over the bound particles (fill, reverse rows,
+        // components) stride over a grid of 4 blocks per SM: one pass covers
+        // 150K bound particles, the ~10 % bound of a 500K free-flight bed
+        c->bound_grid = (unsigned)std::max(1, 4 * nsm);
         // "0": the outer build in every re-list, no conditional node (a profiler
         // does not see the kernel nodes of a graph that has conditional nodes)
         const char* oc = getenv("DEM_B200_OUTER_COND");
@@ -2774,7 +2712,7 @@ int dem_destroy(dem_ctx* c) {
     free_cells(c);
     void* ptrs[] = {c->rec[0], c->rec[1], c->rad, c->q, c->wh,
                     c->staging, c->key, c->sid, c->skeyu, c->sposu, c->njgi, c->njli, c->coff, c->cln, c->ocnt,
-                    c->xo, c->oflag, c->ikey, c->rbar, c->coop_part,
+                    c->xo, c->oflag, c->ikey, c->lb,
                     c->off[0], c->off[1], c->roff, c->ln[0], c->ln[1], c->lp, c->hist[0][0], c->hist[0][1],
                     c->hist[1][0], c->hist[1][1], c->rk, c->ru, c->pf, c->pti, c->rfj, c->rtj, c->scan_tmp, c->words, c->part_mz,
                     c->part_cnt, c->rmax_bits, c->dbgF, c->dbgT, c->dbgC, c->wslot, c->wlist, c->wcount, c->wf, c->arrival,
@@ -2883,6 +2821,7 @@ static int finish_upload(dem_ctx* c) {
     if (c->cc_skip) DEM_CUDA_TRY(cudaMemsetAsync(c->cc_skip, 0, 2 * sizeof(uint), c->stream));
     // the outer list is rebuilt at the first re-list (new positions, radii)
     DEM_CUDA_TRY(cudaMemsetAsync(c->oflag, 0x01, sizeof(uint), c->stream));
+    DEM_CUDA_TRY(cudaMemsetAsync(c->lb, 0, lb_words(c->npad) * sizeof(uint), c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->part_mz, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(unsigned long long),
                                  c->stream));
     DEM_CUDA_TRY(cudaMemsetAsync(c->part_cnt, 0, (size_t)c->cfg.relist_interval * c->npart * sizeof(uint), c->stream));
@@ -2989,13 +2928,37 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
         // (not after the device work that follows them)
         DEM_CUDA_TRY(cudaEventRecord(c->h2d_done, c->stream));
         ppos = spos; ppd = pdis ? sd : nullptr; ppa = angv ? sa : nullptr; prad = sr;
-        double rm = 0.0, v3 = 0.0;
-        for (long long i = 0; i < n; i++) {
-            if (!(rad[i] > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state: radius %lld not positive", i);
-            rm = std::max(rm, rad[i]);
-            v3 += rad[i] * rad[i] * rad[i];
+        // r_max and the solid volume while the copies run: eight interleaved
+        // partial sums (a fixed order, so the same bits every call) keep the
+        // loop off the latency of one serial FP64 chain (0.7 ms at 500K)
+        constexpr int kLanes = 8;
+        double rm[kLanes] = {}, vs[kLanes] = {};
+        bool bad = false;
+        long long i = 0;
+        for (; i + kLanes <= n; i += kLanes) {
+            for (int l = 0; l < kLanes; l++) {
+                const double r = rad[i + l];
+                bad |= !(r > 0.0);
+                rm[l] = std::max(rm[l], r);
+                vs[l] += r * r * r;
+            }
         }
-        c->rmax = rm;
+        for (int l = 0; i < n; i++, l++) {
+            const double r = rad[i];
+            bad |= !(r > 0.0);
+            rm[l] = std::max(rm[l], r);
+            vs[l] += r * r * r;
+        }
+        if (bad) {
+            for (long long k = 0; k < n; k++)
+                if (!(rad[k] > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state: radius %lld not positive", k);
+        }
+        double rmx = 0.0, v3 = 0.0;
+        for (int l = 0; l < kLanes; l++) {
+            rmx = std::max(rmx, rm[l]);
+            v3 += vs[l];
+        }
+        c->rmax = rmx;
         c->vol = 4.0 / 3.0 * M_PI * v3;
         bool cell_ordered = false;
         if (order == kOrderCells && c->reorder) {

@@ -11,7 +11,7 @@ enum : uint {
     kStCapacity = 1u,
     kStNonfinite = 2u,
     kStSkin = 4u,
-    kStBarrier = 8u,   // a window-kernel grid barrier ran out of time
+    kStBarrier = 8u,   // a bounded wait (window-kernel grid barrier, scan look-back) ran out of time
 };
 
 // device words: [0] status bits, [1] max row count
@@ -231,9 +231,8 @@ struct dem_ctx {
     uint* ikey = nullptr;    // np: each particle's cell on the configured grid at the last re-list
     cudaStream_t cstream = 0;        // captures the outer build into its conditional node
     bool outer_cond = true;          // DEM_B200_OUTER_COND=0: build in every re-list
-    unsigned coop_grid = 0;          // blocks of the cooperative re-list (0: the per-kernel re-list)
-    uint* coop_part = nullptr;       // 3 per block: its scan totals
-    uint* rbar = nullptr;            // its grid barrier
+    unsigned bound_grid = 0;         // blocks of the re-list passes over the bound particles (grid-stride)
+    uint* lb = nullptr;              // the candidate pass's look-back: [0] tile ticket, then 3 64-bit words per tile
     cudaStream_t stream2 = 0;        // free-particle branch of the window graph
     cudaEvent_t evfork = nullptr, evjoin = nullptr;
     bool free_in_window = false;     // capturing: the free particles run as one window kernel

@@ -98,12 +98,14 @@ def test_lists_from_the_outer_list_equal_fresh_lists(dem, orc, wl, cuda, prec):
 
 @pytest.mark.parametrize("mode", ["pccp", "pp"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_cooperative_relist_equals_per_kernel_relist(dem, wl, cuda, monkeypatch, prec, mode):
-    """The re-list after the outer list as one kernel per pass (the default)
-    and as one cooperative launch (DEM_B200_RELIST_COOP=1: filter, scans,
-    fill, reverse rows and component pass as phases between grid barriers)
-    give the same lists, batches and states bit for bit, on a sparse bed
-    (cluster batches) and a dense lattice."""
+def test_relist_deterministic_and_bound_count(dem, wl, cuda, prec, mode):
+    """The re-list's single-pass scans (tiles that start in any order add up
+    the totals their predecessors publish), the fill and the component pass
+    over the bound list, and the lock-free unions give the same lists,
+    batches and states in two contexts, bit for bit, on a sparse bed
+    (cluster batches) and a dense lattice; the bound count (the bound scan's
+    total) equals the particles that have a listed pair or lie within
+    r + skin/2 of a wall at the re-list's positions."""
     from _cases import dense_lattice
     p = dem.PREC_FP64 if prec == "fp64" else dem.PREC_MIXED
     fm = dem.FORCE_PCCP if mode == "pccp" else dem.FORCE_PP
@@ -112,10 +114,8 @@ def test_cooperative_relist_equals_per_kernel_relist(dem, wl, cuda, monkeypatch,
         pdis = rng.normal(0, 2e-6, 3 * w.n)
         a = make_engine(dem, w, p, force_mode=fm)
         a.upload(w.pos, w.rad, pdis, None)
-        monkeypatch.setenv("DEM_B200_RELIST_COOP", "1")
         b = make_engine(dem, w, p, force_mode=fm)
         b.upload(w.pos, w.rad, pdis, None)
-        monkeypatch.delenv("DEM_B200_RELIST_COOP")
         for steps in (4 * w.relist_interval, 3):
             a.step(steps)
             b.step(steps)
@@ -127,6 +127,24 @@ def test_cooperative_relist_equals_per_kernel_relist(dem, wl, cuda, monkeypatch,
         sa, sb = a.scalars(), b.scalars()
         assert sa["status"] == 0 and sb["status"] == 0
         assert sa["maxhz"] == sb["maxhz"] and sa["contacts"] == sb["contacts"] and sa["pairs"] == sb["pairs"]
+        # the bound count at a re-list
+        K = w.relist_interval
+        a.step(K - 3)                     # to the window's end
+        pos = a.download()[0].reshape(-1, 3)
+        a.step(1)                         # the re-list at these positions
+        lp, ln, _ = a.pairs()
+        r = w.rad.astype(np.float32).astype(np.float64) if prec == "mixed" else w.rad
+        mg = r + 0.5 * w.skin
+        hx, hy = 0.5 * w.world[0], 0.5 * w.world[1]
+        near = ((pos[:, 2] < mg) | (pos[:, 0] + hx < mg) | (hx - pos[:, 0] < mg) | (pos[:, 1] + hy < mg)
+                | (hy - pos[:, 1] < mg))
+        bound = near.copy()
+        bound[lp] = True
+        bound[ln] = True
+        work = a.window_work()
+        assert work["bound"] == int(bound.sum())
+        assert work["wall_candidates"] == int(near.sum())
+        assert work["pairs"] == lp.size
         a.close()
         b.close()
 

@@ -1532,36 +1532,63 @@ template <typename Real> struct BatchSmem {
     R4<Real> *fo, *ti, *tj;
     uint* scan;
 };
+// The block's shared-memory layout: byte offsets fixed at compile time (each
+// array 16-byte aligned), so every array is the base plus a constant.
+template <typename Real> struct BatchOff {
+    static constexpr uint P = BatchCap<Real>::P, Q = BatchCap<Real>::Q;
+    static constexpr size_t al(size_t b) { return (b + 15) & ~size_t(15); }
+    static constexpr size_t x = 0;
+    static constexpr size_t d = x + al(P * sizeof(V3<double>));
+    static constexpr size_t wh = d + al(P * sizeof(V3<double>));
+    static constexpr size_t q = wh + al(P * sizeof(V3<double>));
+    static constexpr size_t wf = q + al(P * sizeof(float4));
+    static constexpr size_t wt = wf + al(P * sizeof(R4<Real>));
+    static constexpr size_t a = wt + al(P * sizeof(R4<Real>));
+    static constexpr size_t r = a + al(P * sizeof(V3<Real>));
+    static constexpr size_t km = r + al(P * sizeof(Real));
+    static constexpr size_t ki = km + al(P * sizeof(double));
+    static constexpr size_t gid = ki + al(P * sizeof(float));
+    static constexpr size_t ws = gid + al(P * 4);
+    static constexpr size_t pb = ws + al(P * 4);
+    static constexpr size_t pl = pb + al(P * 4);
+    static constexpr size_t rb = pl + al(P * 4);
+    static constexpr size_t rl = rb + al(P * 4);
+    static constexpr size_t wl = rl + al(P * 4);
+    static constexpr size_t wli = wl + al(P * 4);
+    static constexpr size_t ph = wli + al(P * 4);
+    static constexpr size_t fo = ph + al(Q * sizeof(V3<double>));
+    static constexpr size_t ti = fo + al(Q * sizeof(R4<Real>));
+    static constexpr size_t tj = ti + al(Q * sizeof(R4<Real>));
+    static constexpr size_t plo = tj + al(Q * sizeof(R4<Real>));
+    static constexpr size_t phi = plo + al(Q * 4);
+    static constexpr size_t pk = phi + al(Q * 4);
+    static constexpr size_t prv = pk + al(Q * 4);
+    static constexpr size_t scan = prv + al(Q * 4);
+    static constexpr size_t end = scan + al(34 * 4);
+};
 template <typename Real> __host__ __device__ inline size_t batch_smem_layout(unsigned char* base, BatchSmem<Real>* L) {
-    constexpr uint P = BatchCap<Real>::P, Q = BatchCap<Real>::Q;
-    size_t o = 0;
-    auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
-    BatchSmem<Real> l;
-    l.x = (V3<double>*)take(P * sizeof(V3<double>));
-    l.d = (V3<double>*)take(P * sizeof(V3<double>));
-    l.wh = (V3<double>*)take(P * sizeof(V3<double>));
-    l.q = (float4*)take(P * sizeof(float4));
-    l.wf = (R4<Real>*)take(P * sizeof(R4<Real>));
-    l.wt = (R4<Real>*)take(P * sizeof(R4<Real>));
-    l.a = (V3<Real>*)take(P * sizeof(V3<Real>));
-    l.r = (Real*)take(P * sizeof(Real));
-    l.km = (double*)take(P * sizeof(double));
-    l.ki = (float*)take(P * sizeof(float));
-    l.gid = (uint*)take(P * 4); l.ws = (uint*)take(P * 4); l.pb = (uint*)take(P * 4);
-    l.pl = (uint*)take(P * 4); l.rb = (uint*)take(P * 4); l.rl = (uint*)take(P * 4);
-    l.wl = (uint*)take(P * 4); l.wli = (uint*)take(P * 4);
-    l.ph = (V3<double>*)take(Q * sizeof(V3<double>));
-    l.fo = (R4<Real>*)take(Q * sizeof(R4<Real>));
-    l.ti = (R4<Real>*)take(Q * sizeof(R4<Real>));
-    l.tj = (R4<Real>*)take(Q * sizeof(R4<Real>));
-    l.plo = (uint*)take(Q * 4); l.phi = (uint*)take(Q * 4); l.pk = (uint*)take(Q * 4); l.prv = (uint*)take(Q * 4);
-    l.scan = (uint*)take(34 * 4);
-    if (L) *L = l;
-    return o;
+    using O = BatchOff<Real>;
+    if (L) {
+        L->x = (V3<double>*)(base + O::x); L->d = (V3<double>*)(base + O::d); L->wh = (V3<double>*)(base + O::wh);
+        L->q = (float4*)(base + O::q); L->wf = (R4<Real>*)(base + O::wf); L->wt = (R4<Real>*)(base + O::wt);
+        L->a = (V3<Real>*)(base + O::a); L->r = (Real*)(base + O::r); L->km = (double*)(base + O::km);
+        L->ki = (float*)(base + O::ki); L->gid = (uint*)(base + O::gid); L->ws = (uint*)(base + O::ws);
+        L->pb = (uint*)(base + O::pb); L->pl = (uint*)(base + O::pl); L->rb = (uint*)(base + O::rb);
+        L->rl = (uint*)(base + O::rl); L->wl = (uint*)(base + O::wl); L->wli = (uint*)(base + O::wli);
+        L->ph = (V3<double>*)(base + O::ph); L->fo = (R4<Real>*)(base + O::fo); L->ti = (R4<Real>*)(base + O::ti);
+        L->tj = (R4<Real>*)(base + O::tj); L->plo = (uint*)(base + O::plo); L->phi = (uint*)(base + O::phi);
+        L->pk = (uint*)(base + O::pk); L->prv = (uint*)(base + O::prv); L->scan = (uint*)(base + O::scan);
+    }
+    return O::end;
 }
 
+// k_batch's register cap: the mixed kernel at 80 (40 bytes of spills) leaves
+// room on its SM for two blocks of k_free_run (256 x 48 registers), which
+// then runs beside the batches instead of after them; FP64 keeps 128.
+template <typename Real> struct BatchRegs { static constexpr int value = sizeof(Real) == 4 ? 80 : 128; };
+
 template <typename Real>
-__global__ void __launch_bounds__(kBatchThreads) k_batch(StepArgs<Real> a, int K, const uint* __restrict__ corder,
+__global__ void __maxnreg__(BatchRegs<Real>::value) k_batch(StepArgs<Real> a, int K, const uint* __restrict__ corder,
                                                          const uint* __restrict__ cbatch, uint* cloc,
                                                          StepPartials part, size_t clr1) {
     if (a.ccw[1]) return;   // a component or a batch too large: the grid-barrier window kernel has the window
@@ -2283,10 +2310,6 @@ template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const Wi
     int rc = launch_window<Real>(c, lst, tape, 1);
     if (rc) return rc;
     DEM_CUDA_TRY(cudaEventRecord(c->evfork, c->stream));
-    DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
-    rc = launch_free<Real>(c, lst, 0, K, c->stream2, 1);
-    if (rc) return rc;
-    DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
     StepArgs<Real> a = step_args<Real>(c, lst, 0);
     a.batch = 1;
     a.dbgF = a.dbgT = nullptr;
@@ -2297,9 +2320,26 @@ template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const Wi
         a.ta = (Real*)tape->ta;
         a.tstep0 = tape->step0;
     }
-    k_batch<Real><<<c->batch_grid, kBatchThreads, c->batch_smem, c->stream>>>(
-        a, K, (const uint*)c->cc_order, (const uint*)c->cc_batch, c->cc_loc, partials(c, K - 1), (size_t)c->nblk);
-    DEM_LAUNCH_CHECK();
+    // the batches first and at the higher priority: their blocks (one per SM)
+    // take their SMs before the free particles' blocks fill the room beside them
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c->batch_grid);
+        cfg.blockDim = dim3(kBatchThreads);
+        cfg.dynamicSmemBytes = c->batch_smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributePriority;
+        at[0].val.priority = c->prio_hi;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<Real>, a, K, (const uint*)c->cc_order,
+                                        (const uint*)c->cc_batch, c->cc_loc, partials(c, K - 1), (size_t)c->nblk));
+    }
+    DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
+    rc = launch_free<Real>(c, lst, 0, K, c->stream2, 1);
+    if (rc) return rc;
+    DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
     DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->evjoin, 0));
     return DEM_OK;
 }
@@ -2694,6 +2734,11 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     }
     e = cudaEventCreateWithFlags(&c->ext_ready, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->h2d_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+        int lo = 0, hi = 0;
+        e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        c->prio_hi = hi;
+    }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evfork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evjoin, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);

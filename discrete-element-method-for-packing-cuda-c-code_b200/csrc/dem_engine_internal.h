@@ -235,6 +235,7 @@ struct dem_ctx {
     uint* lb = nullptr;              // the candidate pass's look-back: [0] tile ticket, then 3 64-bit words per tile
     cudaStream_t stream2 = 0;        // free-particle branch of the window graph
     cudaEvent_t evfork = nullptr, evjoin = nullptr;
+    int prio_hi = 0;                 // the device's highest stream priority (the batch kernel's launches)
     bool free_in_window = false;     // capturing: the free particles run as one window kernel
     uint* bar = nullptr;             // window-kernel grid barrier: [0] arrival counter
     unsigned win_grid = 1;           // window-kernel blocks (all co-resident)

@@ -441,27 +441,17 @@ __device__ __forceinline__ unsigned long long lb_load(const unsigned long long* 
     asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ uint pick3(const uint (&v)[3], uint k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
-
-// One look-back round for one count: the lanes hold the words of 32
-// consecutive earlier tiles, nearest first; adds the values up to the
-// nearest inclusive word (all 32 when there is none).
-__device__ __forceinline__ void lb_round(unsigned long long w, uint& pre, bool& done) {
-    if (done) return;   // uniform over the warp
-    const uint m = __ballot_sync(0xffffffffu, (w >> 32) == 2ull);
-    const int lim = m ? __ffs(m) - 1 : 31;
-    pre += __reduce_add_sync(0xffffffffu, (int)lane_id() <= lim ? (uint)w : 0u);
-    done = m != 0u;
-}
-
 template <typename Real>
 __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAMS, EngineWords* words, uint* lb,
                                                                 uint* __restrict__ off, uint* __restrict__ roff,
                                                                 uint* __restrict__ bpos, uint* __restrict__ blist,
                                                                 uint* __restrict__ flist) {
+    constexpr int W = kFilterThreads / 32;
     __shared__ uint s_tile;
-    __shared__ uint s_w[3][kFilterThreads / 32];
-    __shared__ uint s_pre[3];
+    __shared__ uint s_w[3][W];
+    __shared__ uint s_red[3][W];
+    __shared__ uint s_agg[3], s_pre[3];
+    __shared__ int s_near[3];
     pdl_trigger();
     if (threadIdx.x == 0) s_tile = atomicAdd(lb, 1u);
     __syncthreads();
@@ -488,11 +478,9 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
         if (lane == 31) s_w[a][warp] = inc[a];
     }
     __syncthreads();
-    if (warp == 0) {
-        constexpr int W = kFilterThreads / 32;
-        uint agg[3];
+    if (warp == 0) {   // warp totals -> warp offsets; the tile's totals
 #pragma unroll
-        for (int a = 0; a < 3; a++) {   // warp totals -> warp offsets; the tile's totals
+        for (int a = 0; a < 3; a++) {
             const uint w = (int)lane < W ? s_w[a][lane] : 0u;
             uint wi = w;
 #pragma unroll
@@ -501,41 +489,66 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
                 if ((int)lane >= d) wi += t;
             }
             if ((int)lane < W) s_w[a][lane] = wi - w;
-            agg[a] = __shfl_sync(0xffffffffu, wi, W - 1);
+            if ((int)lane == W - 1) s_agg[a] = wi;
         }
-        unsigned long long* st = reinterpret_cast<unsigned long long*>(lb + 2);
-        uint pre[3] = {0u, 0u, 0u};
-        if (tile == 0) {
-            if (lane < 3) lb_store(st + lane, kLbIncl | pick3(agg, lane));
-        } else {
-            if (lane < 3) lb_store(st + 3 * (size_t)tile + lane, kLbAgg | pick3(agg, lane));
-            bool d0 = false, d1 = false, d2 = false;
-            for (long long base = (long long)tile - 1; !(d0 && d1 && d2); base -= 32) {
-                const long long t = base - (long long)lane;
-                unsigned long long w0 = kLbIncl, w1 = kLbIncl, w2 = kLbIncl;   // before tile 0: zero
-                if (t >= 0) {
-                    const unsigned long long* q = st + 3 * t;
-                    for (int spin = 0;; spin++) {
-                        w0 = lb_load(q); w1 = lb_load(q + 1); w2 = lb_load(q + 2);
-                        if ((w0 >> 32) && (w1 >> 32) && (w2 >> 32)) break;
-                        if (spin >= kLbSpin) {   // never published: record it, count the tile as zero
-                            atomicOr(&words->status, kStBarrier);
-                            w0 = w1 = w2 = kLbIncl;
-                            break;
-                        }
-                        __nanosleep(32);
+    }
+    __syncthreads();
+    // publish the tile's totals; the prefix: the whole block looks back over
+    // kFilterThreads earlier tiles per round (thread k: tile - 1 - k), adding
+    // every word up to the nearest inclusive one
+    unsigned long long* st = reinterpret_cast<unsigned long long*>(lb + 2);
+    const uint me = threadIdx.x;
+    uint pre = 0;   // threads 0..2: the prefix of count `me`
+    if (tile == 0) {
+        if (me < 3) lb_store(st + me, kLbIncl | s_agg[me]);
+    } else {
+        if (me < 3) lb_store(st + 3 * (size_t)tile + me, kLbAgg | s_agg[me]);
+        bool done[3] = {false, false, false};
+        for (long long base = (long long)tile - 1; !(done[0] && done[1] && done[2]); base -= kFilterThreads) {
+            const long long t = base - (long long)me;
+            unsigned long long w[3] = {kLbIncl, kLbIncl, kLbIncl};   // before tile 0: zero
+            if (t >= 0) {
+                const unsigned long long* q = st + 3 * t;
+                for (int spin = 0;; spin++) {
+                    w[0] = lb_load(q); w[1] = lb_load(q + 1); w[2] = lb_load(q + 2);
+                    if ((w[0] >> 32) && (w[1] >> 32) && (w[2] >> 32)) break;
+                    if (spin >= kLbSpin) {   // never published: record it, count the tile as zero
+                        atomicOr(&words->status, kStBarrier);
+                        w[0] = w[1] = w[2] = kLbIncl;
+                        break;
                     }
+                    __nanosleep(32);
                 }
-                lb_round(w0, pre[0], d0);
-                lb_round(w1, pre[1], d1);
-                lb_round(w2, pre[2], d2);
             }
-            if (lane < 3) lb_store(st + 3 * (size_t)tile + lane, kLbIncl | (pick3(pre, lane) + pick3(agg, lane)));
+            if (me < 3) s_near[me] = kFilterThreads;
+            __syncthreads();
+#pragma unroll
+            for (int a = 0; a < 3; a++) {   // the nearest inclusive word of each count
+                const uint m = __ballot_sync(0xffffffffu, (w[a] >> 32) == 2ull);
+                if (!done[a] && lane == 0 && m) atomicMin(&s_near[a], (int)(warp * 32 + __ffs(m) - 1));
+            }
+            __syncthreads();
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const uint x = (!done[a] && (int)me <= s_near[a]) ? (uint)w[a] : 0u;
+                const uint sx = __reduce_add_sync(0xffffffffu, x);
+                if (lane == 0) s_red[a][warp] = sx;
+            }
+            __syncthreads();
+            const bool dme = me == 0 ? done[0] : (me == 1 ? done[1] : done[2]);
+            if (me < 3 && !dme)
+                for (int k = 0; k < W; k++) pre += s_red[me][k];
+#pragma unroll
+            for (int a = 0; a < 3; a++) done[a] = done[a] || s_near[a] < kFilterThreads;
+            __syncthreads();   // s_near and s_red are written again next round
         }
-        if (lane < 3) s_pre[lane] = pick3(pre, lane);
-        if (tile == gridDim.x - 1 && lane < 3) {   // the totals
-            uint* tot = lane == 0 ? off : (lane == 1 ? roff : bpos);
-            tot[n] = pick3(pre, lane) + pick3(agg, lane);
+        if (me < 3) lb_store(st + 3 * (size_t)tile + me, kLbIncl | (pre + s_agg[me]));
+    }
+    if (me < 3) {
+        s_pre[me] = pre;
+        if (tile == gridDim.x - 1) {   // the totals
+            uint* tot = me == 0 ? off : (me == 1 ? roff : bpos);
+            tot[n] = pre + s_agg[me];
         }
     }
     __syncthreads();

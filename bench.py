@@ -51,11 +51,11 @@ def launches_per_window(work):
     """Kernels a window graph launches when its outer candidate list stays
     valid (a rebuild adds the 10 launches of the conditional node's body):
     the outer check, the candidate pass with its scans, the fill, the reverse
-    rows, and with cluster batches the component slots, particle slots and
-    batches; then the window kernel, which with cluster batches exits unless
-    a batch is too large, the free particles and the batches."""
+    rows, and with cluster batches the component pass; then the window
+    kernel, which with cluster batches exits unless a batch is too large, the
+    batches and the free particles."""
     batching = work.get("batched", -1) >= 0
-    relist = 4 + (3 if batching else 0)
+    relist = 4 + (1 if batching else 0)
     return relist + (3 if batching else 1)
 
 

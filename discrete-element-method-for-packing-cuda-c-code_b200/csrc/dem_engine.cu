@@ -348,11 +348,12 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
     long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                   \
         const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap, double hx, double hy,        \
         double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist, uint* __restrict__ wcount,          \
-        uint* __restrict__ cc_parent, uint* __restrict__ cc_zero, long long np, uint* __restrict__ ikey,           \
-        uint* __restrict__ njgi, uint* __restrict__ njli, uint* __restrict__ bflag, uint* __restrict__ scr
+        uint* __restrict__ cc_parent, uint* __restrict__ cc_zero, uint* __restrict__ cc_base, long long np,        \
+        uint* __restrict__ ikey, uint* __restrict__ njgi, uint* __restrict__ njli, uint* __restrict__ bflag,         \
+        uint* __restrict__ scr
 #define DEM_FILTER_ARGS \
-    n, S, R, g, skin, coff, cln, ccap, hx, hy, half_skin, wslot, wlist, wcount, cc_parent, cc_zero, np, ikey, njgi, \
-        njli, bflag, scr
+    n, S, R, g, skin, coff, cln, ccap, hx, hy, half_skin, wslot, wlist, wcount, cc_parent, cc_zero, cc_base, np, ikey, \
+        njgi, njli, bflag, scr
 // The three counts of one particle: row (j > i), reverse row (j < i), bound.
 struct FilterCounts { uint up, down, bound; };
 template <typename Real> __device__ __forceinline__ FilterCounts filter_item(long long ii, DEM_FILTER_PARAMS) {
@@ -409,6 +410,7 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
         if (cc_parent && bound) {   // the coming re-list's components start as singletons
             cc_parent[i] = i;
             cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
+            cc_base[i] = kEmpty;
         }
         o.up = nup;
         o.down = nall - nup;
@@ -431,7 +433,10 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
 constexpr int kFilterThreads = 256;
 constexpr unsigned long long kLbAgg = 1ull << 32, kLbIncl = 2ull << 32;
 constexpr int kLbSpin = 1 << 22;   // a look-back word not published after this many polls: kStBarrier
-inline size_t lb_words(long long np) { return 2 + 6 * (size_t)grid_for(np, kFilterThreads); }
+// [0, 2 + 6 T) the candidate pass's words, [2 + 6 T, 4 + 8 T) the component
+// pass's (T: the tiles of np particles)
+inline size_t lb_words(long long np) { return 4 + 8 * (size_t)grid_for(np, kFilterThreads); }
+inline size_t lb_cc(long long np) { return 2 + 6 * (size_t)grid_for(np, kFilterThreads); }
 
 __device__ __forceinline__ void lb_store(unsigned long long* p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -445,7 +450,8 @@ template <typename Real>
 __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAMS, EngineWords* words, uint* lb,
                                                                 uint* __restrict__ off, uint* __restrict__ roff,
                                                                 uint* __restrict__ bpos, uint* __restrict__ blist,
-                                                                uint* __restrict__ flist) {
+                                                                uint* __restrict__ flist, uint* __restrict__ ccw,
+                                                                uint* __restrict__ bw, long long nbb) {
     constexpr int W = kFilterThreads / 32;
     __shared__ uint s_tile;
     __shared__ uint s_w[3][W];
@@ -461,6 +467,11 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
         return;
     }
     const long long ii = (long long)tile * kFilterThreads + threadIdx.x;
+    if (ccw) {   // the component pass's words and batch windows start empty
+        const long long nthr = (long long)gridDim.x * kFilterThreads;
+        if (ii < 4) ccw[ii] = 0u;
+        for (long long k = ii; k < 3 * nbb; k += nthr) bw[k] = k < nbb ? 0xffffffffu : 0u;
+    }
     const FilterCounts o = filter_item<Real>(ii, DEM_FILTER_ARGS);
     const uint mrow = __reduce_max_sync(0xffffffffu, o.up + o.down);
     const uint lane = lane_id(), warp = threadIdx.x >> 5;
@@ -656,12 +667,13 @@ __global__ void k_nbr_fill(DEM_FILL_PARAMS, const uint* __restrict__ bpos, const
 __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __restrict__ rk, uint* __restrict__ ru,
                            const uint* __restrict__ off, long long cap, uint* parent, const uint* __restrict__ bpos,
                            const uint* __restrict__ blist, uint* __restrict__ csize, uint* __restrict__ cpairs,
-                           const uint* __restrict__ cc_skip) {
+                           const uint* __restrict__ cc_skip, uint* __restrict__ ccw) {
     pdl_wait();
     pdl_trigger();
     if ((long long)off[n] > cap) return;
     if (parent && *cc_skip) parent = nullptr;
     const long long nb = bpos[n];
+    uint mx = 0;   // the largest running component count: the largest component
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
          t += (long long)gridDim.x * blockDim.x) {
         const uint i = blist[t];
@@ -671,10 +683,12 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
         if (parent) {
             const uint r = cc_root(parent, i);
             parent[i] = r;
-            atomicAdd(csize + r, 1u);
+            mx = max(mx, atomicAdd(csize + r, 1u) + 1u);
             atomicAdd(cpairs + r, off[i + 1] - off[i]);
         }
     }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (lane_id() == 0 && mx) atomicMax(ccw + 2, mx);
 }
 
 // ------------------------------------------------------- cluster batches
@@ -684,62 +698,13 @@ __global__ void k_rev_sort(long long n, const uint* __restrict__ roff, uint* __r
 // window.  The re-list finds them with a lock-free union-find over the pairs
 // (hooking the larger root under the smaller, the scheme of ECL-CC,
 // Jaiganesh & Burtscher 2018), groups the bound particles by component into
-// slots (component order by atomics: any order gives the same states, every
-// particle's sums keep their list order), and cuts the slots into batches of
-// whole components, one per resident block of k_batch where they fit (the
-// batch window, cc_target), that one block steps through the window in
-// shared memory.  A batch above the block's capacity (a bed of touching
-// spheres is one component) sends the whole window to the grid-barrier window
-// kernel instead.
-
-// A slot range per component (roots only; one atomic per warp for the slot
-// counter), and the largest component.
-#define DEM_CCBASE_PARAMS                                                                                             \
-    long long n, long long cap, const uint* __restrict__ blist, const uint* __restrict__ bpos,                        \
-    const uint* __restrict__ off, const uint* __restrict__ parent, const uint* __restrict__ size,                     \
-    uint* __restrict__ base, uint* __restrict__ ccw, const uint* __restrict__ cc_skip
-#define DEM_CCBASE_ARGS n, cap, blist, bpos, off, parent, size, base, ccw, cc_skip
-__device__ __forceinline__ void cc_base_warp(long long t, DEM_CCBASE_PARAMS) {
-    if (*cc_skip) {   // no components this re-list: the grid-barrier window kernel has the window
-        if (t == 0) atomicOr(ccw + 1, 1u);
-        return;
-    }
-    if (t == 0 && (long long)off[n] > cap) atomicOr(ccw + 1, 1u);
-    uint i = 0, sz = 0;
-    if (t < (long long)bpos[n]) {
-        i = blist[t];
-        if (parent[i] == i) sz = size[i];
-    }
-    uint inc = sz;
-    const uint lane = lane_id();
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint v = __shfl_up_sync(0xffffffffu, inc, o);
-        if ((int)lane >= o) inc += v;
-    }
-    const uint wtot = __shfl_sync(0xffffffffu, inc, 31);
-    uint wmax = sz;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
-    uint wbase = 0;
-    if (lane == 31 && wtot) {
-        wbase = atomicAdd(ccw, wtot);
-        atomicMax(ccw + 2, wmax);
-    }
-    wbase = __shfl_sync(0xffffffffu, wbase, 31);
-    if (sz) base[i] = wbase + inc - sz;
-}
-
-// Grid-stride over whole warps of the bound list (the first warp always runs:
-// it makes the checks of t == 0).
-__global__ void k_cc_base(DEM_CCBASE_PARAMS) {
-    pdl_wait();
-    pdl_trigger();
-    const long long nthr = (long long)gridDim.x * blockDim.x;
-    const long long nb = max((long long)bpos[n], 1ll);
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t - (long long)lane_id() < nb; t += nthr)
-        cc_base_warp(t, DEM_CCBASE_ARGS);
-}
+// slots (components in root order; members of a component in any order:
+// every particle's sums keep their list order, so the states do not depend
+// on it), and cuts the slots into batches of whole components, one per
+// resident block of k_batch where they fit (the batch window, cc_target),
+// that one block steps through the window in shared memory.  A batch above
+// the block's capacity (a bed of touching spheres is one component) sends
+// the whole window to the grid-barrier window kernel instead.
 
 // The batch window: the bound particles spread over the batch kernel's
 // resident blocks G, at least kBatchMin, at most P minus the largest component
@@ -751,90 +716,188 @@ __device__ __forceinline__ uint cc_target(uint nb, uint G, uint P, uint maxc) {
     return max(t, kBatchMin);
 }
 
-// Each bound particle's slot inside its component's range; each root adds its
-// component to the batch window its first slot falls in: the window's first
-// slot (minimum), particles and pairs.  bw: [0, nbb) first slots, [nbb, 2 nbb)
-// particles, [2 nbb, 3 nbb) pairs.
-#define DEM_CCSLOT_PARAMS                                                                                             \
-    long long n, long long nbb, uint G, uint P, const uint* __restrict__ blist,                                       \
-    const uint* __restrict__ bpos, const uint* __restrict__ parent, const uint* __restrict__ base,                    \
-    const uint* __restrict__ size, const uint* __restrict__ pairs, uint* __restrict__ fill,                           \
-    uint* __restrict__ order, uint* __restrict__ bw, uint* __restrict__ ccw
-#define DEM_CCSLOT_ARGS n, nbb, G, P, blist, bpos, parent, base, size, pairs, fill, order, bw, ccw
-__device__ __forceinline__ void cc_slot_item(long long t, DEM_CCSLOT_PARAMS) {
-    if (ccw[1]) return;   // the window goes to the grid-barrier kernel already
-    const uint nb = bpos[n];
-    const uint tgt = cc_target(nb, G, P, ccw[2]);
-    if (t == 0) ccw[3] = tgt;
-    if (t >= (long long)nb) return;
-    const uint i = blist[t];
-    const uint r = parent[i];
-    if (r >= (uint)n || parent[r] != r) {   // not a root: the window goes to the grid-barrier kernel
-        atomicOr(ccw + 1, 1u);
-        return;
-    }
-    const uint s = base[r] + atomicAdd(fill + r, 1u);
-    if (s >= nb) {
-        atomicOr(ccw + 1, 1u);
-        return;
-    }
-    order[s] = i;
-    if (r == i) {
-        const uint b0 = base[i], bt = b0 / tgt;
-        if ((long long)bt >= nbb) {
-            atomicOr(ccw + 1, 1u);
-            return;
-        }
-        atomicMin(bw + bt, b0);
-        atomicAdd(bw + nbb + bt, size[i]);
-        atomicAdd(bw + 2 * nbb + bt, pairs[i]);
-    }
-}
-
-__global__ void k_cc_slot(DEM_CCSLOT_PARAMS) {
-    pdl_wait();
-    pdl_trigger();
-    const long long nthr = (long long)gridDim.x * blockDim.x;
-    const long long nb = max((long long)bpos[n], 1ll);
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += nthr)
-        cc_slot_item(t, DEM_CCSLOT_ARGS);
-}
-
 // First slot of batch b (the first component whose first slot is b * target
 // or later; all bound particles when none is), and the batch's particles and
-// pairs against the block's capacity (P, Q).
-#define DEM_CCBATCH_PARAMS                                                                                            \
-    long long n, long long nbmax, long long nbb, uint P, uint Q, const uint* __restrict__ bpos,                       \
-    const uint* __restrict__ bw, uint* __restrict__ batch, uint* __restrict__ ccw,                                    \
-    uint* __restrict__ cc_skip
-#define DEM_CCBATCH_ARGS n, nbmax, nbb, P, Q, bpos, bw, batch, ccw, cc_skip
-__device__ __forceinline__ void cc_batches_item(long long b, DEM_CCBATCH_PARAMS) {
-    if (b == 0) {
-        // a component larger than a block (a dense bed): the next kDenseSkip
-        // re-lists skip the component pass (union-find on one giant
-        // component costs more than the window it would batch), then it is
-        // tried again
-        const uint k = *cc_skip;
-        if (k) *cc_skip = k - 1u;
-        else if (ccw[2] > P) *cc_skip = kDenseSkip;
-    }
-    if (b > nbmax || ccw[1]) return;
-    const uint nb = bpos[n], tgt = ccw[3];
-    uint s0 = bw[b];
+// pairs against the block's capacity (P, Q).  bw: [0, nbb) first slots,
+// [nbb, 2 nbb) particles, [2 nbb, 3 nbb) pairs, per batch window.
+__device__ __forceinline__ void cc_batch_entry(uint b, uint nb, uint tgt, long long nbmax, long long nbb, uint P,
+                                               uint Q, const uint* bw, uint* __restrict__ batch, uint* ccw) {
+    uint s0 = __ldcg(bw + b);
     long long k = b;
     // a window with no first slot lies inside a component that started
     // earlier (longer than a block if the search runs out: its batch's count
     // is over P already)
-    while (s0 == 0xffffffffu && k < nbmax && k - b <= (long long)(P / tgt) + 1) s0 = bw[++k];
+    while (s0 == 0xffffffffu && k < nbmax && k - b <= (long long)(P / tgt) + 1) s0 = __ldcg(bw + (++k));
     if (s0 == 0xffffffffu || s0 > nb) s0 = nb;
     batch[b] = s0;
-    if (bw[nbb + b] > P || bw[2 * nbb + b] > Q) atomicOr(ccw + 1, 1u);
+    if (__ldcg(bw + nbb + b) > P || __ldcg(bw + 2 * nbb + b) > Q) atomicOr(ccw + 1, 1u);
 }
 
-__global__ void k_cc_batches(DEM_CCBATCH_PARAMS) {
+// The component pass in one launch, after the reverse rows (which leave
+// every bound particle's root in parent[], the components' particle and pair
+// counts at their roots, and the largest component in ccw[2]).  Tiles of
+// kFilterThreads bound-list entries, taken by ticket: each root's first slot
+// is the exclusive scan, in root order, of the component sizes (decoupled
+// look-back over the tiles before, as in the candidate pass); each member
+// then takes a slot in its component's range (a root precedes its members,
+// so its tile took its ticket earlier; the member waits, bounded, for the
+// root's first slot), and each root adds its component to the batch window
+// its first slot falls in.  The block that finishes last writes the batch
+// table.  ccw: [0] unused, [1] not batchable, [2] largest component, [3]
+// the batch window.  lbc: [0] tile ticket, [1] finished blocks, then one
+// 64-bit look-back word per tile (cleared by the next re-list's fill).
+__global__ void __launch_bounds__(kFilterThreads)
+    k_cc_pass(long long n, long long cap, long long nbmax, long long nbb, uint G, uint P, uint Q,
+              const uint* __restrict__ off, const uint* __restrict__ bpos, const uint* __restrict__ blist,
+              const uint* __restrict__ parent, const uint* __restrict__ size, const uint* __restrict__ pairs,
+              uint* base, uint* __restrict__ fill, uint* __restrict__ order, uint* bw, uint* __restrict__ batch,
+              uint* ccw, uint* __restrict__ cc_skip, uint* lbc, EngineWords* words) {
+    constexpr int W = kFilterThreads / 32;
+    __shared__ uint s_tile, s_last, s_agg, s_pre;
+    __shared__ uint s_w[W], s_red[W];
+    __shared__ int s_near;
     pdl_wait();
     pdl_trigger();
-    cc_batches_item((long long)blockIdx.x * blockDim.x + threadIdx.x, DEM_CCBATCH_ARGS);
+    const uint nb = bpos[n];
+    const uint skip = *cc_skip;
+    const uint maxc = ccw[2];
+    const bool over = (long long)off[n] > cap;
+    const uint tgt = cc_target(nb, G, P, maxc);
+    if (skip || over) {   // no components this re-list: the grid-barrier window kernel has the window
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            atomicOr(ccw + 1, 1u);
+            if (skip) *cc_skip = skip - 1u;
+        }
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) ccw[3] = tgt;
+    const uint ntile = nb == 0 ? 1u : (nb + kFilterThreads - 1) / kFilterThreads;
+    unsigned long long* st = reinterpret_cast<unsigned long long*>(lbc + 2);
+    const uint me = threadIdx.x, lane = lane_id(), warp = me >> 5;
+    for (;;) {
+        if (me == 0) s_tile = atomicAdd(lbc, 1u);
+        __syncthreads();
+        const uint tile = s_tile;
+        if (tile >= ntile) break;
+        const uint t = tile * kFilterThreads + me;
+        uint i = 0, r = kEmpty, sz = 0;
+        if (t < nb) {
+            i = blist[t];
+            r = parent[i];
+            if (r >= (uint)n || parent[r] != r) {   // not a root: the window goes to the grid-barrier kernel
+                atomicOr(ccw + 1, 1u);
+                r = kEmpty;
+            } else if (r == i) {
+                sz = size[i];
+            }
+        }
+        // exclusive scan of the roots' sizes within the tile
+        uint inc = sz;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint x = __shfl_up_sync(0xffffffffu, inc, d);
+            if ((int)lane >= d) inc += x;
+        }
+        if (lane == 31) s_w[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            const uint w = (int)lane < W ? s_w[lane] : 0u;
+            uint wi = w;
+#pragma unroll
+            for (int d = 1; d < W; d <<= 1) {
+                const uint x = __shfl_up_sync(0xffffffffu, wi, d);
+                if ((int)lane >= d) wi += x;
+            }
+            if ((int)lane < W) s_w[lane] = wi - w;
+            if ((int)lane == W - 1) s_agg = wi;
+        }
+        __syncthreads();
+        // the tiles before: published totals up to the nearest inclusive one
+        uint pre = 0;
+        if (tile == 0) {
+            if (me == 0) lb_store(st, kLbIncl | s_agg);
+        } else {
+            if (me == 0) lb_store(st + tile, kLbAgg | s_agg);
+            bool done = false;
+            for (long long b0 = (long long)tile - 1; !done; b0 -= kFilterThreads) {
+                const long long tt = b0 - (long long)me;
+                unsigned long long w = kLbIncl;
+                if (tt >= 0) {
+                    for (int spin = 0;; spin++) {
+                        w = lb_load(st + tt);
+                        if (w >> 32) break;
+                        if (spin >= kLbSpin) {
+                            atomicOr(&words->status, kStBarrier);
+                            atomicOr(ccw + 1, 1u);
+                            w = kLbIncl;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                if (me == 0) s_near = kFilterThreads;
+                __syncthreads();
+                const uint m = __ballot_sync(0xffffffffu, (w >> 32) == 2ull);
+                if (lane == 0 && m) atomicMin(&s_near, (int)(warp * 32 + __ffs(m) - 1));
+                __syncthreads();
+                const uint x = __reduce_add_sync(0xffffffffu, (int)me <= s_near ? (uint)w : 0u);
+                if (lane == 0) s_red[warp] = x;
+                __syncthreads();
+                if (me == 0)
+                    for (int k = 0; k < W; k++) pre += s_red[k];
+                done = s_near < kFilterThreads;
+                __syncthreads();
+            }
+            if (me == 0) lb_store(st + tile, kLbIncl | (pre + s_agg));
+        }
+        if (me == 0) s_pre = pre;
+        __syncthreads();
+        if (r != kEmpty && r == i) {   // the root's first slot
+            const uint b = s_pre + s_w[warp] + inc - sz;
+            asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(base + i), "r"(b) : "memory");
+        }
+        __syncthreads();
+        if (r != kEmpty) {
+            uint b;
+            for (int spin = 0;; spin++) {   // the root's tile started before this one
+                asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(b) : "l"(base + r) : "memory");
+                if (b != kEmpty) break;
+                if (spin >= kLbSpin) {
+                    atomicOr(&words->status, kStBarrier);
+                    atomicOr(ccw + 1, 1u);
+                    break;
+                }
+                __nanosleep(32);
+            }
+            if (b != kEmpty) {
+                const uint s = b + atomicAdd(fill + r, 1u);
+                if (s >= nb) atomicOr(ccw + 1, 1u);
+                else order[s] = i;
+                if (r == i) {
+                    const uint bt = b / tgt;
+                    if ((long long)bt >= nbb) {
+                        atomicOr(ccw + 1, 1u);
+                    } else {
+                        atomicMin(bw + bt, b);
+                        atomicAdd(bw + nbb + bt, size[i]);
+                        atomicAdd(bw + 2 * nbb + bt, pairs[i]);
+                    }
+                }
+            }
+        }
+        __syncthreads();   // s_tile, s_w, s_pre are written again by the next tile
+    }
+    // the block that finishes last: the batch table (and the dense-bed skip)
+    __threadfence();
+    if (me == 0) s_last = atomicAdd(lbc + 1, 1u) == gridDim.x - 1 ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (me == 0 && maxc > P) *cc_skip = kDenseSkip;   // a component larger than a block (a dense bed)
+    if (__ldcg(ccw + 1)) return;
+    const uint nbatch = (nb + tgt - 1) / tgt;
+    const uint bmax = (long long)nbatch < nbmax ? nbatch : (uint)nbmax;
+    for (uint b = me; b <= bmax; b += blockDim.x) cc_batch_entry(b, nb, tgt, nbmax, nbb, P, Q, bw, batch, ccw);
 }
 
 // ------------------------------------------------------------ pair force
@@ -2141,12 +2204,6 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     GridC g = c->grid;
     DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
     const bool cc = c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent;
-    if (cc) {
-        const size_t nbb = (size_t)c->nbatch_max + 2;
-        DEM_CUDA_TRY(cudaMemsetAsync(c->cc_words, 0, 4 * sizeof(uint), s));
-        DEM_CUDA_TRY(cudaMemsetAsync(c->cc_bw, 0xff, nbb * sizeof(uint), s));
-        DEM_CUDA_TRY(cudaMemsetAsync(c->cc_bw + nbb, 0, 2 * nbb * sizeof(uint), s));
-    }
     // every launch after the first is programmatic: each kernel waits for its
     // predecessor before it touches memory, so only the launch latency overlaps
     const bool pdl = c->pdl && !c->profiling;
@@ -2166,8 +2223,9 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     k_filter_scan<Real><<<grid_for(n, kFilterThreads), kFilterThreads, 0, s>>>(
         n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff, (const uint*)c->cln, c->ccap,
         c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin, c->wslot, c->wlist, c->wcount,
-        cc ? c->cc_parent : nullptr, c->cc_size, c->npad, c->ikey, c->njgi, c->njli, c->bflag, c->scr, c->words, c->lb,
-        c->off[dst], c->roff, c->bpos, c->blist, c->flist);
+        cc ? c->cc_parent : nullptr, c->cc_size, c->cc_base, c->npad, c->ikey, c->njgi, c->njli, c->bflag, c->scr,
+        c->words, c->lb, c->off[dst], c->roff, c->bpos, c->blist, c->flist, cc ? c->cc_words : nullptr, c->cc_bw,
+        (long long)c->nbatch_max + 2);
     DEM_LAUNCH_CHECK();
     const unsigned BG = c->bound_grid;
     DEM_CUDA_TRY(launch_ex(
@@ -2176,23 +2234,18 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         c->njli, c->ln[dst], c->lp, planes<double>(c->hist[dst][0], c->cap), (const uint*)c->off[src],
         (const uint*)c->ln[src], planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap,
         c->words, c->carry, (const uint*)c->scr, cc ? c->cc_parent : nullptr, (const uint*)c->bpos,
-        (const uint*)c->blist, (const uint*)c->cc_skip, c->lb, (long long)lb_words(n)));
+        (const uint*)c->blist, (const uint*)c->cc_skip, c->lb, (long long)lb_words(c->npad)));
     DEM_CUDA_TRY(launch_ex(k_rev_sort, BG, B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
                            (const uint*)c->off[dst], c->cap, cc ? c->cc_parent : nullptr, (const uint*)c->bpos,
-                           (const uint*)c->blist, c->cc_size, c->cc_pairs, (const uint*)c->cc_skip));
+                           (const uint*)c->blist, c->cc_size, c->cc_pairs, (const uint*)c->cc_skip, c->cc_words));
     if (cc) {   // the window's components and batches (cluster-batched window path)
         const uint* off = c->off[dst];
         const long long nbb = c->nbatch_max + 2;
-        DEM_CUDA_TRY(launch_ex(k_cc_base, BG, B, s, pdl, n, c->cap, (const uint*)c->blist,
-                               (const uint*)c->bpos, off, (const uint*)c->cc_parent, (const uint*)c->cc_size,
-                               c->cc_base, c->cc_words, (const uint*)c->cc_skip));
-        DEM_CUDA_TRY(launch_ex(k_cc_slot, BG, B, s, pdl, n, nbb, c->batch_grid, BatchCap<Real>::P,
-                               (const uint*)c->blist, (const uint*)c->bpos, (const uint*)c->cc_parent,
-                               (const uint*)c->cc_base, (const uint*)c->cc_size, (const uint*)c->cc_pairs, c->cc_fill,
-                               c->cc_order, c->cc_bw, c->cc_words));
-        DEM_CUDA_TRY(launch_ex(k_cc_batches, grid_for(c->nbatch_max + 1, B), B, s, pdl, n, c->nbatch_max, nbb,
-                               BatchCap<Real>::P, BatchCap<Real>::Q, (const uint*)c->bpos, (const uint*)c->cc_bw,
-                               c->cc_batch, c->cc_words, c->cc_skip));
+        DEM_CUDA_TRY(launch_ex(k_cc_pass, BG, kFilterThreads, s, pdl, n, c->cap, c->nbatch_max, nbb, c->batch_grid,
+                               BatchCap<Real>::P, BatchCap<Real>::Q, off, (const uint*)c->bpos,
+                               (const uint*)c->blist, (const uint*)c->cc_parent, (const uint*)c->cc_size,
+                               (const uint*)c->cc_pairs, c->cc_base, c->cc_fill, c->cc_order, c->cc_bw, c->cc_batch,
+                               c->cc_words, c->cc_skip, c->lb + lb_cc(c->npad), c->words));
     }
     return DEM_OK;
 }

@@ -238,19 +238,36 @@ __device__ __forceinline__ R4<Real> rec_r4(const PRec<Real>* __restrict__ S, con
     return v;
 }
 
-// Switches the build on when the outer list is invalid (oflag) or a particle
-// moved more than odelta since the build.
+// The re-list's first pass over the particles' positions: switches the
+// outer build on (cond: a graph's conditional node) when the outer list is
+// invalid (oflag) or a particle moved more than odelta since the build, and
+// keeps each particle's cell on the configured grid (dem_download_cells)
+// with its wall candidacy in the top bit: within r + skin/2 of a wall (a
+// particle moves less than skin/2 per window, which the step checks, so no
+// other particle can touch a wall before the next re-list -- the pair list's
+// guarantee).  Cell keys stay below 2^31 (the grid is checked).
+constexpr uint kNearWall = 0x80000000u;
 template <typename Real>
-__global__ void k_outer_check(long long n, const PRec<Real>* __restrict__ S, Planes3<double> xo, double odelta2,
-                              const uint* __restrict__ oflag, cudaGraphConditionalHandle h) {
+__global__ void k_outer_check(long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g,
+                              double hx, double hy, double half_skin, uint* __restrict__ ikey, Planes3<double> xo,
+                              double odelta2, const uint* __restrict__ oflag, int cond,
+                              cudaGraphConditionalHandle h) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     bool need = i == 0 && *oflag != 0u;
     if (i < n) {
         const V3<double> p = ld_pos<false>(S + i);
         const double dx = p.x - xo.x[i], dy = p.y - xo.y[i], dz = p.z - xo.z[i];
         need = need || !(dx * dx + dy * dy + dz * dz <= odelta2);
+        const double mg = (double)R[i] + half_skin;
+        const bool near = (p.z < mg) || (p.x + hx < mg) || (hx - p.x < mg) || (p.y + hy < mg) || (hy - p.y < mg);
+        const Real csr = (Real)g.cs;
+        Real xl;
+        const int cx = cell_axis<Real>(p.x, g.ox, csr, g.gx, xl);
+        const int cy = cell_axis<Real>(p.y, g.oy, csr, g.gy, xl);
+        const int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
+        ikey[i] = (((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx) | (near ? kNearWall : 0u);
     }
-    if (__any_sync(0xffffffffu, need) && lane_id() == 0) cudaGraphSetConditional(h, 1u);
+    if (cond && __any_sync(0xffffffffu, need) && lane_id() == 0) cudaGraphSetConditional(h, 1u);
 }
 
 // Cell key of each particle on the outer grid (calcHashD's role,
@@ -334,52 +351,38 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
 }
 
 // The re-list's candidate pass on the outer list, per particle i (id order):
-// the wall candidacy takes a slot (within r + skin/2 of a wall: a particle
-// moves less than skin/2 per window, which the step checks, so no other
-// particle can touch a wall before the next re-list -- the pair list's
-// guarantee), the particle's cell on the configured grid is kept
-// (dem_download_cells), and the outer row is filtered with the exact
-// candidate test on the list coordinates: the counts of the row (j > i) and
-// of the reverse row (j < i), the first kScr row candidates, and the bound
-// flag (any candidate or a wall candidacy).  A bound particle starts the
-// re-list's components (cluster batches) as a singleton; free particles take
-// no part in them.
+// a wall candidacy (found by k_outer_check) takes a slot, and the outer row
+// is filtered with the exact candidate test on the list coordinates: the
+// counts of the row (j > i) and of the reverse row (j < i), the first kScr
+// row candidates, and the bound flag (any candidate or a wall candidacy).  A
+// bound particle starts the re-list's components (cluster batches) as a
+// singleton; free particles take no part in them.
 #define DEM_FILTER_PARAMS                                                                                      \
     long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g, Real skin,                   \
-        const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap, double hx, double hy,        \
-        double half_skin, uint* __restrict__ wslot, uint* __restrict__ wlist, uint* __restrict__ wcount,          \
-        uint* __restrict__ cc_parent, uint* __restrict__ cc_zero, uint* __restrict__ cc_base, long long np,        \
-        uint* __restrict__ ikey, uint* __restrict__ njgi, uint* __restrict__ njli, uint* __restrict__ bflag,         \
-        uint* __restrict__ scr
+        const uint* __restrict__ coff, const uint* __restrict__ cln, long long ccap, uint* __restrict__ wslot,     \
+        uint* __restrict__ wlist, uint* __restrict__ wcount, uint* __restrict__ cc_parent,                         \
+        uint* __restrict__ cc_zero, uint* __restrict__ cc_base, long long np, const uint* __restrict__ ikey,        \
+        uint* __restrict__ njli, uint* __restrict__ bflag, uint* __restrict__ scr
 #define DEM_FILTER_ARGS \
-    n, S, R, g, skin, coff, cln, ccap, hx, hy, half_skin, wslot, wlist, wcount, cc_parent, cc_zero, cc_base, np, ikey, \
-        njgi, njli, bflag, scr
+    n, S, R, g, skin, coff, cln, ccap, wslot, wlist, wcount, cc_parent, cc_zero, cc_base, np, ikey, njli, bflag, scr
 // The three counts of one particle: row (j > i), reverse row (j < i), bound.
 struct FilterCounts { uint up, down, bound; };
 template <typename Real> __device__ __forceinline__ FilterCounts filter_item(long long ii, DEM_FILTER_PARAMS) {
     FilterCounts o = {0u, 0u, 0u};
     if (ii < n) {
         const uint i = (uint)ii;
-        const V3<double> p = ld_pos<false>(S + i);
-        const double mg = (double)R[i] + half_skin;
-        const bool near = (p.z < mg) || (p.x + hx < mg) || (hx - p.x < mg) || (p.y + hy < mg) || (hy - p.y < mg);
-        {
-            const Real csr = (Real)g.cs;
-            Real xl;
-            const int cx = cell_axis<Real>(p.x, g.ox, csr, g.gx, xl);
-            const int cy = cell_axis<Real>(p.y, g.oy, csr, g.gy, xl);
-            const int cz = cell_axis<Real>(p.z, g.oz, csr, g.gz, xl);
-            ikey[i] = ((uint)cz * (uint)g.gy + (uint)cy) * (uint)g.gx + (uint)cx;
-        }
+        const bool near = (ikey[i] & kNearWall) != 0u;
         uint nup = 0, nall = 0;
-        if ((long long)coff[n] <= ccap) {
+        const uint k0 = coff[i], k1 = coff[i + 1];
+        if (k1 > k0 && (long long)coff[n] <= ccap) {   // positions only where there are candidates
+            const V3<double> p = ld_pos<false>(S + i);
             R4<Real> me;
             me.x = (Real)(p.x - g.ox);
             me.y = (Real)(p.y - g.oy);
             me.z = (Real)(p.z - g.oz);
             me.w = R[i];
             uint* out = scr + (size_t)i * kScr;
-            for (uint k = coff[i], k1 = coff[i + 1]; k < k1; k++) {
+            for (uint k = k0; k < k1; k++) {
                 const uint j = cln[k];
                 if (cand_test<Real>(me, rec_r4<Real>(S, R, j, g), skin)) {
                     nall++;
@@ -390,7 +393,6 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
                 }
             }
         }
-        njgi[i] = nup;
         njli[i] = nall - nup;
         // one atomic per warp for its wall candidates (slots only name them)
         const uint act = __activemask();
@@ -432,7 +434,13 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
 // tile); the fill clears them for the next re-list.
 constexpr int kFilterThreads = 256;
 constexpr unsigned long long kLbAgg = 1ull << 32, kLbIncl = 2ull << 32;
-constexpr int kLbSpin = 1 << 22;   // a look-back word not published after this many polls: kStBarrier
+constexpr int kLbSpin = 1 << 16;   // a look-back word not published after this many polls: kStBarrier
+// which bounded wait gave up (EngineWords::pad[0], reported by dem_get_scalars)
+enum : uint { kWaitFilterLb = 1u, kWaitFilterTicket = 2u, kWaitCcLb = 4u, kWaitCcRoot = 8u, kWaitBatchTable = 16u };
+__device__ __forceinline__ void wait_gave_up(EngineWords* w, uint site) {
+    atomicOr(&w->status, kStBarrier);
+    atomicOr(&w->pad[0], site);
+}
 // [0, 2 + 6 T) the candidate pass's words, [2 + 6 T, 4 + 8 T) the component
 // pass's (T: the tiles of np particles)
 inline size_t lb_words(long long np) { return 4 + 8 * (size_t)grid_for(np, kFilterThreads); }
@@ -463,7 +471,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
     __syncthreads();
     const uint tile = s_tile;
     if (tile >= gridDim.x) {   // a ticket left over (the words were not cleared): nothing out of range
-        if (threadIdx.x == 0) atomicOr(&words->status, kStBarrier);
+        if (threadIdx.x == 0) wait_gave_up(words, kWaitFilterTicket);
         return;
     }
     const long long ii = (long long)tile * kFilterThreads + threadIdx.x;
@@ -524,7 +532,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
                     w[0] = lb_load(q); w[1] = lb_load(q + 1); w[2] = lb_load(q + 2);
                     if ((w[0] >> 32) && (w[1] >> 32) && (w[2] >> 32)) break;
                     if (spin >= kLbSpin) {   // never published: record it, count the tile as zero
-                        atomicOr(&words->status, kStBarrier);
+                        wait_gave_up(words, kWaitFilterLb);
                         w[0] = w[1] = w[2] = kLbIncl;
                         break;
                     }
@@ -763,15 +771,13 @@ __global__ void __launch_bounds__(kFilterThreads)
     const uint maxc = ccw[2];
     const bool over = (long long)off[n] > cap;
     const uint tgt = cc_target(nb, G, P, maxc);
-    if (skip || over) {   // no components this re-list: the grid-barrier window kernel has the window
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            atomicOr(ccw + 1, 1u);
-            if (skip) *cc_skip = skip - 1u;
-        }
-        return;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) ccw[3] = tgt;
-    const uint ntile = nb == 0 ? 1u : (nb + kFilterThreads - 1) / kFilterThreads;
+    // skip: no components this re-list (the grid-barrier window kernel has
+    // the window); every block still counts itself finished, and the last
+    // one moves the skip count (cc_skip is read by every block first)
+    const bool run = !(skip || over);
+    if (!run && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(ccw + 1, 1u);
+    if (run && blockIdx.x == 0 && threadIdx.x == 0) ccw[3] = tgt;
+    const uint ntile = !run ? 0u : (nb == 0 ? 1u : (nb + kFilterThreads - 1) / kFilterThreads);
     unsigned long long* st = reinterpret_cast<unsigned long long*>(lbc + 2);
     const uint me = threadIdx.x, lane = lane_id(), warp = me >> 5;
     for (;;) {
@@ -827,7 +833,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                         w = lb_load(st + tt);
                         if (w >> 32) break;
                         if (spin >= kLbSpin) {
-                            atomicOr(&words->status, kStBarrier);
+                            wait_gave_up(words, kWaitCcLb);
                             atomicOr(ccw + 1, 1u);
                             w = kLbIncl;
                             break;
@@ -863,7 +869,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                 asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(b) : "l"(base + r) : "memory");
                 if (b != kEmpty) break;
                 if (spin >= kLbSpin) {
-                    atomicOr(&words->status, kStBarrier);
+                    wait_gave_up(words, kWaitCcRoot);
                     atomicOr(ccw + 1, 1u);
                     break;
                 }
@@ -893,8 +899,11 @@ __global__ void __launch_bounds__(kFilterThreads)
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    if (me == 0 && maxc > P) *cc_skip = kDenseSkip;   // a component larger than a block (a dense bed)
-    if (__ldcg(ccw + 1)) return;
+    if (me == 0) {
+        if (skip) *cc_skip = skip - 1u;
+        else if (maxc > P) *cc_skip = kDenseSkip;   // a component larger than a block (a dense bed)
+    }
+    if (!run || __ldcg(ccw + 1)) return;
     const uint nbatch = (nb + tgt - 1) / tgt;
     const uint bmax = (long long)nbatch < nbmax ? nbatch : (uint)nbmax;
     for (uint b = me; b <= bmax; b += blockDim.x) cc_batch_entry(b, nb, tgt, nbmax, nbb, P, Q, bw, batch, ccw);
@@ -1673,6 +1682,10 @@ __global__ void __maxnreg__(BatchRegs<Real>::value) k_batch(StepArgs<Real> a, in
     batch_smem_layout<Real>(smem, &L);
     const long long nb = a.bpos[a.n];
     const uint tgt = a.ccw[3];
+    if (tgt == 0u) {   // no batch table (cannot happen while ccw[1] is clear): reported, nothing stepped
+        if (threadIdx.x == 0) wait_gave_up(a.words, kWaitBatchTable);
+        return;
+    }
     const uint nbatch = (uint)((nb + tgt - 1) / tgt);
     double mz = 0.0;
     uint cnt = 0, flags = 0;
@@ -2164,6 +2177,15 @@ template <typename Real> int outer_build(dem_ctx* c, const PRec<Real>* S, cudaSt
 // In a capture: k_outer_check, then a conditional node whose body (captured
 // on the context's build stream) is the outer build; the capture goes on
 // after the node.
+template <typename Real>
+int launch_outer_check(dem_ctx* c, const PRec<Real>* S, cudaStream_t s, int cond, cudaGraphConditionalHandle h) {
+    k_outer_check<Real><<<grid_for(c->n, 256), 256, 0, s>>>(
+        c->n, S, (const Real*)c->rad, c->grid, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
+        c->ikey, planes<double>(c->xo, c->npad), c->odelta2, (const uint*)c->oflag, cond, h);
+    DEM_LAUNCH_CHECK();
+    return DEM_OK;
+}
+
 template <typename Real> int outer_build_conditional(dem_ctx* c, const PRec<Real>* S) {
     cudaStream_t s = c->stream;
     cudaStreamCaptureStatus st;
@@ -2173,9 +2195,8 @@ template <typename Real> int outer_build_conditional(dem_ctx* c, const PRec<Real
     DEM_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd));
     cudaGraphConditionalHandle h;
     DEM_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
-    k_outer_check<Real><<<grid_for(c->n, 256), 256, 0, s>>>(c->n, S, planes<double>(c->xo, c->npad), c->odelta2,
-                                                            (const uint*)c->oflag, h);
-    DEM_LAUNCH_CHECK();
+    const int crc = launch_outer_check<Real>(c, S, s, 1, h);
+    if (crc) return crc;
     DEM_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &cg, &deps, &nd));
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
@@ -2215,15 +2236,16 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     if (cst == cudaStreamCaptureStatusActive && c->outer_cond) {
         rc = outer_build_conditional<Real>(c, S);
     } else {
-        rc = outer_build<Real>(c, S, s);
+        rc = launch_outer_check<Real>(c, S, s, 0, cudaGraphConditionalHandle{});
+        if (!rc) rc = outer_build<Real>(c, S, s);
     }
     if (rc) return rc;
     const Real skin = (Real)c->cfg.skin;
     // candidates, their counts' scans, bound and free lists: one pass
     k_filter_scan<Real><<<grid_for(n, kFilterThreads), kFilterThreads, 0, s>>>(
-        n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff, (const uint*)c->cln, c->ccap,
-        c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin, c->wslot, c->wlist, c->wcount,
-        cc ? c->cc_parent : nullptr, c->cc_size, c->cc_base, c->npad, c->ikey, c->njgi, c->njli, c->bflag, c->scr,
+        n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff, (const uint*)c->cln, c->ccap, c->wslot, c->wlist,
+        c->wcount, cc ? c->cc_parent : nullptr, c->cc_size, c->cc_base, c->npad, (const uint*)c->ikey, c->njli,
+        c->bflag, c->scr,
         c->words, c->lb, c->off[dst], c->roff, c->bpos, c->blist, c->flist, cc ? c->cc_words : nullptr, c->cc_bw,
         (long long)c->nbatch_max + 2);
     DEM_LAUNCH_CHECK();
@@ -3373,7 +3395,10 @@ int dem_scalars_from_raw(dem_ctx* c, const void* raw, dem_scalars* out) {
     out->mean_cn = h.n > 0 ? (double)csum / (double)h.n : 0.0;
     out->packing_fraction = mz > 0.0 ? h.vol / (c->cfg.world[0] * c->cfg.world[1] * mz) : 0.0;
     int status = DEM_OK;
-    if (w.status & kStBarrier) status = DEM_ERR_TIMEOUT;
+    if (w.status & kStBarrier) {
+        status = DEM_ERR_TIMEOUT;
+        fail(DEM_ERR_TIMEOUT, "a bounded device wait ran out of time (sites %#x)", w.pad[0]);
+    }
     else if (w.status & kStNonfinite) status = DEM_ERR_NONFINITE;
     else if (w.status & kStCapacity) status = DEM_ERR_CAPACITY;
     else if (w.status & kStSkin) status = DEM_ERR_SKIN;
@@ -3511,6 +3536,7 @@ int dem_download_cells(dem_ctx* c, unsigned int* keys, unsigned int* ids, unsign
     std::vector<uint> key(n);
     DEM_CUDA_TRY(cudaMemcpyAsync(key.data(), c->ikey, n * sizeof(uint), cudaMemcpyDeviceToHost, c->stream));
     DEM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (auto& k : key) k &= ~kNearWall;   // the wall-candidacy bit
     if (c->ordered) {
         const int rp = host_perm(c);
         if (rp) return rp;

@@ -14,7 +14,8 @@ enum : uint {
     kStBarrier = 8u,   // a bounded wait (window-kernel grid barrier, scan look-back) ran out of time
 };
 
-// device words: [0] status bits, [1] max row count
+// device words: [0] status bits, [1] max row count, pad[0]: which bounded
+// waits gave up (kStBarrier)
 struct EngineWords {
     uint status;
     uint max_row;

@@ -134,6 +134,7 @@ int main(int argc, char** argv) {
         dem_scalars sc;
         rc = dem_get_scalars(ctx, &sc);
         if (rc) return die(rc, "dem_get_scalars");
+        if (sc.status != DEM_OK) return die(sc.status, "the step");
         long long na = n;   // particles in the system (m_numParticles)
         if ((rc = dem_active_count(ctx, &na))) return die(rc, "dem_active_count");
         if (it % 1000 == 0) {

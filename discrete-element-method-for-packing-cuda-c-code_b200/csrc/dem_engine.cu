@@ -425,14 +425,16 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
 // (row offsets off, reverse-row offsets roff, bound positions bpos; totals
 // at [n]) by a single-pass scan with decoupled look-back (Merrill & Garland,
 // "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016): tiles
-// of kFilterThreads particles take tickets in the order they start, publish
+// of kFilterTile particles (kFilterItems consecutive ones per thread) take
+// tickets in the order they start, publish
 // their totals, and add up the published words of the tiles before them, so
 // no tile waits on one that has not started.  The tile also writes the bound
 // list (ascending id) and the free list.  Look-back words (lb): [0] the tile
 // ticket, then per tile and count a 64-bit word, the value in the low 32 bits
 // and the kind above (1: the tile's own total, 2: the total through the
 // tile); the fill clears them for the next re-list.
-constexpr int kFilterThreads = 256;
+constexpr int kFilterThreads = 512, kFilterItems = 4, kFilterTile = kFilterThreads * kFilterItems;
+constexpr int kCcThreads = 256;   // the component pass: one bound-list entry per thread and tile
 constexpr unsigned long long kLbAgg = 1ull << 32, kLbIncl = 2ull << 32;
 constexpr int kLbSpin = 1 << 16;   // a look-back word not published after this many polls: kStBarrier
 // which bounded wait gave up (EngineWords::pad[0], reported by dem_get_scalars)
@@ -441,10 +443,10 @@ __device__ __forceinline__ void wait_gave_up(EngineWords* w, uint site) {
     atomicOr(&w->status, kStBarrier);
     atomicOr(&w->pad[0], site);
 }
-// [0, 2 + 6 T) the candidate pass's words, [2 + 6 T, 4 + 8 T) the component
-// pass's (T: the tiles of np particles)
-inline size_t lb_words(long long np) { return 4 + 8 * (size_t)grid_for(np, kFilterThreads); }
-inline size_t lb_cc(long long np) { return 2 + 6 * (size_t)grid_for(np, kFilterThreads); }
+// [0, 2 + 6 T) the candidate pass's words (T: its tiles of np particles),
+// then the component pass's: 2 + 2 Tc (Tc: its tiles of np entries)
+inline size_t lb_cc(long long np) { return 2 + 6 * (size_t)grid_for(np, kFilterTile); }
+inline size_t lb_words(long long np) { return lb_cc(np) + 2 + 2 * (size_t)grid_for(np, kCcThreads); }
 
 __device__ __forceinline__ void lb_store(unsigned long long* p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -474,17 +476,26 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
         if (threadIdx.x == 0) wait_gave_up(words, kWaitFilterTicket);
         return;
     }
-    const long long ii = (long long)tile * kFilterThreads + threadIdx.x;
+    // the thread's kFilterItems consecutive particles
+    const long long i0 = (long long)tile * kFilterTile + (long long)threadIdx.x * kFilterItems;
     if (ccw) {   // the component pass's words and batch windows start empty
         const long long nthr = (long long)gridDim.x * kFilterThreads;
-        if (ii < 4) ccw[ii] = 0u;
-        for (long long k = ii; k < 3 * nbb; k += nthr) bw[k] = k < nbb ? 0xffffffffu : 0u;
+        const long long t0 = (long long)tile * kFilterThreads + threadIdx.x;
+        if (t0 < 4) ccw[t0] = 0u;
+        for (long long k = t0; k < 3 * nbb; k += nthr) bw[k] = k < nbb ? 0xffffffffu : 0u;
     }
-    const FilterCounts o = filter_item<Real>(ii, DEM_FILTER_ARGS);
-    const uint mrow = __reduce_max_sync(0xffffffffu, o.up + o.down);
+    uint up[kFilterItems], dn[kFilterItems], bd[kFilterItems];
+    uint v[3] = {0u, 0u, 0u}, mrow = 0;
+#pragma unroll
+    for (int k = 0; k < kFilterItems; k++) {
+        const FilterCounts o = filter_item<Real>(i0 + k, DEM_FILTER_ARGS);
+        up[k] = o.up; dn[k] = o.down; bd[k] = o.bound;
+        v[0] += o.up; v[1] += o.down; v[2] += o.bound;
+        mrow = max(mrow, o.up + o.down);
+    }
+    mrow = __reduce_max_sync(0xffffffffu, mrow);
     const uint lane = lane_id(), warp = threadIdx.x >> 5;
     if (lane == 0 && mrow) atomicMax(&words->max_row, mrow);
-    const uint v[3] = {o.up, o.down, o.bound};
     uint inc[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -571,14 +582,21 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
         }
     }
     __syncthreads();
-    if (ii < n) {
-        const uint i = (uint)ii;
-        off[i] = s_pre[0] + s_w[0][warp] + inc[0] - v[0];
-        roff[i] = s_pre[1] + s_w[1][warp] + inc[1] - v[1];
-        const uint b = s_pre[2] + s_w[2][warp] + inc[2] - v[2];
-        bpos[i] = b;
-        if (o.bound) blist[b] = i;
-        else flist[i - b] = i;
+    uint e0 = s_pre[0] + s_w[0][warp] + inc[0] - v[0];
+    uint e1 = s_pre[1] + s_w[1][warp] + inc[1] - v[1];
+    uint e2 = s_pre[2] + s_w[2][warp] + inc[2] - v[2];
+#pragma unroll
+    for (int k = 0; k < kFilterItems; k++) {
+        const long long ii = i0 + k;
+        if (ii < n) {
+            const uint i = (uint)ii;
+            off[i] = e0;
+            roff[i] = e1;
+            bpos[i] = e2;
+            if (bd[k]) blist[e2] = i;
+            else flist[i - e2] = i;
+        }
+        e0 += up[k]; e1 += dn[k]; e2 += bd[k];
     }
 }
 
@@ -744,7 +762,7 @@ __device__ __forceinline__ void cc_batch_entry(uint b, uint nb, uint tgt, long l
 // The component pass in one launch, after the reverse rows (which leave
 // every bound particle's root in parent[], the components' particle and pair
 // counts at their roots, and the largest component in ccw[2]).  Tiles of
-// kFilterThreads bound-list entries, taken by ticket: each root's first slot
+// kCcThreads bound-list entries, taken by ticket: each root's first slot
 // is the exclusive scan, in root order, of the component sizes (decoupled
 // look-back over the tiles before, as in the candidate pass); each member
 // then takes a slot in its component's range (a root precedes its members,
@@ -754,13 +772,13 @@ __device__ __forceinline__ void cc_batch_entry(uint b, uint nb, uint tgt, long l
 // table.  ccw: [0] unused, [1] not batchable, [2] largest component, [3]
 // the batch window.  lbc: [0] tile ticket, [1] finished blocks, then one
 // 64-bit look-back word per tile (cleared by the next re-list's fill).
-__global__ void __launch_bounds__(kFilterThreads)
+__global__ void __launch_bounds__(kCcThreads)
     k_cc_pass(long long n, long long cap, long long nbmax, long long nbb, uint G, uint P, uint Q,
               const uint* __restrict__ off, const uint* __restrict__ bpos, const uint* __restrict__ blist,
               const uint* __restrict__ parent, const uint* __restrict__ size, const uint* __restrict__ pairs,
               uint* base, uint* __restrict__ fill, uint* __restrict__ order, uint* bw, uint* __restrict__ batch,
               uint* ccw, uint* __restrict__ cc_skip, uint* lbc, EngineWords* words) {
-    constexpr int W = kFilterThreads / 32;
+    constexpr int W = kCcThreads / 32;
     __shared__ uint s_tile, s_last, s_agg, s_pre;
     __shared__ uint s_w[W], s_red[W];
     __shared__ int s_near;
@@ -777,7 +795,7 @@ __global__ void __launch_bounds__(kFilterThreads)
     const bool run = !(skip || over);
     if (!run && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(ccw + 1, 1u);
     if (run && blockIdx.x == 0 && threadIdx.x == 0) ccw[3] = tgt;
-    const uint ntile = !run ? 0u : (nb == 0 ? 1u : (nb + kFilterThreads - 1) / kFilterThreads);
+    const uint ntile = !run ? 0u : (nb == 0 ? 1u : (nb + kCcThreads - 1) / kCcThreads);
     unsigned long long* st = reinterpret_cast<unsigned long long*>(lbc + 2);
     const uint me = threadIdx.x, lane = lane_id(), warp = me >> 5;
     for (;;) {
@@ -785,7 +803,7 @@ __global__ void __launch_bounds__(kFilterThreads)
         __syncthreads();
         const uint tile = s_tile;
         if (tile >= ntile) break;
-        const uint t = tile * kFilterThreads + me;
+        const uint t = tile * kCcThreads + me;
         uint i = 0, r = kEmpty, sz = 0;
         if (t < nb) {
             i = blist[t];
@@ -825,7 +843,7 @@ __global__ void __launch_bounds__(kFilterThreads)
         } else {
             if (me == 0) lb_store(st + tile, kLbAgg | s_agg);
             bool done = false;
-            for (long long b0 = (long long)tile - 1; !done; b0 -= kFilterThreads) {
+            for (long long b0 = (long long)tile - 1; !done; b0 -= kCcThreads) {
                 const long long tt = b0 - (long long)me;
                 unsigned long long w = kLbIncl;
                 if (tt >= 0) {
@@ -841,7 +859,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                         __nanosleep(32);
                     }
                 }
-                if (me == 0) s_near = kFilterThreads;
+                if (me == 0) s_near = kCcThreads;
                 __syncthreads();
                 const uint m = __ballot_sync(0xffffffffu, (w >> 32) == 2ull);
                 if (lane == 0 && m) atomicMin(&s_near, (int)(warp * 32 + __ffs(m) - 1));
@@ -851,7 +869,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                 __syncthreads();
                 if (me == 0)
                     for (int k = 0; k < W; k++) pre += s_red[k];
-                done = s_near < kFilterThreads;
+                done = s_near < kCcThreads;
                 __syncthreads();
             }
             if (me == 0) lb_store(st + tile, kLbIncl | (pre + s_agg));
@@ -893,12 +911,17 @@ __global__ void __launch_bounds__(kFilterThreads)
         }
         __syncthreads();   // s_tile, s_w, s_pre are written again by the next tile
     }
-    // the block that finishes last: the batch table (and the dense-bed skip)
-    __threadfence();
-    if (me == 0) s_last = atomicAdd(lbc + 1, 1u) == gridDim.x - 1 ? 1u : 0u;
+    // the block that finishes last: the batch table (and the dense-bed skip);
+    // its reads are of words changed by atomics only (bw, ccw), and one fence
+    // after the block barrier orders the block's updates before its count
+    __syncthreads();
+    if (me == 0) {
+        __threadfence();
+        s_last = atomicAdd(lbc + 1, 1u) == gridDim.x - 1 ? 1u : 0u;
+        if (s_last) __threadfence();
+    }
     __syncthreads();
     if (!s_last) return;
-    __threadfence();
     if (me == 0) {
         if (skip) *cc_skip = skip - 1u;
         else if (maxc > P) *cc_skip = kDenseSkip;   // a component larger than a block (a dense bed)
@@ -2242,7 +2265,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     if (rc) return rc;
     const Real skin = (Real)c->cfg.skin;
     // candidates, their counts' scans, bound and free lists: one pass
-    k_filter_scan<Real><<<grid_for(n, kFilterThreads), kFilterThreads, 0, s>>>(
+    k_filter_scan<Real><<<grid_for(n, kFilterTile), kFilterThreads, 0, s>>>(
         n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff, (const uint*)c->cln, c->ccap, c->wslot, c->wlist,
         c->wcount, cc ? c->cc_parent : nullptr, c->cc_size, c->cc_base, c->npad, (const uint*)c->ikey, c->njli,
         c->bflag, c->scr,
@@ -2263,7 +2286,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     if (cc) {   // the window's components and batches (cluster-batched window path)
         const uint* off = c->off[dst];
         const long long nbb = c->nbatch_max + 2;
-        DEM_CUDA_TRY(launch_ex(k_cc_pass, BG, kFilterThreads, s, pdl, n, c->cap, c->nbatch_max, nbb, c->batch_grid,
+        DEM_CUDA_TRY(launch_ex(k_cc_pass, BG, kCcThreads, s, pdl, n, c->cap, c->nbatch_max, nbb, c->batch_grid,
                                BatchCap<Real>::P, BatchCap<Real>::Q, off, (const uint*)c->bpos,
                                (const uint*)c->blist, (const uint*)c->cc_parent, (const uint*)c->cc_size,
                                (const uint*)c->cc_pairs, c->cc_base, c->cc_fill, c->cc_order, c->cc_bw, c->cc_batch,

@@ -250,9 +250,10 @@ constexpr uint kNearWall = 0x80000000u;
 template <typename Real>
 __global__ void k_outer_check(long long n, const PRec<Real>* __restrict__ S, const Real* __restrict__ R, GridC g,
                               double hx, double hy, double half_skin, uint* __restrict__ ikey, Planes3<double> xo,
-                              double odelta2, const uint* __restrict__ oflag, int cond,
+                              double odelta2, const uint* __restrict__ oflag, uint* __restrict__ wcount, int cond,
                               cudaGraphConditionalHandle h) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *wcount = 0u;   // the candidate pass counts the wall candidates
     bool need = i == 0 && *oflag != 0u;
     if (i < n) {
         const V3<double> p = ld_pos<false>(S + i);
@@ -365,16 +366,38 @@ __global__ void k_outer_fill(long long n, const uint* __restrict__ sid2, const R
         uint* __restrict__ njli, uint* __restrict__ bflag, uint* __restrict__ scr
 #define DEM_FILTER_ARGS \
     n, S, R, g, skin, coff, cln, ccap, wslot, wlist, wcount, cc_parent, cc_zero, cc_base, np, ikey, njli, bflag, scr
-// The three counts of one particle: row (j > i), reverse row (j < i), bound.
-struct FilterCounts { uint up, down, bound; };
-template <typename Real> __device__ __forceinline__ FilterCounts filter_item(long long ii, DEM_FILTER_PARAMS) {
-    FilterCounts o = {0u, 0u, 0u};
-    if (ii < n) {
-        const uint i = (uint)ii;
-        const bool near = (ikey[i] & kNearWall) != 0u;
+// The candidate pass for kFilterItems consecutive particles i0, i0+1, ...
+// of one thread: their cell words (wall-candidacy bit) and outer-row bounds
+// are loaded together first, so that the thread waits on one chain of loads
+// rather than one per particle; only particles with outer candidates load
+// positions.  Outputs per particle: row and reverse-row counts, bound flag.
+template <int K> struct FilterCounts { uint up[K], dn[K], bd[K]; };
+template <typename Real, int K>
+__device__ __forceinline__ FilterCounts<K> filter_items(long long i0, DEM_FILTER_PARAMS) {
+    FilterCounts<K> o;
+    uint key[K], cb[K + 1];
+    const bool whole = i0 + K <= n;
+    if (whole && K == 4) {   // i0 is a multiple of 4: aligned 16-byte loads
+        const uint4 kq = *reinterpret_cast<const uint4*>(ikey + i0);
+        const uint4 cq = *reinterpret_cast<const uint4*>(coff + i0);
+        key[0] = kq.x; key[1] = kq.y; key[2] = kq.z; key[3] = kq.w;
+        cb[0] = cq.x; cb[1] = cq.y; cb[2] = cq.z; cb[3] = cq.w;
+        cb[K] = coff[i0 + K];
+    } else {
+#pragma unroll
+        for (int k = 0; k <= K; k++) {   // coff has n + 1 entries
+            if (k < K) key[k] = i0 + k < n ? ikey[i0 + k] : 0u;
+            cb[k] = i0 + k <= n ? coff[i0 + k] : 0u;
+        }
+    }
+    const bool list_ok = (long long)coff[n] <= ccap;
+    uint nwall = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const long long ii = i0 + k;
         uint nup = 0, nall = 0;
-        const uint k0 = coff[i], k1 = coff[i + 1];
-        if (k1 > k0 && (long long)coff[n] <= ccap) {   // positions only where there are candidates
+        if (ii < n && list_ok && cb[k + 1] > cb[k]) {   // positions only where there are candidates
+            const uint i = (uint)ii;
             const V3<double> p = ld_pos<false>(S + i);
             R4<Real> me;
             me.x = (Real)(p.x - g.ox);
@@ -382,8 +405,8 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
             me.z = (Real)(p.z - g.oz);
             me.w = R[i];
             uint* out = scr + (size_t)i * kScr;
-            for (uint k = k0; k < k1; k++) {
-                const uint j = cln[k];
+            for (uint q = cb[k]; q < cb[k + 1]; q++) {
+                const uint j = cln[q];
                 if (cand_test<Real>(me, rec_r4<Real>(S, R, j, g), skin)) {
                     nall++;
                     if (j > i) {
@@ -393,30 +416,43 @@ template <typename Real> __device__ __forceinline__ FilterCounts filter_item(lon
                 }
             }
         }
-        njli[i] = nall - nup;
-        // one atomic per warp for its wall candidates (slots only name them)
-        const uint act = __activemask();
-        const uint m = __ballot_sync(act, near);
-        uint base = 0;
-        const int lead = __ffs(act) - 1;
-        if ((int)lane_id() == lead && m) base = atomicAdd(wcount, (uint)__popc(m));
-        base = __shfl_sync(act, base, lead);
-        uint ws = kEmpty;
-        if (near) {
-            ws = base + (uint)__popc(m & ((1u << lane_id()) - 1u));
-            wlist[ws] = i;
+        const bool near = ii < n && (key[k] & kNearWall) != 0u;
+        nwall += near ? 1u : 0u;
+        o.up[k] = nup;
+        o.dn[k] = nall - nup;
+        o.bd[k] = (ii < n && (nall > 0 || near)) ? 1u : 0u;
+    }
+    // wall slots: one atomic per warp for all its wall candidates (slots only
+    // name them; their order does not matter)
+    const uint lane = lane_id();
+    uint incw = nwall;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint t = __shfl_up_sync(0xffffffffu, incw, d);
+        if ((int)lane >= d) incw += t;
+    }
+    const uint wtot = __shfl_sync(0xffffffffu, incw, 31);
+    uint wbase = 0;
+    if (lane == 31 && wtot) wbase = atomicAdd(wcount, wtot);
+    uint ws = __shfl_sync(0xffffffffu, wbase, 31) + incw - nwall;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const long long ii = i0 + k;
+        if (ii >= n) continue;
+        const uint i = (uint)ii;
+        njli[i] = o.dn[k];
+        uint slot = kEmpty;
+        if (key[k] & kNearWall) {
+            slot = ws++;
+            wlist[slot] = i;
         }
-        wslot[i] = ws;
-        const bool bound = nall > 0 || near;
-        bflag[i] = bound ? 1u : 0u;
-        if (cc_parent && bound) {   // the coming re-list's components start as singletons
+        wslot[i] = slot;
+        bflag[i] = o.bd[k];
+        if (cc_parent && o.bd[k]) {   // the coming re-list's components start as singletons
             cc_parent[i] = i;
             cc_zero[i] = 0u; cc_zero[np + i] = 0u; cc_zero[2 * np + i] = 0u;
             cc_base[i] = kEmpty;
         }
-        o.up = nup;
-        o.down = nall - nup;
-        o.bound = bound ? 1u : 0u;
     }
     return o;
 }
@@ -484,14 +520,13 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_scan(DEM_FILTER_PARAM
         if (t0 < 4) ccw[t0] = 0u;
         for (long long k = t0; k < 3 * nbb; k += nthr) bw[k] = k < nbb ? 0xffffffffu : 0u;
     }
-    uint up[kFilterItems], dn[kFilterItems], bd[kFilterItems];
+    const FilterCounts<kFilterItems> fc = filter_items<Real, kFilterItems>(i0, DEM_FILTER_ARGS);
+    const uint *up = fc.up, *dn = fc.dn, *bd = fc.bd;
     uint v[3] = {0u, 0u, 0u}, mrow = 0;
 #pragma unroll
     for (int k = 0; k < kFilterItems; k++) {
-        const FilterCounts o = filter_item<Real>(i0 + k, DEM_FILTER_ARGS);
-        up[k] = o.up; dn[k] = o.down; bd[k] = o.bound;
-        v[0] += o.up; v[1] += o.down; v[2] += o.bound;
-        mrow = max(mrow, o.up + o.down);
+        v[0] += up[k]; v[1] += dn[k]; v[2] += bd[k];
+        mrow = max(mrow, up[k] + dn[k]);
     }
     mrow = __reduce_max_sync(0xffffffffu, mrow);
     const uint lane = lane_id(), warp = threadIdx.x >> 5;
@@ -2204,7 +2239,7 @@ template <typename Real>
 int launch_outer_check(dem_ctx* c, const PRec<Real>* S, cudaStream_t s, int cond, cudaGraphConditionalHandle h) {
     k_outer_check<Real><<<grid_for(c->n, 256), 256, 0, s>>>(
         c->n, S, (const Real*)c->rad, c->grid, c->cfg.world[0] * 0.5, c->cfg.world[1] * 0.5, 0.5 * c->cfg.skin,
-        c->ikey, planes<double>(c->xo, c->npad), c->odelta2, (const uint*)c->oflag, cond, h);
+        c->ikey, planes<double>(c->xo, c->npad), c->odelta2, (const uint*)c->oflag, c->wcount, cond, h);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -2246,7 +2281,6 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
     cudaStream_t s = c->stream;
     const PRec<Real>* S = (const PRec<Real>*)c->rec[c->sbuf];
     GridC g = c->grid;
-    DEM_CUDA_TRY(cudaMemsetAsync(c->wcount, 0, sizeof(uint), s));
     const bool cc = c->batching && c->mode == DEM_FORCE_PCCP && c->cc_parent;
     // every launch after the first is programmatic: each kernel waits for its
     // predecessor before it touches memory, so only the launch latency overlaps

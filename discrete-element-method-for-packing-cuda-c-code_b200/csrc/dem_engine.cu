@@ -1188,6 +1188,10 @@ __device__ __forceinline__ double mixed_km(double dt, float m) { return __ddiv_r
 __device__ __forceinline__ float mixed_ki(float dtr, float I) { return __fdiv_rn(__fmul_rn(dtr, dtr), I); }
 
 // Mixed step with the factors given (the same operations as integrate<float>).
+// FIN = false leaves out the non-finite check, which a caller then makes
+// once on the final state (a non-finite position or displacement stays
+// non-finite through later steps of the same particle).
+template <bool FIN = true>
 __device__ __forceinline__ void integrate_k(V3<float> F, V3<float> T, double km, float kI, float half_skin2,
                                             V3<double>& x, V3<double>& d, V3<float>& a, float4& q, uint& flags,
                                             double& mz) {
@@ -1203,7 +1207,7 @@ __device__ __forceinline__ void integrate_k(V3<float> F, V3<float> T, double km,
     q.z = __fadd_rn(q.z, __double2float_rn(d.z));
     const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
     if (q2 > half_skin2) flags |= kStSkin;
-    if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
+    if (FIN && (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z))) flags |= kStNonfinite;
     mz = x.z > 0.0 ? x.z : 0.0;
 }
 
@@ -1424,10 +1428,11 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Re
     const Real I = (Real)0.4 * m * (r * r);
     const double km = mixed_km(a.pc.dt, (float)m);
     const float kI = mixed_ki((float)a.dtr, (float)I);
+    const Real gz = (Real)0 + -sphere_mass(a.density, r);   // the force of every step: gravity
     for (int s = slot0; s < slot0 + nsteps; s++) {
         if (s == 0) { q.x = 0.f; q.y = 0.f; q.z = 0.f; }
         V3<Real> F = zero3<Real>(), T = zero3<Real>();
-        F.z += -sphere_mass(a.density, r);
+        F.z = gz;
         if (rec) {
             a.dbgF[3 * i] = F.x; a.dbgF[3 * i + 1] = F.y; a.dbgF[3 * i + 2] = F.z;
             a.dbgT[3 * i] = T.x; a.dbgT[3 * i + 1] = T.y; a.dbgT[3 * i + 2] = T.z;
@@ -1435,11 +1440,13 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Re
         }
         double mz;
         if constexpr (sizeof(Real) == 4)   // the factors computed once (the same values integrate computes)
-            integrate_k(F, T, km, kI, a.pc.half_skin2, x, d, av, q, flags, mz);
+            integrate_k<false>(F, T, km, kI, a.pc.half_skin2, x, d, av, q, flags, mz);
         else
             integrate<Real>(F, T, m, I, a.pc.dt, a.dtr, a.pc.half_skin2, x, d, av, q, flags, mz);
         if (s == observe_slot) mz_obs = mz;
     }
+    if constexpr (sizeof(Real) == 4)
+        if (!isfinite(x.x + x.y + x.z) || !isfinite(d.x + d.y + d.z)) flags |= kStNonfinite;
     st_rec(Sout + i, x, d, av, r);
     a.Q[i] = q;
 }

@@ -1455,7 +1455,6 @@ __device__ __forceinline__ void free_item(const StepArgs<Real>& a, const PRec<Re
 template <typename Real>
 __global__ void __launch_bounds__(256) k_free_run(StepArgs<Real> a, int slot0, int nsteps, int observe_slot,
                                                   StepPartials part, size_t clr0, size_t clr1) {
-    if (a.batch && a.ccw[1]) return;   // the grid-barrier window kernel steps this window's free particles too
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz_obs = 0.0;
     uint flags = 0;
@@ -1587,12 +1586,13 @@ __device__ __forceinline__ void free_sweep(const StepArgs<Real>& a, const PRec<R
 template <typename Real>
 __global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int K, StepPartials part, size_t npart,
                                                            uint* bar) {
-    if (a.batch && !a.ccw[1]) return;   // the cluster batches (k_batch, k_free_run) step this window
+    if (a.batch && !a.ccw[1]) return;   // the cluster batches (k_batch) step this window
     uint nbar = 0;
     const uint nw = *a.wcount;
     const uint total = a.off[a.n];
     const long long items = (long long)nw + ((long long)total <= a.cap ? (long long)total : 0ll);
-    const long long nb = a.bpos[a.n], nf = a.n - nb;
+    // a batched window's free particles are k_free_run's (beside this kernel)
+    const long long nb = a.bpos[a.n], nf = a.batch ? 0 : a.n - nb;
     const uint nbb = bound_blocks(items, nb, nf, gridDim.x, a.split);
     const long long warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double mz = 0.0;
@@ -2281,6 +2281,8 @@ template <typename Real> int outer_build_conditional(dem_ctx* c, const PRec<Real
     return DEM_OK;
 }
 
+template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nsteps, cudaStream_t s, int batch = 0);
+
 template <typename Real> int launch_relist(dem_ctx* c, int src) {
     const long long n = c->n;
     const int dst = 1 - src;
@@ -2313,6 +2315,17 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         c->words, c->lb, c->off[dst], c->roff, c->bpos, c->blist, c->flist, cc ? c->cc_words : nullptr, c->cc_bw,
         (long long)c->nbatch_max + 2);
     DEM_LAUNCH_CHECK();
+    if (c->free_early) {
+        // a batched window follows: its free particles need nothing of the
+        // re-list after the free list, and the passes after this one touch
+        // bound particles only, so they step the whole window now, beside
+        // the rest of the re-list (joined at the window's end)
+        DEM_CUDA_TRY(cudaEventRecord(c->evfork, s));
+        DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
+        rc = launch_free<Real>(c, dst, 0, c->cfg.relist_interval, c->stream2, 1);
+        if (rc) return rc;
+        DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
+    }
     const unsigned BG = c->bound_grid;
     DEM_CUDA_TRY(launch_ex(
         k_nbr_fill<Real>, BG, B, s, pdl, n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
@@ -2392,7 +2405,7 @@ template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
 }
 
 // Free particles, window slots slot0 .. slot0+nsteps-1, on stream s.
-template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nsteps, cudaStream_t s, int batch = 0) {
+template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nsteps, cudaStream_t s, int batch) {
     const int obs = c->observe_slot;
     const int os = (obs >= slot0 && obs < slot0 + nsteps) ? obs : slot0;
     StepArgs<Real> a = step_args<Real>(c, lst, slot0);
@@ -2427,7 +2440,9 @@ template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window<Real>, a, K, partials(c, K - 1), c->npart, c->bar));
+    // a batched window's kernel leaves the free particles' partials to k_free_run
+    DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window<Real>, a, K, partials(c, K - 1),
+                                    batch ? (size_t)c->nblk : c->npart, c->bar));
     return DEM_OK;
 }
 
@@ -2461,7 +2476,7 @@ template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const Wi
     const int K = c->cfg.relist_interval;
     int rc = launch_window<Real>(c, lst, tape, 1);
     if (rc) return rc;
-    DEM_CUDA_TRY(cudaEventRecord(c->evfork, c->stream));
+    if (!c->free_early) DEM_CUDA_TRY(cudaEventRecord(c->evfork, c->stream));
     StepArgs<Real> a = step_args<Real>(c, lst, 0);
     a.batch = 1;
     a.dbgF = a.dbgT = nullptr;
@@ -2488,10 +2503,12 @@ template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const Wi
         DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<Real>, a, K, (const uint*)c->cc_order,
                                         (const uint*)c->cc_batch, c->cc_loc, partials(c, K - 1), (size_t)c->nblk));
     }
-    DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
-    rc = launch_free<Real>(c, lst, 0, K, c->stream2, 1);
-    if (rc) return rc;
-    DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
+    if (!c->free_early) {   // else forked by the re-list, right after the candidate pass
+        DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
+        rc = launch_free<Real>(c, lst, 0, K, c->stream2, 1);
+        if (rc) return rc;
+        DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
+    }
     DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->evjoin, 0));
     return DEM_OK;
 }
@@ -2578,22 +2595,26 @@ int enqueue_window(dem_ctx* c, int src) {
     const int K = c->cfg.relist_interval;
     const bool wt = c->wtiming_capture;
     if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[0], c->stream, cudaEventRecordExternal));
+    // a batched window: the free particles start inside the re-list
+    c->free_early = c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel && use_batches(c);
+    c->observe_slot = K - 1;
     int rc = relist(c, src);
-    if (rc) return rc;
+    if (rc) { c->free_early = false; return rc; }
     if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[1], c->stream, cudaEventRecordExternal));
     c->hph = 0;
     const int lst = 1 - src;
-    c->observe_slot = K - 1;
     const bool mixed = c->prec == DEM_PREC_MIXED;
     if (c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel) {
         // every step of the window in one cooperative launch, or the cluster
         // batches beside the free particles
         rc = window_kernel(c, lst, nullptr);
+        c->free_early = false;
         if (rc) return rc;
         if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[2], c->stream, cudaEventRecordExternal));
         c->wtiming_path = 1;
         return DEM_OK;
     }
+    c->free_early = false;
     if (c->mode == DEM_FORCE_PP && !c->record && c->win_kernel) {
         // PP: every step of the window in one cooperative launch
         rc = mixed ? launch_window_pp<float>(c, lst, c->sbuf, c->hph)

@@ -238,6 +238,7 @@ struct dem_ctx {
     cudaEvent_t evfork = nullptr, evjoin = nullptr;
     int prio_hi = 0;                 // the device's highest stream priority (the batch kernel's launches)
     bool free_in_window = false;     // capturing: the free particles run as one window kernel
+    bool free_early = false;         // enqueueing a batched window: the re-list forks its free particles
     uint* bar = nullptr;             // window-kernel grid barrier: [0] arrival counter
     unsigned win_grid = 1;           // window-kernel blocks (all co-resident)
     bool win_kernel = true;          // whole PCCP windows as one cooperative launch

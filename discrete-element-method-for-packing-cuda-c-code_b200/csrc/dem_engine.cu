@@ -1388,7 +1388,8 @@ __device__ __forceinline__ void bound_item(const StepArgs<Real>& a, const Partic
 // PCCP particle kernel: one thread per bound particle (blist[t], t < nB =
 // bpos[n]).
 template <typename Real>
-__global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(StepArgs<Real> a, StepPartials part) {
+__global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(StepArgs<Real> a, StepPartials part,
+                                                                     size_t clr1) {
     pdl_trigger();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double mz = 0.0;
@@ -1407,6 +1408,7 @@ __global__ void __launch_bounds__(256, DEM_PARTICLE_MINB) k_particle(StepArgs<Re
     pdl_wait();
     if (live) bound_item<Real, false>(a, a.pc, i, r, ws, total, o0, o1, r0, r1, mz, cnt, flags);
     block_observables(mz, cnt, flags, a.pc.observe, part, a.words);
+    if (a.pc.observe) clear_partials(part, gridDim.x, clr1);
 }
 
 // Free particle i (no listed pair and no wall candidacy in this window): until
@@ -2198,14 +2200,16 @@ ParticleCommon particle_common(const dem_ctx* c, int slot) {
     return pc;
 }
 
-// Per slot: nblk partials of the (bound-)particle kernel, then nblk of the
-// free-particle kernel.
+// Per slot: fpart partials of the particle kernels (the bound-particle, batch
+// and window kernels: fpart is at least each one's grid), then nblk of the
+// free-particle kernel.  A kernel that writes a region clears the rest of it
+// (or, when it steps every particle, the rest of the slot).
 StepPartials partials(const dem_ctx* c, int slot) {
     return StepPartials{c->part_mz + (size_t)slot * c->npart, c->part_cnt + (size_t)slot * c->npart};
 }
 StepPartials free_partials(const dem_ctx* c, int slot) {
-    return StepPartials{c->part_mz + (size_t)slot * c->npart + c->nblk,
-                        c->part_cnt + (size_t)slot * c->npart + c->nblk};
+    return StepPartials{c->part_mz + (size_t)slot * c->npart + c->fpart,
+                        c->part_cnt + (size_t)slot * c->npart + c->fpart};
 }
 
 // List build from the current state, carrying history from list buffer src
@@ -2400,7 +2404,7 @@ template <typename Real> int launch_pair(dem_ctx* c, int lst, int slot) {
 
 template <typename Real> int launch_particle(dem_ctx* c, int lst, int slot) {
     DEM_CUDA_TRY(launch_ex(k_particle<Real>, grid_for(c->n, 256), 256, c->stream, step_pdl(c, slot, false),
-                           step_args<Real>(c, lst, slot), partials(c, slot)));
+                           step_args<Real>(c, lst, slot), partials(c, slot), (size_t)c->fpart));
     return DEM_OK;
 }
 
@@ -2411,8 +2415,8 @@ template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nst
     StepArgs<Real> a = step_args<Real>(c, lst, slot0);
     a.batch = batch;
     if (nsteps != 1) a.dbgF = a.dbgT = nullptr, a.dbgC = nullptr;
-    k_free_run<Real><<<grid_for(c->n, 256), 256, 0, s>>>(a, slot0, nsteps, obs, free_partials(c, os), c->nblk,
-                                                         c->npart - c->nblk);
+    const unsigned g = grid_for(c->n, 256);
+    k_free_run<Real><<<g, 256, 0, s>>>(a, slot0, nsteps, obs, free_partials(c, os), (size_t)g, (size_t)c->nblk);
     DEM_LAUNCH_CHECK();
     return DEM_OK;
 }
@@ -2442,7 +2446,7 @@ template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape
     cfg.numAttrs = 1;
     // a batched window's kernel leaves the free particles' partials to k_free_run
     DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window<Real>, a, K, partials(c, K - 1),
-                                    batch ? (size_t)c->nblk : c->npart, c->bar));
+                                    batch ? (size_t)c->fpart : c->npart, c->bar));
     return DEM_OK;
 }
 
@@ -2501,7 +2505,7 @@ template <typename Real> int launch_batched_window(dem_ctx* c, int lst, const Wi
         cfg.attrs = at;
         cfg.numAttrs = 1;
         DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<Real>, a, K, (const uint*)c->cc_order,
-                                        (const uint*)c->cc_batch, c->cc_loc, partials(c, K - 1), (size_t)c->nblk));
+                                        (const uint*)c->cc_batch, c->cc_loc, partials(c, K - 1), (size_t)c->fpart));
     }
     if (!c->free_early) {   // else forked by the re-list, right after the candidate pass
         DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
@@ -2526,7 +2530,7 @@ template <typename Real> int launch_pp(dem_ctx* c, int lst, int slot, int sb, in
         planes<double>(c->wh, np), planes<double>(c->hist[lst][hp], c->cap),
         planes<double>(c->hist[lst][1 - hp], c->cap), pp, pw, particle_common(c, slot), (Real)dt, (Real)(1.0 / dt),
         (Real)c->cfg.density, partials(c, slot), c->words, c->record ? c->dbgF : nullptr,
-        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, (size_t)c->nblk, c->npart));
+        c->record ? c->dbgT : nullptr, c->record ? c->dbgC : nullptr, (size_t)grid_for(n, 256), c->npart));
     return DEM_OK;
 }
 
@@ -2871,9 +2875,10 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
             c->nbatch_max = (np + kBatchMin - 1) / kBatchMin + 1;
         }
     }
-    // partials per slot: particle-kernel blocks, free-kernel blocks, and at
-    // least as many as the window kernel has blocks
-    c->npart = std::max<size_t>(2 * (size_t)c->nblk, c->win_grid);
+    // partials per slot: the particle kernels' (at least as many as the
+    // window kernel has blocks), then the free kernel's
+    c->fpart = std::max<size_t>((size_t)c->nblk, c->win_grid);
+    c->npart = c->fpart + c->nblk;
     if ((rc = dalloc(&c->part_mz, (size_t)cfg->relist_interval * c->npart)) ||
         (rc = dalloc(&c->part_cnt, (size_t)cfg->relist_interval * c->npart)))
         return bail(rc);

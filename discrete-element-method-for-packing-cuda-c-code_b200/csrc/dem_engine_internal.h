@@ -289,7 +289,8 @@ struct dem_ctx {
     unsigned long long* part_mz = nullptr;   // relist_interval x npart
     uint* part_cnt = nullptr;                // relist_interval x npart
     unsigned nblk = 0;                       // blocks of the particle kernel
-    size_t npart = 0;                        // partials per slot: 2 nblk (bound, free)
+    size_t fpart = 0;                        // partials per slot of the particle kernels (>= nblk, window grid)
+    size_t npart = 0;                        // partials per slot: fpart + nblk (the free kernel's)
     unsigned long long* rmax_bits = nullptr;
     void* host_pinned = nullptr;     // mirror for scalars
     // debug force record

@@ -2118,9 +2118,12 @@ __global__ void __launch_bounds__(kWinThreads, 1) k_window_pp(StepArgs<Real> a, 
     clear_partials(part, gridDim.x, npart);
 }
 
+// out[0]: the largest positive radius (its bits), out[2]: nonzero when a
+// radius is not positive (or not a number).
 __global__ void k_rmax(long long n, const double* __restrict__ rad, unsigned long long* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double r = i < n ? rad[i] : 0.0;
+    if (__any_sync(0xffffffffu, i < n && !(r > 0.0)) && lane_id() == 0) atomicOr(out + 2, 1ull);
     unsigned long long b = (unsigned long long)__double_as_longlong(r > 0.0 ? r : 0.0);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -2791,7 +2794,7 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         (rc = dalloc(&c->njli, np)) || (rc = dalloc(&c->off[0], np + 1)) || (rc = dalloc(&c->off[1], np + 1)) ||
         (rc = dalloc(&c->roff, np + 1)) || (rc = dalloc(&c->ln[0], cap)) || (rc = dalloc(&c->ln[1], cap)) ||
         (rc = dalloc(&c->lp, cap)) || (rc = dalloc(&c->rk, cap)) || (rc = dalloc(&c->ru, cap)) || (rc = dalloc(&c->words, 1)) ||
-        (rc = dalloc(&c->rmax_bits, 2)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
+        (rc = dalloc(&c->rmax_bits, 3)) || (rc = dalloc(&c->wslot, np)) || (rc = dalloc(&c->wlist, np)) ||
         (rc = dalloc(&c->wcount, 1)) || (rc = dalloc(&c->arrival, np)) || (rc = dalloc(&c->scr, np * kScr)) ||
         (rc = dalloc(&c->bflag, np)) || (rc = dalloc(&c->bpos, np + 1)) || (rc = dalloc(&c->blist, np)) ||
         (rc = dalloc(&c->flist, np)) || (rc = dalloc(&c->bar, kBarWords)) || (rc = dalloc(&c->tpos, np)))
@@ -2912,6 +2915,8 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
     }
     e = cudaEventCreateWithFlags(&c->ext_ready, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->h2d_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_rad, cudaEventDisableTiming);
     if (e == cudaSuccess) {
         int lo = 0, hi = 0;
         e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
@@ -2949,6 +2954,8 @@ int dem_destroy(dem_ctx* c) {
         if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->ext_ready) cudaEventDestroy(c->ext_ready);
     if (c->h2d_done) cudaEventDestroy(c->h2d_done);
+    if (c->ev_up) cudaEventDestroy(c->ev_up);
+    if (c->ev_rad) cudaEventDestroy(c->ev_rad);
     if (c->evfork) cudaEventDestroy(c->evfork);
     if (c->evjoin) cudaEventDestroy(c->evjoin);
     for (cudaEvent_t e : c->wev) cudaEventDestroy(e);
@@ -3143,45 +3150,39 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
     c->hperm.clear();
     c->hperm_stale = false;
     if (host) {
+        // the radii first, on the second stream (after the context's earlier
+        // work, which may still read the staging buffers): r_max, the solid
+        // volume and the radii's validity on the device while the positions
+        // copy, so that the host waits for 24 bytes instead of reducing them
+        DEM_CUDA_TRY(cudaEventRecord(c->ev_up, c->stream));
+        DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->ev_up, 0));
+        DEM_CUDA_TRY(cudaMemcpyAsync(sr, rad, n * sizeof(double), cudaMemcpyHostToDevice, c->stream2));
+        DEM_CUDA_TRY(cudaMemsetAsync(c->rmax_bits, 0, 3 * sizeof(unsigned long long), c->stream2));
+        k_rmax<<<grid_for(n, 256), 256, 0, c->stream2>>>(n, sr, c->rmax_bits);
+        k_vol<<<1, 1024, 0, c->stream2>>>(n, sr, reinterpret_cast<double*>(c->rmax_bits + 1));
+        DEM_LAUNCH_CHECK();
+        DEM_CUDA_TRY(cudaMemcpyAsync(c->host_pinned, c->rmax_bits, 3 * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, c->stream2));
+        DEM_CUDA_TRY(cudaEventRecord(c->ev_rad, c->stream2));
         DEM_CUDA_TRY(cudaMemcpyAsync(spos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (pdis) DEM_CUDA_TRY(cudaMemcpyAsync(sd, pdis, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (angv) DEM_CUDA_TRY(cudaMemcpyAsync(sa, angv, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        DEM_CUDA_TRY(cudaMemcpyAsync(sr, rad, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_rad, 0));
         // the call returns once the copies have read the caller's buffers
         // (not after the device work that follows them)
         DEM_CUDA_TRY(cudaEventRecord(c->h2d_done, c->stream));
         ppos = spos; ppd = pdis ? sd : nullptr; ppa = angv ? sa : nullptr; prad = sr;
-        // r_max and the solid volume while the copies run: eight interleaved
-        // partial sums (a fixed order, so the same bits every call) keep the
-        // loop off the latency of one serial FP64 chain (0.7 ms at 500K)
-        constexpr int kLanes = 8;
-        double rm[kLanes] = {}, vs[kLanes] = {};
-        bool bad = false;
-        long long i = 0;
-        for (; i + kLanes <= n; i += kLanes) {
-            for (int l = 0; l < kLanes; l++) {
-                const double r = rad[i + l];
-                bad |= !(r > 0.0);
-                rm[l] = std::max(rm[l], r);
-                vs[l] += r * r * r;
-            }
-        }
-        for (int l = 0; i < n; i++, l++) {
-            const double r = rad[i];
-            bad |= !(r > 0.0);
-            rm[l] = std::max(rm[l], r);
-            vs[l] += r * r * r;
-        }
-        if (bad) {
+        DEM_CUDA_TRY(cudaEventSynchronize(c->ev_rad));
+        unsigned long long b[3];
+        memcpy(b, c->host_pinned, sizeof(b));
+        if (b[2]) {
+            DEM_CUDA_TRY(cudaEventSynchronize(c->h2d_done));
             for (long long k = 0; k < n; k++)
                 if (!(rad[k] > 0.0)) return fail(DEM_ERR_ARG, "dem_upload_state: radius %lld not positive", k);
         }
-        double rmx = 0.0, v3 = 0.0;
-        for (int l = 0; l < kLanes; l++) {
-            rmx = std::max(rmx, rm[l]);
-            v3 += vs[l];
-        }
-        c->rmax = rmx;
+        double v3;
+        memcpy(&c->rmax, &b[0], sizeof(double));
+        memcpy(&v3, &b[1], sizeof(double));
         c->vol = 4.0 / 3.0 * M_PI * v3;
         bool cell_ordered = false;
         if (order == kOrderCells && c->reorder) {
@@ -3201,7 +3202,7 @@ static int upload_impl(dem_ctx* c, const double* pos, const double* pdis, const 
         // the caller's buffers may have been written on the legacy stream
         DEM_CUDA_TRY(cudaEventRecord(c->ext_ready, 0));
         DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ext_ready, 0));
-        DEM_CUDA_TRY(cudaMemsetAsync(c->rmax_bits, 0, 2 * sizeof(unsigned long long), c->stream));
+        DEM_CUDA_TRY(cudaMemsetAsync(c->rmax_bits, 0, 3 * sizeof(unsigned long long), c->stream));
         k_rmax<<<grid_for(n, 256), 256, 0, c->stream>>>(n, rad, c->rmax_bits);
         k_vol<<<1, 1024, 0, c->stream>>>(n, rad, reinterpret_cast<double*>(c->rmax_bits + 1));
         DEM_LAUNCH_CHECK();

@@ -182,6 +182,7 @@ struct dem_ctx {
     std::vector<uint> hperm;               // host copy (n), fetched on first use after an upload
     bool hperm_stale = false;              // the device copy is newer than hperm
     cudaEvent_t h2d_done = nullptr;        // a host upload's copies have read the caller's buffers
+    cudaEvent_t ev_up = nullptr, ev_rad = nullptr;   // a host upload: its start; its radii reduced
     int device = 0;
     cudaStream_t stream = 0;
     cudaStream_t own_stream = 0;      // non-blocking; used unless dem_set_stream gives one

@@ -383,6 +383,37 @@ def test_nonfinite_is_reported(dem, wl, cuda):
     assert ei.value.code == dem.DEM_ERR_NONFINITE
 
 
+def test_nonfinite_free_particle_in_a_window_is_reported(dem, wl, cuda):
+    """A free particle's non-finite displacement, stepped through whole
+    windows (its check made once on the window's final state), is reported."""
+    w = wl.small_box(n=2000)
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_material(w.pp, w.pw)
+    pdis = np.zeros(3 * w.n)
+    top = int(np.argmax(w.pos[2::3]))   # the highest sphere: free in the first window
+    pdis[3 * top] = np.inf
+    e.upload(w.pos, w.rad, pdis, None)
+    e.step(w.relist_interval)   # one whole window (its graph), re-listed at finite positions
+    with pytest.raises(dem.DemError) as ei:
+        e.scalars()
+    assert ei.value.code == dem.DEM_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("bad", [0.0, -1e-4, np.nan])
+def test_upload_rejects_a_radius_that_is_not_positive(dem, wl, cuda, bad):
+    w = wl.small_box(n=2000)
+    e = dem.Engine(**w.engine_kwargs())
+    e.set_material(w.pp, w.pw)
+    rad = w.rad.copy()
+    rad[777] = bad
+    with pytest.raises(dem.DemError) as ei:
+        e.upload(w.pos, rad)
+    assert ei.value.code == dem.DEM_ERR_ARG and "777" in str(ei.value)
+    e.upload(w.pos, w.rad)   # the context stays usable
+    e.step(3)
+    assert e.scalars()["status"] == 0
+
+
 def test_partial_windows_equal_graph_windows(dem, wl, cuda):
     """dem_step_n(1) x N (eager launches) and dem_step_n(N) (graphs) agree bit
     for bit."""

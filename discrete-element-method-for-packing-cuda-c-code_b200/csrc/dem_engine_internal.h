@@ -119,10 +119,13 @@ struct ParticleCommon {
 // blocks), at least kBatchMin and at most P minus the largest component.
 constexpr uint kBatchMin = 32;
 constexpr uint kDenseSkip = 32;          // re-lists without the component pass after one larger than a block
-constexpr int kBatchThreads = 512;       // k_batch: one particle per thread
+// Blocks of 256 threads holding up to 256 (FP64: 192) particles and 320
+// pairs: three (FP64: two) resident per SM, so that one block's barrier
+// waits overlap another's steps.
+constexpr int kBatchThreads = 256;       // k_batch: one particle per thread
 template <typename Real> struct BatchCap;
-template <> struct BatchCap<float> { static constexpr uint P = 512, Q = 640; };
-template <> struct BatchCap<double> { static constexpr uint P = 384, Q = 640; };
+template <> struct BatchCap<float> { static constexpr uint P = 256, Q = 320; };
+template <> struct BatchCap<double> { static constexpr uint P = 192, Q = 320; };
 
 // Exclusive scan of in[0, m) into out over the block (m <= a few thousand);
 // returns the total to every thread.  tmp: 33 words of shared memory.

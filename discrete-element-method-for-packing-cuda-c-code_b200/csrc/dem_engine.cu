@@ -2322,17 +2322,20 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         c->words, c->lb, c->off[dst], c->roff, c->bpos, c->blist, c->flist, cc ? c->cc_words : nullptr, c->cc_bw,
         (long long)c->nbatch_max + 2);
     DEM_LAUNCH_CHECK();
-    if (c->free_early) {
-        // a batched window follows: its free particles need nothing of the
-        // re-list after the free list, and the passes after this one touch
-        // bound particles only, so they step the whole window now, beside
-        // the rest of the re-list (joined at the window's end)
+    // a batched window follows: its free particles need nothing of the
+    // re-list after the free list, and the passes after the candidate pass
+    // touch bound particles only, so they step the whole window from here,
+    // beside the rest of the re-list (joined at the window's end); the fork
+    // comes after the candidate pass (free_fork 1) or after the fill (2)
+    auto fork_free = [&]() -> int {
         DEM_CUDA_TRY(cudaEventRecord(c->evfork, s));
         DEM_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->evfork, 0));
-        rc = launch_free<Real>(c, dst, 0, c->cfg.relist_interval, c->stream2, 1);
-        if (rc) return rc;
+        const int frc = launch_free<Real>(c, dst, 0, c->cfg.relist_interval, c->stream2, 1);
+        if (frc) return frc;
         DEM_CUDA_TRY(cudaEventRecord(c->evjoin, c->stream2));
-    }
+        return DEM_OK;
+    };
+    if (c->free_early && c->free_fork == 1 && (rc = fork_free())) return rc;
     const unsigned BG = c->bound_grid;
     DEM_CUDA_TRY(launch_ex(
         k_nbr_fill<Real>, BG, B, s, pdl, n, S, (const Real*)c->rad, g, skin, (const uint*)c->coff,
@@ -2341,6 +2344,7 @@ template <typename Real> int launch_relist(dem_ctx* c, int src) {
         (const uint*)c->ln[src], planes<double>(c->hist[src][c->hph], c->cap), c->rk, (R4<Real>*)c->pf, c->cap,
         c->words, c->carry, (const uint*)c->scr, cc ? c->cc_parent : nullptr, (const uint*)c->bpos,
         (const uint*)c->blist, (const uint*)c->cc_skip, c->lb, (long long)lb_words(c->npad)));
+    if (c->free_early && c->free_fork == 2 && (rc = fork_free())) return rc;
     DEM_CUDA_TRY(launch_ex(k_rev_sort, BG, B, s, pdl, n, (const uint*)c->roff, c->rk, c->ru,
                            (const uint*)c->off[dst], c->cap, cc ? c->cc_parent : nullptr, (const uint*)c->bpos,
                            (const uint*)c->blist, c->cc_size, c->cc_pairs, (const uint*)c->cc_skip, c->cc_words));
@@ -2603,7 +2607,7 @@ int enqueue_window(dem_ctx* c, int src) {
     const bool wt = c->wtiming_capture;
     if (wt) DEM_CUDA_TRY(cudaEventRecordWithFlags(c->wev[0], c->stream, cudaEventRecordExternal));
     // a batched window: the free particles start inside the re-list
-    c->free_early = c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel && use_batches(c);
+    c->free_early = c->free_fork > 0 && c->mode == DEM_FORCE_PCCP && !c->record && c->win_kernel && use_batches(c);
     c->observe_slot = K - 1;
     int rc = relist(c, src);
     if (rc) { c->free_early = false; return rc; }
@@ -2855,6 +2859,10 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         c->outer_cond = !(oc && oc[0] == '0');
         const char* pdl = getenv("DEM_B200_PDL");   // "0": plain launches everywhere
         c->pdl = !(pdl && pdl[0] == '0');
+        // where a batched window's free particles start: "0" in the window,
+        // "1" (default) after the re-list's candidate pass, "2" after its fill
+        const char* ff = getenv("DEM_B200_FREE_FORK");
+        c->free_fork = (ff && (ff[0] == '0' || ff[0] == '2')) ? ff[0] - '0' : 1;
         const char* ro = getenv("DEM_B200_REORDER");   // "0": keep the caller's particle order
         c->reorder = !(ro && ro[0] == '0');
         const char* sp = getenv("DEM_B200_SPLIT");   // window kernels' bound items per thread (0: no split)

@@ -243,6 +243,7 @@ struct dem_ctx {
     int prio_hi = 0;                 // the device's highest stream priority (the batch kernel's launches)
     bool free_in_window = false;     // capturing: the free particles run as one window kernel
     bool free_early = false;         // enqueueing a batched window: the re-list forks its free particles
+    int free_fork = 1;               // where (DEM_B200_FREE_FORK): 0 in the window, 1 after the candidate pass, 2 after the fill
     uint* bar = nullptr;             // window-kernel grid barrier: [0] arrival counter
     unsigned win_grid = 1;           // window-kernel blocks (all co-resident)
     bool win_kernel = true;          // whole PCCP windows as one cooperative launch

@@ -522,6 +522,37 @@ def test_cluster_batches_equal_grid_barrier_window(dem, wl, cuda, monkeypatch, p
         b.close()
 
 
+@pytest.mark.parametrize("fork", ["0", "2"])
+def test_free_particles_fork_point_is_invisible(dem, wl, cuda, monkeypatch, fork):
+    """A batched window's free particles stepped from the re-list's second
+    stream after the candidate pass (the default), after the fill
+    (DEM_B200_FREE_FORK=2) or in the window beside the batches
+    (DEM_B200_FREE_FORK=0): the same states, lists and observables, on a
+    sparse bed (batched) and a dense lattice (the grid-barrier window kernel
+    beside the free kernel)."""
+    from _cases import dense_lattice
+    for w in (wl.small_box(n=3000), dense_lattice(dem, nx=10, ny=10, nz=8)):
+        rng = np.random.default_rng(5)
+        pdis = rng.normal(0, 2e-6, 3 * w.n)
+        a = make_engine(dem, w)
+        a.upload(w.pos, w.rad, pdis, None)
+        monkeypatch.setenv("DEM_B200_FREE_FORK", fork)
+        b = make_engine(dem, w)
+        b.upload(w.pos, w.rad, pdis, None)
+        monkeypatch.delenv("DEM_B200_FREE_FORK")
+        a.step(6 * w.relist_interval)
+        b.step(6 * w.relist_interval)
+        assert a.window_work() == b.window_work()
+        for x, y in zip(a.download(), b.download()):
+            np.testing.assert_array_equal(x, y)
+        for x, y in zip(a.pairs(), b.pairs()):
+            np.testing.assert_array_equal(x, y)
+        sa, sb = a.scalars(), b.scalars()
+        assert sa["maxhz"] == sb["maxhz"] and sa["contacts"] == sb["contacts"] and sa["pairs"] == sb["pairs"]
+        a.close()
+        b.close()
+
+
 def test_plain_launches_equal_programmatic_launches(dem, wl, cuda, monkeypatch):
     """Re-list and step kernels launched programmatically (the default) and
     launched plainly (DEM_B200_PDL=0) agree bit for bit, with the per-step

@@ -439,8 +439,9 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
     """bed_500k: the 500,000 spheres compacted into a bed (velocity
     proportional to height, then gravity) and settled on the GPU, untimed;
     then windows of the production cadence on it, timed: the mixed form (the
-    default force mode, with the window kernel's time and roofline) and the
-    FP64 plain form, with the bed's pairs, contacts and packing fraction."""
+    default force mode, with the window kernel's time and roofline), the
+    FP64 plain form and the mixed particle-parallel (PP) form, with the bed's
+    pairs, contacts and packing fraction."""
     import dem_b200.workloads as wmod
     t0 = time.perf_counter()
     w0 = wmod.bed_500k_initial()
@@ -462,10 +463,11 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
     out = {"workload": w.name, "n_particles": w.n, "box_mm": list(w.world),
            "init": w.meta["init"], "settle_steps": w.meta["settle_steps"], "settle_s": settle_s,
            "settle_status": w.meta["settled"]["status"]}
-    for prec, key in ((dem.PREC_MIXED, "mixed"), (dem.PREC_FP64, "fp64")):
+    for prec, key, fm in ((dem.PREC_MIXED, "mixed", dem.FORCE_PCCP), (dem.PREC_FP64, "fp64", dem.FORCE_PCCP),
+                          (dem.PREC_MIXED, "mixed_pp", dem.FORCE_PP)):
         if key not in args.bed_precisions.split(","):
             continue
-        e = dem.Engine(**{**w.engine_kwargs(), "precision": prec})
+        e = dem.Engine(**{**w.engine_kwargs(), "precision": prec, "force_mode": fm})
         e.set_stream(stream.cuda_stream)
         e.set_material(w.pp, w.pw)
         e.upload(w.pos, w.rad, pdis, angv)
@@ -480,13 +482,13 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
         s = e.scalars(raise_on_status=False)
         ncells = e.grid_info()[2]
         e.close()
-        bp = BYTES_PER_PARTICLE[key]
+        bp = BYTES_PER_PARTICLE[key.split("_")[0]]
         kbytes, rbytes = window_bytes(w.n, work, win, bp, ncells)
         r = {"value": w.n * kb * win / (ms / 1e3), "unit": UNIT, "windows": kb, "ms_per_dem_step": ms / (kb * win),
              "pairs_per_particle": s["pairs"] / w.n, "contacts_per_particle": s["contacts"] / w.n,
              "mean_cn": s["mean_cn"], "packing_fraction": s["packing_fraction"], "status": s["status"],
              "window_work": work, "kernel_ms": kt}
-        if kt["window_kernel_ms"] > 0:
+        if kt["window_kernel_ms"] > 0 and fm == dem.FORCE_PCCP:
             r["roofline"] = roofline("k_window", kbytes, kt["window_kernel_ms"], peak, peak_kind, w.name,
                                      traffic=profile_traffic(f"k_window_bed500k_{key}"),
                                      note="every sphere bound: B_p x 20 per sphere + 56 B x 20 per pair")
@@ -494,6 +496,8 @@ def settled_bed(dem, torch, stream, flush, args, peak, peak_kind):
         out[key] = r
     if "mixed" in out and "fp64" in out:
         out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if "mixed" in out and "mixed_pp" in out:   # the particle-parallel force mode on the same bed
+        out["pp_over_pccp"] = out["mixed_pp"]["value"] / out["mixed"]["value"]
     out["roofline"] = out.get("mixed", {}).get("roofline")
     return out
 
@@ -692,7 +696,8 @@ def main():
     ap.add_argument("--bed-windows", type=int, default=10)
     ap.add_argument("--bed-save", default="", help="save the settled bed (npz) for later --bed-load runs")
     ap.add_argument("--bed-load", default="", help="time a bed saved by --bed-save instead of settling one")
-    ap.add_argument("--bed-precisions", default="mixed,fp64", help="bed rows to time (mixed, fp64)")
+    ap.add_argument("--bed-precisions", default="mixed,fp64,mixed_pp",
+                    help="bed rows to time (mixed, fp64; mixed_pp: the particle-parallel force mode)")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

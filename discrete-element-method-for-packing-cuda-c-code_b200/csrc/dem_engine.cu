@@ -1585,8 +1585,8 @@ __device__ __forceinline__ void free_sweep(const StepArgs<Real>& a, const PRec<R
     }
 }
 
-template <typename Real>
-__global__ void __launch_bounds__(kWinThreads, 1) k_window(StepArgs<Real> a, int K, StepPartials part, size_t npart,
+template <typename Real, int MINB>
+__global__ void __launch_bounds__(kWinThreads, MINB) k_window(StepArgs<Real> a, int K, StepPartials part, size_t npart,
                                                            uint* bar) {
     if (a.batch && !a.ccw[1]) return;   // the cluster batches (k_batch) step this window
     uint nbar = 0;
@@ -2428,6 +2428,10 @@ template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nst
     return DEM_OK;
 }
 
+// The window kernel's instance: one block per SM (up to 128 registers), or
+// two (64 registers, with spills; DEM_B200_WINDOW_MINB=2).
+template <typename Real> auto window_fn(int minb) { return minb == 2 ? k_window<Real, 2> : k_window<Real, 1>; }
+
 // The window kernel: all K steps of the window in one cooperative launch.
 template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape* tape, int batch = 0) {
     const int K = c->cfg.relist_interval;
@@ -2452,7 +2456,7 @@ template <typename Real> int launch_window(dem_ctx* c, int lst, const WindowTape
     cfg.attrs = at;
     cfg.numAttrs = 1;
     // a batched window's kernel leaves the free particles' partials to k_free_run
-    DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_window<Real>, a, K, partials(c, K - 1),
+    DEM_CUDA_TRY(cudaLaunchKernelEx(&cfg, window_fn<Real>(c->win_minb), a, K, partials(c, K - 1),
                                     batch ? (size_t)c->fpart : c->npart, c->bar));
     return DEM_OK;
 }
@@ -2839,9 +2843,13 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
         if (c->mode == DEM_FORCE_PP)
             e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window_pp<float>, kWinThreads, 0)
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window_pp<double>, kWinThreads, 0);
-        else
-            e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<float>, kWinThreads, 0)
-                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window<double>, kWinThreads, 0);
+        else {
+            const char* wm = getenv("DEM_B200_WINDOW_MINB");   // "2": two window-kernel blocks per SM
+            c->win_minb = (wm && wm[0] == '2') ? 2 : 1;
+            e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, window_fn<float>(c->win_minb), kWinThreads, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, window_fn<double>(c->win_minb), kWinThreads,
+                                                                   0);
+        }
         if (e != cudaSuccess) return bail(cuda_fail(e, "window kernel occupancy", __FILE__, __LINE__));
         int coop = 0;
         e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);

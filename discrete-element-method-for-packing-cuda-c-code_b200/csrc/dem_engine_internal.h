@@ -241,6 +241,7 @@ struct dem_ctx {
     cudaStream_t stream2 = 0;        // free-particle branch of the window graph
     cudaEvent_t evfork = nullptr, evjoin = nullptr;
     int prio_hi = 0;                 // the device's highest stream priority (the batch kernel's launches)
+    int win_minb = 1;                // window-kernel blocks per SM (DEM_B200_WINDOW_MINB)
     bool free_in_window = false;     // capturing: the free particles run as one window kernel
     bool free_early = false;         // enqueueing a batched window: the re-list forks its free particles
     int free_fork = 1;               // where (DEM_B200_FREE_FORK): 0 in the window, 1 after the candidate pass, 2 after the fill

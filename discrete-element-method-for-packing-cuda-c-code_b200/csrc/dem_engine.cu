@@ -2429,7 +2429,7 @@ template <typename Real> int launch_free(dem_ctx* c, int lst, int slot0, int nst
 }
 
 // The window kernel's instance: one block per SM (up to 128 registers), or
-// two (64 registers, with spills; DEM_B200_WINDOW_MINB=2).
+// two (64 registers, with spills).
 template <typename Real> auto window_fn(int minb) { return minb == 2 ? k_window<Real, 2> : k_window<Real, 1>; }
 
 // The window kernel: all K steps of the window in one cooperative launch.
@@ -2844,8 +2844,11 @@ int dem_create(const dem_config* cfg, dem_ctx** out) {
             e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window_pp<float>, kWinThreads, 0)
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, k_window_pp<double>, kWinThreads, 0);
         else {
-            const char* wm = getenv("DEM_B200_WINDOW_MINB");   // "2": two window-kernel blocks per SM
-            c->win_minb = (wm && wm[0] == '2') ? 2 : 1;
+            // window-kernel blocks per SM: two in the mixed form (64 registers;
+            // the settled 500,000-sphere bed 7.5 % faster), one in FP64 (its
+            // spills at 64 made it 5 % slower); DEM_B200_WINDOW_MINB=1|2 overrides
+            const char* wm = getenv("DEM_B200_WINDOW_MINB");
+            c->win_minb = (wm && (wm[0] == '1' || wm[0] == '2')) ? wm[0] - '0' : (mx ? 2 : 1);
             e = mx ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, window_fn<float>(c->win_minb), kWinThreads, 0)
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wper, window_fn<double>(c->win_minb), kWinThreads,
                                                                    0);

@@ -45,7 +45,7 @@ extern "C" {
 #define DEM_ERR_SKIN        5  /* a particle moved more than skin/2 inside a window */
 #define DEM_ERR_IO          6  /* deck / output file error                          */
 #define DEM_ERR_STATE       7  /* call out of order (e.g. step before upload)       */
-#define DEM_ERR_TIMEOUT     8  /* a bounded device-side wait ran out (window kernel) */
+#define DEM_ERR_TIMEOUT     8  /* a bounded device-side wait ran out (window kernel's grid barrier, re-list scans) */
 
 /* Text of the last error raised on the calling host thread. */
 const char* dem_last_error_string(void);
